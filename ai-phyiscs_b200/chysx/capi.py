@@ -1,0 +1,211 @@
+"""ctypes binding of the C ABI (include/chysx_cloth.h).
+
+This is the binding a ctypes-based host (or a test) uses to drive the
+library without the pybind11 facade; it loads the same in-tree
+``libchysx_cloth.so`` the facade links.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libchysx_cloth.so")
+
+OK, ERR_INVALID_ARGUMENT, ERR_OUT_OF_RANGE, ERR_RUNTIME, ERR_CUDA = range(5)
+SOLVE_CONVERGED, SOLVE_MAX_ITER, SOLVE_NONFINITE = range(3)
+WARM = {"zero": 0, "previous": 1, "learned": 2}
+
+u = ctypes.c_uint64
+i32p = ctypes.POINTER(ctypes.c_int32)
+f32p = ctypes.POINTER(ctypes.c_float)
+ip = ctypes.POINTER(ctypes.c_int)
+dp = ctypes.POINTER(ctypes.c_double)
+H = ctypes.c_void_p
+
+
+class Material(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_float) for n in
+                ("lame_mu", "lame_lambda", "bending", "density", "damping", "gx", "gy", "gz")]
+
+
+# name -> (restype, argtypes); every symbol include/chysx_cloth.h declares
+SIGNATURES = {
+    "chysx_last_error": (ctypes.c_char_p, []),
+    "chysx_cloth_create": (ctypes.c_int, [ctypes.POINTER(H)]),
+    "chysx_cloth_destroy": (ctypes.c_int, [H]),
+    "chysx_cloth_set_material": (ctypes.c_int, [H, ctypes.POINTER(Material)]),
+    "chysx_cloth_get_material": (ctypes.c_int, [H, ctypes.POINTER(Material)]),
+    "chysx_cloth_set_external_buffers": (ctypes.c_int, [H, u, u, ctypes.c_int, u, u]),
+    "chysx_cloth_set_mesh": (ctypes.c_int, [H, i32p, ctypes.c_int]),
+    "chysx_cloth_num_edges": (ctypes.c_int, [H, ip]),
+    "chysx_cloth_get_edges": (ctypes.c_int, [H, i32p]),
+    "chysx_cloth_set_pins": (ctypes.c_int, [H, i32p, f32p, ctypes.c_int, ctypes.c_float]),
+    "chysx_cloth_clear_pins": (ctypes.c_int, [H]),
+    "chysx_cloth_num_pins": (ctypes.c_int, [H, ip]),
+    "chysx_cloth_update_pin_targets": (ctypes.c_int, [H, f32p, ctypes.c_int, u]),
+    "chysx_cloth_build_springs": (ctypes.c_int, [H, ctypes.c_float, f32p, u]),
+    "chysx_cloth_num_springs": (ctypes.c_int, [H, ip]),
+    "chysx_cloth_build_fem_stretch": (ctypes.c_int, [H, ctypes.c_float, f32p, u]),
+    "chysx_cloth_redistribute_mass": (ctypes.c_int, [H, ctypes.c_float, u, ctypes.c_int, u]),
+    "chysx_cloth_set_pcg_iterations": (ctypes.c_int, [H, ctypes.c_int]),
+    "chysx_cloth_pcg_iterations": (ctypes.c_int, [H, ip]),
+    "chysx_cloth_set_solver": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_double, ctypes.c_int]),
+    "chysx_cloth_set_options": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int, ctypes.c_float]),
+    "chysx_cloth_step": (ctypes.c_int, [H, ctypes.c_float, u]),
+    "chysx_cloth_last_stats": (ctypes.c_int, [H, ip, dp, ip]),
+    "chysx_cloth_num_particles": (ctypes.c_int, [H, ip]),
+    "chysx_cloth_num_off_diag_blocks": (ctypes.c_int, [H, ip]),
+    "chysx_cloth_debug_dump": (ctypes.c_int, [H, f32p, i32p, i32p, f32p, f32p, f32p]),
+    "chysx_topology_pattern": (ctypes.c_int, [ctypes.c_int, i32p, ctypes.c_int, i32p, ctypes.c_int,
+                                              i32p, i32p, ctypes.c_int, ip, ip, ip]),
+}
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with ai-phyiscs_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class ChysxError(RuntimeError):
+    pass
+
+
+def check(rc: int) -> None:
+    if rc == OK:
+        return
+    msg = lib().chysx_last_error().decode()
+    if rc == ERR_INVALID_ARGUMENT:
+        raise ValueError(msg)
+    if rc == ERR_OUT_OF_RANGE:
+        raise IndexError(msg)
+    raise ChysxError(msg)
+
+
+def _p(a, t):
+    return ctypes.cast(None, t) if a is None else a.ctypes.data_as(t)
+
+
+class Cloth:
+    """Thin object wrapper over the C ABI handle."""
+
+    def __init__(self):
+        self._L = lib()
+        h = H()
+        check(self._L.chysx_cloth_create(ctypes.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self._L.chysx_cloth_destroy(self.h)
+            self.h = None
+
+    def set_material(self, density=0.05, damping=0.0, gravity=(0.0, 0.0, -9.81)):
+        m = Material(0.0, 0.0, 0.0, density, damping, *gravity)
+        check(self._L.chysx_cloth_set_material(self.h, ctypes.byref(m)))
+
+    def set_external_buffers(self, pos, vel, n, inv_mass=0, force=0):
+        check(self._L.chysx_cloth_set_external_buffers(self.h, pos, vel, n, inv_mass, force))
+
+    def set_mesh(self, tris):
+        t = np.ascontiguousarray(tris, np.int32)
+        check(self._L.chysx_cloth_set_mesh(self.h, _p(t, i32p), t.shape[0]))
+
+    def edges(self):
+        n = ctypes.c_int()
+        check(self._L.chysx_cloth_num_edges(self.h, ctypes.byref(n)))
+        out = np.zeros((n.value, 2), np.int32)
+        check(self._L.chysx_cloth_get_edges(self.h, _p(out, i32p)))
+        return out
+
+    def set_pins(self, idx, targets, k=1.0e6):
+        i = np.ascontiguousarray(idx, np.int32)
+        t = np.ascontiguousarray(targets, np.float32)
+        check(self._L.chysx_cloth_set_pins(self.h, _p(i, i32p), _p(t, f32p), i.shape[0], k))
+
+    def num_pins(self):
+        n = ctypes.c_int()
+        check(self._L.chysx_cloth_num_pins(self.h, ctypes.byref(n)))
+        return n.value
+
+    def update_pin_targets(self, targets, stream=0):
+        t = np.ascontiguousarray(targets, np.float32)
+        check(self._L.chysx_cloth_update_pin_targets(self.h, _p(t, f32p), t.shape[0], stream))
+
+    def build_springs(self, k, stream=0):
+        if np.ndim(k):
+            ke = np.ascontiguousarray(k, np.float32)
+            check(self._L.chysx_cloth_build_springs(self.h, 0.0, _p(ke, f32p), stream))
+        else:
+            check(self._L.chysx_cloth_build_springs(self.h, float(k), _p(None, f32p), stream))
+
+    def build_fem_stretch(self, k, stream=0):
+        if np.ndim(k):
+            kt = np.ascontiguousarray(k, np.float32)
+            check(self._L.chysx_cloth_build_fem_stretch(self.h, 0.0, _p(kt, f32p), stream))
+        else:
+            check(self._L.chysx_cloth_build_fem_stretch(self.h, float(k), _p(None, f32p), stream))
+
+    def redistribute_mass(self, density, inv_mass_ptr, n, stream=0):
+        check(self._L.chysx_cloth_redistribute_mass(self.h, density, inv_mass_ptr, n, stream))
+
+    def set_solver(self, max_iter=50, rel_tol=0.0, warm_start="previous"):
+        check(self._L.chysx_cloth_set_solver(self.h, max_iter, rel_tol, WARM[warm_start]))
+
+    def set_pcg_iterations(self, m):
+        check(self._L.chysx_cloth_set_pcg_iterations(self.h, m))
+
+    def set_options(self, springs_in_step=True, apply_external_force=False, fem_det_eps=1.0e-6):
+        check(self._L.chysx_cloth_set_options(self.h, int(springs_in_step), int(apply_external_force),
+                                              fem_det_eps))
+
+    def step(self, dt, stream=0):
+        check(self._L.chysx_cloth_step(self.h, dt, stream))
+
+    def last_stats(self):
+        it, st = ctypes.c_int(), ctypes.c_int()
+        rr = ctypes.c_double()
+        check(self._L.chysx_cloth_last_stats(self.h, ctypes.byref(it), ctypes.byref(rr), ctypes.byref(st)))
+        return it.value, rr.value, st.value
+
+    def debug_dump(self):
+        n, nnz = ctypes.c_int(), ctypes.c_int()
+        check(self._L.chysx_cloth_num_particles(self.h, ctypes.byref(n)))
+        check(self._L.chysx_cloth_num_off_diag_blocks(self.h, ctypes.byref(nnz)))
+        n, nnz = n.value, nnz.value
+        diag = np.zeros((n, 3, 3), np.float32)
+        rp = np.zeros(n + 1, np.int32)
+        col = np.zeros(max(nnz, 1), np.int32)
+        vals = np.zeros((max(nnz, 1), 3, 3), np.float32)
+        rhs = np.zeros((n, 3), np.float32)
+        dx = np.zeros((n, 3), np.float32)
+        check(self._L.chysx_cloth_debug_dump(self.h, _p(diag, f32p), _p(rp, i32p), _p(col, i32p),
+                                             _p(vals, f32p), _p(rhs, f32p), _p(dx, f32p)))
+        return diag, rp, col[:nnz], vals[:nnz], rhs, dx
+
+
+def topology_pattern(n, tris, edges=None):
+    """Host-only: (row_offsets, col_indices, ell_entries, max_width) of the
+    off-diagonal block pattern for a mesh (+ spring edges)."""
+    t = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+    e = np.zeros((0, 2), np.int32) if edges is None else np.ascontiguousarray(edges, np.int32).reshape(-1, 2)
+    rp = np.zeros(n + 1, np.int32)
+    cap = 6 * t.shape[0] + 2 * e.shape[0] + 1
+    col = np.zeros(cap, np.int32)
+    nnz, ell, w = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    check(lib().chysx_topology_pattern(n, _p(t, i32p), t.shape[0], _p(e, i32p), e.shape[0], _p(rp, i32p),
+                                       _p(col, i32p), cap, ctypes.byref(nnz), ctypes.byref(ell), ctypes.byref(w)))
+    return rp, col[:nnz.value], ell.value, w.value

@@ -1,0 +1,699 @@
+// Device kernels of the B200-native implicit cloth step.
+//
+// Data layout in HBM (all owned by the simulator unless noted):
+//   caller's pos / vel / inv_mass / force : float3 AoS (12 B), borrowed
+//   b, r, z, x(=dx), Ap, p0, p1           : float4 per row (16-B vector loads,
+//                                           .w unused), rows padded to 32
+//   diag, minv                            : symmetric 3x3 blocks as 6 planes
+//                                           per 32-row slice (xx,xy,xz,yy,yz,zz)
+//   col, val                              : sliced ELL (see topology.h); val
+//                                           holds 6 planes per entry column
+// Every Hessian block of this path is symmetric (pin kI, spring H_blk,
+// Baraff-Witkin blocks c_a c_b M_u + d_a d_b M_v, inertia), so a block is
+// stored as 6 floats (24 B) instead of the reference's 9 (36 B).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace chysx_b200 {
+
+constexpr int kWarp = 32;
+
+// ---------------------------------------------------------------------------
+// Views passed by value to kernels
+// ---------------------------------------------------------------------------
+struct DevTopo {
+    int n;
+    int n_slices;
+    const int* __restrict__ slice_off;
+    const int* __restrict__ col;
+    float* val;
+    float* diag;
+    float* minv;
+    const int* __restrict__ tinc_off;
+    const int* __restrict__ tinc;
+    const unsigned* __restrict__ tinc_meta;
+    const int* __restrict__ sinc_off;
+    const int* __restrict__ sinc;
+    const unsigned* __restrict__ sinc_meta;
+    const int* __restrict__ pin_off;
+    const int* __restrict__ pin_row;
+    const float* __restrict__ pin_tgt;  // 3 floats per sorted pin
+};
+
+struct ElemData {
+    const int* __restrict__ tris;      // 3 per triangle
+    const float4* __restrict__ dminv;  // row-major 2x2 (Mat2f layout)
+    const float* __restrict__ area;
+    const float* __restrict__ ktri;
+    const int* __restrict__ edges;     // 2 per edge
+    const float* __restrict__ rest;
+    const float* __restrict__ kedge;
+    float pin_k;
+    int use_tris;
+    int use_springs;
+};
+
+struct StepArgs {
+    float* pos;
+    float* vel;
+    const float* inv_mass;
+    const float* force;
+    int n;
+    float dt;
+    float gx, gy, gz;
+    float damping;
+    int apply_force;
+};
+
+struct Vecs {
+    float4* b;
+    float4* r;
+    float4* z;
+    float4* x;
+    float4* ap;
+    float4* p0;
+    float4* p1;
+};
+
+struct SolverCfg {
+    int max_iter;
+    int use_tol;
+    double rel_tol;
+};
+
+// Device-resident solver scalars.  Written only by the single "last block"
+// of each grid reduction, read by every block of the next kernel.
+struct SolveState {
+    double rho, sigma, rr, bb, tol2, rr0;
+    double alpha, beta;
+    float alpha_f, beta_f;
+    int iter, max_iter, done, status, use_tol, fallback;
+    unsigned counter[4];
+};
+
+enum : int { kSolveConverged = 0, kSolveMaxIter = 1, kSolveNonfinite = 2 };
+
+// ---------------------------------------------------------------------------
+// Small math
+// ---------------------------------------------------------------------------
+struct S6 {
+    float xx, xy, xz, yy, yz, zz;
+};
+
+__device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float len3(float3 a) { return sqrtf(dot3(a, a)); }
+__device__ __forceinline__ float3 ld3(const float* p, int i) {
+    const float* q = p + 3 * (size_t)i;
+    return f3(q[0], q[1], q[2]);
+}
+__device__ __forceinline__ void st3(float* p, int i, float3 v) {
+    float* q = p + 3 * (size_t)i;
+    q[0] = v.x; q[1] = v.y; q[2] = v.z;
+}
+__device__ __forceinline__ float3 xyz(float4 v) { return f3(v.x, v.y, v.z); }
+__device__ __forceinline__ float4 f4(float3 v) { return make_float4(v.x, v.y, v.z, 0.f); }
+
+__device__ __forceinline__ float3 mul(const S6& a, float3 v) {
+    return f3(a.xx * v.x + a.xy * v.y + a.xz * v.z,
+              a.xy * v.x + a.yy * v.y + a.yz * v.z,
+              a.xz * v.x + a.yz * v.y + a.zz * v.z);
+}
+__device__ __forceinline__ void axpy6(S6& d, float s, const S6& a) {
+    d.xx += s * a.xx; d.xy += s * a.xy; d.xz += s * a.xz;
+    d.yy += s * a.yy; d.yz += s * a.yz; d.zz += s * a.zz;
+}
+// Adjugate inverse (no determinant guard), the symmetric specialisation of
+// math::inverse(Mat3f) (src/math/matrix.cuh:219-235).
+__device__ __forceinline__ S6 inverse6(const S6& m) {
+    const float a00 = m.yy * m.zz - m.yz * m.yz;
+    const float a01 = -m.xy * m.zz + m.xz * m.yz;
+    const float a02 = m.xy * m.yz - m.xz * m.yy;
+    const float a11 = m.xx * m.zz - m.xz * m.xz;
+    const float a12 = -m.xx * m.yz + m.xz * m.xy;
+    const float a22 = m.xx * m.yy - m.xy * m.xy;
+    const float det = m.xx * a00 + m.xy * a01 + m.xz * a02;
+    const float inv = 1.0f / det;
+    return S6{a00 * inv, a01 * inv, a02 * inv, a11 * inv, a12 * inv, a22 * inv};
+}
+// 6 planes strided by 32 floats (one slice).
+__device__ __forceinline__ S6 ld6(const float* p) {
+    return S6{p[0], p[32], p[64], p[96], p[128], p[160]};
+}
+__device__ __forceinline__ void st6(float* p, const S6& a) {
+    p[0] = a.xx; p[32] = a.xy; p[64] = a.xz; p[96] = a.yy; p[128] = a.yz; p[160] = a.zz;
+}
+
+// ---------------------------------------------------------------------------
+// Single-pass deterministic grid reduction of NV doubles.  Each block writes
+// its partial, the last block to arrive (atomic ticket, no waiting) sums the
+// partials in block order and returns true with the totals in `out`.
+// ---------------------------------------------------------------------------
+template <int BLOCK, int NV>
+__device__ __forceinline__ bool grid_reduce(double (&v)[NV], double* __restrict__ part,
+                                            unsigned* counter, double (&out)[NV]) {
+    constexpr int W = BLOCK / 32;
+    __shared__ double sred[NV][W];
+    __shared__ int s_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double x = v[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sred[q][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double s = 0.0;
+#pragma unroll
+            for (int w = 0; w < W; ++w) s += sred[q][w];
+            part[(size_t)blockIdx.x * NV + q] = s;
+        }
+        __threadfence();
+        // wraps to 0 after the last ticket, so the counter is ready for the
+        // next launch without a reset (and self-heals if it was ever dirty)
+        const unsigned prev = atomicInc(counter, gridDim.x - 1);
+        s_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+    double acc[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += BLOCK) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[q] += __ldcg(part + (size_t)b * NV + q);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double x = acc[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sred[q][warp] = x;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) s += sred[q][w];
+        out[q] = s;
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool finite_d(double x) { return isfinite(x); }
+
+// ---------------------------------------------------------------------------
+// Element physics (FP32, same formulas as the reference kernels)
+// ---------------------------------------------------------------------------
+
+// Spring contribution to row `end` (0: row is edges[e].x, 1: row is .y).
+// Gradient: spring_constraint.cu:76-103; block: spring_constraint.cu:110-151.
+__device__ __forceinline__ void spring_row(const ElemData& el, const float* pos, int e, int end,
+                                           float3& g, S6& blk) {
+    const int ia = el.edges[2 * e], ib = el.edges[2 * e + 1];
+    const float3 d = ld3(pos, ia) - ld3(pos, ib);
+    float l = len3(d);
+    if (l < 1.0e-6f) l = 1.0e-6f;
+    const float inv_l = 1.0f / l;
+    const float3 dh = d * inv_l;
+    const float k = el.kedge[e];
+    const float L = el.rest[e];
+    const float3 gv = dh * (k * (l - L));
+    g = end == 0 ? g + gv : g - gv;
+    const float a = k * L * inv_l;
+    const float diag_term = (l < L) ? 0.0f : (k - a);
+    blk = S6{diag_term + a * dh.x * dh.x, a * dh.x * dh.y, a * dh.x * dh.z,
+             diag_term + a * dh.y * dh.y, a * dh.y * dh.z, diag_term + a * dh.z * dh.z};
+}
+
+// Baraff-Witkin stretch of triangle t seen from its local vertex `la`:
+// gradient triangle_stretch_constraint.cu:153-217, Hessian :231-311 written
+// as H_ab = dwu_a dwu_b Mu + dwv_a dwv_b Mv with
+//   Mu = k_eff (u u^T + [cu > 0] cu/lu (I - u u^T)), Mv likewise.
+struct TriRow {
+    float3 g;       // gradient at the row's vertex
+    S6 Mu, Mv;
+    float du[3], dv[3];
+};
+
+__device__ __forceinline__ void tri_row(const ElemData& el, const float* pos, int t, int la,
+                                        TriRow& o) {
+    const int v0 = el.tris[3 * t], v1 = el.tris[3 * t + 1], v2 = el.tris[3 * t + 2];
+    const float3 x0 = ld3(pos, v0), x1 = ld3(pos, v1), x2 = ld3(pos, v2);
+    const float4 Dm = el.dminv[t];  // (0,0) (0,1) (1,0) (1,1)
+    const float3 a = x1 - x0, b = x2 - x0;
+    const float3 wu = a * Dm.x + b * Dm.z;
+    const float3 wv = a * Dm.y + b * Dm.w;
+    float lu = len3(wu), lv = len3(wv);
+    if (lu < 1.0e-6f) lu = 1.0e-6f;
+    if (lv < 1.0e-6f) lv = 1.0e-6f;
+    const float inv_lu = 1.0f / lu, inv_lv = 1.0f / lv;
+    const float cu = lu - 1.0f, cv = lv - 1.0f;
+    const float3 uh = wu * inv_lu, vh = wv * inv_lv;
+    o.du[0] = -Dm.x - Dm.z; o.du[1] = Dm.x; o.du[2] = Dm.z;
+    o.dv[0] = -Dm.y - Dm.w; o.dv[1] = Dm.y; o.dv[2] = Dm.w;
+    const float k_eff = el.area[t] * el.ktri[t];
+    const float dua = la == 0 ? o.du[0] : (la == 1 ? o.du[1] : o.du[2]);
+    const float dva = la == 0 ? o.dv[0] : (la == 1 ? o.dv[1] : o.dv[2]);
+    o.g = (uh * (cu * dua) + vh * (cv * dva)) * k_eff;
+    const float su = cu > 0.0f ? k_eff * cu * inv_lu : 0.0f;
+    const float sv = cv > 0.0f ? k_eff * cv * inv_lv : 0.0f;
+    // k_eff u u^T + su (I - u u^T) = (k_eff - su) u u^T + su I
+    const float cuu = k_eff - su, cvv = k_eff - sv;
+    o.Mu = S6{cuu * uh.x * uh.x + su, cuu * uh.x * uh.y, cuu * uh.x * uh.z,
+              cuu * uh.y * uh.y + su, cuu * uh.y * uh.z, cuu * uh.z * uh.z + su};
+    o.Mv = S6{cvv * vh.x * vh.x + sv, cvv * vh.x * vh.y, cvv * vh.x * vh.z,
+              cvv * vh.y * vh.y + sv, cvv * vh.y * vh.z, cvv * vh.z * vh.z + sv};
+}
+
+__device__ __forceinline__ float sel3(const float (&a)[3], int i) {
+    return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]);
+}
+
+__device__ __forceinline__ void smem_acc6(float* s, int stride, int slot, float c, const S6& a) {
+    float* q = s + (size_t)slot * 6 * stride;
+    q[0] += c * a.xx; q[stride] += c * a.xy; q[2 * stride] += c * a.xz;
+    q[3 * stride] += c * a.yy; q[4 * stride] += c * a.yz; q[5 * stride] += c * a.zz;
+}
+
+// ---------------------------------------------------------------------------
+// Fused per-row assembly: predictor (cloth_simulator.cu:83-106), mass
+// (:66-77), gradient at x_n (pins/springs/stretch), RHS (:127-142), Hessian
+// rows (pins, springs, stretch, inertia :199-210), block-Jacobi inverse
+// (pcg_solver.cu:41-42) and, for the zero guess, the PCG start
+// r = b, z = M^-1 b (pcg_solver.cu:386-404) with FP64 r.z and b.b.
+// One thread owns one row and writes every block of it exactly once.
+// ---------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, double* part,
+                SolverCfg cfg, int zero_guess, cudaGraphConditionalHandle cond) {
+    extern __shared__ float s_off[];  // [width * 6][BLOCK]
+    const int tid = threadIdx.x;
+    const int i = blockIdx.x * BLOCK + tid;
+    double red[2] = {0.0, 0.0};
+    if (i < a.n) {
+        const int s = i >> 5, lane = i & 31;
+        const int so = t.slice_off[s];
+        const int w = (t.slice_off[s + 1] - so) >> 5;
+        for (int q = 0; q < 6 * w; ++q) s_off[q * BLOCK + tid] = 0.0f;
+
+        const float3 x = ld3(a.pos, i);
+        const float3 vel = ld3(a.vel, i);
+        float m = 1.0f;
+        if (a.inv_mass) {
+            const float wi = a.inv_mass[i];
+            m = (wi > 1.0e-12f) ? (1.0f / wi) : 1.0e8f;
+        }
+        float3 acc = f3(a.gx, a.gy, a.gz);
+        if (a.apply_force && a.force) {
+            const float im = (m > 0.0f) ? (1.0f / m) : 0.0f;
+            const float3 f = ld3(a.force, i);
+            acc = f3(acc.x + f.x * im, acc.y + f.y * im, acc.z + f.z * im);
+        }
+        const float dt = a.dt;
+        const float3 xt = f3(x.x + dt * vel.x + dt * dt * acc.x, x.y + dt * vel.y + dt * dt * acc.y,
+                             x.z + dt * vel.z + dt * dt * acc.z);
+
+        float3 g = f3(0.f, 0.f, 0.f);
+        S6 D{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        // pins (pin_constraint.cu:61-92)
+        for (int p = t.pin_off[s]; p < t.pin_off[s + 1]; ++p) {
+            if (t.pin_row[p] == i) {
+                const float3 tg = ld3(t.pin_tgt, p);
+                g = g + (x - tg) * el.pin_k;
+                D.xx += el.pin_k; D.yy += el.pin_k; D.zz += el.pin_k;
+            }
+        }
+        // springs
+        if (el.use_springs) {
+            const int o = t.sinc_off[s];
+            const int ws = (t.sinc_off[s + 1] - o) >> 5;
+            for (int k = 0; k < ws; ++k) {
+                const int e = t.sinc[o + k * 32 + lane];
+                if (e < 0) continue;
+                const unsigned meta = t.sinc_meta[o + k * 32 + lane];
+                S6 H;
+                spring_row(el, a.pos, e, (int)(meta & 1u), g, H);
+                axpy6(D, 1.0f, H);
+                const unsigned slot = (meta >> 8) & 0xFFu;
+                if (slot == 0xFFu) axpy6(D, -1.0f, H);
+                else smem_acc6(s_off + tid, BLOCK, (int)slot, -1.0f, H);
+            }
+        }
+        // Baraff-Witkin stretch
+        if (el.use_tris) {
+            const int o = t.tinc_off[s];
+            const int wt = (t.tinc_off[s + 1] - o) >> 5;
+            for (int k = 0; k < wt; ++k) {
+                const int tri = t.tinc[o + k * 32 + lane];
+                if (tri < 0) continue;
+                const unsigned meta = t.tinc_meta[o + k * 32 + lane];
+                const int la = (int)(meta & 3u);
+                TriRow tr;
+                tri_row(el, a.pos, tri, la, tr);
+                g = g + tr.g;
+                const float dua = sel3(tr.du, la), dva = sel3(tr.dv, la);
+                axpy6(D, dua * dua, tr.Mu);
+                axpy6(D, dva * dva, tr.Mv);
+#pragma unroll
+                for (int q = 1; q <= 2; ++q) {
+                    const int lb = (la + q) % 3;
+                    const unsigned slot = (meta >> (8 * q)) & 0xFFu;
+                    const float cu_ = dua * sel3(tr.du, lb), cv_ = dva * sel3(tr.dv, lb);
+                    if (slot == 0xFFu) {
+                        axpy6(D, cu_, tr.Mu);
+                        axpy6(D, cv_, tr.Mv);
+                    } else {
+                        smem_acc6(s_off + tid, BLOCK, (int)slot, cu_, tr.Mu);
+                        smem_acc6(s_off + tid, BLOCK, (int)slot, cv_, tr.Mv);
+                    }
+                }
+            }
+        }
+        // RHS and inertia
+        const float inv_dt2 = 1.0f / (dt * dt);
+        const float mi = m * inv_dt2;
+        const float3 b = f3(mi * (xt.x - x.x) - g.x, mi * (xt.y - x.y) - g.y, mi * (xt.z - x.z) - g.z);
+        D.xx += mi; D.yy += mi; D.zz += mi;
+
+        // write the row: diagonal, off-diagonal blocks, M^-1
+        st6(t.diag + (size_t)s * 6 * 32 + lane, D);
+        float* vb = t.val + (size_t)so * 6 + lane;
+        for (int k = 0; k < w; ++k) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) vb[(k * 6 + c) * 32] = s_off[(k * 6 + c) * BLOCK + tid];
+        }
+        const S6 Mi = inverse6(D);
+        st6(t.minv + (size_t)s * 6 * 32 + lane, Mi);
+        v.b[i] = f4(b);
+        red[1] = (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z;
+        if (zero_guess) {
+            const float3 z = mul(Mi, b);
+            v.r[i] = f4(b);
+            v.z[i] = f4(z);
+            v.x[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            red[0] = (double)b.x * z.x + (double)b.y * z.y + (double)b.z * z.z;
+        }
+    }
+    double out[2];
+    if (grid_reduce<BLOCK, 2>(red, part, &st->counter[0], out) && threadIdx.x == 0) {
+        const double bb = out[1];
+        st->bb = bb;
+        st->use_tol = cfg.use_tol;
+        st->max_iter = cfg.max_iter;
+        st->tol2 = cfg.rel_tol * cfg.rel_tol * bb;
+        st->iter = 0;
+        st->beta = 0.0;
+        st->beta_f = 0.0f;
+        st->fallback = 0;
+        if (zero_guess) {
+            st->rho = out[0];
+            st->rr = bb;
+            st->rr0 = bb;
+            const bool bad = !finite_d(out[0]) || !finite_d(bb);
+            const bool conv = cfg.use_tol && bb <= st->tol2;
+            st->status = bad ? kSolveNonfinite : kSolveConverged;
+            st->done = (bad || conv || cfg.max_iter <= 0) ? 1 : 0;
+            if (cond) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
+        } else {
+            st->status = finite_d(bb) ? kSolveConverged : kSolveNonfinite;
+            st->done = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Warm-start initialisation (pcg_solver.cu:29-51 residual + :386-404):
+// r = b - A x0, z = M^-1 r.  The last block keeps the guess only if it is
+// finite and ||r0|| <= ||b||; otherwise it flags a zero-guess fallback that
+// `warm_fixup_kernel` applies.
+// ---------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+warm_init_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphConditionalHandle cond) {
+    const int i = blockIdx.x * BLOCK + threadIdx.x;
+    double red[3] = {0.0, 0.0, 0.0};  // r.z, r.r, b.M^-1 b
+    if (i < t.n) {
+        const int s = i >> 5, lane = i & 31;
+        const int so = t.slice_off[s];
+        const int w = (t.slice_off[s + 1] - so) >> 5;
+        const S6 D = ld6(t.diag + (size_t)s * 6 * 32 + lane);
+        const float3 xi = xyz(v.x[i]);
+        float3 ax = mul(D, xi);
+        const float* vb = t.val + (size_t)so * 6 + lane;
+        for (int k = 0; k < w; ++k) {
+            const int j = t.col[so + k * 32 + lane];
+            const S6 B = ld6(vb + k * 6 * 32);
+            ax = ax + mul(B, xyz(v.x[j]));
+        }
+        const float3 b = xyz(v.b[i]);
+        const float3 r = b - ax;
+        const S6 Mi = ld6(t.minv + (size_t)s * 6 * 32 + lane);
+        const float3 z = mul(Mi, r);
+        const float3 zb = mul(Mi, b);
+        v.r[i] = f4(r);
+        v.z[i] = f4(z);
+        red[0] = (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
+        red[1] = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
+        red[2] = (double)b.x * zb.x + (double)b.y * zb.y + (double)b.z * zb.z;
+    }
+    double out[3];
+    if (grid_reduce<BLOCK, 3>(red, part, &st->counter[1], out) && threadIdx.x == 0) {
+        const double bb = st->bb;
+        const bool warm_ok = finite_d(out[0]) && finite_d(out[1]) && out[1] <= bb;
+        st->fallback = warm_ok ? 0 : 1;
+        st->rho = warm_ok ? out[0] : out[2];
+        st->rr = warm_ok ? out[1] : bb;
+        st->rr0 = st->rr;
+        const bool bad = !finite_d(st->rho) || !finite_d(st->rr);
+        const bool conv = st->use_tol && st->rr <= st->tol2;
+        if (bad) st->status = kSolveNonfinite;
+        st->done = (bad || conv || st->max_iter <= 0 || st->status == kSolveNonfinite) ? 1 : 0;
+        if (cond) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
+    }
+}
+
+__global__ void warm_fixup_kernel(DevTopo t, Vecs v, const SolveState* st) {
+    if (!st->fallback) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= t.n) return;
+    const int s = i >> 5, lane = i & 31;
+    const S6 Mi = ld6(t.minv + (size_t)s * 6 * 32 + lane);
+    const float4 b = v.b[i];
+    v.x[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    v.r[i] = b;
+    v.z[i] = f4(mul(Mi, xyz(b)));
+}
+
+// ---------------------------------------------------------------------------
+// PCG iteration, kernel 1: p = z + beta p (own row and, recomputed
+// identically, every gathered neighbour: double-buffered p), Ap = A p
+// (block_csr.cu:54-83), sigma = p.Ap in FP64; the last block forms
+// alpha = rho / sigma (pcg_solver.cu:421-423, 456-464).
+// ---------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+pcg_spmv_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphConditionalHandle cond) {
+    if (st->done) return;
+    const int it = st->iter;
+    const float beta = st->beta_f;
+    const bool first = (it == 0);
+    const float4* __restrict__ pold = (it & 1) ? v.p1 : v.p0;
+    float4* __restrict__ pnew = (it & 1) ? v.p0 : v.p1;
+    const int i = blockIdx.x * BLOCK + threadIdx.x;
+    double red[1] = {0.0};
+    if (i < t.n) {
+        const int s = i >> 5, lane = i & 31;
+        const int so = t.slice_off[s];
+        const int w = (t.slice_off[s + 1] - so) >> 5;
+        const float4 zi = v.z[i];
+        float3 pi = xyz(zi);
+        if (!first) {
+            const float4 po = pold[i];
+            pi = f3(fmaf(beta, po.x, zi.x), fmaf(beta, po.y, zi.y), fmaf(beta, po.z, zi.z));
+        }
+        pnew[i] = f4(pi);
+        const S6 D = ld6(t.diag + (size_t)s * 6 * 32 + lane);
+        float3 acc = mul(D, pi);
+        const float* vb = t.val + (size_t)so * 6 + lane;
+        const int* cb = t.col + so + lane;
+        for (int k = 0; k < w; ++k) {
+            const int j = cb[k * 32];
+            const S6 B = ld6(vb + k * 6 * 32);
+            const float4 zj = v.z[j];
+            float3 pj = xyz(zj);
+            if (!first) {
+                const float4 po = pold[j];
+                pj = f3(fmaf(beta, po.x, zj.x), fmaf(beta, po.y, zj.y), fmaf(beta, po.z, zj.z));
+            }
+            acc = acc + mul(B, pj);
+        }
+        v.ap[i] = f4(acc);
+        red[0] = (double)pi.x * acc.x + (double)pi.y * acc.y + (double)pi.z * acc.z;
+    }
+    double out[1];
+    if (grid_reduce<BLOCK, 1>(red, part, &st->counter[2], out) && threadIdx.x == 0) {
+        const double sigma = out[0];
+        st->sigma = sigma;
+        const double alpha = (sigma > 1.0e-37 || sigma < -1.0e-37) ? st->rho / sigma : 0.0;
+        st->alpha = alpha;
+        st->alpha_f = (float)alpha;
+        if (!finite_d(sigma) || !finite_d(alpha)) {
+            st->status = kSolveNonfinite;
+            st->done = 1;
+            if (cond) cudaGraphSetConditional(cond, 0u);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// PCG iteration, kernel 2: x += alpha p, r -= alpha Ap, z = M^-1 r, FP64
+// r.z and r.r (pcg_solver.cu:406-434); the last block forms beta
+// (:436-454), counts the iteration, tests ||r||^2 <= tol^2 ||b||^2 and sets
+// the graph's loop condition.
+// ---------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+pcg_update_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphConditionalHandle cond) {
+    if (st->done) {
+        if (cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(cond, 0u);
+        return;
+    }
+    const int it = st->iter;
+    const float alpha = st->alpha_f;
+    const float4* __restrict__ p = (it & 1) ? v.p0 : v.p1;
+    const int i = blockIdx.x * BLOCK + threadIdx.x;
+    double red[2] = {0.0, 0.0};
+    if (i < t.n) {
+        const int s = i >> 5, lane = i & 31;
+        const float4 pi = p[i], api = v.ap[i], xi = v.x[i], ri = v.r[i];
+        const float3 xn = f3(fmaf(alpha, pi.x, xi.x), fmaf(alpha, pi.y, xi.y), fmaf(alpha, pi.z, xi.z));
+        const float3 rn = f3(fmaf(-alpha, api.x, ri.x), fmaf(-alpha, api.y, ri.y), fmaf(-alpha, api.z, ri.z));
+        const S6 Mi = ld6(t.minv + (size_t)s * 6 * 32 + lane);
+        const float3 zn = mul(Mi, rn);
+        v.x[i] = f4(xn);
+        v.r[i] = f4(rn);
+        v.z[i] = f4(zn);
+        red[0] = (double)rn.x * zn.x + (double)rn.y * zn.y + (double)rn.z * zn.z;
+        red[1] = (double)rn.x * rn.x + (double)rn.y * rn.y + (double)rn.z * rn.z;
+    }
+    double out[2];
+    if (grid_reduce<BLOCK, 2>(red, part, &st->counter[3], out) && threadIdx.x == 0) {
+        const double rho_new = out[0], rr = out[1];
+        const double rho = st->rho;
+        const double beta = (rho > 1.0e-37 || rho < -1.0e-37) ? rho_new / rho : 0.0;
+        st->beta = beta;
+        st->beta_f = (float)beta;
+        st->rho = rho_new;
+        st->rr = rr;
+        const int iter = it + 1;
+        st->iter = iter;
+        const bool bad = !finite_d(rho_new) || !finite_d(rr);
+        const bool conv = st->use_tol && rr <= st->tol2;
+        int done = 0;
+        if (bad) {
+            st->status = kSolveNonfinite;
+            done = 1;
+        } else if (conv) {
+            st->status = kSolveConverged;
+            done = 1;
+        } else if (iter >= st->max_iter) {
+            st->status = st->use_tol ? kSolveMaxIter : kSolveConverged;
+            done = 1;
+        }
+        st->done = done;
+        if (cond) cudaGraphSetConditional(cond, done ? 0u : 1u);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// x_{n+1} = x_n + dx, v_{n+1} = dx/dt * exp(-c dt)  (cloth_simulator.cu:222-244)
+// The caller's buffers are left untouched when the solve met NaN/Inf.
+// ---------------------------------------------------------------------------
+__global__ void finalize_kernel(StepArgs a, Vecs v, const SolveState* st) {
+    if (st->status == kSolveNonfinite) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const float4 d = v.x[i];
+    const float3 xn = ld3(a.pos, i);
+    st3(a.pos, i, f3(xn.x + d.x, xn.y + d.y, xn.z + d.z));
+    const float inv_dt = 1.0f / a.dt;
+    float3 vn = f3(d.x * inv_dt, d.y * inv_dt, d.z * inv_dt);
+    if (a.damping > 0.0f) {
+        const float decay = expf(-a.damping * a.dt);
+        vn = vn * decay;
+    }
+    st3(a.vel, i, vn);
+}
+
+// ---------------------------------------------------------------------------
+// Setup kernels
+// ---------------------------------------------------------------------------
+
+// triangle_stretch_constraint.cu:50-110
+__global__ void rest_shape_kernel(const int* __restrict__ tris, const float* __restrict__ pos,
+                                  float4* __restrict__ dminv, float* __restrict__ area, int T,
+                                  float det_eps, float cos_t, float sin_t) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    const float3 a = ld3(pos, tris[3 * t]), b = ld3(pos, tris[3 * t + 1]), c = ld3(pos, tris[3 * t + 2]);
+    const float3 ab = b - a, ac = c - a;
+    const float lab = len3(ab), lac = len3(ac);
+    const float3 abh = (lab > 1.0e-6f) ? ab * (1.0f / lab) : f3(1.f, 0.f, 0.f);
+    const float u_c = dot3(abh, ac);
+    const float v_c2 = lac * lac - u_c * u_c;
+    const float v_c = (v_c2 > 0.0f) ? sqrtf(v_c2) : 0.0f;
+    area[t] = 0.5f * lab * v_c;
+    const float det = lab * v_c;
+    float i00 = 1.f, i01 = 0.f, i10 = 0.f, i11 = 1.f;
+    if (det > det_eps) {
+        const float inv_det = 1.0f / (lab * v_c - u_c * 0.0f);
+        i00 = v_c * inv_det;
+        i01 = -u_c * inv_det;
+        i10 = -0.0f * inv_det;
+        i11 = lab * inv_det;
+    }
+    dminv[t] = make_float4(i00 * cos_t + i01 * (-sin_t), i00 * sin_t + i01 * cos_t,
+                           i10 * cos_t + i11 * (-sin_t), i10 * sin_t + i11 * cos_t);
+}
+
+// spring_constraint.cu:41-52
+__global__ void rest_length_kernel(const int* __restrict__ edges, const float* __restrict__ pos,
+                                   float* __restrict__ rest, int E) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    rest[e] = len3(ld3(pos, edges[2 * e]) - ld3(pos, edges[2 * e + 1]));
+}
+
+// Lumped area-weighted mass, cloth_simulator.cu:151-190, gathered per vertex
+// over its incident triangles (in triangle order) instead of atomics.
+__global__ void lumped_inv_mass_kernel(const int* __restrict__ vt_off, const int* __restrict__ vt_list,
+                                       const int* __restrict__ tris, const float* __restrict__ pos,
+                                       float density_over_3, float* __restrict__ inv_mass, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float m = 0.0f;
+    for (int q = vt_off[i]; q < vt_off[i + 1]; ++q) {
+        const int t = vt_list[q];
+        const float3 x0 = ld3(pos, tris[3 * t]), x1 = ld3(pos, tris[3 * t + 1]), x2 = ld3(pos, tris[3 * t + 2]);
+        const float3 e1 = x1 - x0, e2 = x2 - x0;
+        const float3 cr = f3(e1.y * e2.z - e1.z * e2.y, e1.z * e2.x - e1.x * e2.z, e1.x * e2.y - e1.y * e2.x);
+        m += density_over_3 * (0.5f * len3(cr));
+    }
+    inv_mass[i] = (m > 1.0e-12f) ? (1.0f / m) : 0.0f;
+}
+
+}  // namespace chysx_b200

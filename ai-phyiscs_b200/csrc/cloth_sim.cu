@@ -1,0 +1,823 @@
+// Host orchestration of the B200-native cloth step and its C ABI
+// (include/chysx_cloth.h).
+//
+// One step() is one CUDA-graph launch:
+//
+//   assemble ─┬─(warm start)─ warm_init ─ warm_fixup ─┐
+//             └───────────────(zero guess)────────────┴─ WHILE(cond) { pcg_spmv ; pcg_update } ─ finalize
+//
+// The WHILE node's condition is written on the device by the last block of
+// each grid reduction (converged, max_iter, or NaN), so the whole step runs
+// with no host round trip and exactly as many iterations as the solve needs.
+// The graph is built once per topology / solver-mode change; per-step values
+// (dt, caller pointers) are patched into the two kernel nodes that read them.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/chysx_cloth.h"
+#include "cloth_kernels.cuh"
+#include "topology.h"
+
+namespace chysx_b200 {
+
+namespace {
+
+thread_local std::string g_err;
+
+struct CudaFailure : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaFailure(std::string("chysx: ") + what + " failed: " + cudaGetErrorString(e));
+}
+
+template <class T>
+class DevBuf {
+public:
+    DevBuf() = default;
+    ~DevBuf() { reset(); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    void resize(size_t n) {
+        if (n == n_) return;
+        reset();
+        if (n) ck(cudaMalloc(reinterpret_cast<void**>(&p_), n * sizeof(T)), "cudaMalloc");
+        n_ = n;
+    }
+    void upload(const T* h, size_t n) {
+        resize(n);
+        if (n) ck(cudaMemcpy(p_, h, n * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+    }
+    void upload(const std::vector<T>& v) { upload(v.data(), v.size()); }
+    void zero() {
+        if (n_) ck(cudaMemset(p_, 0, n_ * sizeof(T)), "cudaMemset");
+    }
+    void reset() {
+        if (p_) cudaFree(p_);
+        p_ = nullptr;
+        n_ = 0;
+    }
+    T* get() const { return p_; }
+    size_t size() const { return n_; }
+
+private:
+    T* p_ = nullptr;
+    size_t n_ = 0;
+};
+
+constexpr int kVecBlock = 256;
+int grid_for(int n, int block) { return (n + block - 1) / block; }
+
+template <class T>
+bool same_bytes(const T& a, const T& b) {
+    return std::memcmp(&a, &b, sizeof(T)) == 0;
+}
+
+}  // namespace
+
+class ClothSim {
+public:
+    ~ClothSim() { destroy_graph(); }
+
+    chysx_cloth_material mat{0.0f, 0.0f, 0.0f, 0.05f, 0.0f, 0.0f, 0.0f, -9.81f};
+
+    // ---- caller buffers (borrowed) -------------------------------------
+    void set_external_buffers(uintptr_t p, uintptr_t v, int count, uintptr_t w, uintptr_t f) {
+        pos_ = p; vel_ = v; n_ = count; inv_mass_ = w; force_ = f;
+    }
+
+    // ---- mesh ----------------------------------------------------------
+    void set_mesh(const int32_t* t, int T) {
+        if (T < 0) throw std::invalid_argument("ClothSimulator::set_mesh: negative triangle count");
+        if (T > 0 && !t) throw std::invalid_argument("ClothSimulator::set_mesh: null triangle array");
+        tris_.assign(t, t + 3 * (size_t)T);
+        // sorted unique undirected edges (src/cloth/cloth_simulator.cu:328-346)
+        std::vector<long long> keys;
+        keys.reserve(3 * (size_t)T);
+        for (int q = 0; q < T; ++q) {
+            const int v[3] = {t[3 * q], t[3 * q + 1], t[3 * q + 2]};
+            for (int a = 0; a < 3; ++a) {
+                const int x = v[a], y = v[(a + 1) % 3];
+                const long long lo = std::min(x, y), hi = std::max(x, y);
+                keys.push_back((lo << 32) | (unsigned long long)(unsigned)hi);
+            }
+        }
+        std::sort(keys.begin(), keys.end());
+        keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+        edges_.resize(2 * keys.size());
+        for (size_t e = 0; e < keys.size(); ++e) {
+            edges_[2 * e] = (int)(keys[e] >> 32);
+            edges_[2 * e + 1] = (int)(unsigned)(keys[e] & 0xffffffffULL);
+        }
+        mesh_on_device_ = false;  // uploaded on first device use
+        vt_n_ = -1;
+        topo_dirty_ = true;
+    }
+    void ensure_mesh_on_device() {
+        if (mesh_on_device_) return;
+        d_tris_.upload(tris_);
+        d_edges_.upload(edges_);
+        mesh_on_device_ = true;
+    }
+    int num_edges() const { return (int)(edges_.size() / 2); }
+    const std::vector<int>& edges() const { return edges_; }
+
+    // ---- pins ----------------------------------------------------------
+    void set_pins(const int32_t* idx, const float* tgt, int P, float k) {
+        if (P < 0) throw std::invalid_argument("PinConstraint::set_pins: negative count");
+        if (P > 0 && (!idx || !tgt)) throw std::invalid_argument("ClothSimulator::set_pins: null array");
+        pin_idx_.assign(idx, idx + P);
+        pin_tgt_.assign(tgt, tgt + 3 * (size_t)P);
+        pin_k_ = k;
+        topo_dirty_ = true;
+    }
+    void clear_pins() {
+        pin_idx_.clear();
+        pin_tgt_.clear();
+        topo_dirty_ = true;
+    }
+    int num_pins() const { return (int)pin_idx_.size(); }
+    void update_pin_targets(const float* tgt, int P, uintptr_t stream) {
+        if (!tgt || P <= 0) return;
+        if (P != num_pins())
+            throw std::invalid_argument(
+                "ClothSimulator::update_pin_targets: n_pins does not match the currently installed pin "
+                "set; call set_pins(...) to change the pin set instead.");
+        std::memcpy(pin_tgt_.data(), tgt, 3 * (size_t)P * sizeof(float));
+        if (!topo_dirty_ && (int)topo_.pin_perm.size() == P) {
+            std::vector<float> sorted(3 * (size_t)P);
+            for (int c = 0; c < P; ++c)
+                for (int q = 0; q < 3; ++q) sorted[3 * c + q] = pin_tgt_[3 * (size_t)topo_.pin_perm[c] + q];
+            // pageable source: returns once staged, ordered on `stream`
+            ck(cudaMemcpyAsync(d_pin_tgt_.get(), sorted.data(), sorted.size() * sizeof(float),
+                               cudaMemcpyHostToDevice, reinterpret_cast<cudaStream_t>(stream)),
+               "cudaMemcpyAsync(pin targets)");
+        }
+    }
+
+    // ---- springs / stretch ---------------------------------------------
+    void build_springs(float k, const float* k_per_edge, uintptr_t stream) {
+        const int E = num_edges();
+        springs_built_ = true;
+        topo_dirty_ = true;
+        if (E == 0) {
+            d_rest_.reset();
+            d_kedge_.reset();
+            return;
+        }
+        if (!pos_)
+            throw std::runtime_error(
+                "ClothSimulator::build_springs_from_current_positions: external positions must be set "
+                "first via set_external_buffers().");
+        check_indices(edges_, "spring edge");
+        ensure_mesh_on_device();
+        std::vector<float> ke(E, k);
+        if (k_per_edge) std::memcpy(ke.data(), k_per_edge, E * sizeof(float));
+        d_kedge_.upload(ke);
+        d_rest_.resize(E);
+        rest_length_kernel<<<grid_for(E, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+            d_edges_.get(), reinterpret_cast<const float*>(pos_), d_rest_.get(), E);
+        ck(cudaGetLastError(), "rest_length_kernel launch");
+    }
+    int num_springs() const { return springs_built_ ? num_edges() : 0; }
+
+    void build_stretch(float k, const float* k_per_tri, uintptr_t stream) {
+        const int T = (int)(tris_.size() / 3);
+        stretch_built_ = true;
+        topo_dirty_ = true;
+        if (T == 0) {
+            d_dminv_.reset();
+            d_area_.reset();
+            d_ktri_.reset();
+            return;
+        }
+        if (!pos_)
+            throw std::runtime_error(
+                "ClothSimulator::build_fem_stretch_from_current_positions: external positions must be "
+                "set first via set_external_buffers().");
+        check_indices(tris_, "triangle");
+        ensure_mesh_on_device();
+        std::vector<float> kt(T, k);
+        if (k_per_tri) std::memcpy(kt.data(), k_per_tri, T * sizeof(float));
+        d_ktri_.upload(kt);
+        d_dminv_.resize(T);
+        d_area_.resize(T);
+        rest_shape_kernel<<<grid_for(T, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+            d_tris_.get(), reinterpret_cast<const float*>(pos_), d_dminv_.get(), d_area_.get(), T,
+            det_eps_, 1.0f, 0.0f);
+        ck(cudaGetLastError(), "rest_shape_kernel launch");
+    }
+
+    // ---- mass ----------------------------------------------------------
+    void redistribute_mass(float rho, uintptr_t inv_mass, int count, uintptr_t stream) {
+        if (count <= 0) return;
+        if (!inv_mass)
+            throw std::invalid_argument(
+                "ClothSimulator::redistribute_mass_area_weighted: inv_mass_ptr must be non-null");
+        if (rho <= 0.0f)
+            throw std::invalid_argument(
+                "ClothSimulator::redistribute_mass_area_weighted: surface_density must be positive");
+        if (tris_.empty())
+            throw std::runtime_error(
+                "ClothSimulator::redistribute_mass_area_weighted: call set_mesh(...) before "
+                "redistributing mass.");
+        if (!pos_ || n_ < count)
+            throw std::runtime_error(
+                "ClothSimulator::redistribute_mass_area_weighted: external positions must be set first "
+                "via set_external_buffers().");
+        ensure_mesh_on_device();
+        if (vt_n_ != count) {
+            std::vector<int> off, list;
+            build_vertex_triangles(count, tris_, off, list);
+            d_vt_off_.upload(off);
+            d_vt_list_.upload(list);
+            vt_n_ = count;
+        }
+        lumped_inv_mass_kernel<<<grid_for(count, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+            d_vt_off_.get(), d_vt_list_.get(), d_tris_.get(), reinterpret_cast<const float*>(pos_),
+            rho / 3.0f, reinterpret_cast<float*>(inv_mass), count);
+        ck(cudaGetLastError(), "lumped_inv_mass_kernel launch");
+    }
+
+    // ---- solver --------------------------------------------------------
+    void set_pcg_iterations(int m) {
+        if (m < 0 || m > 10000000)
+            throw std::invalid_argument("set_pcg_iterations: max_iter must be in [0, 1e7]");
+        max_iter_ = m;
+    }
+    int pcg_iterations() const { return max_iter_; }
+    void set_solver(int m, double tol, int warm) {
+        if (m < 0 || m > 10000000) throw std::invalid_argument("set_solver: max_iter must be in [0, 1e7]");
+        if (!(tol >= 0.0) || !std::isfinite(tol)) throw std::invalid_argument("set_solver: rel_tol must be >= 0");
+        if (warm < CHYSX_WARM_ZERO || warm > CHYSX_WARM_LEARNED)
+            throw std::invalid_argument("set_solver: unknown warm_start mode");
+        if (warm == CHYSX_WARM_LEARNED && !warm_guess_)
+            throw std::runtime_error("set_solver: learned warm start needs a network (load one first)");
+        if (warm != warm_mode_) graph_dirty_ = true;
+        max_iter_ = m;
+        rel_tol_ = tol;
+        warm_mode_ = warm;
+    }
+    void set_options(int sis, int af, float eps) {
+        if (!(eps >= 0.0f)) throw std::invalid_argument("set_options: fem_det_eps must be >= 0");
+        if ((sis != 0) != springs_in_step_) topo_dirty_ = true;
+        springs_in_step_ = sis != 0;
+        apply_force_ = af != 0;
+        det_eps_ = eps;
+    }
+
+    // ---- step ----------------------------------------------------------
+    void step(float dt, uintptr_t stream) {
+        if (n_ <= 0) return;
+        if (!pos_ || !vel_)
+            throw std::runtime_error(
+                "chysx::cloth::ClothSimulator::step: pos / vel spans must be set via "
+                "set_external_buffers() before stepping.");
+        if (!(dt > 0.0f)) throw std::invalid_argument("chysx::cloth::ClothSimulator::step: dt must be positive");
+        ensure_mesh_on_device();
+        if (topo_dirty_ || topo_.n != n_) rebuild_topology();
+        if (graph_dirty_) build_graph();
+        update_step_nodes(dt);
+        ck(cudaGraphLaunch(exec_, reinterpret_cast<cudaStream_t>(stream)), "cudaGraphLaunch(step)");
+        last_stream_ = stream;
+        stepped_ = true;
+    }
+
+    void last_stats(int* iters, double* relres, int* status) {
+        SolveState s{};
+        if (stepped_) {
+            ck(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(last_stream_)), "cudaStreamSynchronize");
+            ck(cudaMemcpy(&s, d_state_.get(), sizeof(SolveState), cudaMemcpyDeviceToHost), "cudaMemcpy(state)");
+        }
+        if (iters) *iters = s.iter;
+        if (relres) *relres = (s.bb > 0.0) ? std::sqrt(std::max(s.rr, 0.0) / s.bb) : 0.0;
+        if (status) *status = s.status;
+    }
+
+    int num_particles() const { return n_; }
+    int num_off_diag_blocks() const { return (int)topo_.nnz(); }
+
+    void debug_dump(float* diag, int32_t* rp, int32_t* col, float* vals, float* rhs, float* dx) {
+        const int n = topo_.n;
+        if (n == 0) return;
+        ck(cudaDeviceSynchronize(), "cudaDeviceSynchronize(debug_dump)");
+        const size_t np = topo_.n_pad;
+        std::vector<float> hd(np * 6), hv(d_val_.size());
+        std::vector<float4> hb(np), hx(np);
+        ck(cudaMemcpy(hd.data(), d_diag_.get(), hd.size() * 4, cudaMemcpyDeviceToHost), "dump diag");
+        if (!hv.empty()) ck(cudaMemcpy(hv.data(), d_val_.get(), hv.size() * 4, cudaMemcpyDeviceToHost), "dump val");
+        ck(cudaMemcpy(hb.data(), d_b_.get(), np * sizeof(float4), cudaMemcpyDeviceToHost), "dump rhs");
+        ck(cudaMemcpy(hx.data(), d_x_.get(), np * sizeof(float4), cudaMemcpyDeviceToHost), "dump dx");
+        auto put9 = [](float* o, const float* s6, size_t stride) {
+            const float xx = s6[0], xy = s6[stride], xz = s6[2 * stride], yy = s6[3 * stride],
+                        yz = s6[4 * stride], zz = s6[5 * stride];
+            o[0] = xx; o[1] = xy; o[2] = xz; o[3] = xy; o[4] = yy; o[5] = yz; o[6] = xz; o[7] = yz; o[8] = zz;
+        };
+        for (int i = 0; i < n; ++i) {
+            if (diag) put9(diag + 9 * (size_t)i, &hd[(size_t)(i >> 5) * 192 + (i & 31)], 32);
+            if (rhs) { rhs[3 * i] = hb[i].x; rhs[3 * i + 1] = hb[i].y; rhs[3 * i + 2] = hb[i].z; }
+            if (dx) { dx[3 * i] = hx[i].x; dx[3 * i + 1] = hx[i].y; dx[3 * i + 2] = hx[i].z; }
+        }
+        if (rp) std::copy(topo_.csr_ptr.begin(), topo_.csr_ptr.end(), rp);
+        if (col) std::copy(topo_.csr_col.begin(), topo_.csr_col.end(), col);
+        if (vals) {
+            for (int r = 0; r < n; ++r) {
+                const int s = r >> 5;
+                const int so = topo_.slice_off[s];
+                for (int q = topo_.csr_ptr[r]; q < topo_.csr_ptr[r + 1]; ++q) {
+                    const int e = topo_.csr_to_ell[q];
+                    const int kk = (e - so) >> 5;
+                    put9(vals + 9 * (size_t)q, &hv[(size_t)so * 6 + (size_t)kk * 192 + (e & 31)], 32);
+                }
+            }
+        }
+    }
+
+    // learned warm start hook (set by the network module)
+    bool warm_guess_ = false;
+
+private:
+    void check_indices(const std::vector<int>& idx, const char* what) const {
+        for (int v : idx)
+            if (v < 0 || v >= n_)
+                throw std::out_of_range(std::string(what) + " vertex index " + std::to_string(v) +
+                                        " out of range [0, " + std::to_string(n_) + ")");
+    }
+
+    void rebuild_topology() {
+        const bool use_tris = stretch_built_ && d_dminv_.size() > 0;
+        const bool use_springs = springs_built_ && springs_in_step_ && d_rest_.size() > 0;
+        build_topology(n_, tris_, use_tris, edges_, use_springs, pin_idx_, topo_);
+        use_tris_ = use_tris;
+        use_springs_ = use_springs;
+        d_slice_off_.upload(topo_.slice_off);
+        d_col_.upload(topo_.col);
+        d_val_.resize(std::max<size_t>(1, (size_t)topo_.ell_entries() * 6));
+        d_val_.zero();
+        d_diag_.resize((size_t)topo_.n_pad * 6);
+        d_minv_.resize((size_t)topo_.n_pad * 6);
+        d_tinc_off_.upload(topo_.tinc_off);
+        d_tinc_.upload(topo_.tinc);
+        d_tinc_meta_.upload(topo_.tinc_meta);
+        d_sinc_off_.upload(topo_.sinc_off);
+        d_sinc_.upload(topo_.sinc);
+        d_sinc_meta_.upload(topo_.sinc_meta);
+        d_pin_off_.upload(topo_.pin_off);
+        d_pin_row_.upload(topo_.pin_row);
+        {
+            std::vector<float> sorted(3 * topo_.pin_row.size());
+            for (size_t c = 0; c < topo_.pin_row.size(); ++c)
+                for (int q = 0; q < 3; ++q) sorted[3 * c + q] = pin_tgt_[3 * (size_t)topo_.pin_perm[c] + q];
+            d_pin_tgt_.upload(sorted);
+        }
+        const size_t np = topo_.n_pad;
+        if (d_x_.size() != np) {
+            // a resize starts the warm-start history from zero
+            // (src/cloth/cloth_simulator.cu:802-811)
+            for (DevBuf<float4>* b : {&d_b_, &d_r_, &d_z_, &d_x_, &d_ap_, &d_p0_, &d_p1_}) {
+                b->resize(np);
+                b->zero();
+            }
+        }
+        // assembly block size: per-thread shared accumulators of 6*width floats
+        const int W = std::max(1, topo_.max_width);
+        asm_block_ = (W <= 16) ? 128 : (W <= 32 ? 64 : 32);
+        asm_smem_ = (size_t)6 * W * asm_block_ * sizeof(float);
+        const int max_grid = std::max(grid_for(n_, asm_block_), grid_for(n_, kVecBlock));
+        d_part_.resize((size_t)std::max(1, max_grid) * 3);
+        d_state_.resize(1);
+        d_state_.zero();
+        topo_dirty_ = false;
+        graph_dirty_ = true;
+    }
+
+    DevTopo dev_topo() const {
+        DevTopo t;
+        t.n = n_;
+        t.n_slices = topo_.n_slices;
+        t.slice_off = d_slice_off_.get();
+        t.col = d_col_.get();
+        t.val = d_val_.get();
+        t.diag = d_diag_.get();
+        t.minv = d_minv_.get();
+        t.tinc_off = d_tinc_off_.get();
+        t.tinc = d_tinc_.get();
+        t.tinc_meta = d_tinc_meta_.get();
+        t.sinc_off = d_sinc_off_.get();
+        t.sinc = d_sinc_.get();
+        t.sinc_meta = d_sinc_meta_.get();
+        t.pin_off = d_pin_off_.get();
+        t.pin_row = d_pin_row_.get();
+        t.pin_tgt = d_pin_tgt_.get();
+        return t;
+    }
+    ElemData elem_data() const {
+        ElemData e;
+        e.tris = d_tris_.get();
+        e.dminv = d_dminv_.get();
+        e.area = d_area_.get();
+        e.ktri = d_ktri_.get();
+        e.edges = d_edges_.get();
+        e.rest = d_rest_.get();
+        e.kedge = d_kedge_.get();
+        e.pin_k = pin_k_;
+        e.use_tris = use_tris_ ? 1 : 0;
+        e.use_springs = use_springs_ ? 1 : 0;
+        return e;
+    }
+    Vecs vecs() const {
+        return Vecs{d_b_.get(), d_r_.get(), d_z_.get(), d_x_.get(), d_ap_.get(), d_p0_.get(), d_p1_.get()};
+    }
+    StepArgs step_args(float dt) const {
+        StepArgs a;
+        a.pos = reinterpret_cast<float*>(pos_);
+        a.vel = reinterpret_cast<float*>(vel_);
+        a.inv_mass = reinterpret_cast<const float*>(inv_mass_);
+        a.force = reinterpret_cast<const float*>(force_);
+        a.n = n_;
+        a.dt = dt;
+        a.gx = mat.gx; a.gy = mat.gy; a.gz = mat.gz;
+        a.damping = mat.damping;
+        a.apply_force = apply_force_ ? 1 : 0;
+        return a;
+    }
+    SolverCfg solver_cfg() const {
+        SolverCfg c;
+        c.max_iter = max_iter_;
+        c.use_tol = rel_tol_ > 0.0 ? 1 : 0;
+        c.rel_tol = rel_tol_;
+        return c;
+    }
+
+    const void* assemble_fn() const {
+        if (asm_block_ == 128) return reinterpret_cast<const void*>(&assemble_kernel<128>);
+        if (asm_block_ == 64) return reinterpret_cast<const void*>(&assemble_kernel<64>);
+        return reinterpret_cast<const void*>(&assemble_kernel<32>);
+    }
+
+    void asm_params(cudaKernelNodeParams& p, void** args) {
+        p = cudaKernelNodeParams{};
+        p.func = const_cast<void*>(assemble_fn());
+        p.gridDim = dim3(grid_for(n_, asm_block_));
+        p.blockDim = dim3(asm_block_);
+        p.sharedMemBytes = (unsigned)asm_smem_;
+        p.kernelParams = args;
+    }
+
+    void destroy_graph() {
+        if (exec_) cudaGraphExecDestroy(exec_);
+        if (graph_) cudaGraphDestroy(graph_);
+        exec_ = nullptr;
+        graph_ = nullptr;
+    }
+
+    void build_graph() {
+        destroy_graph();
+        if (asm_smem_ > 48 * 1024)
+            ck(cudaFuncSetAttribute(assemble_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asm_smem_),
+               "cudaFuncSetAttribute(assemble smem)");
+        ck(cudaGraphCreate(&graph_, 0), "cudaGraphCreate");
+        ck(cudaGraphConditionalHandleCreate(&cond_, graph_, 1, cudaGraphCondAssignDefault),
+           "cudaGraphConditionalHandleCreate");
+        DevTopo t = dev_topo();
+        ElemData el = elem_data();
+        Vecs v = vecs();
+        SolveState* st = d_state_.get();
+        double* part = d_part_.get();
+        const bool warm = warm_mode_ != CHYSX_WARM_ZERO;
+        int zero_guess = warm ? 0 : 1;
+        cur_args_ = step_args(1.0f / 60.0f);
+        cur_cfg_ = solver_cfg();
+        cudaGraphConditionalHandle cond = cond_;
+
+        void* aargs[] = {&cur_args_, &el, &t, &v, &st, &part, &cur_cfg_, &zero_guess, &cond};
+        cudaKernelNodeParams ap;
+        asm_params(ap, aargs);
+        ck(cudaGraphAddKernelNode(&asm_node_, graph_, nullptr, 0, &ap), "add assemble node");
+        cudaGraphNode_t last = asm_node_;
+
+        const int vgrid = std::max(1, grid_for(n_, kVecBlock));
+        if (warm) {
+            cudaKernelNodeParams p{};
+            void* iargs[] = {&t, &v, &st, &part, &cond};
+            p.func = reinterpret_cast<void*>(&warm_init_kernel<kVecBlock>);
+            p.gridDim = dim3(vgrid);
+            p.blockDim = dim3(kVecBlock);
+            p.kernelParams = iargs;
+            cudaGraphNode_t n1;
+            ck(cudaGraphAddKernelNode(&n1, graph_, &last, 1, &p), "add warm_init node");
+            void* fargs[] = {&t, &v, &st};
+            cudaKernelNodeParams pf{};
+            pf.func = reinterpret_cast<void*>(&warm_fixup_kernel);
+            pf.gridDim = dim3(vgrid);
+            pf.blockDim = dim3(kVecBlock);
+            pf.kernelParams = fargs;
+            cudaGraphNode_t n2;
+            ck(cudaGraphAddKernelNode(&n2, graph_, &n1, 1, &pf), "add warm_fixup node");
+            last = n2;
+        }
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond_;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t loop;
+        ck(cudaGraphAddNode(&loop, graph_, &last, 1, &cp), "add while node");
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        {
+            void* kargs[] = {&t, &v, &st, &part, &cond};
+            cudaKernelNodeParams p1{};
+            p1.func = reinterpret_cast<void*>(&pcg_spmv_kernel<kVecBlock>);
+            p1.gridDim = dim3(vgrid);
+            p1.blockDim = dim3(kVecBlock);
+            p1.kernelParams = kargs;
+            cudaGraphNode_t k1;
+            ck(cudaGraphAddKernelNode(&k1, body, nullptr, 0, &p1), "add pcg_spmv node");
+            cudaKernelNodeParams p2 = p1;
+            p2.func = reinterpret_cast<void*>(&pcg_update_kernel<kVecBlock>);
+            cudaGraphNode_t k2;
+            ck(cudaGraphAddKernelNode(&k2, body, &k1, 1, &p2), "add pcg_update node");
+        }
+        {
+            void* fargs[] = {&cur_args_, &v, &st};
+            cudaKernelNodeParams p{};
+            p.func = reinterpret_cast<void*>(&finalize_kernel);
+            p.gridDim = dim3(vgrid);
+            p.blockDim = dim3(kVecBlock);
+            p.kernelParams = fargs;
+            ck(cudaGraphAddKernelNode(&fin_node_, graph_, &loop, 1, &p), "add finalize node");
+        }
+        ck(cudaGraphInstantiate(&exec_, graph_, 0), "cudaGraphInstantiate(step)");
+        graph_dirty_ = false;
+        // node args as instantiated; the first step patches them
+        node_args_ = cur_args_;
+        node_cfg_ = cur_cfg_;
+        nodes_valid_ = true;
+    }
+
+    void update_step_nodes(float dt) {
+        StepArgs a = step_args(dt);
+        SolverCfg c = solver_cfg();
+        if (nodes_valid_ && same_bytes(a, node_args_) && same_bytes(c, node_cfg_)) return;
+        DevTopo t = dev_topo();
+        ElemData el = elem_data();
+        Vecs v = vecs();
+        SolveState* st = d_state_.get();
+        double* part = d_part_.get();
+        int zero_guess = warm_mode_ != CHYSX_WARM_ZERO ? 0 : 1;
+        cudaGraphConditionalHandle cond = cond_;
+        void* aargs[] = {&a, &el, &t, &v, &st, &part, &c, &zero_guess, &cond};
+        cudaKernelNodeParams ap;
+        asm_params(ap, aargs);
+        ck(cudaGraphExecKernelNodeSetParams(exec_, asm_node_, &ap), "update assemble node");
+        const int vgrid = std::max(1, grid_for(n_, kVecBlock));
+        void* fargs[] = {&a, &v, &st};
+        cudaKernelNodeParams p{};
+        p.func = reinterpret_cast<void*>(&finalize_kernel);
+        p.gridDim = dim3(vgrid);
+        p.blockDim = dim3(kVecBlock);
+        p.kernelParams = fargs;
+        ck(cudaGraphExecKernelNodeSetParams(exec_, fin_node_, &p), "update finalize node");
+        node_args_ = a;
+        node_cfg_ = c;
+        nodes_valid_ = true;
+    }
+
+    // caller buffers
+    uintptr_t pos_ = 0, vel_ = 0, inv_mass_ = 0, force_ = 0;
+    int n_ = 0;
+    // mesh
+    std::vector<int> tris_, edges_;
+    DevBuf<int> d_tris_, d_edges_, d_vt_off_, d_vt_list_;
+    int vt_n_ = -1;
+    bool mesh_on_device_ = false;
+    // elements
+    bool springs_built_ = false, stretch_built_ = false;
+    DevBuf<float> d_rest_, d_kedge_, d_area_, d_ktri_;
+    DevBuf<float4> d_dminv_;
+    std::vector<int> pin_idx_;
+    std::vector<float> pin_tgt_;
+    float pin_k_ = 1.0e6f;
+    // options (defaults reproduce the reference)
+    bool springs_in_step_ = true, apply_force_ = false;
+    float det_eps_ = 1.0e-6f;
+    int max_iter_ = 50;
+    double rel_tol_ = 0.0;
+    int warm_mode_ = CHYSX_WARM_PREVIOUS;
+    // topology + system
+    bool topo_dirty_ = true, use_tris_ = false, use_springs_ = false;
+    HostTopology topo_;
+    DevBuf<int> d_slice_off_, d_col_, d_tinc_off_, d_tinc_, d_sinc_off_, d_sinc_, d_pin_off_, d_pin_row_;
+    DevBuf<unsigned> d_tinc_meta_, d_sinc_meta_;
+    DevBuf<float> d_val_, d_diag_, d_minv_, d_pin_tgt_;
+    DevBuf<float4> d_b_, d_r_, d_z_, d_x_, d_ap_, d_p0_, d_p1_;
+    DevBuf<double> d_part_;
+    DevBuf<SolveState> d_state_;
+    int asm_block_ = 128;
+    size_t asm_smem_ = 0;
+    // graph
+    bool graph_dirty_ = true, nodes_valid_ = false;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t exec_ = nullptr;
+    cudaGraphNode_t asm_node_ = nullptr, fin_node_ = nullptr;
+    cudaGraphConditionalHandle cond_ = 0;
+    StepArgs cur_args_{}, node_args_{};
+    SolverCfg cur_cfg_{}, node_cfg_{};
+    uintptr_t last_stream_ = 0;
+    bool stepped_ = false;
+};
+
+}  // namespace chysx_b200
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using chysx_b200::ClothSim;
+
+struct chysx_cloth {
+    ClothSim sim;
+};
+
+namespace {
+
+template <class F>
+int guard(F&& f) {
+    try {
+        f();
+        return CHYSX_OK;
+    } catch (const std::invalid_argument& e) {
+        chysx_b200::g_err = e.what();
+        return CHYSX_ERR_INVALID_ARGUMENT;
+    } catch (const std::out_of_range& e) {
+        chysx_b200::g_err = e.what();
+        return CHYSX_ERR_OUT_OF_RANGE;
+    } catch (const chysx_b200::CudaFailure& e) {
+        chysx_b200::g_err = e.what();
+        return CHYSX_ERR_CUDA;
+    } catch (const std::bad_alloc&) {
+        chysx_b200::g_err = "host allocation failed";
+        return CHYSX_ERR_RUNTIME;
+    } catch (const std::exception& e) {
+        chysx_b200::g_err = e.what();
+        return CHYSX_ERR_RUNTIME;
+    }
+}
+
+int null_handle() {
+    chysx_b200::g_err = "null chysx_cloth handle";
+    return CHYSX_ERR_INVALID_ARGUMENT;
+}
+
+}  // namespace
+
+#define CHYSX_H(h)            \
+    if (!(h)) return null_handle()
+
+extern "C" {
+
+const char* chysx_last_error(void) { return chysx_b200::g_err.c_str(); }
+
+int chysx_cloth_create(chysx_cloth** out) {
+    if (!out) return null_handle();
+    return guard([&] { *out = new chysx_cloth(); });
+}
+int chysx_cloth_destroy(chysx_cloth* h) {
+    delete h;
+    return CHYSX_OK;
+}
+int chysx_cloth_set_material(chysx_cloth* h, const chysx_cloth_material* m) {
+    CHYSX_H(h);
+    if (!m) return null_handle();
+    h->sim.mat = *m;
+    return CHYSX_OK;
+}
+int chysx_cloth_get_material(const chysx_cloth* h, chysx_cloth_material* out) {
+    CHYSX_H(h);
+    if (!out) return null_handle();
+    *out = h->sim.mat;
+    return CHYSX_OK;
+}
+int chysx_cloth_set_external_buffers(chysx_cloth* h, uintptr_t pos, uintptr_t vel, int count,
+                                     uintptr_t inv_mass, uintptr_t force) {
+    CHYSX_H(h);
+    h->sim.set_external_buffers(pos, vel, count, inv_mass, force);
+    return CHYSX_OK;
+}
+int chysx_cloth_set_mesh(chysx_cloth* h, const int32_t* tris, int n) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_mesh(tris, n); });
+}
+int chysx_cloth_num_edges(const chysx_cloth* h, int* out) {
+    CHYSX_H(h);
+    if (out) *out = h->sim.num_edges();
+    return CHYSX_OK;
+}
+int chysx_cloth_get_edges(const chysx_cloth* h, int32_t* out) {
+    CHYSX_H(h);
+    if (out) std::copy(h->sim.edges().begin(), h->sim.edges().end(), out);
+    return CHYSX_OK;
+}
+int chysx_cloth_set_pins(chysx_cloth* h, const int32_t* idx, const float* targets, int n, float k) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_pins(idx, targets, n, k); });
+}
+int chysx_cloth_clear_pins(chysx_cloth* h) {
+    CHYSX_H(h);
+    h->sim.clear_pins();
+    return CHYSX_OK;
+}
+int chysx_cloth_num_pins(const chysx_cloth* h, int* out) {
+    CHYSX_H(h);
+    if (out) *out = h->sim.num_pins();
+    return CHYSX_OK;
+}
+int chysx_cloth_update_pin_targets(chysx_cloth* h, const float* targets, int n, uintptr_t stream) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.update_pin_targets(targets, n, stream); });
+}
+int chysx_cloth_build_springs(chysx_cloth* h, float k, const float* k_per_edge, uintptr_t stream) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.build_springs(k, k_per_edge, stream); });
+}
+int chysx_cloth_num_springs(const chysx_cloth* h, int* out) {
+    CHYSX_H(h);
+    if (out) *out = h->sim.num_springs();
+    return CHYSX_OK;
+}
+int chysx_cloth_build_fem_stretch(chysx_cloth* h, float k, const float* k_per_tri, uintptr_t stream) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.build_stretch(k, k_per_tri, stream); });
+}
+int chysx_cloth_redistribute_mass(chysx_cloth* h, float rho, uintptr_t inv_mass, int n, uintptr_t stream) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.redistribute_mass(rho, inv_mass, n, stream); });
+}
+int chysx_cloth_set_pcg_iterations(chysx_cloth* h, int m) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_pcg_iterations(m); });
+}
+int chysx_cloth_pcg_iterations(const chysx_cloth* h, int* out) {
+    CHYSX_H(h);
+    if (out) *out = h->sim.pcg_iterations();
+    return CHYSX_OK;
+}
+int chysx_cloth_set_solver(chysx_cloth* h, int max_iter, double rel_tol, int warm) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_solver(max_iter, rel_tol, warm); });
+}
+int chysx_cloth_set_options(chysx_cloth* h, int sis, int af, float eps) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_options(sis, af, eps); });
+}
+int chysx_cloth_step(chysx_cloth* h, float dt, uintptr_t stream) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.step(dt, stream); });
+}
+int chysx_cloth_last_stats(chysx_cloth* h, int* iters, double* relres, int* status) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.last_stats(iters, relres, status); });
+}
+int chysx_cloth_num_particles(const chysx_cloth* h, int* out) {
+    CHYSX_H(h);
+    if (out) *out = h->sim.num_particles();
+    return CHYSX_OK;
+}
+int chysx_cloth_num_off_diag_blocks(const chysx_cloth* h, int* out) {
+    CHYSX_H(h);
+    if (out) *out = h->sim.num_off_diag_blocks();
+    return CHYSX_OK;
+}
+int chysx_cloth_debug_dump(chysx_cloth* h, float* diag, int32_t* rp, int32_t* col, float* vals, float* rhs,
+                           float* dx) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.debug_dump(diag, rp, col, vals, rhs, dx); });
+}
+
+int chysx_topology_pattern(int n, const int32_t* tris, int n_tris, const int32_t* edges, int n_edges,
+                           int32_t* row_offsets, int32_t* col_indices, int max_nnz, int* nnz_out,
+                           int* ell_entries_out, int* max_width_out) {
+    return guard([&] {
+        std::vector<int> t(tris, tris + 3 * (size_t)std::max(0, n_tris));
+        std::vector<int> e(edges, edges + 2 * (size_t)std::max(0, n_edges));
+        chysx_b200::HostTopology topo;
+        chysx_b200::build_topology(n, t, n_tris > 0, e, n_edges > 0, {}, topo);
+        if (nnz_out) *nnz_out = (int)topo.nnz();
+        if (ell_entries_out) *ell_entries_out = (int)topo.ell_entries();
+        if (max_width_out) *max_width_out = topo.max_width;
+        if (row_offsets) std::copy(topo.csr_ptr.begin(), topo.csr_ptr.end(), row_offsets);
+        if (col_indices) {
+            if (topo.nnz() > max_nnz) throw std::invalid_argument("chysx_topology_pattern: col_indices too small");
+            std::copy(topo.csr_col.begin(), topo.csr_col.end(), col_indices);
+        }
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,219 @@
+// pybind11 facade `_chysx_native` over the C ABI (include/chysx_cloth.h).
+//
+// Mirrors the cloth part of the reference's module (src/bindings.cpp:25-600):
+// ClothMaterial with the same fields, ClothSimulator with the same method
+// names, argument names, defaults and exception types (ValueError for
+// std::invalid_argument, IndexError for std::out_of_range, RuntimeError
+// otherwise).  Every call goes through the extern "C" entry points; this
+// file holds no simulation logic.
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/chysx_cloth.h"
+
+namespace py = pybind11;
+
+namespace {
+
+void check(int rc) {
+    if (rc == CHYSX_OK) return;
+    const std::string msg = chysx_last_error();
+    if (rc == CHYSX_ERR_INVALID_ARGUMENT) throw py::value_error(msg);
+    if (rc == CHYSX_ERR_OUT_OF_RANGE) throw py::index_error(msg);
+    throw std::runtime_error(msg);
+}
+
+class PyClothSimulator {
+public:
+    PyClothSimulator() { check(chysx_cloth_create(&h_)); }
+    ~PyClothSimulator() { chysx_cloth_destroy(h_); }
+    PyClothSimulator(const PyClothSimulator&) = delete;
+    PyClothSimulator& operator=(const PyClothSimulator&) = delete;
+    chysx_cloth* h() const { return h_; }
+
+private:
+    chysx_cloth* h_ = nullptr;
+};
+
+using F32 = py::array_t<float, py::array::c_style | py::array::forcecast>;
+using I32 = py::array_t<int32_t, py::array::c_style | py::array::forcecast>;
+
+}  // namespace
+
+PYBIND11_MODULE(_chysx_native, m) {
+    m.doc() = "ChysX cloth step, B200-native (sm_100a) implementation";
+
+    py::class_<chysx_cloth_material>(m, "ClothMaterial",
+                                     "Plain-old-data material parameters for the cloth simulator.")
+        .def(py::init([] { return chysx_cloth_material{0.0f, 0.0f, 0.0f, 0.05f, 0.0f, 0.0f, 0.0f, -9.81f}; }))
+        .def_readwrite("lame_mu", &chysx_cloth_material::lame_mu)
+        .def_readwrite("lame_lambda", &chysx_cloth_material::lame_lambda)
+        .def_readwrite("bending", &chysx_cloth_material::bending)
+        .def_readwrite("density", &chysx_cloth_material::density)
+        .def_readwrite("damping", &chysx_cloth_material::damping)
+        .def_readwrite("gx", &chysx_cloth_material::gx)
+        .def_readwrite("gy", &chysx_cloth_material::gy)
+        .def_readwrite("gz", &chysx_cloth_material::gz);
+
+    py::class_<PyClothSimulator>(m, "ClothSimulator", "Implicit-Euler cloth simulator (device-pointer API).")
+        .def(py::init<>())
+        .def("set_material",
+             [](PyClothSimulator& s, const chysx_cloth_material& mat) { check(chysx_cloth_set_material(s.h(), &mat)); },
+             py::arg("material"))
+        .def("material",
+             [](const PyClothSimulator& s) {
+                 chysx_cloth_material out;
+                 check(chysx_cloth_get_material(s.h(), &out));
+                 return out;
+             })
+        .def("set_external_buffers",
+             [](PyClothSimulator& s, std::uintptr_t pos, std::uintptr_t vel, int n, std::uintptr_t inv_mass,
+                std::uintptr_t force) { check(chysx_cloth_set_external_buffers(s.h(), pos, vel, n, inv_mass, force)); },
+             py::arg("pos_ptr"), py::arg("vel_ptr"), py::arg("particle_count"), py::arg("inv_mass_ptr") = 0,
+             py::arg("force_ptr") = 0)
+        .def("step",
+             [](PyClothSimulator& s, float dt, std::uintptr_t stream) { check(chysx_cloth_step(s.h(), dt, stream)); },
+             py::arg("dt"), py::arg("cuda_stream") = 0)
+        .def("set_pins",
+             [](PyClothSimulator& s, I32 indices, F32 targets, float stiffness) {
+                 if (indices.ndim() != 1) throw py::value_error("ClothSimulator.set_pins: indices must be 1-D");
+                 if (targets.ndim() != 2 || targets.shape(1) != 3)
+                     throw py::value_error("ClothSimulator.set_pins: targets must have shape (N, 3)");
+                 if (indices.shape(0) != targets.shape(0))
+                     throw py::value_error("ClothSimulator.set_pins: indices and targets must have the same length");
+                 check(chysx_cloth_set_pins(s.h(), indices.data(), targets.data(), (int)indices.shape(0), stiffness));
+             },
+             py::arg("indices"), py::arg("targets"), py::arg("stiffness") = 1.0e6f)
+        .def("clear_pins", [](PyClothSimulator& s) { check(chysx_cloth_clear_pins(s.h())); })
+        .def("num_pins",
+             [](const PyClothSimulator& s) {
+                 int n = 0;
+                 check(chysx_cloth_num_pins(s.h(), &n));
+                 return n;
+             })
+        .def("update_pin_targets",
+             [](PyClothSimulator& s, F32 targets, std::uintptr_t stream) {
+                 if (targets.ndim() != 2 || targets.shape(1) != 3)
+                     throw py::value_error(
+                         "ClothSimulator.update_pin_targets: targets must have shape (N, 3) and dtype float32");
+                 check(chysx_cloth_update_pin_targets(s.h(), targets.data(), (int)targets.shape(0), stream));
+             },
+             py::arg("targets"), py::arg("cuda_stream") = 0)
+        .def("set_mesh",
+             [](PyClothSimulator& s, I32 tris) {
+                 if (tris.ndim() != 2 || tris.shape(1) != 3)
+                     throw py::value_error("ClothSimulator.set_mesh: triangles must have shape (M, 3) and dtype int32");
+                 check(chysx_cloth_set_mesh(s.h(), tris.data(), (int)tris.shape(0)));
+             },
+             py::arg("triangles"))
+        .def("edges",
+             [](const PyClothSimulator& s) {
+                 int e = 0;
+                 check(chysx_cloth_num_edges(s.h(), &e));
+                 py::array_t<int32_t> out({e, 2});
+                 check(chysx_cloth_get_edges(s.h(), out.mutable_data()));
+                 return out;
+             })
+        .def("build_springs_from_current_positions",
+             [](PyClothSimulator& s, py::object stiffness, std::uintptr_t stream) {
+                 if (py::isinstance<py::array>(stiffness)) {
+                     F32 k = stiffness.cast<F32>();
+                     int e = 0;
+                     check(chysx_cloth_num_edges(s.h(), &e));
+                     if (k.ndim() != 1 || k.shape(0) != e)
+                         throw py::value_error("per-edge stiffness must have shape (num_edges,)");
+                     check(chysx_cloth_build_springs(s.h(), 0.0f, k.data(), stream));
+                 } else {
+                     check(chysx_cloth_build_springs(s.h(), stiffness.cast<float>(), nullptr, stream));
+                 }
+             },
+             py::arg("stiffness"), py::arg("cuda_stream") = 0)
+        .def("num_springs",
+             [](const PyClothSimulator& s) {
+                 int n = 0;
+                 check(chysx_cloth_num_springs(s.h(), &n));
+                 return n;
+             })
+        .def("redistribute_mass_area_weighted",
+             [](PyClothSimulator& s, float rho, std::uintptr_t inv_mass, int n, std::uintptr_t stream) {
+                 check(chysx_cloth_redistribute_mass(s.h(), rho, inv_mass, n, stream));
+             },
+             py::arg("surface_density"), py::arg("inv_mass_ptr"), py::arg("particle_count"),
+             py::arg("cuda_stream") = 0)
+        .def("build_fem_stretch_from_current_positions",
+             [](PyClothSimulator& s, py::object stiffness, std::uintptr_t stream) {
+                 if (py::isinstance<py::array>(stiffness)) {
+                     F32 k = stiffness.cast<F32>();
+                     if (k.ndim() != 1) throw py::value_error("per-triangle stiffness must be 1-D");
+                     check(chysx_cloth_build_fem_stretch(s.h(), 0.0f, k.data(), stream));
+                 } else {
+                     check(chysx_cloth_build_fem_stretch(s.h(), stiffness.cast<float>(), nullptr, stream));
+                 }
+             },
+             py::arg("stiffness"), py::arg("cuda_stream") = 0)
+        .def("set_pcg_iterations",
+             [](PyClothSimulator& s, int m) { check(chysx_cloth_set_pcg_iterations(s.h(), m)); }, py::arg("max_iter"))
+        .def("pcg_iterations",
+             [](const PyClothSimulator& s) {
+                 int m = 0;
+                 check(chysx_cloth_pcg_iterations(s.h(), &m));
+                 return m;
+             })
+        .def("set_solver",
+             [](PyClothSimulator& s, int max_iter, double rel_tol, const std::string& warm) {
+                 int w = -1;
+                 if (warm == "zero") w = CHYSX_WARM_ZERO;
+                 if (warm == "previous") w = CHYSX_WARM_PREVIOUS;
+                 if (warm == "learned") w = CHYSX_WARM_LEARNED;
+                 if (w < 0) throw py::value_error("warm_start must be 'zero', 'previous' or 'learned'");
+                 check(chysx_cloth_set_solver(s.h(), max_iter, rel_tol, w));
+             },
+             py::arg("max_iter") = 50, py::arg("rel_tol") = 0.0, py::arg("warm_start") = "previous")
+        .def("set_options",
+             [](PyClothSimulator& s, bool springs_in_step, bool apply_external_force, float fem_det_eps) {
+                 check(chysx_cloth_set_options(s.h(), springs_in_step, apply_external_force, fem_det_eps));
+             },
+             py::arg("springs_in_step") = true, py::arg("apply_external_force") = false,
+             py::arg("fem_det_eps") = 1.0e-6f)
+        .def("last_stats",
+             [](PyClothSimulator& s) {
+                 int it = 0, st = 0;
+                 double rr = 0.0;
+                 check(chysx_cloth_last_stats(s.h(), &it, &rr, &st));
+                 return py::make_tuple(it, rr, st);
+             },
+             "(iterations, relative residual ||r||/||b||, status) of the last step; synchronises.")
+        .def("num_particles",
+             [](const PyClothSimulator& s) {
+                 int n = 0;
+                 check(chysx_cloth_num_particles(s.h(), &n));
+                 return n;
+             })
+        .def("num_off_diag_blocks",
+             [](const PyClothSimulator& s) {
+                 int n = 0;
+                 check(chysx_cloth_num_off_diag_blocks(s.h(), &n));
+                 return n;
+             })
+        .def("debug_dump_last_solve", [](PyClothSimulator& s) {
+            int n = 0, nnz = 0;
+            check(chysx_cloth_num_particles(s.h(), &n));
+            check(chysx_cloth_num_off_diag_blocks(s.h(), &nnz));
+            py::array_t<float> diag({n, 3, 3});
+            py::array_t<int32_t> row_offsets({n + 1});
+            py::array_t<int32_t> col_indices({nnz});
+            py::array_t<float> values({nnz, 3, 3});
+            py::array_t<float> rhs({n, 3});
+            py::array_t<float> dx({n, 3});
+            if (n > 0)
+                check(chysx_cloth_debug_dump(s.h(), diag.mutable_data(), row_offsets.mutable_data(),
+                                             nnz > 0 ? col_indices.mutable_data() : nullptr,
+                                             nnz > 0 ? values.mutable_data() : nullptr, rhs.mutable_data(),
+                                             dx.mutable_data()));
+            return py::make_tuple(diag, row_offsets, col_indices, values, rhs, dx);
+        });
+}

@@ -1,0 +1,216 @@
+// Host topology builder; see topology.h for the layout.
+#include "topology.h"
+
+#include <algorithm>
+#include <stdexcept>
+#include <string>
+
+namespace chysx_b200 {
+
+namespace {
+
+void check_vertex(int v, int n) {
+    if (v < 0 || v >= n)
+        throw std::out_of_range("vertex index " + std::to_string(v) + " out of range [0, " +
+                                std::to_string(n) + ")");
+}
+
+// Lays out per-row variable-length lists as sliced ELL: returns the slice
+// offsets and fills `out` (pad value `pad`) through `emit(row, k) -> value`.
+template <class Count, class Emit, class T>
+void slice_layout(int n, int n_slices, Count count, Emit emit, T pad, std::vector<int>& off,
+                  std::vector<T>& out) {
+    off.assign(n_slices + 1, 0);
+    for (int s = 0; s < n_slices; ++s) {
+        int w = 0;
+        for (int l = 0; l < kSlice; ++l) {
+            const int r = s * kSlice + l;
+            if (r < n) w = std::max(w, count(r));
+        }
+        off[s + 1] = off[s] + w * kSlice;
+    }
+    out.assign(off.back(), pad);
+    for (int s = 0; s < n_slices; ++s) {
+        const int w = (off[s + 1] - off[s]) / kSlice;
+        for (int l = 0; l < kSlice; ++l) {
+            const int r = s * kSlice + l;
+            if (r >= n) continue;
+            const int c = count(r);
+            for (int k = 0; k < c && k < w; ++k) out[off[s] + k * kSlice + l] = emit(r, k);
+        }
+    }
+}
+
+}  // namespace
+
+void build_vertex_triangles(int n, const std::vector<int>& tris, std::vector<int>& off,
+                            std::vector<int>& list) {
+    const int T = (int)(tris.size() / 3);
+    off.assign(n + 1, 0);
+    for (int t = 0; t < T; ++t)
+        for (int a = 0; a < 3; ++a) {
+            check_vertex(tris[3 * t + a], n);
+            off[tris[3 * t + a] + 1]++;
+        }
+    for (int i = 0; i < n; ++i) off[i + 1] += off[i];
+    list.assign(off[n], 0);
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (int t = 0; t < T; ++t)
+        for (int a = 0; a < 3; ++a) list[fill[tris[3 * t + a]]++] = t;
+}
+
+void build_topology(int n, const std::vector<int>& tris, bool use_tris,
+                    const std::vector<int>& edges, bool use_springs,
+                    const std::vector<int>& pins, HostTopology& o) {
+    if (n < 0) throw std::invalid_argument("negative particle count");
+    o = HostTopology();
+    o.n = n;
+    o.n_slices = (n + kSlice - 1) / kSlice;
+    o.n_pad = o.n_slices * kSlice;
+    const int T = use_tris ? (int)(tris.size() / 3) : 0;
+    const int E = use_springs ? (int)(edges.size() / 2) : 0;
+
+    // ---- adjacency: triangle pairs (src/cloth/cloth_simulator.cu:720-739)
+    // plus spring edges, per-row sort + unique (src/sparse/block_csr.cu:111-135)
+    std::vector<int> raw_off(n + 1, 0);
+    for (int t = 0; t < T; ++t) {
+        const int* v = &tris[3 * t];
+        for (int a = 0; a < 3; ++a) check_vertex(v[a], n);
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                if (a != b && v[a] != v[b]) raw_off[v[a] + 1]++;
+    }
+    for (int e = 0; e < E; ++e) {
+        const int a = edges[2 * e], b = edges[2 * e + 1];
+        check_vertex(a, n);
+        check_vertex(b, n);
+        if (a != b) { raw_off[a + 1]++; raw_off[b + 1]++; }
+    }
+    for (int i = 0; i < n; ++i) raw_off[i + 1] += raw_off[i];
+    std::vector<int> raw(raw_off[n]);
+    {
+        std::vector<int> fill(raw_off.begin(), raw_off.end() - 1);
+        for (int t = 0; t < T; ++t) {
+            const int* v = &tris[3 * t];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    if (a != b && v[a] != v[b]) raw[fill[v[a]]++] = v[b];
+        }
+        for (int e = 0; e < E; ++e) {
+            const int a = edges[2 * e], b = edges[2 * e + 1];
+            if (a != b) { raw[fill[a]++] = b; raw[fill[b]++] = a; }
+        }
+    }
+    o.csr_ptr.assign(n + 1, 0);
+    o.csr_col.clear();
+    o.csr_col.reserve(raw.size() / 2 + 1);
+    for (int i = 0; i < n; ++i) {
+        auto b = raw.begin() + raw_off[i], e = raw.begin() + raw_off[i + 1];
+        std::sort(b, e);
+        auto last = std::unique(b, e);
+        const int deg = (int)(last - b);
+        if (deg > kMaxRowWidth)
+            throw std::runtime_error("particle " + std::to_string(i) + " has " + std::to_string(deg) +
+                                     " neighbours; at most " + std::to_string(kMaxRowWidth) +
+                                     " are supported");
+        o.csr_col.insert(o.csr_col.end(), b, last);
+        o.csr_ptr[i + 1] = (int)o.csr_col.size();
+    }
+    auto deg = [&](int r) { return o.csr_ptr[r + 1] - o.csr_ptr[r]; };
+    auto slot_of = [&](int r, int c) -> unsigned {
+        if (r == c) return kDiagSlot;
+        auto b = o.csr_col.begin() + o.csr_ptr[r], e = o.csr_col.begin() + o.csr_ptr[r + 1];
+        auto it = std::lower_bound(b, e, c);
+        if (it == e || *it != c) throw std::logic_error("topology: missing (row, col) pair");
+        return (unsigned)(it - b);
+    };
+
+    // ---- sliced ELL matrix pattern; pads point at the row itself
+    slice_layout(n, o.n_slices, deg, [&](int r, int k) { return o.csr_col[o.csr_ptr[r] + k]; }, 0,
+                 o.slice_off, o.col);
+    for (int s = 0; s < o.n_slices; ++s) {
+        const int w = (o.slice_off[s + 1] - o.slice_off[s]) / kSlice;
+        o.max_width = std::max(o.max_width, w);
+        for (int l = 0; l < kSlice; ++l) {
+            const int r = s * kSlice + l;
+            const int d = r < n ? deg(r) : 0;
+            for (int k = d; k < w; ++k) o.col[o.slice_off[s] + k * kSlice + l] = r;
+        }
+    }
+    o.csr_to_ell.assign(o.csr_col.size(), 0);
+    for (int r = 0; r < n; ++r) {
+        const int s = r / kSlice, l = r % kSlice;
+        for (int k = 0; k < deg(r); ++k) o.csr_to_ell[o.csr_ptr[r] + k] = o.slice_off[s] + k * kSlice + l;
+    }
+
+    // ---- triangle incidence (sorted by triangle id per row)
+    {
+        std::vector<int> cnt_off(n + 1, 0);
+        for (int t = 0; t < T; ++t)
+            for (int a = 0; a < 3; ++a) cnt_off[tris[3 * t + a] + 1]++;
+        for (int i = 0; i < n; ++i) cnt_off[i + 1] += cnt_off[i];
+        std::vector<int> ids(cnt_off[n]);
+        std::vector<uint32_t> meta(cnt_off[n]);
+        std::vector<int> fill(cnt_off.begin(), cnt_off.end() - 1);
+        for (int t = 0; t < T; ++t) {
+            const int* v = &tris[3 * t];
+            for (int a = 0; a < 3; ++a) {
+                const int r = v[a];
+                const unsigned s1 = slot_of(r, v[(a + 1) % 3]);
+                const unsigned s2 = slot_of(r, v[(a + 2) % 3]);
+                ids[fill[r]] = t;
+                meta[fill[r]] = (unsigned)a | (s1 << 8) | (s2 << 16);
+                fill[r]++;
+            }
+        }
+        auto cnt = [&](int r) { return cnt_off[r + 1] - cnt_off[r]; };
+        slice_layout(n, o.n_slices, cnt, [&](int r, int k) { return ids[cnt_off[r] + k]; }, -1,
+                     o.tinc_off, o.tinc);
+        std::vector<int> dummy_off;
+        slice_layout(n, o.n_slices, cnt, [&](int r, int k) { return meta[cnt_off[r] + k]; }, 0u,
+                     dummy_off, o.tinc_meta);
+    }
+    // ---- spring incidence
+    {
+        std::vector<int> cnt_off(n + 1, 0);
+        for (int e = 0; e < E; ++e) {
+            cnt_off[edges[2 * e] + 1]++;
+            cnt_off[edges[2 * e + 1] + 1]++;
+        }
+        for (int i = 0; i < n; ++i) cnt_off[i + 1] += cnt_off[i];
+        std::vector<int> ids(cnt_off[n]);
+        std::vector<uint32_t> meta(cnt_off[n]);
+        std::vector<int> fill(cnt_off.begin(), cnt_off.end() - 1);
+        for (int e = 0; e < E; ++e) {
+            const int a = edges[2 * e], b = edges[2 * e + 1];
+            ids[fill[a]] = e;
+            meta[fill[a]] = 0u | (slot_of(a, b) << 8);
+            fill[a]++;
+            ids[fill[b]] = e;
+            meta[fill[b]] = 1u | (slot_of(b, a) << 8);
+            fill[b]++;
+        }
+        auto cnt = [&](int r) { return cnt_off[r + 1] - cnt_off[r]; };
+        slice_layout(n, o.n_slices, cnt, [&](int r, int k) { return ids[cnt_off[r] + k]; }, -1,
+                     o.sinc_off, o.sinc);
+        std::vector<int> dummy_off;
+        slice_layout(n, o.n_slices, cnt, [&](int r, int k) { return meta[cnt_off[r] + k]; }, 0u,
+                     dummy_off, o.sinc_meta);
+    }
+    // ---- pins sorted by row, per-slice ranges
+    {
+        const int P = (int)pins.size();
+        for (int c = 0; c < P; ++c) check_vertex(pins[c], n);
+        o.pin_perm.resize(P);
+        for (int c = 0; c < P; ++c) o.pin_perm[c] = c;
+        std::stable_sort(o.pin_perm.begin(), o.pin_perm.end(),
+                         [&](int a, int b) { return pins[a] < pins[b]; });
+        o.pin_row.resize(P);
+        for (int c = 0; c < P; ++c) o.pin_row[c] = pins[o.pin_perm[c]];
+        o.pin_off.assign(o.n_slices + 1, 0);
+        for (int c = 0; c < P; ++c) o.pin_off[o.pin_row[c] / kSlice + 1]++;
+        for (int s = 0; s < o.n_slices; ++s) o.pin_off[s + 1] += o.pin_off[s];
+    }
+}
+
+}  // namespace chysx_b200

@@ -1,0 +1,63 @@
+// Host-side sparsity and gather-list construction for the cloth system.
+//
+// The global system keeps the reference's split storage (per-row diagonal
+// 3x3 block + off-diagonal block rows with sorted, unique columns,
+// src/sparse/block_csr.cu:91-147), laid out as a sliced ELLPACK matrix with
+// slices of kSlice = 32 consecutive rows (one warp): entry (row, k) of slice
+// s lives at slice_off[s] + k*32 + (row & 31), so a warp reading entry k of
+// its 32 rows issues one coalesced 128-byte load per component.  Rows shorter
+// than the slice width are padded with col = row and zero blocks.
+//
+// Assembly is row-owned instead of element-scatter: each row gets the list
+// of elements incident to it (triangle + its local vertex, spring + its
+// end), together with the slot in that row of every other element vertex,
+// so one thread writes its row's blocks exactly once with no atomics and no
+// zero-fill pass (replaces BlockCSR3::set_zero + resolve_slots + atomic
+// scatter, src/sparse/block_csr.cu:149-204, block_csr_atomic.cuh:33-45).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace chysx_b200 {
+
+constexpr int kSlice = 32;
+constexpr unsigned kDiagSlot = 0xFFu;   // "other vertex is this row": goes to the diagonal
+constexpr int kMaxRowWidth = 254;       // slots are stored in 8 bits
+
+struct HostTopology {
+    int n = 0;          // rows (particles)
+    int n_slices = 0;
+    int n_pad = 0;      // n_slices * 32
+    int max_width = 0;  // widest off-diagonal slice
+    // reference-format adjacency (row_offsets / col_indices)
+    std::vector<int> csr_ptr, csr_col;
+    // sliced ELL matrix pattern
+    std::vector<int> slice_off;  // [n_slices + 1], in entries (multiples of 32)
+    std::vector<int> col;        // [slice_off.back()]
+    std::vector<int> csr_to_ell; // ELL entry of each CSR entry (debug dump)
+    // triangle incidence: tri id, meta = local | slot_next << 8 | slot_prev << 16
+    std::vector<int> tinc_off, tinc;
+    std::vector<uint32_t> tinc_meta;
+    // spring incidence: edge id, meta = end | slot_other << 8
+    std::vector<int> sinc_off, sinc;
+    std::vector<uint32_t> sinc_meta;
+    // pins sorted by row; pin_perm[sorted] = caller's index
+    std::vector<int> pin_off, pin_row, pin_perm;
+    long long nnz() const { return (long long)csr_col.size(); }
+    long long ell_entries() const { return slice_off.empty() ? 0 : slice_off.back(); }
+};
+
+// Builds the pattern from triangles (if use_tris), spring edges (if
+// use_springs) and pins.  Throws std::out_of_range for a vertex index outside
+// [0, n) and std::runtime_error when a row exceeds kMaxRowWidth neighbours.
+void build_topology(int n, const std::vector<int>& tris, bool use_tris,
+                    const std::vector<int>& edges, bool use_springs,
+                    const std::vector<int>& pins, HostTopology& out);
+
+// Per-vertex incident-triangle lists (sorted by triangle id), used by the
+// deterministic mass redistribution.
+void build_vertex_triangles(int n, const std::vector<int>& tris, std::vector<int>& off,
+                            std::vector<int>& list);
+
+}  // namespace chysx_b200

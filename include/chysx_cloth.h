@@ -1,0 +1,174 @@
+/*
+ * chysx_cloth.h — C ABI of the B200-native implicit cloth step.
+ *
+ * Drop-in boundary for ChysX's ClothSimulator hot path
+ * (caixiao-0725/Ai-Phyiscs, src/cloth/cloth_simulator.h and the pybind11
+ * facade src/bindings.cpp:25-600).  Plain pointers and sizes only; device
+ * buffers are passed as uintptr_t (a cudaMalloc'd address), CUDA streams as
+ * uintptr_t (a cudaStream_t, 0 = legacy default stream), exactly as the
+ * reference's Python layer passes Warp pointers.
+ *
+ * Every function returns a status code (CHYSX_OK on success).  On failure
+ * chysx_last_error() returns a thread-local message.  The status codes map
+ * onto the exception types the reference raises:
+ *   CHYSX_ERR_INVALID_ARGUMENT -> std::invalid_argument (Python ValueError)
+ *   CHYSX_ERR_OUT_OF_RANGE     -> std::out_of_range     (Python IndexError)
+ *   CHYSX_ERR_RUNTIME          -> std::runtime_error    (Python RuntimeError)
+ *   CHYSX_ERR_CUDA             -> CUDA failure          (Python RuntimeError)
+ */
+#ifndef CHYSX_CLOTH_H_
+#define CHYSX_CLOTH_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    CHYSX_OK = 0,
+    CHYSX_ERR_INVALID_ARGUMENT = 1,
+    CHYSX_ERR_OUT_OF_RANGE = 2,
+    CHYSX_ERR_RUNTIME = 3,
+    CHYSX_ERR_CUDA = 4
+};
+
+/* Outcome of the last PCG solve (chysx_cloth_last_stats). */
+enum {
+    CHYSX_SOLVE_CONVERGED = 0, /* ||r||/||b|| <= rel_tol, or fixed count done */
+    CHYSX_SOLVE_MAX_ITER = 1,  /* rel_tol > 0 and max_iter reached first */
+    CHYSX_SOLVE_NONFINITE = 2  /* NaN/Inf met; caller's pos/vel left untouched */
+};
+
+/* Initial guess of the PCG solve. */
+enum {
+    CHYSX_WARM_ZERO = 0,     /* zero guess (plain PCG) */
+    CHYSX_WARM_PREVIOUS = 1, /* previous step's dx (reference behaviour,
+                                src/cloth/cloth_simulator.cu:1219-1228) */
+    CHYSX_WARM_LEARNED = 2   /* per-vertex network guess, zero-guess fallback */
+};
+
+/* POD material, field-for-field src/cloth/cloth_material.h:20-43. */
+typedef struct chysx_cloth_material {
+    float lame_mu;
+    float lame_lambda;
+    float bending;
+    float density;
+    float damping;
+    float gx;
+    float gy;
+    float gz;
+} chysx_cloth_material;
+
+typedef struct chysx_cloth chysx_cloth; /* opaque simulator handle */
+
+/* Thread-local message of the last failing call on this thread. */
+const char* chysx_last_error(void);
+
+/* ClothSimulator() / ~ClothSimulator(): src/cloth/cloth_simulator.h:67-75. */
+int chysx_cloth_create(chysx_cloth** out);
+int chysx_cloth_destroy(chysx_cloth* h);
+
+/* ClothSimulator::set_material (copy): src/cloth/cloth_simulator.h:81. */
+int chysx_cloth_set_material(chysx_cloth* h, const chysx_cloth_material* m);
+int chysx_cloth_get_material(const chysx_cloth* h, chysx_cloth_material* out);
+
+/* ClothSimulator::set_external_buffers: src/cloth/cloth_simulator.h:95-99,
+ * src/cloth/cloth_simulator.cu:248-258.  Borrowed float3 (12-byte AoS)
+ * device arrays; inv_mass / force may be 0.  Never copied or freed. */
+int chysx_cloth_set_external_buffers(chysx_cloth* h, uintptr_t pos, uintptr_t vel,
+                                     int particle_count, uintptr_t inv_mass,
+                                     uintptr_t force);
+
+/* ClothSimulator::set_mesh: src/cloth/cloth_simulator.cu:315-377.  Host
+ * int32 triangle triples; builds the sorted unique edge list. */
+int chysx_cloth_set_mesh(chysx_cloth* h, const int32_t* tris, int n_triangles);
+int chysx_cloth_num_edges(const chysx_cloth* h, int* out);
+int chysx_cloth_get_edges(const chysx_cloth* h, int32_t* out /* 2*num_edges */);
+
+/* ClothSimulator::set_pins / clear_pins / update_pin_targets:
+ * src/cloth/cloth_simulator.cu:277-313 (host index + float3 target arrays). */
+int chysx_cloth_set_pins(chysx_cloth* h, const int32_t* idx, const float* targets, int n,
+                         float stiffness);
+int chysx_cloth_clear_pins(chysx_cloth* h);
+int chysx_cloth_num_pins(const chysx_cloth* h, int* out);
+int chysx_cloth_update_pin_targets(chysx_cloth* h, const float* targets, int n,
+                                   uintptr_t stream);
+
+/* ClothSimulator::build_springs_from_current_positions:
+ * src/cloth/cloth_simulator.cu:379-398.  k_per_edge (host, num_edges
+ * floats, may be NULL) overrides the scalar stiffness per edge. */
+int chysx_cloth_build_springs(chysx_cloth* h, float stiffness, const float* k_per_edge,
+                              uintptr_t stream);
+int chysx_cloth_num_springs(const chysx_cloth* h, int* out);
+
+/* ClothSimulator::build_fem_stretch_from_current_positions:
+ * src/cloth/cloth_simulator.cu:400-421.  k_per_tri (host, may be NULL)
+ * overrides the scalar per-area stiffness per triangle. */
+int chysx_cloth_build_fem_stretch(chysx_cloth* h, float stiffness, const float* k_per_tri,
+                                  uintptr_t stream);
+
+/* ClothSimulator::redistribute_mass_area_weighted:
+ * src/cloth/cloth_simulator.cu:516-575.  Writes the caller's inv_mass. */
+int chysx_cloth_redistribute_mass(chysx_cloth* h, float surface_density, uintptr_t inv_mass,
+                                  int particle_count, uintptr_t stream);
+
+/* ClothSimulator::set_pcg_iterations / pcg_iterations:
+ * src/cloth/cloth_simulator.h:597-600. */
+int chysx_cloth_set_pcg_iterations(chysx_cloth* h, int max_iter);
+int chysx_cloth_pcg_iterations(const chysx_cloth* h, int* out);
+
+/* Solver controls the reference lacks (no counterpart; defaults reproduce
+ * the reference: max_iter 50, rel_tol 0 = fixed iteration count, warm start
+ * from the previous dx).  rel_tol > 0 stops when ||r||/||b|| <= rel_tol
+ * with FP64 norms. */
+int chysx_cloth_set_solver(chysx_cloth* h, int max_iter, double rel_tol, int warm_start);
+
+/* Behaviour switches (no counterpart in the reference).  springs_in_step:
+ * assemble springs into step() (the reference skips them,
+ * src/cloth/cloth_simulator.cu:921; default 1).  apply_external_force: use
+ * the force buffer in the predictor (the reference passes nullptr,
+ * src/cloth/cloth_simulator.cu:892-894; default 0).  fem_det_eps: rest-shape
+ * degeneracy threshold (src/constraint/cloth/triangle_stretch_constraint.cu:
+ * 39,88-91; default 1e-6). */
+int chysx_cloth_set_options(chysx_cloth* h, int springs_in_step, int apply_external_force,
+                            float fem_det_eps);
+
+/* ClothSimulator::step: src/cloth/cloth_simulator.cu:814-1261.  Enqueues the
+ * whole step (assembly, PCG, update) on `stream` as one CUDA graph launch and
+ * returns without synchronising. */
+int chysx_cloth_step(chysx_cloth* h, float dt, uintptr_t stream);
+
+/* Iterations, relative residual ||r||/||b|| and CHYSX_SOLVE_* status of the
+ * last step (synchronises the last step's stream).  Replaces
+ * PCGSolver::last_residual (src/solver/pcg_solver.cu:897-923). */
+int chysx_cloth_last_stats(chysx_cloth* h, int* iterations, double* rel_residual, int* status);
+
+/* ClothSimulator::num_particles / num_off_diag_blocks (used by the
+ * reference's debug dump, src/bindings.cpp:551-596). */
+int chysx_cloth_num_particles(const chysx_cloth* h, int* out);
+int chysx_cloth_num_off_diag_blocks(const chysx_cloth* h, int* out);
+
+/* debug_dump_last_solve in the reference's layout (src/bindings.cpp:551-596,
+ * src/cloth/cloth_simulator.cu:1272-1348): diag (N*9 row-major), row_offsets
+ * (N+1), col_indices (nnz), values (nnz*9), rhs (N*3), dx (N*3); host
+ * buffers, synchronises the device. */
+int chysx_cloth_debug_dump(chysx_cloth* h, float* diag, int32_t* row_offsets,
+                           int32_t* col_indices, float* values, float* rhs, float* dx);
+
+/* Host-only introspection of the off-diagonal block pattern the step
+ * assembles for a mesh (no counterpart in the reference; the equivalent there
+ * is BlockCSR3::build_topology, src/sparse/block_csr.cu:91-147, fed by
+ * src/cloth/cloth_simulator.cu:698-793).  Triangle pairs plus spring edges,
+ * sorted unique columns per row; row_offsets has n+1 entries, col_indices
+ * up to max_nnz.  Also reports the sliced-ELL entry count and widest slice.
+ * Needs no GPU. */
+int chysx_topology_pattern(int n, const int32_t* tris, int n_tris, const int32_t* edges, int n_edges,
+                           int32_t* row_offsets, int32_t* col_indices, int max_nnz, int* nnz_out,
+                           int* ell_entries_out, int* max_width_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHYSX_CLOTH_H_ */
