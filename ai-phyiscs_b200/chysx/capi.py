@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libchysx_cloth.so")
 
 OK, ERR_INVALID_ARGUMENT, ERR_OUT_OF_RANGE, ERR_RUNTIME, ERR_CUDA = range(5)
-SOLVE_CONVERGED, SOLVE_MAX_ITER, SOLVE_NONFINITE = range(3)
+SOLVE_CONVERGED, SOLVE_MAX_ITER, SOLVE_NONFINITE, SOLVE_KERNEL_ERROR = range(4)
 WARM = {"zero": 0, "previous": 1, "learned": 2}
 
 u = ctypes.c_uint64
@@ -59,6 +59,10 @@ SIGNATURES = {
     "chysx_cloth_num_particles": (ctypes.c_int, [H, ip]),
     "chysx_cloth_num_off_diag_blocks": (ctypes.c_int, [H, ip]),
     "chysx_cloth_debug_dump": (ctypes.c_int, [H, f32p, i32p, i32p, f32p, f32p, f32p]),
+    "chysx_cloth_set_tuning": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "chysx_cloth_launched_grid": (ctypes.c_int, [H, ip]),
+    "chysx_cloth_enable_timing": (ctypes.c_int, [H, ctypes.c_int]),
+    "chysx_cloth_last_timing": (ctypes.c_int, [H, f32p, f32p, f32p]),
     "chysx_topology_pattern": (ctypes.c_int, [ctypes.c_int, i32p, ctypes.c_int, i32p, ctypes.c_int,
                                               i32p, i32p, ctypes.c_int, ip, ip, ip]),
 }
@@ -171,6 +175,27 @@ class Cloth:
     def set_options(self, springs_in_step=True, apply_external_force=False, fem_det_eps=1.0e-6):
         check(self._L.chysx_cloth_set_options(self.h, int(springs_in_step), int(apply_external_force),
                                               fem_det_eps))
+
+    def set_tuning(self, solver_path=0, block=0, grid=0):
+        check(self._L.chysx_cloth_set_tuning(self.h, solver_path, block, grid))
+
+    def launched_grid(self):
+        g = ctypes.c_int()
+        check(self._L.chysx_cloth_launched_grid(self.h, ctypes.byref(g)))
+        return g.value
+
+    def num_off_diag_blocks(self):
+        v = ctypes.c_int()
+        check(self._L.chysx_cloth_num_off_diag_blocks(self.h, ctypes.byref(v)))
+        return v.value
+
+    def enable_timing(self, on=True):
+        check(self._L.chysx_cloth_enable_timing(self.h, int(on)))
+
+    def last_timing(self):
+        a, b, f = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        check(self._L.chysx_cloth_last_timing(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(f)))
+        return a.value, b.value, f.value
 
     def step(self, dt, stream=0):
         check(self._L.chysx_cloth_step(self.h, dt, stream))

@@ -1,14 +1,19 @@
 // Host orchestration of the B200-native cloth step and its C ABI
 // (include/chysx_cloth.h).
 //
-// One step() is one CUDA-graph launch:
+// One step() is one CUDA-graph launch.  Default (persistent) path:
+//
+//   assemble ─ reset ─ pcg_persistent (cooperative, all iterations) ─ finalize
+//
+// Alternative (loop) path, kept for A/B measurement:
 //
 //   assemble ─┬─(warm start)─ warm_init ─ warm_fixup ─┐
 //             └───────────────(zero guess)────────────┴─ WHILE(cond) { pcg_spmv ; pcg_update } ─ finalize
 //
-// The WHILE node's condition is written on the device by the last block of
-// each grid reduction (converged, max_iter, or NaN), so the whole step runs
-// with no host round trip and exactly as many iterations as the solve needs.
+// In the loop path the WHILE node's condition is written on the device by the
+// last block of each grid reduction (converged, max_iter, or NaN).  Either way
+// the whole step runs with no host round trip and exactly as many iterations
+// as the solve needs.
 // The graph is built once per topology / solver-mode change; per-step values
 // (dt, caller pointers) are patched into the two kernel nodes that read them.
 #include <cuda_runtime.h>
@@ -23,6 +28,7 @@
 
 #include "../../include/chysx_cloth.h"
 #include "cloth_kernels.cuh"
+#include "pcg_persistent.cuh"
 #include "topology.h"
 
 namespace chysx_b200 {
@@ -85,7 +91,11 @@ bool same_bytes(const T& a, const T& b) {
 
 class ClothSim {
 public:
-    ~ClothSim() { destroy_graph(); }
+    ~ClothSim() {
+        destroy_graph();
+        for (auto& e : ev_)
+            if (e) cudaEventDestroy(e);
+    }
 
     chysx_cloth_material mat{0.0f, 0.0f, 0.0f, 0.05f, 0.0f, 0.0f, 0.0f, -9.81f};
 
@@ -292,14 +302,57 @@ public:
     }
 
     void last_stats(int* iters, double* relres, int* status) {
-        SolveState s{};
+        int it = 0, st = 0;
+        double rr = 0.0, bb = 0.0;
         if (stepped_) {
             ck(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(last_stream_)), "cudaStreamSynchronize");
-            ck(cudaMemcpy(&s, d_state_.get(), sizeof(SolveState), cudaMemcpyDeviceToHost), "cudaMemcpy(state)");
+            if (graph_path_ == kPathPersistent) {
+                InstState s{};
+                ck(cudaMemcpy(&s, d_inst_.get(), sizeof(InstState), cudaMemcpyDeviceToHost), "cudaMemcpy(state)");
+                it = s.iter; st = s.status; rr = s.rr; bb = s.bb;
+            } else {
+                SolveState s{};
+                ck(cudaMemcpy(&s, d_state_.get(), sizeof(SolveState), cudaMemcpyDeviceToHost), "cudaMemcpy(state)");
+                it = s.iter; st = s.status; rr = s.rr; bb = s.bb;
+            }
         }
-        if (iters) *iters = s.iter;
-        if (relres) *relres = (s.bb > 0.0) ? std::sqrt(std::max(s.rr, 0.0) / s.bb) : 0.0;
-        if (status) *status = s.status;
+        if (iters) *iters = it;
+        if (relres) *relres = (bb > 0.0) ? std::sqrt(std::max(rr, 0.0) / bb) : 0.0;
+        if (status) *status = st;
+    }
+
+    // Solver kernel selection (no counterpart in the reference): path 0 =
+    // persistent cooperative PCG, 1 = graph WHILE loop of two kernels.
+    // block / grid of the persistent kernel (0 = automatic).
+    void set_tuning(int path, int block, int grid) {
+        if (path < 0 || path > 1) throw std::invalid_argument("set_tuning: path must be 0 or 1");
+        if (block != 0 && block != 128 && block != 256 && block != 512)
+            throw std::invalid_argument("set_tuning: block must be 0, 128, 256 or 512");
+        if (grid < 0) throw std::invalid_argument("set_tuning: grid must be >= 0");
+        solver_path_ = path;
+        pcg_block_ = block ? block : 256;
+        pcg_grid_req_ = grid;
+        graph_dirty_ = true;
+    }
+    int launched_grid() const { return plan_.grid; }
+
+    // Optional event-record nodes around the graph's phases (measurement only).
+    void enable_timing(int on) {
+        if ((on != 0) != timing_) graph_dirty_ = true;
+        timing_ = on != 0;
+        if (timing_ && !ev_[0])
+            for (auto& e : ev_) ck(cudaEventCreate(&e), "cudaEventCreate");
+    }
+    void last_timing(float* assemble_ms, float* solve_ms, float* finalize_ms) {
+        if (!timing_ || !stepped_ || !ev_[0]) throw std::runtime_error("timing is not enabled");
+        ck(cudaEventSynchronize(ev_[3]), "cudaEventSynchronize");
+        float a = 0.f, b = 0.f, c = 0.f;
+        ck(cudaEventElapsedTime(&a, ev_[0], ev_[1]), "cudaEventElapsedTime");
+        ck(cudaEventElapsedTime(&b, ev_[1], ev_[2]), "cudaEventElapsedTime");
+        ck(cudaEventElapsedTime(&c, ev_[2], ev_[3]), "cudaEventElapsedTime");
+        if (assemble_ms) *assemble_ms = a;
+        if (solve_ms) *solve_ms = b;
+        if (finalize_ms) *finalize_ms = c;
     }
 
     int num_particles() const { return n_; }
@@ -480,6 +533,152 @@ private:
     }
 
     void build_graph() {
+        if (solver_path_ == kPathPersistent) build_graph_persistent();
+        else build_graph_loop();
+    }
+
+    // Appends an event-record node after `dep` when timing is on.
+    cudaGraphNode_t timing_node(int k, cudaGraphNode_t dep) {
+        if (!timing_) return dep;
+        cudaGraphNode_t node;
+        ck(cudaGraphAddEventRecordNode(&node, graph_, dep ? &dep : nullptr, dep ? 1 : 0, ev_[k]),
+           "cudaGraphAddEventRecordNode");
+        return node;
+    }
+
+    const void* persistent_fn() const {
+        if (pcg_block_ == 128) return reinterpret_cast<const void*>(&pcg_persistent_kernel<128>);
+        if (pcg_block_ == 512) return reinterpret_cast<const void*>(&pcg_persistent_kernel<512>);
+        return reinterpret_cast<const void*>(&pcg_persistent_kernel<256>);
+    }
+
+    BatchPlan batch_plan() const {
+        BatchPlan bp;
+        bp.n_inst = plan_.n_inst;
+        bp.max_slices_per_cta = plan_.max_slices_per_cta;
+        bp.max_inst_per_cta = plan_.max_inst_per_cta;
+        bp.slice_inst = d_slice_inst_.get();
+        bp.inst_slice = d_inst_slice_.get();
+        bp.cta_slice = d_cta_slice_.get();
+        bp.cta_inst_lo = d_cta_inst_lo_.get();
+        bp.cta_inst_hi = d_cta_inst_hi_.get();
+        bp.inst_cta_lo = d_inst_cta_lo_.get();
+        bp.inst_slot = d_inst_slot_.get();
+        bp.slots = d_slots_.get();
+        bp.inst = d_inst_.get();
+        bp.bar = d_bar_.get();
+        return bp;
+    }
+
+    // Plans the persistent launch: as many co-resident CTAs as useful, one
+    // warp per slice at least.
+    void plan_persistent() {
+        int dev = 0, sms = 0;
+        ck(cudaGetDevice(&dev), "cudaGetDevice");
+        ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+        const int W = pcg_block_ / 32;
+        const int n_slices = std::max(1, topo_.n_slices);
+        // shared memory depends on the plan; iterate once with a generous bound
+        int grid = pcg_grid_req_ > 0 ? pcg_grid_req_ : std::max(1, (n_slices + W - 1) / W);
+        for (int pass = 0; pass < 3; ++pass) {
+            build_plan({0, n_slices}, grid, plan_);
+            pers_smem_ = (size_t)plan_.max_slices_per_cta * 4 * sizeof(double) +
+                         (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
+            if (pers_smem_ > 48 * 1024)
+                ck(cudaFuncSetAttribute(persistent_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pers_smem_),
+                   "cudaFuncSetAttribute(persistent smem)");
+            int per_sm = 0;
+            ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_fn(), pcg_block_, pers_smem_),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+            if (per_sm < 1) throw std::runtime_error("persistent PCG kernel cannot be resident (shared memory)");
+            const int cap = per_sm * sms;
+            if (plan_.grid <= cap) break;
+            grid = cap;
+        }
+        d_slice_inst_.upload(plan_.slice_inst);
+        d_inst_slice_.upload(plan_.inst_slice);
+        d_cta_slice_.upload(plan_.cta_slice);
+        d_cta_inst_lo_.upload(plan_.cta_inst_lo);
+        d_cta_inst_hi_.upload(plan_.cta_inst_hi);
+        d_inst_cta_lo_.upload(plan_.inst_cta_lo);
+        d_inst_slot_.upload(plan_.inst_slot);
+        d_slots_.resize((size_t)std::max(1, plan_.inst_slot.back()) * 4);
+        d_inst_.resize(plan_.n_inst);
+        d_inst_.zero();
+        d_bar_.resize(1);
+        d_bar_.zero();
+    }
+
+    void build_graph_persistent() {
+        destroy_graph();
+        if (asm_smem_ > 48 * 1024)
+            ck(cudaFuncSetAttribute(assemble_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asm_smem_),
+               "cudaFuncSetAttribute(assemble smem)");
+        plan_persistent();
+        ck(cudaGraphCreate(&graph_, 0), "cudaGraphCreate");
+        DevTopo t = dev_topo();
+        ElemData el = elem_data();
+        Vecs v = vecs();
+        SolveState* st = d_state_.get();
+        double* part = d_part_.get();
+        BatchPlan bp = batch_plan();
+        const bool warm = warm_mode_ != CHYSX_WARM_ZERO;
+        int zero_guess = warm ? 0 : 1;
+        int warm_i = warm ? 1 : 0;
+        cur_args_ = step_args(1.0f / 60.0f);
+        cur_cfg_ = solver_cfg();
+        cudaGraphConditionalHandle no_cond = 0;
+        void* aargs[] = {&cur_args_, &el, &t, &v, &st, &part, &cur_cfg_, &zero_guess, &no_cond};
+        cudaKernelNodeParams ap;
+        asm_params(ap, aargs);
+        cudaGraphNode_t t0 = timing_node(0, nullptr);
+        ck(cudaGraphAddKernelNode(&asm_node_, graph_, t0 ? &t0 : nullptr, t0 ? 1 : 0, &ap), "add assemble node");
+        cudaGraphNode_t t1 = timing_node(1, asm_node_);
+        cudaGraphNode_t reset;
+        {
+            void* rargs[] = {&bp};
+            cudaKernelNodeParams p{};
+            p.func = reinterpret_cast<void*>(&pcg_persistent_reset_kernel);
+            p.gridDim = dim3(grid_for(std::max(1, plan_.n_inst), 256));
+            p.blockDim = dim3(256);
+            p.kernelParams = rargs;
+            ck(cudaGraphAddKernelNode(&reset, graph_, &t1, 1, &p), "add reset node");
+        }
+        {
+            void* pargs[] = {&t, &v, &bp, &cur_cfg_, &warm_i};
+            cudaKernelNodeParams p{};
+            p.func = const_cast<void*>(persistent_fn());
+            p.gridDim = dim3(plan_.grid);
+            p.blockDim = dim3(pcg_block_);
+            p.sharedMemBytes = (unsigned)pers_smem_;
+            p.kernelParams = pargs;
+            ck(cudaGraphAddKernelNode(&pcg_node_, graph_, &reset, 1, &p), "add persistent PCG node");
+            cudaLaunchAttributeValue coop{};
+            coop.cooperative = 1;
+            ck(cudaGraphKernelNodeSetAttribute(pcg_node_, cudaLaunchAttributeCooperative, &coop),
+               "cooperative attribute");
+        }
+        {
+            const int vgrid = std::max(1, grid_for(n_, kVecBlock));
+            void* fargs[] = {&cur_args_, &v, &bp};
+            cudaKernelNodeParams p{};
+            p.func = reinterpret_cast<void*>(&finalize_batch_kernel);
+            p.gridDim = dim3(vgrid);
+            p.blockDim = dim3(kVecBlock);
+            p.kernelParams = fargs;
+            cudaGraphNode_t t2 = timing_node(2, pcg_node_);
+            ck(cudaGraphAddKernelNode(&fin_node_, graph_, &t2, 1, &p), "add finalize node");
+            timing_node(3, fin_node_);
+        }
+        ck(cudaGraphInstantiate(&exec_, graph_, 0), "cudaGraphInstantiate(step)");
+        graph_path_ = kPathPersistent;
+        graph_dirty_ = false;
+        node_args_ = cur_args_;
+        node_cfg_ = cur_cfg_;
+        nodes_valid_ = true;
+    }
+
+    void build_graph_loop() {
         destroy_graph();
         if (asm_smem_ > 48 * 1024)
             ck(cudaFuncSetAttribute(assemble_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asm_smem_),
@@ -501,8 +700,9 @@ private:
         void* aargs[] = {&cur_args_, &el, &t, &v, &st, &part, &cur_cfg_, &zero_guess, &cond};
         cudaKernelNodeParams ap;
         asm_params(ap, aargs);
-        ck(cudaGraphAddKernelNode(&asm_node_, graph_, nullptr, 0, &ap), "add assemble node");
-        cudaGraphNode_t last = asm_node_;
+        cudaGraphNode_t t0 = timing_node(0, nullptr);
+        ck(cudaGraphAddKernelNode(&asm_node_, graph_, t0 ? &t0 : nullptr, t0 ? 1 : 0, &ap), "add assemble node");
+        cudaGraphNode_t last = timing_node(1, asm_node_);
 
         const int vgrid = std::max(1, grid_for(n_, kVecBlock));
         if (warm) {
@@ -553,9 +753,12 @@ private:
             p.gridDim = dim3(vgrid);
             p.blockDim = dim3(kVecBlock);
             p.kernelParams = fargs;
-            ck(cudaGraphAddKernelNode(&fin_node_, graph_, &loop, 1, &p), "add finalize node");
+            cudaGraphNode_t t2 = timing_node(2, loop);
+            ck(cudaGraphAddKernelNode(&fin_node_, graph_, &t2, 1, &p), "add finalize node");
+            timing_node(3, fin_node_);
         }
         ck(cudaGraphInstantiate(&exec_, graph_, 0), "cudaGraphInstantiate(step)");
+        graph_path_ = kPathLoop;
         graph_dirty_ = false;
         // node args as instantiated; the first step patches them
         node_args_ = cur_args_;
@@ -573,6 +776,34 @@ private:
         SolveState* st = d_state_.get();
         double* part = d_part_.get();
         int zero_guess = warm_mode_ != CHYSX_WARM_ZERO ? 0 : 1;
+        if (graph_path_ == kPathPersistent) {
+            cudaGraphConditionalHandle no_cond = 0;
+            BatchPlan bp = batch_plan();
+            int warm_i = 1 - zero_guess;
+            void* aargs[] = {&a, &el, &t, &v, &st, &part, &c, &zero_guess, &no_cond};
+            cudaKernelNodeParams ap;
+            asm_params(ap, aargs);
+            ck(cudaGraphExecKernelNodeSetParams(exec_, asm_node_, &ap), "update assemble node");
+            void* pargs[] = {&t, &v, &bp, &c, &warm_i};
+            cudaKernelNodeParams pp{};
+            pp.func = const_cast<void*>(persistent_fn());
+            pp.gridDim = dim3(plan_.grid);
+            pp.blockDim = dim3(pcg_block_);
+            pp.sharedMemBytes = (unsigned)pers_smem_;
+            pp.kernelParams = pargs;
+            ck(cudaGraphExecKernelNodeSetParams(exec_, pcg_node_, &pp), "update persistent PCG node");
+            void* fargs[] = {&a, &v, &bp};
+            cudaKernelNodeParams fp{};
+            fp.func = reinterpret_cast<void*>(&finalize_batch_kernel);
+            fp.gridDim = dim3(std::max(1, grid_for(n_, kVecBlock)));
+            fp.blockDim = dim3(kVecBlock);
+            fp.kernelParams = fargs;
+            ck(cudaGraphExecKernelNodeSetParams(exec_, fin_node_, &fp), "update finalize node");
+            node_args_ = a;
+            node_cfg_ = c;
+            nodes_valid_ = true;
+            return;
+        }
         cudaGraphConditionalHandle cond = cond_;
         void* aargs[] = {&a, &el, &t, &v, &st, &part, &c, &zero_guess, &cond};
         cudaKernelNodeParams ap;
@@ -623,6 +854,20 @@ private:
     DevBuf<SolveState> d_state_;
     int asm_block_ = 128;
     size_t asm_smem_ = 0;
+    // persistent PCG plan
+    static constexpr int kPathPersistent = 0, kPathLoop = 1;
+    int solver_path_ = kPathPersistent, graph_path_ = kPathPersistent;
+    int pcg_block_ = 256, pcg_grid_req_ = 0;
+    HostPlan plan_;
+    size_t pers_smem_ = 0;
+    DevBuf<int> d_slice_inst_, d_inst_slice_, d_cta_slice_, d_cta_inst_lo_, d_cta_inst_hi_, d_inst_cta_lo_,
+        d_inst_slot_;
+    DevBuf<double> d_slots_;
+    DevBuf<InstState> d_inst_;
+    DevBuf<GridBarrier> d_bar_;
+    cudaGraphNode_t pcg_node_ = nullptr;
+    bool timing_ = false;
+    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     // graph
     bool graph_dirty_ = true, nodes_valid_ = false;
     cudaGraph_t graph_ = nullptr;
@@ -799,6 +1044,25 @@ int chysx_cloth_debug_dump(chysx_cloth* h, float* diag, int32_t* rp, int32_t* co
                            float* dx) {
     CHYSX_H(h);
     return guard([&] { h->sim.debug_dump(diag, rp, col, vals, rhs, dx); });
+}
+
+int chysx_cloth_set_tuning(chysx_cloth* h, int solver_path, int block, int grid) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_tuning(solver_path, block, grid); });
+}
+int chysx_cloth_launched_grid(const chysx_cloth* h, int* out) {
+    CHYSX_H(h);
+    if (out) *out = h->sim.launched_grid();
+    return CHYSX_OK;
+}
+
+int chysx_cloth_enable_timing(chysx_cloth* h, int on) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.enable_timing(on); });
+}
+int chysx_cloth_last_timing(chysx_cloth* h, float* assemble_ms, float* solve_ms, float* finalize_ms) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.last_timing(assemble_ms, solve_ms, finalize_ms); });
 }
 
 int chysx_topology_pattern(int n, const int32_t* tris, int n_tris, const int32_t* edges, int n_edges,

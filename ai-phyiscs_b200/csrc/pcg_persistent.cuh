@@ -1,0 +1,457 @@
+// Persistent block-Jacobi PCG over one or many cloth instances.
+//
+// One cooperative launch runs the whole solve: the CTAs stay resident and
+// meet at a software grid barrier twice per iteration (after A p, after the
+// x/r/z update), replacing the reference's 8 launches per iteration
+// (src/solver/pcg_solver.cu:542-592) and the two-kernel graph loop.  The same
+// kernel solves a packed batch: every instance owns a contiguous range of
+// 32-row slices, keeps its own rho/alpha/beta/iteration count, and stops
+// (its rows are skipped) when ||r_b|| <= tol ||b_b|| or max_iter is reached;
+// the kernel ends when every instance is done.
+//
+// Reductions are deterministic: per-slice FP64 warp sums -> per-(CTA,
+// instance) segment sums in fixed slice order -> per-instance totals summed
+// over the segment slots in CTA order by every CTA that needs them.
+//
+// The barrier waits are bounded (globaltimer); on a timeout a CTA raises
+// the barrier's error flag, every CTA leaves the loop at its next barrier,
+// and the solve status becomes kSolveKernelError so the caller's buffers
+// are left untouched.
+#pragma once
+
+#include "cloth_kernels.cuh"
+
+namespace chysx_b200 {
+
+constexpr int kSolveKernelError = 3;
+constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
+
+struct alignas(128) GridBarrier {
+    unsigned count;
+    unsigned pad0[31];
+    unsigned gen;
+    unsigned pad1[31];
+    int error;
+    unsigned ndone;  // instances finished
+    unsigned pad2[30];
+};
+
+struct InstState {
+    double rho, rr, bb, tol2, rr0;
+    int iter, status, done, fallback;
+};
+
+struct BatchPlan {
+    int n_inst;
+    int max_slices_per_cta;
+    int max_inst_per_cta;
+    const int* __restrict__ slice_inst;   // [n_slices] instance of each slice
+    const int* __restrict__ inst_slice;   // [n_inst + 1] slice range of each instance
+    const int* __restrict__ cta_slice;    // [grid + 1] slice range of each CTA
+    const int* __restrict__ cta_inst_lo;  // [grid] first instance a CTA touches
+    const int* __restrict__ cta_inst_hi;  // [grid] last instance (inclusive), lo-1 if none
+    const int* __restrict__ inst_cta_lo;  // [n_inst] first CTA touching an instance
+    const int* __restrict__ inst_slot;    // [n_inst + 1] segment-slot ranges
+    double* slots;                        // [inst_slot[n_inst] * 4]
+    InstState* inst;                      // [n_inst]
+    GridBarrier* bar;
+};
+
+struct LocalInst {
+    double rho, rr, bb, tol2, sigma;
+    float alpha, beta;
+    int iter, done, status, fallback;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Returns false (uniformly across the CTA) once any CTA has flagged an error.
+__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned& gen, int* s_flag) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned g = gen;
+        const unsigned arrived = atomicAdd(&gb->count, 1u);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(&gb->count, 0u);
+            __threadfence();
+            atomicExch(&gb->gen, g + 1u);
+        } else {
+            const unsigned long long t0 = global_ns();
+            unsigned spins = 0;
+            while (ld_acquire_gpu(&gb->gen) == g) {
+                if ((++spins & 255u) == 0) {
+                    if (*(volatile int*)&gb->error) break;
+                    if (global_ns() - t0 > kBarrierTimeoutNs) {
+                        atomicExch(&gb->error, 1);
+                        break;
+                    }
+                }
+            }
+        }
+        __threadfence();
+        gen = g + 1u;
+        *s_flag = *(volatile int*)&gb->error;
+    }
+    __syncthreads();
+    return *s_flag == 0;
+}
+
+__device__ __forceinline__ float4 ldcg4(const float4* p) { return __ldcg(p); }
+
+// ---------------------------------------------------------------------------
+// Segmented reductions
+// ---------------------------------------------------------------------------
+// spart[(s - s0) * 4 + q] holds slice partials; write, for every instance
+// this CTA touches, the sum over its slices into the instance's slot.
+template <int BLOCK, int NV>
+__device__ __forceinline__ void write_segment_slots(const BatchPlan& bp, const double* spart, int s0, int s1,
+                                                    int il0, int il1) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int W = BLOCK / 32;
+    for (int b = il0 + warp; b <= il1; b += W) {
+        const int lo = max(s0, bp.inst_slice[b]), hi = min(s1, bp.inst_slice[b + 1]);
+        double acc[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+        for (int s = lo + lane; s < hi; s += 32) {
+#pragma unroll
+            for (int q = 0; q < NV; ++q) acc[q] += spart[(s - s0) * 4 + q];
+        }
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        }
+        if (lane == 0) {
+            const int slot = bp.inst_slot[b] + ((int)blockIdx.x - bp.inst_cta_lo[b]);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) bp.slots[(size_t)slot * 4 + q] = acc[q];
+        }
+    }
+}
+
+// Warp `warp` sums instance b's slots (after a barrier); every lane gets it.
+template <int NV>
+__device__ __forceinline__ void read_instance_total(const BatchPlan& bp, int b, double (&out)[NV]) {
+    const int lane = threadIdx.x & 31;
+    const int lo = bp.inst_slot[b], hi = bp.inst_slot[b + 1];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) out[q] = 0.0;
+    for (int k = lo + lane; k < hi; k += 32) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) out[q] += __ldcg(bp.slots + (size_t)k * 4 + q);
+    }
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) out[q] += __shfl_xor_sync(0xffffffffu, out[q], o);
+    }
+}
+
+__device__ __forceinline__ double warp_sum(double x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+// ---------------------------------------------------------------------------
+// The kernel
+// ---------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm) {
+    extern __shared__ double s_mem[];
+    __shared__ int s_flag;
+    __shared__ int s_exit;
+    constexpr int W = BLOCK / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
+    const int il0 = bp.cta_inst_lo[blockIdx.x], il1 = bp.cta_inst_hi[blockIdx.x];
+    double* spart = s_mem;
+    LocalInst* li = reinterpret_cast<LocalInst*>(s_mem + (size_t)bp.max_slices_per_cta * 4);
+    GridBarrier* gb = bp.bar;
+    unsigned gen = 0;
+    if (threadIdx.x == 0) {
+        gen = *(volatile unsigned*)&gb->gen;
+        s_flag = 0;
+    }
+    bool ok = true;
+
+    // ---- phase 0: initial residual and per-instance start ----------------
+    // zero guess: r = b, z = M^-1 b were written by the assembly kernel.
+    // warm guess: r = b - A x0, z = M^-1 r (pcg_solver.cu:29-51).
+    for (int s = s0 + warp; s < s1; s += W) {
+        const int i = s * 32 + lane;
+        double rz = 0.0, rr = 0.0, bb = 0.0, bmb = 0.0;
+        if (i < t.n) {
+            const float3 b = xyz(v.b[i]);
+            const S6 Mi = ld6(t.minv + (size_t)s * 192 + lane);
+            const float3 zb = mul(Mi, b);
+            bb = (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z;
+            bmb = (double)b.x * zb.x + (double)b.y * zb.y + (double)b.z * zb.z;
+            if (warm) {
+                const int so = t.slice_off[s];
+                const int w = (t.slice_off[s + 1] - so) >> 5;
+                const S6 D = ld6(t.diag + (size_t)s * 192 + lane);
+                float3 ax = mul(D, xyz(v.x[i]));
+                const float* vb = t.val + (size_t)so * 6 + lane;
+                for (int k = 0; k < w; ++k) {
+                    const int j = t.col[so + k * 32 + lane];
+                    ax = ax + mul(ld6(vb + k * 192), xyz(v.x[j]));
+                }
+                const float3 r = b - ax;
+                const float3 z = mul(Mi, r);
+                v.r[i] = f4(r);
+                v.z[i] = f4(z);
+                rz = (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
+                rr = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
+            } else {
+                rz = bmb;
+                rr = bb;
+            }
+        }
+        rz = warp_sum(rz); rr = warp_sum(rr); bb = warp_sum(bb); bmb = warp_sum(bmb);
+        if (lane == 0) {
+            double* sp = spart + (s - s0) * 4;
+            sp[0] = rz; sp[1] = rr; sp[2] = bb; sp[3] = bmb;
+        }
+    }
+    __syncthreads();
+    write_segment_slots<BLOCK, 4>(bp, spart, s0, s1, il0, il1);
+    ok = grid_sync(gb, gen, &s_flag);
+    if (ok) {
+        for (int b = il0 + warp; b <= il1; b += W) {
+            double tot[4];
+            read_instance_total<4>(bp, b, tot);
+            if (lane == 0) {
+                LocalInst& L = li[b - il0];
+                const double bb = tot[2];
+                const bool warm_ok = !warm || (isfinite(tot[0]) && isfinite(tot[1]) && tot[1] <= bb);
+                L.fallback = warm_ok ? 0 : 1;
+                L.rho = warm_ok ? tot[0] : tot[3];
+                L.rr = warm_ok ? tot[1] : bb;
+                L.bb = bb;
+                L.tol2 = cfg.rel_tol * cfg.rel_tol * bb;
+                L.iter = 0;
+                L.alpha = 0.0f;
+                L.beta = 0.0f;
+                const bool bad = !isfinite(L.rho) || !isfinite(L.rr) || !isfinite(bb);
+                const bool conv = cfg.use_tol && L.rr <= L.tol2;
+                L.status = bad ? kSolveNonfinite : kSolveConverged;
+                L.done = (bad || conv || cfg.max_iter <= 0) ? 1 : 0;
+                if ((int)blockIdx.x == bp.inst_cta_lo[b]) {
+                    InstState& G = bp.inst[b];
+                    G.rr0 = L.rr;
+                    G.bb = bb;
+                    G.fallback = L.fallback;
+                    if (L.done) {
+                        G.rho = L.rho; G.rr = L.rr; G.iter = 0; G.status = L.status; G.done = 1;
+                        atomicAdd(&gb->ndone, 1u);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (warm) {
+            // zero-guess fallback for instances whose guess was worse than zero
+            bool any = false;
+            for (int b = il0; b <= il1; ++b) any |= li[b - il0].fallback != 0;
+            if (any) {
+                for (int s = s0 + warp; s < s1; s += W) {
+                    const int i = s * 32 + lane;
+                    if (i >= t.n || !li[bp.slice_inst[s] - il0].fallback) continue;
+                    const S6 Mi = ld6(t.minv + (size_t)s * 192 + lane);
+                    const float4 b = v.b[i];
+                    v.x[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    v.r[i] = b;
+                    v.z[i] = f4(mul(Mi, xyz(b)));
+                }
+            }
+            ok = grid_sync(gb, gen, &s_flag);
+        }
+    }
+
+    // ---- iterations ---------------------------------------------------------
+    const int iter_cap = cfg.max_iter + 2;  // belt: every instance is done by max_iter
+    for (int guard = 0; ok && guard < iter_cap; ++guard) {
+        // phase 1: p = z + beta p (own row and recomputed for neighbours),
+        // Ap = A p, sigma = p.Ap
+        for (int s = s0 + warp; s < s1; s += W) {
+            const LocalInst& L = li[bp.slice_inst[s] - il0];
+            const int i = s * 32 + lane;
+            double sig = 0.0;
+            if (!L.done && i < t.n) {
+                const bool first = L.iter == 0;
+                const float beta = L.beta;
+                const float4* pold = (L.iter & 1) ? v.p1 : v.p0;
+                float4* pnew = (L.iter & 1) ? v.p0 : v.p1;
+                const int so = t.slice_off[s];
+                const int w = (t.slice_off[s + 1] - so) >> 5;
+                const float4 zi = ldcg4(v.z + i);
+                float3 pi = xyz(zi);
+                if (!first) {
+                    const float4 po = ldcg4(pold + i);
+                    pi = f3(fmaf(beta, po.x, zi.x), fmaf(beta, po.y, zi.y), fmaf(beta, po.z, zi.z));
+                }
+                pnew[i] = f4(pi);
+                float3 acc = mul(ld6(t.diag + (size_t)s * 192 + lane), pi);
+                const float* vb = t.val + (size_t)so * 6 + lane;
+                const int* cb = t.col + so + lane;
+                for (int k = 0; k < w; ++k) {
+                    const int j = cb[k * 32];
+                    const S6 B = ld6(vb + k * 192);
+                    const float4 zj = ldcg4(v.z + j);
+                    float3 pj = xyz(zj);
+                    if (!first) {
+                        const float4 po = ldcg4(pold + j);
+                        pj = f3(fmaf(beta, po.x, zj.x), fmaf(beta, po.y, zj.y), fmaf(beta, po.z, zj.z));
+                    }
+                    acc = acc + mul(B, pj);
+                }
+                v.ap[i] = f4(acc);
+                sig = (double)pi.x * acc.x + (double)pi.y * acc.y + (double)pi.z * acc.z;
+            }
+            sig = warp_sum(sig);
+            if (lane == 0) spart[(s - s0) * 4] = sig;
+        }
+        __syncthreads();
+        write_segment_slots<BLOCK, 1>(bp, spart, s0, s1, il0, il1);
+        ok = grid_sync(gb, gen, &s_flag);
+        if (!ok) break;
+        // ndone only changes in phase 3 and phase 0, i.e. never between this
+        // barrier and the next, so every CTA takes the same decision here
+        if (threadIdx.x == 0) s_exit = *(volatile unsigned*)&gb->ndone >= (unsigned)bp.n_inst;
+        __syncthreads();
+        if (s_exit) break;
+
+        // phase 2: alpha = rho / sigma; x += alpha p; r -= alpha Ap; z = M^-1 r
+        for (int b = il0 + warp; b <= il1; b += W) {
+            LocalInst& L = li[b - il0];
+            if (L.done) continue;
+            double tot[1];
+            read_instance_total<1>(bp, b, tot);
+            if (lane == 0) {
+                const double sigma = tot[0];
+                const double alpha = (sigma > 1.0e-37 || sigma < -1.0e-37) ? L.rho / sigma : 0.0;
+                L.sigma = sigma;
+                L.alpha = (float)alpha;
+                if (!isfinite(sigma) || !isfinite(alpha)) L.status = kSolveNonfinite;
+            }
+        }
+        __syncthreads();
+        for (int s = s0 + warp; s < s1; s += W) {
+            const LocalInst& L = li[bp.slice_inst[s] - il0];
+            const int i = s * 32 + lane;
+            double rz = 0.0, rr = 0.0;
+            if (!L.done && i < t.n) {
+                const float alpha = L.alpha;
+                const float4 pi = ((L.iter & 1) ? v.p0 : v.p1)[i];
+                const float4 api = v.ap[i], xi = v.x[i], ri = v.r[i];
+                const float3 xn = f3(fmaf(alpha, pi.x, xi.x), fmaf(alpha, pi.y, xi.y), fmaf(alpha, pi.z, xi.z));
+                const float3 rn = f3(fmaf(-alpha, api.x, ri.x), fmaf(-alpha, api.y, ri.y), fmaf(-alpha, api.z, ri.z));
+                const float3 zn = mul(ld6(t.minv + (size_t)s * 192 + lane), rn);
+                v.x[i] = f4(xn);
+                v.r[i] = f4(rn);
+                v.z[i] = f4(zn);
+                rz = (double)rn.x * zn.x + (double)rn.y * zn.y + (double)rn.z * zn.z;
+                rr = (double)rn.x * rn.x + (double)rn.y * rn.y + (double)rn.z * rn.z;
+            }
+            rz = warp_sum(rz);
+            rr = warp_sum(rr);
+            if (lane == 0) {
+                spart[(s - s0) * 4] = rz;
+                spart[(s - s0) * 4 + 1] = rr;
+            }
+        }
+        __syncthreads();
+        write_segment_slots<BLOCK, 2>(bp, spart, s0, s1, il0, il1);
+        ok = grid_sync(gb, gen, &s_flag);
+        if (!ok) break;
+
+        // phase 3: beta, iteration count, convergence (pcg_solver.cu:436-454)
+        for (int b = il0 + warp; b <= il1; b += W) {
+            LocalInst& L = li[b - il0];
+            if (L.done) continue;
+            double tot[2];
+            read_instance_total<2>(bp, b, tot);
+            if (lane == 0) {
+                const double rho_new = tot[0], rr = tot[1];
+                const double beta = (L.rho > 1.0e-37 || L.rho < -1.0e-37) ? rho_new / L.rho : 0.0;
+                L.beta = (float)beta;
+                L.rho = rho_new;
+                L.rr = rr;
+                L.iter += 1;
+                const bool bad = L.status == kSolveNonfinite || !isfinite(rho_new) || !isfinite(rr);
+                const bool conv = cfg.use_tol && rr <= L.tol2;
+                int done = 0;
+                if (bad) { L.status = kSolveNonfinite; done = 1; }
+                else if (conv) { L.status = kSolveConverged; done = 1; }
+                else if (L.iter >= cfg.max_iter) { L.status = cfg.use_tol ? kSolveMaxIter : kSolveConverged; done = 1; }
+                if (done) {
+                    L.done = 1;
+                    if ((int)blockIdx.x == bp.inst_cta_lo[b]) {
+                        InstState& G = bp.inst[b];
+                        G.rho = L.rho; G.rr = L.rr; G.iter = L.iter; G.status = L.status; G.done = 1;
+                        atomicAdd(&gb->ndone, 1u);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // a barrier failure leaves every unfinished instance flagged
+    if (!ok && threadIdx.x == 0) {
+        for (int b = il0; b <= il1; ++b) {
+            if ((int)blockIdx.x == bp.inst_cta_lo[b]) {
+                InstState& G = bp.inst[b];
+                G.status = kSolveKernelError;
+                G.iter = li[b - il0].iter;
+                G.done = 1;
+            }
+        }
+    }
+}
+
+// x_{n+1} = x_n + dx, v = dx/dt * exp(-c dt) (cloth_simulator.cu:222-244) for
+// the rows of every instance whose solve finished without NaN/Inf or a
+// kernel error; other instances keep the caller's state.
+__global__ void finalize_batch_kernel(StepArgs a, Vecs v, BatchPlan bp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const int st = bp.inst[bp.slice_inst[i >> 5]].status;
+    if (st == kSolveNonfinite || st == kSolveKernelError) return;
+    const float4 d = v.x[i];
+    const float3 xn = ld3(a.pos, i);
+    st3(a.pos, i, f3(xn.x + d.x, xn.y + d.y, xn.z + d.z));
+    const float inv_dt = 1.0f / a.dt;
+    float3 vn = f3(d.x * inv_dt, d.y * inv_dt, d.z * inv_dt);
+    if (a.damping > 0.0f) vn = vn * expf(-a.damping * a.dt);
+    st3(a.vel, i, vn);
+}
+
+// Resets the barrier and per-instance states before a solve.
+__global__ void pcg_persistent_reset_kernel(BatchPlan bp) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b == 0) {
+        bp.bar->count = 0u;
+        bp.bar->error = 0;
+        bp.bar->ndone = 0u;
+    }
+    if (b < bp.n_inst) {
+        InstState& G = bp.inst[b];
+        G.rho = 0.0; G.rr = 0.0; G.bb = 0.0; G.tol2 = 0.0; G.rr0 = 0.0;
+        G.iter = 0; G.status = kSolveConverged; G.done = 0; G.fallback = 0;
+    }
+}
+
+}  // namespace chysx_b200

@@ -59,6 +59,41 @@ void build_vertex_triangles(int n, const std::vector<int>& tris, std::vector<int
         for (int a = 0; a < 3; ++a) list[fill[tris[3 * t + a]]++] = t;
 }
 
+void build_plan(const std::vector<int>& inst_slice, int grid, HostPlan& o) {
+    o = HostPlan();
+    const int n_inst = (int)inst_slice.size() - 1;
+    if (n_inst < 1) throw std::invalid_argument("build_plan: no instances");
+    const int n_slices = inst_slice.back();
+    for (int b = 0; b < n_inst; ++b)
+        if (inst_slice[b + 1] <= inst_slice[b]) throw std::invalid_argument("build_plan: empty instance");
+    grid = std::max(1, std::min(grid, n_slices));
+    o.grid = grid;
+    o.n_inst = n_inst;
+    o.inst_slice = inst_slice;
+    o.slice_inst.resize(n_slices);
+    for (int b = 0; b < n_inst; ++b)
+        for (int s = inst_slice[b]; s < inst_slice[b + 1]; ++s) o.slice_inst[s] = b;
+    o.cta_slice.resize(grid + 1);
+    for (int c = 0; c <= grid; ++c) o.cta_slice[c] = (int)((long long)c * n_slices / grid);
+    o.cta_inst_lo.resize(grid);
+    o.cta_inst_hi.resize(grid);
+    o.inst_cta_lo.assign(n_inst, -1);
+    std::vector<int> inst_cta_hi(n_inst, -1);
+    for (int c = 0; c < grid; ++c) {
+        const int s0 = o.cta_slice[c], s1 = o.cta_slice[c + 1];
+        o.max_slices_per_cta = std::max(o.max_slices_per_cta, s1 - s0);
+        o.cta_inst_lo[c] = o.slice_inst[s0];
+        o.cta_inst_hi[c] = o.slice_inst[s1 - 1];
+        o.max_inst_per_cta = std::max(o.max_inst_per_cta, o.cta_inst_hi[c] - o.cta_inst_lo[c] + 1);
+        for (int b = o.cta_inst_lo[c]; b <= o.cta_inst_hi[c]; ++b) {
+            if (o.inst_cta_lo[b] < 0) o.inst_cta_lo[b] = c;
+            inst_cta_hi[b] = c;
+        }
+    }
+    o.inst_slot.assign(n_inst + 1, 0);
+    for (int b = 0; b < n_inst; ++b) o.inst_slot[b + 1] = o.inst_slot[b] + (inst_cta_hi[b] - o.inst_cta_lo[b] + 1);
+}
+
 void build_topology(int n, const std::vector<int>& tris, bool use_tris,
                     const std::vector<int>& edges, bool use_springs,
                     const std::vector<int>& pins, HostTopology& o) {

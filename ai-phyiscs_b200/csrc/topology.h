@@ -55,6 +55,22 @@ void build_topology(int n, const std::vector<int>& tris, bool use_tris,
                     const std::vector<int>& edges, bool use_springs,
                     const std::vector<int>& pins, HostTopology& out);
 
+// Work split of the persistent PCG kernel: `grid` CTAs each take a
+// contiguous, balanced range of slices; instances own contiguous slice
+// ranges.  Each (CTA, instance) pair that overlaps gets one reduction slot;
+// an instance's slots are contiguous and ordered by CTA.
+struct HostPlan {
+    int grid = 0;
+    int n_inst = 0;
+    int max_slices_per_cta = 0;
+    int max_inst_per_cta = 0;
+    std::vector<int> slice_inst, inst_slice, cta_slice, cta_inst_lo, cta_inst_hi, inst_cta_lo, inst_slot;
+};
+
+// inst_slice: [n_inst + 1] slice offsets (every instance non-empty).
+// grid is clamped to [1, n_slices].
+void build_plan(const std::vector<int>& inst_slice, int grid, HostPlan& out);
+
 // Per-vertex incident-triangle lists (sorted by triangle id), used by the
 // deterministic mass redistribution.
 void build_vertex_triangles(int n, const std::vector<int>& tris, std::vector<int>& off,

@@ -1,0 +1,416 @@
+"""Benchmark of the implicit cloth step (assembly + block-Jacobi PCG to
+||r||/||b|| <= 1e-6 + update) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload grid256]
+                    [--impl ours|reference] [--warm zero|previous|learned]
+
+Prints one JSON line.  A "step" is one cloth time step of the workload
+(seeded synthetic scene; the default `grid256` is the 256x256 plain-method
+configuration: per-edge spring k log-U[1e2,1e4], Baraff-Witkin k=1e4, two
+corners pinned, dt=1/60).  `value` is cloth steps/s over the K timed steps
+with the scene resident in HBM; `e2e` is the same through the C ABI with
+pinned host buffers and the H2D/D2H copies of positions and velocities
+inside the timed region.  N>1 (torchrun) runs one replica of the workload
+per GPU (weak scaling) and reports the whole-job rate.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "ai-phyiscs_b200"))
+
+from chysx import scenes  # noqa: E402
+
+METRIC = "cloth steps/s & PCG iters/step at rel-res 1e-6: learned+batched vs plain PCG, 1 B200"
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def workload(name):
+    if name == "grid256":
+        return scenes.config_large(max_iter=30000)
+    if name == "grid1024":
+        return scenes.config_huge(max_iter=60000)
+    if name == "grid10":
+        return scenes.config_small(max_iter=100)
+    if name.startswith("grid"):
+        return scenes.config_large(side=int(name[4:]), max_iter=30000)
+    raise SystemExit(f"unknown workload {name}")
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes
+# ---------------------------------------------------------------------------
+def pcg_bytes_per_iteration(n, nnz):
+    """Bytes one PCG iteration of the persistent kernel must move in its own
+    storage format: phase 1 reads z, p_old (16 B each), the diagonal block
+    (24 B), nnz off-diagonal (col 4 B + symmetric block 24 B) and writes p,
+    Ap (16 B each); phase 2 reads p, Ap, x, r (16 B each) and M^-1 (24 B) and
+    writes x, r, z (16 B each).  Gathered neighbour vectors are counted once
+    (their owner's read)."""
+    return n * (16 + 16 + 24 + 16 + 16) + nnz * 28 + n * (4 * 16 + 24 + 3 * 16)
+
+
+def reference_format_bytes_per_iteration(n, nnz):
+    """The reference's split BSR (36-B blocks, int32 cols/rows, float3
+    vectors): B_spmv = 64N + 40nnz + 4, plus the fused vector update 156N."""
+    return 64 * n + 40 * nnz + 4 + 156 * n
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def read_traffic(workload_name):
+    """Per-iteration DRAM bytes of the PCG kernel from the committed ncu
+    summary for this workload, if one exists (profiles/pcg_<workload>.txt
+    carries a line `dram_bytes_per_iteration: <int>`)."""
+    path = os.path.join(ROOT, "profiles", f"pcg_persistent_{workload_name}.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_iteration:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4)
+                          if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (test infrastructure: the oracle port)
+# ---------------------------------------------------------------------------
+def oracle_setup(sc, fp64, threads):
+    import oracle.oracle as O
+
+    O.set_threads(threads)
+    n = sc["pos"].shape[0]
+    s = O.OracleCloth(fp64)
+    s.set_material(sc["density"], sc.get("damping", 0.0), sc["gravity"])
+    s.set_state(sc["pos"], sc["vel"], np.ones(n, np.float32))
+    s.set_mesh(sc["tris"])
+    s.set_options(True, False, sc.get("det_eps", 1e-6))
+    im = s.redistribute_mass(sc["density"])
+    s.set_state(sc["pos"], sc["vel"], im)
+    s.build_springs(sc["k_spring"])
+    s.build_stretch(sc["k_stretch"])
+    s.set_pins(sc["pin_idx"], sc["pin_targets"], sc.get("k_pin", 1e6))
+    return s
+
+
+def cpu_step_costs(sc, threads, iters_per_step, budget_s):
+    """Times assembly (a 0-iteration step) and a bounded number of PCG
+    iterations on the CPU port; returns (t_assembly, t_iteration, M)."""
+    s = oracle_setup(sc, fp64=False, threads=threads)
+    s.set_solver(0, 0.0, "zero")
+    t0 = time.perf_counter()
+    s.step(sc["dt"])
+    t_asm = time.perf_counter() - t0
+    s = oracle_setup(sc, fp64=False, threads=threads)
+    probe = 10
+    s.set_solver(probe, 0.0, "zero")
+    t0 = time.perf_counter()
+    s.step(sc["dt"])
+    t_probe = time.perf_counter() - t0
+    t_it = max((t_probe - t_asm) / probe, 1e-9)
+    m = int(max(probe, min(iters_per_step, (budget_s - t_asm) / t_it)))
+    s = oracle_setup(sc, fp64=False, threads=threads)
+    s.set_solver(m, 0.0, "zero")
+    t0 = time.perf_counter()
+    s.step(sc["dt"])
+    t = time.perf_counter() - t0
+    return t_asm, max((t - t_asm) / m, 1e-9), m
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return None
+    sc = workload(args.workload)
+    threads = cpu_threads()
+    import oracle.oracle as O
+
+    # iterations per step needed at rel-res 1e-6 by the CPU port itself:
+    # the first warm-up step is a complete solve
+    s = oracle_setup(sc, fp64=False, threads=threads)
+    s.set_solver(sc["max_iter"], 1e-6, "zero")
+    t0 = time.perf_counter()
+    s.step(sc["dt"])
+    full_step_s = time.perf_counter() - t0
+    iters = s.stats()[0]
+    per_step = []
+    budget = max(0.2, min(2.0, 150.0 / max(1, args.steps + args.warmup)))
+    samples = []
+    for k in range(args.warmup + args.steps):
+        t_asm, t_it, m = cpu_step_costs(sc, threads, iters, budget)
+        if k >= args.warmup:
+            per_step.append(t_asm + iters * t_it)
+            samples.append(m)
+    sec = float(np.mean(per_step))
+    value = 1.0 / sec
+    n_rows = sc["pos"].shape[0]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 dots)", "data": "synthetic",
+        "pcg_iters_per_step": iters,
+        "config": {"workload": args.workload, "particles": n_rows, "rel_tol": 1e-6, "warm_start": "zero"},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
+                         "sample": (f"each step: assembly + {int(np.mean(samples))} PCG iterations of the "
+                                    f"{args.workload} workload on the FP32 CPU port ({threads} threads), "
+                                    f"scaled to the {iters} iterations/step a full solve took "
+                                    f"(first full step: {full_step_s:.1f} s)")},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from chysx import capi
+    from chysx.runner import GpuCloth
+
+    torch.cuda.set_device(local_rank)
+    sc = workload(args.workload)
+    rel_tol = 1e-6
+    g = GpuCloth(sc, max_iter=sc["max_iter"], rel_tol=rel_tol, warm_start=args.warm)
+    g.sim.set_tuning(args.path, args.block, args.grid)
+    g.sim.enable_timing(True)
+    n = sc["pos"].shape[0]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        g.step()
+    torch.cuda.synchronize()
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    iters, solve_ms, asm_ms, statuses = [], [], [], []
+    clocks = ClockSampler(local_rank)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.zero_()  # L2 flush between timed steps (outside the events)
+        ev0[k].record()
+        g.step()
+        ev1[k].record()
+        it, rr, st = g.stats()  # synchronises after the end event
+        a_ms, s_ms, _ = g.sim.last_timing()
+        iters.append(it)
+        solve_ms.append(s_ms)
+        asm_ms.append(a_ms)
+        statuses.append(st)
+    torch.cuda.synchronize()
+    barrier()
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+    step_ms = [ev0[k].elapsed_time(ev1[k]) for k in range(args.steps)]
+    total_ms = float(np.sum(step_ms))
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    total_ms_max = float(t.item())
+
+    # end to end through the C ABI with pinned host buffers
+    e2e_sim = GpuCloth(sc, max_iter=sc["max_iter"], rel_tol=rel_tol, warm_start=args.warm)
+    e2e_sim.sim.set_tuning(args.path, args.block, args.grid)
+    host_pos = torch.from_numpy(sc["pos"].copy()).pin_memory()
+    host_vel = torch.from_numpy(sc["vel"].copy()).pin_memory()
+    for _ in range(args.warmup):
+        e2e_sim.pos.copy_(host_pos, non_blocking=True)
+        e2e_sim.vel.copy_(host_vel, non_blocking=True)
+        e2e_sim.step()
+        host_pos.copy_(e2e_sim.pos, non_blocking=True)
+        host_vel.copy_(e2e_sim.vel, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = args.steps
+    e0.record()
+    for _ in range(e2e_steps):
+        e2e_sim.pos.copy_(host_pos, non_blocking=True)
+        e2e_sim.vel.copy_(host_vel, non_blocking=True)
+        e2e_sim.step()
+        host_pos.copy_(e2e_sim.pos, non_blocking=True)
+        host_vel.copy_(e2e_sim.vel, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    t2 = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t2, op=torch.distributed.ReduceOp.MAX)
+    e2e_ms_max = float(t2.item())
+
+    if rank != 0:
+        return None
+    nnz = g.sim.num_off_diag_blocks()
+    iters = np.array(iters)
+    solve_ms = np.array(solve_ms)
+    b_it = pcg_bytes_per_iteration(n, nnz)
+    b_ref = reference_format_bytes_per_iteration(n, nnz)
+    achieved = float(np.sum(iters * b_it) / (np.sum(solve_ms) * 1e-3) / 1e9)
+    achieved_ref = float(np.sum(iters * b_ref) / (np.sum(solve_ms) * 1e-3) / 1e9)
+    peak, peak_kind = read_peaks()
+    traffic_it = read_traffic(args.workload)
+    steps_total = args.steps * world
+    value = steps_total / (total_ms_max * 1e-3)
+    mean_iters = float(iters.mean())
+
+    # CPU baseline: single-threaded FP32 port, bounded sample
+    t_asm, t_it, m = cpu_step_costs(sc, 1, int(mean_iters), budget_s=args.cpu_budget)
+    cpu_value = 1.0 / (t_asm + mean_iters * t_it)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 dots)", "data": "synthetic",
+        "config": {"workload": args.workload, "particles": n, "off_diag_blocks": int(nnz),
+                   "rel_tol": rel_tol, "warm_start": args.warm,
+                   "solver_path": "persistent" if args.path == 0 else "graph-loop",
+                   "pcg_grid": g.sim.launched_grid(), "l2": "flushed between steps (256 MiB write)"},
+        "pcg_iters_per_step": mean_iters,
+        "pcg_iters_per_step_minmax": [int(iters.min()), int(iters.max())],
+        "solve_status": sorted(set(int(s) for s in statuses)),
+        "us_per_pcg_iteration": float(np.sum(solve_ms) * 1e3 / np.sum(iters)),
+        "assembly_ms": float(np.mean(asm_ms)),
+        "roofline": {"bound": "hbm", "kernel": "pcg_persistent_kernel", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": (traffic_it * mean_iters) if traffic_it else None,
+                     "algorithmic_bytes_per_iteration": b_it,
+                     "reference_format_bytes_per_iteration": b_ref,
+                     "achieved_reference_format": achieved_ref},
+        "cpu_baseline": {"value": cpu_value, "unit": "steps/s", "cores": 1, "kind": "port",
+                         "sample": (f"1 step of {args.workload}: assembly + {m} PCG iterations on the "
+                                    f"single-threaded FP32 CPU port, scaled to {mean_iters:.0f} "
+                                    f"iterations/step")},
+        "e2e": {"value": e2e_steps * world / (e2e_ms_max * 1e-3), "unit": "steps/s",
+                "h2d_bytes_per_step": 2 * 12 * n, "d2h_bytes_per_step": 2 * 12 * n},
+        "gpu_launches": (4 if args.path == 0 else -1) * args.steps,
+        "clocks": clk,
+        "wall_s": wall,
+    }
+    if args.path == 1:
+        # assemble + WHILE{2 per iteration} + finalize
+        line["gpu_launches"] = int(2 * args.steps + 2 * np.sum(iters))
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="grid256")
+    ap.add_argument("--warm", default="zero", choices=["zero", "previous", "learned"])
+    ap.add_argument("--path", type=int, default=0, help="0 persistent PCG, 1 graph loop")
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--grid", type=int, default=0)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference_arm(args, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        line = run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

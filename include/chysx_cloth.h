@@ -37,7 +37,8 @@ enum {
 enum {
     CHYSX_SOLVE_CONVERGED = 0, /* ||r||/||b|| <= rel_tol, or fixed count done */
     CHYSX_SOLVE_MAX_ITER = 1,  /* rel_tol > 0 and max_iter reached first */
-    CHYSX_SOLVE_NONFINITE = 2  /* NaN/Inf met; caller's pos/vel left untouched */
+    CHYSX_SOLVE_NONFINITE = 2, /* NaN/Inf met; caller's pos/vel left untouched */
+    CHYSX_SOLVE_KERNEL_ERROR = 3 /* solver grid barrier timed out; pos/vel untouched */
 };
 
 /* Initial guess of the PCG solve. */
@@ -155,6 +156,22 @@ int chysx_cloth_num_off_diag_blocks(const chysx_cloth* h, int* out);
  * buffers, synchronises the device. */
 int chysx_cloth_debug_dump(chysx_cloth* h, float* diag, int32_t* row_offsets,
                            int32_t* col_indices, float* values, float* rhs, float* dx);
+
+/* Solver kernel selection (no counterpart in the reference, whose PCG is a
+ * fixed chain of 8 launches per iteration, src/solver/pcg_solver.cu:542-592):
+ * solver_path 0 = one persistent cooperative kernel per solve (default),
+ * 1 = CUDA-graph WHILE loop of two kernels per iteration.  block (0, 128,
+ * 256, 512) and grid (0 = automatic) size the persistent kernel. */
+int chysx_cloth_set_tuning(chysx_cloth* h, int solver_path, int block, int grid);
+/* CTAs of the persistent PCG launch chosen at the last graph build. */
+int chysx_cloth_launched_grid(const chysx_cloth* h, int* out);
+
+/* Measurement hooks (no counterpart in the reference): when enabled, the
+ * step graph records CUDA events around assembly, the PCG solve and the
+ * finalize kernel on the step's stream; last_timing synchronises on the
+ * last event and returns the three durations of the last step. */
+int chysx_cloth_enable_timing(chysx_cloth* h, int on);
+int chysx_cloth_last_timing(chysx_cloth* h, float* assemble_ms, float* solve_ms, float* finalize_ms);
 
 /* Host-only introspection of the off-diagonal block pattern the step
  * assembles for a mesh (no counterpart in the reference; the equivalent there

@@ -1,0 +1,77 @@
+// TEST INFRASTRUCTURE ONLY: a minimal pybind11 module over the reference's
+// chysx::cloth::ClothSimulator (compiled from the reference sources by
+// oracle/build_ref.sh).  It binds only the cloth step and the calls the
+// parity harness needs, with the reference's own method semantics; the
+// reference's full bindings.cpp pulls in rigid/IK/coupled subsystems that
+// are not part of this path.
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+
+#include <cstdint>
+#include <stdexcept>
+
+#include "cloth/cloth_material.h"
+#include "cloth/cloth_simulator.h"
+#include "math/vec.cuh"
+
+#ifndef REF_MODULE_NAME
+#define REF_MODULE_NAME _chysx_ref
+#endif
+
+namespace py = pybind11;
+using chysx::cloth::ClothSimulator;
+
+PYBIND11_MODULE(REF_MODULE_NAME, m) {
+    py::class_<ClothSimulator>(m, "ClothSimulator", py::module_local())
+        .def(py::init<>())
+        .def("set_material",
+             [](ClothSimulator& s, float density, float damping, float gx, float gy, float gz) {
+                 chysx::cloth::ClothMaterial mat;
+                 mat.density = density;
+                 mat.damping = damping;
+                 mat.gx = gx;
+                 mat.gy = gy;
+                 mat.gz = gz;
+                 s.set_material(mat);
+             })
+        .def("set_external_buffers", &ClothSimulator::set_external_buffers, py::arg("pos_ptr"),
+             py::arg("vel_ptr"), py::arg("particle_count"), py::arg("inv_mass_ptr") = 0, py::arg("force_ptr") = 0)
+        .def("set_mesh",
+             [](ClothSimulator& s, py::array_t<int, py::array::c_style | py::array::forcecast> tris) {
+                 s.set_mesh(reinterpret_cast<const chysx::math::Vec3i*>(tris.data()), (int)tris.shape(0));
+             })
+        .def("set_pins",
+             [](ClothSimulator& s, py::array_t<int, py::array::c_style | py::array::forcecast> idx,
+                py::array_t<float, py::array::c_style | py::array::forcecast> tgt, float k) {
+                 s.set_pins(idx.data(), reinterpret_cast<const chysx::math::Vec3f*>(tgt.data()),
+                            (int)idx.shape(0), k);
+             })
+        .def("build_springs_from_current_positions", &ClothSimulator::build_springs_from_current_positions,
+             py::arg("stiffness"), py::arg("cuda_stream") = 0)
+        .def("build_fem_stretch_from_current_positions",
+             &ClothSimulator::build_fem_stretch_from_current_positions, py::arg("stiffness"),
+             py::arg("cuda_stream") = 0)
+        .def("redistribute_mass_area_weighted", &ClothSimulator::redistribute_mass_area_weighted,
+             py::arg("surface_density"), py::arg("inv_mass_ptr"), py::arg("particle_count"),
+             py::arg("cuda_stream") = 0)
+        .def("set_pcg_iterations", &ClothSimulator::set_pcg_iterations)
+        .def("step", &ClothSimulator::step, py::arg("dt"), py::arg("cuda_stream") = 0)
+        .def("debug_dump_last_solve", [](const ClothSimulator& s) {
+            const int n = s.num_particles();
+            const int nnz = s.num_off_diag_blocks();
+            py::array_t<float> diag({n, 3, 3});
+            py::array_t<int> rp({n + 1});
+            py::array_t<int> col({nnz});
+            py::array_t<float> vals({nnz, 3, 3});
+            py::array_t<float> rhs({n, 3});
+            py::array_t<float> dx({n, 3});
+            if (n > 0) {
+                s.debug_copy_hessian_diag(diag.mutable_data());
+                s.debug_copy_hessian_csr(rp.mutable_data(), nnz > 0 ? col.mutable_data() : nullptr,
+                                         nnz > 0 ? vals.mutable_data() : nullptr);
+                s.debug_copy_last_rhs(rhs.mutable_data());
+                s.debug_copy_last_dx(dx.mutable_data());
+            }
+            return py::make_tuple(diag, rp, col, vals, rhs, dx);
+        });
+}

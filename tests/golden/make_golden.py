@@ -1,0 +1,98 @@
+"""Generate the reference golden fixtures in tests/golden/ (run on a B200).
+
+The reference has no CPU implementation and no golden vectors for this path,
+so the fixtures are produced by running the reference's own ClothSimulator,
+compiled from its sources by ``oracle/build_ref.sh`` into ``oracle/_ref/``:
+
+    bash oracle/build_ref.sh                       # here (needs the sources)
+    python tests/golden/make_golden.py             # on a GPU box
+
+Each fixture records, for one seeded scene, the reference's assembled system
+(``debug_dump_last_solve``: diag, row_offsets, col_indices, values, rhs, dx),
+the particle state it was assembled from, and final trajectories.  Two builds
+are used: ``_chysx_ref`` (unmodified: springs are built but skipped by
+step(), src/cloth/cloth_simulator.cu:921) and ``_chysx_ref_springs`` (the
+three spring call sites enabled).  The fixtures are small (<= 16x16 grids).
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
+sys.path.insert(0, os.path.join(ROOT, "ai-phyiscs_b200"))
+
+import torch  # noqa: E402
+
+from chysx import scenes  # noqa: E402
+
+
+def run_reference(mod, sc, pcg_iters, steps, dump_at=()):
+    """Run `steps` reference steps; for each step in dump_at record the state
+    before the step and the system dumped after it."""
+    n = sc["pos"].shape[0]
+    pos = torch.from_numpy(sc["pos"].copy()).cuda()
+    vel = torch.from_numpy(sc["vel"].copy()).cuda()
+    inv = torch.ones(n, dtype=torch.float32, device="cuda")
+    s = mod.ClothSimulator()
+    s.set_material(sc["density"], sc.get("damping", 0.0), *sc["gravity"])
+    s.set_external_buffers(pos.data_ptr(), vel.data_ptr(), n, inv.data_ptr())
+    s.set_mesh(sc["tris"])
+    s.redistribute_mass_area_weighted(sc["density"], inv.data_ptr(), n)
+    s.build_springs_from_current_positions(float(sc["k_spring"]))
+    s.build_fem_stretch_from_current_positions(float(sc["k_stretch"]))
+    s.set_pins(sc["pin_idx"].astype(np.int32), sc["pin_targets"].astype(np.float32), float(sc["k_pin"]))
+    s.set_pcg_iterations(pcg_iters)
+    torch.cuda.synchronize()
+    out = {"inv_mass": inv.cpu().numpy()}
+    for k in range(steps):
+        if k in dump_at:
+            torch.cuda.synchronize()
+            out[f"s{k}_pos"] = pos.cpu().numpy()
+            out[f"s{k}_vel"] = vel.cpu().numpy()
+        s.step(sc["dt"])
+        if k in dump_at:
+            torch.cuda.synchronize()
+            diag, rp, col, vals, rhs, dx = s.debug_dump_last_solve()
+            for name, a in zip(("diag", "row_offsets", "col_indices", "values", "rhs", "dx"),
+                               (diag, rp, col, vals, rhs, dx)):
+                out[f"s{k}_{name}"] = np.array(a)
+    torch.cuda.synchronize()
+    out["final_pos"] = pos.cpu().numpy()
+    out["final_vel"] = vel.cpu().numpy()
+    return out
+
+
+def scene_grid16():
+    pos, tris, _ = scenes.jittered_grid(16, seed=5)
+    sc = scenes._finish("grid16_jitter", pos, tris, 500.0, 5.0e3, [240, 255], 40, 2000, 0.0)
+    return sc
+
+
+def main(out_dir=HERE):
+    os.makedirs(out_dir, exist_ok=True)
+    import _chysx_ref  # noqa: F401
+    import _chysx_ref_springs  # noqa: F401
+
+    mods = {"nosprings": sys.modules["_chysx_ref"], "springs": sys.modules["_chysx_ref_springs"]}
+    c1 = scenes.config_small()
+    for tag, mod in mods.items():
+        out = {}
+        a = run_reference(mod, c1, 100, 200, dump_at=(0, 50, 199))
+        out.update({f"it100_{k}": v for k, v in a.items()})
+        b = run_reference(mod, c1, 1000, 200, dump_at=(0, 50))
+        out.update({f"it1000_{k}": v for k, v in b.items()})
+        np.savez_compressed(os.path.join(out_dir, f"ref_grid10_{tag}.npz"), **out)
+        print(tag, "grid10 done", flush=True)
+    g = scene_grid16()
+    a = run_reference(mods["springs"], g, 2000, 40, dump_at=(0, 20, 39))
+    np.savez_compressed(os.path.join(out_dir, "ref_grid16_springs.npz"), **a)
+    print("grid16 done", flush=True)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else HERE)

@@ -1,0 +1,264 @@
+"""GPU parity tests of the CUDA cloth step against the CPU oracle, through the
+C ABI (and once through the pybind11 facade).
+
+Tolerances (stated per test) follow from FP32 assembly: rounding the assembled
+matrix to FP32 alone moves one step's dx by ~1e-6 m on the 10x10 patch
+(cond(A) ~ 6e5), which compounds to a few 1e-4 m over 200 steps; the FP32
+oracle (same arithmetic class, different summation order) shows the same
+spread against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+import oracle.oracle as O
+from chysx import capi, scenes
+from chysx.runner import GpuCloth
+
+pytestmark = pytest.mark.gpu
+
+PATHS = [0, 1]  # 0 = persistent cooperative PCG, 1 = graph WHILE loop
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    import torch
+
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    yield
+
+
+def make(sc, path=0, **kw):
+    g = GpuCloth(sc, **kw)
+    if g.api == "capi":
+        g.sim.set_tuning(path)
+    return g
+
+
+def oracle_sim(sc, fp64=True, tol=1e-10, max_iter=20000, warm="zero", springs_in_step=True):
+    n = sc["pos"].shape[0]
+    s = O.OracleCloth(fp64)
+    s.set_material(sc["density"], sc.get("damping", 0.0), sc["gravity"])
+    s.set_state(sc["pos"], sc["vel"], np.ones(n, np.float32), sc.get("force"))
+    s.set_mesh(sc["tris"])
+    s.set_options(springs_in_step, False, sc.get("det_eps", 1e-6))
+    im = s.redistribute_mass(sc["density"])
+    s.set_state(sc["pos"], sc["vel"], im, sc.get("force"))
+    if sc.get("k_spring") is not None:
+        s.build_springs(sc["k_spring"])
+    if sc.get("k_stretch") is not None:
+        s.build_stretch(sc["k_stretch"])
+    if len(sc["pin_idx"]):
+        s.set_pins(sc["pin_idx"], sc["pin_targets"], sc.get("k_pin", 1e6))
+    s.set_solver(max_iter, tol, warm)
+    return s
+
+
+def rel(a, b):
+    return float(np.abs(np.asarray(a, np.float64) - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_first_step_system_and_solution_match_oracle(path):
+    sc = scenes.config_small()
+    g = make(sc, path, max_iter=2000, rel_tol=1e-8)
+    g.step()
+    it, rr, st = g.stats()
+    assert st == capi.SOLVE_CONVERGED and rr <= 1e-8
+    diag, rp, col, vals, rhs, dx = g.dump()
+    o = oracle_sim(sc, tol=1e-10)
+    o.step(sc["dt"])
+    od, orp, ocol, ovals, orhs, odx = o.dump_system()
+    np.testing.assert_array_equal(rp, orp)
+    np.testing.assert_array_equal(col, ocol)
+    assert rel(diag, od) < 1e-6      # FP32 assembly
+    assert rel(vals, ovals) < 1e-6
+    # at rest the elastic gradient is FP32 round-off of zero: compare absolutely
+    assert np.abs(rhs - orhs).max() < 2e-3 * np.abs(orhs).max()
+    assert np.abs(dx - odx).max() < 1e-6   # metres
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_grid10_trajectory_matches_oracle(path):
+    sc = scenes.config_small()
+    g = make(sc, path, max_iter=5000, rel_tol=1e-8)
+    iters = g.run(200)
+    p = g.positions()
+    p64, _, it64 = O.run_scene(sc, fp64=True, rel_tol=1e-8, max_iter=5000)
+    p32, _, it32 = O.run_scene(sc, fp64=False, rel_tol=1e-8, max_iter=5000)
+    # tolerance: FP32 floor over 200 steps (see module docstring)
+    assert np.abs(p - p64).max() < 1.5e-3
+    assert np.abs(p - p32).max() < 1.5e-3
+    # early part of the trajectory stays within 1e-4 m of the FP64 oracle
+    g2 = make(sc, path, max_iter=5000, rel_tol=1e-8)
+    g2.run(40)
+    p40, _, _ = O.run_scene(sc, steps=40, fp64=True, rel_tol=1e-8, max_iter=5000)
+    assert np.abs(g2.positions() - p40).max() < 1e-4
+    assert abs(iters.mean() - it32.mean()) < 0.15 * it32.mean()
+
+
+def test_paths_agree():
+    sc = scenes.config_small()
+    a = make(sc, 0, max_iter=5000, rel_tol=1e-8)
+    b = make(sc, 1, max_iter=5000, rel_tol=1e-8)
+    a.run(20)
+    b.run(20)
+    assert np.abs(a.positions() - b.positions()).max() < 1e-5
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_fixed_iteration_mode_runs_exact_count(path):
+    sc = scenes.config_small()
+    g = make(sc, path, max_iter=37, rel_tol=0.0, warm_start="previous")
+    g.step()
+    it, _, st = g.stats()
+    assert it == 37 and st == capi.SOLVE_CONVERGED
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_max_iter_status(path):
+    sc = scenes.config_small()
+    g = make(sc, path, max_iter=5, rel_tol=1e-12, warm_start="zero")
+    g.step()
+    it, rr, st = g.stats()
+    assert it == 5 and st == capi.SOLVE_MAX_ITER and rr > 1e-12
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_warm_start_previous_converges_to_same_state(path):
+    sc = scenes.config_small(steps=60)
+    z = make(sc, path, max_iter=5000, rel_tol=1e-8, warm_start="zero")
+    w = make(sc, path, max_iter=5000, rel_tol=1e-8, warm_start="previous")
+    iz = z.run(60)
+    iw = w.run(60)
+    assert np.abs(z.positions() - w.positions()).max() < 2e-4
+    assert iw.sum() < iz.sum()
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_warm_start_survives_gravity_flip(path):
+    # the previous dx becomes a poor guess; the solve must still converge
+    sc = scenes.config_small(steps=30)
+    g = make(sc, path, max_iter=5000, rel_tol=1e-8, warm_start="previous")
+    g.run(15)
+    g.sim.set_material(density=sc["density"], damping=0.0, gravity=(0.0, 30.0, 0.0))
+    g.step()
+    it, rr, st = g.stats()
+    assert st == capi.SOLVE_CONVERGED and rr <= 1e-8
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_nonfinite_input_leaves_caller_state_untouched(path):
+    import torch
+
+    sc = scenes.config_small()
+    g = make(sc, path, max_iter=500, rel_tol=1e-6)
+    g.run(3)
+    g.pos[17, 1] = float("nan")
+    before_p = g.pos.clone()
+    before_v = g.vel.clone()
+    g.step()
+    _, _, st = g.stats()
+    assert st == capi.SOLVE_NONFINITE
+    torch.cuda.synchronize()
+    assert torch.equal(torch.nan_to_num(g.pos, 7.0), torch.nan_to_num(before_p, 7.0))
+    assert torch.equal(g.vel, before_v)
+
+
+def test_free_fall_without_elements_is_exact():
+    sc = scenes.config_small(side=6)
+    sc = dict(sc, k_spring=None, k_stretch=None, pin_idx=np.zeros(0, np.int32),
+              pin_targets=np.zeros((0, 3), np.float32))
+    g = make(sc, 0, max_iter=100, rel_tol=1e-10)
+    g.step()
+    p = g.positions()
+    o = oracle_sim(sc)
+    o.step(sc["dt"])
+    np.testing.assert_allclose(p, o.state()[0], atol=2e-7)
+
+
+def test_duplicate_pins_degenerate_triangle_and_isolated_vertex():
+    sc = scenes.config_small(side=5)
+    n = sc["pos"].shape[0]
+    pos = np.concatenate([sc["pos"], [[3.0, 1.0, 3.0]]]).astype(np.float32)  # isolated vertex
+    tris = np.concatenate([sc["tris"], [[0, 0, 6]], [[2, 7, 2]]]).astype(np.int32)
+    sc = dict(sc, pos=pos, vel=np.zeros_like(pos), tris=tris, edges=scenes.unique_edges(tris),
+              pin_idx=np.array([0, 0, 4], np.int32), pin_targets=pos[[0, 0, 4]].copy())
+    g = make(sc, 0, max_iter=5000, rel_tol=1e-9)
+    for _ in range(3):
+        g.step()
+    o = oracle_sim(sc, tol=1e-11)
+    for _ in range(3):
+        o.step(sc["dt"])
+    assert np.abs(g.positions() - o.state()[0]).max() < 1e-5
+    assert n + 1 == g.positions().shape[0]
+
+
+def test_errors_follow_reference_exception_types():
+    sc = scenes.config_small(side=4)
+    g = make(sc, 0, max_iter=10, rel_tol=0.0)
+    with pytest.raises(ValueError):
+        g.step(dt=0.0)
+    with pytest.raises(ValueError):
+        g.step(dt=-1.0)
+    g.sim.set_pins([0, 99], [[0, 0, 0], [0, 0, 0]])
+    with pytest.raises(IndexError):
+        g.step()
+
+
+def test_pybind_facade_matches_capi_bitwise():
+    sc = scenes.config_small()
+    a = GpuCloth(sc, max_iter=2000, rel_tol=1e-7, api="capi")
+    b = GpuCloth(sc, max_iter=2000, rel_tol=1e-7, api="pybind")
+    a.run(10, record_iters=False)
+    b.run(10, record_iters=False)
+    assert np.array_equal(a.positions(), b.positions())
+    assert b.sim.last_stats()[2] == capi.SOLVE_CONVERGED
+
+
+def test_user_stream_matches_default_stream():
+    import torch
+
+    sc = scenes.config_small()
+    a = make(sc, 0, max_iter=2000, rel_tol=1e-7)
+    b = make(sc, 0, max_iter=2000, rel_tol=1e-7)
+    s = torch.cuda.Stream()
+    for _ in range(5):
+        a.step()
+        b.step(stream=s.cuda_stream)
+    s.synchronize()
+    assert np.array_equal(a.positions(), b.positions())
+
+
+def test_deterministic_repeat():
+    sc = scenes.config_large(side=48)
+    a = make(sc, 0, max_iter=5000, rel_tol=1e-6)
+    b = make(sc, 0, max_iter=5000, rel_tol=1e-6)
+    a.run(3, record_iters=False)
+    b.run(3, record_iters=False)
+    assert np.array_equal(a.positions(), b.positions())
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_256_grid_converged_system_properties(path):
+    """Full-size 256x256 workload: properties that do not need the oracle."""
+    sc = scenes.config_large()
+    g = make(sc, path, max_iter=30000, rel_tol=1e-6)
+    g.run(2)
+    it, rr, st = g.stats()
+    assert st == capi.SOLVE_CONVERGED and rr <= 1e-6
+    diag, rp, col, vals, rhs, dx = g.dump()
+    n = diag.shape[0]
+    # blocks are symmetric and the stored (i,j) and (j,i) copies are identical
+    assert np.array_equal(diag, np.transpose(diag, (0, 2, 1)))
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    key = rows.astype(np.int64) * n + col
+    tkey = col.astype(np.int64) * n + rows
+    order = np.argsort(key)
+    pos_t = order[np.searchsorted(key[order], tkey)]
+    assert np.array_equal(vals, np.transpose(vals[pos_t], (0, 2, 1)))
+    # true residual of the FP32 system, evaluated in FP64
+    x = dx.astype(np.float64)
+    ax = np.einsum("nij,nj->ni", diag.astype(np.float64), x)
+    np.add.at(ax, rows, np.einsum("kij,kj->ki", vals.astype(np.float64), x[col]))
+    true_rel = np.linalg.norm(rhs - ax) / np.linalg.norm(rhs)
+    assert true_rel < 1e-4
