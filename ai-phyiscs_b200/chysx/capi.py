@@ -59,8 +59,21 @@ SIGNATURES = {
     "chysx_cloth_num_particles": (ctypes.c_int, [H, ip]),
     "chysx_cloth_num_off_diag_blocks": (ctypes.c_int, [H, ip]),
     "chysx_cloth_debug_dump": (ctypes.c_int, [H, f32p, i32p, i32p, f32p, f32p, f32p]),
+    "chysx_cloth_set_network": (ctypes.c_int, [H, f32p, ctypes.c_int]),
+    "chysx_cloth_set_feature_output": (ctypes.c_int, [H, u, u]),
+    "chysx_cloth_guess_kept": (ctypes.c_int, [H, ip]),
+    "chysx_mlp_num_params": (ctypes.c_int, []),
+    "chysx_mlp_num_features": (ctypes.c_int, []),
+    "chysx_mlp_workspace_bytes": (ctypes.c_uint64, [ctypes.c_int]),
+    "chysx_mlp_gradients": (ctypes.c_int, [u, u, u, ctypes.c_int, u, dp, u, ctypes.c_uint64, u]),
+    "chysx_mlp_predict": (ctypes.c_int, [u, u, ctypes.c_int, u, u, ctypes.c_uint64, u]),
+    "chysx_mlp_train_step": (ctypes.c_int, [u, u, u, u, u, u, ctypes.c_int, ctypes.c_float, ctypes.c_int, u,
+                                            ctypes.c_uint64, dp, u]),
+    "chysx_cloth_set_instances": (ctypes.c_int, [H, i32p, ctypes.c_int]),
+    "chysx_cloth_num_instances": (ctypes.c_int, [H, ip]),
+    "chysx_cloth_instance_stats": (ctypes.c_int, [H, ctypes.c_int, ip, dp, ip]),
     "chysx_cloth_set_tuning": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
-    "chysx_cloth_launched_grid": (ctypes.c_int, [H, ip]),
+    "chysx_cloth_solver_info": (ctypes.c_int, [H, ip, ip, ip]),
     "chysx_cloth_enable_timing": (ctypes.c_int, [H, ctypes.c_int]),
     "chysx_cloth_last_timing": (ctypes.c_int, [H, f32p, f32p, f32p]),
     "chysx_topology_pattern": (ctypes.c_int, [ctypes.c_int, i32p, ctypes.c_int, i32p, ctypes.c_int,
@@ -176,13 +189,46 @@ class Cloth:
         check(self._L.chysx_cloth_set_options(self.h, int(springs_in_step), int(apply_external_force),
                                               fem_det_eps))
 
+    def set_network(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        check(self._L.chysx_cloth_set_network(self.h, _p(p, f32p), p.shape[0]))
+
+    def set_feature_output(self, features_ptr, predictions_ptr=0):
+        check(self._L.chysx_cloth_set_feature_output(self.h, features_ptr, predictions_ptr))
+
+    def guess_kept(self):
+        v = ctypes.c_int()
+        check(self._L.chysx_cloth_guess_kept(self.h, ctypes.byref(v)))
+        return v.value
+
+    def set_instances(self, offsets):
+        o = None if offsets is None else np.ascontiguousarray(offsets, np.int32)
+        n = 0 if o is None else o.shape[0] - 1
+        check(self._L.chysx_cloth_set_instances(self.h, _p(o, i32p), n))
+
+    def num_instances(self):
+        v = ctypes.c_int()
+        check(self._L.chysx_cloth_num_instances(self.h, ctypes.byref(v)))
+        return v.value
+
+    def instance_stats(self):
+        n = self.num_instances()
+        it = np.zeros(n, np.int32)
+        rr = np.zeros(n, np.float64)
+        st = np.zeros(n, np.int32)
+        check(self._L.chysx_cloth_instance_stats(self.h, n, it.ctypes.data_as(ip), rr.ctypes.data_as(dp),
+                                                  st.ctypes.data_as(ip)))
+        return it, rr, st
+
     def set_tuning(self, solver_path=0, block=0, grid=0):
         check(self._L.chysx_cloth_set_tuning(self.h, solver_path, block, grid))
 
-    def launched_grid(self):
-        g = ctypes.c_int()
-        check(self._L.chysx_cloth_launched_grid(self.h, ctypes.byref(g)))
-        return g.value
+    def solver_info(self):
+        """(kernel, grid, block) of the last graph build; kernel is
+        'resident', 'loop' or 'streamed'."""
+        p, g, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self._L.chysx_cloth_solver_info(self.h, ctypes.byref(p), ctypes.byref(g), ctypes.byref(b)))
+        return ("resident", "loop", "streamed")[p.value], g.value, b.value
 
     def num_off_diag_blocks(self):
         v = ctypes.c_int()

@@ -13,7 +13,7 @@ import numpy as np
 
 class GpuCloth:
     def __init__(self, scene, *, max_iter=None, rel_tol=None, warm_start="zero", springs_in_step=True,
-                 apply_force=False, api="capi", device="cuda"):
+                 apply_force=False, api="capi", device="cuda", instances=None):
         import torch
 
         self.torch = torch
@@ -36,6 +36,8 @@ class GpuCloth:
             s.set_material(density=scene["density"], damping=scene.get("damping", 0.0), gravity=scene["gravity"])
             s.set_external_buffers(self.pos.data_ptr(), self.vel.data_ptr(), n, self.inv_mass.data_ptr(), fptr)
             s.set_mesh(scene["tris"])
+            if instances is not None:
+                s.set_instances(instances)
             s.set_options(springs_in_step, apply_force, scene.get("det_eps", 1.0e-6))
             s.redistribute_mass(scene["density"], self.inv_mass.data_ptr(), n)
             if scene.get("k_spring") is not None:

@@ -60,7 +60,9 @@ struct StepArgs {
     float* vel;
     const float* inv_mass;
     const float* force;
-    int n;
+    const int* row_to_ext;  // internal row -> particle (-1 padding), null = identity
+    int n;                  // internal rows
+    int want_features;      // leave per-row feature inputs in ap / b.w
     float dt;
     float gx, gy, gz;
     float damping;
@@ -304,23 +306,39 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
     const int tid = threadIdx.x;
     const int i = blockIdx.x * BLOCK + tid;
     double red[2] = {0.0, 0.0};
-    if (i < a.n) {
+    const int e = (i < a.n) ? (a.row_to_ext ? a.row_to_ext[i] : i) : -1;
+    if (i < a.n && e < 0) {
+        // padding row of a batched layout: identity block, zero right-hand side
+        const int s = i >> 5, lane = i & 31;
+        const int so = t.slice_off[s];
+        const int w = (t.slice_off[s + 1] - so) >> 5;
+        const S6 I{1.f, 0.f, 0.f, 1.f, 0.f, 1.f};
+        st6(t.diag + (size_t)s * 6 * 32 + lane, I);
+        st6(t.minv + (size_t)s * 6 * 32 + lane, I);
+        float* vb = t.val + (size_t)so * 6 + lane;
+        for (int q = 0; q < 6 * w; ++q) vb[q * 32] = 0.0f;
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        v.b[i] = z4;
+        v.r[i] = z4;
+        v.z[i] = z4;
+        v.x[i] = z4;
+    } else if (i < a.n) {
         const int s = i >> 5, lane = i & 31;
         const int so = t.slice_off[s];
         const int w = (t.slice_off[s + 1] - so) >> 5;
         for (int q = 0; q < 6 * w; ++q) s_off[q * BLOCK + tid] = 0.0f;
 
-        const float3 x = ld3(a.pos, i);
-        const float3 vel = ld3(a.vel, i);
+        const float3 x = ld3(a.pos, e);
+        const float3 vel = ld3(a.vel, e);
         float m = 1.0f;
         if (a.inv_mass) {
-            const float wi = a.inv_mass[i];
+            const float wi = a.inv_mass[e];
             m = (wi > 1.0e-12f) ? (1.0f / wi) : 1.0e8f;
         }
         float3 acc = f3(a.gx, a.gy, a.gz);
         if (a.apply_force && a.force) {
             const float im = (m > 0.0f) ? (1.0f / m) : 0.0f;
-            const float3 f = ld3(a.force, i);
+            const float3 f = ld3(a.force, e);
             acc = f3(acc.x + f.x * im, acc.y + f.y * im, acc.z + f.z * im);
         }
         const float dt = a.dt;
@@ -329,12 +347,15 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
 
         float3 g = f3(0.f, 0.f, 0.f);
         S6 D{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float pinned = 0.f, logk = 0.f;
+        int n_springs = 0;
         // pins (pin_constraint.cu:61-92)
         for (int p = t.pin_off[s]; p < t.pin_off[s + 1]; ++p) {
             if (t.pin_row[p] == i) {
                 const float3 tg = ld3(t.pin_tgt, p);
                 g = g + (x - tg) * el.pin_k;
                 D.xx += el.pin_k; D.yy += el.pin_k; D.zz += el.pin_k;
+                pinned = 1.f;
             }
         }
         // springs
@@ -347,6 +368,10 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
                 const unsigned meta = t.sinc_meta[o + k * 32 + lane];
                 S6 H;
                 spring_row(el, a.pos, e, (int)(meta & 1u), g, H);
+                if (a.want_features) {
+                    logk += log10f(fmaxf(el.kedge[e], 1.0e-30f));
+                    ++n_springs;
+                }
                 axpy6(D, 1.0f, H);
                 const unsigned slot = (meta >> 8) & 0xFFu;
                 if (slot == 0xFFu) axpy6(D, -1.0f, H);
@@ -398,7 +423,11 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
         }
         const S6 Mi = inverse6(D);
         st6(t.minv + (size_t)s * 6 * 32 + lane, Mi);
-        v.b[i] = f4(b);
+        v.b[i] = make_float4(b.x, b.y, b.z, n_springs ? logk / (float)n_springs : 0.f);
+        if (a.want_features) {
+            const float im = 1.0f / m;
+            v.ap[i] = make_float4(-g.x * im, -g.y * im, -g.z * im, pinned);
+        }
         red[1] = (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z;
         if (zero_guess) {
             const float3 z = mul(Mi, b);
@@ -627,16 +656,18 @@ __global__ void finalize_kernel(StepArgs a, Vecs v, const SolveState* st) {
     if (st->status == kSolveNonfinite) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
+    const int e = a.row_to_ext ? a.row_to_ext[i] : i;
+    if (e < 0) return;
     const float4 d = v.x[i];
-    const float3 xn = ld3(a.pos, i);
-    st3(a.pos, i, f3(xn.x + d.x, xn.y + d.y, xn.z + d.z));
+    const float3 xn = ld3(a.pos, e);
+    st3(a.pos, e, f3(xn.x + d.x, xn.y + d.y, xn.z + d.z));
     const float inv_dt = 1.0f / a.dt;
     float3 vn = f3(d.x * inv_dt, d.y * inv_dt, d.z * inv_dt);
     if (a.damping > 0.0f) {
         const float decay = expf(-a.damping * a.dt);
         vn = vn * decay;
     }
-    st3(a.vel, i, vn);
+    st3(a.vel, e, vn);
 }
 
 // ---------------------------------------------------------------------------

@@ -30,6 +30,7 @@
 #include "cloth_kernels.cuh"
 #include "pcg_persistent.cuh"
 #include "topology.h"
+#include "warm_mlp.cuh"
 
 namespace chysx_b200 {
 
@@ -88,6 +89,96 @@ bool same_bytes(const T& a, const T& b) {
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Network training entry points (stateless, device pointers)
+// ---------------------------------------------------------------------------
+constexpr size_t kWsAlign = 256;
+size_t align_up(size_t v) { return (v + kWsAlign - 1) / kWsAlign * kWsAlign; }
+int train_blocks(int rows) { return std::max(1, std::min(1184, (rows + 16 * kTrainWarps - 1) / (16 * kTrainWarps))); }
+
+size_t mlp_workspace_bytes(int rows) {
+    const size_t r = (size_t)std::max(rows, 1);
+    return align_up(sizeof(MlpPacked)) + 8 * align_up(r * 64 * sizeof(__nv_bfloat16)) +
+           align_up((size_t)train_blocks(rows) * kTrainWarps * sizeof(double));
+}
+
+// Forward + backward (when targets != 0) of rows feature vectors; grads in
+// the flat parameter layout (normalisation entries zero); optional predicted
+// dv output.  Loss = mean squared error of the standardised outputs.
+void mlp_gradients(uintptr_t params, uintptr_t features, uintptr_t targets, int rows, uintptr_t grad, double* loss,
+                   uintptr_t dv_out, uintptr_t workspace, uint64_t ws_bytes, uintptr_t stream_u) {
+    if (rows <= 0) throw std::invalid_argument("mlp: rows must be positive");
+    if (!params || !features || !workspace) throw std::invalid_argument("mlp: null device pointer");
+    if (ws_bytes < mlp_workspace_bytes(rows)) throw std::invalid_argument("mlp: workspace too small");
+    if (targets && !grad) throw std::invalid_argument("mlp: gradients need an output buffer");
+    auto stream = reinterpret_cast<cudaStream_t>(stream_u);
+    unsigned char* ws = reinterpret_cast<unsigned char*>(workspace);
+    MlpPacked* packed = reinterpret_cast<MlpPacked*>(ws);
+    size_t off = align_up(sizeof(MlpPacked));
+    MlpTrainBufs bufs;
+    const size_t mat = align_up((size_t)rows * 64 * sizeof(__nv_bfloat16));
+    for (int l = 0; l < 4; ++l) {
+        bufs.act[l] = reinterpret_cast<__nv_bfloat16*>(ws + off);
+        off += mat;
+    }
+    for (int l = 0; l < 4; ++l) {
+        bufs.dz[l] = reinterpret_cast<__nv_bfloat16*>(ws + off);
+        off += mat;
+    }
+    bufs.sse = reinterpret_cast<double*>(ws + off);
+    bufs.out = reinterpret_cast<float*>(dv_out);
+    mlp_pack_kernel<<<8, 256, 0, stream>>>(reinterpret_cast<const float*>(params), packed);
+    ck(cudaGetLastError(), "mlp_pack_kernel launch");
+    static bool smem_set = false;
+    if (!smem_set) {
+        ck(cudaFuncSetAttribute(mlp_train_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem),
+           "cudaFuncSetAttribute(mlp_train_tile_kernel)");
+        smem_set = true;
+    }
+    const int blocks = train_blocks(rows);
+    // with no targets the kernel still runs the backward on zero residuals;
+    // a zero-target buffer is not needed because target rows are only read
+    // when targets != 0
+    mlp_train_tile_kernel<<<blocks, kTrainWarps * 32, kTrainSmem, stream>>>(
+        packed, reinterpret_cast<const float*>(features), reinterpret_cast<const float*>(targets), rows,
+        2.0f / (3.0f * (float)rows), bufs);
+    ck(cudaGetLastError(), "mlp_train_tile_kernel launch");
+    if (targets) {
+        using O = MlpOffsets;
+        float* g = reinterpret_cast<float*>(grad);
+        ck(cudaMemsetAsync(g, 0, sizeof(float) * O::w1, stream), "cudaMemsetAsync(grad)");
+        struct L { int in, out, w, b; } layers[4] = {
+            {kMlpIn, kMlpHid, O::w1, O::b1}, {kMlpHid, kMlpHid, O::w2, O::b2},
+            {kMlpHid, kMlpHid, O::w3, O::b3}, {kMlpHid, kMlpOut, O::w4, O::b4}};
+        for (int l = 0; l < 4; ++l) {
+            const int tiles = ((layers[l].in + 15) / 16) * ((layers[l].out + 7) / 8);
+            mlp_dw_kernel<<<(tiles + 3) / 4, 128, 0, stream>>>(bufs.act[l], bufs.dz[l], rows, layers[l].in,
+                                                               layers[l].out, g + layers[l].w, g + layers[l].b);
+            ck(cudaGetLastError(), "mlp_dw_kernel launch");
+        }
+        if (loss) {
+            std::vector<double> part((size_t)blocks * kTrainWarps);
+            ck(cudaMemcpyAsync(part.data(), bufs.sse, part.size() * sizeof(double), cudaMemcpyDeviceToHost, stream),
+               "cudaMemcpyAsync(loss)");
+            ck(cudaStreamSynchronize(stream), "cudaStreamSynchronize(loss)");
+            double s = 0.0;
+            for (double v : part) s += v;
+            *loss = s / (3.0 * rows);
+        }
+    }
+}
+
+void mlp_adam(uintptr_t params, uintptr_t grad, uintptr_t m1, uintptr_t m2, float lr, int t, uintptr_t stream_u) {
+    if (!params || !grad || !m1 || !m2) throw std::invalid_argument("mlp_adam: null device pointer");
+    if (t < 1) throw std::invalid_argument("mlp_adam: step must be >= 1");
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f / (1.0f - std::pow(b1, (float)t)), c2 = 1.0f / (1.0f - std::pow(b2, (float)t));
+    mlp_adam_kernel<<<16, 256, 0, reinterpret_cast<cudaStream_t>(stream_u)>>>(
+        reinterpret_cast<float*>(params), reinterpret_cast<const float*>(grad), reinterpret_cast<float*>(m1),
+        reinterpret_cast<float*>(m2), MlpOffsets::w1, MlpOffsets::total, lr, b1, b2, 1e-8f, c1, c2);
+    ck(cudaGetLastError(), "mlp_adam_kernel launch");
+}
 
 class ClothSim {
 public:
@@ -293,7 +384,7 @@ public:
                 "set_external_buffers() before stepping.");
         if (!(dt > 0.0f)) throw std::invalid_argument("chysx::cloth::ClothSimulator::step: dt must be positive");
         ensure_mesh_on_device();
-        if (topo_dirty_ || topo_.n != n_) rebuild_topology();
+        if (topo_dirty_ || topo_.n_ext != n_) rebuild_topology();
         if (graph_dirty_) build_graph();
         update_step_nodes(dt);
         ck(cudaGraphLaunch(exec_, reinterpret_cast<cudaStream_t>(stream)), "cudaGraphLaunch(step)");
@@ -307,9 +398,17 @@ public:
         if (stepped_) {
             ck(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(last_stream_)), "cudaStreamSynchronize");
             if (graph_path_ == kPathPersistent) {
-                InstState s{};
-                ck(cudaMemcpy(&s, d_inst_.get(), sizeof(InstState), cudaMemcpyDeviceToHost), "cudaMemcpy(state)");
-                it = s.iter; st = s.status; rr = s.rr; bb = s.bb;
+                // a batch reports its slowest / worst instance
+                std::vector<InstState> s(plan_.n_inst);
+                ck(cudaMemcpy(s.data(), d_inst_.get(), s.size() * sizeof(InstState), cudaMemcpyDeviceToHost),
+                   "cudaMemcpy(state)");
+                double worst = -1.0;
+                for (const InstState& q : s) {
+                    it = std::max(it, q.iter);
+                    st = std::max(st, q.status);
+                    const double rel = q.bb > 0.0 ? std::max(q.rr, 0.0) / q.bb : 0.0;
+                    if (rel > worst) { worst = rel; rr = q.rr; bb = q.bb; }
+                }
             } else {
                 SolveState s{};
                 ck(cudaMemcpy(&s, d_state_.get(), sizeof(SolveState), cudaMemcpyDeviceToHost), "cudaMemcpy(state)");
@@ -321,11 +420,74 @@ public:
         if (status) *status = st;
     }
 
+    // Learned warm start: loads a network (flat FP32 parameters, MlpOffsets).
+    void set_network(const float* params, int n) {
+        if (n != MlpOffsets::total)
+            throw std::invalid_argument("set_network: expected " + std::to_string(MlpOffsets::total) + " parameters");
+        if (!params) throw std::invalid_argument("set_network: null parameters");
+        for (int q = 0; q < n; ++q)
+            if (!std::isfinite(params[q])) throw std::invalid_argument("set_network: non-finite parameter");
+        d_net_params_.upload(params, n);
+        d_net_.resize(1);
+        mlp_pack_kernel<<<8, 256>>>(d_net_params_.get(), d_net_.get());
+        ck(cudaGetLastError(), "mlp_pack_kernel launch");
+        ck(cudaDeviceSynchronize(), "cudaDeviceSynchronize(set_network)");
+        warm_guess_ = true;
+        graph_dirty_ = true;
+    }
+    // Exports each step's raw per-particle features (n x 20 floats, caller
+    // order) to a device buffer; 0 disables.
+    void set_feature_output(uintptr_t ptr, uintptr_t pred) {
+        if ((ptr != 0) != (feat_out_ != 0)) graph_dirty_ = true;
+        feat_out_ = ptr;
+        pred_out_ = ptr ? pred : 0;
+        nodes_valid_ = false;  // node arguments changed
+    }
+    // instances whose solve kept the warm-start guess in the last step
+    int guess_kept() {
+        if (!stepped_ || graph_path_ != kPathPersistent) return 0;
+        ck(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(last_stream_)), "cudaStreamSynchronize");
+        std::vector<InstState> s(plan_.n_inst);
+        ck(cudaMemcpy(s.data(), d_inst_.get(), s.size() * sizeof(InstState), cudaMemcpyDeviceToHost),
+           "cudaMemcpy(instance states)");
+        if (warm_mode_ == CHYSX_WARM_ZERO) return 0;
+        int kept = 0;
+        for (const InstState& q : s) kept += q.fallback ? 0 : 1;
+        return kept;
+    }
+    bool want_features() const { return warm_mode_ == CHYSX_WARM_LEARNED || feat_out_ != 0; }
+
+    // Declares independent cloth instances: particles [off[b], off[b+1]).
+    void set_instances(const int32_t* off, int n_inst) {
+        if (n_inst < 0) throw std::invalid_argument("set_instances: negative instance count");
+        if (n_inst > 0 && !off) throw std::invalid_argument("set_instances: null offsets");
+        if (n_inst == 0) inst_offsets_.clear();
+        else inst_offsets_.assign(off, off + n_inst + 1);
+        topo_dirty_ = true;
+    }
+    int num_instances() const { return inst_offsets_.empty() ? 1 : (int)inst_offsets_.size() - 1; }
+    void instance_stats(int n, int* iters, double* relres, int* status) {
+        if (!stepped_ || graph_path_ != kPathPersistent)
+            throw std::runtime_error("instance_stats: needs a step taken with the persistent solver");
+        if (n != plan_.n_inst) throw std::invalid_argument("instance_stats: wrong instance count");
+        ck(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(last_stream_)), "cudaStreamSynchronize");
+        std::vector<InstState> s(n);
+        ck(cudaMemcpy(s.data(), d_inst_.get(), s.size() * sizeof(InstState), cudaMemcpyDeviceToHost),
+           "cudaMemcpy(instance states)");
+        for (int b = 0; b < n; ++b) {
+            if (iters) iters[b] = s[b].iter;
+            if (relres) relres[b] = s[b].bb > 0.0 ? std::sqrt(std::max(s[b].rr, 0.0) / s[b].bb) : 0.0;
+            if (status) status[b] = s[b].status;
+        }
+    }
+
     // Solver kernel selection (no counterpart in the reference): path 0 =
-    // persistent cooperative PCG, 1 = graph WHILE loop of two kernels.
-    // block / grid of the persistent kernel (0 = automatic).
+    // persistent cooperative PCG (register-resident rows when the system is
+    // small enough, else streamed), 1 = graph WHILE loop of two kernels,
+    // 2 = streamed persistent kernel forced.  block / grid of the streamed
+    // persistent kernel (0 = automatic).
     void set_tuning(int path, int block, int grid) {
-        if (path < 0 || path > 1) throw std::invalid_argument("set_tuning: path must be 0 or 1");
+        if (path < 0 || path > 2) throw std::invalid_argument("set_tuning: path must be 0, 1 or 2");
         if (block != 0 && block != 128 && block != 256 && block != 512)
             throw std::invalid_argument("set_tuning: block must be 0, 128, 256 or 512");
         if (grid < 0) throw std::invalid_argument("set_tuning: grid must be >= 0");
@@ -334,7 +496,13 @@ public:
         pcg_grid_req_ = grid;
         graph_dirty_ = true;
     }
-    int launched_grid() const { return plan_.grid; }
+    // kernel actually used by the last graph build: 0 resident, 1 loop, 2 streamed
+    void solver_info(int* path, int* grid, int* block) const {
+        const int used = graph_path_ == kPathLoop ? 1 : (resident_ ? 0 : 2);
+        if (path) *path = used;
+        if (grid) *grid = used == 1 ? 0 : plan_.grid;
+        if (block) *block = used == 1 ? kVecBlock : (resident_ ? resident_warps_ * 32 : pcg_block_);
+    }
 
     // Optional event-record nodes around the graph's phases (measurement only).
     void enable_timing(int on) {
@@ -359,8 +527,8 @@ public:
     int num_off_diag_blocks() const { return (int)topo_.nnz(); }
 
     void debug_dump(float* diag, int32_t* rp, int32_t* col, float* vals, float* rhs, float* dx) {
-        const int n = topo_.n;
-        if (n == 0) return;
+        const int n = topo_.n_ext;
+        if (n == 0 || topo_.n == 0) return;
         ck(cudaDeviceSynchronize(), "cudaDeviceSynchronize(debug_dump)");
         const size_t np = topo_.n_pad;
         std::vector<float> hd(np * 6), hv(d_val_.size());
@@ -369,28 +537,27 @@ public:
         if (!hv.empty()) ck(cudaMemcpy(hv.data(), d_val_.get(), hv.size() * 4, cudaMemcpyDeviceToHost), "dump val");
         ck(cudaMemcpy(hb.data(), d_b_.get(), np * sizeof(float4), cudaMemcpyDeviceToHost), "dump rhs");
         ck(cudaMemcpy(hx.data(), d_x_.get(), np * sizeof(float4), cudaMemcpyDeviceToHost), "dump dx");
-        auto put9 = [](float* o, const float* s6, size_t stride) {
-            const float xx = s6[0], xy = s6[stride], xz = s6[2 * stride], yy = s6[3 * stride],
-                        yz = s6[4 * stride], zz = s6[5 * stride];
+        auto put9 = [](float* o, const float* s6) {
+            const float xx = s6[0], xy = s6[32], xz = s6[64], yy = s6[96], yz = s6[128], zz = s6[160];
             o[0] = xx; o[1] = xy; o[2] = xz; o[3] = xy; o[4] = yy; o[5] = yz; o[6] = xz; o[7] = yz; o[8] = zz;
         };
-        for (int i = 0; i < n; ++i) {
-            if (diag) put9(diag + 9 * (size_t)i, &hd[(size_t)(i >> 5) * 192 + (i & 31)], 32);
-            if (rhs) { rhs[3 * i] = hb[i].x; rhs[3 * i + 1] = hb[i].y; rhs[3 * i + 2] = hb[i].z; }
-            if (dx) { dx[3 * i] = hx[i].x; dx[3 * i + 1] = hx[i].y; dx[3 * i + 2] = hx[i].z; }
-        }
-        if (rp) std::copy(topo_.csr_ptr.begin(), topo_.csr_ptr.end(), rp);
-        if (col) std::copy(topo_.csr_col.begin(), topo_.csr_col.end(), col);
-        if (vals) {
-            for (int r = 0; r < n; ++r) {
-                const int s = r >> 5;
-                const int so = topo_.slice_off[s];
-                for (int q = topo_.csr_ptr[r]; q < topo_.csr_ptr[r + 1]; ++q) {
-                    const int e = topo_.csr_to_ell[q];
-                    const int kk = (e - so) >> 5;
-                    put9(vals + 9 * (size_t)q, &hv[(size_t)so * 6 + (size_t)kk * 192 + (e & 31)], 32);
+        const bool mapped = !topo_.ext_to_row.empty();
+        int k_out = 0;
+        if (rp) rp[0] = 0;
+        for (int e = 0; e < n; ++e) {
+            const int r = mapped ? topo_.ext_to_row[e] : e;
+            if (diag) put9(diag + 9 * (size_t)e, &hd[(size_t)(r >> 5) * 192 + (r & 31)]);
+            if (rhs) { rhs[3 * e] = hb[r].x; rhs[3 * e + 1] = hb[r].y; rhs[3 * e + 2] = hb[r].z; }
+            if (dx) { dx[3 * e] = hx[r].x; dx[3 * e + 1] = hx[r].y; dx[3 * e + 2] = hx[r].z; }
+            const int so = topo_.slice_off[r >> 5];
+            for (int q = topo_.csr_ptr[r]; q < topo_.csr_ptr[r + 1]; ++q, ++k_out) {
+                if (col) col[k_out] = mapped ? topo_.row_to_ext[topo_.csr_col[q]] : topo_.csr_col[q];
+                if (vals) {
+                    const int el = topo_.csr_to_ell[q];
+                    put9(vals + 9 * (size_t)k_out, &hv[(size_t)so * 6 + (size_t)((el - so) >> 5) * 192 + (el & 31)]);
                 }
             }
+            if (rp) rp[e + 1] = k_out;
         }
     }
 
@@ -408,7 +575,11 @@ private:
     void rebuild_topology() {
         const bool use_tris = stretch_built_ && d_dminv_.size() > 0;
         const bool use_springs = springs_built_ && springs_in_step_ && d_rest_.size() > 0;
-        build_topology(n_, tris_, use_tris, edges_, use_springs, pin_idx_, topo_);
+        if (!inst_offsets_.empty() && inst_offsets_.back() != n_)
+            throw std::invalid_argument("set_instances: offsets do not cover the particle count");
+        build_topology(n_, tris_, use_tris, edges_, use_springs, pin_idx_, inst_offsets_, topo_);
+        if (topo_.row_to_ext.empty()) d_row_to_ext_.reset();
+        else d_row_to_ext_.upload(topo_.row_to_ext);
         use_tris_ = use_tris;
         use_springs_ = use_springs;
         d_slice_off_.upload(topo_.slice_off);
@@ -444,7 +615,7 @@ private:
         const int W = std::max(1, topo_.max_width);
         asm_block_ = (W <= 16) ? 128 : (W <= 32 ? 64 : 32);
         asm_smem_ = (size_t)6 * W * asm_block_ * sizeof(float);
-        const int max_grid = std::max(grid_for(n_, asm_block_), grid_for(n_, kVecBlock));
+        const int max_grid = std::max(grid_for(topo_.n, asm_block_), grid_for(topo_.n, kVecBlock));
         d_part_.resize((size_t)std::max(1, max_grid) * 3);
         d_state_.resize(1);
         d_state_.zero();
@@ -454,7 +625,7 @@ private:
 
     DevTopo dev_topo() const {
         DevTopo t;
-        t.n = n_;
+        t.n = topo_.n;
         t.n_slices = topo_.n_slices;
         t.slice_off = d_slice_off_.get();
         t.col = d_col_.get();
@@ -495,11 +666,13 @@ private:
         a.vel = reinterpret_cast<float*>(vel_);
         a.inv_mass = reinterpret_cast<const float*>(inv_mass_);
         a.force = reinterpret_cast<const float*>(force_);
-        a.n = n_;
+        a.row_to_ext = d_row_to_ext_.get();
+        a.n = topo_.n;
         a.dt = dt;
         a.gx = mat.gx; a.gy = mat.gy; a.gz = mat.gz;
         a.damping = mat.damping;
         a.apply_force = apply_force_ ? 1 : 0;
+        a.want_features = want_features() ? 1 : 0;
         return a;
     }
     SolverCfg solver_cfg() const {
@@ -519,7 +692,7 @@ private:
     void asm_params(cudaKernelNodeParams& p, void** args) {
         p = cudaKernelNodeParams{};
         p.func = const_cast<void*>(assemble_fn());
-        p.gridDim = dim3(grid_for(n_, asm_block_));
+        p.gridDim = dim3(grid_for(topo_.n, asm_block_));
         p.blockDim = dim3(asm_block_);
         p.sharedMemBytes = (unsigned)asm_smem_;
         p.kernelParams = args;
@@ -533,8 +706,44 @@ private:
     }
 
     void build_graph() {
-        if (solver_path_ == kPathPersistent) build_graph_persistent();
-        else build_graph_loop();
+        if (solver_path_ == kPathLoop && topo_.inst_slice.size() > 2)
+            throw std::invalid_argument("the graph-loop solver path solves a single instance; use path 0 or 2");
+        if (solver_path_ == kPathLoop) build_graph_loop();
+        else build_graph_persistent();
+    }
+
+    void guess_params(cudaKernelNodeParams& p, void** args) const {
+        p = cudaKernelNodeParams{};
+        p.func = reinterpret_cast<void*>(&learned_guess_kernel);
+        const int slices = std::max(1, topo_.n_slices);
+        p.gridDim = dim3(std::max(1, std::min(2048, (slices + kGuessWarps - 1) / kGuessWarps)));
+        p.blockDim = dim3(kGuessWarps * 32);
+        p.kernelParams = args;
+    }
+    // Appends the feature / learned-guess node after `dep` when needed.
+    cudaGraphNode_t add_guess_node(cudaGraphNode_t dep, StepArgs& a, DevTopo& t, Vecs& v) {
+        guess_node_ = nullptr;
+        if (!want_features()) return dep;
+        const MlpPacked* net = d_net_.get();
+        float* fo = reinterpret_cast<float*>(feat_out_);
+        float* po = reinterpret_cast<float*>(pred_out_);
+        int predict = warm_mode_ == CHYSX_WARM_LEARNED ? 1 : 0;
+        void* args[] = {&a, &t, &v, &net, &fo, &po, &predict};
+        cudaKernelNodeParams p;
+        guess_params(p, args);
+        ck(cudaGraphAddKernelNode(&guess_node_, graph_, &dep, 1, &p), "add learned-guess node");
+        return guess_node_;
+    }
+    void patch_guess_node(StepArgs& a, DevTopo& t, Vecs& v) {
+        if (!guess_node_) return;
+        const MlpPacked* net = d_net_.get();
+        float* fo = reinterpret_cast<float*>(feat_out_);
+        float* po = reinterpret_cast<float*>(pred_out_);
+        int predict = warm_mode_ == CHYSX_WARM_LEARNED ? 1 : 0;
+        void* args[] = {&a, &t, &v, &net, &fo, &po, &predict};
+        cudaKernelNodeParams p;
+        guess_params(p, args);
+        ck(cudaGraphExecKernelNodeSetParams(exec_, guess_node_, &p), "update learned-guess node");
     }
 
     // Appends an event-record node after `dep` when timing is on.
@@ -546,7 +755,12 @@ private:
         return node;
     }
 
+    static constexpr int kResidentMaxWidth = 8;
     const void* persistent_fn() const {
+        if (resident_) {
+            return resident_warps_ == 16 ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, kResidentMaxWidth>)
+                                         : reinterpret_cast<const void*>(&pcg_resident_kernel<8, kResidentMaxWidth>);
+        }
         if (pcg_block_ == 128) return reinterpret_cast<const void*>(&pcg_persistent_kernel<128>);
         if (pcg_block_ == 512) return reinterpret_cast<const void*>(&pcg_persistent_kernel<512>);
         return reinterpret_cast<const void*>(&pcg_persistent_kernel<256>);
@@ -572,16 +786,42 @@ private:
 
     // Plans the persistent launch: as many co-resident CTAs as useful, one
     // warp per slice at least.
+    // Register-resident plan: one slice per warp, W warps per CTA, all CTAs
+    // co-resident.  Returns false when the system does not fit.
+    bool plan_resident(int sms) {
+        if (solver_path_ != kPathPersistent || topo_.max_width > kResidentMaxWidth) return false;
+        const int n_slices = std::max(1, topo_.n_slices);
+        for (int W : {16, 8}) {
+            resident_ = true;
+            resident_warps_ = W;
+            const int grid = (n_slices + W - 1) / W;
+            build_plan(topo_.inst_slice, grid, plan_);
+            pers_smem_ = (size_t)W * 4 * sizeof(double) + (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
+            int per_sm = 0;
+            ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_fn(), W * 32, pers_smem_),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor(resident)");
+            if (per_sm >= 1 && plan_.grid <= per_sm * sms && plan_.max_slices_per_cta <= W) return true;
+        }
+        resident_ = false;
+        return false;
+    }
+
     void plan_persistent() {
         int dev = 0, sms = 0;
         ck(cudaGetDevice(&dev), "cudaGetDevice");
         ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+        if (plan_resident(sms)) {
+            upload_plan();
+            d_zp_.resize(2 * (size_t)std::max(1, topo_.n_pad));
+            d_zp_.zero();
+            return;
+        }
         const int W = pcg_block_ / 32;
         const int n_slices = std::max(1, topo_.n_slices);
         // shared memory depends on the plan; iterate once with a generous bound
         int grid = pcg_grid_req_ > 0 ? pcg_grid_req_ : std::max(1, (n_slices + W - 1) / W);
         for (int pass = 0; pass < 3; ++pass) {
-            build_plan({0, n_slices}, grid, plan_);
+            build_plan(topo_.inst_slice, grid, plan_);
             pers_smem_ = (size_t)plan_.max_slices_per_cta * 4 * sizeof(double) +
                          (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
             if (pers_smem_ > 48 * 1024)
@@ -595,6 +835,10 @@ private:
             if (plan_.grid <= cap) break;
             grid = cap;
         }
+        upload_plan();
+    }
+
+    void upload_plan() {
         d_slice_inst_.upload(plan_.slice_inst);
         d_inst_slice_.upload(plan_.inst_slice);
         d_cta_slice_.upload(plan_.cta_slice);
@@ -633,7 +877,8 @@ private:
         asm_params(ap, aargs);
         cudaGraphNode_t t0 = timing_node(0, nullptr);
         ck(cudaGraphAddKernelNode(&asm_node_, graph_, t0 ? &t0 : nullptr, t0 ? 1 : 0, &ap), "add assemble node");
-        cudaGraphNode_t t1 = timing_node(1, asm_node_);
+        cudaGraphNode_t t1 = add_guess_node(asm_node_, cur_args_, t, v);
+        t1 = timing_node(1, t1);
         cudaGraphNode_t reset;
         {
             void* rargs[] = {&bp};
@@ -645,11 +890,13 @@ private:
             ck(cudaGraphAddKernelNode(&reset, graph_, &t1, 1, &p), "add reset node");
         }
         {
-            void* pargs[] = {&t, &v, &bp, &cur_cfg_, &warm_i};
+            ZP* zp0 = d_zp_.get();
+            ZP* zp1 = zp0 + std::max(1, topo_.n_pad);
+            void* pargs[] = {&t, &v, &bp, &cur_cfg_, &warm_i, &zp0, &zp1};
             cudaKernelNodeParams p{};
             p.func = const_cast<void*>(persistent_fn());
             p.gridDim = dim3(plan_.grid);
-            p.blockDim = dim3(pcg_block_);
+            p.blockDim = dim3(resident_ ? resident_warps_ * 32 : pcg_block_);
             p.sharedMemBytes = (unsigned)pers_smem_;
             p.kernelParams = pargs;
             ck(cudaGraphAddKernelNode(&pcg_node_, graph_, &reset, 1, &p), "add persistent PCG node");
@@ -659,7 +906,7 @@ private:
                "cooperative attribute");
         }
         {
-            const int vgrid = std::max(1, grid_for(n_, kVecBlock));
+            const int vgrid = std::max(1, grid_for(topo_.n, kVecBlock));
             void* fargs[] = {&cur_args_, &v, &bp};
             cudaKernelNodeParams p{};
             p.func = reinterpret_cast<void*>(&finalize_batch_kernel);
@@ -702,9 +949,10 @@ private:
         asm_params(ap, aargs);
         cudaGraphNode_t t0 = timing_node(0, nullptr);
         ck(cudaGraphAddKernelNode(&asm_node_, graph_, t0 ? &t0 : nullptr, t0 ? 1 : 0, &ap), "add assemble node");
-        cudaGraphNode_t last = timing_node(1, asm_node_);
+        cudaGraphNode_t last = add_guess_node(asm_node_, cur_args_, t, v);
+        last = timing_node(1, last);
 
-        const int vgrid = std::max(1, grid_for(n_, kVecBlock));
+        const int vgrid = std::max(1, grid_for(topo_.n, kVecBlock));
         if (warm) {
             cudaKernelNodeParams p{};
             void* iargs[] = {&t, &v, &st, &part, &cond};
@@ -784,21 +1032,24 @@ private:
             cudaKernelNodeParams ap;
             asm_params(ap, aargs);
             ck(cudaGraphExecKernelNodeSetParams(exec_, asm_node_, &ap), "update assemble node");
-            void* pargs[] = {&t, &v, &bp, &c, &warm_i};
+            ZP* zp0 = d_zp_.get();
+            ZP* zp1 = zp0 + std::max(1, topo_.n_pad);
+            void* pargs[] = {&t, &v, &bp, &c, &warm_i, &zp0, &zp1};
             cudaKernelNodeParams pp{};
             pp.func = const_cast<void*>(persistent_fn());
             pp.gridDim = dim3(plan_.grid);
-            pp.blockDim = dim3(pcg_block_);
+            pp.blockDim = dim3(resident_ ? resident_warps_ * 32 : pcg_block_);
             pp.sharedMemBytes = (unsigned)pers_smem_;
             pp.kernelParams = pargs;
             ck(cudaGraphExecKernelNodeSetParams(exec_, pcg_node_, &pp), "update persistent PCG node");
             void* fargs[] = {&a, &v, &bp};
             cudaKernelNodeParams fp{};
             fp.func = reinterpret_cast<void*>(&finalize_batch_kernel);
-            fp.gridDim = dim3(std::max(1, grid_for(n_, kVecBlock)));
+            fp.gridDim = dim3(std::max(1, grid_for(topo_.n, kVecBlock)));
             fp.blockDim = dim3(kVecBlock);
             fp.kernelParams = fargs;
             ck(cudaGraphExecKernelNodeSetParams(exec_, fin_node_, &fp), "update finalize node");
+            patch_guess_node(a, t, v);
             node_args_ = a;
             node_cfg_ = c;
             nodes_valid_ = true;
@@ -809,7 +1060,7 @@ private:
         cudaKernelNodeParams ap;
         asm_params(ap, aargs);
         ck(cudaGraphExecKernelNodeSetParams(exec_, asm_node_, &ap), "update assemble node");
-        const int vgrid = std::max(1, grid_for(n_, kVecBlock));
+        const int vgrid = std::max(1, grid_for(topo_.n, kVecBlock));
         void* fargs[] = {&a, &v, &st};
         cudaKernelNodeParams p{};
         p.func = reinterpret_cast<void*>(&finalize_kernel);
@@ -817,6 +1068,7 @@ private:
         p.blockDim = dim3(kVecBlock);
         p.kernelParams = fargs;
         ck(cudaGraphExecKernelNodeSetParams(exec_, fin_node_, &p), "update finalize node");
+        patch_guess_node(a, t, v);
         node_args_ = a;
         node_cfg_ = c;
         nodes_valid_ = true;
@@ -866,6 +1118,15 @@ private:
     DevBuf<InstState> d_inst_;
     DevBuf<GridBarrier> d_bar_;
     cudaGraphNode_t pcg_node_ = nullptr;
+    DevBuf<float> d_net_params_;
+    DevBuf<MlpPacked> d_net_;
+    uintptr_t feat_out_ = 0, pred_out_ = 0;
+    cudaGraphNode_t guess_node_ = nullptr;
+    std::vector<int> inst_offsets_;
+    DevBuf<int> d_row_to_ext_;
+    bool resident_ = false;
+    int resident_warps_ = 16;
+    DevBuf<ZP> d_zp_;
     bool timing_ = false;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     // graph
@@ -1046,13 +1307,66 @@ int chysx_cloth_debug_dump(chysx_cloth* h, float* diag, int32_t* rp, int32_t* co
     return guard([&] { h->sim.debug_dump(diag, rp, col, vals, rhs, dx); });
 }
 
+int chysx_cloth_set_network(chysx_cloth* h, const float* params, int n_params) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_network(params, n_params); });
+}
+int chysx_cloth_set_feature_output(chysx_cloth* h, uintptr_t features, uintptr_t predictions) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_feature_output(features, predictions); });
+}
+int chysx_cloth_guess_kept(chysx_cloth* h, int* kept) {
+    CHYSX_H(h);
+    return guard([&] {
+        const int k = h->sim.guess_kept();
+        if (kept) *kept = k;
+    });
+}
+int chysx_mlp_num_params(void) { return chysx_b200::MlpOffsets::total; }
+int chysx_mlp_num_features(void) { return chysx_b200::kMlpIn; }
+uint64_t chysx_mlp_workspace_bytes(int rows) { return chysx_b200::mlp_workspace_bytes(rows); }
+int chysx_mlp_gradients(uintptr_t params, uintptr_t features, uintptr_t targets, int rows, uintptr_t grad,
+                        double* loss, uintptr_t workspace, uint64_t workspace_bytes, uintptr_t stream) {
+    return guard([&] {
+        chysx_b200::mlp_gradients(params, features, targets, rows, grad, loss, 0, workspace, workspace_bytes,
+                                  stream);
+    });
+}
+int chysx_mlp_predict(uintptr_t params, uintptr_t features, int rows, uintptr_t dv, uintptr_t workspace,
+                      uint64_t workspace_bytes, uintptr_t stream) {
+    return guard([&] {
+        chysx_b200::mlp_gradients(params, features, 0, rows, 0, nullptr, dv, workspace, workspace_bytes, stream);
+    });
+}
+int chysx_mlp_train_step(uintptr_t params, uintptr_t grad, uintptr_t m1, uintptr_t m2, uintptr_t features,
+                         uintptr_t targets, int rows, float lr, int adam_step, uintptr_t workspace,
+                         uint64_t workspace_bytes, double* loss, uintptr_t stream) {
+    return guard([&] {
+        chysx_b200::mlp_gradients(params, features, targets, rows, grad, loss, 0, workspace, workspace_bytes,
+                                  stream);
+        chysx_b200::mlp_adam(params, grad, m1, m2, lr, adam_step, stream);
+    });
+}
+int chysx_cloth_set_instances(chysx_cloth* h, const int32_t* offsets, int n_instances) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_instances(offsets, n_instances); });
+}
+int chysx_cloth_num_instances(const chysx_cloth* h, int* out) {
+    CHYSX_H(h);
+    if (out) *out = h->sim.num_instances();
+    return CHYSX_OK;
+}
+int chysx_cloth_instance_stats(chysx_cloth* h, int n, int* iters, double* relres, int* status) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.instance_stats(n, iters, relres, status); });
+}
 int chysx_cloth_set_tuning(chysx_cloth* h, int solver_path, int block, int grid) {
     CHYSX_H(h);
     return guard([&] { h->sim.set_tuning(solver_path, block, grid); });
 }
-int chysx_cloth_launched_grid(const chysx_cloth* h, int* out) {
+int chysx_cloth_solver_info(const chysx_cloth* h, int* path, int* grid, int* block) {
     CHYSX_H(h);
-    if (out) *out = h->sim.launched_grid();
+    h->sim.solver_info(path, grid, block);
     return CHYSX_OK;
 }
 
@@ -1072,7 +1386,7 @@ int chysx_topology_pattern(int n, const int32_t* tris, int n_tris, const int32_t
         std::vector<int> t(tris, tris + 3 * (size_t)std::max(0, n_tris));
         std::vector<int> e(edges, edges + 2 * (size_t)std::max(0, n_edges));
         chysx_b200::HostTopology topo;
-        chysx_b200::build_topology(n, t, n_tris > 0, e, n_edges > 0, {}, topo);
+        chysx_b200::build_topology(n, t, n_tris > 0, e, n_edges > 0, {}, {}, topo);
         if (nnz_out) *nnz_out = (int)topo.nnz();
         if (ell_entries_out) *ell_entries_out = (int)topo.ell_entries();
         if (max_width_out) *max_width_out = topo.max_width;

@@ -57,6 +57,12 @@ struct BatchPlan {
     GridBarrier* bar;
 };
 
+// (z, p) of one row for the register-resident kernel's neighbour exchange
+struct ZP {
+    float4 z;
+    float4 p;
+};
+
 struct LocalInst {
     double rho, rr, bb, tol2, sigma;
     float alpha, beta;
@@ -74,32 +80,30 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-// Returns false (uniformly across the CTA) once any CTA has flagged an error.
-__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned& gen, int* s_flag) {
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Count-based grid barrier: every CTA adds 1 to a monotonic counter (a
+// fire-and-forget release reduction) and thread 0 polls it with acquire
+// loads until it reaches this barrier's target.  The wait is bounded in time;
+// returns false (uniformly across the CTA) once any CTA flagged an error.
+__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned& target, int* s_flag) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned g = gen;
-        const unsigned arrived = atomicAdd(&gb->count, 1u);
-        if (arrived == gridDim.x - 1) {
-            atomicExch(&gb->count, 0u);
-            __threadfence();
-            atomicExch(&gb->gen, g + 1u);
-        } else {
-            const unsigned long long t0 = global_ns();
-            unsigned spins = 0;
-            while (ld_acquire_gpu(&gb->gen) == g) {
-                if ((++spins & 255u) == 0) {
-                    if (*(volatile int*)&gb->error) break;
-                    if (global_ns() - t0 > kBarrierTimeoutNs) {
-                        atomicExch(&gb->error, 1);
-                        break;
-                    }
+        target += gridDim.x;
+        red_release_add(&gb->count, 1u);
+        const unsigned long long t0 = global_ns();
+        unsigned spins = 0;
+        while ((int)(ld_acquire_gpu(&gb->count) - target) < 0) {
+            if ((++spins & 255u) == 0) {
+                if (*(volatile int*)&gb->error) break;
+                if (global_ns() - t0 > kBarrierTimeoutNs) {
+                    atomicExch(&gb->error, 1);
+                    break;
                 }
             }
         }
-        __threadfence();
-        gen = g + 1u;
         *s_flag = *(volatile int*)&gb->error;
     }
     __syncthreads();
@@ -165,11 +169,117 @@ __device__ __forceinline__ double warp_sum(double x) {
 }
 
 // ---------------------------------------------------------------------------
+// Per-instance scalar steps shared by the persistent kernels.  Each runs on
+// one warp per instance (the whole warp reads the instance's slots) and
+// lane 0 updates the CTA-local copy; the first CTA touching an instance
+// also publishes its state and counts it when it finishes.
+// ---------------------------------------------------------------------------
+template <int W>
+__device__ __forceinline__ void instances_start(const BatchPlan& bp, LocalInst* li, int il0, int il1,
+                                                const SolverCfg& cfg, int warm) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int b = il0 + warp; b <= il1; b += W) {
+        double tot[4];
+        read_instance_total<4>(bp, b, tot);
+        if (lane != 0) continue;
+        LocalInst& L = li[b - il0];
+        const double bb = tot[2];
+        const bool warm_ok = !warm || (isfinite(tot[0]) && isfinite(tot[1]) && tot[1] <= bb);
+        L.fallback = warm_ok ? 0 : 1;
+        L.rho = warm_ok ? tot[0] : tot[3];
+        L.rr = warm_ok ? tot[1] : bb;
+        L.bb = bb;
+        L.tol2 = cfg.rel_tol * cfg.rel_tol * bb;
+        L.iter = 0;
+        L.alpha = 0.0f;
+        L.beta = 0.0f;
+        const bool bad = !isfinite(L.rho) || !isfinite(L.rr) || !isfinite(bb);
+        const bool conv = cfg.use_tol && L.rr <= L.tol2;
+        L.status = bad ? kSolveNonfinite : kSolveConverged;
+        L.done = (bad || conv || cfg.max_iter <= 0) ? 1 : 0;
+        if ((int)blockIdx.x == bp.inst_cta_lo[b]) {
+            InstState& G = bp.inst[b];
+            G.rr0 = L.rr;
+            G.bb = bb;
+            G.fallback = L.fallback;
+            if (L.done) {
+                G.rho = L.rho; G.rr = L.rr; G.iter = 0; G.status = L.status; G.done = 1;
+                atomicAdd(&bp.bar->ndone, 1u);
+            }
+        }
+    }
+}
+
+template <int W>
+__device__ __forceinline__ void instances_alpha(const BatchPlan& bp, LocalInst* li, int il0, int il1) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int b = il0 + warp; b <= il1; b += W) {
+        LocalInst& L = li[b - il0];
+        if (L.done) continue;
+        double tot[1];
+        read_instance_total<1>(bp, b, tot);
+        if (lane == 0) {
+            const double sigma = tot[0];
+            const double alpha = (sigma > 1.0e-37 || sigma < -1.0e-37) ? L.rho / sigma : 0.0;
+            L.sigma = sigma;
+            L.alpha = (float)alpha;
+            if (!isfinite(sigma) || !isfinite(alpha)) L.status = kSolveNonfinite;
+        }
+    }
+}
+
+template <int W>
+__device__ __forceinline__ void instances_beta(const BatchPlan& bp, LocalInst* li, int il0, int il1,
+                                               const SolverCfg& cfg) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int b = il0 + warp; b <= il1; b += W) {
+        LocalInst& L = li[b - il0];
+        if (L.done) continue;
+        double tot[2];
+        read_instance_total<2>(bp, b, tot);
+        if (lane != 0) continue;
+        const double rho_new = tot[0], rr = tot[1];
+        const double beta = (L.rho > 1.0e-37 || L.rho < -1.0e-37) ? rho_new / L.rho : 0.0;
+        L.beta = (float)beta;
+        L.rho = rho_new;
+        L.rr = rr;
+        L.iter += 1;
+        const bool bad = L.status == kSolveNonfinite || !isfinite(rho_new) || !isfinite(rr);
+        const bool conv = cfg.use_tol && rr <= L.tol2;
+        int done = 0;
+        if (bad) { L.status = kSolveNonfinite; done = 1; }
+        else if (conv) { L.status = kSolveConverged; done = 1; }
+        else if (L.iter >= cfg.max_iter) { L.status = cfg.use_tol ? kSolveMaxIter : kSolveConverged; done = 1; }
+        if (done) {
+            L.done = 1;
+            if ((int)blockIdx.x == bp.inst_cta_lo[b]) {
+                InstState& G = bp.inst[b];
+                G.rho = L.rho; G.rr = L.rr; G.iter = L.iter; G.status = L.status; G.done = 1;
+                atomicAdd(&bp.bar->ndone, 1u);
+            }
+        }
+    }
+}
+
+// A barrier failure leaves every unfinished instance flagged.
+__device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalInst* li, int il0, int il1) {
+    if (threadIdx.x != 0) return;
+    for (int b = il0; b <= il1; ++b) {
+        if ((int)blockIdx.x == bp.inst_cta_lo[b]) {
+            InstState& G = bp.inst[b];
+            G.status = kSolveKernelError;
+            G.iter = li[b - il0].iter;
+            G.done = 1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // The kernel
 // ---------------------------------------------------------------------------
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
-pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm) {
+pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP*, ZP*) {
     extern __shared__ double s_mem[];
     __shared__ int s_flag;
     __shared__ int s_exit;
@@ -180,11 +290,8 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm) 
     double* spart = s_mem;
     LocalInst* li = reinterpret_cast<LocalInst*>(s_mem + (size_t)bp.max_slices_per_cta * 4);
     GridBarrier* gb = bp.bar;
-    unsigned gen = 0;
-    if (threadIdx.x == 0) {
-        gen = *(volatile unsigned*)&gb->gen;
-        s_flag = 0;
-    }
+    unsigned gen = 0;  // barrier target; the counter starts at 0 every solve
+    if (threadIdx.x == 0) s_flag = 0;
     bool ok = true;
 
     // ---- phase 0: initial residual and per-instance start ----------------
@@ -230,37 +337,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm) 
     write_segment_slots<BLOCK, 4>(bp, spart, s0, s1, il0, il1);
     ok = grid_sync(gb, gen, &s_flag);
     if (ok) {
-        for (int b = il0 + warp; b <= il1; b += W) {
-            double tot[4];
-            read_instance_total<4>(bp, b, tot);
-            if (lane == 0) {
-                LocalInst& L = li[b - il0];
-                const double bb = tot[2];
-                const bool warm_ok = !warm || (isfinite(tot[0]) && isfinite(tot[1]) && tot[1] <= bb);
-                L.fallback = warm_ok ? 0 : 1;
-                L.rho = warm_ok ? tot[0] : tot[3];
-                L.rr = warm_ok ? tot[1] : bb;
-                L.bb = bb;
-                L.tol2 = cfg.rel_tol * cfg.rel_tol * bb;
-                L.iter = 0;
-                L.alpha = 0.0f;
-                L.beta = 0.0f;
-                const bool bad = !isfinite(L.rho) || !isfinite(L.rr) || !isfinite(bb);
-                const bool conv = cfg.use_tol && L.rr <= L.tol2;
-                L.status = bad ? kSolveNonfinite : kSolveConverged;
-                L.done = (bad || conv || cfg.max_iter <= 0) ? 1 : 0;
-                if ((int)blockIdx.x == bp.inst_cta_lo[b]) {
-                    InstState& G = bp.inst[b];
-                    G.rr0 = L.rr;
-                    G.bb = bb;
-                    G.fallback = L.fallback;
-                    if (L.done) {
-                        G.rho = L.rho; G.rr = L.rr; G.iter = 0; G.status = L.status; G.done = 1;
-                        atomicAdd(&gb->ndone, 1u);
-                    }
-                }
-            }
-        }
+        instances_start<W>(bp, li, il0, il1, cfg, warm);
         __syncthreads();
         if (warm) {
             // zero-guess fallback for instances whose guess was worse than zero
@@ -335,19 +412,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm) 
         if (s_exit) break;
 
         // phase 2: alpha = rho / sigma; x += alpha p; r -= alpha Ap; z = M^-1 r
-        for (int b = il0 + warp; b <= il1; b += W) {
-            LocalInst& L = li[b - il0];
-            if (L.done) continue;
-            double tot[1];
-            read_instance_total<1>(bp, b, tot);
-            if (lane == 0) {
-                const double sigma = tot[0];
-                const double alpha = (sigma > 1.0e-37 || sigma < -1.0e-37) ? L.rho / sigma : 0.0;
-                L.sigma = sigma;
-                L.alpha = (float)alpha;
-                if (!isfinite(sigma) || !isfinite(alpha)) L.status = kSolveNonfinite;
-            }
-        }
+        instances_alpha<W>(bp, li, il0, il1);
         __syncthreads();
         for (int s = s0 + warp; s < s1; s += W) {
             const LocalInst& L = li[bp.slice_inst[s] - il0];
@@ -379,47 +444,191 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm) 
         if (!ok) break;
 
         // phase 3: beta, iteration count, convergence (pcg_solver.cu:436-454)
-        for (int b = il0 + warp; b <= il1; b += W) {
-            LocalInst& L = li[b - il0];
-            if (L.done) continue;
-            double tot[2];
-            read_instance_total<2>(bp, b, tot);
-            if (lane == 0) {
-                const double rho_new = tot[0], rr = tot[1];
-                const double beta = (L.rho > 1.0e-37 || L.rho < -1.0e-37) ? rho_new / L.rho : 0.0;
-                L.beta = (float)beta;
-                L.rho = rho_new;
-                L.rr = rr;
-                L.iter += 1;
-                const bool bad = L.status == kSolveNonfinite || !isfinite(rho_new) || !isfinite(rr);
-                const bool conv = cfg.use_tol && rr <= L.tol2;
-                int done = 0;
-                if (bad) { L.status = kSolveNonfinite; done = 1; }
-                else if (conv) { L.status = kSolveConverged; done = 1; }
-                else if (L.iter >= cfg.max_iter) { L.status = cfg.use_tol ? kSolveMaxIter : kSolveConverged; done = 1; }
-                if (done) {
-                    L.done = 1;
-                    if ((int)blockIdx.x == bp.inst_cta_lo[b]) {
-                        InstState& G = bp.inst[b];
-                        G.rho = L.rho; G.rr = L.rr; G.iter = L.iter; G.status = L.status; G.done = 1;
-                        atomicAdd(&gb->ndone, 1u);
-                    }
-                }
-            }
-        }
+        instances_beta<W>(bp, li, il0, il1, cfg);
         __syncthreads();
     }
-    // a barrier failure leaves every unfinished instance flagged
-    if (!ok && threadIdx.x == 0) {
-        for (int b = il0; b <= il1; ++b) {
-            if ((int)blockIdx.x == bp.inst_cta_lo[b]) {
-                InstState& G = bp.inst[b];
-                G.status = kSolveKernelError;
-                G.iter = li[b - il0].iter;
-                G.done = 1;
+    if (!ok) instances_fail(bp, li, il0, il1);
+}
+
+
+// ---------------------------------------------------------------------------
+// Register-resident variant for systems with at most one 32-row slice per
+// warp: every thread owns one row for the whole solve and keeps its diagonal
+// block, Jacobi inverse, off-diagonal blocks + columns (up to MAXW) and
+// x, r, z, p in registers.  Per iteration it publishes only p (phase 1) and
+// z (phase 2) for its neighbours, packed as one 32-byte entry per row in a
+// double-buffered array, so a neighbour's (z, p_old) pair is one sector.
+// Same phases, reductions, barrier and per-instance logic as
+// pcg_persistent_kernel.
+// ---------------------------------------------------------------------------
+
+template <int W, int MAXW>
+__global__ void __launch_bounds__(W * 32)
+pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP* zp0, ZP* zp1) {
+    extern __shared__ double s_mem[];
+    __shared__ int s_flag;
+    __shared__ int s_exit;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
+    const int il0 = bp.cta_inst_lo[blockIdx.x], il1 = bp.cta_inst_hi[blockIdx.x];
+    double* spart = s_mem;  // [W * 4]
+    LocalInst* li = reinterpret_cast<LocalInst*>(s_mem + (size_t)W * 4);
+    GridBarrier* gb = bp.bar;
+    unsigned target = 0;
+    if (threadIdx.x == 0) s_flag = 0;
+    bool ok = true;
+
+    const int s = s0 + warp;
+    const bool has = s < s1;
+    const int i = s * 32 + lane;
+    const bool row = has && i < t.n;
+    const int li_idx = has ? bp.slice_inst[s] - il0 : 0;
+
+    // ---- load the row --------------------------------------------------
+    S6 D{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, Mi{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    S6 B[MAXW];
+    int cols[MAXW];
+    int w = 0;
+    float3 b = f3(0.f, 0.f, 0.f), x = b, r = b, z = b, p = b;
+#pragma unroll
+    for (int k = 0; k < MAXW; ++k) {
+        B[k] = S6{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        cols[k] = row ? i : 0;
+    }
+    if (row) {
+        D = ld6(t.diag + (size_t)s * 192 + lane);
+        Mi = ld6(t.minv + (size_t)s * 192 + lane);
+        b = xyz(v.b[i]);
+        const int so = t.slice_off[s];
+        w = (t.slice_off[s + 1] - so) >> 5;
+#pragma unroll
+        for (int k = 0; k < MAXW; ++k) {
+            if (k < w) {
+                cols[k] = t.col[so + k * 32 + lane];
+                B[k] = ld6(t.val + (size_t)so * 6 + (size_t)k * 192 + lane);
             }
         }
     }
+
+    // ---- phase 0 -------------------------------------------------------
+    {
+        double rz = 0.0, rr = 0.0, bb = 0.0, bmb = 0.0;
+        if (row) {
+            const float3 zb = mul(Mi, b);
+            bb = (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z;
+            bmb = (double)b.x * zb.x + (double)b.y * zb.y + (double)b.z * zb.z;
+            if (warm) {
+                x = xyz(v.x[i]);
+                float3 ax = mul(D, x);
+#pragma unroll
+                for (int k = 0; k < MAXW; ++k)
+                    if (k < w) ax = ax + mul(B[k], xyz(v.x[cols[k]]));
+                r = b - ax;
+                z = mul(Mi, r);
+                rz = (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
+                rr = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
+            } else {
+                r = b;
+                z = zb;
+                rz = bmb;
+                rr = bb;
+            }
+            zp0[i].z = f4(z);
+        }
+        rz = warp_sum(rz); rr = warp_sum(rr); bb = warp_sum(bb); bmb = warp_sum(bmb);
+        if (lane == 0 && has) {
+            double* sp = spart + warp * 4;
+            sp[0] = rz; sp[1] = rr; sp[2] = bb; sp[3] = bmb;
+        }
+    }
+    __syncthreads();
+    write_segment_slots<W * 32, 4>(bp, spart, s0, s1, il0, il1);
+    ok = grid_sync(gb, target, &s_flag);
+    if (ok) {
+        instances_start<W>(bp, li, il0, il1, cfg, warm);
+        __syncthreads();
+        if (warm) {
+            if (row && li[li_idx].fallback) {
+                x = f3(0.f, 0.f, 0.f);
+                r = b;
+                z = mul(Mi, b);
+                zp0[i].z = f4(z);
+            }
+            ok = grid_sync(gb, target, &s_flag);
+        }
+    }
+
+    // ---- iterations ----------------------------------------------------
+    const int iter_cap = cfg.max_iter + 2;
+    float3 ap = f3(0.f, 0.f, 0.f);
+    for (int guard = 0; ok && guard < iter_cap; ++guard) {
+        double sig = 0.0;
+        if (row && !li[li_idx].done) {
+            const LocalInst& L = li[li_idx];
+            const bool first = L.iter == 0;
+            const float beta = L.beta;
+            const ZP* E = (L.iter & 1) ? zp1 : zp0;
+            ZP* En = (L.iter & 1) ? zp0 : zp1;
+            p = first ? z : f3(fmaf(beta, p.x, z.x), fmaf(beta, p.y, z.y), fmaf(beta, p.z, z.z));
+            En[i].p = f4(p);
+            float3 acc = mul(D, p);
+#pragma unroll
+            for (int k = 0; k < MAXW; ++k) {
+                if (k >= w) continue;
+                const float4 zj = __ldcg(&E[cols[k]].z);
+                float3 pj = xyz(zj);
+                if (!first) {
+                    const float4 po = __ldcg(&E[cols[k]].p);
+                    pj = f3(fmaf(beta, po.x, zj.x), fmaf(beta, po.y, zj.y), fmaf(beta, po.z, zj.z));
+                }
+                acc = acc + mul(B[k], pj);
+            }
+            ap = acc;
+            sig = (double)p.x * acc.x + (double)p.y * acc.y + (double)p.z * acc.z;
+        }
+        sig = warp_sum(sig);
+        if (lane == 0 && has) spart[warp * 4] = sig;
+        __syncthreads();
+        write_segment_slots<W * 32, 1>(bp, spart, s0, s1, il0, il1);
+        ok = grid_sync(gb, target, &s_flag);
+        if (!ok) break;
+        if (threadIdx.x == 0) s_exit = *(volatile unsigned*)&gb->ndone >= (unsigned)bp.n_inst;
+        __syncthreads();
+        if (s_exit) break;
+
+        instances_alpha<W>(bp, li, il0, il1);
+        __syncthreads();
+        double rz = 0.0, rr = 0.0;
+        if (row && !li[li_idx].done) {
+            const LocalInst& L = li[li_idx];
+            const float alpha = L.alpha;
+            ZP* En = (L.iter & 1) ? zp0 : zp1;
+            x = f3(fmaf(alpha, p.x, x.x), fmaf(alpha, p.y, x.y), fmaf(alpha, p.z, x.z));
+            r = f3(fmaf(-alpha, ap.x, r.x), fmaf(-alpha, ap.y, r.y), fmaf(-alpha, ap.z, r.z));
+            z = mul(Mi, r);
+            En[i].z = f4(z);
+            rz = (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
+            rr = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
+        }
+        rz = warp_sum(rz);
+        rr = warp_sum(rr);
+        if (lane == 0 && has) {
+            spart[warp * 4] = rz;
+            spart[warp * 4 + 1] = rr;
+        }
+        __syncthreads();
+        write_segment_slots<W * 32, 2>(bp, spart, s0, s1, il0, il1);
+        ok = grid_sync(gb, target, &s_flag);
+        if (!ok) break;
+        instances_beta<W>(bp, li, il0, il1, cfg);
+        __syncthreads();
+    }
+    if (row) {
+        v.x[i] = f4(x);
+        v.r[i] = f4(r);
+        v.z[i] = f4(z);
+    }
+    if (!ok) instances_fail(bp, li, il0, il1);
 }
 
 // x_{n+1} = x_n + dx, v = dx/dt * exp(-c dt) (cloth_simulator.cu:222-244) for
@@ -428,15 +637,17 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm) 
 __global__ void finalize_batch_kernel(StepArgs a, Vecs v, BatchPlan bp) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
+    const int e = a.row_to_ext ? a.row_to_ext[i] : i;
+    if (e < 0) return;
     const int st = bp.inst[bp.slice_inst[i >> 5]].status;
     if (st == kSolveNonfinite || st == kSolveKernelError) return;
     const float4 d = v.x[i];
-    const float3 xn = ld3(a.pos, i);
-    st3(a.pos, i, f3(xn.x + d.x, xn.y + d.y, xn.z + d.z));
+    const float3 xn = ld3(a.pos, e);
+    st3(a.pos, e, f3(xn.x + d.x, xn.y + d.y, xn.z + d.z));
     const float inv_dt = 1.0f / a.dt;
     float3 vn = f3(d.x * inv_dt, d.y * inv_dt, d.z * inv_dt);
     if (a.damping > 0.0f) vn = vn * expf(-a.damping * a.dt);
-    st3(a.vel, i, vn);
+    st3(a.vel, e, vn);
 }
 
 // Resets the barrier and per-instance states before a solve.

@@ -199,6 +199,55 @@ PYBIND11_MODULE(_chysx_native, m) {
                  check(chysx_cloth_num_off_diag_blocks(s.h(), &n));
                  return n;
              })
+        .def("set_instances",
+             [](PyClothSimulator& s, py::object offsets) {
+                 if (offsets.is_none()) {
+                     check(chysx_cloth_set_instances(s.h(), nullptr, 0));
+                     return;
+                 }
+                 I32 o = offsets.cast<I32>();
+                 if (o.ndim() != 1 || o.shape(0) < 2)
+                     throw py::value_error("set_instances: offsets must be 1-D with at least 2 entries");
+                 check(chysx_cloth_set_instances(s.h(), o.data(), (int)o.shape(0) - 1));
+             },
+             py::arg("offsets"),
+             "Declare independent cloth instances: particles [offsets[b], offsets[b+1]); None = one system.")
+        .def("instance_stats",
+             [](PyClothSimulator& s) {
+                 int n = 0;
+                 check(chysx_cloth_num_instances(s.h(), &n));
+                 py::array_t<int32_t> it(n), st(n);
+                 py::array_t<double> rr(n);
+                 check(chysx_cloth_instance_stats(s.h(), n, it.mutable_data(), rr.mutable_data(), st.mutable_data()));
+                 return py::make_tuple(it, rr, st);
+             })
+        .def("set_network",
+             [](PyClothSimulator& s, F32 params) {
+                 if (params.ndim() != 1) throw py::value_error("set_network: params must be 1-D float32");
+                 check(chysx_cloth_set_network(s.h(), params.data(), (int)params.shape(0)));
+             },
+             py::arg("params"))
+        .def("set_feature_output",
+             [](PyClothSimulator& s, std::uintptr_t features, std::uintptr_t predictions) {
+                 check(chysx_cloth_set_feature_output(s.h(), features, predictions));
+             },
+             py::arg("features_ptr"), py::arg("predictions_ptr") = 0)
+        .def("guess_kept",
+             [](PyClothSimulator& s) {
+                 int k = 0;
+                 check(chysx_cloth_guess_kept(s.h(), &k));
+                 return k;
+             })
+        .def("set_tuning",
+             [](PyClothSimulator& s, int path, int block, int grid) { check(chysx_cloth_set_tuning(s.h(), path, block, grid)); },
+             py::arg("solver_path") = 0, py::arg("block") = 0, py::arg("grid") = 0)
+        .def("solver_info",
+             [](const PyClothSimulator& s) {
+                 int p = 0, g = 0, b = 0;
+                 check(chysx_cloth_solver_info(s.h(), &p, &g, &b));
+                 static const char* names[] = {"resident", "loop", "streamed"};
+                 return py::make_tuple(names[p], g, b);
+             })
         .def("debug_dump_last_solve", [](PyClothSimulator& s) {
             int n = 0, nnz = 0;
             check(chysx_cloth_num_particles(s.h(), &n));

@@ -94,16 +94,58 @@ void build_plan(const std::vector<int>& inst_slice, int grid, HostPlan& o) {
     for (int b = 0; b < n_inst; ++b) o.inst_slot[b + 1] = o.inst_slot[b] + (inst_cta_hi[b] - o.inst_cta_lo[b] + 1);
 }
 
-void build_topology(int n, const std::vector<int>& tris, bool use_tris,
-                    const std::vector<int>& edges, bool use_springs,
-                    const std::vector<int>& pins, HostTopology& o) {
-    if (n < 0) throw std::invalid_argument("negative particle count");
+void build_topology(int n_ext, const std::vector<int>& tris_ext, bool use_tris,
+                    const std::vector<int>& edges_ext, bool use_springs,
+                    const std::vector<int>& pins_ext, const std::vector<int>& inst_offsets,
+                    HostTopology& o) {
+    if (n_ext < 0) throw std::invalid_argument("negative particle count");
     o = HostTopology();
+    o.n_ext = n_ext;
+    const int T = use_tris ? (int)(tris_ext.size() / 3) : 0;
+    const int E = use_springs ? (int)(edges_ext.size() / 2) : 0;
+    for (int q = 0; q < 3 * T; ++q) check_vertex(tris_ext[q], n_ext);
+    for (int q = 0; q < 2 * E; ++q) check_vertex(edges_ext[q], n_ext);
+    for (int v : pins_ext) check_vertex(v, n_ext);
+
+    // ---- internal row layout
+    int n = n_ext;
+    const int n_inst = inst_offsets.empty() ? 1 : (int)inst_offsets.size() - 1;
+    std::vector<int> inst_of;  // instance of every particle (instances only)
+    if (!inst_offsets.empty()) {
+        if (n_inst < 1 || inst_offsets.front() != 0 || inst_offsets.back() != n_ext)
+            throw std::invalid_argument("instance offsets must run from 0 to the particle count");
+        o.ext_to_row.resize(n_ext);
+        inst_of.resize(n_ext);
+        o.inst_slice.assign(n_inst + 1, 0);
+        int row = 0;
+        for (int b = 0; b < n_inst; ++b) {
+            const int lo = inst_offsets[b], hi = inst_offsets[b + 1];
+            if (hi <= lo) throw std::invalid_argument("instance offsets must be strictly increasing");
+            for (int e = lo; e < hi; ++e) {
+                o.ext_to_row[e] = row + (e - lo);
+                inst_of[e] = b;
+            }
+            row += ((hi - lo) + kSlice - 1) / kSlice * kSlice;
+            o.inst_slice[b + 1] = row / kSlice;
+        }
+        n = row;
+        o.row_to_ext.assign(n, -1);
+        for (int e = 0; e < n_ext; ++e) o.row_to_ext[o.ext_to_row[e]] = e;
+        for (int t = 0; t < T; ++t) {
+            const int b = inst_of[tris_ext[3 * t]];
+            if (inst_of[tris_ext[3 * t + 1]] != b || inst_of[tris_ext[3 * t + 2]] != b)
+                throw std::invalid_argument("triangle " + std::to_string(t) + " connects two instances");
+        }
+    }
+    auto R = [&](int e) { return o.ext_to_row.empty() ? e : o.ext_to_row[e]; };
+    std::vector<int> tris(3 * (size_t)T), edges(2 * (size_t)E), pins(pins_ext.size());
+    for (int q = 0; q < 3 * T; ++q) tris[q] = R(tris_ext[q]);
+    for (int q = 0; q < 2 * E; ++q) edges[q] = R(edges_ext[q]);
+    for (size_t q = 0; q < pins.size(); ++q) pins[q] = R(pins_ext[q]);
     o.n = n;
     o.n_slices = (n + kSlice - 1) / kSlice;
     o.n_pad = o.n_slices * kSlice;
-    const int T = use_tris ? (int)(tris.size() / 3) : 0;
-    const int E = use_springs ? (int)(edges.size() / 2) : 0;
+    if (inst_offsets.empty()) o.inst_slice = {0, std::max(1, o.n_slices)};
 
     // ---- adjacency: triangle pairs (src/cloth/cloth_simulator.cu:720-739)
     // plus spring edges, per-row sort + unique (src/sparse/block_csr.cu:111-135)

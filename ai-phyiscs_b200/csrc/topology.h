@@ -26,7 +26,9 @@ constexpr unsigned kDiagSlot = 0xFFu;   // "other vertex is this row": goes to t
 constexpr int kMaxRowWidth = 254;       // slots are stored in 8 bits
 
 struct HostTopology {
-    int n = 0;          // rows (particles)
+    int n = 0;          // internal rows: particles, plus padding rows that
+                        // start every instance on a fresh 32-row slice
+    int n_ext = 0;      // particles in the caller's buffers
     int n_slices = 0;
     int n_pad = 0;      // n_slices * 32
     int max_width = 0;  // widest off-diagonal slice
@@ -44,16 +46,24 @@ struct HostTopology {
     std::vector<uint32_t> sinc_meta;
     // pins sorted by row; pin_perm[sorted] = caller's index
     std::vector<int> pin_off, pin_row, pin_perm;
+    // instances: internal rows <-> particles (empty when they coincide)
+    std::vector<int> row_to_ext, ext_to_row;
+    std::vector<int> inst_slice;  // [n_inst + 1] slice range of every instance
     long long nnz() const { return (long long)csr_col.size(); }
     long long ell_entries() const { return slice_off.empty() ? 0 : slice_off.back(); }
 };
 
 // Builds the pattern from triangles (if use_tris), spring edges (if
-// use_springs) and pins.  Throws std::out_of_range for a vertex index outside
-// [0, n) and std::runtime_error when a row exceeds kMaxRowWidth neighbours.
+// use_springs) and pins over n particles.  inst_offsets (empty, or n_inst+1
+// increasing particle offsets from 0 to n) splits the particles into
+// independent instances; every instance then starts on its own slice and no
+// element may connect two instances.  Throws std::out_of_range for a vertex
+// index outside [0, n), std::invalid_argument for an element spanning two
+// instances, std::runtime_error when a row exceeds kMaxRowWidth neighbours.
 void build_topology(int n, const std::vector<int>& tris, bool use_tris,
                     const std::vector<int>& edges, bool use_springs,
-                    const std::vector<int>& pins, HostTopology& out);
+                    const std::vector<int>& pins, const std::vector<int>& inst_offsets,
+                    HostTopology& out);
 
 // Work split of the persistent PCG kernel: `grid` CTAs each take a
 // contiguous, balanced range of slices; instances own contiguous slice

@@ -341,14 +341,17 @@ def run_ours(args, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 dots)", "data": "synthetic",
         "config": {"workload": args.workload, "particles": n, "off_diag_blocks": int(nnz),
                    "rel_tol": rel_tol, "warm_start": args.warm,
-                   "solver_path": "persistent" if args.path == 0 else "graph-loop",
-                   "pcg_grid": g.sim.launched_grid(), "l2": "flushed between steps (256 MiB write)"},
+                   "pcg_kernel": g.sim.solver_info()[0], "pcg_grid": g.sim.solver_info()[1],
+                   "pcg_block": g.sim.solver_info()[2], "l2": "flushed between steps (256 MiB write)"},
         "pcg_iters_per_step": mean_iters,
         "pcg_iters_per_step_minmax": [int(iters.min()), int(iters.max())],
         "solve_status": sorted(set(int(s) for s in statuses)),
         "us_per_pcg_iteration": float(np.sum(solve_ms) * 1e3 / np.sum(iters)),
         "assembly_ms": float(np.mean(asm_ms)),
-        "roofline": {"bound": "hbm", "kernel": "pcg_persistent_kernel", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": {"resident": "pcg_resident_kernel",
+                                                "streamed": "pcg_persistent_kernel",
+                                                "loop": "pcg_spmv_kernel+pcg_update_kernel"}[g.sim.solver_info()[0]],
+                     "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": (traffic_it * mean_iters) if traffic_it else None,
                      "algorithmic_bytes_per_iteration": b_it,
@@ -360,7 +363,7 @@ def run_ours(args, rank, world, local_rank):
                                     f"iterations/step")},
         "e2e": {"value": e2e_steps * world / (e2e_ms_max * 1e-3), "unit": "steps/s",
                 "h2d_bytes_per_step": 2 * 12 * n, "d2h_bytes_per_step": 2 * 12 * n},
-        "gpu_launches": (4 if args.path == 0 else -1) * args.steps,
+        "gpu_launches": 4 * args.steps,
         "clocks": clk,
         "wall_s": wall,
     }
@@ -378,7 +381,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="grid256")
     ap.add_argument("--warm", default="zero", choices=["zero", "previous", "learned"])
-    ap.add_argument("--path", type=int, default=0, help="0 persistent PCG, 1 graph loop")
+    ap.add_argument("--path", type=int, default=0,
+                    help="0 persistent PCG (resident when it fits), 1 graph loop, 2 streamed persistent")
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--grid", type=int, default=0)
     ap.add_argument("--cpu-budget", type=float, default=15.0)

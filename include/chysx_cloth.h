@@ -157,14 +157,68 @@ int chysx_cloth_num_off_diag_blocks(const chysx_cloth* h, int* out);
 int chysx_cloth_debug_dump(chysx_cloth* h, float* diag, int32_t* row_offsets,
                            int32_t* col_indices, float* values, float* rhs, float* dx);
 
+/* Learned warm start (no counterpart in the reference).  A per-vertex
+ * network (20 1-ring features -> 3 x 64 GELU -> dv, BF16 on tensor cores)
+ * predicts each step's velocity change; the PCG starts from dx0 = dt (v + dv)
+ * and still runs to the same tolerance, falling back to the zero guess per
+ * instance when ||b - A dx0|| > ||b||.  set_network takes the flat FP32
+ * parameter vector (chysx_mlp_num_params() floats: input mean/std, output
+ * mean/std, then W1 [20][64], b1, W2 [64][64], b2, W3, b3, W4 [64][3], b4)
+ * and enables set_solver(..., CHYSX_WARM_LEARNED). */
+int chysx_cloth_set_network(chysx_cloth* h, const float* params, int n_params);
+/* Every following step also writes its raw features (particle_count x 20
+ * floats, caller order) to this device buffer (0 = off): the training-data
+ * tap.  The target of a step is v_{n+1} - v_n (undamped).  With a network
+ * loaded and the learned warm start on, `predictions` (may be 0) receives
+ * the predicted dv (particle_count x 3). */
+int chysx_cloth_set_feature_output(chysx_cloth* h, uintptr_t features, uintptr_t predictions);
+/* Number of instances whose last solve kept the warm-start guess (the rest
+ * fell back to the zero guess); synchronises. */
+int chysx_cloth_guess_kept(chysx_cloth* h, int* kept);
+int chysx_mlp_num_params(void);
+int chysx_mlp_num_features(void);
+/* Device workspace needed by the training / prediction calls for `rows`. */
+uint64_t chysx_mlp_workspace_bytes(int rows);
+/* Loss (mean squared error of standardised dv) and its gradient in the flat
+ * parameter layout, for `rows` feature / target rows (device pointers;
+ * synchronises `stream` to return the loss). */
+int chysx_mlp_gradients(uintptr_t params, uintptr_t features, uintptr_t targets, int rows, uintptr_t grad,
+                        double* loss, uintptr_t workspace, uint64_t workspace_bytes, uintptr_t stream);
+/* Predicted dv (rows x 3) for feature rows. */
+int chysx_mlp_predict(uintptr_t params, uintptr_t features, int rows, uintptr_t dv, uintptr_t workspace,
+                      uint64_t workspace_bytes, uintptr_t stream);
+/* One Adam step (lr, step count >= 1) on the FP32 master parameters, using
+ * the gradient of the minibatch; m1 / m2 are the moment buffers. */
+int chysx_mlp_train_step(uintptr_t params, uintptr_t grad, uintptr_t m1, uintptr_t m2, uintptr_t features,
+                         uintptr_t targets, int rows, float lr, int adam_step, uintptr_t workspace,
+                         uint64_t workspace_bytes, double* loss, uintptr_t stream);
+
+/* Batched solve (no counterpart in the reference): the particles of the
+ * external buffers form n_instances independent cloths, instance b owning
+ * particles [offsets[b], offsets[b+1]) (offsets[0] = 0, offsets[n] = the
+ * particle count; no triangle may connect two instances).  All instances are
+ * assembled into one concatenated block system and solved by one persistent
+ * PCG kernel with a separate convergence test per instance; last_stats then
+ * reports the slowest / worst instance.  n_instances = 0 restores the single
+ * system. */
+int chysx_cloth_set_instances(chysx_cloth* h, const int32_t* offsets, int n_instances);
+int chysx_cloth_num_instances(const chysx_cloth* h, int* out);
+/* Per-instance iterations, relative residual and status of the last step
+ * (arrays of n = num_instances entries; synchronises). */
+int chysx_cloth_instance_stats(chysx_cloth* h, int n, int* iterations, double* rel_residual,
+                               int* status);
+
 /* Solver kernel selection (no counterpart in the reference, whose PCG is a
  * fixed chain of 8 launches per iteration, src/solver/pcg_solver.cu:542-592):
- * solver_path 0 = one persistent cooperative kernel per solve (default),
- * 1 = CUDA-graph WHILE loop of two kernels per iteration.  block (0, 128,
- * 256, 512) and grid (0 = automatic) size the persistent kernel. */
+ * solver_path 0 = one persistent cooperative kernel per solve, with rows held
+ * in registers when the system fits (default), 1 = CUDA-graph WHILE loop of
+ * two kernels per iteration, 2 = the streamed persistent kernel forced.
+ * block (0, 128, 256, 512) and grid (0 = automatic) size the streamed
+ * persistent kernel. */
 int chysx_cloth_set_tuning(chysx_cloth* h, int solver_path, int block, int grid);
-/* CTAs of the persistent PCG launch chosen at the last graph build. */
-int chysx_cloth_launched_grid(const chysx_cloth* h, int* out);
+/* Kernel used at the last graph build: path 0 register-resident persistent,
+ * 1 graph loop, 2 streamed persistent; with its grid and block size. */
+int chysx_cloth_solver_info(const chysx_cloth* h, int* path, int* grid, int* block);
 
 /* Measurement hooks (no counterpart in the reference): when enabled, the
  * step graph records CUDA events around assembly, the PCG solve and the

@@ -22,7 +22,7 @@ def gpu_from(sc, fx, pre, springs, path=0, tol=1e-9):
     return g
 
 
-@pytest.mark.parametrize("path", [0, 1])
+@pytest.mark.parametrize("path", [0, 1, 2])
 @pytest.mark.parametrize("fixture,pre,springs,steps,converged", DUMPS)
 def test_cuda_system_matches_reference(fixture, pre, springs, steps, converged, path):
     import torch

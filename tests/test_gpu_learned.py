@@ -1,0 +1,195 @@
+"""GPU: the learned warm start's tensor-core kernels against the FP64 network
+oracle, the simulator's feature tap against a CPU recomputation, and the
+learned guess's effect on the solve (same converged state, zero-guess
+fallback when the guess is worse)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle.mlp_oracle as M
+import oracle.oracle as O
+from chysx import capi, learned, scenes
+from chysx.runner import GpuCloth
+
+pytestmark = pytest.mark.gpu
+
+# BF16 activations and gradients: tensor-core FP32 accumulation vs FP64
+# with the same BF16 rounding points.
+TOL_GRAD = 2e-2   # relative (per layer, Frobenius norm)
+TOL_PRED = 1e-2   # relative to the output scale
+
+
+def _rand_params(rng):
+    mu_in = rng.standard_normal(M.N_IN) * 0.1
+    sd_in = rng.uniform(0.5, 2.0, M.N_IN)
+    p = M.init_params(rng, mu_in, sd_in, np.array([0.1, -0.2, 0.05]), np.array([0.5, 1.5, 1.0]))
+    for k in ("b1", "b2", "b3", "b4"):
+        a, b = M.OFF[k]
+        p[a:b] = rng.standard_normal(b - a) * 0.1
+    return p.astype(np.float32)
+
+
+def _dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+@pytest.mark.parametrize("rows", [1, 37, 4096])
+def test_gradient_matches_oracle(rows):
+    import torch
+
+    rng = np.random.default_rng(rows)
+    p = _rand_params(rng)
+    feat = (rng.standard_normal((rows, M.N_IN)) * 1.5).astype(np.float32)
+    targ = (rng.standard_normal((rows, M.N_OUT)) * 0.7).astype(np.float32)
+    ws = torch.empty(int(capi.lib().chysx_mlp_workspace_bytes(rows)), dtype=torch.uint8, device="cuda")
+    dp, df, dt = _dev(p), _dev(feat), _dev(targ)
+    grad = torch.zeros_like(dp)
+    loss = ctypes.c_double()
+    capi.check(capi.lib().chysx_mlp_gradients(dp.data_ptr(), df.data_ptr(), dt.data_ptr(), rows, grad.data_ptr(),
+                                              ctypes.byref(loss), ws.data_ptr(), ws.numel(), 0))
+    g = grad.cpu().numpy().astype(np.float64)
+    oloss, og = M.loss_and_grad(p, feat, targ, emulate_bf16=True)
+    assert abs(loss.value - oloss) <= 1e-3 * oloss
+    for k in ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4"):
+        a, b = M.OFF[k]
+        err = np.linalg.norm(g[a:b] - og[a:b]) / max(np.linalg.norm(og[a:b]), 1e-30)
+        assert err < TOL_GRAD, (k, err)
+    assert np.all(g[:M.OFF["w1"][0]] == 0.0)
+
+
+def test_prediction_matches_oracle():
+    import torch
+
+    rng = np.random.default_rng(5)
+    p = _rand_params(rng)
+    rows = 1000
+    feat = (rng.standard_normal((rows, M.N_IN))).astype(np.float32)
+    ws = torch.empty(int(capi.lib().chysx_mlp_workspace_bytes(rows)), dtype=torch.uint8, device="cuda")
+    out = torch.zeros((rows, 3), dtype=torch.float32, device="cuda")
+    dp, df = _dev(p), _dev(feat)
+    capi.check(capi.lib().chysx_mlp_predict(dp.data_ptr(), df.data_ptr(), rows, out.data_ptr(), ws.data_ptr(),
+                                            ws.numel(), 0))
+    ref = M.predict(p, feat)
+    assert np.abs(out.cpu().numpy() - ref).max() < TOL_PRED * np.abs(ref).max()
+
+
+def _features_cpu(sc, pos, vel, inv_mass, grad, dt):
+    """Recompute the 20 features of the feature tap from the state and the
+    oracle's elastic gradient."""
+    n = pos.shape[0]
+    nb = [set() for _ in range(n)]
+    for t in sc["tris"]:
+        for a in range(3):
+            for b in range(3):
+                if t[a] != t[b]:
+                    nb[t[a]].add(int(t[b]))
+    m = np.where(inv_mass > 1e-12, 1.0 / np.maximum(inv_mass, 1e-30), 1e8)
+    acc = -grad / m[:, None]
+    g = np.array(sc["gravity"])
+    pinned = np.zeros(n)
+    pinned[sc["pin_idx"]] = 1.0
+    ks = np.asarray(sc["k_spring"], np.float64) * np.ones(sc["edges"].shape[0])
+    logk = np.zeros(n)
+    cnt = np.zeros(n)
+    for (a, b), k in zip(sc["edges"], ks):
+        for v in (a, b):
+            logk[v] += np.log10(k)
+            cnt[v] += 1
+    logk = np.where(cnt > 0, logk / np.maximum(cnt, 1), 0.0)
+    F = np.zeros((n, 20))
+    for i in range(n):
+        js = sorted(nb[i])
+        d = pos[js] - pos[i]
+        F[i, 0:3] = vel[i]
+        F[i, 3:6] = dt * g
+        F[i, 6:9] = d.mean(0) / np.linalg.norm(d, axis=1).mean()
+        F[i, 9:12] = (vel[js] - vel[i]).mean(0)
+        F[i, 12:15] = dt * acc[i]
+        F[i, 15:18] = dt * acc[js].mean(0)
+        F[i, 18] = pinned[i]
+        F[i, 19] = logk[i]
+    return F
+
+
+def test_feature_tap_matches_cpu_recomputation():
+    import torch
+
+    sc = scenes.config_small()
+    g = GpuCloth(sc, max_iter=3000, rel_tol=1e-8, warm_start="zero")
+    g.run(20, record_iters=False)
+    n = sc["pos"].shape[0]
+    fbuf = torch.zeros((n, 20), dtype=torch.float32, device="cuda")
+    g.sim.set_feature_output(fbuf.data_ptr())
+    pos, vel = g.positions(), g.velocities()
+    inv = g.inv_mass.cpu().numpy().astype(np.float64)
+    g.step()
+    feat = fbuf.cpu().numpy()
+    # the oracle's elastic gradient at the same state: grad = M/dt^2 (xt - x) - rhs
+    o = O.OracleCloth(True)
+    o.set_material(sc["density"], 0.0, sc["gravity"])
+    o.set_state(pos.astype(np.float32), vel.astype(np.float32), inv.astype(np.float32))
+    o.set_mesh(sc["tris"])
+    o.set_options(True, False, 1e-6)
+    o.set_state(sc["pos"], sc["vel"], inv.astype(np.float32))
+    o.build_springs(sc["k_spring"])
+    o.build_stretch(sc["k_stretch"])
+    o.set_pins(sc["pin_idx"], sc["pin_targets"])
+    o.set_state(pos.astype(np.float32), vel.astype(np.float32), inv.astype(np.float32))
+    o.set_solver(0, 0.0, "zero")
+    o.step(sc["dt"])
+    rhs = o.dump_system()[4]
+    m = 1.0 / inv
+    dt = np.float32(sc["dt"])
+    gvec = np.array(sc["gravity"], np.float32)
+    xt = pos.astype(np.float32) + dt * vel.astype(np.float32) + dt * dt * gvec
+    grad = (m / (dt * dt))[:, None] * (xt.astype(np.float64) - pos) - rhs
+    ref = _features_cpu(sc, pos, vel, inv, grad, float(dt))
+    scale = np.maximum(np.abs(ref).max(0), 1e-3)
+    err = np.abs(feat - ref) / scale
+    # elastic features carry the FP32 round-off of near-cancelling forces
+    assert err[:, :12].max() < 1e-4 and err[:, 18:].max() < 1e-5
+    assert err[:, 12:18].max() < 5e-2
+
+
+def test_in_step_prediction_matches_oracle_and_guess_is_used():
+    import torch
+
+    rng = np.random.default_rng(9)
+    sc = scenes.config_small()
+    n = sc["pos"].shape[0]
+    p = _rand_params(rng)
+    g = GpuCloth(sc, max_iter=3000, rel_tol=1e-8, warm_start="zero")
+    g.run(10, record_iters=False)
+    g.sim.set_network(p)
+    g.sim.set_solver(3000, 1e-8, "learned")
+    fbuf = torch.zeros((n, 20), dtype=torch.float32, device="cuda")
+    pbuf = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    g.sim.set_feature_output(fbuf.data_ptr(), pbuf.data_ptr())
+    g.step()
+    assert g.stats()[2] == capi.SOLVE_CONVERGED
+    ref = M.predict(p, fbuf.cpu().numpy())
+    assert np.abs(pbuf.cpu().numpy() - ref).max() < TOL_PRED * np.abs(ref).max()
+
+
+def test_learned_mode_reaches_the_same_state():
+    rng = np.random.default_rng(3)
+    sc = scenes.config_small(steps=30)
+    z = GpuCloth(sc, max_iter=5000, rel_tol=1e-8, warm_start="zero")
+    z.run(30, record_iters=False)
+    w = GpuCloth(sc, max_iter=5000, rel_tol=1e-8, warm_start="zero")
+    w.sim.set_network(_rand_params(rng))
+    w.sim.set_solver(5000, 1e-8, "learned")
+    w.run(30, record_iters=False)
+    assert np.abs(z.positions() - w.positions()).max() < 2e-4
+
+
+def test_training_reduces_loss_on_collected_data():
+    feats, targs = learned.collect(total_steps=64, batch=8, steps_per_scene=8, samples_per_step=128,
+                                   log=lambda *_: None)
+    assert feats.shape[1] == 20 and targs.shape[1] == 3 and feats.shape[0] == targs.shape[0]
+    assert bool(feats.isfinite().all()) and bool(targs.isfinite().all())
+    params, hist = learned.train(feats, targs, epochs=4, batch_rows=1024, log=lambda *_: None)
+    assert hist[-1][2] < 0.9 * hist[0][2] or hist[-1][2] < 0.5

@@ -16,7 +16,9 @@ from chysx.runner import GpuCloth
 
 pytestmark = pytest.mark.gpu
 
-PATHS = [0, 1]  # 0 = persistent cooperative PCG, 1 = graph WHILE loop
+# 0 = persistent PCG (register-resident rows when the system fits),
+# 1 = graph WHILE loop of two kernels, 2 = streamed persistent kernel
+PATHS = [0, 1, 2]
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -72,8 +74,9 @@ def test_first_step_system_and_solution_match_oracle(path):
     np.testing.assert_array_equal(col, ocol)
     assert rel(diag, od) < 1e-6      # FP32 assembly
     assert rel(vals, ovals) < 1e-6
-    # at rest the elastic gradient is FP32 round-off of zero: compare absolutely
-    assert np.abs(rhs - orhs).max() < 2e-3 * np.abs(orhs).max()
+    # at rest the elastic gradient is FP32 round-off of zero (the reference
+    # shows the same 1e-4 N spread): compare absolutely
+    assert np.abs(rhs - orhs).max() < 5e-4
     assert np.abs(dx - odx).max() < 1e-6   # metres
 
 
@@ -98,11 +101,23 @@ def test_grid10_trajectory_matches_oracle(path):
 
 def test_paths_agree():
     sc = scenes.config_small()
-    a = make(sc, 0, max_iter=5000, rel_tol=1e-8)
-    b = make(sc, 1, max_iter=5000, rel_tol=1e-8)
-    a.run(20)
-    b.run(20)
-    assert np.abs(a.positions() - b.positions()).max() < 1e-5
+    runs = []
+    for path in PATHS:
+        g = make(sc, path, max_iter=5000, rel_tol=1e-8)
+        g.run(20)
+        runs.append(g.positions())
+    assert g.sim.solver_info()[0] == "streamed"
+    for p in runs[1:]:
+        assert np.abs(runs[0] - p).max() < 1e-5
+
+
+def test_solver_kernel_selection():
+    small = make(scenes.config_small(), 0, max_iter=50, rel_tol=0.0)
+    small.step()
+    assert small.sim.solver_info()[0] == "resident"
+    loop = make(scenes.config_small(), 1, max_iter=50, rel_tol=0.0)
+    loop.step()
+    assert loop.sim.solver_info()[0] == "loop"
 
 
 @pytest.mark.parametrize("path", PATHS)
