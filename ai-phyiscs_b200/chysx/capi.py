@@ -73,6 +73,7 @@ SIGNATURES = {
     "chysx_cloth_num_instances": (ctypes.c_int, [H, ip]),
     "chysx_cloth_instance_stats": (ctypes.c_int, [H, ctypes.c_int, ip, dp, ip]),
     "chysx_cloth_set_tuning": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "chysx_cloth_set_pcg_variant": (ctypes.c_int, [H, ctypes.c_int]),
     "chysx_cloth_solver_info": (ctypes.c_int, [H, ip, ip, ip]),
     "chysx_cloth_enable_timing": (ctypes.c_int, [H, ctypes.c_int]),
     "chysx_cloth_last_timing": (ctypes.c_int, [H, f32p, f32p, f32p]),
@@ -225,10 +226,13 @@ class Cloth:
 
     def solver_info(self):
         """(kernel, grid, block) of the last graph build; kernel is
-        'resident', 'loop' or 'streamed'."""
+        'resident', 'loop', 'streamed' or 'resident-1r' (single reduction)."""
         p, g, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check(self._L.chysx_cloth_solver_info(self.h, ctypes.byref(p), ctypes.byref(g), ctypes.byref(b)))
-        return ("resident", "loop", "streamed")[p.value], g.value, b.value
+        return ("resident", "loop", "streamed", "resident-1r")[p.value], g.value, b.value
+
+    def set_pcg_variant(self, variant):
+        check(self._L.chysx_cloth_set_pcg_variant(self.h, int(variant)))
 
     def num_off_diag_blocks(self):
         v = ctypes.c_int()

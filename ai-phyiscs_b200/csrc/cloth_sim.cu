@@ -486,6 +486,11 @@ public:
     // small enough, else streamed), 1 = graph WHILE loop of two kernels,
     // 2 = streamed persistent kernel forced.  block / grid of the streamed
     // persistent kernel (0 = automatic).
+    void set_variant(int variant) {
+        if (variant < 0 || variant > 1) throw std::invalid_argument("set_variant: variant must be 0 or 1");
+        if (variant != pcg_variant_) graph_dirty_ = true;
+        pcg_variant_ = variant;
+    }
     void set_tuning(int path, int block, int grid) {
         if (path < 0 || path > 2) throw std::invalid_argument("set_tuning: path must be 0, 1 or 2");
         if (block != 0 && block != 128 && block != 256 && block != 512)
@@ -496,9 +501,10 @@ public:
         pcg_grid_req_ = grid;
         graph_dirty_ = true;
     }
-    // kernel actually used by the last graph build: 0 resident, 1 loop, 2 streamed
+    // kernel actually used by the last graph build: 0 resident, 1 loop,
+    // 2 streamed, 3 resident single-reduction
     void solver_info(int* path, int* grid, int* block) const {
-        const int used = graph_path_ == kPathLoop ? 1 : (resident_ ? 0 : 2);
+        const int used = graph_path_ == kPathLoop ? 1 : (resident_ ? (single_reduction_ ? 3 : 0) : 2);
         if (path) *path = used;
         if (grid) *grid = used == 1 ? 0 : plan_.grid;
         if (block) *block = used == 1 ? kVecBlock : (resident_ ? resident_warps_ * 32 : pcg_block_);
@@ -757,6 +763,11 @@ private:
 
     static constexpr int kResidentMaxWidth = 8;
     const void* persistent_fn() const {
+        if (resident_ && single_reduction_) {
+            return resident_warps_ == 16
+                       ? reinterpret_cast<const void*>(&pcg_resident_cg1_kernel<16, kResidentMaxWidth>)
+                       : reinterpret_cast<const void*>(&pcg_resident_cg1_kernel<8, kResidentMaxWidth>);
+        }
         if (resident_) {
             return resident_warps_ == 16 ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, kResidentMaxWidth>)
                                          : reinterpret_cast<const void*>(&pcg_resident_kernel<8, kResidentMaxWidth>);
@@ -764,6 +775,14 @@ private:
         if (pcg_block_ == 128) return reinterpret_cast<const void*>(&pcg_persistent_kernel<128>);
         if (pcg_block_ == 512) return reinterpret_cast<const void*>(&pcg_persistent_kernel<512>);
         return reinterpret_cast<const void*>(&pcg_persistent_kernel<256>);
+    }
+
+    // neighbour-exchange buffer k of the resident kernels (null otherwise)
+    void* exchange_buffer(int k) const {
+        const size_t np = (size_t)std::max(1, topo_.n_pad);
+        if (resident_ && single_reduction_) return d_umq_.get() + k * np;
+        if (resident_) return d_zp_.get() + k * np;
+        return nullptr;
     }
 
     BatchPlan batch_plan() const {
@@ -791,12 +810,18 @@ private:
     bool plan_resident(int sms) {
         if (solver_path_ != kPathPersistent || topo_.max_width > kResidentMaxWidth) return false;
         const int n_slices = std::max(1, topo_.n_slices);
+        single_reduction_ = pcg_variant_ == 1 && topo_.inst_slice.size() == 2;
         for (int W : {16, 8}) {
             resident_ = true;
             resident_warps_ = W;
             const int grid = (n_slices + W - 1) / W;
             build_plan(topo_.inst_slice, grid, plan_);
             pers_smem_ = (size_t)W * 4 * sizeof(double) + (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
+            if (single_reduction_)
+                pers_smem_ += (size_t)kResidentMaxWidth * W * 32 * (6 * sizeof(float) + sizeof(int));
+            if (pers_smem_ > 48 * 1024)
+                ck(cudaFuncSetAttribute(persistent_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pers_smem_),
+                   "cudaFuncSetAttribute(resident smem)");
             int per_sm = 0;
             ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_fn(), W * 32, pers_smem_),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor(resident)");
@@ -812,10 +837,16 @@ private:
         ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
         if (plan_resident(sms)) {
             upload_plan();
-            d_zp_.resize(2 * (size_t)std::max(1, topo_.n_pad));
-            d_zp_.zero();
+            if (single_reduction_) {
+                d_umq_.resize(2 * (size_t)std::max(1, topo_.n_pad));
+                d_umq_.zero();
+            } else {
+                d_zp_.resize(2 * (size_t)std::max(1, topo_.n_pad));
+                d_zp_.zero();
+            }
             return;
         }
+        single_reduction_ = false;
         const int W = pcg_block_ / 32;
         const int n_slices = std::max(1, topo_.n_slices);
         // shared memory depends on the plan; iterate once with a generous bound
@@ -890,9 +921,9 @@ private:
             ck(cudaGraphAddKernelNode(&reset, graph_, &t1, 1, &p), "add reset node");
         }
         {
-            ZP* zp0 = d_zp_.get();
-            ZP* zp1 = zp0 + std::max(1, topo_.n_pad);
-            void* pargs[] = {&t, &v, &bp, &cur_cfg_, &warm_i, &zp0, &zp1};
+            void* ex0 = exchange_buffer(0);
+            void* ex1 = exchange_buffer(1);
+            void* pargs[] = {&t, &v, &bp, &cur_cfg_, &warm_i, &ex0, &ex1};
             cudaKernelNodeParams p{};
             p.func = const_cast<void*>(persistent_fn());
             p.gridDim = dim3(plan_.grid);
@@ -1032,9 +1063,9 @@ private:
             cudaKernelNodeParams ap;
             asm_params(ap, aargs);
             ck(cudaGraphExecKernelNodeSetParams(exec_, asm_node_, &ap), "update assemble node");
-            ZP* zp0 = d_zp_.get();
-            ZP* zp1 = zp0 + std::max(1, topo_.n_pad);
-            void* pargs[] = {&t, &v, &bp, &c, &warm_i, &zp0, &zp1};
+            void* ex0 = exchange_buffer(0);
+            void* ex1 = exchange_buffer(1);
+            void* pargs[] = {&t, &v, &bp, &c, &warm_i, &ex0, &ex1};
             cudaKernelNodeParams pp{};
             pp.func = const_cast<void*>(persistent_fn());
             pp.gridDim = dim3(plan_.grid);
@@ -1124,9 +1155,11 @@ private:
     cudaGraphNode_t guess_node_ = nullptr;
     std::vector<int> inst_offsets_;
     DevBuf<int> d_row_to_ext_;
-    bool resident_ = false;
+    bool resident_ = false, single_reduction_ = false;
     int resident_warps_ = 16;
+    int pcg_variant_ = 0;  // 0 PCG with two reductions, 1 single-reduction PCG
     DevBuf<ZP> d_zp_;
+    DevBuf<UMQ> d_umq_;
     bool timing_ = false;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     // graph
@@ -1363,6 +1396,10 @@ int chysx_cloth_instance_stats(chysx_cloth* h, int n, int* iters, double* relres
 int chysx_cloth_set_tuning(chysx_cloth* h, int solver_path, int block, int grid) {
     CHYSX_H(h);
     return guard([&] { h->sim.set_tuning(solver_path, block, grid); });
+}
+int chysx_cloth_set_pcg_variant(chysx_cloth* h, int variant) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_variant(variant); });
 }
 int chysx_cloth_solver_info(const chysx_cloth* h, int* path, int* grid, int* block) {
     CHYSX_H(h);

@@ -631,6 +631,249 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     if (!ok) instances_fail(bp, li, il0, il1);
 }
 
+
+// ---------------------------------------------------------------------------
+// Single-reduction variant of the register-resident solve (Chronopoulos-Gear
+// PCG): one grid barrier per iteration instead of two.  With u = M^-1 r,
+// w = A u, m = M^-1 w, q = M^-1 s, s = A p:
+//   q_k = m_k + b_k q_k-1,  s_k = w_k + b_k s_k-1,  p_k = u_k + b_k p_k-1
+//   x += a_k p_k,  r -= a_k s_k,  u_k+1 = u_k - a_k q_k
+//   w_k+1 = A u_k+1,  m_k+1 = M^-1 w_k+1
+//   g = (r,u), d = (w,u), rr = (r,r) in one reduction
+//   b_k+1 = g_k+1 / g_k,  a_k+1 = g_k+1 / (d_k+1 - b_k+1 g_k+1 / a_k)
+// Every row publishes (u_k, m_k, q_k-1); a neighbour's u_k+1 is rebuilt from
+// them with the owner's exact FMA sequence, so A u_k+1 sees one consistent
+// vector and needs no second barrier.  Mathematically the same iterates as
+// PCG (pcg_solver.cu:467-593); round-off differs.  Off-diagonal blocks of
+// the CTA's rows live in shared memory.
+// ---------------------------------------------------------------------------
+struct UMQ {
+    float4 u;
+    float4 m;
+    float4 q;
+    float4 pad;
+};
+
+__device__ __forceinline__ float3 fma3(float a, float3 x, float3 y) {
+    return f3(fmaf(a, x.x, y.x), fmaf(a, x.y, y.y), fmaf(a, x.z, y.z));
+}
+
+template <int W, int MAXW>
+__global__ void __launch_bounds__(W * 32, 1)
+pcg_resident_cg1_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, UMQ* e0, UMQ* e1) {
+    extern __shared__ double s_mem[];
+    __shared__ int s_flag;
+    __shared__ int s_exit;
+    constexpr int R = W * 32;  // rows per CTA
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
+    const int il0 = bp.cta_inst_lo[blockIdx.x], il1 = bp.cta_inst_hi[blockIdx.x];
+    double* spart = s_mem;  // [W * 4]
+    LocalInst* li = reinterpret_cast<LocalInst*>(s_mem + (size_t)W * 4);
+    float* sblk = reinterpret_cast<float*>(li + bp.max_inst_per_cta);  // [MAXW * 6][R]
+    int* scol = reinterpret_cast<int*>(sblk + (size_t)MAXW * 6 * R);   // [MAXW][R]
+    GridBarrier* gb = bp.bar;
+    unsigned target = 0;
+    if (threadIdx.x == 0) s_flag = 0;
+    bool ok = true;
+
+    const int s = s0 + warp;
+    const bool has = s < s1;
+    const int i = s * 32 + lane;
+    const bool row = has && i < t.n;
+    const int li_idx = has ? bp.slice_inst[s] - il0 : 0;
+    const int tid = threadIdx.x;
+
+    S6 D{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, Mi{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int w = 0;
+    float3 b = f3(0.f, 0.f, 0.f);
+    if (row) {
+        D = ld6(t.diag + (size_t)s * 192 + lane);
+        Mi = ld6(t.minv + (size_t)s * 192 + lane);
+        b = xyz(v.b[i]);
+        const int so = t.slice_off[s];
+        w = (t.slice_off[s + 1] - so) >> 5;
+        for (int k = 0; k < MAXW; ++k) {
+            if (k < w) {
+                scol[k * R + tid] = t.col[so + k * 32 + lane];
+                const float* src = t.val + (size_t)so * 6 + (size_t)k * 192 + lane;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) sblk[(k * 6 + c) * R + tid] = src[c * 32];
+            }
+        }
+    }
+    auto offdiag = [&](int k) {
+        return S6{sblk[(k * 6 + 0) * R + tid], sblk[(k * 6 + 1) * R + tid], sblk[(k * 6 + 2) * R + tid],
+                  sblk[(k * 6 + 3) * R + tid], sblk[(k * 6 + 4) * R + tid], sblk[(k * 6 + 5) * R + tid]};
+    };
+
+    // ---- initial residual: r0 = b - A x0, u0 = M^-1 r0 (phase 0a) -----------
+    float3 x = f3(0.f, 0.f, 0.f), r = b, u = f3(0.f, 0.f, 0.f);
+    double rz = 0.0, rr = 0.0, bb = 0.0, bmb = 0.0;
+    if (row) {
+        const float3 zb = mul(Mi, b);
+        bb = (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z;
+        bmb = (double)b.x * zb.x + (double)b.y * zb.y + (double)b.z * zb.z;
+        if (warm) {
+            x = xyz(v.x[i]);
+            float3 ax = mul(D, x);
+            for (int k = 0; k < w; ++k) ax = ax + mul(offdiag(k), xyz(v.x[scol[k * R + tid]]));
+            r = b - ax;
+            u = mul(Mi, r);
+            rz = (double)r.x * u.x + (double)r.y * u.y + (double)r.z * u.z;
+            rr = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
+        } else {
+            u = zb;
+            rz = bmb;
+            rr = bb;
+        }
+    }
+    {
+        double a0 = warp_sum(rz), a1 = warp_sum(rr), a2 = warp_sum(bb), a3 = warp_sum(bmb);
+        if (lane == 0 && has) {
+            double* sp = spart + warp * 4;
+            sp[0] = a0; sp[1] = a1; sp[2] = a2; sp[3] = a3;
+        }
+    }
+    __syncthreads();
+    write_segment_slots<R, 4>(bp, spart, s0, s1, il0, il1);
+    ok = grid_sync(gb, target, &s_flag);
+    if (ok) {
+        instances_start<W>(bp, li, il0, il1, cfg, warm);
+        __syncthreads();
+        if (row && li[li_idx].fallback) {
+            x = f3(0.f, 0.f, 0.f);
+            r = b;
+            u = mul(Mi, b);
+        }
+        if (row) e0[i].u = f4(u);
+    }
+    // ---- w0 = A u0, m0 = M^-1 w0, first (g, d) -----------------------------------
+    if (ok) ok = grid_sync(gb, target, &s_flag);
+    float3 wv = f3(0.f, 0.f, 0.f), m = wv, q = wv, sv = wv, p = wv;
+    if (ok) {
+        double d = 0.0;
+        if (row) {
+            wv = mul(D, u);
+            for (int k = 0; k < w; ++k) wv = wv + mul(offdiag(k), xyz(__ldcg(&e0[scol[k * R + tid]].u)));
+            m = mul(Mi, wv);
+            d = (double)wv.x * u.x + (double)wv.y * u.y + (double)wv.z * u.z;
+            e0[i].m = f4(m);
+            e0[i].q = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        d = warp_sum(d);
+        if (lane == 0 && has) spart[warp * 4] = d;
+        __syncthreads();
+        write_segment_slots<R, 1>(bp, spart, s0, s1, il0, il1);
+        ok = grid_sync(gb, target, &s_flag);
+    }
+    if (ok) {
+        // a0 = g0 / d0, b0 = 0 (L.rho holds g; L.sigma holds alpha in FP64)
+        for (int bq = il0 + warp; bq <= il1; bq += W) {
+            LocalInst& L = li[bq - il0];
+            double tot[1];
+            read_instance_total<1>(bp, bq, tot);
+            if (lane == 0 && !L.done) {
+                const double a = (tot[0] > 1.0e-37 || tot[0] < -1.0e-37) ? L.rho / tot[0] : 0.0;
+                L.sigma = a;
+                L.alpha = (float)a;
+                L.beta = 0.0f;
+                if (!isfinite(a)) L.status = kSolveNonfinite;
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- iterations: one reduction each ------------------------------------
+    const int iter_cap = cfg.max_iter + 2;
+    // single instance only (the host guarantees it): every CTA holds the same
+    // instance state, so the exit decision below is uniform across the grid
+    for (int guard = 0; ok && guard < iter_cap; ++guard) {
+        if (threadIdx.x == 0) s_exit = li[0].done;
+        __syncthreads();
+        if (s_exit) break;
+        double g = 0.0, d = 0.0, r2 = 0.0;
+        if (row && !li[li_idx].done) {
+            const LocalInst& L = li[li_idx];
+            const float alpha = L.alpha, beta = L.beta;
+            const UMQ* E = (L.iter & 1) ? e1 : e0;
+            UMQ* En = (L.iter & 1) ? e0 : e1;
+            q = fma3(beta, q, m);
+            sv = fma3(beta, sv, wv);
+            p = fma3(beta, p, u);
+            x = fma3(alpha, p, x);
+            r = fma3(-alpha, sv, r);
+            u = fma3(-alpha, q, u);  // == what neighbours rebuild below
+            float3 acc = mul(D, u);
+            for (int k = 0; k < w; ++k) {
+                const UMQ* ej = E + scol[k * R + tid];
+                const float3 uj = xyz(__ldcg(&ej->u)), mj = xyz(__ldcg(&ej->m)), qj = xyz(__ldcg(&ej->q));
+                const float3 qn = fma3(beta, qj, mj);
+                acc = acc + mul(offdiag(k), fma3(-alpha, qn, uj));
+            }
+            wv = acc;
+            m = mul(Mi, wv);
+            En[i].u = f4(u);
+            En[i].m = f4(m);
+            En[i].q = f4(q);
+            g = (double)r.x * u.x + (double)r.y * u.y + (double)r.z * u.z;
+            d = (double)wv.x * u.x + (double)wv.y * u.y + (double)wv.z * u.z;
+            r2 = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
+        }
+        g = warp_sum(g);
+        d = warp_sum(d);
+        r2 = warp_sum(r2);
+        if (lane == 0 && has) {
+            spart[warp * 4] = g;
+            spart[warp * 4 + 1] = d;
+            spart[warp * 4 + 2] = r2;
+        }
+        __syncthreads();
+        write_segment_slots<R, 3>(bp, spart, s0, s1, il0, il1);
+        ok = grid_sync(gb, target, &s_flag);
+        if (!ok) break;
+        for (int bq = il0 + warp; bq <= il1; bq += W) {
+            LocalInst& L = li[bq - il0];
+            if (L.done) continue;
+            double tot[3];
+            read_instance_total<3>(bp, bq, tot);
+            if (lane != 0) continue;
+            const double g1 = tot[0], d1 = tot[1], rr1 = tot[2];
+            const double g0 = L.rho, a0 = L.sigma;
+            const double be = (g0 > 1.0e-37 || g0 < -1.0e-37) ? g1 / g0 : 0.0;
+            const double den = d1 - (a0 != 0.0 ? be * g1 / a0 : 0.0);
+            const double al = (den > 1.0e-37 || den < -1.0e-37) ? g1 / den : 0.0;
+            L.rho = g1;
+            L.rr = rr1;
+            L.beta = (float)be;
+            L.alpha = (float)al;
+            L.sigma = al;
+            L.iter += 1;
+            const bool bad = L.status == kSolveNonfinite || !isfinite(g1) || !isfinite(rr1) || !isfinite(al);
+            const bool conv = cfg.use_tol && rr1 <= L.tol2;
+            int done = 0;
+            if (bad) { L.status = kSolveNonfinite; done = 1; }
+            else if (conv) { L.status = kSolveConverged; done = 1; }
+            else if (L.iter >= cfg.max_iter) { L.status = cfg.use_tol ? kSolveMaxIter : kSolveConverged; done = 1; }
+            if (done) {
+                L.done = 1;
+                if ((int)blockIdx.x == bp.inst_cta_lo[bq]) {
+                    InstState& G = bp.inst[bq];
+                    G.rho = L.rho; G.rr = L.rr; G.iter = L.iter; G.status = L.status; G.done = 1;
+                    atomicAdd(&gb->ndone, 1u);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (row) {
+        v.x[i] = f4(x);
+        v.r[i] = f4(r);
+        v.z[i] = f4(u);
+    }
+    if (!ok) instances_fail(bp, li, il0, il1);
+}
+
 // x_{n+1} = x_n + dx, v = dx/dt * exp(-c dt) (cloth_simulator.cu:222-244) for
 // the rows of every instance whose solve finished without NaN/Inf or a
 // kernel error; other instances keep the caller's state.

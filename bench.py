@@ -36,14 +36,19 @@ L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
 
 def workload(name):
+    """Returns (scene, instance offsets or None)."""
     if name == "grid256":
-        return scenes.config_large(max_iter=30000)
+        return scenes.config_large(max_iter=30000), None
     if name == "grid1024":
-        return scenes.config_huge(max_iter=60000)
+        return scenes.config_huge(max_iter=100000), None
     if name == "grid10":
-        return scenes.config_small(max_iter=100)
+        return scenes.config_small(max_iter=100), None
+    if name.startswith("batch"):
+        count = int(name[5:]) if len(name) > 5 else 512
+        sc, offs = scenes.concat(scenes.batch_instances(count=count, seed=1, max_iter=30000))
+        return sc, offs
     if name.startswith("grid"):
-        return scenes.config_large(side=int(name[4:]), max_iter=30000)
+        return scenes.config_large(side=int(name[4:]), max_iter=30000), None
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -182,6 +187,49 @@ def cpu_step_costs(sc, threads, iters_per_step, budget_s):
     return t_asm, max((t - t_asm) / m, 1e-9), m
 
 
+def time_reference_gpu(sc, iters, steps=3, warmup=2):
+    """Times the compiled reference ClothSimulator (oracle/_ref, built from the
+    reference sources) on the same scene with its PCG fixed at `iters`
+    iterations per step -- the same solver work as our converged steps.  The
+    reference supports one scalar spring / stretch stiffness, so per-element
+    stiffness arrays are replaced by their geometric mean (timing only).
+    Returns steps/s or None when the module is absent."""
+    import glob
+
+    import torch
+
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    if not glob.glob(os.path.join(ref_dir, "_chysx_ref_springs*.so")):
+        return None
+    sys.path.insert(0, ref_dir)
+    import _chysx_ref_springs as R
+
+    n = sc["pos"].shape[0]
+    pos = torch.from_numpy(np.ascontiguousarray(sc["pos"], np.float32)).cuda()
+    vel = torch.zeros_like(pos)
+    inv = torch.ones(n, dtype=torch.float32, device="cuda")
+    sim = R.ClothSimulator()
+    sim.set_material(sc["density"], 0.0, *sc["gravity"])
+    sim.set_external_buffers(pos.data_ptr(), vel.data_ptr(), n, inv.data_ptr())
+    sim.set_mesh(np.ascontiguousarray(sc["tris"], np.int32))
+    sim.redistribute_mass_area_weighted(sc["density"], inv.data_ptr(), n)
+    gm = lambda k: float(np.exp(np.mean(np.log(np.asarray(k, np.float64)))))
+    sim.build_springs_from_current_positions(gm(sc["k_spring"]))
+    sim.build_fem_stretch_from_current_positions(gm(sc["k_stretch"]))
+    sim.set_pins(sc["pin_idx"].astype(np.int32), sc["pin_targets"].astype(np.float32), float(sc["k_pin"]))
+    sim.set_pcg_iterations(int(iters))
+    for _ in range(warmup):
+        sim.step(sc["dt"])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        sim.step(sc["dt"])
+    e1.record()
+    torch.cuda.synchronize()
+    return steps / (e0.elapsed_time(e1) * 1e-3)
+
+
 def cpu_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -192,7 +240,7 @@ def cpu_threads():
 def run_reference_arm(args, rank):
     if rank != 0:
         return None
-    sc = workload(args.workload)
+    sc, _ = workload(args.workload)
     threads = cpu_threads()
     import oracle.oracle as O
 
@@ -241,10 +289,22 @@ def run_ours(args, rank, world, local_rank):
     from chysx.runner import GpuCloth
 
     torch.cuda.set_device(local_rank)
-    sc = workload(args.workload)
+    sc, offs = workload(args.workload)
     rel_tol = 1e-6
-    g = GpuCloth(sc, max_iter=sc["max_iter"], rel_tol=rel_tol, warm_start=args.warm)
-    g.sim.set_tuning(args.path, args.block, args.grid)
+
+    def make_sim():
+        sim = GpuCloth(sc, max_iter=sc["max_iter"], rel_tol=rel_tol, warm_start="zero", instances=offs)
+        sim.sim.set_tuning(args.path, args.block, args.grid)
+        sim.sim.set_pcg_variant(args.variant)
+        if args.warm == "learned":
+            from chysx import learned
+
+            params, _ = learned.load(args.net)
+            sim.sim.set_network(params)
+        sim.sim.set_solver(sc["max_iter"], rel_tol, args.warm)
+        return sim
+
+    g = make_sim()
     g.sim.enable_timing(True)
     n = sc["pos"].shape[0]
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
@@ -287,8 +347,7 @@ def run_ours(args, rank, world, local_rank):
     total_ms_max = float(t.item())
 
     # end to end through the C ABI with pinned host buffers
-    e2e_sim = GpuCloth(sc, max_iter=sc["max_iter"], rel_tol=rel_tol, warm_start=args.warm)
-    e2e_sim.sim.set_tuning(args.path, args.block, args.grid)
+    e2e_sim = make_sim()
     host_pos = torch.from_numpy(sc["pos"].copy()).pin_memory()
     host_vel = torch.from_numpy(sc["vel"].copy()).pin_memory()
     for _ in range(args.warmup):
@@ -331,16 +390,30 @@ def run_ours(args, rank, world, local_rank):
     value = steps_total / (total_ms_max * 1e-3)
     mean_iters = float(iters.mean())
 
-    # CPU baseline: single-threaded FP32 port, bounded sample
-    t_asm, t_it, m = cpu_step_costs(sc, 1, int(mean_iters), budget_s=args.cpu_budget)
-    cpu_value = 1.0 / (t_asm + mean_iters * t_it)
+    # CPU baseline: single-threaded FP32 port, bounded sample.  A batch is
+    # charged the row-weighted mean of its per-instance iteration counts (the
+    # GPU stops each instance at its own convergence).
+    cpu_iters = mean_iters
+    if offs is not None:
+        it_b = g.sim.instance_stats()[0].astype(np.float64)
+        cpu_iters = float(np.sum(np.diff(offs) * it_b) / np.sum(np.diff(offs)))
+    t_asm, t_it, m = cpu_step_costs(sc, 1, int(cpu_iters), budget_s=args.cpu_budget)
+    cpu_value = 1.0 / (t_asm + cpu_iters * t_it)
+
+    ref_gpu = None
+    if args.reference_gpu and offs is None:
+        try:
+            ref_gpu = time_reference_gpu(sc, int(round(mean_iters)))
+        except Exception as exc:  # reported, never fatal to our own line
+            ref_gpu = f"failed: {exc}"
 
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 dots)", "data": "synthetic",
         "config": {"workload": args.workload, "particles": n, "off_diag_blocks": int(nnz),
-                   "rel_tol": rel_tol, "warm_start": args.warm,
+                   "rel_tol": rel_tol, "warm_start": args.warm, "pcg_variant": args.variant,
+                   "instances": 1 if offs is None else len(offs) - 1,
                    "pcg_kernel": g.sim.solver_info()[0], "pcg_grid": g.sim.solver_info()[1],
                    "pcg_block": g.sim.solver_info()[2], "l2": "flushed between steps (256 MiB write)"},
         "pcg_iters_per_step": mean_iters,
@@ -349,6 +422,7 @@ def run_ours(args, rank, world, local_rank):
         "us_per_pcg_iteration": float(np.sum(solve_ms) * 1e3 / np.sum(iters)),
         "assembly_ms": float(np.mean(asm_ms)),
         "roofline": {"bound": "hbm", "kernel": {"resident": "pcg_resident_kernel",
+                                                "resident-1r": "pcg_resident_cg1_kernel",
                                                 "streamed": "pcg_persistent_kernel",
                                                 "loop": "pcg_spmv_kernel+pcg_update_kernel"}[g.sim.solver_info()[0]],
                      "achieved": achieved,
@@ -359,10 +433,14 @@ def run_ours(args, rank, world, local_rank):
                      "achieved_reference_format": achieved_ref},
         "cpu_baseline": {"value": cpu_value, "unit": "steps/s", "cores": 1, "kind": "port",
                          "sample": (f"1 step of {args.workload}: assembly + {m} PCG iterations on the "
-                                    f"single-threaded FP32 CPU port, scaled to {mean_iters:.0f} "
+                                    f"single-threaded FP32 CPU port, scaled to {cpu_iters:.0f} "
                                     f"iterations/step")},
         "e2e": {"value": e2e_steps * world / (e2e_ms_max * 1e-3), "unit": "steps/s",
                 "h2d_bytes_per_step": 2 * 12 * n, "d2h_bytes_per_step": 2 * 12 * n},
+        "reference_gpu": None if ref_gpu is None else {
+            "value": ref_gpu, "unit": "steps/s", "pcg_iterations_fixed": int(round(mean_iters)),
+            "note": "compiled reference ClothSimulator (springs enabled), same scene with geometric-mean "
+                    "stiffness, PCG fixed at our mean iterations/step, stream 0"},
         "gpu_launches": 4 * args.steps,
         "clocks": clk,
         "wall_s": wall,
@@ -385,7 +463,10 @@ def main():
                     help="0 persistent PCG (resident when it fits), 1 graph loop, 2 streamed persistent")
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--grid", type=int, default=0)
+    ap.add_argument("--variant", type=int, default=0, help="0 PCG, 1 single-reduction PCG (resident kernel)")
+    ap.add_argument("--net", default=os.path.join(ROOT, "ai-phyiscs_b200", "chysx", "data", "warmstart.npz"))
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--reference-gpu", type=int, default=1, help="also time the compiled reference module")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

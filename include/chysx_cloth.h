@@ -216,8 +216,15 @@ int chysx_cloth_instance_stats(chysx_cloth* h, int n, int* iterations, double* r
  * block (0, 128, 256, 512) and grid (0 = automatic) size the streamed
  * persistent kernel. */
 int chysx_cloth_set_tuning(chysx_cloth* h, int solver_path, int block, int grid);
+/* PCG recurrence (no counterpart in the reference): 0 = the reference's PCG
+ * (two reductions per iteration, src/solver/pcg_solver.cu:467-593; default),
+ * 1 = single-reduction PCG (Chronopoulos-Gear: same iterates in exact
+ * arithmetic, one grid barrier per iteration), used by the register-resident
+ * kernel for a single instance. */
+int chysx_cloth_set_pcg_variant(chysx_cloth* h, int variant);
 /* Kernel used at the last graph build: path 0 register-resident persistent,
- * 1 graph loop, 2 streamed persistent; with its grid and block size. */
+ * 1 graph loop, 2 streamed persistent, 3 register-resident single-reduction;
+ * with its grid and block size. */
 int chysx_cloth_solver_info(const chysx_cloth* h, int* path, int* grid, int* block);
 
 /* Measurement hooks (no counterpart in the reference): when enabled, the

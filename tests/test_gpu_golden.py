@@ -7,7 +7,7 @@ import pytest
 
 from chysx import capi
 from chysx.runner import GpuCloth
-from golden_util import (DUMPS, TOL_BLOCK_REL, TOL_DX_CONVERGED, TOL_RHS_ABS, TOL_TRAJ, load, rel,
+from golden_util import (DUMPS, TOL_BLOCK_REL, TOL_DX_CONVERGED, TOL_RHS_ABS, TOL_TRAJ_FP32, load, rel,
                          scene_for)
 
 pytestmark = pytest.mark.gpu
@@ -52,7 +52,7 @@ def test_cuda_trajectory_matches_reference(fixture, pre, steps):
     sc = scene_for(fixture)
     g = gpu_from(sc, fx, pre, True, tol=1e-8)
     g.run(steps, record_iters=False)
-    assert np.abs(g.positions() - fx[pre + "final_pos"]).max() < TOL_TRAJ
+    assert np.abs(g.positions() - fx[pre + "final_pos"]).max() < TOL_TRAJ_FP32
 
 
 def test_cuda_reference_semantics_fixed_iterations():
