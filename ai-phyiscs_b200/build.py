@@ -26,8 +26,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 LIB = os.path.join(PKG, "libchysx_cloth.so")
 CU_SOURCES = [os.path.join(CSRC, f) for f in ("cloth_sim.cu", "topology.cpp")]
-CU_DEPS = CU_SOURCES + [os.path.join(CSRC, f) for f in ("cloth_kernels.cuh", "topology.h")] + [
-    os.path.join(INCLUDE, "chysx_cloth.h")]
+CU_DEPS = CU_SOURCES + [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))
+                        if f.endswith((".cuh", ".h"))] + [os.path.join(INCLUDE, "chysx_cloth.h")]
 
 
 def _ext_suffix() -> str:
