@@ -290,7 +290,9 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     sc, offs = workload(args.workload)
-    rel_tol = 1e-6
+    rel_tol = 0.0 if args.pcg_fixed else 1e-6
+    if args.pcg_fixed:
+        sc["max_iter"] = args.pcg_fixed
 
     def make_sim():
         sim = GpuCloth(sc, max_iter=sc["max_iter"], rel_tol=rel_tol, warm_start="zero", instances=offs)
@@ -347,10 +349,11 @@ def run_ours(args, rank, world, local_rank):
     total_ms_max = float(t.item())
 
     # end to end through the C ABI with pinned host buffers
-    e2e_sim = make_sim()
+    e2e_steps = args.steps if args.legs == "all" else 0
+    e2e_sim = make_sim() if e2e_steps else g
     host_pos = torch.from_numpy(sc["pos"].copy()).pin_memory()
     host_vel = torch.from_numpy(sc["vel"].copy()).pin_memory()
-    for _ in range(args.warmup):
+    for _ in range(args.warmup if e2e_steps else 0):
         e2e_sim.pos.copy_(host_pos, non_blocking=True)
         e2e_sim.vel.copy_(host_vel, non_blocking=True)
         e2e_sim.step()
@@ -359,7 +362,6 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2e_steps = args.steps
     e0.record()
     for _ in range(e2e_steps):
         e2e_sim.pos.copy_(host_pos, non_blocking=True)
@@ -397,11 +399,13 @@ def run_ours(args, rank, world, local_rank):
     if offs is not None:
         it_b = g.sim.instance_stats()[0].astype(np.float64)
         cpu_iters = float(np.sum(np.diff(offs) * it_b) / np.sum(np.diff(offs)))
-    t_asm, t_it, m = cpu_step_costs(sc, 1, int(cpu_iters), budget_s=args.cpu_budget)
-    cpu_value = 1.0 / (t_asm + cpu_iters * t_it)
+    cpu_value = None
+    if args.legs == "all":
+        t_asm, t_it, m = cpu_step_costs(sc, 1, int(cpu_iters), budget_s=args.cpu_budget)
+        cpu_value = 1.0 / (t_asm + cpu_iters * t_it)
 
     ref_gpu = None
-    if args.reference_gpu and offs is None:
+    if args.reference_gpu and offs is None and args.legs == "all":
         try:
             ref_gpu = time_reference_gpu(sc, int(round(mean_iters)))
         except Exception as exc:  # reported, never fatal to our own line
@@ -431,11 +435,11 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic_bytes_per_iteration": b_it,
                      "reference_format_bytes_per_iteration": b_ref,
                      "achieved_reference_format": achieved_ref},
-        "cpu_baseline": {"value": cpu_value, "unit": "steps/s", "cores": 1, "kind": "port",
+        "cpu_baseline": None if cpu_value is None else {"value": cpu_value, "unit": "steps/s", "cores": 1, "kind": "port",
                          "sample": (f"1 step of {args.workload}: assembly + {m} PCG iterations on the "
                                     f"single-threaded FP32 CPU port, scaled to {cpu_iters:.0f} "
                                     f"iterations/step")},
-        "e2e": {"value": e2e_steps * world / (e2e_ms_max * 1e-3), "unit": "steps/s",
+        "e2e": None if not e2e_steps else {"value": e2e_steps * world / (e2e_ms_max * 1e-3), "unit": "steps/s",
                 "h2d_bytes_per_step": 2 * 12 * n, "d2h_bytes_per_step": 2 * 12 * n},
         "reference_gpu": None if ref_gpu is None else {
             "value": ref_gpu, "unit": "steps/s", "pcg_iterations_fixed": int(round(mean_iters)),
@@ -467,6 +471,10 @@ def main():
     ap.add_argument("--net", default=os.path.join(ROOT, "ai-phyiscs_b200", "chysx", "data", "warmstart.npz"))
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--reference-gpu", type=int, default=1, help="also time the compiled reference module")
+    ap.add_argument("--pcg-fixed", type=int, default=0,
+                    help="K > 0: fixed K PCG iterations per step (rel_tol 0), the small profiling case")
+    ap.add_argument("--legs", default="all", choices=["all", "device"],
+                    help="device: only the device-timed leg (no e2e, CPU or reference legs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
