@@ -69,6 +69,7 @@ SIGNATURES = {
     "chysx_mlp_predict": (ctypes.c_int, [u, u, ctypes.c_int, u, u, ctypes.c_uint64, u]),
     "chysx_mlp_train_step": (ctypes.c_int, [u, u, u, u, u, u, ctypes.c_int, ctypes.c_float, ctypes.c_int, u,
                                             ctypes.c_uint64, dp, u]),
+    "chysx_mlp_gradients_noalloc": (ctypes.c_int, [u, u, u, ctypes.c_int, u, dp, u]),
     "chysx_cloth_set_instances": (ctypes.c_int, [H, i32p, ctypes.c_int]),
     "chysx_cloth_num_instances": (ctypes.c_int, [H, ip]),
     "chysx_cloth_instance_stats": (ctypes.c_int, [H, ctypes.c_int, ip, dp, ip]),

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -178,6 +179,78 @@ void mlp_adam(uintptr_t params, uintptr_t grad, uintptr_t m1, uintptr_t m2, floa
         reinterpret_cast<float*>(params), reinterpret_cast<const float*>(grad), reinterpret_cast<float*>(m1),
         reinterpret_cast<float*>(m2), MlpOffsets::w1, MlpOffsets::total, lr, b1, b2, 1e-8f, c1, c2);
     ck(cudaGetLastError(), "mlp_adam_kernel launch");
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of mlp_gradients: its workspace is a fixed static
+// device array of this file (one copy per device, allocated by the driver
+// when the module loads), sized for kNoAllocMaxRows rows.
+// ---------------------------------------------------------------------------
+constexpr int kNoAllocMaxRows = CHYSX_MLP_NOALLOC_MAX_ROWS;
+constexpr size_t align_up_c(size_t v) { return (v + kWsAlign - 1) / kWsAlign * kWsAlign; }
+// loss partials of mlp_train_tile_kernel: one per warp of train_blocks(rows)
+constexpr int kNoAllocPartials = (kNoAllocMaxRows + 16 * kTrainWarps - 1) / (16 * kTrainWarps) * kTrainWarps;
+// the layout of mlp_workspace_bytes(kNoAllocMaxRows)
+constexpr size_t kNoAllocScratchBytes =
+    align_up_c(sizeof(MlpPacked)) + 8 * align_up_c((size_t)kNoAllocMaxRows * 64 * sizeof(__nv_bfloat16)) +
+    align_up_c((size_t)kNoAllocPartials * sizeof(double));
+static_assert(kNoAllocPartials <= 1184 * kTrainWarps, "partials follow train_blocks()");
+
+static __device__ __align__(256) unsigned char g_mlp_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Set-up, once per device and with that device current: the device address
+// of this device's copy of the scratch array.  The lookup may load the
+// module, so the first call on a device belongs before any stream capture.
+unsigned char* noalloc_scratch() {
+    int dev = -1;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        throw std::out_of_range("chysx_mlp_gradients_noalloc: device ordinal beyond 63");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        if (mlp_workspace_bytes(kNoAllocMaxRows) > kNoAllocScratchBytes)
+            throw std::logic_error("chysx_mlp_gradients_noalloc: static scratch smaller than the workspace layout");
+        void* p = nullptr;
+        ck(cudaGetSymbolAddress(&p, g_mlp_noalloc_scratch), "cudaGetSymbolAddress(mlp scratch)");
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    return g_noalloc_ptr[dev];
+}
+
+// mlp_gradients on the static scratch.  Nothing in the scratch must start at
+// zero (every byte read is written earlier in the same call); the loss is
+// summed on the host in the same order as mlp_gradients, from a stack copy of
+// the per-warp partials.  Calls overlapping in time on one device race on the
+// one scratch array.
+void mlp_gradients_noalloc(uintptr_t params, uintptr_t features, uintptr_t targets, int rows, uintptr_t grad,
+                           double* loss, uintptr_t stream_u) {
+    if (rows <= 0) throw std::invalid_argument("chysx_mlp_gradients_noalloc: rows must be positive");
+    if (rows > kNoAllocMaxRows)
+        throw std::invalid_argument("chysx_mlp_gradients_noalloc: rows = " + std::to_string(rows) +
+                                    " exceeds the static scratch limit of " + std::to_string(kNoAllocMaxRows) +
+                                    " rows (CHYSX_MLP_NOALLOC_MAX_ROWS); use chysx_mlp_gradients with a workspace");
+    if (!params || !features || !targets || !grad)
+        throw std::invalid_argument("chysx_mlp_gradients_noalloc: null device pointer");
+    unsigned char* ws = noalloc_scratch();
+    mlp_gradients(params, features, targets, rows, grad, nullptr, 0, reinterpret_cast<uintptr_t>(ws),
+                  kNoAllocScratchBytes, stream_u);
+    if (loss) {
+        auto stream = reinterpret_cast<cudaStream_t>(stream_u);
+        const int n = train_blocks(rows) * kTrainWarps;
+        // mlp_gradients' workspace layout: packed net, 8 row matrices, partials
+        const size_t off = align_up(sizeof(MlpPacked)) + 8 * align_up((size_t)rows * 64 * sizeof(__nv_bfloat16));
+        double part[kNoAllocPartials];
+        ck(cudaMemcpyAsync(part, ws + off, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, stream),
+           "cudaMemcpyAsync(loss)");
+        ck(cudaStreamSynchronize(stream), "cudaStreamSynchronize(loss)");
+        double s = 0.0;
+        for (int i = 0; i < n; ++i) s += part[i];
+        *loss = s / (3.0 * rows);
+    }
 }
 
 class ClothSim {
@@ -1379,6 +1452,10 @@ int chysx_mlp_train_step(uintptr_t params, uintptr_t grad, uintptr_t m1, uintptr
                                   stream);
         chysx_b200::mlp_adam(params, grad, m1, m2, lr, adam_step, stream);
     });
+}
+int chysx_mlp_gradients_noalloc(uintptr_t params, uintptr_t features, uintptr_t targets, int rows,
+                                uintptr_t grad, double* loss, uintptr_t stream) {
+    return guard([&] { chysx_b200::mlp_gradients_noalloc(params, features, targets, rows, grad, loss, stream); });
 }
 int chysx_cloth_set_instances(chysx_cloth* h, const int32_t* offsets, int n_instances) {
     CHYSX_H(h);

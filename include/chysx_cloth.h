@@ -193,6 +193,35 @@ int chysx_mlp_train_step(uintptr_t params, uintptr_t grad, uintptr_t m1, uintptr
                          uintptr_t targets, int rows, float lr, int adam_step, uintptr_t workspace,
                          uint64_t workspace_bytes, double* loss, uintptr_t stream);
 
+/* Largest `rows` accepted by chysx_mlp_gradients_noalloc. */
+#define CHYSX_MLP_NOALLOC_MAX_ROWS 4096
+/* chysx_mlp_gradients without a workspace argument (no counterpart in the
+ * reference, which has no training entry point at all).  Same kernels, same
+ * results; the workspace is a fixed static device array inside this library
+ * (4,243,712 bytes per device, enough for CHYSX_MLP_NOALLOC_MAX_ROWS rows),
+ * so the call allocates no device memory and, on success, no host memory.
+ * It is for callers that cannot allocate: a host program that drives the
+ * training through this C ABI (ctypes, cgo, JNI) without a device allocator
+ * of its own, and a caller that keeps cudaMalloc / cudaFree out of its loop
+ * because they can synchronise the device while the solver runs.
+ *   - rows > CHYSX_MLP_NOALLOC_MAX_ROWS (or rows <= 0, a null pointer, or
+ *     targets = 0) returns CHYSX_ERR_INVALID_ARGUMENT and launches nothing;
+ *     use chysx_mlp_gradients with a caller workspace for larger batches.
+ *   - The first call on each device is its set-up: with that device current
+ *     it looks up the device address of the scratch array (which may load
+ *     the library's device code).  Make that first call before any stream
+ *     capture on the device.
+ *   - Nothing in the scratch has to start at zero: every byte the kernels
+ *     read was written earlier in the same call.  The first 46 entries of
+ *     `grad` (the normalisation slots) are zeroed by the call itself.
+ *   - All calls on one device share the one scratch array: two calls that
+ *     overlap in time (different streams, or host threads without ordering)
+ *     race on it and corrupt each other's results.  Issue them on one stream
+ *     or order them with events.
+ *   - loss != NULL synchronises `stream`, as chysx_mlp_gradients does. */
+int chysx_mlp_gradients_noalloc(uintptr_t params, uintptr_t features, uintptr_t targets, int rows,
+                                uintptr_t grad, double* loss, uintptr_t stream);
+
 /* Batched solve (no counterpart in the reference): the particles of the
  * external buffers form n_instances independent cloths, instance b owning
  * particles [offsets[b], offsets[b+1]) (offsets[0] = 0, offsets[n] = the

@@ -155,6 +155,18 @@ def test_argument_errors_map_like_the_reference():
     c.step(0.01)
 
 
+def test_no_alloc_gradients_reject_sizes_before_any_device_work():
+    # CHYSX_MLP_NOALLOC_MAX_ROWS = 4096; checked before any CUDA call
+    L = capi.lib()
+    for rows in (4097, 1 << 20, 0, -5):
+        assert L.chysx_mlp_gradients_noalloc(16, 16, 16, rows, 16, None, 0) == capi.ERR_INVALID_ARGUMENT
+    assert "4096" in L.chysx_last_error().decode() or "positive" in L.chysx_last_error().decode()
+    assert L.chysx_mlp_gradients_noalloc(16, 16, 16, 4097, 16, None, 0) == capi.ERR_INVALID_ARGUMENT
+    assert "CHYSX_MLP_NOALLOC_MAX_ROWS" in L.chysx_last_error().decode()
+    # the static scratch is the workspace layout at the limit
+    assert L.chysx_mlp_workspace_bytes(4096) == 4243712
+
+
 def test_material_round_trip():
     c = capi.Cloth()
     c.set_material(density=0.3, damping=0.5, gravity=(1.0, 2.0, 3.0))
