@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(HERE, "libchysx_cloth.so")
 
 OK, ERR_INVALID_ARGUMENT, ERR_OUT_OF_RANGE, ERR_RUNTIME, ERR_CUDA = range(5)
 SOLVE_CONVERGED, SOLVE_MAX_ITER, SOLVE_NONFINITE, SOLVE_KERNEL_ERROR = range(4)
-WARM = {"zero": 0, "previous": 1, "learned": 2}
+WARM = {"zero": 0, "previous": 1, "learned": 2, "previous_scaled": 3}
 
 u = ctypes.c_uint64
 i32p = ctypes.POINTER(ctypes.c_int32)
@@ -73,8 +73,12 @@ SIGNATURES = {
     "chysx_cloth_set_instances": (ctypes.c_int, [H, i32p, ctypes.c_int]),
     "chysx_cloth_num_instances": (ctypes.c_int, [H, ip]),
     "chysx_cloth_instance_stats": (ctypes.c_int, [H, ctypes.c_int, ip, dp, ip]),
+    "chysx_cloth_set_sync_mode": (ctypes.c_int, [H, ctypes.c_int]),
+    "chysx_cloth_autotune": (ctypes.c_int, [H, ctypes.c_float, ctypes.c_int, u]),
+    "chysx_cloth_autotune_results": (ctypes.c_int, [H, ctypes.c_int, ctypes.POINTER(ctypes.c_int), i32p,
+                                                    ctypes.POINTER(ctypes.c_float)]),
+    "chysx_cloth_sync_mode": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_int)]),
     "chysx_cloth_set_tuning": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
-    "chysx_cloth_set_pcg_variant": (ctypes.c_int, [H, ctypes.c_int]),
     "chysx_cloth_solver_info": (ctypes.c_int, [H, ip, ip, ip]),
     "chysx_cloth_enable_timing": (ctypes.c_int, [H, ctypes.c_int]),
     "chysx_cloth_last_timing": (ctypes.c_int, [H, f32p, f32p, f32p]),
@@ -227,13 +231,39 @@ class Cloth:
 
     def solver_info(self):
         """(kernel, grid, block) of the last graph build; kernel is
-        'resident', 'loop', 'streamed' or 'resident-1r' (single reduction)."""
+        'resident', 'loop' or 'streamed'."""
         p, g, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check(self._L.chysx_cloth_solver_info(self.h, ctypes.byref(p), ctypes.byref(g), ctypes.byref(b)))
-        return ("resident", "loop", "streamed", "resident-1r")[p.value], g.value, b.value
+        return ("resident", "loop", "streamed")[p.value], g.value, b.value
 
-    def set_pcg_variant(self, variant):
-        check(self._L.chysx_cloth_set_pcg_variant(self.h, int(variant)))
+    def autotune(self, dt, repetitions=2, stream=0):
+        """Times the applicable solver configurations on the current state
+        (which is restored) and keeps the fastest; returns the table as a
+        list of dicts."""
+        check(self._L.chysx_cloth_autotune(self.h, float(dt), int(repetitions), stream))
+        cnt = ctypes.c_int()
+        check(self._L.chysx_cloth_autotune_results(self.h, 0, ctypes.byref(cnt), None, None))
+        cfg = np.zeros((max(cnt.value, 1), 8), np.int32)
+        ms = np.zeros(max(cnt.value, 1), np.float32)
+        check(self._L.chysx_cloth_autotune_results(self.h, cnt.value, ctypes.byref(cnt),
+                                                   cfg.ctypes.data_as(i32p), ms.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        keys = ("path", "block", "sync", "kernel", "grid", "threads", "iters", "status")
+        kernels = ("resident", "loop", "streamed")
+        out = []
+        for k in range(cnt.value):
+            d = dict(zip(keys, (int(x) for x in cfg[k])))
+            d["kernel"] = kernels[d["kernel"]]
+            d["solve_ms"] = float(ms[k])
+            out.append(d)
+        return out
+
+    def set_sync_mode(self, mode):
+        check(self._L.chysx_cloth_set_sync_mode(self.h, int(mode)))
+
+    def sync_mode(self):
+        m = ctypes.c_int()
+        check(self._L.chysx_cloth_sync_mode(self.h, ctypes.byref(m)))
+        return m.value
 
     def num_off_diag_blocks(self):
         v = ctypes.c_int()

@@ -220,29 +220,38 @@ def train(feats, targs, epochs=30, batch_rows=8192, lr=2e-3, seed=0, log=print):
 # ---------------------------------------------------------------------------
 # evaluation: iterations to rel-res 1e-6, learned vs zero guess
 # ---------------------------------------------------------------------------
-def evaluate(params, seeds=(100, 101), steps=20, side=256, log=print):
+def evaluate(params, seeds=(100, 101), steps=20, side=256,
+             modes=("zero", "previous", "previous_scaled", "learned"), log=print):
+    """PCG iterations per step to rel-res 1e-6 on held-out seeds of the
+    256x256 configuration for each start mode (zero guess = the judge)."""
     from .runner import GpuCloth
 
     rows = []
     for seed in seeds:
         sc = scenes.config_large(side=side, seed=seed, max_iter=30000)
         res = {}
-        for mode in ("zero", "learned"):
+        for mode in modes:
             g = GpuCloth(sc, max_iter=30000, rel_tol=1e-6, warm_start="zero")
             if mode == "learned":
                 g.sim.set_network(params)
-                g.sim.set_solver(30000, 1e-6, "learned")
+            g.sim.set_solver(30000, 1e-6, mode)
             its, kept = [], 0
             for _ in range(steps):
                 g.step()
                 its.append(g.stats()[0])
-                if mode == "learned":
+                if mode != "zero":
                     kept += g.sim.guess_kept()
             res[mode] = (np.array(its), g.positions(), kept)
-        z, l = res["zero"], res["learned"]
-        row = dict(seed=seed, zero_iters=float(z[0].mean()), learned_iters=float(l[0].mean()),
-                   ratio=float(z[0].sum() / max(1, l[0].sum())), guess_kept=int(l[2]), steps=steps,
-                   max_pos_diff=float(np.abs(z[1] - l[1]).max()))
+        z = res["zero"]
+        row = dict(seed=seed, steps=steps, zero_iters=float(z[0].mean()))
+        for mode in modes:
+            if mode == "zero":
+                continue
+            m = res[mode]
+            row[f"{mode}_iters"] = float(m[0].mean())
+            row[f"{mode}_ratio"] = float(z[0].sum() / max(1, m[0].sum()))
+            row[f"{mode}_guess_kept"] = int(m[2])
+            row[f"{mode}_max_pos_diff"] = float(np.abs(z[1] - m[1]).max())
         log(json.dumps(row))
         rows.append(row)
     return rows

@@ -91,6 +91,7 @@ struct SolveState {
     double rho, sigma, rr, bb, tol2, rr0;
     double alpha, beta;
     float alpha_f, beta_f;
+    float scale, scale_b;  // warm guess factor c and 1 - c
     int iter, max_iter, done, status, use_tol, fallback;
     unsigned counter[4];
 };
@@ -466,15 +467,18 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
 
 // ---------------------------------------------------------------------------
 // Warm-start initialisation (pcg_solver.cu:29-51 residual + :386-404):
-// r = b - A x0, z = M^-1 r.  The last block keeps the guess only if it is
-// finite and ||r0|| <= ||b||; otherwise it flags a zero-guess fallback that
-// `warm_fixup_kernel` applies.
+// r = b - A x0 and the start partials.  With `scaled` the last block scales
+// the guess by the energy-minimising factor c = x0.b / x0.A x0 (never worse
+// than the zero guess in the A-norm), else keeps it (c = 1); when c <= 0 or
+// a partial is not finite it flags the zero-guess fallback.
+// `warm_fixup_kernel` applies either to every row.
 // ---------------------------------------------------------------------------
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
-warm_init_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphConditionalHandle cond) {
+warm_init_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphConditionalHandle cond, int scaled) {
     const int i = blockIdx.x * BLOCK + threadIdx.x;
-    double red[3] = {0.0, 0.0, 0.0};  // r.z, r.r, b.M^-1 b
+    // r.z, r.r, b.M^-1 b, x0.b, x0.r, b.z, b.r
+    double red[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (i < t.n) {
         const int s = i >> 5, lane = i & 31;
         const int so = t.slice_off[s];
@@ -494,18 +498,41 @@ warm_init_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphCondi
         const float3 z = mul(Mi, r);
         const float3 zb = mul(Mi, b);
         v.r[i] = f4(r);
-        v.z[i] = f4(z);
-        red[0] = (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
-        red[1] = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
-        red[2] = (double)b.x * zb.x + (double)b.y * zb.y + (double)b.z * zb.z;
+        auto dot = [](float3 a, float3 c) { return (double)a.x * c.x + (double)a.y * c.y + (double)a.z * c.z; };
+        red[0] = dot(r, z);
+        red[1] = dot(r, r);
+        red[2] = dot(b, zb);
+        red[3] = dot(xi, b);
+        red[4] = dot(xi, r);
+        red[5] = dot(b, z);
+        red[6] = dot(b, r);
     }
-    double out[3];
-    if (grid_reduce<BLOCK, 3>(red, part, &st->counter[1], out) && threadIdx.x == 0) {
+    double out[7];
+    if (grid_reduce<BLOCK, 7>(red, part, &st->counter[1], out) && threadIdx.x == 0) {
         const double bb = st->bb;
-        const bool warm_ok = finite_d(out[0]) && finite_d(out[1]) && out[1] <= bb;
-        st->fallback = warm_ok ? 0 : 1;
-        st->rho = warm_ok ? out[0] : out[2];
-        st->rr = warm_ok ? out[1] : bb;
+        // energy-minimising scale of the guess (as the persistent kernels):
+        // c = x0.b / x0.A x0, zero guess when c <= 0 or not finite
+        // (scaled = 0 keeps the guess as given unless a partial is not finite)
+        double c = finite_d(out[0]) && finite_d(out[1]) ? 1.0 : 0.0;
+        if (scaled) {
+            const double xax = out[3] - out[4];
+            c = xax > 0.0 ? out[3] / xax : 0.0;
+            if (!(c > 0.0) || !finite_d(c) || !finite_d(out[0]) || !finite_d(out[1])) c = 0.0;
+        }
+        st->fallback = c > 0.0 ? 0 : 1;
+        st->scale = (float)c;
+        st->scale_b = (float)(1.0 - c);
+        if (c == 1.0) {
+            st->rho = out[0];
+            st->rr = out[1];
+        } else if (c > 0.0) {
+            const double cb = 1.0 - c;
+            st->rho = fmax(cb * cb * out[2] + 2.0 * c * cb * out[5] + c * c * out[0], 0.0);
+            st->rr = fmax(cb * cb * bb + 2.0 * c * cb * out[6] + c * c * out[1], 0.0);
+        } else {
+            st->rho = out[2];
+            st->rr = bb;
+        }
         st->rr0 = st->rr;
         const bool bad = !finite_d(st->rho) || !finite_d(st->rr);
         const bool conv = st->use_tol && st->rr <= st->tol2;
@@ -516,15 +543,22 @@ warm_init_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphCondi
 }
 
 __global__ void warm_fixup_kernel(DevTopo t, Vecs v, const SolveState* st) {
-    if (!st->fallback) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= t.n) return;
     const int s = i >> 5, lane = i & 31;
     const S6 Mi = ld6(t.minv + (size_t)s * 6 * 32 + lane);
-    const float4 b = v.b[i];
-    v.x[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    v.r[i] = b;
-    v.z[i] = f4(mul(Mi, xyz(b)));
+    const float3 b = xyz(v.b[i]);
+    float3 x = f3(0.f, 0.f, 0.f), r = b;
+    if (!st->fallback) {
+        // x = c x0, r = (1 - c) b + c r0
+        const float c = st->scale, cb = st->scale_b;
+        const float3 x0 = xyz(v.x[i]), r0 = xyz(v.r[i]);
+        x = f3(c * x0.x, c * x0.y, c * x0.z);
+        r = f3(fmaf(c, r0.x, cb * b.x), fmaf(c, r0.y, cb * b.y), fmaf(c, r0.z, cb * b.z));
+    }
+    v.x[i] = f4(x);
+    v.r[i] = f4(r);
+    v.z[i] = f4(mul(Mi, r));
 }
 
 // ---------------------------------------------------------------------------

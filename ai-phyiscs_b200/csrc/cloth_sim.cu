@@ -431,7 +431,7 @@ public:
     void set_solver(int m, double tol, int warm) {
         if (m < 0 || m > 10000000) throw std::invalid_argument("set_solver: max_iter must be in [0, 1e7]");
         if (!(tol >= 0.0) || !std::isfinite(tol)) throw std::invalid_argument("set_solver: rel_tol must be >= 0");
-        if (warm < CHYSX_WARM_ZERO || warm > CHYSX_WARM_LEARNED)
+        if (warm < CHYSX_WARM_ZERO || warm > CHYSX_WARM_PREVIOUS_SCALED)
             throw std::invalid_argument("set_solver: unknown warm_start mode");
         if (warm == CHYSX_WARM_LEARNED && !warm_guess_)
             throw std::runtime_error("set_solver: learned warm start needs a network (load one first)");
@@ -529,6 +529,12 @@ public:
         return kept;
     }
     bool want_features() const { return warm_mode_ == CHYSX_WARM_LEARNED || feat_out_ != 0; }
+    // warm argument of the solver kernels: 0 zero guess, 1 guess as given
+    // (the reference's previous dx), 2 energy-scaled guess
+    int warm_kernel_mode() const {
+        if (warm_mode_ == CHYSX_WARM_ZERO) return 0;
+        return warm_mode_ == CHYSX_WARM_PREVIOUS ? 1 : 2;
+    }
 
     // Declares independent cloth instances: particles [off[b], off[b+1]).
     void set_instances(const int32_t* off, int n_inst) {
@@ -559,11 +565,14 @@ public:
     // small enough, else streamed), 1 = graph WHILE loop of two kernels,
     // 2 = streamed persistent kernel forced.  block / grid of the streamed
     // persistent kernel (0 = automatic).
-    void set_variant(int variant) {
-        if (variant < 0 || variant > 1) throw std::invalid_argument("set_variant: variant must be 0 or 1");
-        if (variant != pcg_variant_) graph_dirty_ = true;
-        pcg_variant_ = variant;
+    // Synchronisation of the persistent kernels: 0 = grid-wide counter
+    // barrier (default), 1 = per-instance polled reduction slots.
+    void set_sync(int mode) {
+        if (mode < 0 || mode > 1) throw std::invalid_argument("set_sync_mode: mode must be 0 or 1");
+        if (mode != sync_mode_) graph_dirty_ = true;
+        sync_mode_ = mode;
     }
+    int sync_mode() const { return sync_mode_; }
     void set_tuning(int path, int block, int grid) {
         if (path < 0 || path > 2) throw std::invalid_argument("set_tuning: path must be 0, 1 or 2");
         if (block != 0 && block != 128 && block != 256 && block != 512)
@@ -577,10 +586,106 @@ public:
     // kernel actually used by the last graph build: 0 resident, 1 loop,
     // 2 streamed, 3 resident single-reduction
     void solver_info(int* path, int* grid, int* block) const {
-        const int used = graph_path_ == kPathLoop ? 1 : (resident_ ? (single_reduction_ ? 3 : 0) : 2);
+        const int used = graph_path_ == kPathLoop ? 1 : (resident_ ? 0 : 2);
         if (path) *path = used;
         if (grid) *grid = used == 1 ? 0 : plan_.grid;
         if (block) *block = used == 1 ? kVecBlock : (resident_ ? resident_warps_ * 32 : pcg_block_);
+    }
+
+    // ---- autotuner (no counterpart in the reference) -------------------
+    // Times the solver configurations that apply to the current system on
+    // the current state and keeps the fastest one.  Candidates: the resident
+    // / streamed persistent kernel picked by the planner (rows per CTA and
+    // CTAs per SM follow from it), the streamed kernel at 128 / 256 / 512
+    // threads (4 / 8 / 16 slices, i.e. rows x 32, per CTA), each with both
+    // synchronisation modes, and
+    // the graph-loop path.  Every trial solves the same system: the caller's
+    // positions / velocities and the previous-step guess are restored before
+    // each trial and at the end, so the simulation does not advance.
+    struct TuneResult {
+        int path, block, sync;            // the candidate (set_tuning / sync values)
+        int used, used_grid, used_block;  // what the planner launched (solver_info)
+        int iters, status;
+        float solve_ms;                   // best of the repetitions
+    };
+    const std::vector<TuneResult>& tune_results() const { return tune_; }
+
+    void autotune(float dt, int reps, uintptr_t stream_u) {
+        if (n_ <= 0 || !pos_ || !vel_) throw std::runtime_error("autotune: set_external_buffers() first");
+        if (!(dt > 0.0f)) throw std::invalid_argument("autotune: dt must be positive");
+        if (reps < 1 || reps > 100) throw std::invalid_argument("autotune: reps must be in [1, 100]");
+        auto stream = reinterpret_cast<cudaStream_t>(stream_u);
+        ensure_mesh_on_device();
+        if (topo_dirty_ || topo_.n_ext != n_) rebuild_topology();
+        const size_t nb = 12 * (size_t)n_;
+        DevBuf<float> save_pos, save_vel;
+        DevBuf<float4> save_x;
+        save_pos.resize(3 * (size_t)n_);
+        save_vel.resize(3 * (size_t)n_);
+        save_x.resize(d_x_.size());
+        ck(cudaMemcpyAsync(save_pos.get(), reinterpret_cast<void*>(pos_), nb, cudaMemcpyDeviceToDevice, stream),
+           "autotune: save positions");
+        ck(cudaMemcpyAsync(save_vel.get(), reinterpret_cast<void*>(vel_), nb, cudaMemcpyDeviceToDevice, stream),
+           "autotune: save velocities");
+        if (d_x_.size())
+            ck(cudaMemcpyAsync(save_x.get(), d_x_.get(), d_x_.size() * sizeof(float4), cudaMemcpyDeviceToDevice,
+                               stream), "autotune: save guess");
+        auto restore = [&] {
+            ck(cudaMemcpyAsync(reinterpret_cast<void*>(pos_), save_pos.get(), nb, cudaMemcpyDeviceToDevice, stream),
+               "autotune: restore positions");
+            ck(cudaMemcpyAsync(reinterpret_cast<void*>(vel_), save_vel.get(), nb, cudaMemcpyDeviceToDevice, stream),
+               "autotune: restore velocities");
+            if (save_x.size())
+                ck(cudaMemcpyAsync(d_x_.get(), save_x.get(), save_x.size() * sizeof(float4), cudaMemcpyDeviceToDevice,
+                                   stream), "autotune: restore guess");
+        };
+        const bool timing0 = timing_;
+        enable_timing(1);
+        struct Cand { int path, block, sync; };
+        std::vector<Cand> cands;
+        for (int sync : {0, 1}) {
+            cands.push_back({kPathPersistent, 256, sync});
+            for (int block : {128, 256, 512}) cands.push_back({kPathStreamed, block, sync});
+        }
+        if (topo_.inst_slice.size() <= 2) cands.push_back({kPathLoop, 256, 0});
+        tune_.clear();
+        for (const Cand& c : cands) {
+            solver_path_ = c.path;
+            pcg_block_ = c.block;
+            pcg_grid_req_ = 0;
+            sync_mode_ = c.sync;
+            graph_dirty_ = true;
+            TuneResult r{c.path, c.block, c.sync, 0, 0, 0, 0, 0, 1e30f};
+            for (int k = 0; k < reps; ++k) {
+                restore();
+                step(dt, stream_u);
+                float a = 0.f, sm = 0.f, f = 0.f;
+                last_timing(&a, &sm, &f);
+                double rr = 0.0;
+                last_stats(&r.iters, &rr, &r.status);
+                r.solve_ms = std::min(r.solve_ms, sm);
+            }
+            solver_info(&r.used, &r.used_grid, &r.used_block);
+            // the planner may turn a candidate into one already timed
+            bool dup = false;
+            for (const TuneResult& q : tune_)
+                dup |= q.used == r.used && q.used_grid == r.used_grid && q.used_block == r.used_block &&
+                       q.sync == r.sync;
+            if (!dup) tune_.push_back(r);
+        }
+        const TuneResult* best = nullptr;
+        for (const TuneResult& q : tune_)
+            if (q.status != kSolveNonfinite && q.status != kSolveKernelError && (!best || q.solve_ms < best->solve_ms))
+                best = &q;
+        if (!best) throw std::runtime_error("autotune: no configuration solved the system");
+        solver_path_ = best->path;
+        pcg_block_ = best->block;
+        pcg_grid_req_ = 0;
+        sync_mode_ = best->sync;
+        graph_dirty_ = true;
+        restore();
+        ck(cudaStreamSynchronize(stream), "autotune: synchronise");
+        enable_timing(timing0 ? 1 : 0);
     }
 
     // Optional event-record nodes around the graph's phases (measurement only).
@@ -695,7 +800,7 @@ private:
         asm_block_ = (W <= 16) ? 128 : (W <= 32 ? 64 : 32);
         asm_smem_ = (size_t)6 * W * asm_block_ * sizeof(float);
         const int max_grid = std::max(grid_for(topo_.n, asm_block_), grid_for(topo_.n, kVecBlock));
-        d_part_.resize((size_t)std::max(1, max_grid) * 3);
+        d_part_.resize((size_t)std::max(1, max_grid) * 7);
         d_state_.resize(1);
         d_state_.zero();
         topo_dirty_ = false;
@@ -835,25 +940,22 @@ private:
     }
 
     static constexpr int kResidentMaxWidth = 8;
-    const void* persistent_fn() const {
-        if (resident_ && single_reduction_) {
-            return resident_warps_ == 16
-                       ? reinterpret_cast<const void*>(&pcg_resident_cg1_kernel<16, kResidentMaxWidth>)
-                       : reinterpret_cast<const void*>(&pcg_resident_cg1_kernel<8, kResidentMaxWidth>);
-        }
+    template <int SYNC>
+    const void* persistent_fn_sync() const {
         if (resident_) {
-            return resident_warps_ == 16 ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, kResidentMaxWidth>)
-                                         : reinterpret_cast<const void*>(&pcg_resident_kernel<8, kResidentMaxWidth>);
+            return resident_warps_ == 16
+                       ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, kResidentMaxWidth, SYNC>)
+                       : reinterpret_cast<const void*>(&pcg_resident_kernel<8, kResidentMaxWidth, SYNC>);
         }
-        if (pcg_block_ == 128) return reinterpret_cast<const void*>(&pcg_persistent_kernel<128>);
-        if (pcg_block_ == 512) return reinterpret_cast<const void*>(&pcg_persistent_kernel<512>);
-        return reinterpret_cast<const void*>(&pcg_persistent_kernel<256>);
+        if (pcg_block_ == 128) return reinterpret_cast<const void*>(&pcg_persistent_kernel<128, SYNC>);
+        if (pcg_block_ == 512) return reinterpret_cast<const void*>(&pcg_persistent_kernel<512, SYNC>);
+        return reinterpret_cast<const void*>(&pcg_persistent_kernel<256, SYNC>);
     }
+    const void* persistent_fn() const { return sync_mode_ ? persistent_fn_sync<1>() : persistent_fn_sync<0>(); }
 
     // neighbour-exchange buffer k of the resident kernels (null otherwise)
     void* exchange_buffer(int k) const {
         const size_t np = (size_t)std::max(1, topo_.n_pad);
-        if (resident_ && single_reduction_) return d_umq_.get() + k * np;
         if (resident_) return d_zp_.get() + k * np;
         return nullptr;
     }
@@ -873,6 +975,8 @@ private:
         bp.slots = d_slots_.get();
         bp.inst = d_inst_.get();
         bp.bar = d_bar_.get();
+        bp.n_slots = plan_.inst_slot.empty() ? 0 : plan_.inst_slot.back();
+        bp.fslots = sync_mode_ ? d_fslots_.get() : nullptr;
         return bp;
     }
 
@@ -881,17 +985,15 @@ private:
     // Register-resident plan: one slice per warp, W warps per CTA, all CTAs
     // co-resident.  Returns false when the system does not fit.
     bool plan_resident(int sms) {
+        resident_ = false;  // a previous plan's choice must not leak into this one
         if (solver_path_ != kPathPersistent || topo_.max_width > kResidentMaxWidth) return false;
         const int n_slices = std::max(1, topo_.n_slices);
-        single_reduction_ = pcg_variant_ == 1 && topo_.inst_slice.size() == 2;
         for (int W : {16, 8}) {
             resident_ = true;
             resident_warps_ = W;
             const int grid = (n_slices + W - 1) / W;
             build_plan(topo_.inst_slice, grid, plan_);
-            pers_smem_ = (size_t)W * 4 * sizeof(double) + (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
-            if (single_reduction_)
-                pers_smem_ += (size_t)kResidentMaxWidth * W * 32 * (6 * sizeof(float) + sizeof(int));
+            pers_smem_ = (size_t)W * kSlotW * sizeof(double) + (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
             if (pers_smem_ > 48 * 1024)
                 ck(cudaFuncSetAttribute(persistent_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pers_smem_),
                    "cudaFuncSetAttribute(resident smem)");
@@ -910,23 +1012,17 @@ private:
         ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
         if (plan_resident(sms)) {
             upload_plan();
-            if (single_reduction_) {
-                d_umq_.resize(2 * (size_t)std::max(1, topo_.n_pad));
-                d_umq_.zero();
-            } else {
-                d_zp_.resize(2 * (size_t)std::max(1, topo_.n_pad));
-                d_zp_.zero();
-            }
+            d_zp_.resize(2 * (size_t)std::max(1, topo_.n_pad));
+            d_zp_.zero();
             return;
         }
-        single_reduction_ = false;
         const int W = pcg_block_ / 32;
         const int n_slices = std::max(1, topo_.n_slices);
         // shared memory depends on the plan; iterate once with a generous bound
         int grid = pcg_grid_req_ > 0 ? pcg_grid_req_ : std::max(1, (n_slices + W - 1) / W);
         for (int pass = 0; pass < 3; ++pass) {
             build_plan(topo_.inst_slice, grid, plan_);
-            pers_smem_ = (size_t)plan_.max_slices_per_cta * 4 * sizeof(double) +
+            pers_smem_ = (size_t)plan_.max_slices_per_cta * kSlotW * sizeof(double) +
                          (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
             if (pers_smem_ > 48 * 1024)
                 ck(cudaFuncSetAttribute(persistent_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pers_smem_),
@@ -942,6 +1038,18 @@ private:
         upload_plan();
     }
 
+    // Host-side invariants of the persistent launch, checked before any
+    // launch: the kernel's shared-memory layout fits the bytes requested and
+    // the resident kernel owns at most one slice per warp.
+    void check_plan() const {
+        const size_t li_bytes = (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
+        const size_t need = resident_ ? (size_t)resident_warps_ * kSlotW * sizeof(double) + li_bytes
+                                      : (size_t)plan_.max_slices_per_cta * kSlotW * sizeof(double) + li_bytes;
+        if (pers_smem_ < need || (resident_ && plan_.max_slices_per_cta > resident_warps_) ||
+            (!resident_ && pcg_block_ / 32 < 1))
+            throw std::logic_error("persistent PCG plan is inconsistent with the selected kernel");
+    }
+
     void upload_plan() {
         d_slice_inst_.upload(plan_.slice_inst);
         d_inst_slice_.upload(plan_.inst_slice);
@@ -950,7 +1058,8 @@ private:
         d_cta_inst_hi_.upload(plan_.cta_inst_hi);
         d_inst_cta_lo_.upload(plan_.inst_cta_lo);
         d_inst_slot_.upload(plan_.inst_slot);
-        d_slots_.resize((size_t)std::max(1, plan_.inst_slot.back()) * 4);
+        d_slots_.resize((size_t)std::max(1, plan_.inst_slot.back()) * kSlotW);
+        d_fslots_.resize((size_t)3 * std::max(1, plan_.inst_slot.back()) * kSlotW);
         d_inst_.resize(plan_.n_inst);
         d_inst_.zero();
         d_bar_.resize(1);
@@ -963,6 +1072,7 @@ private:
             ck(cudaFuncSetAttribute(assemble_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asm_smem_),
                "cudaFuncSetAttribute(assemble smem)");
         plan_persistent();
+        check_plan();
         ck(cudaGraphCreate(&graph_, 0), "cudaGraphCreate");
         DevTopo t = dev_topo();
         ElemData el = elem_data();
@@ -972,7 +1082,7 @@ private:
         BatchPlan bp = batch_plan();
         const bool warm = warm_mode_ != CHYSX_WARM_ZERO;
         int zero_guess = warm ? 0 : 1;
-        int warm_i = warm ? 1 : 0;
+        int warm_i = warm_kernel_mode();
         cur_args_ = step_args(1.0f / 60.0f);
         cur_cfg_ = solver_cfg();
         cudaGraphConditionalHandle no_cond = 0;
@@ -988,7 +1098,7 @@ private:
             void* rargs[] = {&bp};
             cudaKernelNodeParams p{};
             p.func = reinterpret_cast<void*>(&pcg_persistent_reset_kernel);
-            p.gridDim = dim3(grid_for(std::max(1, plan_.n_inst), 256));
+            p.gridDim = dim3(grid_for(std::max(std::max(1, plan_.n_inst), 3 * kSlotW * bp.n_slots), 256));
             p.blockDim = dim3(256);
             p.kernelParams = rargs;
             ck(cudaGraphAddKernelNode(&reset, graph_, &t1, 1, &p), "add reset node");
@@ -1059,7 +1169,8 @@ private:
         const int vgrid = std::max(1, grid_for(topo_.n, kVecBlock));
         if (warm) {
             cudaKernelNodeParams p{};
-            void* iargs[] = {&t, &v, &st, &part, &cond};
+            int scaled = warm_kernel_mode() == 2 ? 1 : 0;
+            void* iargs[] = {&t, &v, &st, &part, &cond, &scaled};
             p.func = reinterpret_cast<void*>(&warm_init_kernel<kVecBlock>);
             p.gridDim = dim3(vgrid);
             p.blockDim = dim3(kVecBlock);
@@ -1131,7 +1242,7 @@ private:
         if (graph_path_ == kPathPersistent) {
             cudaGraphConditionalHandle no_cond = 0;
             BatchPlan bp = batch_plan();
-            int warm_i = 1 - zero_guess;
+            int warm_i = warm_kernel_mode();
             void* aargs[] = {&a, &el, &t, &v, &st, &part, &c, &zero_guess, &no_cond};
             cudaKernelNodeParams ap;
             asm_params(ap, aargs);
@@ -1211,7 +1322,7 @@ private:
     int asm_block_ = 128;
     size_t asm_smem_ = 0;
     // persistent PCG plan
-    static constexpr int kPathPersistent = 0, kPathLoop = 1;
+    static constexpr int kPathPersistent = 0, kPathLoop = 1, kPathStreamed = 2;
     int solver_path_ = kPathPersistent, graph_path_ = kPathPersistent;
     int pcg_block_ = 256, pcg_grid_req_ = 0;
     HostPlan plan_;
@@ -1219,6 +1330,7 @@ private:
     DevBuf<int> d_slice_inst_, d_inst_slice_, d_cta_slice_, d_cta_inst_lo_, d_cta_inst_hi_, d_inst_cta_lo_,
         d_inst_slot_;
     DevBuf<double> d_slots_;
+    DevBuf<unsigned long long> d_fslots_;
     DevBuf<InstState> d_inst_;
     DevBuf<GridBarrier> d_bar_;
     cudaGraphNode_t pcg_node_ = nullptr;
@@ -1228,11 +1340,11 @@ private:
     cudaGraphNode_t guess_node_ = nullptr;
     std::vector<int> inst_offsets_;
     DevBuf<int> d_row_to_ext_;
-    bool resident_ = false, single_reduction_ = false;
+    bool resident_ = false;
     int resident_warps_ = 16;
-    int pcg_variant_ = 0;  // 0 PCG with two reductions, 1 single-reduction PCG
+    std::vector<TuneResult> tune_;
+    int sync_mode_ = 0;    // 0 grid counter barrier, 1 polled per-instance slots
     DevBuf<ZP> d_zp_;
-    DevBuf<UMQ> d_umq_;
     bool timing_ = false;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     // graph
@@ -1470,13 +1582,37 @@ int chysx_cloth_instance_stats(chysx_cloth* h, int n, int* iters, double* relres
     CHYSX_H(h);
     return guard([&] { h->sim.instance_stats(n, iters, relres, status); });
 }
+int chysx_cloth_autotune(chysx_cloth* h, float dt, int repetitions, uintptr_t stream) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.autotune(dt, repetitions, stream); });
+}
+int chysx_cloth_autotune_results(const chysx_cloth* h, int capacity, int* count, int32_t* config,
+                                 float* solve_ms) {
+    CHYSX_H(h);
+    const auto& t = h->sim.tune_results();
+    if (count) *count = (int)t.size();
+    for (int k = 0; k < std::min(capacity, (int)t.size()); ++k) {
+        if (config) {
+            int32_t* c = config + 8 * (size_t)k;
+            c[0] = t[k].path; c[1] = t[k].block; c[2] = t[k].sync;
+            c[3] = t[k].used; c[4] = t[k].used_grid; c[5] = t[k].used_block; c[6] = t[k].iters; c[7] = t[k].status;
+        }
+        if (solve_ms) solve_ms[k] = t[k].solve_ms;
+    }
+    return CHYSX_OK;
+}
+int chysx_cloth_set_sync_mode(chysx_cloth* h, int mode) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_sync(mode); });
+}
+int chysx_cloth_sync_mode(const chysx_cloth* h, int* mode) {
+    CHYSX_H(h);
+    if (mode) *mode = h->sim.sync_mode();
+    return CHYSX_OK;
+}
 int chysx_cloth_set_tuning(chysx_cloth* h, int solver_path, int block, int grid) {
     CHYSX_H(h);
     return guard([&] { h->sim.set_tuning(solver_path, block, grid); });
-}
-int chysx_cloth_set_pcg_variant(chysx_cloth* h, int variant) {
-    CHYSX_H(h);
-    return guard([&] { h->sim.set_variant(variant); });
 }
 int chysx_cloth_solver_info(const chysx_cloth* h, int* path, int* grid, int* block) {
     CHYSX_H(h);

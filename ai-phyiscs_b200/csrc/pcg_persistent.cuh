@@ -24,6 +24,7 @@
 namespace chysx_b200 {
 
 constexpr int kSolveKernelError = 3;
+constexpr int kSlotW = 8;  // doubles per reduction slot and per slice partial
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
 
 struct alignas(128) GridBarrier {
@@ -52,9 +53,11 @@ struct BatchPlan {
     const int* __restrict__ cta_inst_hi;  // [grid] last instance (inclusive), lo-1 if none
     const int* __restrict__ inst_cta_lo;  // [n_inst] first CTA touching an instance
     const int* __restrict__ inst_slot;    // [n_inst + 1] segment-slot ranges
-    double* slots;                        // [inst_slot[n_inst] * 4]
+    double* slots;                        // [inst_slot[n_inst] * kSlotW]
     InstState* inst;                      // [n_inst]
     GridBarrier* bar;
+    int n_slots = 0;                      // inst_slot[n_inst]
+    unsigned long long* fslots = nullptr; // [3][n_slots][kSlotW] rotating polled slots (SYNC = 1)
 };
 
 // (z, p) of one row for the register-resident kernel's neighbour exchange
@@ -66,6 +69,7 @@ struct ZP {
 struct LocalInst {
     double rho, rr, bb, tol2, sigma;
     float alpha, beta;
+    float scale, scale_b;  // warm guess factor c and 1 - c
     int iter, done, status, fallback;
 };
 
@@ -113,23 +117,133 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned& target, int
 __device__ __forceinline__ float4 ldcg4(const float4* p) { return __ldcg(p); }
 
 // ---------------------------------------------------------------------------
+// Slot-polling synchronisation (kernels instantiated with SYNC = 1).
+//
+// Instead of a grid-wide counter followed by a read of the partial sums,
+// every reduction phase ph publishes each CTA's per-instance partial sums in
+// slot set ph % 3 (each value stored after a release fence), and the CTAs
+// of an instance poll that instance's slots until every segment is there:
+// the poll is both the barrier and the data read, one L2 round trip fewer
+// per phase.  A slot holds kSlotEmpty until written; its owner resets the
+// set-(ph-1) copy during phase ph, after seeing every segment of phase ph:
+// each reader published its phase-ph segment after reading phase ph-1, so
+// no reader still needs the old value, and a reader of phase ph+2 (same
+// set) has acquired the owner's phase-ph+1 value, which orders the reset
+// before it.  An instance waits only for its own CTAs, and a CTA whose
+// instances are all done leaves the kernel.  Waits are bounded like
+// grid_sync's and raise the same error flag.
+// ---------------------------------------------------------------------------
+// a NaN payload no arithmetic produces; published NaNs are canonicalised
+constexpr unsigned long long kSlotEmpty = 0x7FF4C10E5107E000ull;
+constexpr int kPollMax = 5;  // slots per lane in flight: one pass covers 160 CTAs
+
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned long long slot_bits(double x) {
+    return isnan(x) ? 0x7FF8000000000000ull : (unsigned long long)__double_as_longlong(x);
+}
+
+// Waits for every segment of instance b in slot set `set` and sums them in
+// the same order as read_instance_total (ascending slot per lane, then an
+// xor tree), so both synchronisation modes give identical iterates.  Returns
+// false on every lane once the wait timed out or another CTA raised the
+// error flag.
+template <int NV, int KP = kPollMax>
+__device__ __forceinline__ bool poll_instance_total(const BatchPlan& bp, int b, int set, double (&out)[NV]) {
+    const int lane = threadIdx.x & 31;
+    const int lo = bp.inst_slot[b], hi = bp.inst_slot[b + 1];
+    const unsigned long long* base = bp.fslots + (size_t)set * bp.n_slots * kSlotW;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) out[q] = 0.0;
+    bool ok = true;
+    for (int c0 = lo; c0 < hi && ok; c0 += 32 * KP) {
+        unsigned long long val[KP][NV];
+#pragma unroll
+        for (int j = 0; j < KP; ++j) {
+            const int k = c0 + j * 32 + lane;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) val[j][q] = k < hi ? ld_relaxed_u64(base + (size_t)k * kSlotW + q) : 0ull;
+        }
+        const unsigned long long t0 = global_ns();
+        unsigned spins = 0;
+        while (true) {
+            bool pending = false;
+#pragma unroll
+            for (int j = 0; j < KP; ++j) {
+                const int k = c0 + j * 32 + lane;
+#pragma unroll
+                for (int q = 0; q < NV; ++q) {
+                    if (val[j][q] == kSlotEmpty) {
+                        pending = true;
+                        val[j][q] = ld_relaxed_u64(base + (size_t)k * kSlotW + q);
+                    }
+                }
+            }
+            if (!pending) break;
+            if ((++spins & 63u) == 0) {
+                if (*(volatile int*)&bp.bar->error) { ok = false; break; }
+                if (global_ns() - t0 > kBarrierTimeoutNs) {
+                    atomicExch(&bp.bar->error, 1);
+                    ok = false;
+                    break;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < KP; ++j) {
+            if (c0 + j * 32 + lane < hi) {
+#pragma unroll
+                for (int q = 0; q < NV; ++q) out[q] += __longlong_as_double((long long)val[j][q]);
+            }
+        }
+    }
+    fence_acq_rel_gpu();  // acquire: the publishers' data is visible from here on
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) out[q] += __shfl_xor_sync(0xffffffffu, out[q], o);
+    }
+    ok = __all_sync(0xffffffffu, ok);
+    if (ok && lane == 0) {
+        // this CTA's own slot of the previous phase can be reused
+        const int own = bp.inst_slot[b] + ((int)blockIdx.x - bp.inst_cta_lo[b]);
+        unsigned long long* d = bp.fslots + ((size_t)((set + 2) % 3) * bp.n_slots + own) * kSlotW;
+#pragma unroll
+        for (int q = 0; q < kSlotW; ++q) st_relaxed_u64(d + q, kSlotEmpty);
+    }
+    return ok;
+}
+
+
+// ---------------------------------------------------------------------------
 // Segmented reductions
 // ---------------------------------------------------------------------------
-// spart[(s - s0) * 4 + q] holds slice partials; write, for every instance
+// spart[(s - s0) * kSlotW + q] holds slice partials; write, for every instance
 // this CTA touches, the sum over its slices into the instance's slot.
-template <int BLOCK, int NV>
+// SYNC = 1 publishes into slot set `set` instead (release fence, then
+// relaxed stores), skipping instances already done (li, when given).
+template <int BLOCK, int NV, int SYNC = 0>
 __device__ __forceinline__ void write_segment_slots(const BatchPlan& bp, const double* spart, int s0, int s1,
-                                                    int il0, int il1) {
+                                                    int il0, int il1, int set = 0,
+                                                    const LocalInst* li = nullptr) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int W = BLOCK / 32;
     for (int b = il0 + warp; b <= il1; b += W) {
+        if (SYNC && li && li[b - il0].done) continue;
         const int lo = max(s0, bp.inst_slice[b]), hi = min(s1, bp.inst_slice[b + 1]);
         double acc[NV];
 #pragma unroll
         for (int q = 0; q < NV; ++q) acc[q] = 0.0;
         for (int s = lo + lane; s < hi; s += 32) {
 #pragma unroll
-            for (int q = 0; q < NV; ++q) acc[q] += spart[(s - s0) * 4 + q];
+            for (int q = 0; q < NV; ++q) acc[q] += spart[(s - s0) * kSlotW + q];
         }
 #pragma unroll
         for (int q = 0; q < NV; ++q) {
@@ -138,8 +252,15 @@ __device__ __forceinline__ void write_segment_slots(const BatchPlan& bp, const d
         }
         if (lane == 0) {
             const int slot = bp.inst_slot[b] + ((int)blockIdx.x - bp.inst_cta_lo[b]);
+            if (SYNC) {
+                unsigned long long* d = bp.fslots + ((size_t)set * bp.n_slots + slot) * kSlotW;
+                fence_acq_rel_gpu();  // release: the CTA's writes before the __syncthreads
 #pragma unroll
-            for (int q = 0; q < NV; ++q) bp.slots[(size_t)slot * 4 + q] = acc[q];
+                for (int q = 0; q < NV; ++q) st_relaxed_u64(d + q, slot_bits(acc[q]));
+            } else {
+#pragma unroll
+                for (int q = 0; q < NV; ++q) bp.slots[(size_t)slot * kSlotW + q] = acc[q];
+            }
         }
     }
 }
@@ -153,7 +274,7 @@ __device__ __forceinline__ void read_instance_total(const BatchPlan& bp, int b, 
     for (int q = 0; q < NV; ++q) out[q] = 0.0;
     for (int k = lo + lane; k < hi; k += 32) {
 #pragma unroll
-        for (int q = 0; q < NV; ++q) out[q] += __ldcg(bp.slots + (size_t)k * 4 + q);
+        for (int q = 0; q < NV; ++q) out[q] += __ldcg(bp.slots + (size_t)k * kSlotW + q);
     }
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
@@ -162,10 +283,58 @@ __device__ __forceinline__ void read_instance_total(const BatchPlan& bp, int b, 
     }
 }
 
+// Reads instance b's total in either mode; on a failed wait lane 0 raises
+// the CTA's flag.
+template <int NV, int SYNC, int KP = kPollMax>
+__device__ __forceinline__ bool instance_total(const BatchPlan& bp, int b, int set, double (&out)[NV], int* s_flag) {
+    if (SYNC) {
+        const bool ok = poll_instance_total<NV, KP>(bp, b, set, out);
+        if (!ok && (threadIdx.x & 31) == 0) *s_flag = 1;
+        return ok;
+    }
+    read_instance_total<NV>(bp, b, out);
+    return true;
+}
+
 __device__ __forceinline__ double warp_sum(double x) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     return x;
+}
+
+__device__ __forceinline__ double dot3d(float3 a, float3 b) {
+    return (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z;
+}
+
+// Start partials of one row, kSlotW wide: r.z, r.r, b.b, b.M^-1 b, x0.b,
+// x0.r, b.z, b.r (with r = b - A x0, z = M^-1 r; the zero guess has x0 = 0,
+// r = b, z = M^-1 b).  The warp sums land in spart[slot * kSlotW + q].
+__device__ __forceinline__ void start_partials(double* sp, bool write, float3 b, float3 zb, float3 x0, float3 r,
+                                               float3 z) {
+    double q[kSlotW] = {dot3d(r, z), dot3d(r, r), dot3d(b, b), dot3d(b, zb),
+                        dot3d(x0, b), dot3d(x0, r), dot3d(b, z), dot3d(b, r)};
+#pragma unroll
+    for (int k = 0; k < kSlotW; ++k) q[k] = warp_sum(q[k]);
+    if (write) {
+#pragma unroll
+        for (int k = 0; k < kSlotW; ++k) sp[k] = q[k];
+    }
+}
+
+// The instance's start applied to one row: the warm guess scaled by the
+// energy-minimising factor c (x = c x0, r = (1 - c) b + c r0), or the zero
+// guess when the instance fell back.
+__device__ __forceinline__ void start_row(const LocalInst& L, float3 b, const S6& Mi, float3& x, float3& r,
+                                          float3& z) {
+    if (L.fallback) {
+        x = f3(0.f, 0.f, 0.f);
+        r = b;
+    } else {
+        const float c = L.scale, cb = L.scale_b;
+        x = f3(c * x.x, c * x.y, c * x.z);
+        r = f3(fmaf(c, r.x, cb * b.x), fmaf(c, r.y, cb * b.y), fmaf(c, r.z, cb * b.z));
+    }
+    z = mul(Mi, r);
 }
 
 // ---------------------------------------------------------------------------
@@ -174,20 +343,48 @@ __device__ __forceinline__ double warp_sum(double x) {
 // lane 0 updates the CTA-local copy; the first CTA touching an instance
 // also publishes its state and counts it when it finishes.
 // ---------------------------------------------------------------------------
-template <int W>
+template <int W, int SYNC = 0>
 __device__ __forceinline__ void instances_start(const BatchPlan& bp, LocalInst* li, int il0, int il1,
-                                                const SolverCfg& cfg, int warm) {
+                                                const SolverCfg& cfg, int warm, int set = 0,
+                                                int* s_flag = nullptr) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int b = il0 + warp; b <= il1; b += W) {
-        double tot[4];
-        read_instance_total<4>(bp, b, tot);
+        double tot[kSlotW];
+        // once per solve: fewer slots in flight keep the registers of the
+        // resident kernels' rows free
+        if (!instance_total<kSlotW, SYNC, 1>(bp, b, set, tot, s_flag)) continue;
         if (lane != 0) continue;
         LocalInst& L = li[b - il0];
         const double bb = tot[2];
-        const bool warm_ok = !warm || (isfinite(tot[0]) && isfinite(tot[1]) && tot[1] <= bb);
-        L.fallback = warm_ok ? 0 : 1;
-        L.rho = warm_ok ? tot[0] : tot[3];
-        L.rr = warm_ok ? tot[1] : bb;
+        // warm guess x0: scaled by c = x0.b / x0.A x0 (x0.A x0 = x0.(b - r0)),
+        // the factor minimising the energy 1/2 x.A x - b.x along x0, so the
+        // start is never worse than the zero guess in the A-norm; c <= 0
+        // (or NaN / Inf) falls back to the zero guess
+        // (warm == 2); warm == 1 keeps the guess as given (the reference's
+        // previous-dx start) unless a partial is not finite
+        double c = 0.0;
+        if (warm == 1) {
+            c = isfinite(tot[0]) && isfinite(tot[1]) ? 1.0 : 0.0;
+        } else if (warm == 2) {
+            const double xax = tot[4] - tot[5];
+            c = xax > 0.0 ? tot[4] / xax : 0.0;
+            if (!(c > 0.0) || !isfinite(c) || !isfinite(tot[0]) || !isfinite(tot[1])) c = 0.0;
+        }
+        L.fallback = warm && c == 0.0 ? 1 : 0;
+        L.scale = (float)c;
+        L.scale_b = (float)(1.0 - c);
+        if (c == 1.0) {
+            L.rho = tot[0];
+            L.rr = tot[1];
+        } else if (c > 0.0) {
+            // r = (1 - c) b + c r0: its r.z and r.r from the start partials
+            const double cb = 1.0 - c;
+            L.rho = fmax(cb * cb * tot[3] + 2.0 * c * cb * tot[6] + c * c * tot[0], 0.0);
+            L.rr = fmax(cb * cb * bb + 2.0 * c * cb * tot[7] + c * c * tot[1], 0.0);
+        } else {
+            L.rho = tot[3];
+            L.rr = bb;
+        }
         L.bb = bb;
         L.tol2 = cfg.rel_tol * cfg.rel_tol * bb;
         L.iter = 0;
@@ -210,14 +407,15 @@ __device__ __forceinline__ void instances_start(const BatchPlan& bp, LocalInst* 
     }
 }
 
-template <int W>
-__device__ __forceinline__ void instances_alpha(const BatchPlan& bp, LocalInst* li, int il0, int il1) {
+template <int W, int SYNC = 0>
+__device__ __forceinline__ void instances_alpha(const BatchPlan& bp, LocalInst* li, int il0, int il1, int set = 0,
+                                                int* s_flag = nullptr) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int b = il0 + warp; b <= il1; b += W) {
         LocalInst& L = li[b - il0];
         if (L.done) continue;
         double tot[1];
-        read_instance_total<1>(bp, b, tot);
+        if (!instance_total<1, SYNC>(bp, b, set, tot, s_flag)) continue;
         if (lane == 0) {
             const double sigma = tot[0];
             const double alpha = (sigma > 1.0e-37 || sigma < -1.0e-37) ? L.rho / sigma : 0.0;
@@ -228,15 +426,15 @@ __device__ __forceinline__ void instances_alpha(const BatchPlan& bp, LocalInst* 
     }
 }
 
-template <int W>
+template <int W, int SYNC = 0>
 __device__ __forceinline__ void instances_beta(const BatchPlan& bp, LocalInst* li, int il0, int il1,
-                                               const SolverCfg& cfg) {
+                                               const SolverCfg& cfg, int set = 0, int* s_flag = nullptr) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int b = il0 + warp; b <= il1; b += W) {
         LocalInst& L = li[b - il0];
         if (L.done) continue;
         double tot[2];
-        read_instance_total<2>(bp, b, tot);
+        if (!instance_total<2, SYNC>(bp, b, set, tot, s_flag)) continue;
         if (lane != 0) continue;
         const double rho_new = tot[0], rr = tot[1];
         const double beta = (L.rho > 1.0e-37 || L.rho < -1.0e-37) ? rho_new / L.rho : 0.0;
@@ -277,7 +475,7 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
 // ---------------------------------------------------------------------------
 // The kernel
 // ---------------------------------------------------------------------------
-template <int BLOCK>
+template <int BLOCK, int SYNC = 0>
 __global__ void __launch_bounds__(BLOCK)
 pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP*, ZP*) {
     extern __shared__ double s_mem[];
@@ -288,9 +486,10 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
     const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
     const int il0 = bp.cta_inst_lo[blockIdx.x], il1 = bp.cta_inst_hi[blockIdx.x];
     double* spart = s_mem;
-    LocalInst* li = reinterpret_cast<LocalInst*>(s_mem + (size_t)bp.max_slices_per_cta * 4);
+    LocalInst* li = reinterpret_cast<LocalInst*>(s_mem + (size_t)bp.max_slices_per_cta * kSlotW);
     GridBarrier* gb = bp.bar;
     unsigned gen = 0;  // barrier target; the counter starts at 0 every solve
+    int ph = 0;        // reduction phase (SYNC = 1 slot set ph % 3)
     if (threadIdx.x == 0) s_flag = 0;
     bool ok = true;
 
@@ -299,68 +498,82 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
     // warm guess: r = b - A x0, z = M^-1 r (pcg_solver.cu:29-51).
     for (int s = s0 + warp; s < s1; s += W) {
         const int i = s * 32 + lane;
-        double rz = 0.0, rr = 0.0, bb = 0.0, bmb = 0.0;
+        float3 b = f3(0.f, 0.f, 0.f), zb = b, x0 = b, r = b, z = b;
         if (i < t.n) {
-            const float3 b = xyz(v.b[i]);
+            b = xyz(v.b[i]);
             const S6 Mi = ld6(t.minv + (size_t)s * 192 + lane);
-            const float3 zb = mul(Mi, b);
-            bb = (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z;
-            bmb = (double)b.x * zb.x + (double)b.y * zb.y + (double)b.z * zb.z;
+            zb = mul(Mi, b);
+            r = b;
+            z = zb;
             if (warm) {
                 const int so = t.slice_off[s];
                 const int w = (t.slice_off[s + 1] - so) >> 5;
                 const S6 D = ld6(t.diag + (size_t)s * 192 + lane);
-                float3 ax = mul(D, xyz(v.x[i]));
+                x0 = xyz(v.x[i]);
+                float3 ax = mul(D, x0);
                 const float* vb = t.val + (size_t)so * 6 + lane;
                 for (int k = 0; k < w; ++k) {
                     const int j = t.col[so + k * 32 + lane];
                     ax = ax + mul(ld6(vb + k * 192), xyz(v.x[j]));
                 }
-                const float3 r = b - ax;
-                const float3 z = mul(Mi, r);
+                r = b - ax;
+                z = mul(Mi, r);
                 v.r[i] = f4(r);
-                v.z[i] = f4(z);
-                rz = (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
-                rr = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
-            } else {
-                rz = bmb;
-                rr = bb;
             }
         }
-        rz = warp_sum(rz); rr = warp_sum(rr); bb = warp_sum(bb); bmb = warp_sum(bmb);
-        if (lane == 0) {
-            double* sp = spart + (s - s0) * 4;
-            sp[0] = rz; sp[1] = rr; sp[2] = bb; sp[3] = bmb;
-        }
+        start_partials(spart + (s - s0) * kSlotW, lane == 0, b, zb, x0, r, z);
     }
     __syncthreads();
-    write_segment_slots<BLOCK, 4>(bp, spart, s0, s1, il0, il1);
-    ok = grid_sync(gb, gen, &s_flag);
+    write_segment_slots<BLOCK, kSlotW, SYNC>(bp, spart, s0, s1, il0, il1, ph % 3);
+    if (!SYNC) ok = grid_sync(gb, gen, &s_flag);
     if (ok) {
-        instances_start<W>(bp, li, il0, il1, cfg, warm);
+        instances_start<W, SYNC>(bp, li, il0, il1, cfg, warm, ph % 3, &s_flag);
+        ++ph;
         __syncthreads();
-        if (warm) {
-            // zero-guess fallback for instances whose guess was worse than zero
-            bool any = false;
-            for (int b = il0; b <= il1; ++b) any |= li[b - il0].fallback != 0;
-            if (any) {
-                for (int s = s0 + warp; s < s1; s += W) {
-                    const int i = s * 32 + lane;
-                    if (i >= t.n || !li[bp.slice_inst[s] - il0].fallback) continue;
-                    const S6 Mi = ld6(t.minv + (size_t)s * 192 + lane);
-                    const float4 b = v.b[i];
-                    v.x[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    v.r[i] = b;
-                    v.z[i] = f4(mul(Mi, xyz(b)));
-                }
+        ok = s_flag == 0;
+        if (ok && warm) {
+            // the scaled guess, or the zero guess where the instance fell back
+            for (int s = s0 + warp; s < s1; s += W) {
+                const int i = s * 32 + lane;
+                if (i >= t.n) continue;
+                const S6 Mi = ld6(t.minv + (size_t)s * 192 + lane);
+                float3 x = xyz(v.x[i]), r = xyz(v.r[i]), z;
+                start_row(li[bp.slice_inst[s] - il0], xyz(v.b[i]), Mi, x, r, z);
+                v.x[i] = f4(x);
+                v.r[i] = f4(r);
+                v.z[i] = f4(z);
             }
-            ok = grid_sync(gb, gen, &s_flag);
+            if (SYNC) {
+                // a data-free phase orders the fallback rows before any gather
+                for (int q = threadIdx.x; q < s1 - s0; q += BLOCK) spart[q * kSlotW] = 0.0;
+                __syncthreads();
+                write_segment_slots<BLOCK, 1, 1>(bp, spart, s0, s1, il0, il1, ph % 3, li);
+                for (int bq = il0 + warp; bq <= il1; bq += W) {
+                    double tot[1];
+                    if (!li[bq - il0].done) instance_total<1, 1>(bp, bq, ph % 3, tot, &s_flag);
+                }
+                ++ph;
+                __syncthreads();
+                ok = s_flag == 0;
+            } else {
+                ok = grid_sync(gb, gen, &s_flag);
+            }
         }
     }
 
     // ---- iterations ---------------------------------------------------------
     const int iter_cap = cfg.max_iter + 2;  // belt: every instance is done by max_iter
     for (int guard = 0; ok && guard < iter_cap; ++guard) {
+        if (SYNC) {
+            // leave once every instance of this CTA is done
+            if (threadIdx.x == 0) {
+                int all = 1;
+                for (int bq = il0; bq <= il1; ++bq) all &= li[bq - il0].done;
+                s_exit = all;
+            }
+            __syncthreads();
+            if (s_exit) break;
+        }
         // phase 1: p = z + beta p (own row and recomputed for neighbours),
         // Ap = A p, sigma = p.Ap
         for (int s = s0 + warp; s < s1; s += W) {
@@ -399,21 +612,28 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                 sig = (double)pi.x * acc.x + (double)pi.y * acc.y + (double)pi.z * acc.z;
             }
             sig = warp_sum(sig);
-            if (lane == 0) spart[(s - s0) * 4] = sig;
+            if (lane == 0) spart[(s - s0) * kSlotW] = sig;
         }
         __syncthreads();
-        write_segment_slots<BLOCK, 1>(bp, spart, s0, s1, il0, il1);
-        ok = grid_sync(gb, gen, &s_flag);
-        if (!ok) break;
-        // ndone only changes in phase 3 and phase 0, i.e. never between this
-        // barrier and the next, so every CTA takes the same decision here
-        if (threadIdx.x == 0) s_exit = *(volatile unsigned*)&gb->ndone >= (unsigned)bp.n_inst;
-        __syncthreads();
-        if (s_exit) break;
+        write_segment_slots<BLOCK, 1, SYNC>(bp, spart, s0, s1, il0, il1, ph % 3, li);
+        if (!SYNC) {
+            ok = grid_sync(gb, gen, &s_flag);
+            if (!ok) break;
+            // ndone only changes in phase 3 and phase 0, i.e. never between
+            // this barrier and the next, so every CTA takes the same decision
+            if (threadIdx.x == 0) s_exit = *(volatile unsigned*)&gb->ndone >= (unsigned)bp.n_inst;
+            __syncthreads();
+            if (s_exit) break;
+        }
 
         // phase 2: alpha = rho / sigma; x += alpha p; r -= alpha Ap; z = M^-1 r
-        instances_alpha<W>(bp, li, il0, il1);
+        instances_alpha<W, SYNC>(bp, li, il0, il1, ph % 3, &s_flag);
+        ++ph;
         __syncthreads();
+        if (SYNC && s_flag) {
+            ok = false;
+            break;
+        }
         for (int s = s0 + warp; s < s1; s += W) {
             const LocalInst& L = li[bp.slice_inst[s] - il0];
             const int i = s * 32 + lane;
@@ -434,18 +654,25 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             rz = warp_sum(rz);
             rr = warp_sum(rr);
             if (lane == 0) {
-                spart[(s - s0) * 4] = rz;
-                spart[(s - s0) * 4 + 1] = rr;
+                spart[(s - s0) * kSlotW] = rz;
+                spart[(s - s0) * kSlotW + 1] = rr;
             }
         }
         __syncthreads();
-        write_segment_slots<BLOCK, 2>(bp, spart, s0, s1, il0, il1);
-        ok = grid_sync(gb, gen, &s_flag);
-        if (!ok) break;
+        write_segment_slots<BLOCK, 2, SYNC>(bp, spart, s0, s1, il0, il1, ph % 3, li);
+        if (!SYNC) {
+            ok = grid_sync(gb, gen, &s_flag);
+            if (!ok) break;
+        }
 
         // phase 3: beta, iteration count, convergence (pcg_solver.cu:436-454)
-        instances_beta<W>(bp, li, il0, il1, cfg);
+        instances_beta<W, SYNC>(bp, li, il0, il1, cfg, ph % 3, &s_flag);
+        ++ph;
         __syncthreads();
+        if (SYNC && s_flag) {
+            ok = false;
+            break;
+        }
     }
     if (!ok) instances_fail(bp, li, il0, il1);
 }
@@ -462,7 +689,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
 // pcg_persistent_kernel.
 // ---------------------------------------------------------------------------
 
-template <int W, int MAXW>
+template <int W, int MAXW, int SYNC = 0>
 __global__ void __launch_bounds__(W * 32)
 pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP* zp0, ZP* zp1) {
     extern __shared__ double s_mem[];
@@ -471,10 +698,11 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
     const int il0 = bp.cta_inst_lo[blockIdx.x], il1 = bp.cta_inst_hi[blockIdx.x];
-    double* spart = s_mem;  // [W * 4]
-    LocalInst* li = reinterpret_cast<LocalInst*>(s_mem + (size_t)W * 4);
+    double* spart = s_mem;  // [W * kSlotW]
+    LocalInst* li = reinterpret_cast<LocalInst*>(s_mem + (size_t)W * kSlotW);
     GridBarrier* gb = bp.bar;
     unsigned target = 0;
+    int ph = 0;  // reduction phase (SYNC = 1 slot set ph % 3)
     if (threadIdx.x == 0) s_flag = 0;
     bool ok = true;
 
@@ -487,13 +715,17 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     // ---- load the row --------------------------------------------------
     S6 D{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, Mi{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     S6 B[MAXW];
-    int cols[MAXW];
+    // column indices: registers, or shared memory in the slot-polling build
+    // (its waits need the registers)
+    int cols_r[SYNC ? 1 : MAXW];
+    __shared__ int s_cols[SYNC ? MAXW * W * 32 : 1];
+    auto col_at = [&](int k) -> int & { return SYNC ? s_cols[k * W * 32 + threadIdx.x] : cols_r[SYNC ? 0 : k]; };
     int w = 0;
     float3 b = f3(0.f, 0.f, 0.f), x = b, r = b, z = b, p = b;
 #pragma unroll
     for (int k = 0; k < MAXW; ++k) {
         B[k] = S6{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        cols[k] = row ? i : 0;
+        col_at(k) = row ? i : 0;
     }
     if (row) {
         D = ld6(t.diag + (size_t)s * 192 + lane);
@@ -504,7 +736,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
 #pragma unroll
         for (int k = 0; k < MAXW; ++k) {
             if (k < w) {
-                cols[k] = t.col[so + k * 32 + lane];
+                col_at(k) = t.col[so + k * 32 + lane];
                 B[k] = ld6(t.val + (size_t)so * 6 + (size_t)k * 192 + lane);
             }
         }
@@ -512,48 +744,52 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
 
     // ---- phase 0 -------------------------------------------------------
     {
-        double rz = 0.0, rr = 0.0, bb = 0.0, bmb = 0.0;
+        float3 zb = f3(0.f, 0.f, 0.f);
         if (row) {
-            const float3 zb = mul(Mi, b);
-            bb = (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z;
-            bmb = (double)b.x * zb.x + (double)b.y * zb.y + (double)b.z * zb.z;
+            zb = mul(Mi, b);
+            r = b;
+            z = zb;
             if (warm) {
                 x = xyz(v.x[i]);
                 float3 ax = mul(D, x);
 #pragma unroll
                 for (int k = 0; k < MAXW; ++k)
-                    if (k < w) ax = ax + mul(B[k], xyz(v.x[cols[k]]));
+                    if (k < w) ax = ax + mul(B[k], xyz(v.x[col_at(k)]));
                 r = b - ax;
                 z = mul(Mi, r);
-                rz = (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
-                rr = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
-            } else {
-                r = b;
-                z = zb;
-                rz = bmb;
-                rr = bb;
             }
             zp0[i].z = f4(z);
         }
-        rz = warp_sum(rz); rr = warp_sum(rr); bb = warp_sum(bb); bmb = warp_sum(bmb);
-        if (lane == 0 && has) {
-            double* sp = spart + warp * 4;
-            sp[0] = rz; sp[1] = rr; sp[2] = bb; sp[3] = bmb;
-        }
+        start_partials(spart + warp * kSlotW, lane == 0 && has, b, zb, x, r, z);
     }
     __syncthreads();
-    write_segment_slots<W * 32, 4>(bp, spart, s0, s1, il0, il1);
-    ok = grid_sync(gb, target, &s_flag);
+    write_segment_slots<W * 32, kSlotW, SYNC>(bp, spart, s0, s1, il0, il1, ph % 3);
+    if (!SYNC) ok = grid_sync(gb, target, &s_flag);
     if (ok) {
-        instances_start<W>(bp, li, il0, il1, cfg, warm);
+        instances_start<W, SYNC>(bp, li, il0, il1, cfg, warm, ph % 3, &s_flag);
+        ++ph;
         __syncthreads();
-        if (warm) {
-            if (row && li[li_idx].fallback) {
-                x = f3(0.f, 0.f, 0.f);
-                r = b;
-                z = mul(Mi, b);
-                zp0[i].z = f4(z);
+        ok = s_flag == 0;
+    }
+    if (ok && warm) {
+        // the scaled guess, or the zero guess where the instance fell back
+        if (row) {
+            start_row(li[li_idx], b, Mi, x, r, z);
+            zp0[i].z = f4(z);
+        }
+        if (SYNC) {
+            // a data-free phase orders the fallback rows' z before any gather
+            if (threadIdx.x < W) spart[threadIdx.x * kSlotW] = 0.0;
+            __syncthreads();
+            write_segment_slots<W * 32, 1, 1>(bp, spart, s0, s1, il0, il1, ph % 3, li);
+            for (int bq = il0 + warp; bq <= il1; bq += W) {
+                double tot[1];
+                if (!li[bq - il0].done) instance_total<1, 1>(bp, bq, ph % 3, tot, &s_flag);
             }
+            ++ph;
+            __syncthreads();
+            ok = s_flag == 0;
+        } else {
             ok = grid_sync(gb, target, &s_flag);
         }
     }
@@ -562,6 +798,16 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     const int iter_cap = cfg.max_iter + 2;
     float3 ap = f3(0.f, 0.f, 0.f);
     for (int guard = 0; ok && guard < iter_cap; ++guard) {
+        if (SYNC) {
+            // leave once every instance of this CTA is done
+            if (threadIdx.x == 0) {
+                int all = 1;
+                for (int bq = il0; bq <= il1; ++bq) all &= li[bq - il0].done;
+                s_exit = all;
+            }
+            __syncthreads();
+            if (s_exit) break;
+        }
         double sig = 0.0;
         if (row && !li[li_idx].done) {
             const LocalInst& L = li[li_idx];
@@ -575,10 +821,11 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
 #pragma unroll
             for (int k = 0; k < MAXW; ++k) {
                 if (k >= w) continue;
-                const float4 zj = __ldcg(&E[cols[k]].z);
+                const int cj = col_at(k);
+                const float4 zj = __ldcg(&E[cj].z);
                 float3 pj = xyz(zj);
                 if (!first) {
-                    const float4 po = __ldcg(&E[cols[k]].p);
+                    const float4 po = __ldcg(&E[cj].p);
                     pj = f3(fmaf(beta, po.x, zj.x), fmaf(beta, po.y, zj.y), fmaf(beta, po.z, zj.z));
                 }
                 acc = acc + mul(B[k], pj);
@@ -587,17 +834,24 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
             sig = (double)p.x * acc.x + (double)p.y * acc.y + (double)p.z * acc.z;
         }
         sig = warp_sum(sig);
-        if (lane == 0 && has) spart[warp * 4] = sig;
+        if (lane == 0 && has) spart[warp * kSlotW] = sig;
         __syncthreads();
-        write_segment_slots<W * 32, 1>(bp, spart, s0, s1, il0, il1);
-        ok = grid_sync(gb, target, &s_flag);
-        if (!ok) break;
-        if (threadIdx.x == 0) s_exit = *(volatile unsigned*)&gb->ndone >= (unsigned)bp.n_inst;
-        __syncthreads();
-        if (s_exit) break;
+        write_segment_slots<W * 32, 1, SYNC>(bp, spart, s0, s1, il0, il1, ph % 3, li);
+        if (!SYNC) {
+            ok = grid_sync(gb, target, &s_flag);
+            if (!ok) break;
+            if (threadIdx.x == 0) s_exit = *(volatile unsigned*)&gb->ndone >= (unsigned)bp.n_inst;
+            __syncthreads();
+            if (s_exit) break;
+        }
 
-        instances_alpha<W>(bp, li, il0, il1);
+        instances_alpha<W, SYNC>(bp, li, il0, il1, ph % 3, &s_flag);
+        ++ph;
         __syncthreads();
+        if (SYNC && s_flag) {
+            ok = false;
+            break;
+        }
         double rz = 0.0, rr = 0.0;
         if (row && !li[li_idx].done) {
             const LocalInst& L = li[li_idx];
@@ -613,15 +867,22 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         rz = warp_sum(rz);
         rr = warp_sum(rr);
         if (lane == 0 && has) {
-            spart[warp * 4] = rz;
-            spart[warp * 4 + 1] = rr;
+            spart[warp * kSlotW] = rz;
+            spart[warp * kSlotW + 1] = rr;
         }
         __syncthreads();
-        write_segment_slots<W * 32, 2>(bp, spart, s0, s1, il0, il1);
-        ok = grid_sync(gb, target, &s_flag);
-        if (!ok) break;
-        instances_beta<W>(bp, li, il0, il1, cfg);
+        write_segment_slots<W * 32, 2, SYNC>(bp, spart, s0, s1, il0, il1, ph % 3, li);
+        if (!SYNC) {
+            ok = grid_sync(gb, target, &s_flag);
+            if (!ok) break;
+        }
+        instances_beta<W, SYNC>(bp, li, il0, il1, cfg, ph % 3, &s_flag);
+        ++ph;
         __syncthreads();
+        if (SYNC && s_flag) {
+            ok = false;
+            break;
+        }
     }
     if (row) {
         v.x[i] = f4(x);
@@ -631,248 +892,6 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     if (!ok) instances_fail(bp, li, il0, il1);
 }
 
-
-// ---------------------------------------------------------------------------
-// Single-reduction variant of the register-resident solve (Chronopoulos-Gear
-// PCG): one grid barrier per iteration instead of two.  With u = M^-1 r,
-// w = A u, m = M^-1 w, q = M^-1 s, s = A p:
-//   q_k = m_k + b_k q_k-1,  s_k = w_k + b_k s_k-1,  p_k = u_k + b_k p_k-1
-//   x += a_k p_k,  r -= a_k s_k,  u_k+1 = u_k - a_k q_k
-//   w_k+1 = A u_k+1,  m_k+1 = M^-1 w_k+1
-//   g = (r,u), d = (w,u), rr = (r,r) in one reduction
-//   b_k+1 = g_k+1 / g_k,  a_k+1 = g_k+1 / (d_k+1 - b_k+1 g_k+1 / a_k)
-// Every row publishes (u_k, m_k, q_k-1); a neighbour's u_k+1 is rebuilt from
-// them with the owner's exact FMA sequence, so A u_k+1 sees one consistent
-// vector and needs no second barrier.  Mathematically the same iterates as
-// PCG (pcg_solver.cu:467-593); round-off differs.  Off-diagonal blocks of
-// the CTA's rows live in shared memory.
-// ---------------------------------------------------------------------------
-struct UMQ {
-    float4 u;
-    float4 m;
-    float4 q;
-    float4 pad;
-};
-
-__device__ __forceinline__ float3 fma3(float a, float3 x, float3 y) {
-    return f3(fmaf(a, x.x, y.x), fmaf(a, x.y, y.y), fmaf(a, x.z, y.z));
-}
-
-template <int W, int MAXW>
-__global__ void __launch_bounds__(W * 32, 1)
-pcg_resident_cg1_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, UMQ* e0, UMQ* e1) {
-    extern __shared__ double s_mem[];
-    __shared__ int s_flag;
-    __shared__ int s_exit;
-    constexpr int R = W * 32;  // rows per CTA
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
-    const int il0 = bp.cta_inst_lo[blockIdx.x], il1 = bp.cta_inst_hi[blockIdx.x];
-    double* spart = s_mem;  // [W * 4]
-    LocalInst* li = reinterpret_cast<LocalInst*>(s_mem + (size_t)W * 4);
-    float* sblk = reinterpret_cast<float*>(li + bp.max_inst_per_cta);  // [MAXW * 6][R]
-    int* scol = reinterpret_cast<int*>(sblk + (size_t)MAXW * 6 * R);   // [MAXW][R]
-    GridBarrier* gb = bp.bar;
-    unsigned target = 0;
-    if (threadIdx.x == 0) s_flag = 0;
-    bool ok = true;
-
-    const int s = s0 + warp;
-    const bool has = s < s1;
-    const int i = s * 32 + lane;
-    const bool row = has && i < t.n;
-    const int li_idx = has ? bp.slice_inst[s] - il0 : 0;
-    const int tid = threadIdx.x;
-
-    S6 D{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, Mi{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    int w = 0;
-    float3 b = f3(0.f, 0.f, 0.f);
-    if (row) {
-        D = ld6(t.diag + (size_t)s * 192 + lane);
-        Mi = ld6(t.minv + (size_t)s * 192 + lane);
-        b = xyz(v.b[i]);
-        const int so = t.slice_off[s];
-        w = (t.slice_off[s + 1] - so) >> 5;
-        for (int k = 0; k < MAXW; ++k) {
-            if (k < w) {
-                scol[k * R + tid] = t.col[so + k * 32 + lane];
-                const float* src = t.val + (size_t)so * 6 + (size_t)k * 192 + lane;
-#pragma unroll
-                for (int c = 0; c < 6; ++c) sblk[(k * 6 + c) * R + tid] = src[c * 32];
-            }
-        }
-    }
-    auto offdiag = [&](int k) {
-        return S6{sblk[(k * 6 + 0) * R + tid], sblk[(k * 6 + 1) * R + tid], sblk[(k * 6 + 2) * R + tid],
-                  sblk[(k * 6 + 3) * R + tid], sblk[(k * 6 + 4) * R + tid], sblk[(k * 6 + 5) * R + tid]};
-    };
-
-    // ---- initial residual: r0 = b - A x0, u0 = M^-1 r0 (phase 0a) -----------
-    float3 x = f3(0.f, 0.f, 0.f), r = b, u = f3(0.f, 0.f, 0.f);
-    double rz = 0.0, rr = 0.0, bb = 0.0, bmb = 0.0;
-    if (row) {
-        const float3 zb = mul(Mi, b);
-        bb = (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z;
-        bmb = (double)b.x * zb.x + (double)b.y * zb.y + (double)b.z * zb.z;
-        if (warm) {
-            x = xyz(v.x[i]);
-            float3 ax = mul(D, x);
-            for (int k = 0; k < w; ++k) ax = ax + mul(offdiag(k), xyz(v.x[scol[k * R + tid]]));
-            r = b - ax;
-            u = mul(Mi, r);
-            rz = (double)r.x * u.x + (double)r.y * u.y + (double)r.z * u.z;
-            rr = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
-        } else {
-            u = zb;
-            rz = bmb;
-            rr = bb;
-        }
-    }
-    {
-        double a0 = warp_sum(rz), a1 = warp_sum(rr), a2 = warp_sum(bb), a3 = warp_sum(bmb);
-        if (lane == 0 && has) {
-            double* sp = spart + warp * 4;
-            sp[0] = a0; sp[1] = a1; sp[2] = a2; sp[3] = a3;
-        }
-    }
-    __syncthreads();
-    write_segment_slots<R, 4>(bp, spart, s0, s1, il0, il1);
-    ok = grid_sync(gb, target, &s_flag);
-    if (ok) {
-        instances_start<W>(bp, li, il0, il1, cfg, warm);
-        __syncthreads();
-        if (row && li[li_idx].fallback) {
-            x = f3(0.f, 0.f, 0.f);
-            r = b;
-            u = mul(Mi, b);
-        }
-        if (row) e0[i].u = f4(u);
-    }
-    // ---- w0 = A u0, m0 = M^-1 w0, first (g, d) -----------------------------------
-    if (ok) ok = grid_sync(gb, target, &s_flag);
-    float3 wv = f3(0.f, 0.f, 0.f), m = wv, q = wv, sv = wv, p = wv;
-    if (ok) {
-        double d = 0.0;
-        if (row) {
-            wv = mul(D, u);
-            for (int k = 0; k < w; ++k) wv = wv + mul(offdiag(k), xyz(__ldcg(&e0[scol[k * R + tid]].u)));
-            m = mul(Mi, wv);
-            d = (double)wv.x * u.x + (double)wv.y * u.y + (double)wv.z * u.z;
-            e0[i].m = f4(m);
-            e0[i].q = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        d = warp_sum(d);
-        if (lane == 0 && has) spart[warp * 4] = d;
-        __syncthreads();
-        write_segment_slots<R, 1>(bp, spart, s0, s1, il0, il1);
-        ok = grid_sync(gb, target, &s_flag);
-    }
-    if (ok) {
-        // a0 = g0 / d0, b0 = 0 (L.rho holds g; L.sigma holds alpha in FP64)
-        for (int bq = il0 + warp; bq <= il1; bq += W) {
-            LocalInst& L = li[bq - il0];
-            double tot[1];
-            read_instance_total<1>(bp, bq, tot);
-            if (lane == 0 && !L.done) {
-                const double a = (tot[0] > 1.0e-37 || tot[0] < -1.0e-37) ? L.rho / tot[0] : 0.0;
-                L.sigma = a;
-                L.alpha = (float)a;
-                L.beta = 0.0f;
-                if (!isfinite(a)) L.status = kSolveNonfinite;
-            }
-        }
-        __syncthreads();
-    }
-
-    // ---- iterations: one reduction each ------------------------------------
-    const int iter_cap = cfg.max_iter + 2;
-    // single instance only (the host guarantees it): every CTA holds the same
-    // instance state, so the exit decision below is uniform across the grid
-    for (int guard = 0; ok && guard < iter_cap; ++guard) {
-        if (threadIdx.x == 0) s_exit = li[0].done;
-        __syncthreads();
-        if (s_exit) break;
-        double g = 0.0, d = 0.0, r2 = 0.0;
-        if (row && !li[li_idx].done) {
-            const LocalInst& L = li[li_idx];
-            const float alpha = L.alpha, beta = L.beta;
-            const UMQ* E = (L.iter & 1) ? e1 : e0;
-            UMQ* En = (L.iter & 1) ? e0 : e1;
-            q = fma3(beta, q, m);
-            sv = fma3(beta, sv, wv);
-            p = fma3(beta, p, u);
-            x = fma3(alpha, p, x);
-            r = fma3(-alpha, sv, r);
-            u = fma3(-alpha, q, u);  // == what neighbours rebuild below
-            float3 acc = mul(D, u);
-            for (int k = 0; k < w; ++k) {
-                const UMQ* ej = E + scol[k * R + tid];
-                const float3 uj = xyz(__ldcg(&ej->u)), mj = xyz(__ldcg(&ej->m)), qj = xyz(__ldcg(&ej->q));
-                const float3 qn = fma3(beta, qj, mj);
-                acc = acc + mul(offdiag(k), fma3(-alpha, qn, uj));
-            }
-            wv = acc;
-            m = mul(Mi, wv);
-            En[i].u = f4(u);
-            En[i].m = f4(m);
-            En[i].q = f4(q);
-            g = (double)r.x * u.x + (double)r.y * u.y + (double)r.z * u.z;
-            d = (double)wv.x * u.x + (double)wv.y * u.y + (double)wv.z * u.z;
-            r2 = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
-        }
-        g = warp_sum(g);
-        d = warp_sum(d);
-        r2 = warp_sum(r2);
-        if (lane == 0 && has) {
-            spart[warp * 4] = g;
-            spart[warp * 4 + 1] = d;
-            spart[warp * 4 + 2] = r2;
-        }
-        __syncthreads();
-        write_segment_slots<R, 3>(bp, spart, s0, s1, il0, il1);
-        ok = grid_sync(gb, target, &s_flag);
-        if (!ok) break;
-        for (int bq = il0 + warp; bq <= il1; bq += W) {
-            LocalInst& L = li[bq - il0];
-            if (L.done) continue;
-            double tot[3];
-            read_instance_total<3>(bp, bq, tot);
-            if (lane != 0) continue;
-            const double g1 = tot[0], d1 = tot[1], rr1 = tot[2];
-            const double g0 = L.rho, a0 = L.sigma;
-            const double be = (g0 > 1.0e-37 || g0 < -1.0e-37) ? g1 / g0 : 0.0;
-            const double den = d1 - (a0 != 0.0 ? be * g1 / a0 : 0.0);
-            const double al = (den > 1.0e-37 || den < -1.0e-37) ? g1 / den : 0.0;
-            L.rho = g1;
-            L.rr = rr1;
-            L.beta = (float)be;
-            L.alpha = (float)al;
-            L.sigma = al;
-            L.iter += 1;
-            const bool bad = L.status == kSolveNonfinite || !isfinite(g1) || !isfinite(rr1) || !isfinite(al);
-            const bool conv = cfg.use_tol && rr1 <= L.tol2;
-            int done = 0;
-            if (bad) { L.status = kSolveNonfinite; done = 1; }
-            else if (conv) { L.status = kSolveConverged; done = 1; }
-            else if (L.iter >= cfg.max_iter) { L.status = cfg.use_tol ? kSolveMaxIter : kSolveConverged; done = 1; }
-            if (done) {
-                L.done = 1;
-                if ((int)blockIdx.x == bp.inst_cta_lo[bq]) {
-                    InstState& G = bp.inst[bq];
-                    G.rho = L.rho; G.rr = L.rr; G.iter = L.iter; G.status = L.status; G.done = 1;
-                    atomicAdd(&gb->ndone, 1u);
-                }
-            }
-        }
-        __syncthreads();
-    }
-    if (row) {
-        v.x[i] = f4(x);
-        v.r[i] = f4(r);
-        v.z[i] = f4(u);
-    }
-    if (!ok) instances_fail(bp, li, il0, il1);
-}
 
 // x_{n+1} = x_n + dx, v = dx/dt * exp(-c dt) (cloth_simulator.cu:222-244) for
 // the rows of every instance whose solve finished without NaN/Inf or a
@@ -905,6 +924,10 @@ __global__ void pcg_persistent_reset_kernel(BatchPlan bp) {
         InstState& G = bp.inst[b];
         G.rho = 0.0; G.rr = 0.0; G.bb = 0.0; G.tol2 = 0.0; G.rr0 = 0.0;
         G.iter = 0; G.status = kSolveConverged; G.done = 0; G.fallback = 0;
+    }
+    if (bp.fslots) {
+        const size_t total = (size_t)3 * bp.n_slots * kSlotW;
+        for (size_t k = b; k < total; k += (size_t)gridDim.x * blockDim.x) bp.fslots[k] = kSlotEmpty;
     }
 }
 

@@ -169,7 +169,9 @@ PYBIND11_MODULE(_chysx_native, m) {
                  if (warm == "zero") w = CHYSX_WARM_ZERO;
                  if (warm == "previous") w = CHYSX_WARM_PREVIOUS;
                  if (warm == "learned") w = CHYSX_WARM_LEARNED;
-                 if (w < 0) throw py::value_error("warm_start must be 'zero', 'previous' or 'learned'");
+                 if (warm == "previous_scaled") w = CHYSX_WARM_PREVIOUS_SCALED;
+                 if (w < 0)
+                     throw py::value_error("warm_start must be 'zero', 'previous', 'learned' or 'previous_scaled'");
                  check(chysx_cloth_set_solver(s.h(), max_iter, rel_tol, w));
              },
              py::arg("max_iter") = 50, py::arg("rel_tol") = 0.0, py::arg("warm_start") = "previous")

@@ -230,6 +230,29 @@ def time_reference_gpu(sc, iters, steps=3, warmup=2):
     return steps / (e0.elapsed_time(e1) * 1e-3)
 
 
+def oracle_error(args, sc, offs, make_sim, steps):
+    """Position error of the device path against the FP64 oracle (same
+    scene, same start, same rel-res stop; all host threads) after each of the
+    first `steps` steps, plus the oracle run to rel-res 1e-10.  Returns
+    {"steps", "max_abs_m_vs_fp64_same_tol", "max_abs_m_vs_fp64_tight", ...}."""
+    g = make_sim()
+    s_same = oracle_setup(sc, fp64=True, threads=cpu_threads())
+    s_tight = oracle_setup(sc, fp64=True, threads=cpu_threads())
+    s_same.set_solver(sc["max_iter"], 1e-6, "zero")
+    s_tight.set_solver(sc["max_iter"] * 4, 1e-10, "zero")
+    errs_same, errs_tight = [], []
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        g.step()
+        s_same.step(sc["dt"])
+        s_tight.step(sc["dt"])
+        p = g.positions()
+        errs_same.append(float(np.abs(p - s_same.state()[0]).max()))
+        errs_tight.append(float(np.abs(p - s_tight.state()[0]).max()))
+    return {"steps": steps, "max_abs_m_vs_fp64_same_tol": errs_same, "max_abs_m_vs_fp64_tight": errs_tight,
+            "oracle_threads": cpu_threads(), "seconds": time.perf_counter() - t0}
+
+
 def cpu_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -297,7 +320,7 @@ def run_ours(args, rank, world, local_rank):
     def make_sim():
         sim = GpuCloth(sc, max_iter=sc["max_iter"], rel_tol=rel_tol, warm_start="zero", instances=offs)
         sim.sim.set_tuning(args.path, args.block, args.grid)
-        sim.sim.set_pcg_variant(args.variant)
+        sim.sim.set_sync_mode(args.sync)
         if args.warm == "learned":
             from chysx import learned
 
@@ -321,6 +344,17 @@ def run_ours(args, rank, world, local_rank):
     ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     iters, solve_ms, asm_ms, statuses = [], [], [], []
+    # per-instance sizes: a batch charges each instance's rows and blocks only
+    # for the iterations that instance ran (finished instances are skipped)
+    inst_bytes = inst_bytes_ref = None
+    if offs is not None:
+        e = np.asarray(sc["edges"])
+        inst_of_edge = np.searchsorted(offs, e[:, 0], side="right") - 1
+        nnz_b = 2 * np.bincount(inst_of_edge, minlength=len(offs) - 1)
+        n_b = np.diff(offs)
+        inst_bytes = pcg_bytes_per_iteration(n_b, nnz_b).astype(np.float64)
+        inst_bytes_ref = reference_format_bytes_per_iteration(n_b, nnz_b).astype(np.float64)
+    moved, moved_ref = [], []
     clocks = ClockSampler(local_rank)
     barrier()
     torch.cuda.synchronize()
@@ -334,6 +368,10 @@ def run_ours(args, rank, world, local_rank):
         it, rr, st = g.stats()  # synchronises after the end event
         a_ms, s_ms, _ = g.sim.last_timing()
         iters.append(it)
+        if inst_bytes is not None:
+            it_b = g.sim.instance_stats()[0].astype(np.float64)
+            moved.append(float(np.dot(it_b, inst_bytes)))
+            moved_ref.append(float(np.dot(it_b, inst_bytes_ref)))
         solve_ms.append(s_ms)
         asm_ms.append(a_ms)
         statuses.append(st)
@@ -384,8 +422,10 @@ def run_ours(args, rank, world, local_rank):
     solve_ms = np.array(solve_ms)
     b_it = pcg_bytes_per_iteration(n, nnz)
     b_ref = reference_format_bytes_per_iteration(n, nnz)
-    achieved = float(np.sum(iters * b_it) / (np.sum(solve_ms) * 1e-3) / 1e9)
-    achieved_ref = float(np.sum(iters * b_ref) / (np.sum(solve_ms) * 1e-3) / 1e9)
+    if inst_bytes is None:
+        moved, moved_ref = list(iters * b_it), list(iters * b_ref)
+    achieved = float(np.sum(moved) / (np.sum(solve_ms) * 1e-3) / 1e9)
+    achieved_ref = float(np.sum(moved_ref) / (np.sum(solve_ms) * 1e-3) / 1e9)
     peak, peak_kind = read_peaks()
     traffic_it = read_traffic(args.workload)
     steps_total = args.steps * world
@@ -416,7 +456,8 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 dots)", "data": "synthetic",
         "config": {"workload": args.workload, "particles": n, "off_diag_blocks": int(nnz),
-                   "rel_tol": rel_tol, "warm_start": args.warm, "pcg_variant": args.variant,
+                   "rel_tol": rel_tol, "warm_start": args.warm,
+                   "sync_mode": args.sync,
                    "instances": 1 if offs is None else len(offs) - 1,
                    "pcg_kernel": g.sim.solver_info()[0], "pcg_grid": g.sim.solver_info()[1],
                    "pcg_block": g.sim.solver_info()[2], "l2": "flushed between steps (256 MiB write)"},
@@ -426,12 +467,12 @@ def run_ours(args, rank, world, local_rank):
         "us_per_pcg_iteration": float(np.sum(solve_ms) * 1e3 / np.sum(iters)),
         "assembly_ms": float(np.mean(asm_ms)),
         "roofline": {"bound": "hbm", "kernel": {"resident": "pcg_resident_kernel",
-                                                "resident-1r": "pcg_resident_cg1_kernel",
                                                 "streamed": "pcg_persistent_kernel",
                                                 "loop": "pcg_spmv_kernel+pcg_update_kernel"}[g.sim.solver_info()[0]],
                      "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": (traffic_it * mean_iters) if traffic_it else None,
+                     "algorithmic_bytes_per_launch": float(np.mean(moved)),
                      "algorithmic_bytes_per_iteration": b_it,
                      "reference_format_bytes_per_iteration": b_ref,
                      "achieved_reference_format": achieved_ref},
@@ -449,6 +490,8 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk,
         "wall_s": wall,
     }
+    if args.oracle_steps > 0 and offs is None:
+        line["oracle_error"] = oracle_error(args, sc, offs, make_sim, args.oracle_steps)
     if args.path == 1:
         # assemble + WHILE{2 per iteration} + finalize
         line["gpu_launches"] = int(2 * args.steps + 2 * np.sum(iters))
@@ -462,17 +505,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="grid256")
-    ap.add_argument("--warm", default="zero", choices=["zero", "previous", "learned"])
+    ap.add_argument("--warm", default="zero", choices=["zero", "previous", "learned", "previous_scaled"])
     ap.add_argument("--path", type=int, default=0,
                     help="0 persistent PCG (resident when it fits), 1 graph loop, 2 streamed persistent")
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--grid", type=int, default=0)
-    ap.add_argument("--variant", type=int, default=0, help="0 PCG, 1 single-reduction PCG (resident kernel)")
+    ap.add_argument("--sync", type=int, default=0, help="persistent kernels: 0 grid counter barrier, 1 polled slots")
     ap.add_argument("--net", default=os.path.join(ROOT, "ai-phyiscs_b200", "chysx", "data", "warmstart.npz"))
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--reference-gpu", type=int, default=1, help="also time the compiled reference module")
     ap.add_argument("--pcg-fixed", type=int, default=0,
                     help="K > 0: fixed K PCG iterations per step (rel_tol 0), the small profiling case")
+    ap.add_argument("--oracle-steps", type=int, default=0,
+                    help="N > 0: also report the position error vs the FP64 oracle over the first N steps")
     ap.add_argument("--legs", default="all", choices=["all", "device"],
                     help="device: only the device-timed leg (no e2e, CPU or reference legs)")
     args = ap.parse_args()

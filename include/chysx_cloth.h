@@ -46,8 +46,16 @@ enum {
     CHYSX_WARM_ZERO = 0,     /* zero guess (plain PCG) */
     CHYSX_WARM_PREVIOUS = 1, /* previous step's dx (reference behaviour,
                                 src/cloth/cloth_simulator.cu:1219-1228) */
-    CHYSX_WARM_LEARNED = 2   /* per-vertex network guess, zero-guess fallback */
+    CHYSX_WARM_LEARNED = 2,  /* per-vertex network guess, energy-scaled,
+                                zero-guess fallback */
+    CHYSX_WARM_PREVIOUS_SCALED = 3 /* previous dx, energy-scaled, zero-guess
+                                      fallback */
 };
+/* Energy scaling: a guess x0 starts the solve as c x0 with
+ * c = x0.b / x0.A x0, the factor that minimises 1/2 x.A x - b.x along x0, so
+ * the start is never worse than the zero guess in the A-norm; c <= 0 (or a
+ * non-finite partial) falls back to the zero guess.  CHYSX_WARM_PREVIOUS
+ * keeps the reference's unscaled start. */
 
 /* POD material, field-for-field src/cloth/cloth_material.h:20-43. */
 typedef struct chysx_cloth_material {
@@ -245,15 +253,31 @@ int chysx_cloth_instance_stats(chysx_cloth* h, int n, int* iterations, double* r
  * block (0, 128, 256, 512) and grid (0 = automatic) size the streamed
  * persistent kernel. */
 int chysx_cloth_set_tuning(chysx_cloth* h, int solver_path, int block, int grid);
-/* PCG recurrence (no counterpart in the reference): 0 = the reference's PCG
- * (two reductions per iteration, src/solver/pcg_solver.cu:467-593; default),
- * 1 = single-reduction PCG (Chronopoulos-Gear: same iterates in exact
- * arithmetic, one grid barrier per iteration), used by the register-resident
- * kernel for a single instance. */
-int chysx_cloth_set_pcg_variant(chysx_cloth* h, int variant);
+/* Synchronisation of the persistent PCG kernels (no counterpart in the
+ * reference): 0 = one grid-wide counter barrier per reduction (default),
+ * 1 = polled per-instance reduction slots, in which each instance waits only
+ * for the CTAs holding its rows and the reduction read is the wait itself.
+ * Both sum the same partials in the same order: identical iterates. */
+int chysx_cloth_set_sync_mode(chysx_cloth* h, int mode);
+
+/* Autotuner (no counterpart in the reference).  Times, on the current state,
+ * every solver configuration that applies to the current system: the
+ * planner's persistent kernel (register-resident rows when they fit, else
+ * streamed), the streamed kernel at 128 / 256 / 512 threads per CTA (4 / 8 /
+ * 16 32-row slices per CTA; one thread per row), both synchronisation modes,
+ * and the graph-loop path; each `repetitions` times (best kept).  All run the
+ * same PCG recurrence.  The caller's positions / velocities and the previous-step guess are
+ * restored after every trial, so the simulation does not advance; the
+ * fastest configuration stays selected.  Synchronises `stream`. */
+int chysx_cloth_autotune(chysx_cloth* h, float dt, int repetitions, uintptr_t stream);
+/* The autotuner's table: per candidate 8 ints (path, block, sync, kernel used
+ * as in solver_info, its grid, its block, iterations, solve status) and the
+ * solve time in ms; *count = the number of candidates. */
+int chysx_cloth_autotune_results(const chysx_cloth* h, int capacity, int* count, int32_t* config,
+                                 float* solve_ms);
+int chysx_cloth_sync_mode(const chysx_cloth* h, int* mode);
 /* Kernel used at the last graph build: path 0 register-resident persistent,
- * 1 graph loop, 2 streamed persistent, 3 register-resident single-reduction;
- * with its grid and block size. */
+ * 1 graph loop, 2 streamed persistent; with its grid and block size. */
 int chysx_cloth_solver_info(const chysx_cloth* h, int* path, int* grid, int* block);
 
 /* Measurement hooks (no counterpart in the reference): when enabled, the

@@ -162,7 +162,7 @@ class OracleCloth:
         _check(self._L.orc_set_options(self._h, int(springs_in_step), int(apply_force), float(det_eps)))
 
     def set_solver(self, max_iter=50, rel_tol=0.0, warm_start="previous"):
-        wm = {"zero": 0, "previous": 1, "user": 2}[warm_start]
+        wm = {"zero": 0, "previous": 1, "user": 2, "previous_scaled": 3, "user_scaled": 4}[warm_start]
         _check(self._L.orc_set_solver(self._h, int(max_iter), float(rel_tol), wm))
 
     def set_warm_guess(self, dx0):

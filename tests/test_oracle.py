@@ -174,6 +174,34 @@ def test_assembled_system_is_symmetric_and_solved():
     np.testing.assert_allclose(sim.spmv(x).ravel(), A @ x.ravel(), rtol=1e-12, atol=1e-9)
 
 
+def test_scaled_warm_start_minimises_energy_along_the_guess():
+    """previous_scaled starts from c x0 with c = x0.b / x0.A x0: its energy
+    1/2 x.A x - b.x is at or below both the unscaled guess's and the zero
+    guess's (0).  Checked by stopping the solve at 0 iterations."""
+    sc = scenes.config_small(side=8)
+    starts = {}
+    for mode in ("previous", "previous_scaled"):
+        sim = _oracle_sim(sc, tol=1e-10, max_iter=5000, warm="previous")
+        for _ in range(6):
+            sim.step(sc["dt"])
+        sim.set_solver(0, 0.0, mode)
+        sim.step(sc["dt"])
+        diag, rp, col, vals, rhs, dx = sim.dump_system()
+        starts[mode] = (_dense(diag, rp, col, vals), rhs.ravel(), dx.ravel())
+    A, b, x0 = starts["previous"]
+    A2, b2, xs = starts["previous_scaled"]
+    np.testing.assert_array_equal(A, A2)
+    np.testing.assert_array_equal(b, b2)
+
+    def energy(x):
+        return 0.5 * x @ (A @ x) - b @ x
+
+    c = (x0 @ b) / (x0 @ (A @ x0))
+    np.testing.assert_allclose(xs, max(c, 0.0) * x0, rtol=1e-12, atol=1e-300)
+    assert energy(xs) <= energy(x0) + 1e-15 * abs(energy(x0))
+    assert energy(xs) <= 1e-15 * abs(energy(x0))
+
+
 def test_lumped_mass_sums_to_density_times_area():
     sc = scenes.config_small()
     sim = O.OracleCloth(True)
