@@ -943,6 +943,11 @@ private:
     template <int SYNC>
     const void* persistent_fn_sync() const {
         if (resident_) {
+            // rows of a triangulated grid have at most 6 off-diagonal blocks;
+            // the 6-wide build keeps every row in registers without spills
+            if (topo_.max_width <= 6)
+                return resident_warps_ == 16 ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, 6, SYNC>)
+                                             : reinterpret_cast<const void*>(&pcg_resident_kernel<8, 6, SYNC>);
             return resident_warps_ == 16
                        ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, kResidentMaxWidth, SYNC>)
                        : reinterpret_cast<const void*>(&pcg_resident_kernel<8, kResidentMaxWidth, SYNC>);

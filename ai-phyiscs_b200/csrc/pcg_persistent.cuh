@@ -66,11 +66,19 @@ struct ZP {
     float4 p;
 };
 
+// CTA-local copy of one instance's solver state plus, set once per solve,
+// where its slices and reduction slots are (kept in shared memory so the
+// per-phase work reads no global metadata).
 struct LocalInst {
     double rho, rr, bb, tol2, sigma;
     float alpha, beta;
     float scale, scale_b;  // warm guess factor c and 1 - c
     int iter, done, status, fallback;
+    int b;                 // instance id
+    int seg_lo, seg_hi;    // this CTA's slices of it, relative to the CTA's first slice
+    int own_slot;          // this CTA's segment slot
+    int slot_lo, slot_hi;  // the instance's segment slots
+    int first;             // this CTA publishes the instance's state
 };
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
@@ -88,30 +96,25 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Count-based grid barrier: every CTA adds 1 to a monotonic counter (a
-// fire-and-forget release reduction) and thread 0 polls it with acquire
-// loads until it reaches this barrier's target.  The wait is bounded in time;
-// returns false (uniformly across the CTA) once any CTA flagged an error.
-__device__ __forceinline__ bool grid_sync(GridBarrier* gb, unsigned& target, int* s_flag) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        target += gridDim.x;
-        red_release_add(&gb->count, 1u);
-        const unsigned long long t0 = global_ns();
-        unsigned spins = 0;
-        while ((int)(ld_acquire_gpu(&gb->count) - target) < 0) {
-            if ((++spins & 255u) == 0) {
-                if (*(volatile int*)&gb->error) break;
-                if (global_ns() - t0 > kBarrierTimeoutNs) {
-                    atomicExch(&gb->error, 1);
-                    break;
-                }
+// Count-based grid barrier, run by one thread (lane 0 of warp 0): a
+// fire-and-forget release reduction on a monotonic counter, then acquire
+// loads until it reaches this barrier's target.  The wait is bounded in
+// time; returns false once any CTA flagged an error.
+__device__ __forceinline__ bool barrier_arrive_wait(GridBarrier* gb, unsigned& target) {
+    target += gridDim.x;
+    red_release_add(&gb->count, 1u);
+    const unsigned long long t0 = global_ns();
+    unsigned spins = 0;
+    while ((int)(ld_acquire_gpu(&gb->count) - target) < 0) {
+        if ((++spins & 255u) == 0) {
+            if (*(volatile int*)&gb->error) return false;
+            if (global_ns() - t0 > kBarrierTimeoutNs) {
+                atomicExch(&gb->error, 1);
+                return false;
             }
         }
-        *s_flag = *(volatile int*)&gb->error;
     }
-    __syncthreads();
-    return *s_flag == 0;
+    return *(volatile int*)&gb->error == 0;
 }
 
 __device__ __forceinline__ float4 ldcg4(const float4* p) { return __ldcg(p); }
@@ -123,15 +126,14 @@ __device__ __forceinline__ float4 ldcg4(const float4* p) { return __ldcg(p); }
 // every reduction phase ph publishes each CTA's per-instance partial sums in
 // slot set ph % 3 (each value stored after a release fence), and the CTAs
 // of an instance poll that instance's slots until every segment is there:
-// the poll is both the barrier and the data read, one L2 round trip fewer
-// per phase.  A slot holds kSlotEmpty until written; its owner resets the
-// set-(ph-1) copy during phase ph, after seeing every segment of phase ph:
-// each reader published its phase-ph segment after reading phase ph-1, so
-// no reader still needs the old value, and a reader of phase ph+2 (same
-// set) has acquired the owner's phase-ph+1 value, which orders the reset
-// before it.  An instance waits only for its own CTAs, and a CTA whose
-// instances are all done leaves the kernel.  Waits are bounded like
-// grid_sync's and raise the same error flag.
+// the poll is both the barrier and the data read.  A slot holds kSlotEmpty
+// until written; its owner resets the set-(ph-1) copy during phase ph, after
+// seeing every segment of phase ph: each reader published its phase-ph
+// segment after reading phase ph-1, so no reader still needs the old value,
+// and a reader of phase ph+2 (same set) has acquired the owner's phase-ph+1
+// value, which orders the reset before it.  An instance waits only for its
+// own CTAs, and a CTA whose instances are all done leaves the kernel.  Waits
+// are bounded like the counter barrier's and raise the same error flag.
 // ---------------------------------------------------------------------------
 // a NaN payload no arithmetic produces; published NaNs are canonicalised
 constexpr unsigned long long kSlotEmpty = 0x7FF4C10E5107E000ull;
@@ -150,15 +152,15 @@ __device__ __forceinline__ unsigned long long slot_bits(double x) {
     return isnan(x) ? 0x7FF8000000000000ull : (unsigned long long)__double_as_longlong(x);
 }
 
-// Waits for every segment of instance b in slot set `set` and sums them in
-// the same order as read_instance_total (ascending slot per lane, then an
-// xor tree), so both synchronisation modes give identical iterates.  Returns
-// false on every lane once the wait timed out or another CTA raised the
-// error flag.
-template <int NV, int KP = kPollMax>
-__device__ __forceinline__ bool poll_instance_total(const BatchPlan& bp, int b, int set, double (&out)[NV]) {
+// Waits for every segment of instance L in slot set `set` and sums them in
+// the same order as the counter-barrier read (ascending slot per lane, then
+// an xor tree), so both modes give identical iterates; lane 0 then resets
+// this CTA's slot of the previous set.  Returns false on every lane once the
+// wait timed out or another CTA raised the error flag.
+template <int NV, int KP>
+__device__ __forceinline__ bool poll_total(const BatchPlan& bp, const LocalInst& L, int set, double (&out)[NV]) {
     const int lane = threadIdx.x & 31;
-    const int lo = bp.inst_slot[b], hi = bp.inst_slot[b + 1];
+    const int lo = L.slot_lo, hi = L.slot_hi;
     const unsigned long long* base = bp.fslots + (size_t)set * bp.n_slots * kSlotW;
 #pragma unroll
     for (int q = 0; q < NV; ++q) out[q] = 0.0;
@@ -212,88 +214,11 @@ __device__ __forceinline__ bool poll_instance_total(const BatchPlan& bp, int b, 
     }
     ok = __all_sync(0xffffffffu, ok);
     if (ok && lane == 0) {
-        // this CTA's own slot of the previous phase can be reused
-        const int own = bp.inst_slot[b] + ((int)blockIdx.x - bp.inst_cta_lo[b]);
-        unsigned long long* d = bp.fslots + ((size_t)((set + 2) % 3) * bp.n_slots + own) * kSlotW;
+        unsigned long long* d = bp.fslots + ((size_t)((set + 2) % 3) * bp.n_slots + L.own_slot) * kSlotW;
 #pragma unroll
         for (int q = 0; q < kSlotW; ++q) st_relaxed_u64(d + q, kSlotEmpty);
     }
     return ok;
-}
-
-
-// ---------------------------------------------------------------------------
-// Segmented reductions
-// ---------------------------------------------------------------------------
-// spart[(s - s0) * kSlotW + q] holds slice partials; write, for every instance
-// this CTA touches, the sum over its slices into the instance's slot.
-// SYNC = 1 publishes into slot set `set` instead (release fence, then
-// relaxed stores), skipping instances already done (li, when given).
-template <int BLOCK, int NV, int SYNC = 0>
-__device__ __forceinline__ void write_segment_slots(const BatchPlan& bp, const double* spart, int s0, int s1,
-                                                    int il0, int il1, int set = 0,
-                                                    const LocalInst* li = nullptr) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int W = BLOCK / 32;
-    for (int b = il0 + warp; b <= il1; b += W) {
-        if (SYNC && li && li[b - il0].done) continue;
-        const int lo = max(s0, bp.inst_slice[b]), hi = min(s1, bp.inst_slice[b + 1]);
-        double acc[NV];
-#pragma unroll
-        for (int q = 0; q < NV; ++q) acc[q] = 0.0;
-        for (int s = lo + lane; s < hi; s += 32) {
-#pragma unroll
-            for (int q = 0; q < NV; ++q) acc[q] += spart[(s - s0) * kSlotW + q];
-        }
-#pragma unroll
-        for (int q = 0; q < NV; ++q) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
-        }
-        if (lane == 0) {
-            const int slot = bp.inst_slot[b] + ((int)blockIdx.x - bp.inst_cta_lo[b]);
-            if (SYNC) {
-                unsigned long long* d = bp.fslots + ((size_t)set * bp.n_slots + slot) * kSlotW;
-                fence_acq_rel_gpu();  // release: the CTA's writes before the __syncthreads
-#pragma unroll
-                for (int q = 0; q < NV; ++q) st_relaxed_u64(d + q, slot_bits(acc[q]));
-            } else {
-#pragma unroll
-                for (int q = 0; q < NV; ++q) bp.slots[(size_t)slot * kSlotW + q] = acc[q];
-            }
-        }
-    }
-}
-
-// Warp `warp` sums instance b's slots (after a barrier); every lane gets it.
-template <int NV>
-__device__ __forceinline__ void read_instance_total(const BatchPlan& bp, int b, double (&out)[NV]) {
-    const int lane = threadIdx.x & 31;
-    const int lo = bp.inst_slot[b], hi = bp.inst_slot[b + 1];
-#pragma unroll
-    for (int q = 0; q < NV; ++q) out[q] = 0.0;
-    for (int k = lo + lane; k < hi; k += 32) {
-#pragma unroll
-        for (int q = 0; q < NV; ++q) out[q] += __ldcg(bp.slots + (size_t)k * kSlotW + q);
-    }
-#pragma unroll
-    for (int q = 0; q < NV; ++q) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) out[q] += __shfl_xor_sync(0xffffffffu, out[q], o);
-    }
-}
-
-// Reads instance b's total in either mode; on a failed wait lane 0 raises
-// the CTA's flag.
-template <int NV, int SYNC, int KP = kPollMax>
-__device__ __forceinline__ bool instance_total(const BatchPlan& bp, int b, int set, double (&out)[NV], int* s_flag) {
-    if (SYNC) {
-        const bool ok = poll_instance_total<NV, KP>(bp, b, set, out);
-        if (!ok && (threadIdx.x & 31) == 0) *s_flag = 1;
-        return ok;
-    }
-    read_instance_total<NV>(bp, b, out);
-    return true;
 }
 
 __device__ __forceinline__ double warp_sum(double x) {
@@ -306,9 +231,108 @@ __device__ __forceinline__ double dot3d(float3 a, float3 b) {
     return (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z;
 }
 
+// ---------------------------------------------------------------------------
+// Per-instance bookkeeping
+// ---------------------------------------------------------------------------
+// Where this CTA's instances live (all threads of the CTA, once per solve;
+// a __syncthreads must follow).
+__device__ __forceinline__ void init_local(const BatchPlan& bp, LocalInst* li, int s0, int s1, int il0, int il1) {
+    for (int t = threadIdx.x; t <= il1 - il0; t += blockDim.x) {
+        const int b = il0 + t;
+        LocalInst& L = li[t];
+        L.b = b;
+        L.seg_lo = max(s0, bp.inst_slice[b]) - s0;
+        L.seg_hi = min(s1, bp.inst_slice[b + 1]) - s0;
+        L.slot_lo = bp.inst_slot[b];
+        L.slot_hi = bp.inst_slot[b + 1];
+        L.own_slot = L.slot_lo + ((int)blockIdx.x - bp.inst_cta_lo[b]);
+        L.first = (int)blockIdx.x == bp.inst_cta_lo[b];
+        L.done = 0;
+        L.iter = 0;
+        L.status = kSolveConverged;
+        L.fallback = 0;
+    }
+}
+
+// One reduction phase, run by warp 0 between two __syncthreads: sums the
+// slice partials spart[slice * kSlotW + q] (q < NV) of every unfinished
+// instance of the CTA, publishes the CTA's segment, waits for the other
+// CTAs (counter barrier or polled slots), reads each instance's total in a
+// fixed order and lets lane 0 apply `step(L, total)`.  Returns false (on all
+// lanes) after a failed wait.
+template <int NV, int SYNC, int KP, class Step>
+__device__ __forceinline__ bool warp0_phase(const BatchPlan& bp, const double* spart, LocalInst* li, int nloc,
+                                            int set, unsigned& target, Step&& step) {
+    const int lane = threadIdx.x & 31;
+    for (int t = 0; t < nloc; ++t) {
+        const LocalInst& L = li[t];
+        if (L.done) continue;
+        double acc[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+        for (int sl = L.seg_lo + lane; sl < L.seg_hi; sl += 32) {
+#pragma unroll
+            for (int q = 0; q < NV; ++q) acc[q] += spart[sl * kSlotW + q];
+        }
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[q] = warp_sum(acc[q]);
+        if (lane == 0) {
+            if (SYNC) {
+                unsigned long long* d = bp.fslots + ((size_t)set * bp.n_slots + L.own_slot) * kSlotW;
+                fence_acq_rel_gpu();  // release: the CTA's writes before the __syncthreads
+#pragma unroll
+                for (int q = 0; q < NV; ++q) st_relaxed_u64(d + q, slot_bits(acc[q]));
+            } else {
+#pragma unroll
+                for (int q = 0; q < NV; ++q) bp.slots[(size_t)L.own_slot * kSlotW + q] = acc[q];
+            }
+        }
+    }
+    if (!SYNC) {
+        bool ok = true;
+        if (lane == 0) ok = barrier_arrive_wait(bp.bar, target);
+        if (!__shfl_sync(0xffffffffu, ok, 0)) return false;
+    }
+    for (int t = 0; t < nloc; ++t) {
+        LocalInst& L = li[t];
+        if (L.done) continue;
+        double tot[NV];
+        if (SYNC) {
+            if (!poll_total<NV, KP>(bp, L, set, tot)) return false;
+        } else {
+            // all of a lane's slots in flight at once (fixed unroll), summed
+            // in ascending slot order
+#pragma unroll
+            for (int q = 0; q < NV; ++q) tot[q] = 0.0;
+            for (int c0 = L.slot_lo; c0 < L.slot_hi; c0 += 32 * KP) {
+                double val[KP][NV];
+#pragma unroll
+                for (int j = 0; j < KP; ++j) {
+                    const int k = c0 + j * 32 + lane;
+#pragma unroll
+                    for (int q = 0; q < NV; ++q)
+                        val[j][q] = k < L.slot_hi ? __ldcg(bp.slots + (size_t)k * kSlotW + q) : 0.0;
+                }
+#pragma unroll
+                for (int j = 0; j < KP; ++j) {
+                    if (c0 + j * 32 + lane < L.slot_hi) {
+#pragma unroll
+                        for (int q = 0; q < NV; ++q) tot[q] += val[j][q];
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NV; ++q) tot[q] = warp_sum(tot[q]);
+        }
+        if (lane == 0) step(L, tot);
+        __syncwarp();
+    }
+    return true;
+}
+
 // Start partials of one row, kSlotW wide: r.z, r.r, b.b, b.M^-1 b, x0.b,
 // x0.r, b.z, b.r (with r = b - A x0, z = M^-1 r; the zero guess has x0 = 0,
-// r = b, z = M^-1 b).  The warp sums land in spart[slot * kSlotW + q].
+// r = b, z = M^-1 b).  The warp sums land in sp[q].
 __device__ __forceinline__ void start_partials(double* sp, bool write, float3 b, float3 zb, float3 x0, float3 r,
                                                float3 z) {
     double q[kSlotW] = {dot3d(r, z), dot3d(r, r), dot3d(b, b), dot3d(b, zb),
@@ -337,143 +361,127 @@ __device__ __forceinline__ void start_row(const LocalInst& L, float3 b, const S6
     z = mul(Mi, r);
 }
 
-// ---------------------------------------------------------------------------
-// Per-instance scalar steps shared by the persistent kernels.  Each runs on
-// one warp per instance (the whole warp reads the instance's slots) and
-// lane 0 updates the CTA-local copy; the first CTA touching an instance
-// also publishes its state and counts it when it finishes.
-// ---------------------------------------------------------------------------
-template <int W, int SYNC = 0>
-__device__ __forceinline__ void instances_start(const BatchPlan& bp, LocalInst* li, int il0, int il1,
-                                                const SolverCfg& cfg, int warm, int set = 0,
-                                                int* s_flag = nullptr) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int b = il0 + warp; b <= il1; b += W) {
-        double tot[kSlotW];
-        // once per solve: fewer slots in flight keep the registers of the
-        // resident kernels' rows free
-        if (!instance_total<kSlotW, SYNC, 1>(bp, b, set, tot, s_flag)) continue;
-        if (lane != 0) continue;
-        LocalInst& L = li[b - il0];
-        const double bb = tot[2];
-        // warm guess x0: scaled by c = x0.b / x0.A x0 (x0.A x0 = x0.(b - r0)),
-        // the factor minimising the energy 1/2 x.A x - b.x along x0, so the
-        // start is never worse than the zero guess in the A-norm; c <= 0
-        // (or NaN / Inf) falls back to the zero guess
-        // (warm == 2); warm == 1 keeps the guess as given (the reference's
-        // previous-dx start) unless a partial is not finite
-        double c = 0.0;
-        if (warm == 1) {
-            c = isfinite(tot[0]) && isfinite(tot[1]) ? 1.0 : 0.0;
-        } else if (warm == 2) {
-            const double xax = tot[4] - tot[5];
-            c = xax > 0.0 ? tot[4] / xax : 0.0;
-            if (!(c > 0.0) || !isfinite(c) || !isfinite(tot[0]) || !isfinite(tot[1])) c = 0.0;
-        }
-        L.fallback = warm && c == 0.0 ? 1 : 0;
-        L.scale = (float)c;
-        L.scale_b = (float)(1.0 - c);
-        if (c == 1.0) {
-            L.rho = tot[0];
-            L.rr = tot[1];
-        } else if (c > 0.0) {
-            // r = (1 - c) b + c r0: its r.z and r.r from the start partials
-            const double cb = 1.0 - c;
-            L.rho = fmax(cb * cb * tot[3] + 2.0 * c * cb * tot[6] + c * c * tot[0], 0.0);
-            L.rr = fmax(cb * cb * bb + 2.0 * c * cb * tot[7] + c * c * tot[1], 0.0);
-        } else {
-            L.rho = tot[3];
-            L.rr = bb;
-        }
-        L.bb = bb;
-        L.tol2 = cfg.rel_tol * cfg.rel_tol * bb;
-        L.iter = 0;
-        L.alpha = 0.0f;
-        L.beta = 0.0f;
-        const bool bad = !isfinite(L.rho) || !isfinite(L.rr) || !isfinite(bb);
-        const bool conv = cfg.use_tol && L.rr <= L.tol2;
-        L.status = bad ? kSolveNonfinite : kSolveConverged;
-        L.done = (bad || conv || cfg.max_iter <= 0) ? 1 : 0;
-        if ((int)blockIdx.x == bp.inst_cta_lo[b]) {
-            InstState& G = bp.inst[b];
-            G.rr0 = L.rr;
-            G.bb = bb;
-            G.fallback = L.fallback;
-            if (L.done) {
-                G.rho = L.rho; G.rr = L.rr; G.iter = 0; G.status = L.status; G.done = 1;
-                atomicAdd(&bp.bar->ndone, 1u);
-            }
+// Scalar steps (lane 0 of warp 0, on the CTA-local copy; the instance's
+// first CTA also publishes the state and counts the instance when done).
+// Start: the warm guess x0 is scaled by c = x0.b / x0.A x0 (x0.A x0 =
+// x0.(b - r0)), the factor minimising 1/2 x.A x - b.x along x0, so the start
+// is never worse than the zero guess in the A-norm (warm == 2); warm == 1
+// keeps the guess as given (the reference's previous-dx start).  c <= 0 or
+// a non-finite partial falls back to the zero guess.
+__device__ __forceinline__ void step_start(const BatchPlan& bp, LocalInst& L, const double* tot, const SolverCfg& cfg,
+                                           int warm) {
+    const double bb = tot[2];
+    double c = 0.0;
+    if (warm == 1) {
+        c = isfinite(tot[0]) && isfinite(tot[1]) ? 1.0 : 0.0;
+    } else if (warm == 2) {
+        const double xax = tot[4] - tot[5];
+        c = xax > 0.0 ? tot[4] / xax : 0.0;
+        if (!(c > 0.0) || !isfinite(c) || !isfinite(tot[0]) || !isfinite(tot[1])) c = 0.0;
+    }
+    L.fallback = warm && c == 0.0 ? 1 : 0;
+    L.scale = (float)c;
+    L.scale_b = (float)(1.0 - c);
+    if (c == 1.0) {
+        L.rho = tot[0];
+        L.rr = tot[1];
+    } else if (c > 0.0) {
+        // r = (1 - c) b + c r0: its r.z and r.r from the start partials
+        const double cb = 1.0 - c;
+        L.rho = fmax(cb * cb * tot[3] + 2.0 * c * cb * tot[6] + c * c * tot[0], 0.0);
+        L.rr = fmax(cb * cb * bb + 2.0 * c * cb * tot[7] + c * c * tot[1], 0.0);
+    } else {
+        L.rho = tot[3];
+        L.rr = bb;
+    }
+    L.bb = bb;
+    L.tol2 = cfg.rel_tol * cfg.rel_tol * bb;
+    L.iter = 0;
+    L.alpha = 0.0f;
+    L.beta = 0.0f;
+    const bool bad = !isfinite(L.rho) || !isfinite(L.rr) || !isfinite(bb);
+    const bool conv = cfg.use_tol && L.rr <= L.tol2;
+    L.status = bad ? kSolveNonfinite : kSolveConverged;
+    L.done = (bad || conv || cfg.max_iter <= 0) ? 1 : 0;
+    if (L.first) {
+        InstState& G = bp.inst[L.b];
+        G.rr0 = L.rr;
+        G.bb = bb;
+        G.fallback = L.fallback;
+        if (L.done) {
+            G.rho = L.rho; G.rr = L.rr; G.iter = 0; G.status = L.status; G.done = 1;
+            atomicAdd(&bp.bar->ndone, 1u);
         }
     }
 }
 
-template <int W, int SYNC = 0>
-__device__ __forceinline__ void instances_alpha(const BatchPlan& bp, LocalInst* li, int il0, int il1, int set = 0,
-                                                int* s_flag = nullptr) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int b = il0 + warp; b <= il1; b += W) {
-        LocalInst& L = li[b - il0];
-        if (L.done) continue;
-        double tot[1];
-        if (!instance_total<1, SYNC>(bp, b, set, tot, s_flag)) continue;
-        if (lane == 0) {
-            const double sigma = tot[0];
-            const double alpha = (sigma > 1.0e-37 || sigma < -1.0e-37) ? L.rho / sigma : 0.0;
-            L.sigma = sigma;
-            L.alpha = (float)alpha;
-            if (!isfinite(sigma) || !isfinite(alpha)) L.status = kSolveNonfinite;
-        }
-    }
+// alpha = rho / sigma (pcg_solver.cu:421-423)
+__device__ __forceinline__ void step_alpha(LocalInst& L, const double* tot) {
+    const double sigma = tot[0];
+    const double alpha = (sigma > 1.0e-37 || sigma < -1.0e-37) ? L.rho / sigma : 0.0;
+    L.sigma = sigma;
+    L.alpha = (float)alpha;
+    if (!isfinite(sigma) || !isfinite(alpha)) L.status = kSolveNonfinite;
 }
 
-template <int W, int SYNC = 0>
-__device__ __forceinline__ void instances_beta(const BatchPlan& bp, LocalInst* li, int il0, int il1,
-                                               const SolverCfg& cfg, int set = 0, int* s_flag = nullptr) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int b = il0 + warp; b <= il1; b += W) {
-        LocalInst& L = li[b - il0];
-        if (L.done) continue;
-        double tot[2];
-        if (!instance_total<2, SYNC>(bp, b, set, tot, s_flag)) continue;
-        if (lane != 0) continue;
-        const double rho_new = tot[0], rr = tot[1];
-        const double beta = (L.rho > 1.0e-37 || L.rho < -1.0e-37) ? rho_new / L.rho : 0.0;
-        L.beta = (float)beta;
-        L.rho = rho_new;
-        L.rr = rr;
-        L.iter += 1;
-        const bool bad = L.status == kSolveNonfinite || !isfinite(rho_new) || !isfinite(rr);
-        const bool conv = cfg.use_tol && rr <= L.tol2;
-        int done = 0;
-        if (bad) { L.status = kSolveNonfinite; done = 1; }
-        else if (conv) { L.status = kSolveConverged; done = 1; }
-        else if (L.iter >= cfg.max_iter) { L.status = cfg.use_tol ? kSolveMaxIter : kSolveConverged; done = 1; }
-        if (done) {
-            L.done = 1;
-            if ((int)blockIdx.x == bp.inst_cta_lo[b]) {
-                InstState& G = bp.inst[b];
-                G.rho = L.rho; G.rr = L.rr; G.iter = L.iter; G.status = L.status; G.done = 1;
-                atomicAdd(&bp.bar->ndone, 1u);
-            }
+// beta, iteration count, convergence (pcg_solver.cu:436-454)
+__device__ __forceinline__ void step_beta(const BatchPlan& bp, LocalInst& L, const double* tot, const SolverCfg& cfg) {
+    const double rho_new = tot[0], rr = tot[1];
+    const double beta = (L.rho > 1.0e-37 || L.rho < -1.0e-37) ? rho_new / L.rho : 0.0;
+    L.beta = (float)beta;
+    L.rho = rho_new;
+    L.rr = rr;
+    L.iter += 1;
+    const bool bad = L.status == kSolveNonfinite || !isfinite(rho_new) || !isfinite(rr);
+    const bool conv = cfg.use_tol && rr <= L.tol2;
+    int done = 0;
+    if (bad) { L.status = kSolveNonfinite; done = 1; }
+    else if (conv) { L.status = kSolveConverged; done = 1; }
+    else if (L.iter >= cfg.max_iter) { L.status = cfg.use_tol ? kSolveMaxIter : kSolveConverged; done = 1; }
+    if (done) {
+        L.done = 1;
+        if (L.first) {
+            InstState& G = bp.inst[L.b];
+            G.rho = L.rho; G.rr = L.rr; G.iter = L.iter; G.status = L.status; G.done = 1;
+            atomicAdd(&bp.bar->ndone, 1u);
         }
     }
 }
 
 // A barrier failure leaves every unfinished instance flagged.
-__device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalInst* li, int il0, int il1) {
+__device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalInst* li, int nloc) {
     if (threadIdx.x != 0) return;
-    for (int b = il0; b <= il1; ++b) {
-        if ((int)blockIdx.x == bp.inst_cta_lo[b]) {
-            InstState& G = bp.inst[b];
+    for (int t = 0; t < nloc; ++t) {
+        if (li[t].first) {
+            InstState& G = bp.inst[li[t].b];
             G.status = kSolveKernelError;
-            G.iter = li[b - il0].iter;
+            G.iter = li[t].iter;
             G.done = 1;
         }
     }
 }
 
+// The phase protocol shared by both kernels.  After the CTA's slice
+// partials are in spart and a __syncthreads, this runs the warp-0 phase and
+// leaves, after a closing __syncthreads, s_flag = 1 on a failed wait and
+// (counter mode, with `exit_test`) s_exit = 1 when every instance of the
+// batch is done.
+#define CHYSX_REDUCE_PHASE(NV, KP, exit_test, STEP)                                                  \
+    do {                                                                                             \
+        if (warp == 0) {                                                                             \
+            const bool w0ok = warp0_phase<NV, SYNC, KP>(bp, spart, li, nloc, ph % 3, target, STEP);  \
+            if (lane == 0) {                                                                         \
+                if (!w0ok) s_flag = 1;                                                               \
+                if (!SYNC && (exit_test) && w0ok)                                                    \
+                    s_exit = *(volatile unsigned*)&bp.bar->ndone >= (unsigned)bp.n_inst;            \
+            }                                                                                        \
+        }                                                                                            \
+        ++ph;                                                                                        \
+        __syncthreads();                                                                             \
+    } while (0)
+
 // ---------------------------------------------------------------------------
-// The kernel
+// Streamed persistent kernel: rows are re-read from HBM every iteration.
 // ---------------------------------------------------------------------------
 template <int BLOCK, int SYNC = 0>
 __global__ void __launch_bounds__(BLOCK)
@@ -485,13 +493,19 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
     const int il0 = bp.cta_inst_lo[blockIdx.x], il1 = bp.cta_inst_hi[blockIdx.x];
+    const int nloc = il1 - il0 + 1;
     double* spart = s_mem;
     LocalInst* li = reinterpret_cast<LocalInst*>(s_mem + (size_t)bp.max_slices_per_cta * kSlotW);
-    GridBarrier* gb = bp.bar;
-    unsigned gen = 0;  // barrier target; the counter starts at 0 every solve
-    int ph = 0;        // reduction phase (SYNC = 1 slot set ph % 3)
-    if (threadIdx.x == 0) s_flag = 0;
+    unsigned target = 0;  // barrier target; the counter starts at 0 every solve
+    int ph = 0;           // reduction phase (SYNC = 1 slot set ph % 3)
+    if (threadIdx.x == 0) {
+        s_flag = 0;
+        s_exit = 0;
+    }
+    init_local(bp, li, s0, s1, il0, il1);
+    __syncthreads();
     bool ok = true;
+    auto no_step = [](LocalInst&, const double*) {};
 
     // ---- phase 0: initial residual and per-instance start ----------------
     // zero guess: r = b, z = M^-1 b were written by the assembly kernel.
@@ -524,41 +538,26 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
         start_partials(spart + (s - s0) * kSlotW, lane == 0, b, zb, x0, r, z);
     }
     __syncthreads();
-    write_segment_slots<BLOCK, kSlotW, SYNC>(bp, spart, s0, s1, il0, il1, ph % 3);
-    if (!SYNC) ok = grid_sync(gb, gen, &s_flag);
-    if (ok) {
-        instances_start<W, SYNC>(bp, li, il0, il1, cfg, warm, ph % 3, &s_flag);
-        ++ph;
-        __syncthreads();
-        ok = s_flag == 0;
-        if (ok && warm) {
-            // the scaled guess, or the zero guess where the instance fell back
-            for (int s = s0 + warp; s < s1; s += W) {
-                const int i = s * 32 + lane;
-                if (i >= t.n) continue;
-                const S6 Mi = ld6(t.minv + (size_t)s * 192 + lane);
-                float3 x = xyz(v.x[i]), r = xyz(v.r[i]), z;
-                start_row(li[bp.slice_inst[s] - il0], xyz(v.b[i]), Mi, x, r, z);
-                v.x[i] = f4(x);
-                v.r[i] = f4(r);
-                v.z[i] = f4(z);
-            }
-            if (SYNC) {
-                // a data-free phase orders the fallback rows before any gather
-                for (int q = threadIdx.x; q < s1 - s0; q += BLOCK) spart[q * kSlotW] = 0.0;
-                __syncthreads();
-                write_segment_slots<BLOCK, 1, 1>(bp, spart, s0, s1, il0, il1, ph % 3, li);
-                for (int bq = il0 + warp; bq <= il1; bq += W) {
-                    double tot[1];
-                    if (!li[bq - il0].done) instance_total<1, 1>(bp, bq, ph % 3, tot, &s_flag);
-                }
-                ++ph;
-                __syncthreads();
-                ok = s_flag == 0;
-            } else {
-                ok = grid_sync(gb, gen, &s_flag);
-            }
+    CHYSX_REDUCE_PHASE(kSlotW, 1, false,
+                       ([&](LocalInst& L, const double* tot) { step_start(bp, L, tot, cfg, warm); }));
+    ok = s_flag == 0;
+    if (ok && warm) {
+        // the scaled guess, or the zero guess where the instance fell back
+        for (int s = s0 + warp; s < s1; s += W) {
+            const int i = s * 32 + lane;
+            if (i >= t.n) continue;
+            const S6 Mi = ld6(t.minv + (size_t)s * 192 + lane);
+            float3 x = xyz(v.x[i]), r = xyz(v.r[i]), z;
+            start_row(li[bp.slice_inst[s] - il0], xyz(v.b[i]), Mi, x, r, z);
+            v.x[i] = f4(x);
+            v.r[i] = f4(r);
+            v.z[i] = f4(z);
         }
+        // a data-free phase orders the new rows before any gather
+        for (int q = threadIdx.x; q < s1 - s0; q += BLOCK) spart[q * kSlotW] = 0.0;
+        __syncthreads();
+        CHYSX_REDUCE_PHASE(1, kPollMax, false, no_step);
+        ok = s_flag == 0;
     }
 
     // ---- iterations ---------------------------------------------------------
@@ -568,7 +567,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             // leave once every instance of this CTA is done
             if (threadIdx.x == 0) {
                 int all = 1;
-                for (int bq = il0; bq <= il1; ++bq) all &= li[bq - il0].done;
+                for (int q = 0; q < nloc; ++q) all &= li[q].done;
                 s_exit = all;
             }
             __syncthreads();
@@ -615,25 +614,16 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             if (lane == 0) spart[(s - s0) * kSlotW] = sig;
         }
         __syncthreads();
-        write_segment_slots<BLOCK, 1, SYNC>(bp, spart, s0, s1, il0, il1, ph % 3, li);
-        if (!SYNC) {
-            ok = grid_sync(gb, gen, &s_flag);
-            if (!ok) break;
-            // ndone only changes in phase 3 and phase 0, i.e. never between
-            // this barrier and the next, so every CTA takes the same decision
-            if (threadIdx.x == 0) s_exit = *(volatile unsigned*)&gb->ndone >= (unsigned)bp.n_inst;
-            __syncthreads();
-            if (s_exit) break;
-        }
-
-        // phase 2: alpha = rho / sigma; x += alpha p; r -= alpha Ap; z = M^-1 r
-        instances_alpha<W, SYNC>(bp, li, il0, il1, ph % 3, &s_flag);
-        ++ph;
-        __syncthreads();
-        if (SYNC && s_flag) {
+        // ndone only changes in the start and beta steps, i.e. never between
+        // this barrier and the next, so every CTA takes the same exit decision
+        CHYSX_REDUCE_PHASE(1, kPollMax, true, ([&](LocalInst& L, const double* tot) { step_alpha(L, tot); }));
+        if (s_flag) {
             ok = false;
             break;
         }
+        if (!SYNC && s_exit) break;
+
+        // phase 2: x += alpha p; r -= alpha Ap; z = M^-1 r
         for (int s = s0 + warp; s < s1; s += W) {
             const LocalInst& L = li[bp.slice_inst[s] - il0];
             const int i = s * 32 + lane;
@@ -659,22 +649,15 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             }
         }
         __syncthreads();
-        write_segment_slots<BLOCK, 2, SYNC>(bp, spart, s0, s1, il0, il1, ph % 3, li);
-        if (!SYNC) {
-            ok = grid_sync(gb, gen, &s_flag);
-            if (!ok) break;
-        }
-
-        // phase 3: beta, iteration count, convergence (pcg_solver.cu:436-454)
-        instances_beta<W, SYNC>(bp, li, il0, il1, cfg, ph % 3, &s_flag);
-        ++ph;
-        __syncthreads();
-        if (SYNC && s_flag) {
+        // phase 3: beta, iteration count, convergence
+        CHYSX_REDUCE_PHASE(2, kPollMax, false,
+                           ([&](LocalInst& L, const double* tot) { step_beta(bp, L, tot, cfg); }));
+        if (s_flag) {
             ok = false;
             break;
         }
     }
-    if (!ok) instances_fail(bp, li, il0, il1);
+    if (!ok) instances_fail(bp, li, nloc);
 }
 
 
@@ -685,26 +668,34 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
 // x, r, z, p in registers.  Per iteration it publishes only p (phase 1) and
 // z (phase 2) for its neighbours, packed as one 32-byte entry per row in a
 // double-buffered array, so a neighbour's (z, p_old) pair is one sector.
-// Same phases, reductions, barrier and per-instance logic as
-// pcg_persistent_kernel.
+// The CTA's own rows' z and p are also kept in shared memory: neighbours in
+// the same CTA are read from there, the others from L2, a batch of gathers
+// in flight at once.  Same phases, reductions, barrier and per-instance
+// logic as pcg_persistent_kernel.
 // ---------------------------------------------------------------------------
-
 template <int W, int MAXW, int SYNC = 0>
-__global__ void __launch_bounds__(W * 32)
+__global__ void __launch_bounds__(W * 32, 512 / (W * 32))  // 512 threads of rows per SM
 pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP* zp0, ZP* zp1) {
     extern __shared__ double s_mem[];
     __shared__ int s_flag;
     __shared__ int s_exit;
+    __shared__ float4 s_z[W * 32], s_p[2][W * 32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
     const int il0 = bp.cta_inst_lo[blockIdx.x], il1 = bp.cta_inst_hi[blockIdx.x];
+    const int nloc = il1 - il0 + 1;
+    const int row0 = s0 * 32, nrows = (s1 - s0) * 32;  // the CTA's rows
     double* spart = s_mem;  // [W * kSlotW]
     LocalInst* li = reinterpret_cast<LocalInst*>(s_mem + (size_t)W * kSlotW);
-    GridBarrier* gb = bp.bar;
     unsigned target = 0;
     int ph = 0;  // reduction phase (SYNC = 1 slot set ph % 3)
-    if (threadIdx.x == 0) s_flag = 0;
+    if (threadIdx.x == 0) {
+        s_flag = 0;
+        s_exit = 0;
+    }
+    init_local(bp, li, s0, s1, il0, il1);
     bool ok = true;
+    auto no_step = [](LocalInst&, const double*) {};
 
     const int s = s0 + warp;
     const bool has = s < s1;
@@ -741,6 +732,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
             }
         }
     }
+    __syncthreads();  // init_local
 
     // ---- phase 0 -------------------------------------------------------
     {
@@ -759,39 +751,26 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
                 z = mul(Mi, r);
             }
             zp0[i].z = f4(z);
+            s_z[threadIdx.x] = f4(z);
         }
         start_partials(spart + warp * kSlotW, lane == 0 && has, b, zb, x, r, z);
     }
     __syncthreads();
-    write_segment_slots<W * 32, kSlotW, SYNC>(bp, spart, s0, s1, il0, il1, ph % 3);
-    if (!SYNC) ok = grid_sync(gb, target, &s_flag);
-    if (ok) {
-        instances_start<W, SYNC>(bp, li, il0, il1, cfg, warm, ph % 3, &s_flag);
-        ++ph;
-        __syncthreads();
-        ok = s_flag == 0;
-    }
+    CHYSX_REDUCE_PHASE(kSlotW, 1, false,
+                       ([&](LocalInst& L, const double* tot) { step_start(bp, L, tot, cfg, warm); }));
+    ok = s_flag == 0;
     if (ok && warm) {
         // the scaled guess, or the zero guess where the instance fell back
         if (row) {
             start_row(li[li_idx], b, Mi, x, r, z);
             zp0[i].z = f4(z);
+            s_z[threadIdx.x] = f4(z);
         }
-        if (SYNC) {
-            // a data-free phase orders the fallback rows' z before any gather
-            if (threadIdx.x < W) spart[threadIdx.x * kSlotW] = 0.0;
-            __syncthreads();
-            write_segment_slots<W * 32, 1, 1>(bp, spart, s0, s1, il0, il1, ph % 3, li);
-            for (int bq = il0 + warp; bq <= il1; bq += W) {
-                double tot[1];
-                if (!li[bq - il0].done) instance_total<1, 1>(bp, bq, ph % 3, tot, &s_flag);
-            }
-            ++ph;
-            __syncthreads();
-            ok = s_flag == 0;
-        } else {
-            ok = grid_sync(gb, target, &s_flag);
-        }
+        // a data-free phase orders the new z before any gather
+        if (threadIdx.x < W) spart[threadIdx.x * kSlotW] = 0.0;
+        __syncthreads();
+        CHYSX_REDUCE_PHASE(1, kPollMax, false, no_step);
+        ok = s_flag == 0;
     }
 
     // ---- iterations ----------------------------------------------------
@@ -802,7 +781,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
             // leave once every instance of this CTA is done
             if (threadIdx.x == 0) {
                 int all = 1;
-                for (int bq = il0; bq <= il1; ++bq) all &= li[bq - il0].done;
+                for (int q = 0; q < nloc; ++q) all &= li[q].done;
                 s_exit = all;
             }
             __syncthreads();
@@ -817,18 +796,37 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
             ZP* En = (L.iter & 1) ? zp0 : zp1;
             p = first ? z : f3(fmaf(beta, p.x, z.x), fmaf(beta, p.y, z.y), fmaf(beta, p.z, z.z));
             En[i].p = f4(p);
+            s_p[(L.iter + 1) & 1][threadIdx.x] = f4(p);
+            const float4* sp_old = s_p[L.iter & 1];
             float3 acc = mul(D, p);
+            // gathers in batches of up to 6 entries (the valence of a
+            // triangulated grid): every load of a batch is in flight at once,
+            // padding entries read the row itself and are masked
+            constexpr int kBatch = MAXW < 6 ? MAXW : 6;
 #pragma unroll
-            for (int k = 0; k < MAXW; ++k) {
-                if (k >= w) continue;
-                const int cj = col_at(k);
-                const float4 zj = __ldcg(&E[cj].z);
-                float3 pj = xyz(zj);
-                if (!first) {
-                    const float4 po = __ldcg(&E[cj].p);
-                    pj = f3(fmaf(beta, po.x, zj.x), fmaf(beta, po.y, zj.y), fmaf(beta, po.z, zj.z));
+            for (int k0 = 0; k0 < MAXW; k0 += kBatch) {
+                if (k0 > 0 && k0 >= w) break;
+                float4 zj[kBatch], pj[kBatch];
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k) {
+                    const int cj = k0 + k < MAXW ? col_at(k0 + k) : i;
+                    const int lr = cj - row0;
+                    if ((unsigned)lr < (unsigned)nrows) {
+                        zj[k] = s_z[lr];
+                        pj[k] = sp_old[lr];
+                    } else {
+                        zj[k] = __ldcg(&E[cj].z);
+                        pj[k] = __ldcg(&E[cj].p);
+                    }
                 }
-                acc = acc + mul(B[k], pj);
+#pragma unroll
+                for (int k = 0; k < kBatch; ++k) {
+                    if (k0 + k >= w || k0 + k >= MAXW) continue;
+                    const float3 q = first ? xyz(zj[k])
+                                           : f3(fmaf(beta, pj[k].x, zj[k].x), fmaf(beta, pj[k].y, zj[k].y),
+                                                fmaf(beta, pj[k].z, zj[k].z));
+                    acc = acc + mul(B[k0 + k], q);
+                }
             }
             ap = acc;
             sig = (double)p.x * acc.x + (double)p.y * acc.y + (double)p.z * acc.z;
@@ -836,22 +834,13 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         sig = warp_sum(sig);
         if (lane == 0 && has) spart[warp * kSlotW] = sig;
         __syncthreads();
-        write_segment_slots<W * 32, 1, SYNC>(bp, spart, s0, s1, il0, il1, ph % 3, li);
-        if (!SYNC) {
-            ok = grid_sync(gb, target, &s_flag);
-            if (!ok) break;
-            if (threadIdx.x == 0) s_exit = *(volatile unsigned*)&gb->ndone >= (unsigned)bp.n_inst;
-            __syncthreads();
-            if (s_exit) break;
-        }
-
-        instances_alpha<W, SYNC>(bp, li, il0, il1, ph % 3, &s_flag);
-        ++ph;
-        __syncthreads();
-        if (SYNC && s_flag) {
+        CHYSX_REDUCE_PHASE(1, kPollMax, true, ([&](LocalInst& L, const double* tot) { step_alpha(L, tot); }));
+        if (s_flag) {
             ok = false;
             break;
         }
+        if (!SYNC && s_exit) break;
+
         double rz = 0.0, rr = 0.0;
         if (row && !li[li_idx].done) {
             const LocalInst& L = li[li_idx];
@@ -861,6 +850,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
             r = f3(fmaf(-alpha, ap.x, r.x), fmaf(-alpha, ap.y, r.y), fmaf(-alpha, ap.z, r.z));
             z = mul(Mi, r);
             En[i].z = f4(z);
+            s_z[threadIdx.x] = f4(z);
             rz = (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;
             rr = (double)r.x * r.x + (double)r.y * r.y + (double)r.z * r.z;
         }
@@ -871,15 +861,9 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
             spart[warp * kSlotW + 1] = rr;
         }
         __syncthreads();
-        write_segment_slots<W * 32, 2, SYNC>(bp, spart, s0, s1, il0, il1, ph % 3, li);
-        if (!SYNC) {
-            ok = grid_sync(gb, target, &s_flag);
-            if (!ok) break;
-        }
-        instances_beta<W, SYNC>(bp, li, il0, il1, cfg, ph % 3, &s_flag);
-        ++ph;
-        __syncthreads();
-        if (SYNC && s_flag) {
+        CHYSX_REDUCE_PHASE(2, kPollMax, false,
+                           ([&](LocalInst& L, const double* tot) { step_beta(bp, L, tot, cfg); }));
+        if (s_flag) {
             ok = false;
             break;
         }
@@ -889,9 +873,8 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         v.r[i] = f4(r);
         v.z[i] = f4(z);
     }
-    if (!ok) instances_fail(bp, li, il0, il1);
+    if (!ok) instances_fail(bp, li, nloc);
 }
-
 
 // x_{n+1} = x_n + dx, v = dx/dt * exp(-c dt) (cloth_simulator.cu:222-244) for
 // the rows of every instance whose solve finished without NaN/Inf or a
