@@ -254,15 +254,13 @@ __device__ __forceinline__ void init_local(const BatchPlan& bp, LocalInst* li, i
     }
 }
 
-// One reduction phase, run by warp 0 between two __syncthreads: sums the
-// slice partials spart[slice * kSlotW + q] (q < NV) of every unfinished
-// instance of the CTA, publishes the CTA's segment, waits for the other
-// CTAs (counter barrier or polled slots), reads each instance's total in a
-// fixed order and lets lane 0 apply `step(L, total)`.  Returns false (on all
-// lanes) after a failed wait.
-template <int NV, int SYNC, int KP, class Step>
-__device__ __forceinline__ bool warp0_phase(const BatchPlan& bp, const double* spart, LocalInst* li, int nloc,
-                                            int set, unsigned& target, Step&& step) {
+// Publication of one reduction phase, run by warp 0 after a __syncthreads:
+// sums the slice partials spart[slice * kSlotW + q] (q < NV) of every
+// unfinished instance of the CTA and stores the CTA's segment (plain store
+// in counter mode; release fence + relaxed stores in polled mode).
+template <int NV, int SYNC>
+__device__ __forceinline__ void warp0_publish(const BatchPlan& bp, const double* spart, const LocalInst* li, int nloc,
+                                              int set) {
     const int lane = threadIdx.x & 31;
     for (int t = 0; t < nloc; ++t) {
         const LocalInst& L = li[t];
@@ -288,6 +286,18 @@ __device__ __forceinline__ bool warp0_phase(const BatchPlan& bp, const double* s
             }
         }
     }
+}
+
+// One reduction phase, run by warp 0 between two __syncthreads: publishes
+// the CTA's segments, waits for the other CTAs (counter barrier or polled
+// slots), reads each instance's total in a fixed order and lets lane 0
+// apply `step(L, total)`.  For instances spanning at most 32 * KP CTAs (one
+// pass of loads).  Returns false (on all lanes) after a failed wait.
+template <int NV, int SYNC, int KP, class Step>
+__device__ __forceinline__ bool warp0_phase(const BatchPlan& bp, const double* spart, LocalInst* li, int nloc,
+                                            int set, unsigned& target, Step&& step) {
+    const int lane = threadIdx.x & 31;
+    warp0_publish<NV, SYNC>(bp, spart, li, nloc, set);
     if (!SYNC) {
         bool ok = true;
         if (lane == 0) ok = barrier_arrive_wait(bp.bar, target);
@@ -328,6 +338,109 @@ __device__ __forceinline__ bool warp0_phase(const BatchPlan& bp, const double* s
         __syncwarp();
     }
     return true;
+}
+
+// The same phase with the whole CTA reading the slots, for instances that
+// span many CTAs (the streamed kernel runs up to ~1200): thread j reads (or
+// polls) slots slot_lo + j + BLOCK * i, i < KB, all in flight at once, sums
+// them in ascending order into red[j], and warp 0 adds red[] in a fixed
+// order (lane-strided, then an xor tree).  Called by every thread after the
+// __syncthreads that follows the partials; ends with a __syncthreads and
+// leaves s_flag = 1 after a failed wait.  Both modes sum in the same order.
+template <int NV, int SYNC, int BLOCK, int KB, class Step>
+__device__ __forceinline__ void block_phase(const BatchPlan& bp, const double* spart, LocalInst* li, int nloc,
+                                            int set, unsigned& target, double* red, int* s_flag, Step&& step) {
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid < 32) {
+        warp0_publish<NV, SYNC>(bp, spart, li, nloc, set);
+        if (!SYNC && lane == 0 && !barrier_arrive_wait(bp.bar, target)) *s_flag = 1;
+    }
+    __syncthreads();
+    if (*s_flag) return;
+    for (int t = 0; t < nloc; ++t) {
+        LocalInst& L = li[t];
+        if (L.done) continue;  // uniform: li is only written between barriers
+        double acc[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+        bool ok = true;
+        const unsigned long long* fbase = bp.fslots + (size_t)set * bp.n_slots * kSlotW;
+        for (int c0 = L.slot_lo; c0 < L.slot_hi && ok; c0 += BLOCK * KB) {
+            unsigned long long val[KB][NV];
+#pragma unroll
+            for (int j = 0; j < KB; ++j) {
+                const int k = c0 + j * BLOCK + tid;
+#pragma unroll
+                for (int q = 0; q < NV; ++q) {
+                    if (k >= L.slot_hi) val[j][q] = 0ull;
+                    else if (SYNC) val[j][q] = ld_relaxed_u64(fbase + (size_t)k * kSlotW + q);
+                    else val[j][q] = (unsigned long long)__double_as_longlong(__ldcg(bp.slots + (size_t)k * kSlotW + q));
+                }
+            }
+            if (SYNC) {
+                const unsigned long long t0 = global_ns();
+                unsigned spins = 0;
+                while (true) {
+                    bool pending = false;
+#pragma unroll
+                    for (int j = 0; j < KB; ++j) {
+                        const int k = c0 + j * BLOCK + tid;
+#pragma unroll
+                        for (int q = 0; q < NV; ++q) {
+                            if (val[j][q] == kSlotEmpty) {
+                                pending = true;
+                                val[j][q] = ld_relaxed_u64(fbase + (size_t)k * kSlotW + q);
+                            }
+                        }
+                    }
+                    if (!pending) break;
+                    if ((++spins & 63u) == 0) {
+                        if (*(volatile int*)&bp.bar->error) { ok = false; break; }
+                        if (global_ns() - t0 > kBarrierTimeoutNs) {
+                            atomicExch(&bp.bar->error, 1);
+                            ok = false;
+                            break;
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < KB; ++j) {
+                if (c0 + j * BLOCK + tid < L.slot_hi) {
+#pragma unroll
+                    for (int q = 0; q < NV; ++q) acc[q] += __longlong_as_double((long long)val[j][q]);
+                }
+            }
+        }
+        if (SYNC) fence_acq_rel_gpu();  // acquire: the publishers' data is visible from here on
+        if (!ok) *s_flag = 1;
+#pragma unroll
+        for (int q = 0; q < NV; ++q) red[tid * NV + q] = acc[q];
+        __syncthreads();
+        if (*s_flag) return;
+        if (tid < 32) {
+            double tot[NV];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) tot[q] = 0.0;
+            for (int j = lane; j < BLOCK; j += 32) {
+#pragma unroll
+                for (int q = 0; q < NV; ++q) tot[q] += red[j * NV + q];
+            }
+#pragma unroll
+            for (int q = 0; q < NV; ++q) tot[q] = warp_sum(tot[q]);
+            if (lane == 0) {
+                if (SYNC) {
+                    // this CTA's slot of the previous phase can be reused
+                    unsigned long long* d =
+                        bp.fslots + ((size_t)((set + 2) % 3) * bp.n_slots + L.own_slot) * kSlotW;
+#pragma unroll
+                    for (int q = 0; q < kSlotW; ++q) st_relaxed_u64(d + q, kSlotEmpty);
+                }
+                step(L, tot);
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // Start partials of one row, kSlotW wide: r.z, r.r, b.b, b.M^-1 b, x0.b,
@@ -480,6 +593,16 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
         __syncthreads();                                                                             \
     } while (0)
 
+// The same protocol with block_phase (the whole CTA reads the totals).
+#define CHYSX_BLOCK_PHASE(NV, KB, exit_test, STEP)                                                   \
+    do {                                                                                             \
+        block_phase<NV, SYNC, BLOCK, KB>(bp, spart, li, nloc, ph % 3, target, s_red, &s_flag, STEP);  \
+        if (!SYNC && (exit_test) && threadIdx.x == 0 && !s_flag)                                     \
+            s_exit = *(volatile unsigned*)&bp.bar->ndone >= (unsigned)bp.n_inst;                    \
+        ++ph;                                                                                        \
+        __syncthreads();                                                                             \
+    } while (0)
+
 // ---------------------------------------------------------------------------
 // Streamed persistent kernel: rows are re-read from HBM every iteration.
 // ---------------------------------------------------------------------------
@@ -489,6 +612,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
     extern __shared__ double s_mem[];
     __shared__ int s_flag;
     __shared__ int s_exit;
+    __shared__ double s_red[BLOCK * kSlotW];  // per-thread slot sums of block_phase
     constexpr int W = BLOCK / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
@@ -538,8 +662,8 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
         start_partials(spart + (s - s0) * kSlotW, lane == 0, b, zb, x0, r, z);
     }
     __syncthreads();
-    CHYSX_REDUCE_PHASE(kSlotW, 1, false,
-                       ([&](LocalInst& L, const double* tot) { step_start(bp, L, tot, cfg, warm); }));
+    CHYSX_BLOCK_PHASE(kSlotW, 1, false,
+                      ([&](LocalInst& L, const double* tot) { step_start(bp, L, tot, cfg, warm); }));
     ok = s_flag == 0;
     if (ok && warm) {
         // the scaled guess, or the zero guess where the instance fell back
@@ -556,7 +680,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
         // a data-free phase orders the new rows before any gather
         for (int q = threadIdx.x; q < s1 - s0; q += BLOCK) spart[q * kSlotW] = 0.0;
         __syncthreads();
-        CHYSX_REDUCE_PHASE(1, kPollMax, false, no_step);
+        CHYSX_BLOCK_PHASE(1, 5, false, no_step);
         ok = s_flag == 0;
     }
 
@@ -616,7 +740,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
         __syncthreads();
         // ndone only changes in the start and beta steps, i.e. never between
         // this barrier and the next, so every CTA takes the same exit decision
-        CHYSX_REDUCE_PHASE(1, kPollMax, true, ([&](LocalInst& L, const double* tot) { step_alpha(L, tot); }));
+        CHYSX_BLOCK_PHASE(1, 5, true, ([&](LocalInst& L, const double* tot) { step_alpha(L, tot); }));
         if (s_flag) {
             ok = false;
             break;
@@ -650,8 +774,8 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
         }
         __syncthreads();
         // phase 3: beta, iteration count, convergence
-        CHYSX_REDUCE_PHASE(2, kPollMax, false,
-                           ([&](LocalInst& L, const double* tot) { step_beta(bp, L, tot, cfg); }));
+        CHYSX_BLOCK_PHASE(2, 5, false,
+                          ([&](LocalInst& L, const double* tot) { step_beta(bp, L, tot, cfg); }));
         if (s_flag) {
             ok = false;
             break;

@@ -80,18 +80,25 @@ def read_peaks():
         return 6650.0, "fallback"
 
 
-def read_traffic(workload_name):
-    """Per-iteration DRAM bytes of the PCG kernel from the committed ncu
-    summary for this workload, if one exists (profiles/pcg_<workload>.txt
-    carries a line `dram_bytes_per_iteration: <int>`)."""
-    path = os.path.join(ROOT, "profiles", f"pcg_persistent_{workload_name}.txt")
+def read_traffic(kernel, workload_name):
+    """DRAM bytes of one PCG launch as (fixed part, part per iteration) from
+    the committed ncu summary for this kernel and workload, if one exists
+    (profiles/pcg_<kernel>_<workload>.md carries the lines
+    `dram_bytes_per_launch: <number>` and `dram_bytes_per_iteration:
+    <number>`), else None."""
+    path = os.path.join(ROOT, "profiles", f"pcg_{kernel}_{workload_name}.md")
+    fixed = per_it = None
     try:
         for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                fixed = float(line.split(":", 1)[1])
             if line.startswith("dram_bytes_per_iteration:"):
-                return float(line.split(":", 1)[1])
+                per_it = float(line.split(":", 1)[1])
     except OSError:
-        pass
-    return None
+        return None
+    if fixed is None and per_it is None:
+        return None
+    return (fixed or 0.0, per_it or 0.0)
 
 
 # ---------------------------------------------------------------------------
@@ -427,7 +434,7 @@ def run_ours(args, rank, world, local_rank):
     achieved = float(np.sum(moved) / (np.sum(solve_ms) * 1e-3) / 1e9)
     achieved_ref = float(np.sum(moved_ref) / (np.sum(solve_ms) * 1e-3) / 1e9)
     peak, peak_kind = read_peaks()
-    traffic_it = read_traffic(args.workload)
+    traffic_it = read_traffic(g.sim.solver_info()[0], args.workload)
     steps_total = args.steps * world
     value = steps_total / (total_ms_max * 1e-3)
     mean_iters = float(iters.mean())
@@ -471,7 +478,7 @@ def run_ours(args, rank, world, local_rank):
                                                 "loop": "pcg_spmv_kernel+pcg_update_kernel"}[g.sim.solver_info()[0]],
                      "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": (traffic_it * mean_iters) if traffic_it else None,
+                     "traffic": (traffic_it[0] + traffic_it[1] * mean_iters) if traffic_it else None,
                      "algorithmic_bytes_per_launch": float(np.mean(moved)),
                      "algorithmic_bytes_per_iteration": b_it,
                      "reference_format_bytes_per_iteration": b_ref,
