@@ -49,6 +49,7 @@ SIGNATURES = {
     "chysx_cloth_build_springs": (ctypes.c_int, [H, ctypes.c_float, f32p, u]),
     "chysx_cloth_num_springs": (ctypes.c_int, [H, ip]),
     "chysx_cloth_build_fem_stretch": (ctypes.c_int, [H, ctypes.c_float, f32p, u]),
+    "chysx_cloth_build_fem_shear": (ctypes.c_int, [H, ctypes.c_float, f32p, u]),
     "chysx_cloth_redistribute_mass": (ctypes.c_int, [H, ctypes.c_float, u, ctypes.c_int, u]),
     "chysx_cloth_set_pcg_iterations": (ctypes.c_int, [H, ctypes.c_int]),
     "chysx_cloth_pcg_iterations": (ctypes.c_int, [H, ip]),
@@ -181,6 +182,13 @@ class Cloth:
             check(self._L.chysx_cloth_build_fem_stretch(self.h, 0.0, _p(kt, f32p), stream))
         else:
             check(self._L.chysx_cloth_build_fem_stretch(self.h, float(k), _p(None, f32p), stream))
+
+    def build_fem_shear(self, k, stream=0):
+        if np.ndim(k):
+            kt = np.ascontiguousarray(k, np.float32)
+            check(self._L.chysx_cloth_build_fem_shear(self.h, 0.0, _p(kt, f32p), stream))
+        else:
+            check(self._L.chysx_cloth_build_fem_shear(self.h, float(k), _p(None, f32p), stream))
 
     def redistribute_mass(self, density, inv_mass_ptr, n, stream=0):
         check(self._L.chysx_cloth_redistribute_mass(self.h, density, inv_mass_ptr, n, stream))

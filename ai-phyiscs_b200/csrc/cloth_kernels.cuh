@@ -44,14 +44,19 @@ struct DevTopo {
 
 struct ElemData {
     const int* __restrict__ tris;      // 3 per triangle
-    const float4* __restrict__ dminv;  // row-major 2x2 (Mat2f layout)
+    const float4* __restrict__ dminv;  // stretch: row-major 2x2 (Mat2f layout)
     const float* __restrict__ area;
     const float* __restrict__ ktri;
+    const float4* __restrict__ dminv_s;  // shear: the same with the material axes turned by pi/4
+    const float* __restrict__ area_s;
+    const float* __restrict__ ktri_s;
     const int* __restrict__ edges;     // 2 per edge
     const float* __restrict__ rest;
     const float* __restrict__ kedge;
     float pin_k;
-    int use_tris;
+    int use_tris;     // triangles in the Hessian pattern (stretch or shear)
+    int use_stretch;
+    int use_shear;
     int use_springs;
 };
 
@@ -245,17 +250,21 @@ __device__ __forceinline__ void spring_row(const ElemData& el, const float* pos,
 // gradient triangle_stretch_constraint.cu:153-217, Hessian :231-311 written
 // as H_ab = dwu_a dwu_b Mu + dwv_a dwv_b Mv with
 //   Mu = k_eff (u u^T + [cu > 0] cu/lu (I - u u^T)), Mv likewise.
+// Shear is the same element with the material axes turned by pi/4 in the
+// rest shape (cloth_simulator.cu:423-449, triangle_stretch_constraint.cu:
+// 87-109), i.e. a second (Dm^-1, area, k) set over the same triangles.
 struct TriRow {
     float3 g;       // gradient at the row's vertex
     S6 Mu, Mv;
     float du[3], dv[3];
 };
 
-__device__ __forceinline__ void tri_row(const ElemData& el, const float* pos, int t, int la,
-                                        TriRow& o) {
+__device__ __forceinline__ void tri_row(const ElemData& el, const float4* __restrict__ dminv,
+                                        const float* __restrict__ area, const float* __restrict__ ktri,
+                                        const float* pos, int t, int la, TriRow& o) {
     const int v0 = el.tris[3 * t], v1 = el.tris[3 * t + 1], v2 = el.tris[3 * t + 2];
     const float3 x0 = ld3(pos, v0), x1 = ld3(pos, v1), x2 = ld3(pos, v2);
-    const float4 Dm = el.dminv[t];  // (0,0) (0,1) (1,0) (1,1)
+    const float4 Dm = dminv[t];  // (0,0) (0,1) (1,0) (1,1)
     const float3 a = x1 - x0, b = x2 - x0;
     const float3 wu = a * Dm.x + b * Dm.z;
     const float3 wv = a * Dm.y + b * Dm.w;
@@ -267,7 +276,7 @@ __device__ __forceinline__ void tri_row(const ElemData& el, const float* pos, in
     const float3 uh = wu * inv_lu, vh = wv * inv_lv;
     o.du[0] = -Dm.x - Dm.z; o.du[1] = Dm.x; o.du[2] = Dm.z;
     o.dv[0] = -Dm.y - Dm.w; o.dv[1] = Dm.y; o.dv[2] = Dm.w;
-    const float k_eff = el.area[t] * el.ktri[t];
+    const float k_eff = area[t] * ktri[t];
     const float dua = la == 0 ? o.du[0] : (la == 1 ? o.du[1] : o.du[2]);
     const float dva = la == 0 ? o.dv[0] : (la == 1 ? o.dv[1] : o.dv[2]);
     o.g = (uh * (cu * dua) + vh * (cv * dva)) * k_eff;
@@ -379,17 +388,20 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
                 else smem_acc6(s_off + tid, BLOCK, (int)slot, -1.0f, H);
             }
         }
-        // Baraff-Witkin stretch
+        // Baraff-Witkin stretch, then shear, per incident triangle
         if (el.use_tris) {
             const int o = t.tinc_off[s];
             const int wt = (t.tinc_off[s + 1] - o) >> 5;
             for (int k = 0; k < wt; ++k) {
-                const int tri = t.tinc[o + k * 32 + lane];
-                if (tri < 0) continue;
-                const unsigned meta = t.tinc_meta[o + k * 32 + lane];
-                const int la = (int)(meta & 3u);
+              const int tri = t.tinc[o + k * 32 + lane];
+              if (tri < 0) continue;
+              const unsigned meta = t.tinc_meta[o + k * 32 + lane];
+              const int la = (int)(meta & 3u);
+              for (int set = 0; set < 2; ++set) {
+                if (set == 0 ? !el.use_stretch : !el.use_shear) continue;
                 TriRow tr;
-                tri_row(el, a.pos, tri, la, tr);
+                if (set == 0) tri_row(el, el.dminv, el.area, el.ktri, a.pos, tri, la, tr);
+                else tri_row(el, el.dminv_s, el.area_s, el.ktri_s, a.pos, tri, la, tr);
                 g = g + tr.g;
                 const float dua = sel3(tr.du, la), dva = sel3(tr.dv, la);
                 axpy6(D, dua * dua, tr.Mu);
@@ -407,6 +419,7 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
                         smem_acc6(s_off + tid, BLOCK, (int)slot, cv_, tr.Mv);
                     }
                 }
+              }
             }
         }
         // RHS and inertia

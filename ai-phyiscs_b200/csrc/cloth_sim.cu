@@ -390,6 +390,38 @@ public:
         ck(cudaGetLastError(), "rest_shape_kernel launch");
     }
 
+    // ClothSimulator::build_fem_shear_from_current_positions
+    // (cloth_simulator.cu:423-449): the stretch element over the same
+    // triangles with its rest frame turned by pi/4, a second (Dm^-1, area,
+    // k) set assembled beside the stretch set.
+    void build_shear(float k, const float* k_per_tri, uintptr_t stream) {
+        const int T = (int)(tris_.size() / 3);
+        shear_built_ = true;
+        topo_dirty_ = true;
+        if (T == 0) {
+            d_dminv_s_.reset();
+            d_area_s_.reset();
+            d_ktri_s_.reset();
+            return;
+        }
+        if (!pos_)
+            throw std::runtime_error(
+                "ClothSimulator::build_fem_shear_from_current_positions: external positions must be "
+                "set first via set_external_buffers().");
+        check_indices(tris_, "triangle");
+        ensure_mesh_on_device();
+        std::vector<float> kt(T, k);
+        if (k_per_tri) std::memcpy(kt.data(), k_per_tri, T * sizeof(float));
+        d_ktri_s_.upload(kt);
+        d_dminv_s_.resize(T);
+        d_area_s_.resize(T);
+        const float quarter_pi = 0.7853981633974483f;
+        rest_shape_kernel<<<grid_for(T, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+            d_tris_.get(), reinterpret_cast<const float*>(pos_), d_dminv_s_.get(), d_area_s_.get(), T,
+            det_eps_, std::cos(quarter_pi), std::sin(quarter_pi));
+        ck(cudaGetLastError(), "rest_shape_kernel launch (shear)");
+    }
+
     // ---- mass ----------------------------------------------------------
     void redistribute_mass(float rho, uintptr_t inv_mass, int count, uintptr_t stream) {
         if (count <= 0) return;
@@ -757,7 +789,9 @@ private:
     }
 
     void rebuild_topology() {
-        const bool use_tris = stretch_built_ && d_dminv_.size() > 0;
+        const bool use_stretch = stretch_built_ && d_dminv_.size() > 0;
+        const bool use_shear = shear_built_ && d_dminv_s_.size() > 0;
+        const bool use_tris = use_stretch || use_shear;
         const bool use_springs = springs_built_ && springs_in_step_ && d_rest_.size() > 0;
         if (!inst_offsets_.empty() && inst_offsets_.back() != n_)
             throw std::invalid_argument("set_instances: offsets do not cover the particle count");
@@ -765,6 +799,8 @@ private:
         if (topo_.row_to_ext.empty()) d_row_to_ext_.reset();
         else d_row_to_ext_.upload(topo_.row_to_ext);
         use_tris_ = use_tris;
+        use_stretch_ = use_stretch;
+        use_shear_ = use_shear;
         use_springs_ = use_springs;
         d_slice_off_.upload(topo_.slice_off);
         d_col_.upload(topo_.col);
@@ -833,11 +869,16 @@ private:
         e.dminv = d_dminv_.get();
         e.area = d_area_.get();
         e.ktri = d_ktri_.get();
+        e.dminv_s = d_dminv_s_.get();
+        e.area_s = d_area_s_.get();
+        e.ktri_s = d_ktri_s_.get();
         e.edges = d_edges_.get();
         e.rest = d_rest_.get();
         e.kedge = d_kedge_.get();
         e.pin_k = pin_k_;
         e.use_tris = use_tris_ ? 1 : 0;
+        e.use_stretch = use_stretch_ ? 1 : 0;
+        e.use_shear = use_shear_ ? 1 : 0;
         e.use_springs = use_springs_ ? 1 : 0;
         return e;
     }
@@ -1303,9 +1344,9 @@ private:
     int vt_n_ = -1;
     bool mesh_on_device_ = false;
     // elements
-    bool springs_built_ = false, stretch_built_ = false;
-    DevBuf<float> d_rest_, d_kedge_, d_area_, d_ktri_;
-    DevBuf<float4> d_dminv_;
+    bool springs_built_ = false, stretch_built_ = false, shear_built_ = false;
+    DevBuf<float> d_rest_, d_kedge_, d_area_, d_ktri_, d_area_s_, d_ktri_s_;
+    DevBuf<float4> d_dminv_, d_dminv_s_;
     std::vector<int> pin_idx_;
     std::vector<float> pin_tgt_;
     float pin_k_ = 1.0e6f;
@@ -1316,7 +1357,7 @@ private:
     double rel_tol_ = 0.0;
     int warm_mode_ = CHYSX_WARM_PREVIOUS;
     // topology + system
-    bool topo_dirty_ = true, use_tris_ = false, use_springs_ = false;
+    bool topo_dirty_ = true, use_tris_ = false, use_stretch_ = false, use_shear_ = false, use_springs_ = false;
     HostTopology topo_;
     DevBuf<int> d_slice_off_, d_col_, d_tinc_off_, d_tinc_, d_sinc_off_, d_sinc_, d_pin_off_, d_pin_row_;
     DevBuf<unsigned> d_tinc_meta_, d_sinc_meta_;
@@ -1484,6 +1525,10 @@ int chysx_cloth_num_springs(const chysx_cloth* h, int* out) {
 int chysx_cloth_build_fem_stretch(chysx_cloth* h, float k, const float* k_per_tri, uintptr_t stream) {
     CHYSX_H(h);
     return guard([&] { h->sim.build_stretch(k, k_per_tri, stream); });
+}
+int chysx_cloth_build_fem_shear(chysx_cloth* h, float k, const float* k_per_tri, uintptr_t stream) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.build_shear(k, k_per_tri, stream); });
 }
 int chysx_cloth_redistribute_mass(chysx_cloth* h, float rho, uintptr_t inv_mass, int n, uintptr_t stream) {
     CHYSX_H(h);

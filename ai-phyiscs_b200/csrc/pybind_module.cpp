@@ -155,6 +155,17 @@ PYBIND11_MODULE(_chysx_native, m) {
                  }
              },
              py::arg("stiffness"), py::arg("cuda_stream") = 0)
+        .def("build_fem_shear_from_current_positions",
+             [](PyClothSimulator& s, py::object stiffness, std::uintptr_t stream) {
+                 if (py::isinstance<py::array>(stiffness)) {
+                     F32 k = stiffness.cast<F32>();
+                     if (k.ndim() != 1) throw py::value_error("per-triangle stiffness must be 1-D");
+                     check(chysx_cloth_build_fem_shear(s.h(), 0.0f, k.data(), stream));
+                 } else {
+                     check(chysx_cloth_build_fem_shear(s.h(), stiffness.cast<float>(), nullptr, stream));
+                 }
+             },
+             py::arg("stiffness"), py::arg("cuda_stream") = 0)
         .def("set_pcg_iterations",
              [](PyClothSimulator& s, int m) { check(chysx_cloth_set_pcg_iterations(s.h(), m)); }, py::arg("max_iter"))
         .def("pcg_iterations",

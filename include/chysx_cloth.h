@@ -117,6 +117,14 @@ int chysx_cloth_num_springs(const chysx_cloth* h, int* out);
 int chysx_cloth_build_fem_stretch(chysx_cloth* h, float stiffness, const float* k_per_tri,
                                   uintptr_t stream);
 
+/* ClothSimulator::build_fem_shear_from_current_positions:
+ * src/cloth/cloth_simulator.cu:423-449.  The stretch element with its rest
+ * frame turned by pi/4 (triangle_stretch_constraint.cu:87-109), assembled
+ * beside the stretch set; k_per_tri (host, may be NULL) overrides the scalar
+ * per-area stiffness per triangle. */
+int chysx_cloth_build_fem_shear(chysx_cloth* h, float stiffness, const float* k_per_tri,
+                                uintptr_t stream);
+
 /* ClothSimulator::redistribute_mass_area_weighted:
  * src/cloth/cloth_simulator.cu:516-575.  Writes the caller's inv_mass. */
 int chysx_cloth_redistribute_mass(chysx_cloth* h, float surface_density, uintptr_t inv_mass,

@@ -50,6 +50,7 @@ def lib():
         L.orc_get_edges.argtypes = [vp, _i32p]
         L.orc_build_springs.argtypes = [vp, ctypes.c_float, _f32p]
         L.orc_build_stretch.argtypes = [vp, ctypes.c_float, _f32p, ctypes.c_float]
+        L.orc_build_shear.argtypes = [vp, ctypes.c_float, _f32p]
         L.orc_redistribute_mass.argtypes = [vp, ctypes.c_float, _f32p]
         L.orc_set_pins.argtypes = [vp, _i32p, _f32p, ctypes.c_int, ctypes.c_float]
         L.orc_set_options.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double]
@@ -140,6 +141,10 @@ class OracleCloth:
             ke = np.ascontiguousarray(k, np.float32)
             k = 0.0
         _check(self._L.orc_build_springs(self._h, float(k), _p(ke, _f32p)))
+
+    def build_shear(self, k):
+        kt = np.ascontiguousarray(k, np.float32) if np.ndim(k) else None
+        _check(self._L.orc_build_shear(self._h, 0.0 if np.ndim(k) else float(k), _p(kt, _f32p)))
 
     def build_stretch(self, k, theta=0.0):
         kt = None
@@ -245,6 +250,8 @@ def run_scene(scene, steps=None, fp64=True, rel_tol=None, max_iter=None, warm_st
         sim.build_springs(scene["k_spring"])
     if scene.get("k_stretch") is not None:
         sim.build_stretch(scene["k_stretch"])
+    if scene.get("k_shear") is not None:
+        sim.build_shear(scene["k_shear"])
     if len(scene["pin_idx"]):
         sim.set_pins(scene["pin_idx"], scene["pin_targets"], scene.get("k_pin", 1.0e6))
     sim.set_solver(max_iter=max_iter if max_iter is not None else scene["max_iter"],

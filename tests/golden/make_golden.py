@@ -45,6 +45,8 @@ def run_reference(mod, sc, pcg_iters, steps, dump_at=()):
     s.redistribute_mass_area_weighted(sc["density"], inv.data_ptr(), n)
     s.build_springs_from_current_positions(float(sc["k_spring"]))
     s.build_fem_stretch_from_current_positions(float(sc["k_stretch"]))
+    if sc.get("k_shear") is not None:
+        s.build_fem_shear_from_current_positions(float(sc["k_shear"]))
     s.set_pins(sc["pin_idx"].astype(np.int32), sc["pin_targets"].astype(np.float32), float(sc["k_pin"]))
     s.set_pcg_iterations(pcg_iters)
     torch.cuda.synchronize()
@@ -73,6 +75,21 @@ def scene_grid16():
     return sc
 
 
+def scene_grid10_shear():
+    """Config 1 with a Baraff-Witkin shear set (k = 5e3) beside the stretch set."""
+    sc = scenes.config_small(steps=60)
+    sc["k_shear"] = 5.0e3
+    return sc
+
+
+def make_shear(out_dir=HERE):
+    import _chysx_ref_springs as mod
+
+    a = run_reference(mod, scene_grid10_shear(), 1000, 60, dump_at=(0, 30))
+    np.savez_compressed(os.path.join(out_dir, "ref_grid10_shear.npz"), **a)
+    print("grid10 shear done", flush=True)
+
+
 def main(out_dir=HERE):
     os.makedirs(out_dir, exist_ok=True)
     import _chysx_ref  # noqa: F401
@@ -92,7 +109,13 @@ def main(out_dir=HERE):
     a = run_reference(mods["springs"], g, 2000, 40, dump_at=(0, 20, 39))
     np.savez_compressed(os.path.join(out_dir, "ref_grid16_springs.npz"), **a)
     print("grid16 done", flush=True)
+    make_shear(out_dir)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else HERE)
+    # python make_golden.py [out_dir] [shear]   ("shear": only the shear fixture)
+    out = sys.argv[1] if len(sys.argv) > 1 else HERE
+    if len(sys.argv) > 2 and sys.argv[2] == "shear":
+        make_shear(out)
+    else:
+        main(out)

@@ -5,8 +5,8 @@ import numpy as np
 import pytest
 
 import oracle.oracle as O
-from golden_util import (DUMPS, TOL_BLOCK_REL, TOL_DX_CONVERGED, TOL_RHS_ABS, TOL_TRAJ, load, rel,
-                         scene_for)
+from golden_util import (DUMPS, TOL_BLOCK_REL, TOL_DX_CONVERGED, TOL_RHS_ABS, TOL_TRAJ, TRAJECTORIES, load,
+                         rel, scene_for)
 
 
 def oracle_from(sc, fx, pre, springs, fp64=True, tol=1e-12, iters=20000, warm="zero"):
@@ -17,6 +17,8 @@ def oracle_from(sc, fx, pre, springs, fp64=True, tol=1e-12, iters=20000, warm="z
     s.set_options(springs, False, 1e-6)
     s.build_springs(float(sc["k_spring"]))
     s.build_stretch(float(sc["k_stretch"]))
+    if sc.get("k_shear") is not None:
+        s.build_shear(float(sc["k_shear"]))
     s.set_pins(sc["pin_idx"], sc["pin_targets"], sc["k_pin"])
     s.set_solver(iters, tol, warm)
     return s
@@ -51,8 +53,7 @@ def test_oracle_system_matches_reference(fixture, pre, springs, steps, converged
             assert np.abs(fx[f"{pre}s{k}_dx"] - dx).max() < TOL_DX_CONVERGED
 
 
-@pytest.mark.parametrize("fixture,pre,steps", [("ref_grid10_springs.npz", "it1000_", 200),
-                                               ("ref_grid16_springs.npz", "", 40)])
+@pytest.mark.parametrize("fixture,pre,steps", TRAJECTORIES)
 def test_oracle_trajectory_matches_reference(fixture, pre, steps):
     fx = load(fixture)
     sc = scene_for(fixture)

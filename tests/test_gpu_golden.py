@@ -7,8 +7,8 @@ import pytest
 
 from chysx import capi
 from chysx.runner import GpuCloth
-from golden_util import (DUMPS, TOL_BLOCK_REL, TOL_DX_CONVERGED, TOL_RHS_ABS, TOL_TRAJ_FP32, load, rel,
-                         scene_for)
+from golden_util import (DUMPS, TOL_BLOCK_REL, TOL_DX_CONVERGED, TOL_RHS_ABS, TOL_TRAJ_FP32, TRAJECTORIES,
+                         load, rel, scene_for)
 
 pytestmark = pytest.mark.gpu
 
@@ -45,8 +45,7 @@ def test_cuda_system_matches_reference(fixture, pre, springs, steps, converged, 
             assert np.abs(dx - fx[f"{pre}s{k}_dx"]).max() < TOL_DX_CONVERGED
 
 
-@pytest.mark.parametrize("fixture,pre,steps", [("ref_grid10_springs.npz", "it1000_", 200),
-                                               ("ref_grid16_springs.npz", "", 40)])
+@pytest.mark.parametrize("fixture,pre,steps", TRAJECTORIES)
 def test_cuda_trajectory_matches_reference(fixture, pre, steps):
     fx = load(fixture)
     sc = scene_for(fixture)

@@ -49,6 +49,8 @@ def oracle_sim(sc, fp64=True, tol=1e-10, max_iter=20000, warm="zero", springs_in
         s.build_springs(sc["k_spring"])
     if sc.get("k_stretch") is not None:
         s.build_stretch(sc["k_stretch"])
+    if sc.get("k_shear") is not None:
+        s.build_shear(sc["k_shear"])
     if len(sc["pin_idx"]):
         s.set_pins(sc["pin_idx"], sc["pin_targets"], sc.get("k_pin", 1e6))
     s.set_solver(max_iter, tol, warm)
@@ -78,6 +80,44 @@ def test_first_step_system_and_solution_match_oracle(path):
     # shows the same 1e-4 N spread): compare absolutely
     assert np.abs(rhs - orhs).max() < 5e-4
     assert np.abs(dx - odx).max() < 1e-6   # metres
+
+
+def shear_scene(steps=20, stretch=True):
+    """Config 1 with a Baraff-Witkin shear set (k = 5e3), with or without the
+    stretch set; the corner-pinned patch shears as it swings down."""
+    sc = scenes.config_small(steps=steps)
+    sc["k_shear"] = 5.0e3
+    if not stretch:
+        sc["k_stretch"] = None
+    return sc
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("stretch", [True, False])
+def test_shear_system_and_trajectory_match_oracle(path, stretch):
+    sc = shear_scene(stretch=stretch)
+    g = make(sc, path, max_iter=5000, rel_tol=1e-8)
+    o = oracle_sim(sc, tol=1e-10, max_iter=5000)
+    inv = g.inv_mass.cpu().numpy()
+    for k in range(20):
+        if k == 5:
+            # the system assembled from the GPU's own state (a deformed one)
+            one = oracle_sim(sc, tol=1e-10, max_iter=5000)
+            one.set_state(g.positions().astype(np.float32), g.velocities().astype(np.float32), inv)
+            one.step(sc["dt"])
+        g.step()
+        o.step(sc["dt"])
+        if k == 5:
+            diag, rp, col, vals, rhs, dx = g.dump()
+            od, orp, ocol, ovals, orhs, odx = one.dump_system()
+            np.testing.assert_array_equal(rp, orp)
+            np.testing.assert_array_equal(col, ocol)
+            assert rel(diag, od) < 2e-6
+            assert rel(vals, ovals) < 2e-6
+            assert np.abs(rhs - orhs).max() < 5e-4
+    assert g.stats()[2] == capi.SOLVE_CONVERGED
+    # the 20-step FP32 floor of config 1 (see module docstring)
+    assert np.abs(g.positions() - o.state()[0]).max() < 1e-4
 
 
 @pytest.mark.parametrize("path", PATHS)

@@ -202,6 +202,60 @@ def test_scaled_warm_start_minimises_energy_along_the_guess():
     assert energy(xs) <= 1e-15 * abs(energy(x0))
 
 
+def _shear_sim(sc, shear_as_stretch):
+    """Springs + a Baraff-Witkin set turned by pi/4: either through the shear
+    entry point, or as the stretch set built with theta = pi/4."""
+    n = sc["pos"].shape[0]
+    sim = O.OracleCloth(True)
+    sim.set_material(sc["density"], 0.0, sc["gravity"])
+    sim.set_state(sc["pos"], sc["vel"], np.ones(n, np.float32))
+    sim.set_mesh(sc["tris"])
+    sim.set_options(True, False, 1e-6)
+    im = sim.redistribute_mass(sc["density"])
+    sim.set_state(sc["pos"], sc["vel"], im)
+    sim.build_springs(sc["k_spring"])
+    if shear_as_stretch:
+        sim.build_stretch(4.0e3, theta=float(np.float32(np.pi / 4)))
+    else:
+        sim.build_shear(4.0e3)
+    sim.set_pins(sc["pin_idx"], sc["pin_targets"])
+    sim.set_solver(5000, 1e-10, "zero")
+    return sim
+
+
+def test_shear_set_is_the_stretch_element_turned_by_a_quarter_turn():
+    # cloth_simulator.cu:423-449: shear = stretch energy on rest axes turned by pi/4
+    sc = scenes.config_small(side=6)
+    a, b = _shear_sim(sc, False), _shear_sim(sc, True)
+    for _ in range(4):
+        a.step(sc["dt"])
+        b.step(sc["dt"])
+    for x, y in zip(a.dump_system(), b.dump_system()):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_shear_resists_pure_shear_that_stretch_ignores():
+    # unit right triangle, simple shear x' = x + g y: the axis-aligned stretch
+    # element sees |F e_u| = 1, |F e_v| = sqrt(1 + g^2) > 1; the quarter-turned
+    # one sees both diagonals change length, so its energy is larger and its
+    # gradient pulls the sheared vertex back
+    x = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float64)
+    g = 0.2
+    y = x.copy()
+    y[2, 0] += g
+    dm0, a0 = O.rest_shape(x, 1e-6, 0.0)
+    dm4, a4 = O.rest_shape(x, 1e-6, float(np.pi / 4))
+    e0, g0, _ = O.triangle_eval(y, dm0, a0, 1.0)
+    e4, g4, _ = O.triangle_eval(y, dm4, a4, 1.0)
+    lu = np.hypot(1 + 0.0, 0.0)
+    lv = np.hypot(g, 1.0)
+    assert e0 == pytest.approx(0.5 * a0 * (lu - 1) ** 2 + 0.5 * a0 * (lv - 1) ** 2, rel=1e-9)
+    d1 = np.linalg.norm((y[1] - y[0]) / np.sqrt(2) + (y[2] - y[0]) / np.sqrt(2))
+    d2 = np.linalg.norm(-(y[1] - y[0]) / np.sqrt(2) + (y[2] - y[0]) / np.sqrt(2))
+    assert e4 == pytest.approx(0.5 * a4 * ((d1 - 1) ** 2 + (d2 - 1) ** 2), rel=1e-9)
+    assert e4 > e0 and np.asarray(g4).reshape(3, 3)[2, 0] > 0
+
+
 def test_lumped_mass_sums_to_density_times_area():
     sc = scenes.config_small()
     sim = O.OracleCloth(True)
@@ -266,3 +320,14 @@ def test_errors_map_to_exception_types():
     sim.set_pins([99], [[0, 0, 0]])
     with pytest.raises(ValueError):  # out_of_range is reported as index error (rc 1)
         sim.step(0.01)
+
+
+def test_thread_pool_resizes_between_runs():
+    # resizing the pool after it has run jobs must not replay a finished job
+    sc = scenes.config_small(side=6)
+    for threads in (4, 2, 3, 1, 4):
+        O.set_threads(threads)
+        s = _oracle_sim(sc, tol=1e-10)
+        s.step(sc["dt"])
+        assert s.stats()[2] == 0
+    O.set_threads(1)
