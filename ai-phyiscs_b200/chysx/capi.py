@@ -50,6 +50,8 @@ SIGNATURES = {
     "chysx_cloth_num_springs": (ctypes.c_int, [H, ip]),
     "chysx_cloth_build_fem_stretch": (ctypes.c_int, [H, ctypes.c_float, f32p, u]),
     "chysx_cloth_build_fem_shear": (ctypes.c_int, [H, ctypes.c_float, f32p, u]),
+    "chysx_cloth_build_bending": (ctypes.c_int, [H, ctypes.c_float, u]),
+    "chysx_cloth_num_dihedrals": (ctypes.c_int, [H, ip]),
     "chysx_cloth_redistribute_mass": (ctypes.c_int, [H, ctypes.c_float, u, ctypes.c_int, u]),
     "chysx_cloth_set_pcg_iterations": (ctypes.c_int, [H, ctypes.c_int]),
     "chysx_cloth_pcg_iterations": (ctypes.c_int, [H, ip]),
@@ -189,6 +191,14 @@ class Cloth:
             check(self._L.chysx_cloth_build_fem_shear(self.h, 0.0, _p(kt, f32p), stream))
         else:
             check(self._L.chysx_cloth_build_fem_shear(self.h, float(k), _p(None, f32p), stream))
+
+    def build_bending(self, k, stream=0):
+        check(self._L.chysx_cloth_build_bending(self.h, float(k), stream))
+
+    def num_dihedrals(self):
+        v = ctypes.c_int()
+        check(self._L.chysx_cloth_num_dihedrals(self.h, ctypes.byref(v)))
+        return v.value
 
     def redistribute_mass(self, density, inv_mass_ptr, n, stream=0):
         check(self._L.chysx_cloth_redistribute_mass(self.h, density, inv_mass_ptr, n, stream))

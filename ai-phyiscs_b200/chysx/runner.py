@@ -46,6 +46,8 @@ class GpuCloth:
                 s.build_fem_stretch(scene["k_stretch"])
             if scene.get("k_shear") is not None:
                 s.build_fem_shear(scene["k_shear"])
+            if scene.get("k_bend") is not None:
+                s.build_bending(scene["k_bend"])
             if len(scene["pin_idx"]):
                 s.set_pins(scene["pin_idx"], scene["pin_targets"], scene.get("k_pin", 1.0e6))
             s.set_solver(max_iter, rel_tol, warm_start)
@@ -74,6 +76,8 @@ class GpuCloth:
             if scene.get("k_shear") is not None:
                 k = scene["k_shear"]
                 s.build_fem_shear_from_current_positions(np.asarray(k, np.float32) if np.ndim(k) else float(k))
+            if scene.get("k_bend") is not None:
+                s.build_bending_from_current_positions(float(scene["k_bend"]))
             if len(scene["pin_idx"]):
                 s.set_pins(np.asarray(scene["pin_idx"], np.int32), np.asarray(scene["pin_targets"], np.float32),
                            scene.get("k_pin", 1.0e6))

@@ -40,6 +40,12 @@ struct DevTopo {
     const int* __restrict__ pin_off;
     const int* __restrict__ pin_row;
     const float* __restrict__ pin_tgt;  // 3 floats per sorted pin
+    const int* __restrict__ dinc_off;   // dihedral incidence (bending)
+    const int* __restrict__ dinc;
+    const unsigned* __restrict__ dinc_meta;
+    // off-diagonal blocks: 6 planes (symmetric blocks), or 9 (row-major,
+    // general blocks) once bending makes the off-diagonal blocks unsymmetric
+    int nsym;
 };
 
 struct ElemData {
@@ -53,6 +59,10 @@ struct ElemData {
     const int* __restrict__ edges;     // 2 per edge
     const float* __restrict__ rest;
     const float* __restrict__ kedge;
+    const int4* __restrict__ dih;         // bending dihedrals (v0, v1, v2, v3)
+    const float* __restrict__ rest_angle;
+    float k_bend;
+    int use_bending;
     float pin_k;
     int use_tris;     // triangles in the Hessian pattern (stretch or shear)
     int use_stretch;
@@ -155,6 +165,16 @@ __device__ __forceinline__ S6 ld6(const float* p) {
 }
 __device__ __forceinline__ void st6(float* p, const S6& a) {
     p[0] = a.xx; p[32] = a.xy; p[64] = a.xz; p[96] = a.yy; p[128] = a.yz; p[160] = a.zz;
+}
+// Floats per off-diagonal block of the topology.
+__device__ __forceinline__ int off_width(const DevTopo& t) { return t.nsym ? 9 : 6; }
+// y = B x for the off-diagonal block at p (planes strided by 32 floats):
+// symmetric 6-plane blocks, or row-major 9-plane blocks when nsym.
+__device__ __forceinline__ float3 mul_off(const float* p, int nsym, float3 v) {
+    if (!nsym) return mul(ld6(p), v);
+    return f3(p[0] * v.x + p[32] * v.y + p[64] * v.z,
+              p[96] * v.x + p[128] * v.y + p[160] * v.z,
+              p[192] * v.x + p[224] * v.y + p[256] * v.z);
 }
 
 // ---------------------------------------------------------------------------
@@ -294,10 +314,72 @@ __device__ __forceinline__ float sel3(const float (&a)[3], int i) {
     return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]);
 }
 
-__device__ __forceinline__ void smem_acc6(float* s, int stride, int slot, float c, const S6& a) {
-    float* q = s + (size_t)slot * 6 * stride;
-    q[0] += c * a.xx; q[stride] += c * a.xy; q[2 * stride] += c * a.xz;
-    q[3 * stride] += c * a.yy; q[4 * stride] += c * a.yz; q[5 * stride] += c * a.zz;
+// c * a added to an off-diagonal accumulator of `ow` planes (6: symmetric
+// storage; 9: row-major, the symmetric block mirrored).
+__device__ __forceinline__ void smem_acc6(float* s, int stride, int slot, float c, const S6& a, int ow = 6) {
+    float* q = s + (size_t)slot * ow * stride;
+    if (ow == 6) {
+        q[0] += c * a.xx; q[stride] += c * a.xy; q[2 * stride] += c * a.xz;
+        q[3 * stride] += c * a.yy; q[4 * stride] += c * a.yz; q[5 * stride] += c * a.zz;
+    } else {
+        q[0] += c * a.xx; q[stride] += c * a.xy; q[2 * stride] += c * a.xz;
+        q[3 * stride] += c * a.xy; q[4 * stride] += c * a.yy; q[5 * stride] += c * a.yz;
+        q[6 * stride] += c * a.xz; q[7 * stride] += c * a.yz; q[8 * stride] += c * a.zz;
+    }
+}
+// c * u v^T added to a row-major 9-plane accumulator.
+__device__ __forceinline__ void smem_acc_outer(float* s, int stride, int slot, float c, float3 u, float3 v) {
+    float* q = s + (size_t)slot * 9 * stride;
+    const float ux = c * u.x, uy = c * u.y, uz = c * u.z;
+    q[0] += ux * v.x; q[stride] += ux * v.y; q[2 * stride] += ux * v.z;
+    q[3 * stride] += uy * v.x; q[4 * stride] += uy * v.y; q[5 * stride] += uy * v.z;
+    q[6 * stride] += uz * v.x; q[7 * stride] += uz * v.y; q[8 * stride] += uz * v.z;
+}
+
+// Discrete bending of a dihedral (v0, v1 = hinge; v2, v3 = the two wing
+// vertices), Bridson's formulation as the reference uses it
+// (constraint/cloth/bending_constraint.cu:46-123): signed angle
+// theta = atan2((n1 x n2).e, n1.n2) between the wing normals and its shape
+// gradients a_i = d theta / d x_i.  Energy k/2 (theta - theta0)^2,
+// gradient k (theta - theta0) a_i, Gauss-Newton Hessian k a_i a_j^T.
+// `valid` is false for a collapsed hinge or a wing without height.
+struct Dihedral {
+    float theta;
+    float3 a[4];
+    bool valid;
+};
+
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+    return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+__device__ __forceinline__ Dihedral dihedral(float3 x0, float3 x1, float3 x2, float3 x3) {
+    constexpr float kFloor = 1.0e-12f;
+    Dihedral d;
+    d.valid = false;
+    d.theta = 0.0f;
+    const float3 e = x1 - x0, e2 = x2 - x0, e3 = x3 - x0;
+    const float le = len3(e);
+    if (le < kFloor) return d;
+    const float inv_le = 1.0f / le;
+    const float3 m1 = cross3(e2, e), m2 = cross3(e, e3);
+    const float l1 = len3(m1), l2 = len3(m2);
+    if (l1 < kFloor || l2 < kFloor) return d;
+    const float3 n1 = m1 * (1.0f / l1), n2 = m2 * (1.0f / l2);
+    const float st = fminf(1.0f, fmaxf(-1.0f, dot3(cross3(n1, n2), e * inv_le)));
+    d.theta = atan2f(st, dot3(n1, n2));
+    // foot points of the wing vertices on the hinge and their heights
+    const float inv_le2 = inv_le * inv_le;
+    const float w1 = dot3(e, e2) * inv_le2, w2 = dot3(e, e3) * inv_le2;
+    const float h1 = len3(e2 - e * w1), h2 = len3(e3 - e * w2);
+    if (h1 < kFloor || h2 < kFloor) return d;
+    const float g1 = 1.0f / h1, g2 = 1.0f / h2;
+    d.a[0] = n1 * ((w1 - 1.0f) * g1) + n2 * ((w2 - 1.0f) * g2);
+    d.a[1] = n1 * (-w1 * g1) + n2 * (-w2 * g2);
+    d.a[2] = n1 * g1;
+    d.a[3] = n2 * g2;
+    d.valid = true;
+    return d;
 }
 
 // ---------------------------------------------------------------------------
@@ -312,7 +394,8 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, double* part,
                 SolverCfg cfg, int zero_guess, cudaGraphConditionalHandle cond) {
-    extern __shared__ float s_off[];  // [width * 6][BLOCK]
+    extern __shared__ float s_off[];  // [width * ow][BLOCK]
+    const int ow = off_width(t);
     const int tid = threadIdx.x;
     const int i = blockIdx.x * BLOCK + tid;
     double red[2] = {0.0, 0.0};
@@ -325,8 +408,8 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
         const S6 I{1.f, 0.f, 0.f, 1.f, 0.f, 1.f};
         st6(t.diag + (size_t)s * 6 * 32 + lane, I);
         st6(t.minv + (size_t)s * 6 * 32 + lane, I);
-        float* vb = t.val + (size_t)so * 6 + lane;
-        for (int q = 0; q < 6 * w; ++q) vb[q * 32] = 0.0f;
+        float* vb = t.val + (size_t)so * ow + lane;
+        for (int q = 0; q < ow * w; ++q) vb[q * 32] = 0.0f;
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
         v.b[i] = z4;
         v.r[i] = z4;
@@ -336,7 +419,7 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
         const int s = i >> 5, lane = i & 31;
         const int so = t.slice_off[s];
         const int w = (t.slice_off[s + 1] - so) >> 5;
-        for (int q = 0; q < 6 * w; ++q) s_off[q * BLOCK + tid] = 0.0f;
+        for (int q = 0; q < ow * w; ++q) s_off[q * BLOCK + tid] = 0.0f;
 
         const float3 x = ld3(a.pos, e);
         const float3 vel = ld3(a.vel, e);
@@ -385,7 +468,7 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
                 axpy6(D, 1.0f, H);
                 const unsigned slot = (meta >> 8) & 0xFFu;
                 if (slot == 0xFFu) axpy6(D, -1.0f, H);
-                else smem_acc6(s_off + tid, BLOCK, (int)slot, -1.0f, H);
+                else smem_acc6(s_off + tid, BLOCK, (int)slot, -1.0f, H, ow);
             }
         }
         // Baraff-Witkin stretch, then shear, per incident triangle
@@ -415,11 +498,46 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
                         axpy6(D, cu_, tr.Mu);
                         axpy6(D, cv_, tr.Mv);
                     } else {
-                        smem_acc6(s_off + tid, BLOCK, (int)slot, cu_, tr.Mu);
-                        smem_acc6(s_off + tid, BLOCK, (int)slot, cv_, tr.Mv);
+                        smem_acc6(s_off + tid, BLOCK, (int)slot, cu_, tr.Mu, ow);
+                        smem_acc6(s_off + tid, BLOCK, (int)slot, cv_, tr.Mv, ow);
                     }
                 }
               }
+            }
+        }
+        // bending dihedrals (bending_constraint.cu:163-244): gradient
+        // k (theta - theta0) a_l, Hessian blocks k a_l a_m^T (general blocks)
+        if (el.use_bending) {
+            const int o = t.dinc_off[s];
+            const int wd = (t.dinc_off[s + 1] - o) >> 5;
+            for (int k = 0; k < wd; ++k) {
+                const int d = t.dinc[o + k * 32 + lane];
+                if (d < 0) continue;
+                const unsigned meta = t.dinc_meta[o + k * 32 + lane];
+                const int la = (int)(meta & 3u);
+                const int4 q4 = el.dih[d];
+                const Dihedral f = dihedral(ld3(a.pos, q4.x), ld3(a.pos, q4.y), ld3(a.pos, q4.z), ld3(a.pos, q4.w));
+                if (!f.valid) continue;
+                const float3 al = f.a[la];
+                g = g + al * (el.k_bend * (f.theta - el.rest_angle[d]));
+                const float kb = el.k_bend;
+                D.xx += kb * al.x * al.x; D.xy += kb * al.x * al.y; D.xz += kb * al.x * al.z;
+                D.yy += kb * al.y * al.y; D.yz += kb * al.y * al.z; D.zz += kb * al.z * al.z;
+#pragma unroll
+                for (int q = 1; q <= 3; ++q) {
+                    const float3 am = f.a[(la + q) & 3];
+                    const unsigned slot = (meta >> (8 * q)) & 0xFFu;
+                    if (slot == 0xFFu) {
+                        // a repeated vertex (degenerate dihedral): the block
+                        // lands on the diagonal, kept symmetric
+                        const float h = 0.5f * kb;
+                        D.xx += 2.f * h * al.x * am.x; D.yy += 2.f * h * al.y * am.y; D.zz += 2.f * h * al.z * am.z;
+                        D.xy += h * (al.x * am.y + al.y * am.x); D.xz += h * (al.x * am.z + al.z * am.x);
+                        D.yz += h * (al.y * am.z + al.z * am.y);
+                    } else {
+                        smem_acc_outer(s_off + tid, BLOCK, (int)slot, kb, al, am);
+                    }
+                }
             }
         }
         // RHS and inertia
@@ -430,11 +548,8 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
 
         // write the row: diagonal, off-diagonal blocks, M^-1
         st6(t.diag + (size_t)s * 6 * 32 + lane, D);
-        float* vb = t.val + (size_t)so * 6 + lane;
-        for (int k = 0; k < w; ++k) {
-#pragma unroll
-            for (int c = 0; c < 6; ++c) vb[(k * 6 + c) * 32] = s_off[(k * 6 + c) * BLOCK + tid];
-        }
+        float* vb = t.val + (size_t)so * ow + lane;
+        for (int q = 0; q < ow * w; ++q) vb[q * 32] = s_off[q * BLOCK + tid];
         const S6 Mi = inverse6(D);
         st6(t.minv + (size_t)s * 6 * 32 + lane, Mi);
         v.b[i] = make_float4(b.x, b.y, b.z, n_springs ? logk / (float)n_springs : 0.f);
@@ -499,11 +614,11 @@ warm_init_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphCondi
         const S6 D = ld6(t.diag + (size_t)s * 6 * 32 + lane);
         const float3 xi = xyz(v.x[i]);
         float3 ax = mul(D, xi);
-        const float* vb = t.val + (size_t)so * 6 + lane;
+        const int ow = off_width(t);
+        const float* vb = t.val + (size_t)so * ow + lane;
         for (int k = 0; k < w; ++k) {
             const int j = t.col[so + k * 32 + lane];
-            const S6 B = ld6(vb + k * 6 * 32);
-            ax = ax + mul(B, xyz(v.x[j]));
+            ax = ax + mul_off(vb + k * ow * 32, t.nsym, xyz(v.x[j]));
         }
         const float3 b = xyz(v.b[i]);
         const float3 r = b - ax;
@@ -604,18 +719,18 @@ pcg_spmv_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphCondit
         pnew[i] = f4(pi);
         const S6 D = ld6(t.diag + (size_t)s * 6 * 32 + lane);
         float3 acc = mul(D, pi);
-        const float* vb = t.val + (size_t)so * 6 + lane;
+        const int ow = off_width(t);
+        const float* vb = t.val + (size_t)so * ow + lane;
         const int* cb = t.col + so + lane;
         for (int k = 0; k < w; ++k) {
             const int j = cb[k * 32];
-            const S6 B = ld6(vb + k * 6 * 32);
             const float4 zj = v.z[j];
             float3 pj = xyz(zj);
             if (!first) {
                 const float4 po = pold[j];
                 pj = f3(fmaf(beta, po.x, zj.x), fmaf(beta, po.y, zj.y), fmaf(beta, po.z, zj.z));
             }
-            acc = acc + mul(B, pj);
+            acc = acc + mul_off(vb + k * ow * 32, t.nsym, pj);
         }
         v.ap[i] = f4(acc);
         red[0] = (double)pi.x * acc.x + (double)pi.y * acc.y + (double)pi.z * acc.z;
@@ -746,6 +861,17 @@ __global__ void rest_shape_kernel(const int* __restrict__ tris, const float* __r
     }
     dminv[t] = make_float4(i00 * cos_t + i01 * (-sin_t), i00 * sin_t + i01 * cos_t,
                            i10 * cos_t + i11 * (-sin_t), i10 * sin_t + i11 * cos_t);
+}
+
+// Rest angle of every bending dihedral (bending_constraint.cu:126-142);
+// degenerate dihedrals rest at 0.
+__global__ void bending_rest_kernel(const int4* __restrict__ dih, const float* __restrict__ pos,
+                                    float* __restrict__ rest, int D) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= D) return;
+    const int4 q = dih[d];
+    const Dihedral f = dihedral(ld3(pos, q.x), ld3(pos, q.y), ld3(pos, q.z), ld3(pos, q.w));
+    rest[d] = f.valid ? f.theta : 0.0f;
 }
 
 // spring_constraint.cu:41-52

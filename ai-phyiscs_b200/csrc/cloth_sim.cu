@@ -422,6 +422,41 @@ public:
         ck(cudaGetLastError(), "rest_shape_kernel launch (shear)");
     }
 
+    // ClothSimulator::build_bending_from_current_positions
+    // (cloth_simulator.cu:451-514): dihedrals of the current mesh, rest
+    // angles from the current positions, one stiffness for all.
+    void build_bending(float k, uintptr_t stream) {
+        bending_built_ = true;
+        k_bend_ = k;
+        topo_dirty_ = true;
+        if (tris_.empty()) {
+            dih_.clear();
+            d_dih_.reset();
+            d_rest_angle_.reset();
+            return;
+        }
+        if (!pos_)
+            throw std::runtime_error(
+                "ClothSimulator::build_bending_from_current_positions: external positions must be set "
+                "first via set_external_buffers().");
+        check_indices(tris_, "triangle");
+        build_dihedrals(tris_, dih_);
+        const int D = (int)(dih_.size() / 4);
+        if (D == 0) {
+            d_dih_.reset();
+            d_rest_angle_.reset();
+            return;
+        }
+        std::vector<int4> hd(D);
+        for (int d = 0; d < D; ++d) hd[d] = make_int4(dih_[4 * d], dih_[4 * d + 1], dih_[4 * d + 2], dih_[4 * d + 3]);
+        d_dih_.upload(hd);
+        d_rest_angle_.resize(D);
+        bending_rest_kernel<<<grid_for(D, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+            d_dih_.get(), reinterpret_cast<const float*>(pos_), d_rest_angle_.get(), D);
+        ck(cudaGetLastError(), "bending_rest_kernel launch");
+    }
+    int num_dihedrals() const { return bending_built_ ? (int)(dih_.size() / 4) : 0; }
+
     // ---- mass ----------------------------------------------------------
     void redistribute_mass(float rho, uintptr_t inv_mass, int count, uintptr_t stream) {
         if (count <= 0) return;
@@ -757,6 +792,7 @@ public:
             const float xx = s6[0], xy = s6[32], xz = s6[64], yy = s6[96], yz = s6[128], zz = s6[160];
             o[0] = xx; o[1] = xy; o[2] = xz; o[3] = xy; o[4] = yy; o[5] = yz; o[6] = xz; o[7] = yz; o[8] = zz;
         };
+        const int ow = off_width();
         const bool mapped = !topo_.ext_to_row.empty();
         int k_out = 0;
         if (rp) rp[0] = 0;
@@ -770,7 +806,10 @@ public:
                 if (col) col[k_out] = mapped ? topo_.row_to_ext[topo_.csr_col[q]] : topo_.csr_col[q];
                 if (vals) {
                     const int el = topo_.csr_to_ell[q];
-                    put9(vals + 9 * (size_t)k_out, &hv[(size_t)so * 6 + (size_t)((el - so) >> 5) * 192 + (el & 31)]);
+                    const float* src = &hv[(size_t)so * ow + (size_t)((el - so) >> 5) * ow * 32 + (el & 31)];
+                    if (ow == 6) put9(vals + 9 * (size_t)k_out, src);
+                    else
+                        for (int c = 0; c < 9; ++c) vals[9 * (size_t)k_out + c] = src[c * 32];
                 }
             }
             if (rp) rp[e + 1] = k_out;
@@ -792,19 +831,21 @@ private:
         const bool use_stretch = stretch_built_ && d_dminv_.size() > 0;
         const bool use_shear = shear_built_ && d_dminv_s_.size() > 0;
         const bool use_tris = use_stretch || use_shear;
+        const bool use_bending = bending_built_ && d_dih_.size() > 0;
         const bool use_springs = springs_built_ && springs_in_step_ && d_rest_.size() > 0;
         if (!inst_offsets_.empty() && inst_offsets_.back() != n_)
             throw std::invalid_argument("set_instances: offsets do not cover the particle count");
-        build_topology(n_, tris_, use_tris, edges_, use_springs, pin_idx_, inst_offsets_, topo_);
+        build_topology(n_, tris_, use_tris, edges_, use_springs, pin_idx_, inst_offsets_, topo_, dih_, use_bending);
         if (topo_.row_to_ext.empty()) d_row_to_ext_.reset();
         else d_row_to_ext_.upload(topo_.row_to_ext);
         use_tris_ = use_tris;
         use_stretch_ = use_stretch;
         use_shear_ = use_shear;
         use_springs_ = use_springs;
+        use_bending_ = use_bending;
         d_slice_off_.upload(topo_.slice_off);
         d_col_.upload(topo_.col);
-        d_val_.resize(std::max<size_t>(1, (size_t)topo_.ell_entries() * 6));
+        d_val_.resize(std::max<size_t>(1, (size_t)topo_.ell_entries() * off_width()));
         d_val_.zero();
         d_diag_.resize((size_t)topo_.n_pad * 6);
         d_minv_.resize((size_t)topo_.n_pad * 6);
@@ -814,6 +855,9 @@ private:
         d_sinc_off_.upload(topo_.sinc_off);
         d_sinc_.upload(topo_.sinc);
         d_sinc_meta_.upload(topo_.sinc_meta);
+        d_dinc_off_.upload(topo_.dinc_off);
+        d_dinc_.upload(topo_.dinc);
+        d_dinc_meta_.upload(topo_.dinc_meta);
         d_pin_off_.upload(topo_.pin_off);
         d_pin_row_.upload(topo_.pin_row);
         {
@@ -831,10 +875,11 @@ private:
                 b->zero();
             }
         }
-        // assembly block size: per-thread shared accumulators of 6*width floats
+        // assembly block size: per-thread shared accumulators of
+        // (6 or 9) * width floats
         const int W = std::max(1, topo_.max_width);
-        asm_block_ = (W <= 16) ? 128 : (W <= 32 ? 64 : 32);
-        asm_smem_ = (size_t)6 * W * asm_block_ * sizeof(float);
+        asm_block_ = (W * off_width() <= 96) ? 128 : (W * off_width() <= 192 ? 64 : 32);
+        asm_smem_ = (size_t)off_width() * W * asm_block_ * sizeof(float);
         const int max_grid = std::max(grid_for(topo_.n, asm_block_), grid_for(topo_.n, kVecBlock));
         d_part_.resize((size_t)std::max(1, max_grid) * 7);
         d_state_.resize(1);
@@ -861,6 +906,10 @@ private:
         t.pin_off = d_pin_off_.get();
         t.pin_row = d_pin_row_.get();
         t.pin_tgt = d_pin_tgt_.get();
+        t.dinc_off = d_dinc_off_.get();
+        t.dinc = d_dinc_.get();
+        t.dinc_meta = d_dinc_meta_.get();
+        t.nsym = use_bending_ ? 1 : 0;
         return t;
     }
     ElemData elem_data() const {
@@ -879,6 +928,10 @@ private:
         e.use_tris = use_tris_ ? 1 : 0;
         e.use_stretch = use_stretch_ ? 1 : 0;
         e.use_shear = use_shear_ ? 1 : 0;
+        e.dih = d_dih_.get();
+        e.rest_angle = d_rest_angle_.get();
+        e.k_bend = k_bend_;
+        e.use_bending = use_bending_ ? 1 : 0;
         e.use_springs = use_springs_ ? 1 : 0;
         return e;
     }
@@ -1032,7 +1085,8 @@ private:
     // co-resident.  Returns false when the system does not fit.
     bool plan_resident(int sms) {
         resident_ = false;  // a previous plan's choice must not leak into this one
-        if (solver_path_ != kPathPersistent || topo_.max_width > kResidentMaxWidth) return false;
+        // the register-resident rows hold symmetric blocks only
+        if (solver_path_ != kPathPersistent || topo_.max_width > kResidentMaxWidth || use_bending_) return false;
         const int n_slices = std::max(1, topo_.n_slices);
         for (int W : {16, 8}) {
             resident_ = true;
@@ -1358,6 +1412,15 @@ private:
     int warm_mode_ = CHYSX_WARM_PREVIOUS;
     // topology + system
     bool topo_dirty_ = true, use_tris_ = false, use_stretch_ = false, use_shear_ = false, use_springs_ = false;
+    bool bending_built_ = false, use_bending_ = false;
+    float k_bend_ = 0.0f;
+    std::vector<int> dih_;
+    DevBuf<int4> d_dih_;
+    DevBuf<float> d_rest_angle_;
+    DevBuf<int> d_dinc_off_, d_dinc_;
+    DevBuf<unsigned> d_dinc_meta_;
+    // floats per stored off-diagonal block: bending makes them unsymmetric
+    int off_width() const { return use_bending_ ? 9 : 6; }
     HostTopology topo_;
     DevBuf<int> d_slice_off_, d_col_, d_tinc_off_, d_tinc_, d_sinc_off_, d_sinc_, d_pin_off_, d_pin_row_;
     DevBuf<unsigned> d_tinc_meta_, d_sinc_meta_;
@@ -1529,6 +1592,15 @@ int chysx_cloth_build_fem_stretch(chysx_cloth* h, float k, const float* k_per_tr
 int chysx_cloth_build_fem_shear(chysx_cloth* h, float k, const float* k_per_tri, uintptr_t stream) {
     CHYSX_H(h);
     return guard([&] { h->sim.build_shear(k, k_per_tri, stream); });
+}
+int chysx_cloth_build_bending(chysx_cloth* h, float k, uintptr_t stream) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.build_bending(k, stream); });
+}
+int chysx_cloth_num_dihedrals(const chysx_cloth* h, int* out) {
+    CHYSX_H(h);
+    if (out) *out = h->sim.num_dihedrals();
+    return CHYSX_OK;
 }
 int chysx_cloth_redistribute_mass(chysx_cloth* h, float rho, uintptr_t inv_mass, int n, uintptr_t stream) {
     CHYSX_H(h);

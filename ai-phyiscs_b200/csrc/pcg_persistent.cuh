@@ -649,10 +649,11 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                 const S6 D = ld6(t.diag + (size_t)s * 192 + lane);
                 x0 = xyz(v.x[i]);
                 float3 ax = mul(D, x0);
-                const float* vb = t.val + (size_t)so * 6 + lane;
+                const int ow = off_width(t);
+                const float* vb = t.val + (size_t)so * ow + lane;
                 for (int k = 0; k < w; ++k) {
                     const int j = t.col[so + k * 32 + lane];
-                    ax = ax + mul(ld6(vb + k * 192), xyz(v.x[j]));
+                    ax = ax + mul_off(vb + k * ow * 32, t.nsym, xyz(v.x[j]));
                 }
                 r = b - ax;
                 z = mul(Mi, r);
@@ -718,18 +719,18 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                 }
                 pnew[i] = f4(pi);
                 float3 acc = mul(ld6(t.diag + (size_t)s * 192 + lane), pi);
-                const float* vb = t.val + (size_t)so * 6 + lane;
+                const int ow = off_width(t);
+                const float* vb = t.val + (size_t)so * ow + lane;
                 const int* cb = t.col + so + lane;
                 for (int k = 0; k < w; ++k) {
                     const int j = cb[k * 32];
-                    const S6 B = ld6(vb + k * 192);
                     const float4 zj = ldcg4(v.z + j);
                     float3 pj = xyz(zj);
                     if (!first) {
                         const float4 po = ldcg4(pold + j);
                         pj = f3(fmaf(beta, po.x, zj.x), fmaf(beta, po.y, zj.y), fmaf(beta, po.z, zj.z));
                     }
-                    acc = acc + mul(B, pj);
+                    acc = acc + mul_off(vb + k * ow * 32, t.nsym, pj);
                 }
                 v.ap[i] = f4(acc);
                 sig = (double)pi.x * acc.x + (double)pi.y * acc.y + (double)pi.z * acc.z;
@@ -852,7 +853,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         for (int k = 0; k < MAXW; ++k) {
             if (k < w) {
                 col_at(k) = t.col[so + k * 32 + lane];
-                B[k] = ld6(t.val + (size_t)so * 6 + (size_t)k * 192 + lane);
+                B[k] = ld6(t.val + (size_t)so * 6 + (size_t)k * 192 + lane);  // symmetric blocks only
             }
         }
     }

@@ -12,6 +12,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../../include/chysx_cloth.h"
 
@@ -166,6 +167,11 @@ PYBIND11_MODULE(_chysx_native, m) {
                  }
              },
              py::arg("stiffness"), py::arg("cuda_stream") = 0)
+        .def("build_bending_from_current_positions",
+             [](PyClothSimulator& s, float stiffness, std::uintptr_t stream) {
+                 check(chysx_cloth_build_bending(s.h(), stiffness, stream));
+             },
+             py::arg("stiffness"), py::arg("cuda_stream") = 0)
         .def("set_pcg_iterations",
              [](PyClothSimulator& s, int m) { check(chysx_cloth_set_pcg_iterations(s.h(), m)); }, py::arg("max_iter"))
         .def("pcg_iterations",
@@ -261,6 +267,29 @@ PYBIND11_MODULE(_chysx_native, m) {
                  static const char* names[] = {"resident", "loop", "streamed"};
                  return py::make_tuple(names[p], g, b);
              })
+        .def("set_sync_mode", [](PyClothSimulator& s, int mode) { check(chysx_cloth_set_sync_mode(s.h(), mode)); },
+             py::arg("mode"))
+        .def("autotune",
+             [](PyClothSimulator& s, float dt, int repetitions, std::uintptr_t stream) {
+                 check(chysx_cloth_autotune(s.h(), dt, repetitions, stream));
+                 int count = 0;
+                 check(chysx_cloth_autotune_results(s.h(), 0, &count, nullptr, nullptr));
+                 std::vector<int32_t> cfg(8 * (size_t)std::max(count, 1));
+                 std::vector<float> ms(std::max(count, 1));
+                 check(chysx_cloth_autotune_results(s.h(), count, &count, cfg.data(), ms.data()));
+                 static const char* names[] = {"resident", "loop", "streamed"};
+                 py::list out;
+                 for (int k = 0; k < count; ++k) {
+                     const int32_t* c = &cfg[8 * (size_t)k];
+                     py::dict d;
+                     d["path"] = c[0]; d["block"] = c[1]; d["sync"] = c[2]; d["kernel"] = names[c[3]];
+                     d["grid"] = c[4]; d["threads"] = c[5]; d["iters"] = c[6]; d["status"] = c[7];
+                     d["solve_ms"] = ms[k];
+                     out.append(d);
+                 }
+                 return out;
+             },
+             py::arg("dt"), py::arg("repetitions") = 2, py::arg("cuda_stream") = 0)
         .def("debug_dump_last_solve", [](PyClothSimulator& s) {
             int n = 0, nnz = 0;
             check(chysx_cloth_num_particles(s.h(), &n));

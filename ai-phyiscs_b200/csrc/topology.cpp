@@ -2,8 +2,10 @@
 #include "topology.h"
 
 #include <algorithm>
+#include <map>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 namespace chysx_b200 {
 
@@ -94,17 +96,36 @@ void build_plan(const std::vector<int>& inst_slice, int grid, HostPlan& o) {
     for (int b = 0; b < n_inst; ++b) o.inst_slot[b + 1] = o.inst_slot[b] + (inst_cta_hi[b] - o.inst_cta_lo[b] + 1);
 }
 
+void build_dihedrals(const std::vector<int>& tris, std::vector<int>& out) {
+    out.clear();
+    const int T = (int)(tris.size() / 3);
+    std::map<std::pair<int, int>, int> third;  // directed edge -> third vertex
+    for (int t = 0; t < T; ++t) {
+        const int v[3] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
+        for (int a = 0; a < 3; ++a) third[{v[a], v[(a + 1) % 3]}] = v[(a + 2) % 3];
+    }
+    for (const auto& kv : third) {
+        const int v0 = kv.first.first, v1 = kv.first.second;
+        if (v0 >= v1) continue;  // each undirected edge once
+        auto rev = third.find({v1, v0});
+        if (rev == third.end()) continue;  // boundary edge
+        out.insert(out.end(), {v0, v1, kv.second, rev->second});
+    }
+}
+
 void build_topology(int n_ext, const std::vector<int>& tris_ext, bool use_tris,
                     const std::vector<int>& edges_ext, bool use_springs,
                     const std::vector<int>& pins_ext, const std::vector<int>& inst_offsets,
-                    HostTopology& o) {
+                    HostTopology& o, const std::vector<int>& dih_ext, bool use_bending) {
     if (n_ext < 0) throw std::invalid_argument("negative particle count");
     o = HostTopology();
     o.n_ext = n_ext;
     const int T = use_tris ? (int)(tris_ext.size() / 3) : 0;
     const int E = use_springs ? (int)(edges_ext.size() / 2) : 0;
+    const int D = use_bending ? (int)(dih_ext.size() / 4) : 0;
     for (int q = 0; q < 3 * T; ++q) check_vertex(tris_ext[q], n_ext);
     for (int q = 0; q < 2 * E; ++q) check_vertex(edges_ext[q], n_ext);
+    for (int q = 0; q < 4 * D; ++q) check_vertex(dih_ext[q], n_ext);
     for (int v : pins_ext) check_vertex(v, n_ext);
 
     // ---- internal row layout
@@ -136,9 +157,16 @@ void build_topology(int n_ext, const std::vector<int>& tris_ext, bool use_tris,
             if (inst_of[tris_ext[3 * t + 1]] != b || inst_of[tris_ext[3 * t + 2]] != b)
                 throw std::invalid_argument("triangle " + std::to_string(t) + " connects two instances");
         }
+        for (int d = 0; d < D; ++d) {
+            const int b = inst_of[dih_ext[4 * d]];
+            for (int a = 1; a < 4; ++a)
+                if (inst_of[dih_ext[4 * d + a]] != b)
+                    throw std::invalid_argument("dihedral " + std::to_string(d) + " connects two instances");
+        }
     }
     auto R = [&](int e) { return o.ext_to_row.empty() ? e : o.ext_to_row[e]; };
-    std::vector<int> tris(3 * (size_t)T), edges(2 * (size_t)E), pins(pins_ext.size());
+    std::vector<int> tris(3 * (size_t)T), edges(2 * (size_t)E), pins(pins_ext.size()), dih(4 * (size_t)D);
+    for (int q = 0; q < 4 * D; ++q) dih[q] = R(dih_ext[q]);
     for (int q = 0; q < 3 * T; ++q) tris[q] = R(tris_ext[q]);
     for (int q = 0; q < 2 * E; ++q) edges[q] = R(edges_ext[q]);
     for (size_t q = 0; q < pins.size(); ++q) pins[q] = R(pins_ext[q]);
@@ -163,6 +191,13 @@ void build_topology(int n_ext, const std::vector<int>& tris_ext, bool use_tris,
         check_vertex(b, n);
         if (a != b) { raw_off[a + 1]++; raw_off[b + 1]++; }
     }
+    // bending dihedrals: every vertex pair (cloth_simulator.cu:745-757)
+    for (int d = 0; d < D; ++d) {
+        const int* v = &dih[4 * d];
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b)
+                if (a != b && v[a] != v[b]) raw_off[v[a] + 1]++;
+    }
     for (int i = 0; i < n; ++i) raw_off[i + 1] += raw_off[i];
     std::vector<int> raw(raw_off[n]);
     {
@@ -176,6 +211,12 @@ void build_topology(int n_ext, const std::vector<int>& tris_ext, bool use_tris,
         for (int e = 0; e < E; ++e) {
             const int a = edges[2 * e], b = edges[2 * e + 1];
             if (a != b) { raw[fill[a]++] = b; raw[fill[b]++] = a; }
+        }
+        for (int d = 0; d < D; ++d) {
+            const int* v = &dih[4 * d];
+            for (int a = 0; a < 4; ++a)
+                for (int b = 0; b < 4; ++b)
+                    if (a != b && v[a] != v[b]) raw[fill[v[a]]++] = v[b];
         }
     }
     o.csr_ptr.assign(n + 1, 0);
@@ -273,6 +314,33 @@ void build_topology(int n_ext, const std::vector<int>& tris_ext, bool use_tris,
         std::vector<int> dummy_off;
         slice_layout(n, o.n_slices, cnt, [&](int r, int k) { return meta[cnt_off[r] + k]; }, 0u,
                      dummy_off, o.sinc_meta);
+    }
+    // ---- dihedral incidence (sorted by dihedral id per row)
+    {
+        std::vector<int> cnt_off(n + 1, 0);
+        for (int d = 0; d < D; ++d)
+            for (int a = 0; a < 4; ++a) cnt_off[dih[4 * d + a] + 1]++;
+        for (int i = 0; i < n; ++i) cnt_off[i + 1] += cnt_off[i];
+        std::vector<int> ids(cnt_off[n]);
+        std::vector<uint32_t> meta(cnt_off[n]);
+        std::vector<int> fill(cnt_off.begin(), cnt_off.end() - 1);
+        for (int d = 0; d < D; ++d) {
+            const int* v = &dih[4 * d];
+            for (int a = 0; a < 4; ++a) {
+                const int r = v[a];
+                uint32_t m = (uint32_t)a;
+                for (int q = 1; q <= 3; ++q) m |= slot_of(r, v[(a + q) % 4]) << (8 * q);
+                ids[fill[r]] = d;
+                meta[fill[r]] = m;
+                fill[r]++;
+            }
+        }
+        auto cnt = [&](int r) { return cnt_off[r + 1] - cnt_off[r]; };
+        slice_layout(n, o.n_slices, cnt, [&](int r, int k) { return ids[cnt_off[r] + k]; }, -1,
+                     o.dinc_off, o.dinc);
+        std::vector<int> dummy_off;
+        slice_layout(n, o.n_slices, cnt, [&](int r, int k) { return meta[cnt_off[r] + k]; }, 0u,
+                     dummy_off, o.dinc_meta);
     }
     // ---- pins sorted by row, per-slice ranges
     {

@@ -44,6 +44,10 @@ struct HostTopology {
     // spring incidence: edge id, meta = end | slot_other << 8
     std::vector<int> sinc_off, sinc;
     std::vector<uint32_t> sinc_meta;
+    // dihedral (bending) incidence: dihedral id, meta = local vertex |
+    // slot of local (l+1)%4 << 8 | of (l+2)%4 << 16 | of (l+3)%4 << 24
+    std::vector<int> dinc_off, dinc;
+    std::vector<uint32_t> dinc_meta;
     // pins sorted by row; pin_perm[sorted] = caller's index
     std::vector<int> pin_off, pin_row, pin_perm;
     // instances: internal rows <-> particles (empty when they coincide)
@@ -60,10 +64,22 @@ struct HostTopology {
 // element may connect two instances.  Throws std::out_of_range for a vertex
 // index outside [0, n), std::invalid_argument for an element spanning two
 // instances, std::runtime_error when a row exceeds kMaxRowWidth neighbours.
+// Bending dihedrals (4 vertices each: v0, v1 = the shared edge, v2 = the
+// third vertex of the face containing the directed edge v0 -> v1, v3 = that
+// of the face containing v1 -> v0) add every pair of their vertices to the
+// pattern when use_bending.
 void build_topology(int n, const std::vector<int>& tris, bool use_tris,
                     const std::vector<int>& edges, bool use_springs,
                     const std::vector<int>& pins, const std::vector<int>& inst_offsets,
-                    HostTopology& out);
+                    HostTopology& out, const std::vector<int>& dihedrals = {},
+                    bool use_bending = false);
+
+// Dihedrals of a consistently oriented triangle mesh as the reference finds
+// them (src/cloth/cloth_simulator.cu:467-506): every interior edge v0 < v1
+// whose two directions both occur gives (v0, v1, third(v0->v1),
+// third(v1->v0)); when a directed edge occurs in several triangles the last
+// one wins.  Ordered by (v0, v1).
+void build_dihedrals(const std::vector<int>& tris, std::vector<int>& out);
 
 // Work split of the persistent PCG kernel: `grid` CTAs each take a
 // contiguous, balanced range of slices; instances own contiguous slice

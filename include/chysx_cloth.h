@@ -125,6 +125,16 @@ int chysx_cloth_build_fem_stretch(chysx_cloth* h, float stiffness, const float* 
 int chysx_cloth_build_fem_shear(chysx_cloth* h, float stiffness, const float* k_per_tri,
                                 uintptr_t stream);
 
+/* ClothSimulator::build_bending_from_current_positions:
+ * src/cloth/cloth_simulator.cu:451-514.  One discrete-bending dihedral per
+ * interior edge of the (consistently oriented) mesh, rest angles from the
+ * current positions, stiffness k for all (constraint/cloth/
+ * bending_constraint.h).  Its Hessian blocks are not symmetric, so a step
+ * with bending stores full 3x3 off-diagonal blocks and runs the streamed or
+ * graph-loop PCG kernel. */
+int chysx_cloth_build_bending(chysx_cloth* h, float stiffness, uintptr_t stream);
+int chysx_cloth_num_dihedrals(const chysx_cloth* h, int* out);
+
 /* ClothSimulator::redistribute_mass_area_weighted:
  * src/cloth/cloth_simulator.cu:516-575.  Writes the caller's inv_mass. */
 int chysx_cloth_redistribute_mass(chysx_cloth* h, float surface_density, uintptr_t inv_mass,

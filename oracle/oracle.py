@@ -51,6 +51,11 @@ def lib():
         L.orc_build_springs.argtypes = [vp, ctypes.c_float, _f32p]
         L.orc_build_stretch.argtypes = [vp, ctypes.c_float, _f32p, ctypes.c_float]
         L.orc_build_shear.argtypes = [vp, ctypes.c_float, _f32p]
+        L.orc_build_bending.argtypes = [vp, ctypes.c_float]
+        L.orc_num_dihedrals.argtypes = [vp]
+        L.orc_bending_eval.argtypes = [_f64p, ctypes.c_double, ctypes.c_double, _f64p, _f64p, _f64p]
+        L.orc_bending_angle.argtypes = [_f64p]
+        L.orc_bending_angle.restype = ctypes.c_double
         L.orc_redistribute_mass.argtypes = [vp, ctypes.c_float, _f32p]
         L.orc_set_pins.argtypes = [vp, _i32p, _f32p, ctypes.c_int, ctypes.c_float]
         L.orc_set_options.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double]
@@ -142,6 +147,12 @@ class OracleCloth:
             k = 0.0
         _check(self._L.orc_build_springs(self._h, float(k), _p(ke, _f32p)))
 
+    def build_bending(self, k):
+        _check(self._L.orc_build_bending(self._h, float(k)))
+
+    def num_dihedrals(self):
+        return int(self._L.orc_num_dihedrals(self._h))
+
     def build_shear(self, k):
         kt = np.ascontiguousarray(k, np.float32) if np.ndim(k) else None
         _check(self._L.orc_build_shear(self._h, 0.0 if np.ndim(k) else float(k), _p(kt, _f32p)))
@@ -222,6 +233,22 @@ def triangle_eval(x9, dm_inv, area, k):
     return float(e[0]), g, h
 
 
+def bending_eval(x12, k, theta0):
+    """Energy, gradient (12) and Gauss-Newton Hessian (12 x 12) of one
+    dihedral (v0, v1 hinge; v2, v3 wings), or None when degenerate."""
+    x12 = np.ascontiguousarray(x12, np.float64).reshape(12)
+    e = np.zeros(1)
+    g = np.zeros(12)
+    h = np.zeros((12, 12))
+    ok = lib().orc_bending_eval(_p(x12, _f64p), float(k), float(theta0), _p(e, _f64p), _p(g, _f64p), _p(h, _f64p))
+    return (float(e[0]), g, h) if ok else None
+
+
+def bending_angle(x12):
+    x12 = np.ascontiguousarray(x12, np.float64).reshape(12)
+    return float(lib().orc_bending_angle(_p(x12, _f64p)))
+
+
 def spring_eval(x6, L, k):
     x6 = np.ascontiguousarray(x6, np.float64).reshape(6)
     e = np.zeros(1)
@@ -252,6 +279,8 @@ def run_scene(scene, steps=None, fp64=True, rel_tol=None, max_iter=None, warm_st
         sim.build_stretch(scene["k_stretch"])
     if scene.get("k_shear") is not None:
         sim.build_shear(scene["k_shear"])
+    if scene.get("k_bend") is not None:
+        sim.build_bending(scene["k_bend"])
     if len(scene["pin_idx"]):
         sim.set_pins(scene["pin_idx"], scene["pin_targets"], scene.get("k_pin", 1.0e6))
     sim.set_solver(max_iter=max_iter if max_iter is not None else scene["max_iter"],

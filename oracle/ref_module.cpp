@@ -54,6 +54,9 @@ PYBIND11_MODULE(REF_MODULE_NAME, m) {
         .def("build_fem_shear_from_current_positions",
              &ClothSimulator::build_fem_shear_from_current_positions, py::arg("stiffness"),
              py::arg("cuda_stream") = 0)
+        .def("build_bending_from_current_positions",
+             &ClothSimulator::build_bending_from_current_positions, py::arg("stiffness"),
+             py::arg("cuda_stream") = 0)
         .def("redistribute_mass_area_weighted", &ClothSimulator::redistribute_mass_area_weighted,
              py::arg("surface_density"), py::arg("inv_mass_ptr"), py::arg("particle_count"),
              py::arg("cuda_stream") = 0)

@@ -47,6 +47,8 @@ def run_reference(mod, sc, pcg_iters, steps, dump_at=()):
     s.build_fem_stretch_from_current_positions(float(sc["k_stretch"]))
     if sc.get("k_shear") is not None:
         s.build_fem_shear_from_current_positions(float(sc["k_shear"]))
+    if sc.get("k_bend") is not None:
+        s.build_bending_from_current_positions(float(sc["k_bend"]))
     s.set_pins(sc["pin_idx"].astype(np.int32), sc["pin_targets"].astype(np.float32), float(sc["k_pin"]))
     s.set_pcg_iterations(pcg_iters)
     torch.cuda.synchronize()
@@ -82,6 +84,21 @@ def scene_grid10_shear():
     return sc
 
 
+def scene_grid10_bending():
+    """Config 1 with discrete bending (k = 5e-3) beside springs and stretch."""
+    sc = scenes.config_small(steps=60)
+    sc["k_bend"] = 5.0e-3
+    return sc
+
+
+def make_bending(out_dir=HERE):
+    import _chysx_ref_springs as mod
+
+    a = run_reference(mod, scene_grid10_bending(), 1000, 60, dump_at=(0, 30))
+    np.savez_compressed(os.path.join(out_dir, "ref_grid10_bending.npz"), **a)
+    print("grid10 bending done", flush=True)
+
+
 def make_shear(out_dir=HERE):
     import _chysx_ref_springs as mod
 
@@ -110,12 +127,15 @@ def main(out_dir=HERE):
     np.savez_compressed(os.path.join(out_dir, "ref_grid16_springs.npz"), **a)
     print("grid16 done", flush=True)
     make_shear(out_dir)
+    make_bending(out_dir)
 
 
 if __name__ == "__main__":
-    # python make_golden.py [out_dir] [shear]   ("shear": only the shear fixture)
+    # python make_golden.py [out_dir] [shear|bending]   (only that fixture)
     out = sys.argv[1] if len(sys.argv) > 1 else HERE
     if len(sys.argv) > 2 and sys.argv[2] == "shear":
         make_shear(out)
+    elif len(sys.argv) > 2 and sys.argv[2] == "bending":
+        make_bending(out)
     else:
         main(out)

@@ -19,6 +19,8 @@ def oracle_from(sc, fx, pre, springs, fp64=True, tol=1e-12, iters=20000, warm="z
     s.build_stretch(float(sc["k_stretch"]))
     if sc.get("k_shear") is not None:
         s.build_shear(float(sc["k_shear"]))
+    if sc.get("k_bend") is not None:
+        s.build_bending(float(sc["k_bend"]))
     s.set_pins(sc["pin_idx"], sc["pin_targets"], sc["k_pin"])
     s.set_solver(iters, tol, warm)
     return s

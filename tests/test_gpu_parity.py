@@ -51,6 +51,8 @@ def oracle_sim(sc, fp64=True, tol=1e-10, max_iter=20000, warm="zero", springs_in
         s.build_stretch(sc["k_stretch"])
     if sc.get("k_shear") is not None:
         s.build_shear(sc["k_shear"])
+    if sc.get("k_bend") is not None:
+        s.build_bending(sc["k_bend"])
     if len(sc["pin_idx"]):
         s.set_pins(sc["pin_idx"], sc["pin_targets"], sc.get("k_pin", 1e6))
     s.set_solver(max_iter, tol, warm)
@@ -117,6 +119,39 @@ def test_shear_system_and_trajectory_match_oracle(path, stretch):
             assert np.abs(rhs - orhs).max() < 5e-4
     assert g.stats()[2] == capi.SOLVE_CONVERGED
     # the 20-step FP32 floor of config 1 (see module docstring)
+    assert np.abs(g.positions() - o.state()[0]).max() < 1e-4
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_bending_system_and_trajectory_match_oracle(path):
+    """Discrete bending (k = 5e-3) beside springs and stretch: unsymmetric
+    off-diagonal blocks (stored as full 3x3), so path 0 runs the streamed
+    persistent kernel."""
+    sc = scenes.config_small(steps=20)
+    sc["k_bend"] = 5.0e-3
+    g = make(sc, path, max_iter=5000, rel_tol=1e-8)
+    o = oracle_sim(sc, tol=1e-10, max_iter=5000)
+    assert g.sim.num_dihedrals() == o.num_dihedrals() > 0
+    inv = g.inv_mass.cpu().numpy()
+    for k in range(20):
+        if k == 5:
+            one = oracle_sim(sc, tol=1e-10, max_iter=5000)
+            one.set_state(g.positions().astype(np.float32), g.velocities().astype(np.float32), inv)
+            one.step(sc["dt"])
+        g.step()
+        o.step(sc["dt"])
+        if k == 5:
+            diag, rp, col, vals, rhs, dx = g.dump()
+            od, orp, ocol, ovals, orhs, odx = one.dump_system()
+            np.testing.assert_array_equal(rp, orp)
+            np.testing.assert_array_equal(col, ocol)
+            assert rel(diag, od) < 2e-6
+            assert rel(vals, ovals) < 2e-6
+            assert np.abs(vals - np.transpose(vals, (0, 2, 1))).max() > 0  # unsymmetric blocks stored
+            assert np.abs(rhs - orhs).max() < 5e-4
+    if path == 0:
+        assert g.sim.solver_info()[0] == "streamed"
+    assert g.stats()[2] == capi.SOLVE_CONVERGED
     assert np.abs(g.positions() - o.state()[0]).max() < 1e-4
 
 

@@ -256,6 +256,60 @@ def test_shear_resists_pure_shear_that_stretch_ignores():
     assert e4 > e0 and np.asarray(g4).reshape(3, 3)[2, 0] > 0
 
 
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_bending_element_matches_finite_differences(seed):
+    # bending_constraint.cu:46-123: theta and its shape vectors a_i = d theta / d x_i
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal(12) * 0.5
+    k, th0 = 2.0, 0.3
+    e, g, h = O.bending_eval(x, k, th0)
+    th = O.bending_angle(x)
+    assert e == pytest.approx(0.5 * k * (th - th0) ** 2, rel=1e-12)
+    eps = 1e-6
+    fd_e = np.zeros(12)
+    fd_th = np.zeros(12)
+    for i in range(12):
+        xp, xm = x.copy(), x.copy()
+        xp[i] += eps
+        xm[i] -= eps
+        fd_e[i] = (O.bending_eval(xp, k, th0)[0] - O.bending_eval(xm, k, th0)[0]) / (2 * eps)
+        fd_th[i] = (O.bending_angle(xp) - O.bending_angle(xm)) / (2 * eps)
+    np.testing.assert_allclose(g, fd_e, atol=1e-7 * max(1.0, np.abs(g).max()))
+    # Gauss-Newton Hessian k a a^T with a = d theta / d x
+    np.testing.assert_allclose(h, k * np.outer(fd_th, fd_th), atol=1e-6 * max(1.0, np.abs(h).max()))
+    # the off-diagonal blocks of one dihedral are not symmetric in general
+    assert np.abs(h[0:3, 6:9] - h[0:3, 6:9].T).max() > 1e-3 * np.abs(h).max()
+
+
+def test_dihedrals_are_the_interior_edges_of_the_mesh():
+    sc = scenes.config_small(side=5)
+    sim = O.OracleCloth(True)
+    sim.set_state(sc["pos"], sc["vel"])
+    sim.set_mesh(sc["tris"])
+    sim.build_bending(1e-3)
+    tris = sc["tris"]
+    edges = sc["edges"]
+    count = {tuple(e): 0 for e in edges}
+    for t in tris:
+        for a in range(3):
+            u, v = sorted((int(t[a]), int(t[(a + 1) % 3])))
+            count[(u, v)] += 1
+    assert sim.num_dihedrals() == sum(1 for c in count.values() if c == 2)
+
+
+def test_bending_at_rest_exerts_no_force():
+    sc = scenes.config_small(side=5)
+    n = sc["pos"].shape[0]
+    sim = O.OracleCloth(True)
+    sim.set_material(sc["density"], 0.0, (0.0, 0.0, 0.0))
+    sim.set_state(sc["pos"], sc["vel"], np.ones(n, np.float32))
+    sim.set_mesh(sc["tris"])
+    sim.build_bending(1e-2)
+    sim.set_solver(100, 1e-12, "zero")
+    sim.step(sc["dt"])
+    assert np.abs(sim.dump_system()[4]).max() < 1e-12
+
+
 def test_lumped_mass_sums_to_density_times_area():
     sc = scenes.config_small()
     sim = O.OracleCloth(True)
