@@ -31,6 +31,15 @@ class Material(ctypes.Structure):
                 ("lame_mu", "lame_lambda", "bending", "density", "damping", "gx", "gy", "gz")]
 
 
+class ContactOp(ctypes.Structure):
+    """chysx_contact_op: a device-resident contact list (see the header)."""
+    _fields_ = [("pairs", ctypes.c_uint64), ("weights", ctypes.c_uint64), ("count", ctypes.c_uint64),
+                ("max_contacts", ctypes.c_int), ("stiffness", ctypes.c_float),
+                ("stiffnesses", ctypes.c_uint64), ("slips", ctypes.c_uint64),
+                ("friction_mu", ctypes.c_float), ("friction_epsilon", ctypes.c_float),
+                ("residual_mode", ctypes.c_int)]
+
+
 # name -> (restype, argtypes); every symbol include/chysx_cloth.h declares
 SIGNATURES = {
     "chysx_last_error": (ctypes.c_char_p, []),
@@ -52,6 +61,18 @@ SIGNATURES = {
     "chysx_cloth_build_fem_shear": (ctypes.c_int, [H, ctypes.c_float, f32p, u]),
     "chysx_cloth_build_bending": (ctypes.c_int, [H, ctypes.c_float, u]),
     "chysx_cloth_num_dihedrals": (ctypes.c_int, [H, ip]),
+    "chysx_cloth_add_static_plane": (ctypes.c_int, [H, f32p, ctypes.c_float]),
+    "chysx_cloth_add_static_box": (ctypes.c_int, [H, f32p, f32p, f32p, f32p, f32p]),
+    "chysx_cloth_clear_static_shapes": (ctypes.c_int, [H]),
+    "chysx_cloth_static_shape_counts": (ctypes.c_int, [H, ip, ip]),
+    "chysx_cloth_set_static_contact_thickness": (ctypes.c_int, [H, ctypes.c_float]),
+    "chysx_cloth_set_static_contact_stiffness": (ctypes.c_int, [H, ctypes.c_float]),
+    "chysx_cloth_set_static_contact_friction": (ctypes.c_int, [H, ctypes.c_float]),
+    "chysx_cloth_set_static_contact_friction_epsilon": (ctypes.c_int, [H, ctypes.c_float]),
+    "chysx_cloth_get_static_contact": (ctypes.c_int, [H, f32p, f32p, f32p, f32p]),
+    "chysx_cloth_set_contact_op": (ctypes.c_int, [H, ctypes.POINTER(ContactOp)]),
+    "chysx_cloth_clear_contact_op": (ctypes.c_int, [H]),
+    "chysx_cloth_contact_stats": (ctypes.c_int, [H, ip, ip, ip]),
     "chysx_cloth_redistribute_mass": (ctypes.c_int, [H, ctypes.c_float, u, ctypes.c_int, u]),
     "chysx_cloth_set_pcg_iterations": (ctypes.c_int, [H, ctypes.c_int]),
     "chysx_cloth_pcg_iterations": (ctypes.c_int, [H, ip]),
@@ -199,6 +220,49 @@ class Cloth:
         v = ctypes.c_int()
         check(self._L.chysx_cloth_num_dihedrals(self.h, ctypes.byref(v)))
         return v.value
+
+    def add_static_plane(self, n, d):
+        n = np.ascontiguousarray(n, np.float32).reshape(3)
+        check(self._L.chysx_cloth_add_static_plane(self.h, _p(n, f32p), float(d)))
+
+    def add_static_box(self, center, half_ext, ex=(1, 0, 0), ey=(0, 1, 0), ez=(0, 0, 1)):
+        a = [np.ascontiguousarray(v, np.float32).reshape(3) for v in (center, half_ext, ex, ey, ez)]
+        check(self._L.chysx_cloth_add_static_box(self.h, *[_p(v, f32p) for v in a]))
+
+    def clear_static_shapes(self):
+        check(self._L.chysx_cloth_clear_static_shapes(self.h))
+
+    def set_static_contact(self, thickness, stiffness, friction=0.0, friction_epsilon=1.0e-4):
+        check(self._L.chysx_cloth_set_static_contact_thickness(self.h, float(thickness)))
+        check(self._L.chysx_cloth_set_static_contact_stiffness(self.h, float(stiffness)))
+        check(self._L.chysx_cloth_set_static_contact_friction(self.h, float(friction)))
+        check(self._L.chysx_cloth_set_static_contact_friction_epsilon(self.h, float(friction_epsilon)))
+
+    def static_contact(self):
+        v = [ctypes.c_float() for _ in range(4)]
+        check(self._L.chysx_cloth_get_static_contact(self.h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def static_shape_counts(self):
+        p, b = ctypes.c_int(), ctypes.c_int()
+        check(self._L.chysx_cloth_static_shape_counts(self.h, ctypes.byref(p), ctypes.byref(b)))
+        return p.value, b.value
+
+    def set_contact_op(self, pairs, weights, count, max_contacts, stiffness, stiffnesses=0, slips=0,
+                       friction_mu=0.0, friction_epsilon=1.0e-4, residual_mode=0):
+        """Device addresses of int32 pairs (M, 4), float32 weights (M, 8),
+        the int32 count and the optional per-contact stiffness / slips."""
+        op = ContactOp(pairs, weights, count, max_contacts, stiffness, stiffnesses, slips, friction_mu,
+                       friction_epsilon, residual_mode)
+        check(self._L.chysx_cloth_set_contact_op(self.h, ctypes.byref(op)))
+
+    def clear_contact_op(self):
+        check(self._L.chysx_cloth_clear_contact_op(self.h))
+
+    def contact_stats(self):
+        v = [ctypes.c_int() for _ in range(3)]
+        check(self._L.chysx_cloth_contact_stats(self.h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
 
     def redistribute_mass(self, density, inv_mass_ptr, n, stream=0):
         check(self._L.chysx_cloth_redistribute_mass(self.h, density, inv_mass_ptr, n, stream))

@@ -50,6 +50,12 @@ class GpuCloth:
                 s.build_bending(scene["k_bend"])
             if len(scene["pin_idx"]):
                 s.set_pins(scene["pin_idx"], scene["pin_targets"], scene.get("k_pin", 1.0e6))
+            for n_, d_ in scene.get("planes", ()):
+                s.add_static_plane(n_, d_)
+            for box in scene.get("boxes", ()):
+                s.add_static_box(*box)
+            if scene.get("static_contact") is not None:
+                s.set_static_contact(*scene["static_contact"])
             s.set_solver(max_iter, rel_tol, warm_start)
             self._step = s.step
             self._stats = s.last_stats
@@ -81,6 +87,16 @@ class GpuCloth:
             if len(scene["pin_idx"]):
                 s.set_pins(np.asarray(scene["pin_idx"], np.int32), np.asarray(scene["pin_targets"], np.float32),
                            scene.get("k_pin", 1.0e6))
+            for n_, d_ in scene.get("planes", ()):
+                s.add_static_plane(np.asarray(n_, np.float32), float(d_))
+            for box in scene.get("boxes", ()):
+                s.add_static_box(*[np.asarray(v, np.float32) for v in box])
+            if scene.get("static_contact") is not None:
+                t_, k_, mu_, eps_ = scene["static_contact"]
+                s.set_static_contact_thickness(t_)
+                s.set_static_contact_stiffness(k_)
+                s.set_static_contact_friction(mu_)
+                s.set_static_contact_friction_epsilon(eps_)
             s.set_solver(max_iter, rel_tol, warm_start)
             self._step = s.step
             self._stats = s.last_stats

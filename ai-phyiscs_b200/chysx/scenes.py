@@ -79,6 +79,20 @@ def config_small(side: int = 10, steps: int = 200, max_iter: int = 100, rel_tol:
     return _finish(f"grid{side}", pos, tris, 1.0e3, 1.0e4, [0], steps, max_iter, rel_tol)
 
 
+def config_contact(side: int = 10, steps: int = 60, max_iter: int = 2000, rel_tol: float = 1.0e-6,
+                   friction: float = 0.3, height: float = 0.16):
+    """Static-shape contact: a free side x side patch (1 m, springs k=1e3, BW
+    k=1e4) dropped from `height` onto a table box (half extents 0.25 x 0.05 x
+    0.25 around (0, 0.05, 0), axes rotated 0.3 rad about y) standing on the
+    ground plane y = 0; thickness 0.01 m, contact k=1e4, Coulomb mu."""
+    pos, tris = grid_mesh(side, y=height)
+    c, s = np.cos(0.3), np.sin(0.3)
+    box = ((0.0, 0.05, 0.0), (0.25, 0.05, 0.25), (c, 0.0, -s), (0.0, 1.0, 0.0), (s, 0.0, c))
+    return _finish(f"grid{side}_contact", pos, tris, 1.0e3, 1.0e4, [], steps, max_iter, rel_tol,
+                   planes=[((0.0, 1.0, 0.0), 0.0)], boxes=[box],
+                   static_contact=(0.01, 1.0e4, friction, 1.0e-4))
+
+
 def jittered_grid(side: int, seed: int, size: float = 1.0):
     rng = np.random.default_rng(seed)
     pos, tris = grid_mesh(side, size=size)

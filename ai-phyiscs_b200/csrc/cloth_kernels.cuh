@@ -8,13 +8,18 @@
 //                                           per 32-row slice (xx,xy,xz,yy,yz,zz)
 //   col, val                              : sliced ELL (see topology.h); val
 //                                           holds 6 planes per entry column
-// Every Hessian block of this path is symmetric (pin kI, spring H_blk,
-// Baraff-Witkin blocks c_a c_b M_u + d_a d_b M_v, inertia), so a block is
-// stored as 6 floats (24 B) instead of the reference's 9 (36 B).
+//                                           (9 with bending)
+// Pin kI, spring H_blk, the Baraff-Witkin blocks c_a c_b M_u + d_a d_b M_v,
+// inertia and contact blocks are symmetric, so a block is stored as 6
+// floats (24 B) instead of the reference's 9 (36 B); the bending blocks
+// k a_i a_j^T are not, and a system with bending keeps its off-diagonal
+// blocks as 9 row-major planes.
 #pragma once
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include "contact_types.h"
 
 namespace chysx_b200 {
 
@@ -46,6 +51,7 @@ struct DevTopo {
     // off-diagonal blocks: 6 planes (symmetric blocks), or 9 (row-major,
     // general blocks) once bending makes the off-diagonal blocks unsymmetric
     int nsym;
+    ContactOp co;  // the contact operator's per-row lists (co.active = 0: none)
 };
 
 struct ElemData {
@@ -68,6 +74,7 @@ struct ElemData {
     int use_stretch;
     int use_shear;
     int use_springs;
+    StaticContacts sc;
 };
 
 struct StepArgs {
@@ -176,6 +183,12 @@ __device__ __forceinline__ float3 mul_off(const float* p, int nsym, float3 v) {
               p[96] * v.x + p[128] * v.y + p[160] * v.z,
               p[192] * v.x + p[224] * v.y + p[256] * v.z);
 }
+
+}  // namespace chysx_b200
+
+#include "contact_kernels.cuh"
+
+namespace chysx_b200 {
 
 // ---------------------------------------------------------------------------
 // Single-pass deterministic grid reduction of NV doubles.  Each block writes
@@ -540,10 +553,18 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
                 }
             }
         }
+        // contact operator: gradient and diagonal blocks of the row's slots
+        if (t.co.active) contact_assemble_row(t.co, i, g, D);
+        // static shapes at x_n (cloth_simulator.cu:997-1008, 1189-1193)
+        float3 sn = f3(0.f, 0.f, 0.f);
+        float sdepth = 0.0f;
+        if (el.sc.active) sdepth = static_contact_row(el.sc, x, vel, dt, g, D, sn);
         // RHS and inertia
         const float inv_dt2 = 1.0f / (dt * dt);
         const float mi = m * inv_dt2;
-        const float3 b = f3(mi * (xt.x - x.x) - g.x, mi * (xt.y - x.y) - g.y, mi * (xt.z - x.z) - g.z);
+        float3 b = f3(mi * (xt.x - x.x) - g.x, mi * (xt.y - x.y) - g.y, mi * (xt.z - x.z) - g.z);
+        // Coulomb cone on the assembled residual (cloth_simulator.cu:1073-1078)
+        if (sdepth > 0.0f && el.sc.mu > 0.0f) b = coulomb_project(el.sc, b, sn, sdepth);
         D.xx += mi; D.yy += mi; D.zz += mi;
 
         // write the row: diagonal, off-diagonal blocks, M^-1
@@ -620,6 +641,7 @@ warm_init_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphCondi
             const int j = t.col[so + k * 32 + lane];
             ax = ax + mul_off(vb + k * ow * 32, t.nsym, xyz(v.x[j]));
         }
+        if (t.co.active && t.co.residual) ax = ax + contact_spmv_row(t.co, i, [&](int j) { return xyz(v.x[j]); });
         const float3 b = xyz(v.b[i]);
         const float3 r = b - ax;
         const S6 Mi = ld6(t.minv + (size_t)s * 6 * 32 + lane);
@@ -732,6 +754,13 @@ pcg_spmv_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphCondit
             }
             acc = acc + mul_off(vb + k * ow * 32, t.nsym, pj);
         }
+        if (t.co.active)
+            acc = acc + contact_spmv_row(t.co, i, [&](int j) {
+                      const float4 zj = v.z[j];
+                      if (first) return xyz(zj);
+                      const float4 po = pold[j];
+                      return f3(fmaf(beta, po.x, zj.x), fmaf(beta, po.y, zj.y), fmaf(beta, po.z, zj.z));
+                  });
         v.ap[i] = f4(acc);
         red[0] = (double)pi.x * acc.x + (double)pi.y * acc.y + (double)pi.z * acc.z;
     }

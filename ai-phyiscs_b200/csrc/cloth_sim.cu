@@ -319,6 +319,78 @@ public:
         topo_dirty_ = true;
     }
     int num_pins() const { return (int)pin_idx_.size(); }
+
+    // ---- static-shape contact (cloth_simulator.h:383-452) ---------------
+    void add_static_plane(const float* nv, float d) {
+        if (!nv) throw std::invalid_argument("ClothSimulator.add_static_plane: n must be a (3,) float32 vector");
+        planes_.insert(planes_.end(), {nv[0], nv[1], nv[2], d});
+        static_dirty_ = true;
+    }
+    void add_static_box(const float* c, const float* he, const float* ex, const float* ey, const float* ez) {
+        for (const float* v : {c, he, ex, ey, ez})
+            if (!v) throw std::invalid_argument("ClothSimulator.add_static_box: every argument is a (3,) vector");
+        for (const float* v : {c, he, ex, ey, ez}) boxes_.insert(boxes_.end(), {v[0], v[1], v[2]});
+        static_dirty_ = true;
+    }
+    void clear_static_shapes() {
+        planes_.clear();
+        boxes_.clear();
+        static_dirty_ = true;
+    }
+    int static_planes() const { return (int)(planes_.size() / 4); }
+    int static_boxes() const { return (int)(boxes_.size() / 15); }
+    void set_static_param(int which, float v) {
+        float* dst[4] = {&sc_thickness_, &sc_k_, &sc_mu_, &sc_eps_};
+        if (*dst[which] != v) static_dirty_ = true;
+        *dst[which] = v;
+    }
+    void get_static_params(float* t, float* k, float* mu, float* eps) const {
+        if (t) *t = sc_thickness_;
+        if (k) *k = sc_k_;
+        if (mu) *mu = sc_mu_;
+        if (eps) *eps = sc_eps_;
+    }
+    bool static_active() const { return sc_k_ > 0.0f && (!planes_.empty() || !boxes_.empty()); }
+
+    // ---- contact operator (collision/contact_spmv.h:58-96) --------------
+    void set_contact_op(const chysx_contact_op* op) {
+        if (!op) throw std::invalid_argument("set_contact_op: null operator");
+        // ContactSpMVOp::active (contact_spmv.h:88-92): an inactive op clears
+        if (!(op->max_contacts > 0 && (op->stiffness > 0.0f || op->stiffnesses) && op->pairs)) {
+            clear_contact_op();
+            return;
+        }
+        if (!op->weights || !op->count)
+            throw std::invalid_argument("set_contact_op: weights and count are required");
+        if (op->max_contacts > (1 << 28)) throw std::invalid_argument("set_contact_op: max_contacts above 2^28");
+        if ((op->pairs | op->weights | op->slips) & 15u)
+            throw std::invalid_argument("set_contact_op: pairs, weights and slips must be 16-byte aligned");
+        if ((op->count | op->stiffnesses) & 3u)
+            throw std::invalid_argument("set_contact_op: count and stiffnesses must be 4-byte aligned");
+        if (!(op->friction_mu >= 0.0f) || !(op->friction_epsilon > 0.0f))
+            throw std::invalid_argument("set_contact_op: friction_mu >= 0 and friction_epsilon > 0 required");
+        if (op->residual_mode != 0 && op->residual_mode != 1)
+            throw std::invalid_argument("set_contact_op: residual_mode is 0 or 1");
+        if (!co_active_ || !same_bytes(*op, co_)) graph_dirty_ = true;
+        co_ = *op;
+        co_active_ = true;
+    }
+    void clear_contact_op() {
+        if (co_active_) graph_dirty_ = true;
+        co_active_ = false;
+        co_ = chysx_contact_op{};
+    }
+    void contact_stats(int* live, int* dropped, int* slots) {
+        int st[4] = {0, 0, 0, 0};
+        if (co_active_ && stepped_ && d_co_cnt_.size()) {
+            ck(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(last_stream_)), "cudaStreamSynchronize");
+            ck(cudaMemcpy(st, d_co_cnt_.get() + co_rows_ + 1, sizeof(st), cudaMemcpyDeviceToHost),
+               "cudaMemcpy(contact stats)");
+        }
+        if (live) *live = st[0];
+        if (dropped) *dropped = st[1];
+        if (slots) *slots = st[2];
+    }
     void update_pin_targets(const float* tgt, int P, uintptr_t stream) {
         if (!tgt || P <= 0) return;
         if (P != num_pins())
@@ -525,6 +597,15 @@ public:
         if (!(dt > 0.0f)) throw std::invalid_argument("chysx::cloth::ClothSimulator::step: dt must be positive");
         ensure_mesh_on_device();
         if (topo_dirty_ || topo_.n_ext != n_) rebuild_topology();
+        if (co_active_ && !inst_offsets_.empty())
+            throw std::invalid_argument("the contact operator needs the single-instance layout");
+        if (static_dirty_) {
+            std::vector<float> sh(planes_);
+            sh.insert(sh.end(), boxes_.begin(), boxes_.end());
+            d_shapes_.upload(sh);
+            static_dirty_ = false;
+            graph_dirty_ = true;
+        }
         if (graph_dirty_) build_graph();
         update_step_nodes(dt);
         ck(cudaGraphLaunch(exec_, reinterpret_cast<cudaStream_t>(stream)), "cudaGraphLaunch(step)");
@@ -910,6 +991,11 @@ private:
         t.dinc = d_dinc_.get();
         t.dinc_meta = d_dinc_meta_.get();
         t.nsym = use_bending_ ? 1 : 0;
+        t.co.off = d_co_off_.get();
+        t.co.ent = d_co_ent_.get();
+        t.co.rec = d_co_rec_.get();
+        t.co.active = co_active_ ? 1 : 0;
+        t.co.residual = co_.residual_mode == 0 ? 1 : 0;
         return t;
     }
     ElemData elem_data() const {
@@ -933,6 +1019,14 @@ private:
         e.k_bend = k_bend_;
         e.use_bending = use_bending_ ? 1 : 0;
         e.use_springs = use_springs_ ? 1 : 0;
+        e.sc.shapes = d_shapes_.get();
+        e.sc.n_planes = static_planes();
+        e.sc.n_boxes = static_boxes();
+        e.sc.thickness = sc_thickness_;
+        e.sc.k = sc_k_;
+        e.sc.mu = sc_mu_;
+        e.sc.eps = sc_eps_;
+        e.sc.active = static_active() ? 1 : 0;
         return e;
     }
     Vecs vecs() const {
@@ -1086,7 +1180,9 @@ private:
     bool plan_resident(int sms) {
         resident_ = false;  // a previous plan's choice must not leak into this one
         // the register-resident rows hold symmetric blocks only
-        if (solver_path_ != kPathPersistent || topo_.max_width > kResidentMaxWidth || use_bending_) return false;
+        // (and have no contact-operator gather)
+        if (solver_path_ != kPathPersistent || topo_.max_width > kResidentMaxWidth || use_bending_ || co_active_)
+            return false;
         const int n_slices = std::max(1, topo_.n_slices);
         for (int W : {16, 8}) {
             resident_ = true;
@@ -1166,6 +1262,97 @@ private:
         d_bar_.zero();
     }
 
+    // Sizes the contact operator's buffers for the current rows.
+    void prepare_contact_buffers() {
+        if (!co_active_) return;
+        co_rows_ = topo_.n;
+        const int nb = std::max(1, grid_for(co_rows_, kScanChunk));
+        d_co_cnt_.resize((size_t)co_rows_ + 1 + 4);
+        d_co_cnt_.zero();
+        d_co_off_.resize((size_t)co_rows_ + 1);
+        d_co_bsum_.resize((size_t)nb + 1);
+        d_co_ent_.resize((size_t)std::max(1, 4 * co_.max_contacts));
+        d_co_rec_.resize((size_t)std::max(1, co_.max_contacts));
+    }
+
+    // The per-step contact-list build, ahead of the assembly: zero the
+    // counts, prepare + count, scan, fill.  Returns the last node (or dep).
+    cudaGraphNode_t add_contact_nodes(cudaGraphNode_t dep) {
+        if (!co_active_) return dep;
+        int dev = 0, sms = 0;
+        ck(cudaGetDevice(&dev), "cudaGetDevice");
+        ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+        const int n = co_rows_;
+        const int nb = std::max(1, grid_for(n, kScanChunk));
+        int* cnt = d_co_cnt_.get();
+        int* stats = cnt + n + 1;
+        int* off = d_co_off_.get();
+        int* bsum = d_co_bsum_.get();
+        int* ent = d_co_ent_.get();
+        PrepContact* rec = d_co_rec_.get();
+        cudaGraphNode_t last = dep;
+        auto add = [&](void* fn, dim3 grid, dim3 block, void** args, const char* what) {
+            cudaKernelNodeParams p{};
+            p.func = fn;
+            p.gridDim = grid;
+            p.blockDim = block;
+            p.kernelParams = args;
+            cudaGraphNode_t node;
+            ck(cudaGraphAddKernelNode(&node, graph_, last ? &last : nullptr, last ? 1 : 0, &p), what);
+            last = node;
+        };
+        {
+            cudaMemsetParams mp{};
+            mp.dst = cnt;
+            mp.value = 0;
+            mp.elementSize = 4;
+            mp.width = (size_t)n + 1 + 4;
+            mp.height = 1;
+            cudaGraphNode_t node;
+            ck(cudaGraphAddMemsetNode(&node, graph_, last ? &last : nullptr, last ? 1 : 0, &mp),
+               "add contact memset node");
+            last = node;
+        }
+        ContactInput in;
+        in.pairs = reinterpret_cast<const int4*>(co_.pairs);
+        in.weights = reinterpret_cast<const float4*>(co_.weights);
+        in.count = reinterpret_cast<const int*>(co_.count);
+        in.stiffnesses = reinterpret_cast<const float*>(co_.stiffnesses);
+        in.slips = reinterpret_cast<const float4*>(co_.slips);
+        in.max_contacts = co_.max_contacts;
+        in.stiffness = co_.stiffness;
+        in.mu = co_.friction_mu;
+        in.eps = co_.friction_epsilon;
+        int n_part = topo_.n_ext;
+        const dim3 cgrid(std::max(1, std::min(grid_for(co_.max_contacts, 256), 8 * sms)));
+        {
+            void* a[] = {&in, &n_part, &cnt, &rec, &stats};
+            add(reinterpret_cast<void*>(&contact_prep_kernel), cgrid, dim3(256), a, "add contact prep node");
+        }
+        int nn = n, nbb = nb;
+        {
+            void* a[] = {&cnt, &nn, &off, &bsum};
+            add(reinterpret_cast<void*>(&contact_scan_local_kernel), dim3(nb), dim3(1024), a, "add scan node");
+        }
+        {
+            void* a[] = {&bsum, &nbb};
+            add(reinterpret_cast<void*>(&contact_scan_top_kernel), dim3(1), dim3(1024), a, "add scan node");
+        }
+        {
+            void* a[] = {&off, &nn, &bsum, &nbb, &stats};
+            add(reinterpret_cast<void*>(&contact_scan_add_kernel), dim3(std::max(1, grid_for(n, 256))), dim3(256), a,
+                "add scan node");
+        }
+        {
+            const PrepContact* crec = rec;
+            const int* cstats = stats;
+            const int* coff = off;
+            void* a[] = {&crec, &cstats, &coff, &cnt, &ent};
+            add(reinterpret_cast<void*>(&contact_fill_kernel), cgrid, dim3(256), a, "add contact fill node");
+        }
+        return last;
+    }
+
     void build_graph_persistent() {
         destroy_graph();
         if (asm_smem_ > 48 * 1024)
@@ -1173,6 +1360,7 @@ private:
                "cudaFuncSetAttribute(assemble smem)");
         plan_persistent();
         check_plan();
+        prepare_contact_buffers();
         ck(cudaGraphCreate(&graph_, 0), "cudaGraphCreate");
         DevTopo t = dev_topo();
         ElemData el = elem_data();
@@ -1189,7 +1377,7 @@ private:
         void* aargs[] = {&cur_args_, &el, &t, &v, &st, &part, &cur_cfg_, &zero_guess, &no_cond};
         cudaKernelNodeParams ap;
         asm_params(ap, aargs);
-        cudaGraphNode_t t0 = timing_node(0, nullptr);
+        cudaGraphNode_t t0 = add_contact_nodes(timing_node(0, nullptr));
         ck(cudaGraphAddKernelNode(&asm_node_, graph_, t0 ? &t0 : nullptr, t0 ? 1 : 0, &ap), "add assemble node");
         cudaGraphNode_t t1 = add_guess_node(asm_node_, cur_args_, t, v);
         t1 = timing_node(1, t1);
@@ -1244,6 +1432,7 @@ private:
         if (asm_smem_ > 48 * 1024)
             ck(cudaFuncSetAttribute(assemble_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asm_smem_),
                "cudaFuncSetAttribute(assemble smem)");
+        prepare_contact_buffers();
         ck(cudaGraphCreate(&graph_, 0), "cudaGraphCreate");
         ck(cudaGraphConditionalHandleCreate(&cond_, graph_, 1, cudaGraphCondAssignDefault),
            "cudaGraphConditionalHandleCreate");
@@ -1261,7 +1450,7 @@ private:
         void* aargs[] = {&cur_args_, &el, &t, &v, &st, &part, &cur_cfg_, &zero_guess, &cond};
         cudaKernelNodeParams ap;
         asm_params(ap, aargs);
-        cudaGraphNode_t t0 = timing_node(0, nullptr);
+        cudaGraphNode_t t0 = add_contact_nodes(timing_node(0, nullptr));
         ck(cudaGraphAddKernelNode(&asm_node_, graph_, t0 ? &t0 : nullptr, t0 ? 1 : 0, &ap), "add assemble node");
         cudaGraphNode_t last = add_guess_node(asm_node_, cur_args_, t, v);
         last = timing_node(1, last);
@@ -1456,6 +1645,18 @@ private:
     DevBuf<ZP> d_zp_;
     bool timing_ = false;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+    // static shapes: planes (n, d), boxes (center, half extents, axes)
+    std::vector<float> planes_, boxes_;
+    float sc_thickness_ = 0.0f, sc_k_ = 0.0f, sc_mu_ = 0.0f, sc_eps_ = 1.0e-4f;
+    bool static_dirty_ = false;
+    DevBuf<float> d_shapes_;
+    // contact operator and its per-step row lists
+    chysx_contact_op co_{};
+    bool co_active_ = false;
+    int co_rows_ = 0;           // rows of the lists at the last graph build
+    DevBuf<int> d_co_cnt_;      // [rows + 1] counts, then 4 stats ints
+    DevBuf<int> d_co_off_, d_co_bsum_, d_co_ent_;
+    DevBuf<PrepContact> d_co_rec_;
     // graph
     bool graph_dirty_ = true, nodes_valid_ = false;
     cudaGraph_t graph_ = nullptr;
@@ -1601,6 +1802,64 @@ int chysx_cloth_num_dihedrals(const chysx_cloth* h, int* out) {
     CHYSX_H(h);
     if (out) *out = h->sim.num_dihedrals();
     return CHYSX_OK;
+}
+int chysx_cloth_add_static_plane(chysx_cloth* h, const float* n, float d) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.add_static_plane(n, d); });
+}
+int chysx_cloth_add_static_box(chysx_cloth* h, const float* c, const float* he, const float* ex, const float* ey,
+                               const float* ez) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.add_static_box(c, he, ex, ey, ez); });
+}
+int chysx_cloth_clear_static_shapes(chysx_cloth* h) {
+    CHYSX_H(h);
+    h->sim.clear_static_shapes();
+    return CHYSX_OK;
+}
+int chysx_cloth_static_shape_counts(const chysx_cloth* h, int* planes, int* boxes) {
+    CHYSX_H(h);
+    if (planes) *planes = h->sim.static_planes();
+    if (boxes) *boxes = h->sim.static_boxes();
+    return CHYSX_OK;
+}
+int chysx_cloth_set_static_contact_thickness(chysx_cloth* h, float t) {
+    CHYSX_H(h);
+    h->sim.set_static_param(0, t);
+    return CHYSX_OK;
+}
+int chysx_cloth_set_static_contact_stiffness(chysx_cloth* h, float k) {
+    CHYSX_H(h);
+    h->sim.set_static_param(1, k);
+    return CHYSX_OK;
+}
+int chysx_cloth_set_static_contact_friction(chysx_cloth* h, float mu) {
+    CHYSX_H(h);
+    h->sim.set_static_param(2, mu);
+    return CHYSX_OK;
+}
+int chysx_cloth_set_static_contact_friction_epsilon(chysx_cloth* h, float eps) {
+    CHYSX_H(h);
+    h->sim.set_static_param(3, eps);
+    return CHYSX_OK;
+}
+int chysx_cloth_get_static_contact(const chysx_cloth* h, float* t, float* k, float* mu, float* eps) {
+    CHYSX_H(h);
+    h->sim.get_static_params(t, k, mu, eps);
+    return CHYSX_OK;
+}
+int chysx_cloth_set_contact_op(chysx_cloth* h, const chysx_contact_op* op) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_contact_op(op); });
+}
+int chysx_cloth_clear_contact_op(chysx_cloth* h) {
+    CHYSX_H(h);
+    h->sim.clear_contact_op();
+    return CHYSX_OK;
+}
+int chysx_cloth_contact_stats(chysx_cloth* h, int* live, int* dropped, int* slots) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.contact_stats(live, dropped, slots); });
 }
 int chysx_cloth_redistribute_mass(chysx_cloth* h, float rho, uintptr_t inv_mass, int n, uintptr_t stream) {
     CHYSX_H(h);

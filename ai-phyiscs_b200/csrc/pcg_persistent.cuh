@@ -655,6 +655,8 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                     const int j = t.col[so + k * 32 + lane];
                     ax = ax + mul_off(vb + k * ow * 32, t.nsym, xyz(v.x[j]));
                 }
+                if (t.co.active && t.co.residual)
+                    ax = ax + contact_spmv_row(t.co, i, [&](int j) { return xyz(v.x[j]); });
                 r = b - ax;
                 z = mul(Mi, r);
                 v.r[i] = f4(r);
@@ -732,6 +734,13 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                     }
                     acc = acc + mul_off(vb + k * ow * 32, t.nsym, pj);
                 }
+                if (t.co.active)
+                    acc = acc + contact_spmv_row(t.co, i, [&](int j) {
+                              const float4 zj = ldcg4(v.z + j);
+                              if (first) return xyz(zj);
+                              const float4 po = ldcg4(pold + j);
+                              return f3(fmaf(beta, po.x, zj.x), fmaf(beta, po.y, zj.y), fmaf(beta, po.z, zj.z));
+                          });
                 v.ap[i] = f4(acc);
                 sig = (double)pi.x * acc.x + (double)pi.y * acc.y + (double)pi.z * acc.z;
             }

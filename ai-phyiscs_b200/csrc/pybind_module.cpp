@@ -172,6 +172,109 @@ PYBIND11_MODULE(_chysx_native, m) {
                  check(chysx_cloth_build_bending(s.h(), stiffness, stream));
              },
              py::arg("stiffness"), py::arg("cuda_stream") = 0)
+        // ---- static-shape contact (src/bindings.cpp:596-698) ----------
+        .def("add_static_plane",
+             [](PyClothSimulator& s, F32 n, float d) {
+                 if (n.ndim() != 1 || n.shape(0) != 3)
+                     throw py::value_error("ClothSimulator.add_static_plane: n must be a (3,) float32 vector");
+                 check(chysx_cloth_add_static_plane(s.h(), n.data(), d));
+             },
+             py::arg("n"), py::arg("d"))
+        .def("add_static_box",
+             [](PyClothSimulator& s, F32 center, F32 half_ext, F32 ex, F32 ey, F32 ez) {
+                 const std::pair<F32*, const char*> args[] = {
+                     {&center, "center"}, {&half_ext, "half_ext"}, {&ex, "ex"}, {&ey, "ey"}, {&ez, "ez"}};
+                 for (const auto& a : args)
+                     if (a.first->ndim() != 1 || a.first->shape(0) != 3)
+                         throw py::value_error(std::string("ClothSimulator.add_static_box: ") + a.second +
+                                               " must be a (3,) float32 vector");
+                 check(chysx_cloth_add_static_box(s.h(), center.data(), half_ext.data(), ex.data(), ey.data(),
+                                                  ez.data()));
+             },
+             py::arg("center"), py::arg("half_ext"), py::arg("ex"), py::arg("ey"), py::arg("ez"))
+        .def("clear_static_shapes", [](PyClothSimulator& s) { check(chysx_cloth_clear_static_shapes(s.h())); })
+        .def("set_static_contact_thickness",
+             [](PyClothSimulator& s, float t) { check(chysx_cloth_set_static_contact_thickness(s.h(), t)); },
+             py::arg("thickness"))
+        .def("set_static_contact_stiffness",
+             [](PyClothSimulator& s, float k) { check(chysx_cloth_set_static_contact_stiffness(s.h(), k)); },
+             py::arg("stiffness"))
+        .def("set_static_contact_friction",
+             [](PyClothSimulator& s, float mu) { check(chysx_cloth_set_static_contact_friction(s.h(), mu)); },
+             py::arg("mu"))
+        .def("set_static_contact_friction_epsilon",
+             [](PyClothSimulator& s, float e) { check(chysx_cloth_set_static_contact_friction_epsilon(s.h(), e)); },
+             py::arg("eps_u"))
+        .def("static_contact_thickness",
+             [](const PyClothSimulator& s) {
+                 float v = 0.f;
+                 check(chysx_cloth_get_static_contact(s.h(), &v, nullptr, nullptr, nullptr));
+                 return v;
+             })
+        .def("static_contact_stiffness",
+             [](const PyClothSimulator& s) {
+                 float v = 0.f;
+                 check(chysx_cloth_get_static_contact(s.h(), nullptr, &v, nullptr, nullptr));
+                 return v;
+             })
+        .def("static_contact_friction",
+             [](const PyClothSimulator& s) {
+                 float v = 0.f;
+                 check(chysx_cloth_get_static_contact(s.h(), nullptr, nullptr, &v, nullptr));
+                 return v;
+             })
+        .def("static_contact_friction_epsilon",
+             [](const PyClothSimulator& s) {
+                 float v = 0.f;
+                 check(chysx_cloth_get_static_contact(s.h(), nullptr, nullptr, nullptr, &v));
+                 return v;
+             })
+        .def("static_plane_count",
+             [](const PyClothSimulator& s) {
+                 int p = 0;
+                 check(chysx_cloth_static_shape_counts(s.h(), &p, nullptr));
+                 return p;
+             })
+        .def("static_box_count",
+             [](const PyClothSimulator& s) {
+                 int b = 0;
+                 check(chysx_cloth_static_shape_counts(s.h(), nullptr, &b));
+                 return b;
+             })
+        // ---- contact operator (collision::ContactSpMVOp) --------------
+        .def("set_contact_operator",
+             [](PyClothSimulator& s, std::uintptr_t pairs, std::uintptr_t weights, std::uintptr_t count,
+                int max_contacts, float stiffness, std::uintptr_t stiffnesses, std::uintptr_t slips, float mu,
+                float eps, int residual_mode) {
+                 chysx_contact_op op{};
+                 op.pairs = pairs;
+                 op.weights = weights;
+                 op.count = count;
+                 op.max_contacts = max_contacts;
+                 op.stiffness = stiffness;
+                 op.stiffnesses = stiffnesses;
+                 op.slips = slips;
+                 op.friction_mu = mu;
+                 op.friction_epsilon = eps;
+                 op.residual_mode = residual_mode;
+                 check(chysx_cloth_set_contact_op(s.h(), &op));
+             },
+             py::arg("pairs"), py::arg("weights"), py::arg("count"), py::arg("max_contacts"), py::arg("stiffness"),
+             py::arg("stiffnesses") = 0, py::arg("slips") = 0, py::arg("friction_mu") = 0.0f,
+             py::arg("friction_epsilon") = 1.0e-4f, py::arg("residual_mode") = 0,
+             "Fold a device-resident contact list (int32 pairs (M,4), float32 weights (M,8) = w0..w3, normal, "
+             "depth, int32 count) into every step's system.")
+        .def("clear_contact_operator", [](PyClothSimulator& s) { check(chysx_cloth_clear_contact_op(s.h())); })
+        .def("contact_stats",
+             [](PyClothSimulator& s) {
+                 int live = 0, dropped = 0, slots = 0;
+                 check(chysx_cloth_contact_stats(s.h(), &live, &dropped, &slots));
+                 py::dict d;
+                 d["live"] = live;
+                 d["dropped"] = dropped;
+                 d["slots"] = slots;
+                 return d;
+             })
         .def("set_pcg_iterations",
              [](PyClothSimulator& s, int m) { check(chysx_cloth_set_pcg_iterations(s.h(), m)); }, py::arg("max_iter"))
         .def("pcg_iterations",

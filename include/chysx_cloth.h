@@ -135,6 +135,67 @@ int chysx_cloth_build_fem_shear(chysx_cloth* h, float stiffness, const float* k_
 int chysx_cloth_build_bending(chysx_cloth* h, float stiffness, uintptr_t stream);
 int chysx_cloth_num_dihedrals(const chysx_cloth* h, int* out);
 
+/* Static-shape contact, ClothSimulator::add_static_plane / add_static_box /
+ * clear_static_shapes / set_static_contact_{thickness,stiffness,friction,
+ * friction_epsilon} (src/cloth/cloth_simulator.h:383-452; shapes as
+ * collision::PlaneShape / BoxShape, src/collision/static_contact.h:73-105).
+ * Each particle's deepest penetration below `thickness` adds the penalty
+ * gradient, the lagged IPC friction force, the diagonal block
+ * k n n^T + alpha (I - n n^T) and the Coulomb-cone projection of its residual
+ * (static_contact.cu:111-381); active while stiffness > 0 and a shape exists.
+ * A plane is n (3 floats, unit, pointing to the free side) and d with
+ * n.x + d = 0 on the surface; a box is center, half extents and its three
+ * unit axes (3 floats each). */
+int chysx_cloth_add_static_plane(chysx_cloth* h, const float* n, float d);
+int chysx_cloth_add_static_box(chysx_cloth* h, const float* center, const float* half_ext, const float* ex,
+                               const float* ey, const float* ez);
+int chysx_cloth_clear_static_shapes(chysx_cloth* h);
+int chysx_cloth_static_shape_counts(const chysx_cloth* h, int* planes, int* boxes);
+int chysx_cloth_set_static_contact_thickness(chysx_cloth* h, float thickness);
+int chysx_cloth_set_static_contact_stiffness(chysx_cloth* h, float stiffness);
+int chysx_cloth_set_static_contact_friction(chysx_cloth* h, float mu);
+int chysx_cloth_set_static_contact_friction_epsilon(chysx_cloth* h, float eps_u);
+int chysx_cloth_get_static_contact(const chysx_cloth* h, float* thickness, float* stiffness, float* mu,
+                                   float* eps_u);
+
+/* Contact operator, collision::ContactSpMVOp (src/collision/contact_spmv.h:
+ * 58-96): a contact list filled on the device by the caller's detector
+ * every step (the reference's SelfCollisionDetector output,
+ * src/collision/self_collision.h:22-57) that the step folds into its system
+ * as the penalty Hessian sum_c w_ci w_cj (k n n^T + alpha (I - n n^T)):
+ * gradient and diagonal blocks into the assembly (self_collision_constraint.
+ * cu:45-95, contact_spmv.cu:84-165), the off-diagonal blocks into every
+ * solver SpMV (contact_spmv.cu:171-236; cloth_simulator.cu:941-962,
+ * 1160-1165, 1243-1248).  The pointers are borrowed device addresses read
+ * when each step runs, so the list and *count may change between steps
+ * without any call here.  alpha = mu k depth f1(|u_t|) when friction_mu > 0
+ * and slips are given.  A contact whose stiffness is not finite and
+ * positive is skipped; one with a weighted particle index outside the
+ * particle range is dropped and counted (contact_stats).  Needs the
+ * single-instance layout; a step with a contact operator uses the streamed
+ * or graph-loop PCG kernel. */
+typedef struct chysx_contact_op {
+    uintptr_t pairs;       /* int32 x 4 per contact, 16-byte aligned */
+    uintptr_t weights;     /* float x 8 per contact: w0..w3, nx, ny, nz, depth; 16-byte aligned */
+    uintptr_t count;       /* int32: contacts written this step (clamped to max_contacts) */
+    int max_contacts;
+    float stiffness;       /* uniform k */
+    uintptr_t stiffnesses; /* optional float per contact, overrides stiffness */
+    uintptr_t slips;       /* optional float x 4 per contact: u_t xyz, |u_t|; 16-byte aligned */
+    float friction_mu;
+    float friction_epsilon;
+    /* 0: the warm-start residual r = b - (A + C) x0 (default);
+     * 1: the reference's r = b - A x0 without the off-diagonal contact part
+     *    (src/solver/pcg_solver.cu:512-513 passes alpha = -1, which
+     *    contact_spmv.cu:193-196 skips) */
+    int residual_mode;
+} chysx_contact_op;
+int chysx_cloth_set_contact_op(chysx_cloth* h, const chysx_contact_op* op);
+int chysx_cloth_clear_contact_op(chysx_cloth* h);
+/* Contacts live in the last step, contacts dropped for an out-of-range
+ * index, and row slots written (synchronises). */
+int chysx_cloth_contact_stats(chysx_cloth* h, int* live, int* dropped, int* slots);
+
 /* ClothSimulator::redistribute_mass_area_weighted:
  * src/cloth/cloth_simulator.cu:516-575.  Writes the caller's inv_mass. */
 int chysx_cloth_redistribute_mass(chysx_cloth* h, float surface_density, uintptr_t inv_mass,

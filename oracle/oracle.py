@@ -67,6 +67,13 @@ def lib():
         L.orc_num_particles.argtypes = [vp]
         L.orc_dump_system.argtypes = [vp, _f64p, _i32p, _i32p, _f64p, _f64p, _f64p]
         L.orc_spmv.argtypes = [vp, _f64p, _f64p]
+        L.orc_contact_spmv.argtypes = [vp, _f64p, _f64p]
+        L.orc_add_static_plane.argtypes = [vp, _f32p, ctypes.c_float]
+        L.orc_add_static_box.argtypes = [vp, _f32p, _f32p, _f32p, _f32p, _f32p]
+        L.orc_clear_static_shapes.argtypes = [vp]
+        L.orc_set_static_contact.argtypes = [vp] + [ctypes.c_float] * 4
+        L.orc_set_contacts.argtypes = [vp, _i32p, _f32p, ctypes.c_int, ctypes.c_float, _f32p, _f32p,
+                                       ctypes.c_float, ctypes.c_float, ctypes.c_int]
         L.orc_rest_shape.argtypes = [_f64p, ctypes.c_double, ctypes.c_double, _f64p, _f64p]
         L.orc_triangle_eval.argtypes = [_f64p, _f64p, ctypes.c_double, ctypes.c_double, _f64p, _f64p, _f64p]
         L.orc_spring_eval.argtypes = [_f64p, ctypes.c_double, ctypes.c_double, _f64p, _f64p, _f64p]
@@ -214,6 +221,43 @@ class OracleCloth:
         _check(self._L.orc_spmv(self._h, _p(x, _f64p), _p(y, _f64p)))
         return y
 
+    def contact_spmv(self, x):
+        """The contact operator's off-diagonal part C_off x."""
+        x = np.ascontiguousarray(x, np.float64).reshape(-1, 3)
+        y = np.zeros_like(x)
+        _check(self._L.orc_contact_spmv(self._h, _p(x, _f64p), _p(y, _f64p)))
+        return y
+
+    def add_static_plane(self, n, d):
+        n = np.ascontiguousarray(n, np.float32).reshape(3)
+        _check(self._L.orc_add_static_plane(self._h, _p(n, _f32p), float(d)))
+
+    def add_static_box(self, center, half_ext, ex=(1, 0, 0), ey=(0, 1, 0), ez=(0, 0, 1)):
+        a = [np.ascontiguousarray(v, np.float32).reshape(3) for v in (center, half_ext, ex, ey, ez)]
+        _check(self._L.orc_add_static_box(self._h, *[_p(v, _f32p) for v in a]))
+
+    def clear_static_shapes(self):
+        _check(self._L.orc_clear_static_shapes(self._h))
+
+    def set_static_contact(self, thickness, stiffness, friction=0.0, friction_epsilon=1.0e-4):
+        _check(self._L.orc_set_static_contact(self._h, float(thickness), float(stiffness), float(friction),
+                                              float(friction_epsilon)))
+
+    def set_contacts(self, pairs, weights, stiffness, stiffnesses=None, slips=None, friction=0.0,
+                     friction_epsilon=1.0e-4, residual_mode=0):
+        """Contact operator: pairs (M, 4) int32, weights (M, 8) float32
+        (w0..w3, normal, depth), optional per-contact stiffness (M,) and
+        lagged slips (M, 4); residual_mode 1 reproduces the reference's
+        warm-start residual without the off-diagonal contact part."""
+        pairs = np.ascontiguousarray(pairs, np.int32).reshape(-1, 4)
+        weights = np.ascontiguousarray(weights, np.float32).reshape(-1, 8)
+        ks = None if stiffnesses is None else np.ascontiguousarray(stiffnesses, np.float32).reshape(-1)
+        sl = None if slips is None else np.ascontiguousarray(slips, np.float32).reshape(-1, 4)
+        self._contact_keep = (pairs, weights, ks, sl)
+        _check(self._L.orc_set_contacts(self._h, _p(pairs, _i32p), _p(weights, _f32p), pairs.shape[0],
+                                        float(stiffness), _p(ks, _f32p), _p(sl, _f32p), float(friction),
+                                        float(friction_epsilon), int(residual_mode)))
+
 
 def rest_shape(x9, det_eps=1.0e-6, theta=0.0):
     x9 = np.ascontiguousarray(x9, np.float64).reshape(9)
@@ -258,6 +302,16 @@ def spring_eval(x6, L, k):
     return float(e[0]), g, h
 
 
+def add_static_shapes(sim, scene):
+    """Static planes / boxes and contact parameters of a scene dict."""
+    for n_, d_ in scene.get("planes", ()):
+        sim.add_static_plane(n_, d_)
+    for box in scene.get("boxes", ()):
+        sim.add_static_box(*box)
+    if scene.get("static_contact") is not None:
+        sim.set_static_contact(*scene["static_contact"])
+
+
 def run_scene(scene, steps=None, fp64=True, rel_tol=None, max_iter=None, warm_start="zero",
               springs_in_step=True, apply_force=False, record=False):
     """Run a scene dict (chysx.scenes format) through the oracle.
@@ -283,6 +337,7 @@ def run_scene(scene, steps=None, fp64=True, rel_tol=None, max_iter=None, warm_st
         sim.build_bending(scene["k_bend"])
     if len(scene["pin_idx"]):
         sim.set_pins(scene["pin_idx"], scene["pin_targets"], scene.get("k_pin", 1.0e6))
+    add_static_shapes(sim, scene)
     sim.set_solver(max_iter=max_iter if max_iter is not None else scene["max_iter"],
                    rel_tol=rel_tol if rel_tol is not None else scene["rel_tol"],
                    warm_start=warm_start)

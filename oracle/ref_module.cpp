@@ -7,6 +7,9 @@
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
 
+#include <cuda_runtime.h>
+
+#include <algorithm>
 #include <cstdint>
 #include <stdexcept>
 
@@ -61,6 +64,61 @@ PYBIND11_MODULE(REF_MODULE_NAME, m) {
              py::arg("surface_density"), py::arg("inv_mass_ptr"), py::arg("particle_count"),
              py::arg("cuda_stream") = 0)
         .def("set_pcg_iterations", &ClothSimulator::set_pcg_iterations)
+        // static-shape contact (cloth_simulator.h:383-452)
+        .def("add_static_plane",
+             [](ClothSimulator& s, float nx, float ny, float nz, float d) {
+                 chysx::collision::PlaneShape p;
+                 p.n = chysx::math::Vec3f(nx, ny, nz);
+                 p.d = d;
+                 s.add_static_plane(p);
+             })
+        .def("add_static_box",
+             [](ClothSimulator& s, py::array_t<float, py::array::c_style | py::array::forcecast> v15) {
+                 if (v15.size() != 15) throw std::invalid_argument("add_static_box: 15 floats");
+                 const float* f = v15.data();
+                 chysx::collision::BoxShape b;
+                 b.center = chysx::math::Vec3f(f[0], f[1], f[2]);
+                 b.half_ext = chysx::math::Vec3f(f[3], f[4], f[5]);
+                 b.ex = chysx::math::Vec3f(f[6], f[7], f[8]);
+                 b.ey = chysx::math::Vec3f(f[9], f[10], f[11]);
+                 b.ez = chysx::math::Vec3f(f[12], f[13], f[14]);
+                 s.add_static_box(b);
+             })
+        .def("set_static_contact",
+             [](ClothSimulator& s, float t, float k, float mu, float eps) {
+                 s.set_static_contact_thickness(t);
+                 s.set_static_contact_stiffness(k);
+                 s.set_static_contact_friction(mu);
+                 s.set_static_contact_friction_epsilon(eps);
+             })
+        // self-collision (cloth_simulator.h:238-325)
+        .def("set_self_collision",
+             [](ClothSimulator& s, float thickness, float k, float mu, float eps, int max_contacts) {
+                 s.set_self_collision_max_contacts(max_contacts);
+                 s.set_self_collision_thickness(thickness);
+                 s.set_self_collision_stiffness(k);
+                 s.set_self_collision_friction(mu);
+                 s.set_self_collision_friction_epsilon(eps);
+                 s.set_self_collision_enabled(true);
+             })
+        // The detector's contact list of the last step (pairs, weights,
+        // slips; slips empty when the detector keeps none).
+        .def("self_collision_contacts", [](ClothSimulator& s) {
+            auto& det = s.self_collision_detector();
+            const int cnt = std::min(det.count(0), det.max_contacts());
+            const int c = std::max(cnt, 0);
+            py::array_t<int> pairs({c, 4});
+            py::array_t<float> weights({c, 8});
+            const bool has_slip = det.slips().gpu_size() == (size_t)det.max_contacts() && c > 0;
+            py::array_t<float> slips({has_slip ? c : 0, 4});
+            if (c > 0) {
+                cudaMemcpy(pairs.mutable_data(), det.pairs().gpu_data(), (size_t)c * 16, cudaMemcpyDeviceToHost);
+                cudaMemcpy(weights.mutable_data(), det.weights().gpu_data(), (size_t)c * 32, cudaMemcpyDeviceToHost);
+                if (has_slip)
+                    cudaMemcpy(slips.mutable_data(), det.slips().gpu_data(), (size_t)c * 16, cudaMemcpyDeviceToHost);
+            }
+            return py::make_tuple(pairs, weights, slips);
+        })
         .def("step", &ClothSimulator::step, py::arg("dt"), py::arg("cuda_stream") = 0)
         .def("debug_dump_last_solve", [](const ClothSimulator& s) {
             const int n = s.num_particles();

@@ -49,7 +49,16 @@ def run_reference(mod, sc, pcg_iters, steps, dump_at=()):
         s.build_fem_shear_from_current_positions(float(sc["k_shear"]))
     if sc.get("k_bend") is not None:
         s.build_bending_from_current_positions(float(sc["k_bend"]))
-    s.set_pins(sc["pin_idx"].astype(np.int32), sc["pin_targets"].astype(np.float32), float(sc["k_pin"]))
+    if len(sc["pin_idx"]):
+        s.set_pins(sc["pin_idx"].astype(np.int32), sc["pin_targets"].astype(np.float32), float(sc["k_pin"]))
+    for n_, d_ in sc.get("planes", ()):
+        s.add_static_plane(*[float(v) for v in n_], float(d_))
+    for box in sc.get("boxes", ()):
+        s.add_static_box(np.concatenate([np.asarray(v, np.float32) for v in box]))
+    if sc.get("static_contact") is not None:
+        s.set_static_contact(*[float(v) for v in sc["static_contact"]])
+    if sc.get("self_collision") is not None:
+        s.set_self_collision(*sc["self_collision"])
     s.set_pcg_iterations(pcg_iters)
     torch.cuda.synchronize()
     out = {"inv_mass": inv.cpu().numpy()}
@@ -59,12 +68,20 @@ def run_reference(mod, sc, pcg_iters, steps, dump_at=()):
             out[f"s{k}_pos"] = pos.cpu().numpy()
             out[f"s{k}_vel"] = vel.cpu().numpy()
         s.step(sc["dt"])
+        if not bool(torch.isfinite(pos).all()):
+            out["stopped_at"] = np.array(k)
+            break
         if k in dump_at:
             torch.cuda.synchronize()
             diag, rp, col, vals, rhs, dx = s.debug_dump_last_solve()
             for name, a in zip(("diag", "row_offsets", "col_indices", "values", "rhs", "dx"),
                                (diag, rp, col, vals, rhs, dx)):
                 out[f"s{k}_{name}"] = np.array(a)
+            if sc.get("self_collision") is not None:
+                cp, cw, cs = s.self_collision_contacts()
+                out[f"s{k}_cpairs"] = np.array(cp)
+                out[f"s{k}_cweights"] = np.array(cw)
+                out[f"s{k}_cslips"] = np.array(cs)
     torch.cuda.synchronize()
     out["final_pos"] = pos.cpu().numpy()
     out["final_vel"] = vel.cpu().numpy()
@@ -89,6 +106,37 @@ def scene_grid10_bending():
     sc = scenes.config_small(steps=60)
     sc["k_bend"] = 5.0e-3
     return sc
+
+
+def scene_grid10_contact():
+    """Static-shape contact: config 1's patch, free, dropped onto a rotated
+    table box on the ground plane, Coulomb mu = 0.3 (chysx.scenes.config_contact)."""
+    return scenes.config_contact(friction=0.3, steps=30)
+
+
+def scene_two_sheets():
+    """Self-collision: two 10x10 sheets (0.5 m) in one mesh, the lower one
+    pinned at its corners at y = 0.1, the upper one 7 mm above it, shifted by
+    half a cell; thickness 10 mm, k = 1e3, mu = 0.2, so contacts exist from
+    the first step."""
+    h = 0.5 / 9
+    pa, ta = scenes.grid_mesh(10, size=0.5, y=0.10, origin=(-0.25, -0.25))
+    pb, tb = scenes.grid_mesh(10, size=0.5, y=0.107, origin=(-0.25 + 0.5 * h, -0.25 + 0.5 * h))
+    pos = np.concatenate([pa, pb], 0)
+    tris = np.concatenate([ta, tb + pa.shape[0]], 0)
+    return scenes._finish("two_sheets", pos, tris, 1.0e3, 1.0e4, [0, 9, 90, 99], 3, 1000, 0.0,
+                          self_collision=(0.01, 1.0e3, 0.2, 1.0e-4, 8192))
+
+
+def make_contact(out_dir=HERE):
+    import _chysx_ref_springs as mod
+
+    a = run_reference(mod, scene_grid10_contact(), 1000, 30, dump_at=(0, 8, 14, 22, 29))
+    np.savez_compressed(os.path.join(out_dir, "ref_grid10_contact.npz"), **a)
+    print("grid10 contact done", flush=True)
+    b = run_reference(mod, scene_two_sheets(), 1000, 3, dump_at=(0, 1, 2))
+    np.savez_compressed(os.path.join(out_dir, "ref_two_sheets_selfcontact.npz"), **b)
+    print("two sheets done", flush=True)
 
 
 def make_bending(out_dir=HERE):
@@ -128,14 +176,17 @@ def main(out_dir=HERE):
     print("grid16 done", flush=True)
     make_shear(out_dir)
     make_bending(out_dir)
+    make_contact(out_dir)
 
 
 if __name__ == "__main__":
-    # python make_golden.py [out_dir] [shear|bending]   (only that fixture)
+    # python make_golden.py [out_dir] [shear|bending|contact]   (only that fixture)
     out = sys.argv[1] if len(sys.argv) > 1 else HERE
     if len(sys.argv) > 2 and sys.argv[2] == "shear":
         make_shear(out)
     elif len(sys.argv) > 2 and sys.argv[2] == "bending":
         make_bending(out)
+    elif len(sys.argv) > 2 and sys.argv[2] == "contact":
+        make_contact(out)
     else:
         main(out)
