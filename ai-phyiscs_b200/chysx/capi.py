@@ -79,6 +79,7 @@ SIGNATURES = {
     "chysx_cloth_set_solver": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_double, ctypes.c_int]),
     "chysx_cloth_set_options": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int, ctypes.c_float]),
     "chysx_cloth_step": (ctypes.c_int, [H, ctypes.c_float, u]),
+    "chysx_cloth_step_into": (ctypes.c_int, [H, ctypes.c_float, u, u, u, u, u]),
     "chysx_cloth_last_stats": (ctypes.c_int, [H, ip, dp, ip]),
     "chysx_cloth_num_particles": (ctypes.c_int, [H, ip]),
     "chysx_cloth_num_off_diag_blocks": (ctypes.c_int, [H, ip]),
@@ -359,6 +360,9 @@ class Cloth:
         a, b, f = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
         check(self._L.chysx_cloth_last_timing(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(f)))
         return a.value, b.value, f.value
+
+    def step_into(self, dt, pos_in, vel_in, pos_out, vel_out, stream=0):
+        check(self._L.chysx_cloth_step_into(self.h, dt, pos_in, vel_in, pos_out, vel_out, stream))
 
     def step(self, dt, stream=0):
         check(self._L.chysx_cloth_step(self.h, dt, stream))

@@ -78,8 +78,10 @@ struct ElemData {
 };
 
 struct StepArgs {
-    float* pos;
+    float* pos;      // x_n, v_n (read)
     float* vel;
+    float* pos_out;  // x_{n+1}, v_{n+1} (written; == pos / vel for an in-place step)
+    float* vel_out;
     const float* inv_mass;
     const float* force;
     const int* row_to_ext;  // internal row -> particle (-1 padding), null = identity
@@ -839,26 +841,37 @@ pcg_update_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphCond
     }
 }
 
+// A step whose solve failed leaves the caller's state as it was: in place
+// nothing is written, into separate output buffers x_n and v_n are copied.
+__device__ __forceinline__ void keep_state(const StepArgs& a, int e) {
+    if (a.pos_out == a.pos && a.vel_out == a.vel) return;
+    st3(a.pos_out, e, ld3(a.pos, e));
+    st3(a.vel_out, e, ld3(a.vel, e));
+}
+
 // ---------------------------------------------------------------------------
 // x_{n+1} = x_n + dx, v_{n+1} = dx/dt * exp(-c dt)  (cloth_simulator.cu:222-244)
 // The caller's buffers are left untouched when the solve met NaN/Inf.
 // ---------------------------------------------------------------------------
 __global__ void finalize_kernel(StepArgs a, Vecs v, const SolveState* st) {
-    if (st->status == kSolveNonfinite) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const int e = a.row_to_ext ? a.row_to_ext[i] : i;
     if (e < 0) return;
+    if (st->status == kSolveNonfinite) {
+        keep_state(a, e);
+        return;
+    }
     const float4 d = v.x[i];
     const float3 xn = ld3(a.pos, e);
-    st3(a.pos, e, f3(xn.x + d.x, xn.y + d.y, xn.z + d.z));
+    st3(a.pos_out, e, f3(xn.x + d.x, xn.y + d.y, xn.z + d.z));
     const float inv_dt = 1.0f / a.dt;
     float3 vn = f3(d.x * inv_dt, d.y * inv_dt, d.z * inv_dt);
     if (a.damping > 0.0f) {
         const float decay = expf(-a.damping * a.dt);
         vn = vn * decay;
     }
-    st3(a.vel, e, vn);
+    st3(a.vel_out, e, vn);
 }
 
 // ---------------------------------------------------------------------------

@@ -613,6 +613,30 @@ public:
         stepped_ = true;
     }
 
+    // One step from (pos_in, vel_in) into (pos_out, vel_out): the double-
+    // buffered stepping of a host that keeps state_in and state_out (the
+    // reference's Newton bridge copies state_in to state_out and steps that
+    // in place, README.md:113-130); the inputs become the external buffers.
+    void step_into(float dt, uintptr_t pin, uintptr_t vin, uintptr_t pout, uintptr_t vout, uintptr_t stream) {
+        if (!pin || !vin || !pout || !vout) throw std::invalid_argument("step_into: null state buffer");
+        const uintptr_t bytes = (uintptr_t)n_ * 12u;
+        auto overlap = [&](uintptr_t a, uintptr_t b) { return a != b && a < b + bytes && b < a + bytes; };
+        if (overlap(pin, pout) || overlap(vin, vout) || overlap(pin, vout) || overlap(vin, pout) ||
+            (pout != pin && (pout == vin || vout == pin)) || pout == vout)
+            throw std::invalid_argument("step_into: output buffers must equal or not overlap the inputs");
+        if ((pout == pin) != (vout == vin))
+            throw std::invalid_argument("step_into: step both or neither of pos / vel in place");
+        pos_ = pin;
+        vel_ = vin;
+        pos_out_ = pout;
+        vel_out_ = vout;
+        struct Reset {
+            ClothSim* s;
+            ~Reset() { s->pos_out_ = s->vel_out_ = 0; }
+        } reset{this};
+        step(dt, stream);
+    }
+
     void last_stats(int* iters, double* relres, int* status) {
         int it = 0, st = 0;
         double rr = 0.0, bb = 0.0;
@@ -1036,6 +1060,8 @@ private:
         StepArgs a;
         a.pos = reinterpret_cast<float*>(pos_);
         a.vel = reinterpret_cast<float*>(vel_);
+        a.pos_out = reinterpret_cast<float*>(pos_out_ ? pos_out_ : pos_);
+        a.vel_out = reinterpret_cast<float*>(vel_out_ ? vel_out_ : vel_);
         a.inv_mass = reinterpret_cast<const float*>(inv_mass_);
         a.force = reinterpret_cast<const float*>(force_);
         a.row_to_ext = d_row_to_ext_.get();
@@ -1132,7 +1158,8 @@ private:
     const void* persistent_fn_sync() const {
         if (resident_) {
             // rows of a triangulated grid have at most 6 off-diagonal blocks;
-            // the 6-wide build keeps every row in registers without spills
+            // the 6-wide build fits a row in 128 registers with fewer spills
+            // (ptxas: 56 B of spill stores, the 8-wide build 128 B)
             if (topo_.max_width <= 6)
                 return resident_warps_ == 16 ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, 6, SYNC>)
                                              : reinterpret_cast<const void*>(&pcg_resident_kernel<8, 6, SYNC>);
@@ -1580,6 +1607,7 @@ private:
 
     // caller buffers
     uintptr_t pos_ = 0, vel_ = 0, inv_mass_ = 0, force_ = 0;
+    uintptr_t pos_out_ = 0, vel_out_ = 0;  // step_into's outputs, for that call only
     int n_ = 0;
     // mesh
     std::vector<int> tris_, edges_;
@@ -1885,6 +1913,11 @@ int chysx_cloth_set_options(chysx_cloth* h, int sis, int af, float eps) {
 int chysx_cloth_step(chysx_cloth* h, float dt, uintptr_t stream) {
     CHYSX_H(h);
     return guard([&] { h->sim.step(dt, stream); });
+}
+int chysx_cloth_step_into(chysx_cloth* h, float dt, uintptr_t pos_in, uintptr_t vel_in, uintptr_t pos_out,
+                          uintptr_t vel_out, uintptr_t stream) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.step_into(dt, pos_in, vel_in, pos_out, vel_out, stream); });
 }
 int chysx_cloth_last_stats(chysx_cloth* h, int* iters, double* relres, int* status) {
     CHYSX_H(h);

@@ -1019,14 +1019,17 @@ __global__ void finalize_batch_kernel(StepArgs a, Vecs v, BatchPlan bp) {
     const int e = a.row_to_ext ? a.row_to_ext[i] : i;
     if (e < 0) return;
     const int st = bp.inst[bp.slice_inst[i >> 5]].status;
-    if (st == kSolveNonfinite || st == kSolveKernelError) return;
+    if (st == kSolveNonfinite || st == kSolveKernelError) {
+        keep_state(a, e);
+        return;
+    }
     const float4 d = v.x[i];
     const float3 xn = ld3(a.pos, e);
-    st3(a.pos, e, f3(xn.x + d.x, xn.y + d.y, xn.z + d.z));
+    st3(a.pos_out, e, f3(xn.x + d.x, xn.y + d.y, xn.z + d.z));
     const float inv_dt = 1.0f / a.dt;
     float3 vn = f3(d.x * inv_dt, d.y * inv_dt, d.z * inv_dt);
     if (a.damping > 0.0f) vn = vn * expf(-a.damping * a.dt);
-    st3(a.vel, e, vn);
+    st3(a.vel_out, e, vn);
 }
 
 // Resets the barrier and per-instance states before a solve.

@@ -275,6 +275,14 @@ PYBIND11_MODULE(_chysx_native, m) {
                  d["slots"] = slots;
                  return d;
              })
+        .def("step_into",
+             [](PyClothSimulator& s, float dt, std::uintptr_t pos_in, std::uintptr_t vel_in, std::uintptr_t pos_out,
+                std::uintptr_t vel_out, std::uintptr_t stream) {
+                 check(chysx_cloth_step_into(s.h(), dt, pos_in, vel_in, pos_out, vel_out, stream));
+             },
+             py::arg("dt"), py::arg("pos_in"), py::arg("vel_in"), py::arg("pos_out"), py::arg("vel_out"),
+             py::arg("cuda_stream") = 0,
+             "One step from (pos_in, vel_in) into (pos_out, vel_out) without a copy pass.")
         .def("set_pcg_iterations",
              [](PyClothSimulator& s, int m) { check(chysx_cloth_set_pcg_iterations(s.h(), m)); }, py::arg("max_iter"))
         .def("pcg_iterations",

@@ -232,6 +232,17 @@ int chysx_cloth_step(chysx_cloth* h, float dt, uintptr_t stream);
  * PCGSolver::last_residual (src/solver/pcg_solver.cu:897-923). */
 int chysx_cloth_last_stats(chysx_cloth* h, int* iterations, double* rel_residual, int* status);
 
+/* Double-buffered step, the Newton bridge's stepping (SolverChysX, reference
+ * README.md:113-130, which copies state_in to state_out and then steps
+ * state_out in place): reads x_n, v_n from pos_in / vel_in and writes
+ * x_{n+1}, v_{n+1} to pos_out / vel_out in the same kernels, with no copy
+ * pass; the inputs become the external buffers.  pos_out == pos_in together
+ * with vel_out == vel_in is an in-place step; otherwise the outputs must not
+ * overlap the inputs.  A failed solve (status NONFINITE) copies the inputs to
+ * the outputs.  Float3 AoS device buffers of num_particles entries. */
+int chysx_cloth_step_into(chysx_cloth* h, float dt, uintptr_t pos_in, uintptr_t vel_in, uintptr_t pos_out,
+                          uintptr_t vel_out, uintptr_t stream);
+
 /* ClothSimulator::num_particles / num_off_diag_blocks (used by the
  * reference's debug dump, src/bindings.cpp:551-596). */
 int chysx_cloth_num_particles(const chysx_cloth* h, int* out);

@@ -205,3 +205,25 @@ def test_pybind_facade_mirrors_reference_api():
     sim.set_external_buffers(1, 1, 4)
     with pytest.raises(ValueError):
         sim.step(0.0)
+
+
+def test_bridge_device_addresses_and_host_arrays():
+    """The Newton bridge's duck typing needs no GPU: Warp arrays (.ptr),
+    tensors (data_ptr()), raw addresses; host copies of array-likes."""
+    from chysx.newton_bridge import device_address, host_array
+
+    class W:
+        ptr = 0x7000
+
+    class T:
+        def data_ptr(self):
+            return 0x9000
+
+    assert device_address(W()) == 0x7000
+    assert device_address(T()) == 0x9000
+    assert device_address(0x1234) == 0x1234
+    assert device_address(None) == 0
+    with pytest.raises(TypeError):
+        device_address("x")
+    a = host_array([[0, 1, 2], [2, 1, 3]], np.int32)
+    assert a.dtype == np.int32 and a.shape == (2, 3)
