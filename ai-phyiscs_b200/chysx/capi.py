@@ -105,6 +105,10 @@ SIGNATURES = {
     "chysx_cloth_sync_mode": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_int)]),
     "chysx_cloth_set_tuning": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "chysx_cloth_solver_info": (ctypes.c_int, [H, ip, ip, ip]),
+    "chysx_cloth_set_preconditioner": (ctypes.c_int, [H, ctypes.c_int, ctypes.c_int, ctypes.c_float]),
+    "chysx_cloth_set_row_order": (ctypes.c_int, [H, ctypes.c_int]),
+    "chysx_cloth_row_of_particles": (ctypes.c_int, [H, ctypes.c_int, i32p]),
+    "chysx_cloth_preconditioner": (ctypes.c_int, [H, ip, ip, f32p, ip]),
     "chysx_cloth_enable_timing": (ctypes.c_int, [H, ctypes.c_int]),
     "chysx_cloth_last_timing": (ctypes.c_int, [H, f32p, f32p, f32p]),
     "chysx_topology_pattern": (ctypes.c_int, [ctypes.c_int, i32p, ctypes.c_int, i32p, ctypes.c_int,
@@ -311,6 +315,27 @@ class Cloth:
 
     def set_tuning(self, solver_path=0, block=0, grid=0):
         check(self._L.chysx_cloth_set_tuning(self.h, solver_path, block, grid))
+
+    def set_row_order(self, mode):
+        """0: the caller's particle order; 1 or "spatial": compact blocks."""
+        check(self._L.chysx_cloth_set_row_order(self.h, 1 if mode in (1, "spatial") else 0))
+
+    def row_of_particles(self, n):
+        rows = np.zeros(n, np.int32)
+        check(self._L.chysx_cloth_row_of_particles(self.h, n, rows.ctypes.data_as(i32p)))
+        return rows
+
+    def set_preconditioner(self, kind="block_jacobi", degree=0, ratio=30.0):
+        """"block_jacobi" (reference) or "chebyshev" (CTA-local, odd degree)."""
+        k = {"block_jacobi": 0, "chebyshev": 1}[kind]
+        check(self._L.chysx_cloth_set_preconditioner(self.h, k, int(degree), float(ratio)))
+
+    def preconditioner(self):
+        k, d, u = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        r = ctypes.c_float()
+        check(self._L.chysx_cloth_preconditioner(self.h, ctypes.byref(k), ctypes.byref(d), ctypes.byref(r),
+                                                 ctypes.byref(u)))
+        return ("block_jacobi", "chebyshev")[k.value], d.value, r.value, bool(u.value)
 
     def solver_info(self):
         """(kernel, grid, block) of the last graph build; kernel is

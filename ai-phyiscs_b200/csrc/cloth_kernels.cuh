@@ -107,6 +107,8 @@ struct SolverCfg {
     int max_iter;
     int use_tol;
     double rel_tol;
+    int pc_degree;   // CTA-local Chebyshev preconditioner: polynomial degree (odd); 0 = block-Jacobi
+    float pc_ratio;  // its interval [lambda_max / ratio, lambda_max]
 };
 
 // Device-resident solver scalars.  Written only by the single "last block"

@@ -293,6 +293,7 @@ public:
         }
         mesh_on_device_ = false;  // uploaded on first device use
         vt_n_ = -1;
+        order_.clear();
         topo_dirty_ = true;
     }
     void ensure_mesh_on_device() {
@@ -714,7 +715,27 @@ public:
         if (n_inst > 0 && !off) throw std::invalid_argument("set_instances: null offsets");
         if (n_inst == 0) inst_offsets_.clear();
         else inst_offsets_.assign(off, off + n_inst + 1);
+        order_.clear();
         topo_dirty_ = true;
+    }
+    // Row order (no counterpart in the reference): 0 = the caller's particle
+    // order (default), 1 = spatially compact blocks (recursive coordinate
+    // bisection of the positions at the next topology build, kept until the
+    // mesh, the instances or the particle count change), so that the rows a
+    // CTA holds form a patch of the cloth.
+    void set_row_order(int mode) {
+        if (mode != 0 && mode != 1) throw std::invalid_argument("set_row_order: mode must be 0 or 1");
+        if (mode != row_order_) {
+            order_.clear();
+            topo_dirty_ = true;
+        }
+        row_order_ = mode;
+    }
+    int row_order() const { return row_order_; }
+    // internal row of every particle (identity without a mapped layout)
+    void row_of_particles(int n, int32_t* out) const {
+        if (n != topo_.n_ext) throw std::invalid_argument("row_of_particles: wrong particle count");
+        for (int e = 0; e < n; ++e) out[e] = topo_.ext_to_row.empty() ? e : topo_.ext_to_row[e];
     }
     int num_instances() const { return inst_offsets_.empty() ? 1 : (int)inst_offsets_.size() - 1; }
     void instance_stats(int n, int* iters, double* relres, int* status) {
@@ -755,6 +776,31 @@ public:
         pcg_grid_req_ = grid;
         graph_dirty_ = true;
     }
+    // Preconditioner (no counterpart in the reference, whose PCG is
+    // block-Jacobi): 0 = block-Jacobi (default), 1 = CTA-local Chebyshev of
+    // odd degree on [lambda_max / ratio, lambda_max]; used by the
+    // register-resident kernel, the others stay block-Jacobi.
+    void set_preconditioner(int kind, int degree, float ratio) {
+        if (kind != 0 && kind != 1) throw std::invalid_argument("set_preconditioner: kind must be 0 or 1");
+        if (kind == 1 && (degree < 1 || degree > 63 || degree % 2 == 0))
+            throw std::invalid_argument("set_preconditioner: degree must be odd, 1 to 63");
+        if (kind == 1 && !(ratio > 1.0f && ratio < 1.0e6f))
+            throw std::invalid_argument("set_preconditioner: ratio must be in (1, 1e6)");
+        if (kind != pc_kind_) graph_dirty_ = true;
+        pc_kind_ = kind;
+        pc_degree_ = kind ? degree : 0;
+        pc_ratio_ = kind ? ratio : 0.0f;
+    }
+    void preconditioner(int* kind, int* degree, float* ratio, int* in_use) const {
+        if (kind) *kind = pc_kind_;
+        if (degree) *degree = pc_degree_;
+        if (ratio) *ratio = pc_ratio_;
+        if (in_use) *in_use = pc_active() ? 1 : 0;
+    }
+    // the CTA-local preconditioner runs in the register-resident kernel of
+    // the default synchronisation mode
+    bool pc_active() const { return pc_kind_ == 1 && resident_ && graph_path_ == kPathPersistent && sync_mode_ == 0; }
+
     // kernel actually used by the last graph build: 0 resident, 1 loop,
     // 2 streamed, 3 resident single-reduction
     void solver_info(int* path, int* grid, int* block) const {
@@ -907,8 +953,15 @@ public:
             if (rhs) { rhs[3 * e] = hb[r].x; rhs[3 * e + 1] = hb[r].y; rhs[3 * e + 2] = hb[r].z; }
             if (dx) { dx[3 * e] = hx[r].x; dx[3 * e + 1] = hx[r].y; dx[3 * e + 2] = hx[r].z; }
             const int so = topo_.slice_off[r >> 5];
-            for (int q = topo_.csr_ptr[r]; q < topo_.csr_ptr[r + 1]; ++q, ++k_out) {
-                if (col) col[k_out] = mapped ? topo_.row_to_ext[topo_.csr_col[q]] : topo_.csr_col[q];
+            // the row's entries by particle index (the reference's CSR order),
+            // whatever order the internal rows are in
+            std::vector<std::pair<int, int>> ent;
+            for (int q = topo_.csr_ptr[r]; q < topo_.csr_ptr[r + 1]; ++q)
+                ent.emplace_back(mapped ? topo_.row_to_ext[topo_.csr_col[q]] : topo_.csr_col[q], q);
+            std::sort(ent.begin(), ent.end());
+            for (const auto& cq : ent) {
+                const int q = cq.second;
+                if (col) col[k_out] = cq.first;
                 if (vals) {
                     const int el = topo_.csr_to_ell[q];
                     const float* src = &hv[(size_t)so * ow + (size_t)((el - so) >> 5) * ow * 32 + (el & 31)];
@@ -916,6 +969,7 @@ public:
                     else
                         for (int c = 0; c < 9; ++c) vals[9 * (size_t)k_out + c] = src[c * 32];
                 }
+                ++k_out;
             }
             if (rp) rp[e + 1] = k_out;
         }
@@ -940,9 +994,22 @@ private:
         const bool use_springs = springs_built_ && springs_in_step_ && d_rest_.size() > 0;
         if (!inst_offsets_.empty() && inst_offsets_.back() != n_)
             throw std::invalid_argument("set_instances: offsets do not cover the particle count");
-        build_topology(n_, tris_, use_tris, edges_, use_springs, pin_idx_, inst_offsets_, topo_, dih_, use_bending);
+        if (row_order_ == 1 && (int)order_.size() != n_) {
+            // positions at this build order the rows for the rest of the run
+            std::vector<float> hp(3 * (size_t)n_);
+            if (n_ > 0)
+                ck(cudaMemcpy(hp.data(), reinterpret_cast<const void*>(pos_), hp.size() * sizeof(float),
+                              cudaMemcpyDeviceToHost),
+                   "cudaMemcpy(positions for the row order)");
+            spatial_order(hp.data(), n_, inst_offsets_, order_);
+        }
+        const std::vector<int> no_order;
+        build_topology(n_, tris_, use_tris, edges_, use_springs, pin_idx_, inst_offsets_, topo_, dih_, use_bending,
+                       row_order_ == 1 ? order_ : no_order);
         if (topo_.row_to_ext.empty()) d_row_to_ext_.reset();
         else d_row_to_ext_.upload(topo_.row_to_ext);
+        if (topo_.ext_to_row.empty()) d_ext_to_row_.reset();
+        else d_ext_to_row_.upload(topo_.ext_to_row);
         use_tris_ = use_tris;
         use_stretch_ = use_stretch;
         use_shear_ = use_shear;
@@ -1075,9 +1142,12 @@ private:
     }
     SolverCfg solver_cfg() const {
         SolverCfg c;
+        std::memset(&c, 0, sizeof(c));  // compared bytewise
         c.max_iter = max_iter_;
         c.use_tol = rel_tol_ > 0.0 ? 1 : 0;
         c.rel_tol = rel_tol_;
+        c.pc_degree = pc_kind_ == 1 ? pc_degree_ : 0;
+        c.pc_ratio = pc_kind_ == 1 ? pc_ratio_ : 0.0f;
         return c;
     }
 
@@ -1160,6 +1230,14 @@ private:
             // rows of a triangulated grid have at most 6 off-diagonal blocks;
             // the 6-wide build fits a row in 128 registers with fewer spills
             // (ptxas: 56 B of spill stores, the 8-wide build 128 B)
+            if (pc_kind_ == 1 && SYNC == 0) {
+                if (topo_.max_width <= 6)
+                    return resident_warps_ == 16 ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, 6, 0, 1>)
+                                                 : reinterpret_cast<const void*>(&pcg_resident_kernel<8, 6, 0, 1>);
+                return resident_warps_ == 16
+                           ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, kResidentMaxWidth, 0, 1>)
+                           : reinterpret_cast<const void*>(&pcg_resident_kernel<8, kResidentMaxWidth, 0, 1>);
+            }
             if (topo_.max_width <= 6)
                 return resident_warps_ == 16 ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, 6, SYNC>)
                                              : reinterpret_cast<const void*>(&pcg_resident_kernel<8, 6, SYNC>);
@@ -1350,6 +1428,7 @@ private:
         in.stiffness = co_.stiffness;
         in.mu = co_.friction_mu;
         in.eps = co_.friction_epsilon;
+        in.ext_to_row = d_ext_to_row_.get();
         int n_part = topo_.n_ext;
         const dim3 cgrid(std::max(1, std::min(grid_for(co_.max_contacts, 256), 8 * sms)));
         {
@@ -1665,11 +1744,15 @@ private:
     uintptr_t feat_out_ = 0, pred_out_ = 0;
     cudaGraphNode_t guess_node_ = nullptr;
     std::vector<int> inst_offsets_;
-    DevBuf<int> d_row_to_ext_;
+    DevBuf<int> d_row_to_ext_, d_ext_to_row_;
+    int row_order_ = 0;
+    std::vector<int> order_;  // particles in row order (row_order_ 1)
     bool resident_ = false;
     int resident_warps_ = 16;
     std::vector<TuneResult> tune_;
     int sync_mode_ = 0;    // 0 grid counter barrier, 1 polled per-instance slots
+    int pc_kind_ = 0, pc_degree_ = 0;  // preconditioner: 0 block-Jacobi, 1 CTA-local Chebyshev
+    float pc_ratio_ = 0.0f;
     DevBuf<ZP> d_zp_;
     bool timing_ = false;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -2027,6 +2110,23 @@ int chysx_cloth_sync_mode(const chysx_cloth* h, int* mode) {
 int chysx_cloth_set_tuning(chysx_cloth* h, int solver_path, int block, int grid) {
     CHYSX_H(h);
     return guard([&] { h->sim.set_tuning(solver_path, block, grid); });
+}
+int chysx_cloth_set_row_order(chysx_cloth* h, int mode) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_row_order(mode); });
+}
+int chysx_cloth_row_of_particles(const chysx_cloth* h, int n, int32_t* rows) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.row_of_particles(n, rows); });
+}
+int chysx_cloth_set_preconditioner(chysx_cloth* h, int kind, int degree, float ratio) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_preconditioner(kind, degree, ratio); });
+}
+int chysx_cloth_preconditioner(const chysx_cloth* h, int* kind, int* degree, float* ratio, int* in_use) {
+    CHYSX_H(h);
+    h->sim.preconditioner(kind, degree, ratio, in_use);
+    return CHYSX_OK;
 }
 int chysx_cloth_solver_info(const chysx_cloth* h, int* path, int* grid, int* block) {
     CHYSX_H(h);

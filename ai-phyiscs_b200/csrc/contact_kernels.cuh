@@ -212,6 +212,7 @@ __global__ void contact_prep_kernel(ContactInput in, int n_particles, int* __res
         for (int s = 0; s < 4; ++s) {
             if (wv[s] == 0.0f) rows[s] = -1;
             else if (rows[s] < 0 || rows[s] >= n_particles) bad = true;
+            else if (in.ext_to_row) rows[s] = in.ext_to_row[rows[s]];
         }
         if (bad && live) atomicAdd(&stats[1], 1);
         live = live && !bad;

@@ -40,6 +40,7 @@ struct ContactInput {
     const int* __restrict__ count;
     const float* __restrict__ stiffnesses;  // optional
     const float4* __restrict__ slips;       // optional: u_t xyz, |u_t|
+    const int* __restrict__ ext_to_row;     // particle -> internal row (null: identity)
     int max_contacts;
     float stiffness, mu, eps;
 };

@@ -138,6 +138,13 @@ __device__ __forceinline__ float4 ldcg4(const float4* p) { return __ldcg(p); }
 // a NaN payload no arithmetic produces; published NaNs are canonicalised
 constexpr unsigned long long kSlotEmpty = 0x7FF4C10E5107E000ull;
 constexpr int kPollMax = 5;  // slots per lane in flight: one pass covers 160 CTAs
+// CTA-local Chebyshev preconditioner: power iterations for the block's
+// lambda_max and the margin put on the estimate (24 iterations from a +-1
+// vector land within 4% below lambda_max on cloth blocks)
+constexpr int kPcPowerIts = 24;
+constexpr double kPcMargin = 1.1;
+// fixed pseudo-random sign of vector entry q (multiplicative hash)
+__device__ __forceinline__ float pc_sign(unsigned q) { return ((q * 2654435761u) >> 31) ? -1.0f : 1.0f; }
 
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
@@ -461,6 +468,21 @@ __device__ __forceinline__ void start_partials(double* sp, bool write, float3 b,
 // The instance's start applied to one row: the warm guess scaled by the
 // energy-minimising factor c (x = c x0, r = (1 - c) b + c r0), or the zero
 // guess when the instance fell back.
+// The same start for a general linear preconditioner P: z = P(r) is formed
+// from zb = P(b) and z0 = P(r0) of the unscaled start.
+__device__ __forceinline__ void start_row_linear(const LocalInst& L, float3 b, float3 zb, float3& x, float3& r,
+                                                 float3& z) {
+    if (L.fallback) {
+        x = f3(0.f, 0.f, 0.f);
+        r = b;
+        z = zb;
+    } else {
+        const float c = L.scale, cb = L.scale_b;
+        x = f3(c * x.x, c * x.y, c * x.z);
+        r = f3(fmaf(c, r.x, cb * b.x), fmaf(c, r.y, cb * b.y), fmaf(c, r.z, cb * b.z));
+        z = f3(fmaf(c, z.x, cb * zb.x), fmaf(c, z.y, cb * zb.y), fmaf(c, z.z, cb * zb.z));
+    }
+}
 __device__ __forceinline__ void start_row(const LocalInst& L, float3 b, const S6& Mi, float3& x, float3& r,
                                           float3& z) {
     if (L.fallback) {
@@ -807,13 +829,18 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
 // in flight at once.  Same phases, reductions, barrier and per-instance
 // logic as pcg_persistent_kernel.
 // ---------------------------------------------------------------------------
-template <int W, int MAXW, int SYNC = 0>
+template <int W, int MAXW, int SYNC = 0, int PC = 0>
 __global__ void __launch_bounds__(W * 32, 512 / (W * 32))  // 512 threads of rows per SM
 pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP* zp0, ZP* zp1) {
     extern __shared__ double s_mem[];
     __shared__ int s_flag;
     __shared__ int s_exit;
     __shared__ float4 s_z[W * 32], s_p[2][W * 32];
+    // CTA-local preconditioner: exchange buffers, block sums, Chebyshev
+    // constants (theta, 1/theta, sigma, 2/delta) of this CTA's block
+    __shared__ float4 s_d[PC ? 2 : 1][PC ? W * 32 : 1];
+    __shared__ double s_bsum[PC ? W : 1];
+    __shared__ float s_cheb[4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
     const int il0 = bp.cta_inst_lo[blockIdx.x], il1 = bp.cta_inst_hi[blockIdx.x];
@@ -868,8 +895,109 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     }
     __syncthreads();  // init_local
 
+    // ---- CTA-local Chebyshev preconditioner (PC) ---------------------------
+    // z = P(r): a fixed-degree Chebyshev iteration for A_cc z = r from z = 0,
+    // A_cc the CTA's diagonal block of rows (couplings to other CTAs
+    // dropped), block-Jacobi inner preconditioner; a fixed polynomial, so P is
+    // linear and symmetric and the outer PCG stays plain PCG.  Called by every
+    // thread of the CTA (it synchronises); inactive rows pass r = 0.
+    auto local_spmv = [&](const float4* buf, float3 in) {
+        float3 acc = mul(D, in);
+#pragma unroll
+        for (int k = 0; k < MAXW; ++k) {
+            if (k >= w) continue;
+            const int lr = col_at(k) - row0;
+            if ((unsigned)lr < (unsigned)nrows) acc = acc + mul(B[k], xyz(buf[lr]));
+        }
+        return acc;
+    };
+    auto block_sum = [&](double q) {
+        q = warp_sum(q);
+        if (lane == 0) s_bsum[warp] = q;
+        __syncthreads();
+        double tot = 0.0;
+#pragma unroll
+        for (int k = 0; k < W; ++k) tot += s_bsum[k];
+        __syncthreads();
+        return tot;
+    };
+    auto precond = [&](float3 rin) {
+        const float th_inv = s_cheb[1], sg = s_cheb[2], two_de = s_cheb[3];
+        float rho = 1.0f / sg;
+        float3 res = rin;
+        float3 d = mul(Mi, res) * th_inv;
+        float3 zc = d;
+        for (int m = 1; m < cfg.pc_degree; ++m) {
+            float4* buf = s_d[PC ? (m & 1) : 0];
+            buf[threadIdx.x] = f4(d);
+            __syncthreads();
+            res = res - local_spmv(buf, d);
+            const float rn = 1.0f / (2.0f * sg - rho);
+            const float3 mr = mul(Mi, res);
+            const float c0 = rn * rho, c1 = rn * two_de;
+            d = f3(fmaf(c0, d.x, c1 * mr.x), fmaf(c0, d.y, c1 * mr.y), fmaf(c0, d.z, c1 * mr.z));
+            zc = zc + d;
+            rho = rn;
+        }
+        return zc;
+    };
+    if (PC) {
+        // lambda_max of D^-1 A_cc by power iteration from a fixed +-1 vector,
+        // Rayleigh quotient v.A v / v.D v, times a margin; interval
+        // [lambda / ratio, lambda]
+        float3 pv = f3(0.f, 0.f, 0.f);
+        if (row) pv = f3(pc_sign(3 * i), pc_sign(3 * i + 1), pc_sign(3 * i + 2));
+        for (int it = 0; it < kPcPowerIts; ++it) {
+            float4* buf = s_d[PC ? (it & 1) : 0];
+            buf[threadIdx.x] = f4(pv);
+            __syncthreads();
+            const float3 wv = mul(Mi, local_spmv(buf, pv));
+            const double nn = block_sum(dot3d(wv, wv));
+            const float sc = nn > 0.0 ? (float)(1.0 / sqrt(nn)) : 0.0f;
+            pv = wv * sc;
+        }
+        float4* buf = s_d[PC ? (kPcPowerIts & 1) : 0];
+        buf[threadIdx.x] = f4(pv);
+        __syncthreads();
+        const double num = block_sum(dot3d(pv, local_spmv(buf, pv)));
+        const double den = block_sum(dot3d(pv, mul(D, pv)));
+        if (threadIdx.x == 0) {
+            double hi = den > 0.0 ? kPcMargin * num / den : 1.0;
+            if (!(hi > 0.0) || !isfinite(hi)) hi = 1.0;
+            const double lo = hi / (double)cfg.pc_ratio;
+            const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo);
+            s_cheb[0] = (float)theta;
+            s_cheb[1] = (float)(1.0 / theta);
+            s_cheb[2] = (float)(theta / delta);
+            s_cheb[3] = (float)(2.0 / delta);
+        }
+        __syncthreads();
+    }
+
     // ---- phase 0 -------------------------------------------------------
-    {
+    float3 pc_zb = f3(0.f, 0.f, 0.f);  // P(b), for the start of a scaled guess
+    if (PC) {
+        float3 zb = f3(0.f, 0.f, 0.f);
+        if (row) {
+            r = b;
+            if (warm) {
+                x = xyz(v.x[i]);
+                float3 ax = mul(D, x);
+#pragma unroll
+                for (int k = 0; k < MAXW; ++k)
+                    if (k < w) ax = ax + mul(B[k], xyz(v.x[col_at(k)]));
+                r = b - ax;
+            }
+        }
+        zb = precond(b);
+        z = warm ? precond(r) : zb;
+        pc_zb = zb;
+        if (row) {
+            zp0[i].z = f4(z);
+            s_z[threadIdx.x] = f4(z);
+        }
+        start_partials(spart + warp * kSlotW, lane == 0 && has, b, zb, x, r, z);
+    } else {
         float3 zb = f3(0.f, 0.f, 0.f);
         if (row) {
             zb = mul(Mi, b);
@@ -896,7 +1024,8 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     if (ok && warm) {
         // the scaled guess, or the zero guess where the instance fell back
         if (row) {
-            start_row(li[li_idx], b, Mi, x, r, z);
+            if (PC) start_row_linear(li[li_idx], b, pc_zb, x, r, z);
+            else start_row(li[li_idx], b, Mi, x, r, z);
             zp0[i].z = f4(z);
             s_z[threadIdx.x] = f4(z);
         }
@@ -976,13 +1105,20 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         if (!SYNC && s_exit) break;
 
         double rz = 0.0, rr = 0.0;
-        if (row && !li[li_idx].done) {
-            const LocalInst& L = li[li_idx];
-            const float alpha = L.alpha;
-            ZP* En = (L.iter & 1) ? zp0 : zp1;
+        const bool act = row && !li[li_idx].done;
+        if (act) {
+            const float alpha = li[li_idx].alpha;
             x = f3(fmaf(alpha, p.x, x.x), fmaf(alpha, p.y, x.y), fmaf(alpha, p.z, x.z));
             r = f3(fmaf(-alpha, ap.x, r.x), fmaf(-alpha, ap.y, r.y), fmaf(-alpha, ap.z, r.z));
-            z = mul(Mi, r);
+        }
+        if (PC) {
+            const float3 zn = precond(act ? r : f3(0.f, 0.f, 0.f));
+            if (act) z = zn;
+        }
+        if (act) {
+            const LocalInst& L = li[li_idx];
+            ZP* En = (L.iter & 1) ? zp0 : zp1;
+            if (!PC) z = mul(Mi, r);
             En[i].z = f4(z);
             s_z[threadIdx.x] = f4(z);
             rz = (double)r.x * z.x + (double)r.y * z.y + (double)r.z * z.z;

@@ -283,6 +283,17 @@ PYBIND11_MODULE(_chysx_native, m) {
              py::arg("dt"), py::arg("pos_in"), py::arg("vel_in"), py::arg("pos_out"), py::arg("vel_out"),
              py::arg("cuda_stream") = 0,
              "One step from (pos_in, vel_in) into (pos_out, vel_out) without a copy pass.")
+        .def("set_row_order", [](PyClothSimulator& s, int mode) { check(chysx_cloth_set_row_order(s.h(), mode)); },
+             py::arg("mode"), "0: the caller's particle order; 1: spatially compact row blocks")
+        .def("set_preconditioner",
+             [](PyClothSimulator& s, const std::string& kind, int degree, float ratio) {
+                 int k = -1;
+                 if (kind == "block_jacobi") k = 0;
+                 if (kind == "chebyshev") k = 1;
+                 if (k < 0) throw py::value_error("preconditioner kind must be 'block_jacobi' or 'chebyshev'");
+                 check(chysx_cloth_set_preconditioner(s.h(), k, degree, ratio));
+             },
+             py::arg("kind"), py::arg("degree") = 7, py::arg("ratio") = 30.0f)
         .def("set_pcg_iterations",
              [](PyClothSimulator& s, int m) { check(chysx_cloth_set_pcg_iterations(s.h(), m)); }, py::arg("max_iter"))
         .def("pcg_iterations",

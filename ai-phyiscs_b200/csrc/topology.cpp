@@ -2,6 +2,7 @@
 #include "topology.h"
 
 #include <algorithm>
+#include <cmath>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -61,6 +62,46 @@ void build_vertex_triangles(int n, const std::vector<int>& tris, std::vector<int
         for (int a = 0; a < 3; ++a) list[fill[tris[3 * t + a]]++] = t;
 }
 
+namespace {
+
+void bisect(const float* pos, std::vector<int>& ord, int lo, int hi, int block) {
+    const int m = hi - lo;
+    if (m <= kSlice) return;
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int k = lo; k < hi; ++k)
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = std::min(mn[a], pos[3 * (size_t)ord[k] + a]);
+            mx[a] = std::max(mx[a], pos[3 * (size_t)ord[k] + a]);
+        }
+    int ax = 0;
+    for (int a = 1; a < 3; ++a)
+        if (mx[a] - mn[a] > mx[ax] - mn[ax]) ax = a;
+    const int unit = m > 2 * block ? block : kSlice;
+    int left = (m / 2 + unit - 1) / unit * unit;
+    if (left >= m) left = (m - 1) / kSlice * kSlice;
+    if (left <= 0) return;
+    auto less = [&](int a, int b) {
+        const float pa = pos[3 * (size_t)a + ax], pb = pos[3 * (size_t)b + ax];
+        return pa < pb || (pa == pb && a < b);
+    };
+    std::nth_element(ord.begin() + lo, ord.begin() + lo + left, ord.begin() + hi, less);
+    bisect(pos, ord, lo, lo + left, block);
+    bisect(pos, ord, lo + left, hi, block);
+}
+
+}  // namespace
+
+void spatial_order(const float* pos, int n, const std::vector<int>& inst_offsets, std::vector<int>& order,
+                   int block) {
+    order.resize(n);
+    for (int k = 0; k < n; ++k) order[k] = k;
+    if (inst_offsets.empty()) {
+        bisect(pos, order, 0, n, block);
+        return;
+    }
+    for (size_t b = 0; b + 1 < inst_offsets.size(); ++b) bisect(pos, order, inst_offsets[b], inst_offsets[b + 1], block);
+}
+
 void build_plan(const std::vector<int>& inst_slice, int grid, HostPlan& o) {
     o = HostPlan();
     const int n_inst = (int)inst_slice.size() - 1;
@@ -116,7 +157,8 @@ void build_dihedrals(const std::vector<int>& tris, std::vector<int>& out) {
 void build_topology(int n_ext, const std::vector<int>& tris_ext, bool use_tris,
                     const std::vector<int>& edges_ext, bool use_springs,
                     const std::vector<int>& pins_ext, const std::vector<int>& inst_offsets,
-                    HostTopology& o, const std::vector<int>& dih_ext, bool use_bending) {
+                    HostTopology& o, const std::vector<int>& dih_ext, bool use_bending,
+                    const std::vector<int>& order) {
     if (n_ext < 0) throw std::invalid_argument("negative particle count");
     o = HostTopology();
     o.n_ext = n_ext;
@@ -130,20 +172,28 @@ void build_topology(int n_ext, const std::vector<int>& tris_ext, bool use_tris,
 
     // ---- internal row layout
     int n = n_ext;
-    const int n_inst = inst_offsets.empty() ? 1 : (int)inst_offsets.size() - 1;
-    std::vector<int> inst_of;  // instance of every particle (instances only)
-    if (!inst_offsets.empty()) {
-        if (n_inst < 1 || inst_offsets.front() != 0 || inst_offsets.back() != n_ext)
+    if (!order.empty() && (int)order.size() != n_ext)
+        throw std::invalid_argument("row order must list every particle once");
+    // a row order without instances is one instance over all particles
+    const std::vector<int> whole = {0, n_ext};
+    const std::vector<int>& offs = inst_offsets.empty() && !order.empty() ? whole : inst_offsets;
+    const int n_inst = offs.empty() ? 1 : (int)offs.size() - 1;
+    std::vector<int> inst_of;  // instance of every particle (mapped layouts only)
+    if (!offs.empty()) {
+        if (n_inst < 1 || offs.front() != 0 || offs.back() != n_ext)
             throw std::invalid_argument("instance offsets must run from 0 to the particle count");
-        o.ext_to_row.resize(n_ext);
+        o.ext_to_row.assign(n_ext, -1);
         inst_of.resize(n_ext);
         o.inst_slice.assign(n_inst + 1, 0);
         int row = 0;
         for (int b = 0; b < n_inst; ++b) {
-            const int lo = inst_offsets[b], hi = inst_offsets[b + 1];
+            const int lo = offs[b], hi = offs[b + 1];
             if (hi <= lo) throw std::invalid_argument("instance offsets must be strictly increasing");
-            for (int e = lo; e < hi; ++e) {
-                o.ext_to_row[e] = row + (e - lo);
+            for (int k = lo; k < hi; ++k) {
+                const int e = order.empty() ? k : order[k];
+                if (e < lo || e >= hi || o.ext_to_row[e] >= 0)
+                    throw std::invalid_argument("row order is not a permutation within every instance");
+                o.ext_to_row[e] = row + (k - lo);
                 inst_of[e] = b;
             }
             row += ((hi - lo) + kSlice - 1) / kSlice * kSlice;

@@ -68,11 +68,22 @@ struct HostTopology {
 // third vertex of the face containing the directed edge v0 -> v1, v3 = that
 // of the face containing v1 -> v0) add every pair of their vertices to the
 // pattern when use_bending.
+// `order` (empty: the caller's order) lists the particles in internal row
+// order; within every instance it must be a permutation of that instance's
+// particle range.
 void build_topology(int n, const std::vector<int>& tris, bool use_tris,
                     const std::vector<int>& edges, bool use_springs,
                     const std::vector<int>& pins, const std::vector<int>& inst_offsets,
                     HostTopology& out, const std::vector<int>& dihedrals = {},
-                    bool use_bending = false);
+                    bool use_bending = false, const std::vector<int>& order = {});
+
+// A spatially compact row order: recursive coordinate bisection of each
+// instance's positions (xyz per particle) at the median of the longest box
+// side, with split sizes that are multiples of `block` rows (512) while a
+// part spans more than two blocks and of 32 rows below, so every 32-row slice
+// and every aligned block of rows is a compact patch.  Deterministic.
+void spatial_order(const float* pos, int n, const std::vector<int>& inst_offsets, std::vector<int>& order,
+                   int block = 512);
 
 // Dihedrals of a consistently oriented triangle mesh as the reference finds
 // them (src/cloth/cloth_simulator.cu:467-506): every interior edge v0 < v1

@@ -334,6 +334,10 @@ def run_ours(args, rank, world, local_rank):
             params, _ = learned.load(args.net)
             sim.sim.set_network(params)
         sim.sim.set_solver(sc["max_iter"], rel_tol, args.warm)
+        if args.pc == "chebyshev":
+            sim.sim.set_preconditioner("chebyshev", args.pc_degree, args.pc_ratio)
+        if args.row_order == "spatial":
+            sim.sim.set_row_order(1)
         return sim
 
     g = make_sim()
@@ -446,6 +450,20 @@ def run_ours(args, rank, world, local_rank):
     if offs is not None:
         it_b = g.sim.instance_stats()[0].astype(np.float64)
         cpu_iters = float(np.sum(np.diff(offs) * it_b) / np.sum(np.diff(offs)))
+    # with the CTA-local preconditioner the CPU port and the reference module,
+    # both block-Jacobi, are charged the block-Jacobi iterations the same
+    # steps need (counted on an untimed block-Jacobi run of the same steps)
+    bj_iters = None
+    pc_used = bool(g.sim.preconditioner()[3])
+    if pc_used and args.legs == "all":
+        bj = GpuCloth(sc, max_iter=sc["max_iter"], rel_tol=rel_tol, warm_start="zero", instances=offs)
+        bj.sim.set_solver(sc["max_iter"], rel_tol, args.warm)
+        counts = []
+        for _ in range(args.warmup + args.steps):
+            bj.step()
+            counts.append(bj.stats()[0])
+        bj_iters = float(np.mean(counts[args.warmup:]))
+        cpu_iters = bj_iters
     cpu_value = None
     if args.legs == "all":
         t_asm, t_it, m = cpu_step_costs(sc, 1, int(cpu_iters), budget_s=args.cpu_budget)
@@ -454,7 +472,7 @@ def run_ours(args, rank, world, local_rank):
     ref_gpu = None
     if args.reference_gpu and offs is None and args.legs == "all":
         try:
-            ref_gpu = time_reference_gpu(sc, int(round(mean_iters)))
+            ref_gpu = time_reference_gpu(sc, int(round(bj_iters if bj_iters else mean_iters)))
         except Exception as exc:  # reported, never fatal to our own line
             ref_gpu = f"failed: {exc}"
 
@@ -467,8 +485,11 @@ def run_ours(args, rank, world, local_rank):
                    "sync_mode": args.sync,
                    "instances": 1 if offs is None else len(offs) - 1,
                    "pcg_kernel": g.sim.solver_info()[0], "pcg_grid": g.sim.solver_info()[1],
-                   "pcg_block": g.sim.solver_info()[2], "l2": "flushed between steps (256 MiB write)"},
+                   "pcg_block": g.sim.solver_info()[2], "l2": "flushed between steps (256 MiB write)",
+                   "preconditioner": dict(zip(("kind", "degree", "ratio", "in_use"), g.sim.preconditioner())),
+                   "row_order": args.row_order},
         "pcg_iters_per_step": mean_iters,
+        "block_jacobi_iters_per_step": bj_iters,
         "pcg_iters_per_step_minmax": [int(iters.min()), int(iters.max())],
         "solve_status": sorted(set(int(s) for s in statuses)),
         "us_per_pcg_iteration": float(np.sum(solve_ms) * 1e3 / np.sum(iters)),
@@ -490,9 +511,10 @@ def run_ours(args, rank, world, local_rank):
         "e2e": None if not e2e_steps else {"value": e2e_steps * world / (e2e_ms_max * 1e-3), "unit": "steps/s",
                 "h2d_bytes_per_step": 2 * 12 * n, "d2h_bytes_per_step": 2 * 12 * n},
         "reference_gpu": None if ref_gpu is None else {
-            "value": ref_gpu, "unit": "steps/s", "pcg_iterations_fixed": int(round(mean_iters)),
+            "value": ref_gpu, "unit": "steps/s",
+            "pcg_iterations_fixed": int(round(bj_iters if bj_iters else mean_iters)),
             "note": "compiled reference ClothSimulator (springs enabled), same scene with geometric-mean "
-                    "stiffness, PCG fixed at our mean iterations/step, stream 0"},
+                    "stiffness, PCG fixed at the block-Jacobi iterations/step the same steps take, stream 0"},
         "gpu_launches": 4 * args.steps,
         "clocks": clk,
         "wall_s": wall,
@@ -518,6 +540,13 @@ def main():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--grid", type=int, default=0)
     ap.add_argument("--sync", type=int, default=0, help="persistent kernels: 0 grid counter barrier, 1 polled slots")
+    ap.add_argument("--pc", default="chebyshev", choices=["block_jacobi", "chebyshev"],
+                    help="preconditioner: the reference's block-Jacobi, or the CTA-local Chebyshev (used where "
+                         "the register-resident kernel runs; elsewhere block-Jacobi)")
+    ap.add_argument("--pc-degree", type=int, default=7)
+    ap.add_argument("--row-order", default="spatial", choices=["caller", "spatial"],
+                    help="rows in the caller's particle order, or in spatially compact blocks")
+    ap.add_argument("--pc-ratio", type=float, default=30.0)
     ap.add_argument("--net", default=os.path.join(ROOT, "ai-phyiscs_b200", "chysx", "data", "warmstart.npz"))
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--reference-gpu", type=int, default=1, help="also time the compiled reference module")

@@ -366,6 +366,33 @@ int chysx_cloth_autotune(chysx_cloth* h, float dt, int repetitions, uintptr_t st
 int chysx_cloth_autotune_results(const chysx_cloth* h, int capacity, int* count, int32_t* config,
                                  float* solve_ms);
 int chysx_cloth_sync_mode(const chysx_cloth* h, int* mode);
+/* Row order (no counterpart in the reference, whose rows are the particles):
+ * mode 0 = the caller's particle order (default); mode 1 = spatially
+ * compact blocks: at the next topology build the particles of each instance
+ * are ordered by recursive coordinate bisection of their positions (split
+ * sizes multiples of 512 rows, then of 32), so every 32-row slice and every
+ * block of rows one CTA holds is a patch of the cloth.  The order is kept
+ * until the mesh, the instances or the particle count change.  Results do
+ * not depend on it beyond summation order; the CTA-local preconditioner
+ * gains from it.  row_of_particles reports the internal row of each of the
+ * n particles. */
+int chysx_cloth_set_row_order(chysx_cloth* h, int mode);
+int chysx_cloth_row_of_particles(const chysx_cloth* h, int n, int32_t* rows);
+
+/* Preconditioner (no counterpart in the reference, whose PCG preconditions
+ * with the 3x3 diagonal blocks, src/solver/pcg_solver.cu:29-51): kind 0 =
+ * block-Jacobi (default; the reference's iterates); kind 1 = CTA-local
+ * Chebyshev: z = p(D^-1 A_cc) D^-1 r, A_cc the diagonal block of the rows one
+ * CTA of the register-resident kernel holds (couplings to other CTAs left
+ * out), p the Chebyshev polynomial of odd `degree` on
+ * [lambda_max / ratio, lambda_max], lambda_max estimated per CTA and solve by
+ * power iteration with a 10% margin.  A fixed polynomial, so the outer
+ * iteration stays plain PCG with the same stopping test (||r|| / ||b||);
+ * odd degrees keep p positive on the whole spectrum.  Kind 1 applies where
+ * the register-resident kernel runs with synchronisation mode 0; in_use
+ * reports whether the last graph build uses it. */
+int chysx_cloth_set_preconditioner(chysx_cloth* h, int kind, int degree, float ratio);
+int chysx_cloth_preconditioner(const chysx_cloth* h, int* kind, int* degree, float* ratio, int* in_use);
 /* Kernel used at the last graph build: path 0 register-resident persistent,
  * 1 graph loop, 2 streamed persistent; with its grid and block size. */
 int chysx_cloth_solver_info(const chysx_cloth* h, int* path, int* grid, int* block);

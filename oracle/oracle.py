@@ -68,6 +68,7 @@ def lib():
         L.orc_dump_system.argtypes = [vp, _f64p, _i32p, _i32p, _f64p, _f64p, _f64p]
         L.orc_spmv.argtypes = [vp, _f64p, _f64p]
         L.orc_contact_spmv.argtypes = [vp, _f64p, _f64p]
+        L.orc_set_preconditioner.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
         L.orc_add_static_plane.argtypes = [vp, _f32p, ctypes.c_float]
         L.orc_add_static_box.argtypes = [vp, _f32p, _f32p, _f32p, _f32p, _f32p]
         L.orc_clear_static_shapes.argtypes = [vp]
@@ -227,6 +228,11 @@ class OracleCloth:
         y = np.zeros_like(x)
         _check(self._L.orc_contact_spmv(self._h, _p(x, _f64p), _p(y, _f64p)))
         return y
+
+    def set_preconditioner(self, degree=0, ratio=30.0, block_rows=512):
+        """0: block-Jacobi (the reference's); odd degree: the product's
+        block-local Chebyshev preconditioner on blocks of block_rows rows."""
+        _check(self._L.orc_set_preconditioner(self._h, int(degree), float(ratio), int(block_rows)))
 
     def add_static_plane(self, n, d):
         n = np.ascontiguousarray(n, np.float32).reshape(3)
