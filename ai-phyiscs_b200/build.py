@@ -27,7 +27,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB = os.path.join(PKG, "libchysx_cloth.so")
 CU_SOURCES = [os.path.join(CSRC, f) for f in ("cloth_sim.cu", "topology.cpp")]
 CU_DEPS = CU_SOURCES + [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))
-                        if f.endswith((".cuh", ".h"))] + [os.path.join(INCLUDE, "chysx_cloth.h")]
+                        if f.endswith((".cuh", ".h"))] + [os.path.join(INCLUDE, f) for f in ("chysx_cloth.h",
+                                                                                          "chysx_vbd.h")]
 
 
 def _ext_suffix() -> str:
@@ -35,7 +36,8 @@ def _ext_suffix() -> str:
 
 
 NATIVE = os.path.join(PKG, "_chysx_native" + _ext_suffix())
-PY_SOURCES = [os.path.join(CSRC, "pybind_module.cpp"), os.path.join(INCLUDE, "chysx_cloth.h")]
+PY_SOURCES = [os.path.join(CSRC, "pybind_module.cpp"), os.path.join(INCLUDE, "chysx_cloth.h"),
+              os.path.join(INCLUDE, "chysx_vbd.h")]
 
 
 def _stale(target: str, deps) -> bool:

@@ -28,7 +28,8 @@ from . import _chysx_native
 
 ClothMaterial = _chysx_native.ClothMaterial
 ClothSimulator = _chysx_native.ClothSimulator
+ClothVBDSolver = _chysx_native.ClothVBDSolver
 
 __version__ = "0.1.0"
 
-__all__ = ["ClothMaterial", "ClothSimulator", "__version__"]
+__all__ = ["ClothMaterial", "ClothSimulator", "ClothVBDSolver", "__version__"]

@@ -111,6 +111,17 @@ SIGNATURES = {
     "chysx_cloth_preconditioner": (ctypes.c_int, [H, ip, ip, f32p, ip]),
     "chysx_cloth_enable_timing": (ctypes.c_int, [H, ctypes.c_int]),
     "chysx_cloth_last_timing": (ctypes.c_int, [H, f32p, f32p, f32p]),
+    "chysx_vbd_create": (ctypes.c_int, [ctypes.POINTER(H)]),
+    "chysx_vbd_destroy": (ctypes.c_int, [H]),
+    "chysx_vbd_build_cloth_coloring": (ctypes.c_int, [H, i32p, ctypes.c_int, i32p, ctypes.c_int, ctypes.c_int]),
+    "chysx_vbd_set_coloring": (ctypes.c_int, [H, i32p, ctypes.c_int]),
+    "chysx_vbd_build_tri_adjacency": (ctypes.c_int, [H, i32p, ctypes.c_int, ctypes.c_int]),
+    "chysx_vbd_build_edge_adjacency": (ctypes.c_int, [H, i32p, ctypes.c_int, ctypes.c_int]),
+    "chysx_vbd_num_colors": (ctypes.c_int, [H, ip]),
+    "chysx_vbd_colors": (ctypes.c_int, [H, i32p, ctypes.c_int]),
+    "chysx_vbd_step_cloth": (ctypes.c_int, [H, u, u, u, ctypes.c_int, u, u, u, u, ctypes.c_int, u, u, u, u,
+                                            ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                            ctypes.c_float, ctypes.c_int, u]),
     "chysx_topology_pattern": (ctypes.c_int, [ctypes.c_int, i32p, ctypes.c_int, i32p, ctypes.c_int,
                                               i32p, i32p, ctypes.c_int, ip, ip, ip]),
 }
@@ -412,6 +423,55 @@ class Cloth:
         check(self._L.chysx_cloth_debug_dump(self.h, _p(diag, f32p), _p(rp, i32p), _p(col, i32p),
                                              _p(vals, f32p), _p(rhs, f32p), _p(dx, f32p)))
         return diag, rp, col[:nnz], vals[:nnz], rhs, dx
+
+
+class Vbd:
+    """The cloth VBD solver through the C ABI (include/chysx_vbd.h)."""
+
+    def __init__(self):
+        self._L = lib()
+        h = H()
+        check(self._L.chysx_vbd_create(ctypes.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self._L.chysx_vbd_destroy(h)
+
+    def build_cloth_coloring(self, tris, edges, n):
+        t = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+        e = np.ascontiguousarray(edges, np.int32).reshape(-1, 4)
+        check(self._L.chysx_vbd_build_cloth_coloring(self.h, _p(t, i32p), t.shape[0], _p(e, i32p), e.shape[0], n))
+
+    def set_coloring(self, colors):
+        c = np.ascontiguousarray(colors, np.int32)
+        check(self._L.chysx_vbd_set_coloring(self.h, _p(c, i32p), c.shape[0]))
+
+    def build_tri_adjacency(self, tris, n):
+        t = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+        check(self._L.chysx_vbd_build_tri_adjacency(self.h, _p(t, i32p), t.shape[0], n))
+
+    def build_edge_adjacency(self, edges, n):
+        e = np.ascontiguousarray(edges, np.int32).reshape(-1, 4)
+        check(self._L.chysx_vbd_build_edge_adjacency(self.h, _p(e, i32p), e.shape[0], n))
+
+    def num_colors(self):
+        v = ctypes.c_int()
+        check(self._L.chysx_vbd_num_colors(self.h, ctypes.byref(v)))
+        return v.value
+
+    def colors(self, n):
+        out = np.zeros(n, np.int32)
+        check(self._L.chysx_vbd_colors(self.h, _p(out, i32p), n))
+        return out
+
+    def step_cloth(self, pos, vel, inv_mass, n, tris, poses, areas, mats, n_tris, edges, rest_angle, rest_length,
+                   props, n_edges, gravity, dt, iterations, stream=0):
+        """Device addresses of the step's arrays (see the header)."""
+        check(self._L.chysx_vbd_step_cloth(self.h, pos, vel, inv_mass, n, tris, poses, areas, mats, n_tris, edges,
+                                           rest_angle, rest_length, props, n_edges, *[float(g) for g in gravity],
+                                           float(dt), int(iterations), stream))
 
 
 def topology_pattern(n, tris, edges=None):

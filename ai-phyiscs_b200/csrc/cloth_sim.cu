@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "../../include/chysx_cloth.h"
+#include "../../include/chysx_vbd.h"
 #include "cloth_kernels.cuh"
 #include "pcg_persistent.cuh"
 #include "topology.h"
@@ -1782,10 +1783,17 @@ private:
 
 }  // namespace chysx_b200
 
+#include "vbd_host.cuh"
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
 using chysx_b200::ClothSim;
+using chysx_b200::VbdSolver;
+
+struct chysx_vbd {
+    VbdSolver solver;
+};
 
 struct chysx_cloth {
     ClothSim sim;
@@ -2159,6 +2167,57 @@ int chysx_topology_pattern(int n, const int32_t* tris, int n_tris, const int32_t
             if (topo.nnz() > max_nnz) throw std::invalid_argument("chysx_topology_pattern: col_indices too small");
             std::copy(topo.csr_col.begin(), topo.csr_col.end(), col_indices);
         }
+    });
+}
+
+// ---- cloth VBD solver (include/chysx_vbd.h) -------------------------------
+#define CHYSX_VBD(h)          \
+    if (!(h)) return null_handle()
+
+int chysx_vbd_create(chysx_vbd** out) {
+    if (!out) return null_handle();
+    return guard([&] { *out = new chysx_vbd(); });
+}
+int chysx_vbd_destroy(chysx_vbd* h) {
+    delete h;
+    return CHYSX_OK;
+}
+int chysx_vbd_build_cloth_coloring(chysx_vbd* h, const int32_t* tris, int n_tris, const int32_t* edges, int n_edges,
+                                   int n_particles) {
+    CHYSX_VBD(h);
+    return guard([&] { h->solver.build_cloth_coloring(tris, n_tris, edges, n_edges, n_particles); });
+}
+int chysx_vbd_set_coloring(chysx_vbd* h, const int32_t* colors, int n_particles) {
+    CHYSX_VBD(h);
+    return guard([&] { h->solver.set_coloring(colors, n_particles); });
+}
+int chysx_vbd_build_tri_adjacency(chysx_vbd* h, const int32_t* tris, int n_tris, int n_particles) {
+    CHYSX_VBD(h);
+    return guard([&] { h->solver.build_tri_adjacency(tris, n_tris, n_particles); });
+}
+int chysx_vbd_build_edge_adjacency(chysx_vbd* h, const int32_t* edges, int n_edges, int n_particles) {
+    CHYSX_VBD(h);
+    return guard([&] { h->solver.build_edge_adjacency(edges, n_edges, n_particles); });
+}
+int chysx_vbd_num_colors(const chysx_vbd* h, int* out) {
+    CHYSX_VBD(h);
+    if (out) *out = h->solver.num_colors();
+    return CHYSX_OK;
+}
+int chysx_vbd_colors(const chysx_vbd* h, int32_t* out, int n_particles) {
+    CHYSX_VBD(h);
+    return guard([&] { h->solver.colors(out, n_particles); });
+}
+int chysx_vbd_step_cloth(chysx_vbd* h, uintptr_t pos, uintptr_t vel, uintptr_t inv_mass, int n_particles,
+                         uintptr_t tri_indices, uintptr_t tri_poses, uintptr_t tri_areas, uintptr_t tri_materials,
+                         int n_tris, uintptr_t edge_indices, uintptr_t edge_rest_angle, uintptr_t edge_rest_length,
+                         uintptr_t edge_bending_props, int n_edges, float gx, float gy, float gz, float dt,
+                         int iterations, uintptr_t stream) {
+    CHYSX_VBD(h);
+    return guard([&] {
+        h->solver.step_cloth(pos, vel, inv_mass, n_particles, tri_indices, tri_poses, tri_areas, tri_materials, n_tris,
+                             edge_indices, edge_rest_angle, edge_rest_length, edge_bending_props, n_edges, gx, gy, gz,
+                             dt, iterations, stream);
     });
 }
 

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/chysx_cloth.h"
+#include "../../include/chysx_vbd.h"
 
 namespace py = pybind11;
 
@@ -38,6 +39,18 @@ public:
 
 private:
     chysx_cloth* h_ = nullptr;
+};
+
+class PyVbd {
+public:
+    PyVbd() { check(chysx_vbd_create(&h_)); }
+    ~PyVbd() { chysx_vbd_destroy(h_); }
+    PyVbd(const PyVbd&) = delete;
+    PyVbd& operator=(const PyVbd&) = delete;
+    chysx_vbd* h() const { return h_; }
+
+private:
+    chysx_vbd* h_ = nullptr;
 };
 
 using F32 = py::array_t<float, py::array::c_style | py::array::forcecast>;
@@ -429,4 +442,61 @@ PYBIND11_MODULE(_chysx_native, m) {
                                              dx.mutable_data()));
             return py::make_tuple(diag, row_offsets, col_indices, values, rhs, dx);
         });
+
+    // ---- ClothVBDSolver (src/bindings.cpp:1868-1957) --------------------
+    py::class_<PyVbd>(m, "ClothVBDSolver",
+                      "Vertex Block Descent solver for cloth (triangle membrane + dihedral bending).")
+        .def(py::init<>())
+        .def("build_cloth_coloring",
+             [](PyVbd& s, I32 tris, I32 edges, int n) {
+                 if (tris.ndim() != 2 || tris.shape(1) != 3) throw py::value_error("tri_indices must be (T, 3) int32");
+                 if (edges.ndim() != 2 || edges.shape(1) != 4) throw py::value_error("edge_indices must be (E, 4) int32");
+                 check(chysx_vbd_build_cloth_coloring(s.h(), tris.data(), (int)tris.shape(0), edges.data(),
+                                                      (int)edges.shape(0), n));
+             },
+             py::arg("tri_indices"), py::arg("edge_indices"), py::arg("n_particles"),
+             "Build graph coloring from triangle + bending edge topology.")
+        .def("set_coloring",
+             [](PyVbd& s, I32 colors) {
+                 check(chysx_vbd_set_coloring(s.h(), colors.data(), (int)colors.size()));
+             },
+             py::arg("colors"), "Use an externally computed colour per particle.")
+        .def("build_tri_adjacency",
+             [](PyVbd& s, I32 tris, int n) {
+                 if (tris.ndim() != 2 || tris.shape(1) != 3) throw py::value_error("tri_indices must be (T, 3) int32");
+                 check(chysx_vbd_build_tri_adjacency(s.h(), tris.data(), (int)tris.shape(0), n));
+             },
+             py::arg("tri_indices"), py::arg("n_particles"), "Build per-vertex triangle adjacency (CSR).")
+        .def("build_edge_adjacency",
+             [](PyVbd& s, I32 edges, int n) {
+                 if (edges.ndim() != 2 || edges.shape(1) != 4) throw py::value_error("edge_indices must be (E, 4) int32");
+                 check(chysx_vbd_build_edge_adjacency(s.h(), edges.data(), (int)edges.shape(0), n));
+             },
+             py::arg("edge_indices"), py::arg("n_particles"), "Build per-vertex bending-edge adjacency (CSR).")
+        .def("step_cloth",
+             [](PyVbd& s, std::uintptr_t pos, std::uintptr_t vel, std::uintptr_t inv_mass, int n, std::uintptr_t tri,
+                std::uintptr_t poses, std::uintptr_t areas, std::uintptr_t mats, int n_tris, std::uintptr_t edges,
+                std::uintptr_t rest_angle, std::uintptr_t rest_length, std::uintptr_t props, int n_edges, float gx,
+                float gy, float gz, float dt, int iterations, std::uintptr_t stream) {
+                 check(chysx_vbd_step_cloth(s.h(), pos, vel, inv_mass, n, tri, poses, areas, mats, n_tris, edges,
+                                            rest_angle, rest_length, props, n_edges, gx, gy, gz, dt, iterations,
+                                            stream));
+             },
+             py::arg("pos_ptr"), py::arg("vel_ptr"), py::arg("inv_mass_ptr"), py::arg("n_particles"),
+             py::arg("tri_indices_ptr"), py::arg("tri_poses_ptr"), py::arg("tri_areas_ptr"),
+             py::arg("tri_materials_ptr"), py::arg("n_tris"), py::arg("edge_indices_ptr"),
+             py::arg("edge_rest_angle_ptr"), py::arg("edge_rest_length_ptr"), py::arg("edge_bending_props_ptr"),
+             py::arg("n_edges"), py::arg("gx"), py::arg("gy"), py::arg("gz"), py::arg("dt"), py::arg("iterations"),
+             py::arg("cuda_stream") = 0, "Run one cloth VBD substep.")
+        .def("num_colors",
+             [](const PyVbd& s) {
+                 int c = 0;
+                 check(chysx_vbd_num_colors(s.h(), &c));
+                 return c;
+             })
+        .def("colors", [](const PyVbd& s, int n) {
+            py::array_t<int32_t> out(n);
+            check(chysx_vbd_colors(s.h(), out.mutable_data(), n));
+            return out;
+        }, py::arg("n_particles"));
 }

@@ -527,6 +527,85 @@ def run_ours(args, rank, world, local_rank):
     return line
 
 
+def run_vbd(args):
+    """Cloth VBD (ClothVBDSolver.step_cloth): steps/s of our CUDA-graph step
+    and of the compiled reference's solver on the same problem (same
+    colouring, arrays and iteration count), both device-timed."""
+    import glob
+
+    import torch
+
+    from chysx import capi, scenes, vbd_scenes
+
+    side = int(args.workload.replace("grid", "")) if args.workload.startswith("grid") else 256
+    sc = scenes.config_small(side=side)
+    vb = vbd_scenes.from_scene(sc, pinned=[side * (side - 1), side * side - 1])
+    n = vb["pos"].shape[0]
+    keys = ("pos", "vel", "inv_mass", "tri_indices", "tri_poses", "tri_areas", "tri_materials", "edge_indices",
+            "edge_rest_angle", "edge_rest_length", "edge_bending_props")
+    it = args.vbd_iterations
+
+    def arrays():
+        return {k: torch.from_numpy(np.ascontiguousarray(vb[k])).cuda() for k in keys}
+
+    def ptr_args(d):
+        return [d["pos"].data_ptr(), d["vel"].data_ptr(), d["inv_mass"].data_ptr(), n, d["tri_indices"].data_ptr(),
+                d["tri_poses"].data_ptr(), d["tri_areas"].data_ptr(), d["tri_materials"].data_ptr(),
+                vb["tri_indices"].shape[0], d["edge_indices"].data_ptr(), d["edge_rest_angle"].data_ptr(),
+                d["edge_rest_length"].data_ptr(), d["edge_bending_props"].data_ptr(), vb["edge_indices"].shape[0]]
+
+    def timed(step):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        return args.steps / (e0.elapsed_time(e1) * 1e-3)
+
+    ours = capi.Vbd()
+    ours.build_cloth_coloring(vb["tri_indices"], vb["edge_indices"], n)
+    ours.build_tri_adjacency(vb["tri_indices"], n)
+    ours.build_edge_adjacency(vb["edge_indices"], n)
+    d = arrays()
+    g = [float(x) for x in vb["gravity"]]
+    value = timed(lambda: ours.step_cloth(*ptr_args(d), g, float(vb["dt"]), it))
+    ref_value, ref_colors, same_value = None, None, None
+    ref_dir = os.path.join(ROOT, "oracle", "_ref")
+    if args.reference_gpu and glob.glob(os.path.join(ref_dir, "_chysx_ref_springs*.so")):
+        sys.path.insert(0, ref_dir)
+        import _chysx_ref_springs as R
+
+        ref = R.ClothVBDSolver()
+        ref.build_cloth_coloring(vb["tri_indices"], vb["edge_indices"], n)
+        ref.build_tri_adjacency(vb["tri_indices"], n)
+        ref.build_edge_adjacency(vb["edge_indices"], n)
+        ref_colors = int(ref.num_colors())
+        r = arrays()
+        ref_value = timed(lambda: ref.step_cloth(*ptr_args(r), *g, float(vb["dt"]), it))
+        # ours with the reference's colouring: the same sweeps, the same order
+        same = capi.Vbd()
+        same.set_coloring(np.asarray(ref.colors(), np.int32))
+        same.build_tri_adjacency(vb["tri_indices"], n)
+        same.build_edge_adjacency(vb["edge_indices"], n)
+        s2 = arrays()
+        same_value = timed(lambda: same.step_cloth(*ptr_args(s2), g, float(vb["dt"]), it))
+    return {"metric": "cloth VBD steps/s (ClothVBDSolver.step_cloth)", "value": value, "unit": "steps/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"grid{side}_vbd", "particles": n, "triangles": int(vb["tri_indices"].shape[0]),
+                       "bending_edges": int(vb["edge_indices"].shape[0]), "iterations": it,
+                       "colors": ours.num_colors(), "reference_colors": ref_colors},
+            "gpu_launches": args.steps * (2 + it * ours.num_colors()),
+            "reference_gpu": None if ref_value is None else {
+                "value": ref_value, "unit": "steps/s",
+                "ours_with_reference_coloring": same_value,
+                "note": "compiled reference ClothVBDSolver, same problem and iterations, stream 0"}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -554,6 +633,9 @@ def main():
                     help="K > 0: fixed K PCG iterations per step (rel_tol 0), the small profiling case")
     ap.add_argument("--oracle-steps", type=int, default=0,
                     help="N > 0: also report the position error vs the FP64 oracle over the first N steps")
+    ap.add_argument("--solver", default="pcg", choices=["pcg", "vbd"],
+                    help="pcg: the implicit step (headline); vbd: the cloth VBD solver and the reference's")
+    ap.add_argument("--vbd-iterations", type=int, default=10)
     ap.add_argument("--legs", default="all", choices=["all", "device"],
                     help="device: only the device-timed leg (no e2e, CPU or reference legs)")
     args = ap.parse_args()
@@ -563,6 +645,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.solver == "vbd":
+        print(json.dumps(run_vbd(args)), flush=True)
+        return
     if args.impl == "reference":
         line = run_reference_arm(args, rank)
         if line is not None:

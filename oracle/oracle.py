@@ -25,8 +25,8 @@ _i32p = ctypes.POINTER(ctypes.c_int)
 
 def build(force: bool = False) -> str:
     """Compile the oracle shared library in place (g++ -fopenmp)."""
-    src = os.path.join(_HERE, "cloth_oracle.cpp")
-    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+    srcs = [os.path.join(_HERE, f) for f in ("cloth_oracle.cpp", "vbd_oracle.cpp")]
+    if force or not os.path.exists(_LIB_PATH) or any(os.path.getmtime(_LIB_PATH) < os.path.getmtime(f) for f in srcs):
         subprocess.check_call(["make", "-s", "-C", _HERE, "libchysx_oracle.so"])
     return _LIB_PATH
 
@@ -68,6 +68,15 @@ def lib():
         L.orc_dump_system.argtypes = [vp, _f64p, _i32p, _i32p, _f64p, _f64p, _f64p]
         L.orc_spmv.argtypes = [vp, _f64p, _f64p]
         L.orc_contact_spmv.argtypes = [vp, _f64p, _f64p]
+        L.orc_vbd_step.argtypes = [ctypes.c_int, _f64p, _f64p, _f64p, _i32p, _f64p, _f64p, _f64p, ctypes.c_int,
+                                   _i32p, _f64p, _f64p, _f64p, ctypes.c_int, _i32p, _f64p, ctypes.c_double,
+                                   ctypes.c_int, ctypes.c_int]
+        L.orc_vbd_membrane.argtypes = [ctypes.c_int, _f64p, _f64p, _f64p] + [ctypes.c_double] * 5 + [_f64p, _f64p]
+        L.orc_vbd_membrane_energy.argtypes = [_f64p, _f64p] + [ctypes.c_double] * 3
+        L.orc_vbd_membrane_energy.restype = ctypes.c_double
+        L.orc_vbd_bending.argtypes = [ctypes.c_int, _f64p, _f64p] + [ctypes.c_double] * 5 + [_f64p, _f64p]
+        L.orc_vbd_hinge_angle.argtypes = [_f64p]
+        L.orc_vbd_hinge_angle.restype = ctypes.c_double
         L.orc_set_preconditioner.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
         L.orc_add_static_plane.argtypes = [vp, _f32p, ctypes.c_float]
         L.orc_add_static_box.argtypes = [vp, _f32p, _f32p, _f32p, _f32p, _f32p]
@@ -358,3 +367,59 @@ def run_scene(scene, steps=None, fp64=True, rel_tol=None, max_iter=None, warm_st
     if record:
         return p, v, np.array(iters), np.array(traj)
     return p, v, np.array(iters)
+
+
+# ---------------------------------------------------------------------------
+# Cloth VBD (restatement of the reference's ClothVBDSolver.step_cloth)
+# ---------------------------------------------------------------------------
+
+def _d(a, shape=None):
+    a = np.ascontiguousarray(a, np.float64)
+    return a if shape is None else a.reshape(shape)
+
+
+def vbd_step(vb, pos, vel, iterations, dt, fp64=True):
+    """One VBD step of the problem dict `vb` (chysx.vbd_scenes format) from
+    (pos, vel); returns the new (pos, vel) as float64 arrays."""
+    n = pos.shape[0]
+    p = _d(pos, (n, 3)).copy()
+    v = _d(vel, (n, 3)).copy()
+    tris = np.ascontiguousarray(vb["tri_indices"], np.int32)
+    edges = np.ascontiguousarray(vb["edge_indices"], np.int32)
+    colors = np.ascontiguousarray(vb["colors"], np.int32)
+    args = [_d(vb["inv_mass"]), tris, _d(vb["tri_poses"]), _d(vb["tri_areas"]), _d(vb["tri_materials"])]
+    eargs = [edges, _d(vb["edge_rest_angle"]), _d(vb["edge_rest_length"]), _d(vb["edge_bending_props"])]
+    g = _d(vb["gravity"])
+    rc = lib().orc_vbd_step(n, _p(p, _f64p), _p(v, _f64p), _p(args[0], _f64p), _p(tris, _i32p),
+                            _p(args[2], _f64p), _p(args[3], _f64p), _p(args[4], _f64p), tris.shape[0],
+                            _p(edges, _i32p), _p(eargs[1], _f64p), _p(eargs[2], _f64p), _p(eargs[3], _f64p),
+                            edges.shape[0], _p(colors, _i32p), _p(g, _f64p), float(dt), int(iterations),
+                            1 if fp64 else 0)
+    assert rc == 0
+    return p, v
+
+
+def vbd_membrane(which, x9, p9, dmi, area, mu, lam, damping=0.0, dt=1.0 / 60.0):
+    x9, p9, dmi = _d(x9, 9), _d(p9, 9), _d(dmi, 4)
+    f, h = np.zeros(3), np.zeros(9)
+    lib().orc_vbd_membrane(int(which), _p(x9, _f64p), _p(p9, _f64p), _p(dmi, _f64p), float(area), float(mu),
+                           float(lam), float(damping), float(dt), _p(f, _f64p), _p(h, _f64p))
+    return f, h.reshape(3, 3)
+
+
+def vbd_membrane_energy(x9, dmi, area, mu, lam):
+    x9, dmi = _d(x9, 9), _d(dmi, 4)
+    return float(lib().orc_vbd_membrane_energy(_p(x9, _f64p), _p(dmi, _f64p), float(area), float(mu), float(lam)))
+
+
+def vbd_bending(which, x12, p12, rest_angle, rest_length, k, damping=0.0, dt=1.0 / 60.0):
+    x12, p12 = _d(x12, 12), _d(p12, 12)
+    f, h = np.zeros(3), np.zeros(9)
+    lib().orc_vbd_bending(int(which), _p(x12, _f64p), _p(p12, _f64p), float(rest_angle), float(rest_length),
+                          float(k), float(damping), float(dt), _p(f, _f64p), _p(h, _f64p))
+    return f, h.reshape(3, 3)
+
+
+def vbd_hinge_angle(x12):
+    x12 = _d(x12, 12)
+    return float(lib().orc_vbd_hinge_angle(_p(x12, _f64p)))

@@ -15,6 +15,7 @@
 
 #include "cloth/cloth_material.h"
 #include "cloth/cloth_simulator.h"
+#include "solver/vbd_solver.h"
 #include "math/vec.cuh"
 
 #ifndef REF_MODULE_NAME
@@ -137,5 +138,49 @@ PYBIND11_MODULE(REF_MODULE_NAME, m) {
                 s.debug_copy_last_dx(dx.mutable_data());
             }
             return py::make_tuple(diag, rp, col, vals, rhs, dx);
+        });
+
+    // the reference's cloth VBD solver (src/bindings.cpp:1868-1957), plus a
+    // read-back of its colouring
+    using chysx::solver::VBDSolver;
+    py::class_<VBDSolver>(m, "ClothVBDSolver", py::module_local())
+        .def(py::init<>())
+        .def("build_cloth_coloring",
+             [](VBDSolver& s, py::array_t<int, py::array::c_style | py::array::forcecast> tris,
+                py::array_t<int, py::array::c_style | py::array::forcecast> edges, int n) {
+                 s.build_cloth_coloring(reinterpret_cast<const chysx::math::Vec3i*>(tris.data()), (int)tris.shape(0),
+                                        reinterpret_cast<const chysx::math::Vec4i*>(edges.data()),
+                                        (int)edges.shape(0), n);
+             })
+        .def("build_tri_adjacency",
+             [](VBDSolver& s, py::array_t<int, py::array::c_style | py::array::forcecast> tris, int n) {
+                 s.build_tri_adjacency(reinterpret_cast<const chysx::math::Vec3i*>(tris.data()), (int)tris.shape(0), n);
+             })
+        .def("build_edge_adjacency",
+             [](VBDSolver& s, py::array_t<int, py::array::c_style | py::array::forcecast> edges, int n) {
+                 s.build_edge_adjacency(reinterpret_cast<const chysx::math::Vec4i*>(edges.data()), (int)edges.shape(0),
+                                        n);
+             })
+        .def("step_cloth",
+             [](VBDSolver& s, std::uintptr_t pos, std::uintptr_t vel, std::uintptr_t inv_mass, int n, std::uintptr_t tri,
+                std::uintptr_t poses, std::uintptr_t areas, std::uintptr_t mats, int n_tris, std::uintptr_t edges,
+                std::uintptr_t ra, std::uintptr_t rl, std::uintptr_t props, int n_edges, float gx, float gy, float gz,
+                float dt, int iterations) {
+                 using namespace chysx::math;
+                 chysx::DeviceSpan<Vec3f> p(reinterpret_cast<Vec3f*>(pos), n), v(reinterpret_cast<Vec3f*>(vel), n);
+                 chysx::DeviceSpan<float> w(reinterpret_cast<float*>(inv_mass), n);
+                 s.step_cloth(p, v, w, reinterpret_cast<const Vec3i*>(tri), n_tris, reinterpret_cast<const Mat2f*>(poses),
+                              reinterpret_cast<const float*>(areas), reinterpret_cast<const float*>(mats),
+                              reinterpret_cast<const Vec4i*>(edges), n_edges, reinterpret_cast<const float*>(ra),
+                              reinterpret_cast<const float*>(rl), reinterpret_cast<const float*>(props),
+                              Vec3f(gx, gy, gz), dt, iterations, 0);
+             })
+        .def("num_colors", &VBDSolver::num_colors)
+        .def("colors", [](const VBDSolver& s) {
+            const int n = s.num_particles();
+            py::array_t<int> out(n);
+            if (n > 0) cudaMemcpy(out.mutable_data(), s.particle_colors_ptr(), (size_t)n * sizeof(int),
+                                  cudaMemcpyDeviceToHost);
+            return out;
         });
 }

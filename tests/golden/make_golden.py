@@ -139,6 +139,44 @@ def make_contact(out_dir=HERE):
     print("two sheets done", flush=True)
 
 
+def scene_vbd():
+    """Config 1's patch as a VBD problem (chysx.vbd_scenes.from_scene): the
+    two far corners held (inverse mass 0), membrane mu = lambda = 2e3,
+    bending k = 5e-3, damping 1e-3 on both."""
+    from chysx import vbd_scenes
+
+    return vbd_scenes.from_scene(scenes.config_small(), pinned=[90, 99])
+
+
+def make_vbd(out_dir=HERE, steps=40, iterations=10, record=(0, 1, 9, 10, 29, 30, 39)):
+    import _chysx_ref_springs as mod
+
+    vb = scene_vbd()
+    n = vb["pos"].shape[0]
+    s = mod.ClothVBDSolver()
+    s.build_cloth_coloring(vb["tri_indices"], vb["edge_indices"], n)
+    s.build_tri_adjacency(vb["tri_indices"], n)
+    s.build_edge_adjacency(vb["edge_indices"], n)
+    dev = {k: torch.from_numpy(np.ascontiguousarray(vb[k])).cuda() for k in
+           ("pos", "vel", "inv_mass", "tri_indices", "tri_poses", "tri_areas", "tri_materials", "edge_indices",
+            "edge_rest_angle", "edge_rest_length", "edge_bending_props")}
+    out = {"colors": np.array(s.colors()), "iterations": np.array(iterations)}
+    g = [float(v) for v in vb["gravity"]]
+    for k in range(steps):
+        s.step_cloth(dev["pos"].data_ptr(), dev["vel"].data_ptr(), dev["inv_mass"].data_ptr(), n,
+                     dev["tri_indices"].data_ptr(), dev["tri_poses"].data_ptr(), dev["tri_areas"].data_ptr(),
+                     dev["tri_materials"].data_ptr(), vb["tri_indices"].shape[0], dev["edge_indices"].data_ptr(),
+                     dev["edge_rest_angle"].data_ptr(), dev["edge_rest_length"].data_ptr(),
+                     dev["edge_bending_props"].data_ptr(), vb["edge_indices"].shape[0], *g, float(vb["dt"]),
+                     iterations)
+        if k in record:
+            torch.cuda.synchronize()
+            out[f"s{k}_pos"] = dev["pos"].cpu().numpy()
+            out[f"s{k}_vel"] = dev["vel"].cpu().numpy()
+    np.savez_compressed(os.path.join(out_dir, "ref_grid10_vbd.npz"), **out)
+    print("grid10 vbd done", flush=True)
+
+
 def make_bending(out_dir=HERE):
     import _chysx_ref_springs as mod
 
@@ -177,10 +215,11 @@ def main(out_dir=HERE):
     make_shear(out_dir)
     make_bending(out_dir)
     make_contact(out_dir)
+    make_vbd(out_dir)
 
 
 if __name__ == "__main__":
-    # python make_golden.py [out_dir] [shear|bending|contact]   (only that fixture)
+    # python make_golden.py [out_dir] [shear|bending|contact|vbd]   (only that fixture)
     out = sys.argv[1] if len(sys.argv) > 1 else HERE
     if len(sys.argv) > 2 and sys.argv[2] == "shear":
         make_shear(out)
@@ -188,5 +227,7 @@ if __name__ == "__main__":
         make_bending(out)
     elif len(sys.argv) > 2 and sys.argv[2] == "contact":
         make_contact(out)
+    elif len(sys.argv) > 2 and sys.argv[2] == "vbd":
+        make_vbd(out)
     else:
         main(out)
