@@ -337,8 +337,10 @@ class Cloth:
         return rows
 
     def set_preconditioner(self, kind="block_jacobi", degree=0, ratio=30.0):
-        """"block_jacobi" (reference) or "chebyshev" (CTA-local, odd degree)."""
-        k = {"block_jacobi": 0, "chebyshev": 1}[kind]
+        """"block_jacobi" (reference), "chebyshev" (CTA-local, odd degree) or
+        "chebyshev_coarse" (CTA-local plus a coarse level of one translation
+        per CTA block)."""
+        k = {"block_jacobi": 0, "chebyshev": 1, "chebyshev_coarse": 2}[kind]
         check(self._L.chysx_cloth_set_preconditioner(self.h, k, int(degree), float(ratio)))
 
     def preconditioner(self):
@@ -346,7 +348,7 @@ class Cloth:
         r = ctypes.c_float()
         check(self._L.chysx_cloth_preconditioner(self.h, ctypes.byref(k), ctypes.byref(d), ctypes.byref(r),
                                                  ctypes.byref(u)))
-        return ("block_jacobi", "chebyshev")[k.value], d.value, r.value, bool(u.value)
+        return ("block_jacobi", "chebyshev", "chebyshev_coarse")[k.value], d.value, r.value, u.value
 
     def solver_info(self):
         """(kernel, grid, block) of the last graph build; kernel is

@@ -779,13 +779,15 @@ public:
     }
     // Preconditioner (no counterpart in the reference, whose PCG is
     // block-Jacobi): 0 = block-Jacobi (default), 1 = CTA-local Chebyshev of
-    // odd degree on [lambda_max / ratio, lambda_max]; used by the
+    // odd degree on [lambda_max / ratio, lambda_max], 2 = that plus a coarse
+    // level of one rigid translation per CTA block (single-instance plans of
+    // at most kCoarseMaxBlocks CTAs; otherwise it acts as 1); used by the
     // register-resident kernel, the others stay block-Jacobi.
     void set_preconditioner(int kind, int degree, float ratio) {
-        if (kind != 0 && kind != 1) throw std::invalid_argument("set_preconditioner: kind must be 0 or 1");
-        if (kind == 1 && (degree < 1 || degree > 63 || degree % 2 == 0))
+        if (kind < 0 || kind > 2) throw std::invalid_argument("set_preconditioner: kind must be 0, 1 or 2");
+        if (kind >= 1 && (degree < 1 || degree > 63 || degree % 2 == 0))
             throw std::invalid_argument("set_preconditioner: degree must be odd, 1 to 63");
-        if (kind == 1 && !(ratio > 1.0f && ratio < 1.0e6f))
+        if (kind >= 1 && !(ratio > 1.0f && ratio < 1.0e6f))
             throw std::invalid_argument("set_preconditioner: ratio must be in (1, 1e6)");
         if (kind != pc_kind_) graph_dirty_ = true;
         pc_kind_ = kind;
@@ -796,14 +798,15 @@ public:
         if (kind) *kind = pc_kind_;
         if (degree) *degree = pc_degree_;
         if (ratio) *ratio = pc_ratio_;
-        if (in_use) *in_use = pc_active() ? 1 : 0;
+        if (in_use) *in_use = pc_active() ? (coarse_on_ ? 2 : 1) : 0;
     }
     // the CTA-local preconditioner runs in the register-resident kernel of
-    // the default synchronisation mode
-    bool pc_active() const { return pc_kind_ == 1 && resident_ && graph_path_ == kPathPersistent && sync_mode_ == 0; }
+    // the default synchronisation mode (with the coarse level where the plan
+    // is a single instance)
+    bool pc_active() const { return pc_kind_ >= 1 && resident_ && graph_path_ == kPathPersistent && sync_mode_ == 0; }
 
     // kernel actually used by the last graph build: 0 resident, 1 loop,
-    // 2 streamed, 3 resident single-reduction
+    // 2 streamed
     void solver_info(int* path, int* grid, int* block) const {
         const int used = graph_path_ == kPathLoop ? 1 : (resident_ ? 0 : 2);
         if (path) *path = used;
@@ -1147,8 +1150,8 @@ private:
         c.max_iter = max_iter_;
         c.use_tol = rel_tol_ > 0.0 ? 1 : 0;
         c.rel_tol = rel_tol_;
-        c.pc_degree = pc_kind_ == 1 ? pc_degree_ : 0;
-        c.pc_ratio = pc_kind_ == 1 ? pc_ratio_ : 0.0f;
+        c.pc_degree = pc_kind_ >= 1 ? pc_degree_ : 0;
+        c.pc_ratio = pc_kind_ >= 1 ? pc_ratio_ : 0.0f;
         return c;
     }
 
@@ -1231,7 +1234,15 @@ private:
             // rows of a triangulated grid have at most 6 off-diagonal blocks;
             // the 6-wide build fits a row in 128 registers with fewer spills
             // (ptxas: 56 B of spill stores, the 8-wide build 128 B)
-            if (pc_kind_ == 1 && SYNC == 0) {
+            if (coarse_on_ && SYNC == 0) {
+                if (topo_.max_width <= 6)
+                    return resident_warps_ == 16 ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, 6, 0, 2>)
+                                                 : reinterpret_cast<const void*>(&pcg_resident_kernel<8, 6, 0, 2>);
+                return resident_warps_ == 16
+                           ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, kResidentMaxWidth, 0, 2>)
+                           : reinterpret_cast<const void*>(&pcg_resident_kernel<8, kResidentMaxWidth, 0, 2>);
+            }
+            if (pc_kind_ >= 1 && SYNC == 0) {
                 if (topo_.max_width <= 6)
                     return resident_warps_ == 16 ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, 6, 0, 1>)
                                                  : reinterpret_cast<const void*>(&pcg_resident_kernel<8, 6, 0, 1>);
@@ -1276,6 +1287,7 @@ private:
         bp.bar = d_bar_.get();
         bp.n_slots = plan_.inst_slot.empty() ? 0 : plan_.inst_slot.back();
         bp.fslots = sync_mode_ ? d_fslots_.get() : nullptr;
+        bp.cg = coarse_args();
         return bp;
     }
 
@@ -1295,10 +1307,12 @@ private:
             resident_warps_ = W;
             const int grid = (n_slices + W - 1) / W;
             build_plan(topo_.inst_slice, grid, plan_);
+            plan_coarse();
             pers_smem_ = (size_t)W * kSlotW * sizeof(double) + (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
-            if (pers_smem_ > 48 * 1024)
-                ck(cudaFuncSetAttribute(persistent_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pers_smem_),
-                   "cudaFuncSetAttribute(resident smem)");
+            if (coarse_on_) pers_smem_ += (size_t)9 * coarse_nb_ * sizeof(float);  // 3 rows of A_c^-1
+            // static + dynamic above 48 KB needs the opt-in
+            ck(cudaFuncSetAttribute(persistent_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pers_smem_),
+               "cudaFuncSetAttribute(resident smem)");
             int per_sm = 0;
             ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_fn(), W * 32, pers_smem_),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor(resident)");
@@ -1306,6 +1320,80 @@ private:
         }
         resident_ = false;
         return false;
+    }
+
+    // Coarse level of the two-level preconditioner (kind 2): one block per
+    // CTA of a single-instance resident plan.  Host side: the CTA of every
+    // slice, every block's sorted list of the blocks its rows touch, and the
+    // list position of every ELL entry's column block.
+    void plan_coarse() {
+        coarse_on_ = false;
+        if (pc_kind_ != 2 || !resident_ || sync_mode_ != 0 || plan_.n_inst != 1 || plan_.grid > kCoarseMaxBlocks)
+            return;
+        const int nb = plan_.grid, ns = topo_.n_slices;
+        std::vector<int> slice_cta(std::max(1, ns), 0);
+        for (int c = 0; c < nb; ++c)
+            for (int sl = plan_.cta_slice[c]; sl < plan_.cta_slice[c + 1]; ++sl) slice_cta[sl] = c;
+        std::vector<std::vector<int>> lists(nb);
+        for (int c = 0; c < nb; ++c) {
+            std::vector<int>& l = lists[c];
+            l.push_back(c);
+            for (int sl = plan_.cta_slice[c]; sl < plan_.cta_slice[c + 1]; ++sl)
+                for (int e = topo_.slice_off[sl]; e < topo_.slice_off[sl + 1]; ++e) l.push_back(slice_cta[topo_.col[e] >> 5]);
+            std::sort(l.begin(), l.end());
+            l.erase(std::unique(l.begin(), l.end()), l.end());
+            if ((int)l.size() > kCoarseMaxNbr) return;  // too many touching blocks: local level only
+        }
+        int mn = 1;
+        for (const auto& l : lists) mn = std::max(mn, (int)l.size());
+        std::vector<int> nbr((size_t)nb * mn, -1), cnt(nb), self(nb);
+        for (int c = 0; c < nb; ++c) {
+            cnt[c] = (int)lists[c].size();
+            for (int k = 0; k < cnt[c]; ++k) {
+                nbr[(size_t)c * mn + k] = lists[c][k];
+                if (lists[c][k] == c) self[c] = k;
+            }
+        }
+        std::vector<unsigned char> ell(std::max<size_t>(1, topo_.col.size()), 0);
+        for (int c = 0; c < nb; ++c)
+            for (int sl = plan_.cta_slice[c]; sl < plan_.cta_slice[c + 1]; ++sl)
+                for (int e = topo_.slice_off[sl]; e < topo_.slice_off[sl + 1]; ++e) {
+                    const int cb = slice_cta[topo_.col[e] >> 5];
+                    ell[e] = (unsigned char)(std::lower_bound(lists[c].begin(), lists[c].end(), cb) - lists[c].begin());
+                }
+        d_slice_cta_.upload(slice_cta);
+        d_cnbr_.upload(nbr);
+        d_ccnt_.upload(cnt);
+        d_cself_.upload(self);
+        d_ell_nbr_.upload(ell);
+        d_cac_.resize((size_t)nb * mn * 9);
+        d_cac_.zero();
+        d_cainv_.resize((size_t)9 * nb * nb);
+        d_cainv_.zero();
+        coarse_nb_ = nb;
+        coarse_mn_ = mn;
+        coarse_on_ = true;
+        // static + dynamic above 48 KB needs the opt-in
+        ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_inverse_kernel),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_inverse_smem()),
+           "cudaFuncSetAttribute(coarse inverse smem)");
+    }
+    size_t coarse_inverse_smem() const {
+        return ((size_t)coarse_nb_ * coarse_mn_ * 9 + 6 * 3 * (size_t)coarse_nb_) * sizeof(float);
+    }
+    CoarseArgs coarse_args() const {
+        CoarseArgs c{};
+        c.on = coarse_on_ ? 1 : 0;
+        c.nb = coarse_nb_;
+        c.max_nbr = coarse_mn_;
+        c.slice_cta = d_slice_cta_.get();
+        c.nbr = d_cnbr_.get();
+        c.nbr_cnt = d_ccnt_.get();
+        c.self_idx = d_cself_.get();
+        c.ell_nbr = d_ell_nbr_.get();
+        c.ac = d_cac_.get();
+        c.ainv = d_cainv_.get();
+        return c;
     }
 
     void plan_persistent() {
@@ -1326,9 +1414,9 @@ private:
             build_plan(topo_.inst_slice, grid, plan_);
             pers_smem_ = (size_t)plan_.max_slices_per_cta * kSlotW * sizeof(double) +
                          (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
-            if (pers_smem_ > 48 * 1024)
-                ck(cudaFuncSetAttribute(persistent_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pers_smem_),
-                   "cudaFuncSetAttribute(persistent smem)");
+            // static + dynamic above 48 KB needs the opt-in
+            ck(cudaFuncSetAttribute(persistent_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pers_smem_),
+               "cudaFuncSetAttribute(persistent smem)");
             int per_sm = 0;
             ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_fn(), pcg_block_, pers_smem_),
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
@@ -1360,7 +1448,7 @@ private:
         d_cta_inst_hi_.upload(plan_.cta_inst_hi);
         d_inst_cta_lo_.upload(plan_.inst_cta_lo);
         d_inst_slot_.upload(plan_.inst_slot);
-        d_slots_.resize((size_t)std::max(1, plan_.inst_slot.back()) * kSlotW);
+        d_slots_.resize((size_t)2 * std::max(1, plan_.inst_slot.back()) * kSlotW);  // two sets by phase parity
         d_fslots_.resize((size_t)3 * std::max(1, plan_.inst_slot.back()) * kSlotW);
         d_inst_.resize(plan_.n_inst);
         d_inst_.zero();
@@ -1462,9 +1550,8 @@ private:
 
     void build_graph_persistent() {
         destroy_graph();
-        if (asm_smem_ > 48 * 1024)
-            ck(cudaFuncSetAttribute(assemble_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asm_smem_),
-               "cudaFuncSetAttribute(assemble smem)");
+        ck(cudaFuncSetAttribute(assemble_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asm_smem_),
+           "cudaFuncSetAttribute(assemble smem)");
         plan_persistent();
         check_plan();
         prepare_contact_buffers();
@@ -1487,6 +1574,28 @@ private:
         cudaGraphNode_t t0 = add_contact_nodes(timing_node(0, nullptr));
         ck(cudaGraphAddKernelNode(&asm_node_, graph_, t0 ? &t0 : nullptr, t0 ? 1 : 0, &ap), "add assemble node");
         cudaGraphNode_t t1 = add_guess_node(asm_node_, cur_args_, t, v);
+        if (coarse_on_) {
+            // the coarse system of this step's matrix, before the solve
+            CoarseArgs cg = coarse_args();
+            const int* cslice = d_cta_slice_.get();
+            void* a1[] = {&t, &cslice, &cg};
+            cudaKernelNodeParams p{};
+            p.func = reinterpret_cast<void*>(&coarse_assemble_kernel);
+            p.gridDim = dim3(coarse_nb_);
+            p.blockDim = dim3(288);
+            p.kernelParams = a1;
+            cudaGraphNode_t n1, n2;
+            ck(cudaGraphAddKernelNode(&n1, graph_, &t1, 1, &p), "add coarse assemble node");
+            void* a2[] = {&cg};
+            cudaKernelNodeParams p2{};
+            p2.func = reinterpret_cast<void*>(&coarse_inverse_kernel);
+            p2.gridDim = dim3(coarse_nb_);
+            p2.blockDim = dim3(kCoarseThreads);
+            p2.sharedMemBytes = (unsigned)coarse_inverse_smem();
+            p2.kernelParams = a2;
+            ck(cudaGraphAddKernelNode(&n2, graph_, &n1, 1, &p2), "add coarse inverse node");
+            t1 = n2;
+        }
         t1 = timing_node(1, t1);
         cudaGraphNode_t reset;
         {
@@ -1536,9 +1645,8 @@ private:
 
     void build_graph_loop() {
         destroy_graph();
-        if (asm_smem_ > 48 * 1024)
-            ck(cudaFuncSetAttribute(assemble_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asm_smem_),
-               "cudaFuncSetAttribute(assemble smem)");
+        ck(cudaFuncSetAttribute(assemble_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asm_smem_),
+           "cudaFuncSetAttribute(assemble smem)");
         prepare_contact_buffers();
         ck(cudaGraphCreate(&graph_, 0), "cudaGraphCreate");
         ck(cudaGraphConditionalHandleCreate(&cond_, graph_, 1, cudaGraphCondAssignDefault),
@@ -1752,7 +1860,12 @@ private:
     int resident_warps_ = 16;
     std::vector<TuneResult> tune_;
     int sync_mode_ = 0;    // 0 grid counter barrier, 1 polled per-instance slots
-    int pc_kind_ = 0, pc_degree_ = 0;  // preconditioner: 0 block-Jacobi, 1 CTA-local Chebyshev
+    int pc_kind_ = 0, pc_degree_ = 0;  // preconditioner: 0 block-Jacobi, 1 CTA-local Chebyshev, 2 + coarse level
+    bool coarse_on_ = false;
+    int coarse_nb_ = 0, coarse_mn_ = 0;
+    DevBuf<int> d_slice_cta_, d_cnbr_, d_ccnt_, d_cself_;
+    DevBuf<unsigned char> d_ell_nbr_;
+    DevBuf<float> d_cac_, d_cainv_;
     float pc_ratio_ = 0.0f;
     DevBuf<ZP> d_zp_;
     bool timing_ = false;

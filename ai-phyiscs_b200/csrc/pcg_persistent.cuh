@@ -20,6 +20,7 @@
 #pragma once
 
 #include "cloth_kernels.cuh"
+#include "coarse_types.h"
 
 namespace chysx_b200 {
 
@@ -58,6 +59,7 @@ struct BatchPlan {
     GridBarrier* bar;
     int n_slots = 0;                      // inst_slot[n_inst]
     unsigned long long* fslots = nullptr; // [3][n_slots][kSlotW] rotating polled slots (SYNC = 1)
+    CoarseArgs cg{};                      // coarse level of the two-level preconditioner (cg.on = 0: none)
 };
 
 // (z, p) of one row for the register-resident kernel's neighbour exchange
@@ -103,6 +105,24 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
 __device__ __forceinline__ bool barrier_arrive_wait(GridBarrier* gb, unsigned& target) {
     target += gridDim.x;
     red_release_add(&gb->count, 1u);
+    const unsigned long long t0 = global_ns();
+    unsigned spins = 0;
+    while ((int)(ld_acquire_gpu(&gb->count) - target) < 0) {
+        if ((++spins & 255u) == 0) {
+            if (*(volatile int*)&gb->error) return false;
+            if (global_ns() - t0 > kBarrierTimeoutNs) {
+                atomicExch(&gb->error, 1);
+                return false;
+            }
+        }
+    }
+    return *(volatile int*)&gb->error == 0;
+}
+
+// The wait of barrier_arrive_wait without the arrival, for a second warp of
+// a CTA whose first warp arrives: returns once the counter reaches `target`
+// (bounded in time like the barrier; false on an error).
+__device__ __forceinline__ bool barrier_wait_only(GridBarrier* gb, unsigned target) {
     const unsigned long long t0 = global_ns();
     unsigned spins = 0;
     while ((int)(ld_acquire_gpu(&gb->count) - target) < 0) {
@@ -289,7 +309,7 @@ __device__ __forceinline__ void warp0_publish(const BatchPlan& bp, const double*
                 for (int q = 0; q < NV; ++q) st_relaxed_u64(d + q, slot_bits(acc[q]));
             } else {
 #pragma unroll
-                for (int q = 0; q < NV; ++q) bp.slots[(size_t)L.own_slot * kSlotW + q] = acc[q];
+                for (int q = 0; q < NV; ++q) bp.slots[((size_t)set * bp.n_slots + L.own_slot) * kSlotW + q] = acc[q];
             }
         }
     }
@@ -299,8 +319,10 @@ __device__ __forceinline__ void warp0_publish(const BatchPlan& bp, const double*
 // the CTA's segments, waits for the other CTAs (counter barrier or polled
 // slots), reads each instance's total in a fixed order and lets lane 0
 // apply `step(L, total)`.  For instances spanning at most 32 * KP CTAs (one
-// pass of loads).  Returns false (on all lanes) after a failed wait.
-template <int NV, int SYNC, int KP, class Step>
+// pass of loads).  Publishes NV values per segment and (counter mode) reads
+// back the totals of the first NR.  Returns false (on all lanes) after a
+// failed wait.
+template <int NV, int SYNC, int KP, int NR = NV, class Step>
 __device__ __forceinline__ bool warp0_phase(const BatchPlan& bp, const double* spart, LocalInst* li, int nloc,
                                             int set, unsigned& target, Step&& step) {
     const int lane = threadIdx.x & 31;
@@ -322,29 +344,63 @@ __device__ __forceinline__ bool warp0_phase(const BatchPlan& bp, const double* s
 #pragma unroll
             for (int q = 0; q < NV; ++q) tot[q] = 0.0;
             for (int c0 = L.slot_lo; c0 < L.slot_hi; c0 += 32 * KP) {
-                double val[KP][NV];
+                double val[KP][NR];
 #pragma unroll
                 for (int j = 0; j < KP; ++j) {
                     const int k = c0 + j * 32 + lane;
 #pragma unroll
-                    for (int q = 0; q < NV; ++q)
-                        val[j][q] = k < L.slot_hi ? __ldcg(bp.slots + (size_t)k * kSlotW + q) : 0.0;
+                    for (int q = 0; q < NR; ++q)
+                        val[j][q] = k < L.slot_hi ? __ldcg(bp.slots + ((size_t)set * bp.n_slots + k) * kSlotW + q) : 0.0;
                 }
 #pragma unroll
                 for (int j = 0; j < KP; ++j) {
                     if (c0 + j * 32 + lane < L.slot_hi) {
 #pragma unroll
-                        for (int q = 0; q < NV; ++q) tot[q] += val[j][q];
+                        for (int q = 0; q < NR; ++q) tot[q] += val[j][q];
                     }
                 }
             }
 #pragma unroll
-            for (int q = 0; q < NV; ++q) tot[q] = warp_sum(tot[q]);
+            for (int q = 0; q < NR; ++q) tot[q] = warp_sum(tot[q]);
         }
         if (lane == 0) step(L, tot);
         __syncwarp();
     }
     return true;
+}
+
+// Coarse level of a single-instance two-level plan (counter barrier): this
+// CTA's block of A_c^-1 v, v_k = the values Q0..Q0+2 of slot k (block k) of
+// `set`, A_c^-1's rows 3B..3B+2 in `ainv` ([3][m3]), formed by one warp (warp
+// 1 during a phase, while warp 0 reads the scalar totals).  Lane l takes
+// slots l, l + 32, ...; every lane returns the sums (warp-summed, fixed
+// order).
+__device__ __forceinline__ float3 coarse_slot_dot(float v0, float v1, float v2, int m3, const float* ainv, int k,
+                                                  float3 acc) {
+    const float* a = ainv + 3 * k;
+    acc.x = fmaf(a[0], v0, fmaf(a[1], v1, fmaf(a[2], v2, acc.x)));
+    acc.y = fmaf(a[m3], v0, fmaf(a[m3 + 1], v1, fmaf(a[m3 + 2], v2, acc.y)));
+    acc.z = fmaf(a[2 * m3], v0, fmaf(a[2 * m3 + 1], v1, fmaf(a[2 * m3 + 2], v2, acc.z)));
+    return acc;
+}
+__device__ __forceinline__ float3 warp_sum3(float3 v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+        v.z += __shfl_xor_sync(0xffffffffu, v.z, o);
+    }
+    return v;
+}
+template <int Q0>
+__device__ __forceinline__ float3 warp_coarse_dot(const BatchPlan& bp, int set, const float* ainv) {
+    const int lane = threadIdx.x & 31, m3 = 3 * bp.cg.nb;
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    for (int k = lane; k < bp.n_slots; k += 32) {
+        const double* v = bp.slots + ((size_t)set * bp.n_slots + k) * kSlotW + Q0;
+        acc = coarse_slot_dot((float)__ldcg(v), (float)__ldcg(v + 1), (float)__ldcg(v + 2), m3, ainv, k, acc);
+    }
+    return warp_sum3(acc);
 }
 
 // The same phase with the whole CTA reading the slots, for instances that
@@ -381,7 +437,9 @@ __device__ __forceinline__ void block_phase(const BatchPlan& bp, const double* s
                 for (int q = 0; q < NV; ++q) {
                     if (k >= L.slot_hi) val[j][q] = 0ull;
                     else if (SYNC) val[j][q] = ld_relaxed_u64(fbase + (size_t)k * kSlotW + q);
-                    else val[j][q] = (unsigned long long)__double_as_longlong(__ldcg(bp.slots + (size_t)k * kSlotW + q));
+                    else
+                        val[j][q] = (unsigned long long)__double_as_longlong(
+                            __ldcg(bp.slots + ((size_t)set * bp.n_slots + k) * kSlotW + q));
                 }
             }
             if (SYNC) {
@@ -596,6 +654,14 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
     }
 }
 
+// Slot set of reduction phase ph: the polled mode rotates three sets; the
+// counter mode alternates two by parity, so a CTA that has passed a barrier
+// and publishes the next phase never overwrites values another CTA may
+// still be reading from the phase before (it can only publish phase ph + 2
+// into that set after the barrier of phase ph + 1, which every reader of
+// phase ph must have reached).
+#define slot_set(ph) (SYNC ? (ph) % 3 : (ph) & 1)
+
 // The phase protocol shared by both kernels.  After the CTA's slice
 // partials are in spart and a __syncthreads, this runs the warp-0 phase and
 // leaves, after a closing __syncthreads, s_flag = 1 on a failed wait and
@@ -604,7 +670,7 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
 #define CHYSX_REDUCE_PHASE(NV, KP, exit_test, STEP)                                                  \
     do {                                                                                             \
         if (warp == 0) {                                                                             \
-            const bool w0ok = warp0_phase<NV, SYNC, KP>(bp, spart, li, nloc, ph % 3, target, STEP);  \
+            const bool w0ok = warp0_phase<NV, SYNC, KP>(bp, spart, li, nloc, slot_set(ph), target, STEP); \
             if (lane == 0) {                                                                         \
                 if (!w0ok) s_flag = 1;                                                               \
                 if (!SYNC && (exit_test) && w0ok)                                                    \
@@ -615,10 +681,41 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
         __syncthreads();                                                                             \
     } while (0)
 
+// The same protocol for single-instance two-level plans: warp 0 publishes NV
+// values and reads the totals of the first NR; warp 1 waits on the same
+// counter (the phase's target: every phase so far was one barrier) and
+// writes this CTA's block of A_c^-1 v, v the values Q0..Q0+2, to OUT[0..2].
+#define CHYSX_COARSE_PHASE(NV, NR, Q0, OUT, exit_test, STEP)                                         \
+    do {                                                                                             \
+        if (warp == 0) {                                                                             \
+            const bool w0ok = warp0_phase<NV, 0, kPollMax, NR>(bp, spart, li, nloc, slot_set(ph), target, STEP); \
+            if (lane == 0) {                                                                         \
+                if (!w0ok) s_flag = 1;                                                               \
+                if ((exit_test) && w0ok) s_exit = *(volatile unsigned*)&bp.bar->ndone >= (unsigned)bp.n_inst; \
+            }                                                                                        \
+        } else if (warp == 1) {                                                                      \
+            bool w1ok = true;                                                                        \
+            if (lane == 0) w1ok = barrier_wait_only(bp.bar, (unsigned)(ph + 1) * gridDim.x);         \
+            w1ok = __shfl_sync(0xffffffffu, w1ok, 0);                                                \
+            if (w1ok) {                                                                              \
+                const float3 cw = warp_coarse_dot<Q0>(bp, slot_set(ph), c_ainv);                     \
+                if (lane == 0) {                                                                     \
+                    (OUT)[0] = cw.x;                                                                 \
+                    (OUT)[1] = cw.y;                                                                 \
+                    (OUT)[2] = cw.z;                                                                 \
+                }                                                                                    \
+            } else if (lane == 0) {                                                                  \
+                s_flag = 1;                                                                          \
+            }                                                                                        \
+        }                                                                                            \
+        ++ph;                                                                                        \
+        __syncthreads();                                                                             \
+    } while (0)
+
 // The same protocol with block_phase (the whole CTA reads the totals).
 #define CHYSX_BLOCK_PHASE(NV, KB, exit_test, STEP)                                                   \
     do {                                                                                             \
-        block_phase<NV, SYNC, BLOCK, KB>(bp, spart, li, nloc, ph % 3, target, s_red, &s_flag, STEP);  \
+        block_phase<NV, SYNC, BLOCK, KB>(bp, spart, li, nloc, slot_set(ph), target, s_red, &s_flag, STEP); \
         if (!SYNC && (exit_test) && threadIdx.x == 0 && !s_flag)                                     \
             s_exit = *(volatile unsigned*)&bp.bar->ndone >= (unsigned)bp.n_inst;                    \
         ++ph;                                                                                        \
@@ -817,6 +914,12 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
 }
 
 
+}  // namespace chysx_b200
+
+#include "coarse.cuh"
+
+namespace chysx_b200 {
+
 // ---------------------------------------------------------------------------
 // Register-resident variant for systems with at most one 32-row slice per
 // warp: every thread owns one row for the whole solve and keeps its diagonal
@@ -841,6 +944,8 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     __shared__ float4 s_d[PC ? 2 : 1][PC ? W * 32 : 1];
     __shared__ double s_bsum[PC ? W : 1];
     __shared__ float s_cheb[4];
+    // coarse level: this block of A_c^-1 R^T (A p) and of A_c^-1 R^T r
+    __shared__ float s_cw[4], s_cu[4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
     const int il0 = bp.cta_inst_lo[blockIdx.x], il1 = bp.cta_inst_hi[blockIdx.x];
@@ -974,6 +1079,19 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         __syncthreads();
     }
 
+    // ---- coarse level (PC = 2 with bp.cg.on): rows 3B..3B+2 of A_c^-1 (B
+    // this CTA) in dynamic shared memory behind the LocalInst records; warp 0
+    // forms this block of A_c^-1 R^T v while it reads the blocks' slot sums
+    constexpr bool kCoarse = PC == 2;
+    const bool coarse = kCoarse && bp.cg.on;
+    float* c_ainv = reinterpret_cast<float*>(li + bp.max_inst_per_cta);
+    if (coarse) {
+        const int m3 = 3 * bp.cg.nb;
+        const float* src = bp.cg.ainv + (size_t)3 * blockIdx.x * m3;
+        for (int q = threadIdx.x; q < 3 * m3; q += blockDim.x) c_ainv[q] = src[q];
+        __syncthreads();
+    }
+
     // ---- phase 0 -------------------------------------------------------
     float3 pc_zb = f3(0.f, 0.f, 0.f);  // P(b), for the start of a scaled guess
     if (PC) {
@@ -989,8 +1107,36 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
                 r = b - ax;
             }
         }
-        zb = precond(b);
-        z = warm ? precond(r) : zb;
+        float3 cb = f3(0.f, 0.f, 0.f), cr = cb;
+        if (coarse) {
+            // R^T b and R^T r0 of every block through one exchange phase
+            const float3 sb = row ? b : f3(0.f, 0.f, 0.f), sr = row ? r : f3(0.f, 0.f, 0.f);
+            const double q6[6] = {warp_sum((double)sb.x), warp_sum((double)sb.y), warp_sum((double)sb.z),
+                                  warp_sum((double)sr.x), warp_sum((double)sr.y), warp_sum((double)sr.z)};
+            if (lane == 0 && has)
+                for (int q = 0; q < 6; ++q) spart[warp * kSlotW + q] = q6[q];
+            else if (lane == 0)
+                for (int q = 0; q < 6; ++q) spart[warp * kSlotW + q] = 0.0;
+            __syncthreads();
+            CHYSX_REDUCE_PHASE(6, 1, false, no_step);
+            ok = s_flag == 0;
+            if (ok) {
+                // this block of A_c^-1 R^T b (s_cw) and A_c^-1 R^T r0 (s_cu)
+                if (warp == 0) {
+                    const float3 ub = warp_coarse_dot<0>(bp, slot_set(ph - 1), c_ainv);
+                    const float3 u0 = warp_coarse_dot<3>(bp, slot_set(ph - 1), c_ainv);
+                    if (lane == 0) {
+                        s_cw[0] = ub.x; s_cw[1] = ub.y; s_cw[2] = ub.z;
+                        s_cu[0] = u0.x; s_cu[1] = u0.y; s_cu[2] = u0.z;
+                    }
+                }
+                __syncthreads();
+                cb = f3(s_cw[0], s_cw[1], s_cw[2]);
+                if (warm) cr = f3(s_cu[0], s_cu[1], s_cu[2]);
+            }
+        }
+        zb = precond(b) + cb;
+        z = warm ? precond(r) + cr : zb;
         pc_zb = zb;
         if (row) {
             zp0[i].z = f4(z);
@@ -1035,6 +1181,19 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         CHYSX_REDUCE_PHASE(1, kPollMax, false, no_step);
         ok = s_flag == 0;
     }
+    if (coarse && ok) {
+        // A_c^-1 R^T r of the start: of r0, of the scaled mix of r0 and b,
+        // or of b
+        const LocalInst& L0 = li[0];
+        const bool from_r0 = warm && !L0.fallback;
+        __syncthreads();  // every thread has read s_cw, s_cu
+        if (threadIdx.x < 3) {
+            const float ub = s_cw[threadIdx.x], u0 = s_cu[threadIdx.x];
+            s_cu[threadIdx.x] = from_r0 ? fmaf(L0.scale, u0, L0.scale_b * ub) : ub;
+        }
+        __syncthreads();
+    }
+    float3 c_blk = f3(0.f, 0.f, 0.f);  // this block's coarse correction of the iteration
 
     // ---- iterations ----------------------------------------------------
     const int iter_cap = cfg.max_iter + 2;
@@ -1095,14 +1254,33 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
             sig = (double)p.x * acc.x + (double)p.y * acc.y + (double)p.z * acc.z;
         }
         sig = warp_sum(sig);
+        if (kCoarse) {
+            // the CTA's sum of Ap, for the coarse correction's update (it
+            // only feeds the preconditioner: float warp sums)
+            const bool act = row && !li[li_idx].done;
+            const float3 sa = warp_sum3(act ? ap : f3(0.f, 0.f, 0.f));
+            if (lane == 0 && has) {
+                spart[warp * kSlotW + 1] = sa.x;
+                spart[warp * kSlotW + 2] = sa.y;
+                spart[warp * kSlotW + 3] = sa.z;
+            }
+        }
         if (lane == 0 && has) spart[warp * kSlotW] = sig;
         __syncthreads();
-        CHYSX_REDUCE_PHASE(1, kPollMax, true, ([&](LocalInst& L, const double* tot) { step_alpha(L, tot); }));
+        if (coarse)
+            CHYSX_COARSE_PHASE(4, 1, 1, s_cw, true, ([&](LocalInst& L, const double* tot) { step_alpha(L, tot); }));
+        else
+            CHYSX_REDUCE_PHASE(1, kPollMax, true, ([&](LocalInst& L, const double* tot) { step_alpha(L, tot); }));
         if (s_flag) {
             ok = false;
             break;
         }
         if (!SYNC && s_exit) break;
+        if (coarse) {
+            // A_c^-1 R^T r_new = A_c^-1 R^T r - alpha A_c^-1 R^T A p
+            const float al = li[0].alpha;
+            c_blk = f3(fmaf(-al, s_cw[0], s_cu[0]), fmaf(-al, s_cw[1], s_cu[1]), fmaf(-al, s_cw[2], s_cu[2]));
+        }
 
         double rz = 0.0, rr = 0.0;
         const bool act = row && !li[li_idx].done;
@@ -1113,7 +1291,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         }
         if (PC) {
             const float3 zn = precond(act ? r : f3(0.f, 0.f, 0.f));
-            if (act) z = zn;
+            if (act) z = zn + c_blk;
         }
         if (act) {
             const LocalInst& L = li[li_idx];
@@ -1130,9 +1308,21 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
             spart[warp * kSlotW] = rz;
             spart[warp * kSlotW + 1] = rr;
         }
+        if (kCoarse) {
+            // the CTA's sum of the new r: the coarse correction restarts
+            // from R^T r every iteration (no drift)
+            const float3 sr = warp_sum3(act ? r : f3(0.f, 0.f, 0.f));
+            if (lane == 0 && has) {
+                spart[warp * kSlotW + 2] = sr.x;
+                spart[warp * kSlotW + 3] = sr.y;
+                spart[warp * kSlotW + 4] = sr.z;
+            }
+        }
         __syncthreads();
-        CHYSX_REDUCE_PHASE(2, kPollMax, false,
-                           ([&](LocalInst& L, const double* tot) { step_beta(bp, L, tot, cfg); }));
+        if (coarse)
+            CHYSX_COARSE_PHASE(5, 2, 2, s_cu, false, ([&](LocalInst& L, const double* tot) { step_beta(bp, L, tot, cfg); }));
+        else
+            CHYSX_REDUCE_PHASE(2, kPollMax, false, ([&](LocalInst& L, const double* tot) { step_beta(bp, L, tot, cfg); }));
         if (s_flag) {
             ok = false;
             break;

@@ -303,7 +303,10 @@ PYBIND11_MODULE(_chysx_native, m) {
                  int k = -1;
                  if (kind == "block_jacobi") k = 0;
                  if (kind == "chebyshev") k = 1;
-                 if (k < 0) throw py::value_error("preconditioner kind must be 'block_jacobi' or 'chebyshev'");
+                 if (kind == "chebyshev_coarse") k = 2;
+                 if (k < 0)
+                     throw py::value_error(
+                         "preconditioner kind must be 'block_jacobi', 'chebyshev' or 'chebyshev_coarse'");
                  check(chysx_cloth_set_preconditioner(s.h(), k, degree, ratio));
              },
              py::arg("kind"), py::arg("degree") = 7, py::arg("ratio") = 30.0f)

@@ -334,8 +334,8 @@ def run_ours(args, rank, world, local_rank):
             params, _ = learned.load(args.net)
             sim.sim.set_network(params)
         sim.sim.set_solver(sc["max_iter"], rel_tol, args.warm)
-        if args.pc == "chebyshev":
-            sim.sim.set_preconditioner("chebyshev", args.pc_degree, args.pc_ratio)
+        if args.pc != "block_jacobi":
+            sim.sim.set_preconditioner(args.pc, args.pc_degree, args.pc_ratio)
         if args.row_order == "spatial":
             sim.sim.set_row_order(1)
         return sim
@@ -438,7 +438,12 @@ def run_ours(args, rank, world, local_rank):
     achieved = float(np.sum(moved) / (np.sum(solve_ms) * 1e-3) / 1e9)
     achieved_ref = float(np.sum(moved_ref) / (np.sum(solve_ms) * 1e-3) / 1e9)
     peak, peak_kind = read_peaks()
-    traffic_it = read_traffic(g.sim.solver_info()[0], args.workload)
+    # the ncu summary of the kernel variant that ran (resident kernels: by
+    # preconditioner in use)
+    kern = g.sim.solver_info()[0]
+    if kern == "resident":
+        kern += {0: "", 1: "_chebyshev", 2: "_twolevel"}[int(g.sim.preconditioner()[3])]
+    traffic_it = read_traffic(kern, args.workload)
     steps_total = args.steps * world
     value = steps_total / (total_ms_max * 1e-3)
     mean_iters = float(iters.mean())
@@ -515,7 +520,9 @@ def run_ours(args, rank, world, local_rank):
             "pcg_iterations_fixed": int(round(bj_iters if bj_iters else mean_iters)),
             "note": "compiled reference ClothSimulator (springs enabled), same scene with geometric-mean "
                     "stiffness, PCG fixed at the block-Jacobi iterations/step the same steps take, stream 0"},
-        "gpu_launches": 4 * args.steps,
+        # assemble, reset, persistent PCG, finalize; the two-level
+        # preconditioner adds the coarse assembly and the coarse inverse
+        "gpu_launches": (6 if g.sim.preconditioner()[3] == 2 else 4) * args.steps,
         "clocks": clk,
         "wall_s": wall,
     }
@@ -619,9 +626,10 @@ def main():
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--grid", type=int, default=0)
     ap.add_argument("--sync", type=int, default=0, help="persistent kernels: 0 grid counter barrier, 1 polled slots")
-    ap.add_argument("--pc", default="chebyshev", choices=["block_jacobi", "chebyshev"],
-                    help="preconditioner: the reference's block-Jacobi, or the CTA-local Chebyshev (used where "
-                         "the register-resident kernel runs; elsewhere block-Jacobi)")
+    ap.add_argument("--pc", default="chebyshev_coarse", choices=["block_jacobi", "chebyshev", "chebyshev_coarse"],
+                    help="preconditioner: the reference's block-Jacobi, the CTA-local Chebyshev, or that plus a "
+                         "coarse level of one translation per CTA block (used where the register-resident kernel "
+                         "runs; elsewhere block-Jacobi)")
     ap.add_argument("--pc-degree", type=int, default=7)
     ap.add_argument("--row-order", default="spatial", choices=["caller", "spatial"],
                     help="rows in the caller's particle order, or in spatially compact blocks")

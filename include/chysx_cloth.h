@@ -388,9 +388,14 @@ int chysx_cloth_row_of_particles(const chysx_cloth* h, int n, int32_t* rows);
  * [lambda_max / ratio, lambda_max], lambda_max estimated per CTA and solve by
  * power iteration with a 10% margin.  A fixed polynomial, so the outer
  * iteration stays plain PCG with the same stopping test (||r|| / ||b||);
- * odd degrees keep p positive on the whole spectrum.  Kind 1 applies where
- * the register-resident kernel runs with synchronisation mode 0; in_use
- * reports whether the last graph build uses it. */
+ * odd degrees keep p positive on the whole spectrum.  Kind 2 = kind 1 plus
+ * a coarse level: z += R q(D_c^-1 A_c) D_c^-1 R^T r, R the rigid translation
+ * of every CTA's block of rows, A_c = R^T A R (3 unknowns per CTA, assembled
+ * on the device each step), q a Chebyshev polynomial of degree 7 on
+ * [lambda_c / 100, lambda_c]; it applies to single-instance systems of at
+ * most 160 CTAs and acts as kind 1 elsewhere.  Kinds 1 and 2 apply where the
+ * register-resident kernel runs with synchronisation mode 0; in_use reports
+ * what the last graph build uses (0 block-Jacobi, 1 local, 2 two-level). */
 int chysx_cloth_set_preconditioner(chysx_cloth* h, int kind, int degree, float ratio);
 int chysx_cloth_preconditioner(const chysx_cloth* h, int* kind, int* degree, float* ratio, int* in_use);
 /* Kernel used at the last graph build: path 0 register-resident persistent,

@@ -77,7 +77,7 @@ def lib():
         L.orc_vbd_bending.argtypes = [ctypes.c_int, _f64p, _f64p] + [ctypes.c_double] * 5 + [_f64p, _f64p]
         L.orc_vbd_hinge_angle.argtypes = [_f64p]
         L.orc_vbd_hinge_angle.restype = ctypes.c_double
-        L.orc_set_preconditioner.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
+        L.orc_set_preconditioner.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int]
         L.orc_add_static_plane.argtypes = [vp, _f32p, ctypes.c_float]
         L.orc_add_static_box.argtypes = [vp, _f32p, _f32p, _f32p, _f32p, _f32p]
         L.orc_clear_static_shapes.argtypes = [vp]
@@ -238,10 +238,11 @@ class OracleCloth:
         _check(self._L.orc_contact_spmv(self._h, _p(x, _f64p), _p(y, _f64p)))
         return y
 
-    def set_preconditioner(self, degree=0, ratio=30.0, block_rows=512):
+    def set_preconditioner(self, degree=0, ratio=30.0, block_rows=512, coarse=False):
         """0: block-Jacobi (the reference's); odd degree: the product's
-        block-local Chebyshev preconditioner on blocks of block_rows rows."""
-        _check(self._L.orc_set_preconditioner(self._h, int(degree), float(ratio), int(block_rows)))
+        block-local Chebyshev preconditioner on blocks of block_rows rows;
+        coarse: plus the coarse level of one translation per block."""
+        _check(self._L.orc_set_preconditioner(self._h, int(degree), float(ratio), int(block_rows), int(bool(coarse))))
 
     def add_static_plane(self, n, d):
         n = np.ascontiguousarray(n, np.float32).reshape(3)

@@ -1,0 +1,95 @@
+"""The two-level preconditioner (CTA-local Chebyshev plus a coarse level of
+one rigid translation per CTA block): converged solutions as the FP64
+oracle's block-Jacobi PCG, iteration counts as the oracle's restatement of
+the same two-level operator, the warm starts, its fallback to the local
+level where the coarse level does not apply, and bitwise repeatability."""
+import numpy as np
+import pytest
+
+from chysx import capi, scenes
+from chysx.runner import GpuCloth
+from test_gpu_precond import oracle_sim
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu(sc, kind, degree=7, order=0, **kw):
+    g = GpuCloth(sc, **kw)
+    if order:
+        g.sim.set_row_order(order)
+    if kind != "block_jacobi":
+        g.sim.set_preconditioner(kind, degree, 30.0)
+    return g
+
+
+@pytest.mark.parametrize("side", [64, 128])
+def test_coarse_solution_and_iterations(side):
+    sc = scenes.config_small(side=side, steps=4)
+    g = gpu(sc, "chebyshev_coarse", max_iter=20000, rel_tol=1e-7)
+    g.step()
+    kind, deg, _, used = g.sim.preconditioner()
+    assert (kind, deg, used) == ("chebyshev_coarse", 7, 2)
+    block_rows = g.sim.solver_info()[2]
+    o = oracle_sim(sc, 1e-11)
+    o.step(sc["dt"])
+    assert np.abs(g.dump()[5] - o.dump_system()[5]).max() < 2e-6
+    # the same two-level operator on the CPU (FP32 port, same blocks, same
+    # state): counts within 15% (summation orders differ)
+    c = oracle_sim(sc, 1e-7, fp64=False, degree=7, block_rows=block_rows)
+    c.set_preconditioner(7, 30.0, block_rows, coarse=True)
+    c.set_state(*[a.astype(np.float32) for a in (g.positions(), g.velocities())], g.inv_mass.cpu().numpy())
+    g.step()
+    c.step(sc["dt"])
+    assert g.stats()[2] == capi.SOLVE_CONVERGED
+    gi, ci = g.stats()[0], c.stats()[0]
+    assert abs(gi - ci) <= 0.15 * ci + 2
+
+
+def test_coarse_level_cuts_iterations_on_compact_blocks():
+    """With spatially compact row blocks the coarse level removes most of the
+    iterations the local level leaves (low-frequency error across blocks)."""
+    sc = scenes.config_small(side=128, steps=3)
+    a = gpu(sc, "chebyshev_coarse", order=1, max_iter=20000, rel_tol=1e-7)
+    b = gpu(sc, "chebyshev", order=1, max_iter=20000, rel_tol=1e-7)
+    for _ in range(2):
+        a.step()
+        b.step()
+        assert a.stats()[2] == capi.SOLVE_CONVERGED and b.stats()[2] == capi.SOLVE_CONVERGED
+    assert a.sim.preconditioner()[3] == 2
+    assert a.sim.solver_info()[2] == 512  # 16 slices of 32 rows per CTA
+    assert a.stats()[0] < 0.8 * b.stats()[0]
+    np.testing.assert_allclose(a.positions(), b.positions(), atol=2e-5)
+
+
+@pytest.mark.parametrize("warm", ["zero", "previous", "previous_scaled"])
+def test_coarse_trajectories_with_ragged_blocks(warm):
+    """48 x 48 particles: 4.5 blocks of 512 rows (the last one ragged)."""
+    sc = scenes.config_small(side=48, steps=6)
+    a = gpu(sc, "chebyshev_coarse", max_iter=20000, rel_tol=1e-7, warm_start=warm)
+    b = gpu(sc, "block_jacobi", max_iter=20000, rel_tol=1e-7, warm_start=warm)
+    o = oracle_sim(sc, 1e-11)
+    for _ in range(6):
+        a.step()
+        b.step()
+        o.step(sc["dt"])
+        assert a.stats()[2] == capi.SOLVE_CONVERGED
+    assert a.sim.preconditioner()[3] == 2
+    ref = o.state()[0]
+    assert np.abs(a.positions() - ref).max() <= max(3.0 * np.abs(b.positions() - ref).max(), 2e-5)
+
+
+def test_coarse_is_deterministic_and_falls_back_in_batches():
+    sc = scenes.config_small(side=64, steps=3)
+    runs = []
+    for _ in range(2):
+        g = gpu(sc, "chebyshev_coarse", max_iter=300, rel_tol=0.0)
+        g.run(3, record_iters=False)
+        runs.append(g.positions())
+    np.testing.assert_array_equal(runs[0], runs[1])
+    # a batch of instances keeps the local level only
+    scs = [scenes.config_small(side=s, steps=3) for s in (12, 20)]
+    bsc, offs = scenes.concat(scs)
+    g = gpu(bsc, "chebyshev_coarse", max_iter=20000, rel_tol=1e-7, instances=offs)
+    g.run(2, record_iters=False)
+    assert g.sim.preconditioner()[3] == 1
+    assert all(s == capi.SOLVE_CONVERGED for s in g.sim.instance_stats()[2])
