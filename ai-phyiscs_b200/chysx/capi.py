@@ -348,6 +348,7 @@ class Cloth:
         r = ctypes.c_float()
         check(self._L.chysx_cloth_preconditioner(self.h, ctypes.byref(k), ctypes.byref(d), ctypes.byref(r),
                                                  ctypes.byref(u)))
+        # in_use: 0 block-Jacobi, 1 local, 2 two-level (translations), 3 two-level (translations + linear fields)
         return ("block_jacobi", "chebyshev", "chebyshev_coarse")[k.value], d.value, r.value, u.value
 
     def solver_info(self):

@@ -798,7 +798,7 @@ public:
         if (kind) *kind = pc_kind_;
         if (degree) *degree = pc_degree_;
         if (ratio) *ratio = pc_ratio_;
-        if (in_use) *in_use = pc_active() ? (coarse_on_ ? 2 : 1) : 0;
+        if (in_use) *in_use = pc_active() ? (coarse_on_ ? (coarse_nq_ > 1 ? 3 : 2) : 1) : 0;
     }
     // the CTA-local preconditioner runs in the register-resident kernel of
     // the default synchronisation mode (with the coarse level where the plan
@@ -1175,6 +1175,7 @@ private:
         if (graph_) cudaGraphDestroy(graph_);
         exec_ = nullptr;
         graph_ = nullptr;
+        cfield_node_ = nullptr;
     }
 
     void build_graph() {
@@ -1309,7 +1310,8 @@ private:
             build_plan(topo_.inst_slice, grid, plan_);
             plan_coarse();
             pers_smem_ = (size_t)W * kSlotW * sizeof(double) + (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
-            if (coarse_on_) pers_smem_ += (size_t)9 * coarse_nb_ * sizeof(float);  // 3 rows of A_c^-1
+            if (coarse_on_)  // the coarse block's rows of A_c^-1
+                pers_smem_ += (size_t)9 * coarse_nq_ * coarse_nq_ * coarse_nb_ * sizeof(float);
             // static + dynamic above 48 KB needs the opt-in
             ck(cudaFuncSetAttribute(persistent_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pers_smem_),
                "cudaFuncSetAttribute(resident smem)");
@@ -1322,75 +1324,164 @@ private:
         return false;
     }
 
-    // Coarse level of the two-level preconditioner (kind 2): one block per
-    // CTA of a single-instance resident plan.  Host side: the CTA of every
-    // slice, every block's sorted list of the blocks its rows touch, and the
-    // list position of every ELL entry's column block.
-    void plan_coarse() {
-        coarse_on_ = false;
-        if (pc_kind_ != 2 || !resident_ || sync_mode_ != 0 || plan_.n_inst != 1 || plan_.grid > kCoarseMaxBlocks)
-            return;
-        const int nb = plan_.grid, ns = topo_.n_slices;
-        std::vector<int> slice_cta(std::max(1, ns), 0);
-        for (int c = 0; c < nb; ++c)
-            for (int sl = plan_.cta_slice[c]; sl < plan_.cta_slice[c + 1]; ++sl) slice_cta[sl] = c;
+    // Coarse level of the two-level preconditioner (kind 2) of a
+    // single-instance resident plan: coarse blocks of G consecutive CTAs with
+    // nq fields each; (G, nq) = (4, 4) (translation and linear fields on
+    // 4-CTA blocks) where its coarse system fits the inverse kernel's shared
+    // memory, else (1, 1) (the translation of every CTA block).  Host side:
+    // the coarse block of every slice and its first row, every block's sorted
+    // list of the blocks its rows touch, and the list position of every ELL
+    // entry's column block.
+    bool plan_coarse_with(int G, int nq) {
+        const int grid = plan_.grid, ns = topo_.n_slices;
+        const int nb = (grid + G - 1) / G, U = 3 * nq, m = U * nb;
+        const int rpc = (m + grid - 1) / grid;
+        if (m > kCoarseThreads || rpc > kCoarseMaxRhs) return false;
+        std::vector<int> slice_cb(std::max(1, ns), 0), row0(nb + 1, 0);
+        for (int c = 0; c < grid; ++c)
+            for (int sl = plan_.cta_slice[c]; sl < plan_.cta_slice[c + 1]; ++sl) slice_cb[sl] = c / G;
+        for (int B = 0; B <= nb; ++B) row0[B] = plan_.cta_slice[std::min(grid, B * G)] * 32;
         std::vector<std::vector<int>> lists(nb);
-        for (int c = 0; c < nb; ++c) {
-            std::vector<int>& l = lists[c];
-            l.push_back(c);
-            for (int sl = plan_.cta_slice[c]; sl < plan_.cta_slice[c + 1]; ++sl)
-                for (int e = topo_.slice_off[sl]; e < topo_.slice_off[sl + 1]; ++e) l.push_back(slice_cta[topo_.col[e] >> 5]);
+        for (int B = 0; B < nb; ++B) {
+            std::vector<int>& l = lists[B];
+            l.push_back(B);
+            for (int sl = row0[B] / 32; sl < row0[B + 1] / 32; ++sl)
+                for (int e = topo_.slice_off[sl]; e < topo_.slice_off[sl + 1]; ++e) l.push_back(slice_cb[topo_.col[e] >> 5]);
             std::sort(l.begin(), l.end());
             l.erase(std::unique(l.begin(), l.end()), l.end());
-            if ((int)l.size() > kCoarseMaxNbr) return;  // too many touching blocks: local level only
+            if ((int)l.size() > kCoarseMaxNbr) return false;
         }
         int mn = 1;
         for (const auto& l : lists) mn = std::max(mn, (int)l.size());
+        // band order of the blocks: reverse Cuthill-McKee (breadth-first from
+        // a block of least degree, neighbours by increasing degree, ties by
+        // index), then the band half-width in unknowns
+        std::vector<int> order, perm(nb, -1);
+        std::vector<char> seen(nb, 0);
+        auto degree = [&](int B) { return (int)lists[B].size(); };
+        while ((int)order.size() < nb) {
+            int start = -1;
+            for (int B = 0; B < nb; ++B)
+                if (!seen[B] && (start < 0 || degree(B) < degree(start))) start = B;
+            // pseudo-peripheral start (George-Liu): from the last level of a
+            // breadth-first search, a block of least degree, while the
+            // eccentricity grows
+            for (int rep = 0, ecc = -1; rep < 8; ++rep) {
+                std::vector<int> lev(nb, -1), q{start};
+                lev[start] = 0;
+                for (size_t h = 0; h < q.size(); ++h)
+                    for (int C : lists[q[h]])
+                        if (lev[C] < 0 && !seen[C]) {
+                            lev[C] = lev[q[h]] + 1;
+                            q.push_back(C);
+                        }
+                const int e = lev[q.back()];
+                if (e <= ecc) break;
+                ecc = e;
+                int best = -1;
+                for (int C : q)
+                    if (lev[C] == e && (best < 0 || degree(C) < degree(best))) best = C;
+                start = best;
+            }
+            seen[start] = 1;
+            size_t head = order.size();
+            order.push_back(start);
+            while (head < order.size()) {
+                const int B = order[head++];
+                std::vector<int> nx;
+                for (int C : lists[B])
+                    if (!seen[C]) nx.push_back(C);
+                std::sort(nx.begin(), nx.end(), [&](int a, int b) {
+                    return degree(a) != degree(b) ? degree(a) < degree(b) : a < b;
+                });
+                for (int C : nx) {
+                    seen[C] = 1;
+                    order.push_back(C);
+                }
+            }
+        }
+        std::reverse(order.begin(), order.end());
+        for (int p = 0; p < nb; ++p) perm[order[p]] = p;
+        int bwb = 0;
+        for (int B = 0; B < nb; ++B)
+            for (int C : lists[B]) bwb = std::max(bwb, std::abs(perm[B] - perm[C]));
+        const int bw = std::min(m - 1, (bwb + 1) * U - 1);
+        const size_t direct_smem = ((size_t)m * (bw + 1) + m + (size_t)rpc * m) * sizeof(float);
+        if (direct_smem > kCoarseDirectSmemMax) return false;
         std::vector<int> nbr((size_t)nb * mn, -1), cnt(nb), self(nb);
-        for (int c = 0; c < nb; ++c) {
-            cnt[c] = (int)lists[c].size();
-            for (int k = 0; k < cnt[c]; ++k) {
-                nbr[(size_t)c * mn + k] = lists[c][k];
-                if (lists[c][k] == c) self[c] = k;
+        for (int B = 0; B < nb; ++B) {
+            cnt[B] = (int)lists[B].size();
+            for (int k = 0; k < cnt[B]; ++k) {
+                nbr[(size_t)B * mn + k] = lists[B][k];
+                if (lists[B][k] == B) self[B] = k;
             }
         }
         std::vector<unsigned char> ell(std::max<size_t>(1, topo_.col.size()), 0);
-        for (int c = 0; c < nb; ++c)
-            for (int sl = plan_.cta_slice[c]; sl < plan_.cta_slice[c + 1]; ++sl)
+        for (int B = 0; B < nb; ++B)
+            for (int sl = row0[B] / 32; sl < row0[B + 1] / 32; ++sl)
                 for (int e = topo_.slice_off[sl]; e < topo_.slice_off[sl + 1]; ++e) {
-                    const int cb = slice_cta[topo_.col[e] >> 5];
-                    ell[e] = (unsigned char)(std::lower_bound(lists[c].begin(), lists[c].end(), cb) - lists[c].begin());
+                    const int cb = slice_cb[topo_.col[e] >> 5];
+                    ell[e] = (unsigned char)(std::lower_bound(lists[B].begin(), lists[B].end(), cb) - lists[B].begin());
                 }
-        d_slice_cta_.upload(slice_cta);
+        d_slice_cb_.upload(slice_cb);
+        d_cb_row0_.upload(row0);
         d_cnbr_.upload(nbr);
         d_ccnt_.upload(cnt);
         d_cself_.upload(self);
         d_ell_nbr_.upload(ell);
-        d_cac_.resize((size_t)nb * mn * 9);
+        d_cperm_.upload(perm);
+        coarse_bw_ = bw;
+        if (nq > 1) {
+            d_cw_.resize((size_t)std::max(1, row0[nb]));
+            d_cw_.zero();
+        }
+        d_cac_.resize((size_t)nb * mn * U * U);
         d_cac_.zero();
-        d_cainv_.resize((size_t)9 * nb * nb);
+        d_cainv_.resize((size_t)m * m);
         d_cainv_.zero();
         coarse_nb_ = nb;
         coarse_mn_ = mn;
+        coarse_g_ = G;
+        coarse_nq_ = nq;
+        coarse_rpc_ = rpc;
         coarse_on_ = true;
-        // static + dynamic above 48 KB needs the opt-in
-        ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_inverse_kernel),
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_inverse_smem()),
-           "cudaFuncSetAttribute(coarse inverse smem)");
+        ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_direct_kernel),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_direct_smem()),
+           "cudaFuncSetAttribute(coarse direct smem)");
+        return true;
     }
-    size_t coarse_inverse_smem() const {
-        return ((size_t)coarse_nb_ * coarse_mn_ * 9 + 6 * 3 * (size_t)coarse_nb_) * sizeof(float);
+    void plan_coarse() {
+        coarse_on_ = false;
+        if (pc_kind_ != 2 || !resident_ || sync_mode_ != 0 || plan_.n_inst != 1 || plan_.grid > kCoarseMaxBlocks)
+            return;
+        if (plan_.grid >= 8 && plan_coarse_with(4, 4)) return;
+        plan_coarse_with(1, 1);
+    }
+    // dynamic shared memory of the coarse direct kernel: the FP32 band of
+    // A_c, the scaling and the right-hand sides (below the 227 KB of a CTA)
+    static constexpr size_t kCoarseDirectSmemMax = 220 * 1024;
+    size_t coarse_direct_smem() const {
+        const size_t m = 3 * (size_t)coarse_nq_ * coarse_nb_;
+        return (m * (coarse_bw_ + 1) + m + (size_t)coarse_rpc_ * m) * sizeof(float);
     }
     CoarseArgs coarse_args() const {
         CoarseArgs c{};
         c.on = coarse_on_ ? 1 : 0;
         c.nb = coarse_nb_;
+        c.g = coarse_g_;
+        c.nq = coarse_nq_;
+        c.m = 3 * coarse_nq_ * coarse_nb_;
+        c.rpc = coarse_rpc_;
         c.max_nbr = coarse_mn_;
-        c.slice_cta = d_slice_cta_.get();
+        c.slice_cb = d_slice_cb_.get();
+        c.cb_row0 = d_cb_row0_.get();
         c.nbr = d_cnbr_.get();
         c.nbr_cnt = d_ccnt_.get();
         c.self_idx = d_cself_.get();
         c.ell_nbr = d_ell_nbr_.get();
+        c.perm = d_cperm_.get();
+        c.bw = coarse_bw_;
+        c.w = coarse_nq_ > 1 ? d_cw_.get() : nullptr;
         c.ac = d_cac_.get();
         c.ainv = d_cainv_.get();
         return c;
@@ -1575,25 +1666,37 @@ private:
         ck(cudaGraphAddKernelNode(&asm_node_, graph_, t0 ? &t0 : nullptr, t0 ? 1 : 0, &ap), "add assemble node");
         cudaGraphNode_t t1 = add_guess_node(asm_node_, cur_args_, t, v);
         if (coarse_on_) {
-            // the coarse system of this step's matrix, before the solve
+            // the coarse space and system of this step's matrix, before the solve
             CoarseArgs cg = coarse_args();
-            const int* cslice = d_cta_slice_.get();
-            void* a1[] = {&t, &cslice, &cg};
+            StepArgs sa = cur_args_;
+            cudaGraphNode_t prev = t1;
+            cfield_node_ = nullptr;
+            if (coarse_nq_ > 1) {
+                void* a0[] = {&sa, &cg};
+                cudaKernelNodeParams p0{};
+                p0.func = reinterpret_cast<void*>(&coarse_fields_kernel);
+                p0.gridDim = dim3(coarse_nb_);
+                p0.blockDim = dim3(256);
+                p0.kernelParams = a0;
+                ck(cudaGraphAddKernelNode(&cfield_node_, graph_, &prev, 1, &p0), "add coarse fields node");
+                prev = cfield_node_;
+            }
+            void* a1[] = {&t, &cg};
             cudaKernelNodeParams p{};
             p.func = reinterpret_cast<void*>(&coarse_assemble_kernel);
-            p.gridDim = dim3(coarse_nb_);
+            p.gridDim = dim3(coarse_nb_, coarse_nq_ * coarse_nq_);
             p.blockDim = dim3(288);
             p.kernelParams = a1;
             cudaGraphNode_t n1, n2;
-            ck(cudaGraphAddKernelNode(&n1, graph_, &t1, 1, &p), "add coarse assemble node");
+            ck(cudaGraphAddKernelNode(&n1, graph_, &prev, 1, &p), "add coarse assemble node");
             void* a2[] = {&cg};
             cudaKernelNodeParams p2{};
-            p2.func = reinterpret_cast<void*>(&coarse_inverse_kernel);
-            p2.gridDim = dim3(coarse_nb_);
+            p2.func = reinterpret_cast<void*>(&coarse_direct_kernel);
+            p2.gridDim = dim3(plan_.grid);
             p2.blockDim = dim3(kCoarseThreads);
-            p2.sharedMemBytes = (unsigned)coarse_inverse_smem();
+            p2.sharedMemBytes = (unsigned)coarse_direct_smem();
             p2.kernelParams = a2;
-            ck(cudaGraphAddKernelNode(&n2, graph_, &n1, 1, &p2), "add coarse inverse node");
+            ck(cudaGraphAddKernelNode(&n2, graph_, &n1, 1, &p2), "add coarse direct node");
             t1 = n2;
         }
         t1 = timing_node(1, t1);
@@ -1768,6 +1871,16 @@ private:
             fp.blockDim = dim3(kVecBlock);
             fp.kernelParams = fargs;
             ck(cudaGraphExecKernelNodeSetParams(exec_, fin_node_, &fp), "update finalize node");
+            if (coarse_on_ && cfield_node_) {  // the coarse fields read x_n
+                CoarseArgs cg = coarse_args();
+                void* cargs[] = {&a, &cg};
+                cudaKernelNodeParams cp{};
+                cp.func = reinterpret_cast<void*>(&coarse_fields_kernel);
+                cp.gridDim = dim3(coarse_nb_);
+                cp.blockDim = dim3(256);
+                cp.kernelParams = cargs;
+                ck(cudaGraphExecKernelNodeSetParams(exec_, cfield_node_, &cp), "update coarse fields node");
+            }
             patch_guess_node(a, t, v);
             node_args_ = a;
             node_cfg_ = c;
@@ -1862,9 +1975,10 @@ private:
     int sync_mode_ = 0;    // 0 grid counter barrier, 1 polled per-instance slots
     int pc_kind_ = 0, pc_degree_ = 0;  // preconditioner: 0 block-Jacobi, 1 CTA-local Chebyshev, 2 + coarse level
     bool coarse_on_ = false;
-    int coarse_nb_ = 0, coarse_mn_ = 0;
-    DevBuf<int> d_slice_cta_, d_cnbr_, d_ccnt_, d_cself_;
+    int coarse_nb_ = 0, coarse_mn_ = 0, coarse_g_ = 1, coarse_nq_ = 1, coarse_rpc_ = 1, coarse_bw_ = 0;
+    DevBuf<int> d_slice_cb_, d_cb_row0_, d_cnbr_, d_ccnt_, d_cself_, d_cperm_;
     DevBuf<unsigned char> d_ell_nbr_;
+    DevBuf<float4> d_cw_;
     DevBuf<float> d_cac_, d_cainv_;
     float pc_ratio_ = 0.0f;
     DevBuf<ZP> d_zp_;
@@ -1887,6 +2001,7 @@ private:
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;
     cudaGraphNode_t asm_node_ = nullptr, fin_node_ = nullptr;
+    cudaGraphNode_t cfield_node_ = nullptr;  // coarse fields (two-level preconditioner with linear fields)
     cudaGraphConditionalHandle cond_ = 0;
     StepArgs cur_args_{}, node_args_{};
     SolverCfg cur_cfg_{}, node_cfg_{};

@@ -1,19 +1,20 @@
 // Coarse level of the two-level preconditioner of the register-resident PCG
 // kernel (no counterpart in the reference, whose PCG is block-Jacobi).
 //
-// Each CTA block B of rows contributes three coarse unknowns: the block's
-// rigid translation.  With R the matrix that copies a block's translation to
-// every row of the block, the coarse system is A_c = R^T A R: the 3x3 block
-// (B, C) sums A_ij over rows i of B and columns j of C.  It is block-sparse
-// (a CTA's rows touch a handful of other CTAs' rows).  The preconditioner
+// Coarse block B is the rows of G consecutive CTAs of the plan; its fields
+// are the block's translation and, optionally, its three linear fields along
+// the principal axes of its positions (coarse_types.h).  With R the matrix
+// that maps a block's field amplitudes to its rows, the coarse system is
+// A_c = R^T A R, block-sparse (a block's rows touch a handful of other
+// blocks).  The preconditioner
 //     M^-1 = P_local + R A_c^-1 R^T,
 // P_local the CTA-local Chebyshev polynomial, is a fixed symmetric
 // positive-definite operator, so the outer iteration stays plain PCG.  Per
-// step: coarse_assemble_kernel (one CTA per block, deterministic per-lane
-// partial sums added in lane order) and coarse_inverse_kernel (CTA B solves
-// A_c X = [e_3B e_3B+1 e_3B+2] by block-Jacobi CG, giving rows 3B..3B+2 of
-// A_c^-1); per iteration the resident kernel forms its block of
-// A_c^-1 R^T r as one block sum, the blocks' restricted residuals riding on
+// step: coarse_fields_kernel (the weights), coarse_assemble_kernel (one CTA
+// per block and field pair, deterministic per-lane partial sums added in
+// lane order) and coarse_direct_kernel (every CTA factors A_c and solves
+// for its rows of A_c^-1); per iteration the resident kernel forms its
+// block of A_c^-1 R^T r from the blocks' restricted residuals, which ride on
 // the existing reduction slots.
 #pragma once
 
@@ -28,156 +29,286 @@ __device__ __forceinline__ int sym_plane(int c) {
     return lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
 }
 
-// A_c block row of CTA block B: 9 warps (one per component), lane l takes
-// the rows l of every slice of the block; per-lane sums in shared memory,
-// then each (neighbour, component) sum over lanes in lane order (double).
-__global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, const int* __restrict__ cta_slice,
-                                                              CoarseArgs ca) {
-    __shared__ float acc[9][kCoarseMaxNbr][32];
-    const int B = blockIdx.x;
-    const int c = threadIdx.x >> 5, l = threadIdx.x & 31;
-    for (int q = 0; q < ca.max_nbr; ++q) acc[c][q][l] = 0.0f;
-    const int pl = sym_plane(c);
-    const int self = ca.self_idx[B];
-    for (int s = cta_slice[B]; s < cta_slice[B + 1]; ++s) {
-        const int i = s * 32 + l;
-        if (i >= t.n) break;
-        acc[c][self][l] += t.diag[(size_t)s * 192 + pl * 32 + l];
-        const int so = t.slice_off[s];
-        const int w = (t.slice_off[s + 1] - so) >> 5;
-        for (int k = 0; k < w; ++k) {
-            const int e = so + k * 32 + l;
-            const int nb = ca.ell_nbr[e];
-            acc[c][nb][l] += t.val[(size_t)so * 6 + (size_t)k * 192 + pl * 32 + l];
-        }
+// Weight of field q of internal row i (q = 0: the translation).
+__device__ __forceinline__ float coarse_weight(const CoarseArgs& ca, int i, int q) {
+    if (q == 0) return 1.0f;
+    const float4 w = ca.w[i];
+    return q == 1 ? w.x : (q == 2 ? w.y : w.z);
+}
+
+// Sums of K doubles over a CTA of NT threads; every thread gets the totals.
+template <int K, int NT>
+__device__ __forceinline__ void cta_sums(double* v, double (*red)[K]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const double s = warp_sum(v[q]);
+        if (lane == 0) red[warp][q] = s;
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < ca.max_nbr * 9; q += blockDim.x) {
-        const int nb = q / 9, cc = q % 9;
-        double sum = 0.0;
-        for (int k = 0; k < 32; ++k) sum += acc[cc][nb][k];
-        ca.ac[((size_t)B * ca.max_nbr + nb) * 9 + cc] = (float)sum;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        double tot = 0.0;
+        for (int w = 0; w < NT / 32; ++w) tot += red[w][q];
+        v[q] = tot;
+    }
+    __syncthreads();
+}
+
+// The linear-field weights of coarse block B (nq = 4): centroid and
+// covariance of the block's positions x_n (double), the principal axes by
+// cyclic Jacobi rotations (thread 0), then s_a = (x_i - c).u_a / sd_a for
+// every row, sd_a^2 = the variance along u_a per row; axes with variance
+// below 1e-6 of the largest get weight 0.  Padding rows get weight 0.
+__global__ void __launch_bounds__(256) coarse_fields_kernel(StepArgs a, CoarseArgs ca) {
+    __shared__ double red[8][6];
+    __shared__ float s_ax[3][3], s_isd[3], s_c[3];
+    const int B = blockIdx.x;
+    const int r0 = ca.cb_row0[B], r1 = min(ca.cb_row0[B + 1], a.n);
+    auto ext_of = [&](int i) { return a.row_to_ext ? a.row_to_ext[i] : i; };
+    double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int i = r0 + (int)threadIdx.x; i < r1; i += blockDim.x) {
+        const int e = ext_of(i);
+        if (e < 0) continue;
+        v[0] += a.pos[3 * (size_t)e];
+        v[1] += a.pos[3 * (size_t)e + 1];
+        v[2] += a.pos[3 * (size_t)e + 2];
+        v[3] += 1.0;
+    }
+    cta_sums<6, 256>(v, red);
+    const double cnt = v[3] > 0.0 ? v[3] : 1.0;
+    const double c0 = v[0] / cnt, c1 = v[1] / cnt, c2 = v[2] / cnt;
+    double q[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int i = r0 + (int)threadIdx.x; i < r1; i += blockDim.x) {
+        const int e = ext_of(i);
+        if (e < 0) continue;
+        const double d0 = a.pos[3 * (size_t)e] - c0, d1 = a.pos[3 * (size_t)e + 1] - c1, d2 = a.pos[3 * (size_t)e + 2] - c2;
+        q[0] += d0 * d0; q[1] += d0 * d1; q[2] += d0 * d2;
+        q[3] += d1 * d1; q[4] += d1 * d2; q[5] += d2 * d2;
+    }
+    cta_sums<6, 256>(q, red);
+    if (threadIdx.x == 0) {
+        double A[9] = {q[0], q[1], q[2], q[1], q[3], q[4], q[2], q[4], q[5]};
+        double V[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+        for (int sweep = 0; sweep < 30; ++sweep) {
+            const double off = A[1] * A[1] + A[2] * A[2] + A[5] * A[5];
+            const double dia = A[0] * A[0] + A[4] * A[4] + A[8] * A[8];
+            if (!(off > 1e-30 * dia)) break;  // diagonal to double precision
+            for (int p = 0; p < 2; ++p)
+                for (int r = p + 1; r < 3; ++r) {
+                    const double apr = A[3 * p + r];
+                    if (fabs(apr) < 1e-300) continue;
+                    const double th = 0.5 * (A[3 * r + r] - A[3 * p + p]) / apr;
+                    const double t = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+                    const double cs = 1.0 / sqrt(t * t + 1.0), sn = t * cs;
+                    for (int k = 0; k < 3; ++k) {
+                        const double akp = A[3 * k + p], akr = A[3 * k + r];
+                        A[3 * k + p] = cs * akp - sn * akr;
+                        A[3 * k + r] = sn * akp + cs * akr;
+                    }
+                    for (int k = 0; k < 3; ++k) {
+                        const double apk = A[3 * p + k], ark = A[3 * r + k];
+                        A[3 * p + k] = cs * apk - sn * ark;
+                        A[3 * r + k] = sn * apk + cs * ark;
+                    }
+                    for (int k = 0; k < 3; ++k) {
+                        const double vkp = V[3 * k + p], vkr = V[3 * k + r];
+                        V[3 * k + p] = cs * vkp - sn * vkr;
+                        V[3 * k + r] = sn * vkp + cs * vkr;
+                    }
+                }
+        }
+        int ord[3] = {0, 1, 2};  // by decreasing variance (stable)
+        for (int x = 0; x < 3; ++x)
+            for (int y = 0; y < 2; ++y)
+                if (A[4 * ord[y + 1]] > A[4 * ord[y]]) { const int tmp = ord[y]; ord[y] = ord[y + 1]; ord[y + 1] = tmp; }
+        const double lmax = fmax(A[0], fmax(A[4], A[8]));
+        for (int k = 0; k < 3; ++k) {
+            const int ax = ord[k];
+            const double lam = A[4 * ax];
+            const bool keep = lam > 1e-6 * lmax && lam > 0.0;
+            for (int c = 0; c < 3; ++c) s_ax[k][c] = (float)V[3 * c + ax];
+            s_isd[k] = keep ? (float)(1.0 / sqrt(lam / cnt)) : 0.0f;
+        }
+        s_c[0] = (float)c0; s_c[1] = (float)c1; s_c[2] = (float)c2;
+    }
+    __syncthreads();
+    for (int i = r0 + (int)threadIdx.x; i < ca.cb_row0[B + 1]; i += blockDim.x) {
+        const int e = i < a.n ? ext_of(i) : -1;
+        float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (e >= 0) {
+            const float d0 = a.pos[3 * (size_t)e] - s_c[0], d1 = a.pos[3 * (size_t)e + 1] - s_c[1],
+                        d2 = a.pos[3 * (size_t)e + 2] - s_c[2];
+            w.x = (d0 * s_ax[0][0] + d1 * s_ax[0][1] + d2 * s_ax[0][2]) * s_isd[0];
+            w.y = (d0 * s_ax[1][0] + d1 * s_ax[1][1] + d2 * s_ax[1][2]) * s_isd[1];
+            w.z = (d0 * s_ax[2][0] + d1 * s_ax[2][1] + d2 * s_ax[2][2]) * s_isd[2];
+        }
+        ca.w[i] = w;
     }
 }
 
-// Rows 3B..3B+2 of A_c^-1 (A_c symmetric: the columns), B = blockIdx.x:
-// three block-Jacobi preconditioned CG solves in lockstep, one thread per
-// coarse unknown, A_c in shared memory.  Stops when every relative residual
-// is below kCoarseTol or after kCoarseMaxIts iterations; a non-finite solve
-// leaves zero rows (the coarse level then adds nothing).  Dynamic shared
-// memory: nb * max_nbr * 9 + 6 * 3 nb floats.
-__global__ void __launch_bounds__(kCoarseThreads) coarse_inverse_kernel(CoarseArgs ca) {
-    extern __shared__ float cs_mem[];
-    __shared__ int s_nbr[kCoarseMaxBlocks * kCoarseMaxNbr];
-    __shared__ int s_cnt[kCoarseMaxBlocks];
-    __shared__ double s_red[2][kCoarseThreads / 32][6];
-    const int nb = ca.nb, mn = ca.max_nbr, m3 = 3 * nb;
-    const int B = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    constexpr int kWarps = kCoarseThreads / 32;
-    float* a_s = cs_mem;                        // [nb][mn][9]
-    float* p_s = a_s + (size_t)nb * mn * 9;     // [3][m3] search directions
-    float* r_s = p_s + 3 * m3;                  // [3][m3] residuals
-    for (int q = t; q < nb * mn * 9; q += blockDim.x) a_s[q] = ca.ac[q];
-    for (int q = t; q < nb * mn; q += blockDim.x) s_nbr[q] = ca.nbr[q];
-    for (int q = t; q < nb; q += blockDim.x) s_cnt[q] = ca.nbr_cnt[q];
-    __syncthreads();
-    const bool own = t < m3;
-    const int blk = own ? t / 3 : 0, comp = own ? t % 3 : 0;
-    // row `comp` of the inverse of A_c's diagonal block of `blk` (double)
-    float di[3] = {0.f, 0.f, 0.f};
-    if (own) {
-        const float* a = a_s + ((size_t)blk * mn + ca.self_idx[blk]) * 9;
-        const double a0 = a[0], a1 = a[1], a2 = a[2], a3 = a[3], a4 = a[4], a5 = a[5], a6 = a[6], a7 = a[7], a8 = a[8];
-        const double det = a0 * (a4 * a8 - a5 * a7) - a1 * (a3 * a8 - a5 * a6) + a2 * (a3 * a7 - a4 * a6);
-        const double s = det != 0.0 ? 1.0 / det : 0.0;
-        const double adj[9] = {a4 * a8 - a5 * a7, a2 * a7 - a1 * a8, a1 * a5 - a2 * a4,
-                               a5 * a6 - a3 * a8, a0 * a8 - a2 * a6, a2 * a3 - a0 * a5,
-                               a3 * a7 - a4 * a6, a1 * a6 - a0 * a7, a0 * a4 - a1 * a3};
-        for (int c = 0; c < 3; ++c) di[c] = (float)(adj[3 * comp + c] * s);
-    }
-    // sums of up to 6 values over the CTA, every thread gets the totals
-    auto block_sums = [&](double* v, int k, int set) {
-        for (int q = 0; q < k; ++q) {
-            const double w = warp_sum(v[q]);
-            if (lane == 0) s_red[set][warp][q] = w;
-        }
-        __syncthreads();
-        for (int q = 0; q < k; ++q) {
-            double tot = 0.0;
+// A_c block row of coarse block B for the field pair (q, q') =
+// (blockIdx.y / nq, blockIdx.y % nq): 9 warps (one per component of the
+// 3x3 block), lane l takes the rows l of every slice of the block; per-lane
+// sums of w_iq w_jq' A_ij in shared memory by column block, then each
+// (column block, component) sum over lanes in lane order (double).
+__global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, CoarseArgs ca) {
+    __shared__ float acc[9][kCoarseMaxNbr][32];
+    const int B = blockIdx.x, qa = blockIdx.y / ca.nq, qb = blockIdx.y % ca.nq;
+    const int U = 3 * ca.nq;
+    const int c = threadIdx.x >> 5, l = threadIdx.x & 31;
+    for (int k = 0; k < ca.max_nbr; ++k) acc[c][k][l] = 0.0f;
+    const int pl = sym_plane(c);
+    const int self = ca.self_idx[B];
+    const int s0 = ca.cb_row0[B] >> 5, s1 = ca.cb_row0[B + 1] >> 5;
+    for (int s = s0; s < s1; ++s) {
+        const int i = s * 32 + l;
+        if (i >= t.n) break;
+        const float wi = coarse_weight(ca, i, qa);
+        acc[c][self][l] += wi * coarse_weight(ca, i, qb) * t.diag[(size_t)s * 192 + pl * 32 + l];
+        const int so = t.slice_off[s];
+        const int w = (t.slice_off[s + 1] - so) >> 5;
+        // the row's entries 8 at a time: every load of a batch in flight
+        for (int k0 = 0; k0 < w; k0 += 8) {
+            int cj[8], nb8[8];
+            float wv[8], vv[8];
 #pragma unroll
-            for (int w = 0; w < kWarps; ++w) tot += s_red[set][w][q];
-            v[q] = tot;
+            for (int k = 0; k < 8; ++k) {
+                const bool in = k0 + k < w;
+                const int e = so + (k0 + k) * 32 + l;
+                cj[k] = in ? t.col[e] : i;
+                nb8[k] = in ? ca.ell_nbr[e] : 0;
+                vv[k] = in ? t.val[(size_t)so * 6 + (size_t)(k0 + k) * 192 + pl * 32 + l] : 0.0f;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) wv[k] = coarse_weight(ca, cj[k], qb);
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (k0 + k < w) acc[c][nb8[k]][l] += wi * wv[k] * vv[k];
         }
-    };
-    auto precond = [&](int j) {  // (D_c^-1 r_j)_t from r_s
-        const float* r = r_s + j * m3 + 3 * blk;
-        return own ? di[0] * r[0] + di[1] * r[1] + di[2] * r[2] : 0.f;
-    };
-    float x[3], r[3], z[3], p[3];
-    double rz[3];
-    for (int j = 0; j < 3; ++j) {
-        x[j] = 0.f;
-        r[j] = own && t == 3 * B + j ? 1.f : 0.f;
-        if (own) r_s[j * m3 + t] = r[j];
     }
     __syncthreads();
-    {
-        double v[3];
-        for (int j = 0; j < 3; ++j) {
-            z[j] = precond(j);
-            p[j] = z[j];
-            v[j] = (double)r[j] * z[j];
-        }
-        block_sums(v, 3, 1);
-        for (int j = 0; j < 3; ++j) rz[j] = v[j];
+    for (int x = threadIdx.x; x < ca.max_nbr * 9; x += blockDim.x) {
+        const int k = x / 9, cc = x % 9;
+        double sum = 0.0;
+        for (int y = 0; y < 32; ++y) sum += acc[cc][k][y];
+        const int r = cc / 3, col = cc % 3;
+        ca.ac[(((size_t)B * ca.max_nbr + k) * U + qa * 3 + r) * U + qb * 3 + col] = (float)sum;
     }
-    bool bad = false;
-    for (int it = 0; it < kCoarseMaxIts; ++it) {
-        if (own)
-            for (int j = 0; j < 3; ++j) p_s[j * m3 + t] = p[j];
+}
+
+// Rows blockIdx.x * rpc + j (j < rpc) of A_c^-1 by a direct solve: every
+// CTA factors A_c (band storage in shared memory, FP32, blocks in the band
+// order perm, symmetric diagonal scaling D^-1/2 A_c D^-1/2) by a
+// column-oriented band Cholesky and solves L L^T y = D^-1/2 e_r for its rows;
+// A_c^-1 e_r = D^-1/2 y.  Unknowns of a field of weight 0 everywhere (a
+// dropped axis) have a zero diagonal and get identity rows; a non-positive
+// pivot leaves zero rows (the coarse level then adds nothing this step).
+// The factorisation is the same in every CTA (same operations, same order),
+// so all CTAs agree bitwise.  Dynamic shared memory: (m (bw + 1) + m + rpc m)
+// floats.
+__global__ void __launch_bounds__(kCoarseThreads) coarse_direct_kernel(CoarseArgs ca) {
+    extern __shared__ float cd_mem[];
+    __shared__ int s_fail;
+    const int nb = ca.nb, mn = ca.max_nbr, U = 3 * ca.nq, m = ca.m, bw = ca.bw, W1 = bw + 1, rpc = ca.rpc;
+    const int t = threadIdx.x, nt = blockDim.x;
+    float* L = cd_mem;                   // [m][W1]: L[i W1 + k] = entry (i, i - k)
+    float* dsc = L + (size_t)m * W1;     // [m] 1 / sqrt(A_ii)
+    float* y = dsc + m;                  // [rpc][m] right-hand sides / solutions, band order
+    if (t == 0) s_fail = 0;
+    for (int x = t; x < m * W1; x += nt) L[x] = 0.0;
+    __syncthreads();
+    const int bsz = mn * U * U;
+    for (int x = t; x < nb * bsz; x += nt) {
+        const int B = x / bsz, rem = x % bsz, k = rem / (U * U), e = rem % (U * U);
+        if (k >= ca.nbr_cnt[B]) continue;
+        const int C = ca.nbr[B * mn + k];
+        const int pi = ca.perm[B] * U + e / U, pj = ca.perm[C] * U + e % U;
+        if (pj > pi) continue;  // the lower triangle (A_c symmetric)
+        L[(size_t)pi * W1 + (pi - pj)] = ca.ac[x];
+    }
+    __syncthreads();
+    for (int i = t; i < m; i += nt) {
+        float d = L[(size_t)i * W1];
+        if (!(d > 0.0f)) {  // a dropped field: identity row (its other entries are zero)
+            d = 1.0f;
+            L[(size_t)i * W1] = 1.0f;
+        }
+        dsc[i] = rsqrtf(d);
+    }
+    __syncthreads();
+    for (int x = t; x < m * W1; x += nt) {
+        const int i = x / W1, k = x % W1;
+        if (i - k >= 0) L[x] *= dsc[i] * dsc[i - k];
+    }
+    __syncthreads();
+    // band Cholesky, column j: L_jj = sqrt(a_jj); L_ij /= L_jj; trailing update
+    for (int j = 0; j < m; ++j) {
+        const int hi = min(m - 1, j + bw), cnt = hi - j;
+        const float ajj = L[(size_t)j * W1];
+        const bool piv = ajj > 1e-30f;
+        const float ljj = piv ? sqrtf(ajj) : 1.0f, inv = 1.0f / ljj;
+        __syncthreads();  // every thread has read a_jj
+        if (t == 0) {
+            L[(size_t)j * W1] = ljj;
+            if (!piv) s_fail = 1;
+        }
+        for (int q = t; q < cnt; q += nt) L[(size_t)(j + 1 + q) * W1 + (1 + q)] *= inv;
         __syncthreads();
-        float ap[3] = {0.f, 0.f, 0.f};
-        if (own) {
-            for (int k = 0; k < s_cnt[blk]; ++k) {
-                const float* a = a_s + ((size_t)blk * mn + k) * 9 + 3 * comp;
-                const int cb = 3 * s_nbr[blk * mn + k];
-                const float a0 = a[0], a1 = a[1], a2 = a[2];
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const float* pj = p_s + j * m3 + cb;
-                    ap[j] = fmaf(a0, pj[0], fmaf(a1, pj[1], fmaf(a2, pj[2], ap[j])));
-                }
+        // warp w takes rows i = j+1+a for a = w, w + nwarps, ...; its lanes
+        // the columns k = j+1+b, b <= a
+        for (int a = t >> 5; a < cnt; a += nt >> 5) {
+            const int i = j + 1 + a;
+            float* Li = L + (size_t)i * W1;
+            const float lij = Li[i - j];
+            for (int b = t & 31; b <= a; b += 32) {
+                const int k = j + 1 + b;
+                Li[i - k] -= lij * L[(size_t)k * W1 + (k - j)];
             }
         }
-        double v[6];
-        for (int j = 0; j < 3; ++j) v[j] = (double)p[j] * ap[j];
-        block_sums(v, 3, 0);
-        for (int j = 0; j < 3; ++j) {
-            const double al = (v[j] > 1e-300 || v[j] < -1e-300) ? rz[j] / v[j] : 0.0;
-            if (!isfinite(al)) bad = true;
-            x[j] = fmaf((float)al, p[j], x[j]);
-            r[j] = fmaf(-(float)al, ap[j], r[j]);
-            if (own) r_s[j * m3 + t] = r[j];
-        }
         __syncthreads();
-        for (int j = 0; j < 3; ++j) {
-            z[j] = precond(j);
-            v[j] = (double)r[j] * z[j];
-            v[3 + j] = (double)r[j] * r[j];
-        }
-        block_sums(v, 6, 1);
-        bool conv = true;
-        for (int j = 0; j < 3; ++j) {
-            const double be = (rz[j] > 1e-300 || rz[j] < -1e-300) ? v[j] / rz[j] : 0.0;
-            rz[j] = v[j];
-            p[j] = fmaf((float)be, p[j], z[j]);
-            conv = conv && v[3 + j] <= kCoarseTol * kCoarseTol;
-            if (!isfinite(v[3 + j])) bad = true;
-        }
-        if (bad || conv) break;  // uniform: every thread holds the same totals
     }
-    if (own)
-        for (int j = 0; j < 3; ++j) ca.ainv[(size_t)(3 * B + j) * m3 + t] = bad ? 0.f : x[j];
+    // this CTA's rows r = blockIdx.x rpc + s: right-hand side D^-1/2 e_r in band order
+    const int r0 = blockIdx.x * rpc;
+    for (int x = t; x < rpc * m; x += nt) y[x] = 0.0f;
+    __syncthreads();
+    if (t < rpc && r0 + t < m) {
+        const int r = r0 + t, pr = ca.perm[r / U] * U + r % U;
+        y[(size_t)t * m + pr] = dsc[pr];
+    }
+    __syncthreads();
+    // the triangular solves: warp sr takes right-hand side sr (the band's
+    // entries of a column across its lanes); forward L z = b column by
+    // column, then backward L^T y = z
+    const int sr = t >> 5, ln = t & 31;
+    if (sr < rpc) {
+        float* ys = y + (size_t)sr * m;
+        for (int j = 0; j < m; ++j) {
+            const int cnt = min(m - 1, j + bw) - j;
+            const float yj = ys[j] / L[(size_t)j * W1];
+            for (int q = 1 + ln; q <= cnt; q += 32) ys[j + q] -= L[(size_t)(j + q) * W1 + q] * yj;
+            __syncwarp();
+            if (ln == 0) ys[j] = yj;
+            __syncwarp();
+        }
+        for (int i = m - 1; i >= 0; --i) {
+            const int lo = max(0, i - bw);
+            const float yi = ys[i] / L[(size_t)i * W1];
+            for (int k = lo + ln; k < i; k += 32) ys[k] -= L[(size_t)i * W1 + (i - k)] * yi;
+            __syncwarp();
+            if (ln == 0) ys[i] = yi;
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    // rows of A_c^-1 in the original unknown order: A_c^-1[r][q] = dsc_q y[p(q)]
+    for (int x = t; x < rpc * m; x += nt) {
+        const int s = x / m, q = x % m;
+        if (r0 + s >= m) continue;
+        const int pq = ca.perm[q / U] * U + q % U;
+        const float v = dsc[pq] * y[(size_t)s * m + pq];
+        ca.ainv[(size_t)(r0 + s) * m + q] = (s_fail || !isfinite(v)) ? 0.0f : v;
+    }
 }
 
 }  // namespace chysx_b200

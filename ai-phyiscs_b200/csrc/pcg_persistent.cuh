@@ -25,7 +25,11 @@
 namespace chysx_b200 {
 
 constexpr int kSolveKernelError = 3;
-constexpr int kSlotW = 8;  // doubles per reduction slot and per slice partial
+constexpr int kSlotW = 8;      // doubles per reduction slot and per slice partial
+constexpr int kStartW = 8;     // start partials (the first phase)
+constexpr int kCoarseOff = 2;  // slot entry where the coarse values start (after up to 2 scalars):
+                               // up to 12 floats (48 bytes) there
+constexpr int kCoarsePartW = 12;  // per-slice coarse partials (floats), beside the slice partials
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
 
 struct alignas(128) GridBarrier {
@@ -315,92 +319,186 @@ __device__ __forceinline__ void warp0_publish(const BatchPlan& bp, const double*
     }
 }
 
+// The counter-mode read of a phase (after the barrier): every instance's
+// totals of the first NR values, all of a lane's slots in flight at once
+// (fixed unroll), summed in ascending slot order; lane 0 applies `step`.
+template <int NR, int KP, class Step>
+__device__ __forceinline__ void warp0_read_totals(const BatchPlan& bp, LocalInst* li, int nloc, int set, Step&& step) {
+    const int lane = threadIdx.x & 31;
+    for (int t = 0; t < nloc; ++t) {
+        LocalInst& L = li[t];
+        if (L.done) continue;
+        double tot[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) tot[q] = 0.0;
+        for (int c0 = L.slot_lo; c0 < L.slot_hi; c0 += 32 * KP) {
+            double val[KP][NR];
+#pragma unroll
+            for (int j = 0; j < KP; ++j) {
+                const int k = c0 + j * 32 + lane;
+#pragma unroll
+                for (int q = 0; q < NR; ++q)
+                    val[j][q] = k < L.slot_hi ? __ldcg(bp.slots + ((size_t)set * bp.n_slots + k) * kSlotW + q) : 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < KP; ++j) {
+                if (c0 + j * 32 + lane < L.slot_hi) {
+#pragma unroll
+                    for (int q = 0; q < NR; ++q) tot[q] += val[j][q];
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NR; ++q) tot[q] = warp_sum(tot[q]);
+        if (lane == 0) step(L, tot);
+        __syncwarp();
+    }
+}
+
 // One reduction phase, run by warp 0 between two __syncthreads: publishes
 // the CTA's segments, waits for the other CTAs (counter barrier or polled
 // slots), reads each instance's total in a fixed order and lets lane 0
 // apply `step(L, total)`.  For instances spanning at most 32 * KP CTAs (one
-// pass of loads).  Publishes NV values per segment and (counter mode) reads
-// back the totals of the first NR.  Returns false (on all lanes) after a
-// failed wait.
-template <int NV, int SYNC, int KP, int NR = NV, class Step>
+// pass of loads).  Returns false (on all lanes) after a failed wait.
+template <int NV, int SYNC, int KP, class Step>
 __device__ __forceinline__ bool warp0_phase(const BatchPlan& bp, const double* spart, LocalInst* li, int nloc,
                                             int set, unsigned& target, Step&& step) {
     const int lane = threadIdx.x & 31;
     warp0_publish<NV, SYNC>(bp, spart, li, nloc, set);
-    if (!SYNC) {
+    if constexpr (!SYNC) {
         bool ok = true;
         if (lane == 0) ok = barrier_arrive_wait(bp.bar, target);
         if (!__shfl_sync(0xffffffffu, ok, 0)) return false;
-    }
-    for (int t = 0; t < nloc; ++t) {
-        LocalInst& L = li[t];
-        if (L.done) continue;
-        double tot[NV];
-        if (SYNC) {
+        warp0_read_totals<NV, KP>(bp, li, nloc, set, step);
+        return true;
+    } else {
+        for (int t = 0; t < nloc; ++t) {
+            LocalInst& L = li[t];
+            if (L.done) continue;
+            double tot[NV];
             if (!poll_total<NV, KP>(bp, L, set, tot)) return false;
-        } else {
-            // all of a lane's slots in flight at once (fixed unroll), summed
-            // in ascending slot order
-#pragma unroll
-            for (int q = 0; q < NV; ++q) tot[q] = 0.0;
-            for (int c0 = L.slot_lo; c0 < L.slot_hi; c0 += 32 * KP) {
-                double val[KP][NR];
-#pragma unroll
-                for (int j = 0; j < KP; ++j) {
-                    const int k = c0 + j * 32 + lane;
-#pragma unroll
-                    for (int q = 0; q < NR; ++q)
-                        val[j][q] = k < L.slot_hi ? __ldcg(bp.slots + ((size_t)set * bp.n_slots + k) * kSlotW + q) : 0.0;
-                }
-#pragma unroll
-                for (int j = 0; j < KP; ++j) {
-                    if (c0 + j * 32 + lane < L.slot_hi) {
-#pragma unroll
-                        for (int q = 0; q < NR; ++q) tot[q] += val[j][q];
-                    }
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < NR; ++q) tot[q] = warp_sum(tot[q]);
+            if (lane == 0) step(L, tot);
+            __syncwarp();
         }
-        if (lane == 0) step(L, tot);
-        __syncwarp();
+        return true;
     }
-    return true;
 }
 
-// Coarse level of a single-instance two-level plan (counter barrier): this
-// CTA's block of A_c^-1 v, v_k = the values Q0..Q0+2 of slot k (block k) of
-// `set`, A_c^-1's rows 3B..3B+2 in `ainv` ([3][m3]), formed by one warp (warp
-// 1 during a phase, while warp 0 reads the scalar totals).  Lane l takes
-// slots l, l + 32, ...; every lane returns the sums (warp-summed, fixed
-// order).
-__device__ __forceinline__ float3 coarse_slot_dot(float v0, float v1, float v2, int m3, const float* ainv, int k,
-                                                  float3 acc) {
-    const float* a = ainv + 3 * k;
-    acc.x = fmaf(a[0], v0, fmaf(a[1], v1, fmaf(a[2], v2, acc.x)));
-    acc.y = fmaf(a[m3], v0, fmaf(a[m3 + 1], v1, fmaf(a[m3 + 2], v2, acc.y)));
-    acc.z = fmaf(a[2 * m3], v0, fmaf(a[2 * m3 + 1], v1, fmaf(a[2 * m3 + 2], v2, acc.z)));
-    return acc;
-}
-__device__ __forceinline__ float3 warp_sum3(float3 v) {
+// ---- coarse level of a single-instance two-level plan (counter barrier) --
+// Coarse values of a phase sit in slot entries kCoarseOff.. of every CTA;
+// coarse block C's value is the sum over its CTAs C G .. C G + G - 1.
+
+// Per-warp restriction of one row's v: the U = 3 nq sums over the warp's
+// lanes of w_iq v (w_i0 = 1), written to dst[0..U) (fixed summation order).
+// nq = 4: recursive halving of 16 values (12 used), 16 shuffles; value k's
+// total lands in lanes 2k and 2k + 1.
+__device__ __forceinline__ void warp_restrict(int nq, float3 v, float4 w, float* dst) {
+    const int lane = threadIdx.x & 31;
+    if (nq == 1) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
-        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
-        v.z += __shfl_xor_sync(0xffffffffu, v.z, o);
+        for (int o = 16; o > 0; o >>= 1) {
+            v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+            v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+            v.z += __shfl_xor_sync(0xffffffffu, v.z, o);
+        }
+        if (lane == 0) {
+            dst[0] = v.x;
+            dst[1] = v.y;
+            dst[2] = v.z;
+        }
+        return;
     }
-    return v;
+    float a[16] = {v.x, v.y, v.z, w.x * v.x, w.x * v.y, w.x * v.z, w.y * v.x, w.y * v.y,
+                   w.y * v.z, w.z * v.x, w.z * v.y, w.z * v.z, 0.f, 0.f, 0.f, 0.f};
+    float b8[8], b4[4], b2[2];
+    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4, h2 = lane & 2;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        b8[k] = (h16 ? a[k + 8] : a[k]) + __shfl_xor_sync(0xffffffffu, h16 ? a[k] : a[k + 8], 16);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        b4[k] = (h8 ? b8[k + 4] : b8[k]) + __shfl_xor_sync(0xffffffffu, h8 ? b8[k] : b8[k + 4], 8);
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+        b2[k] = (h4 ? b4[k + 2] : b4[k]) + __shfl_xor_sync(0xffffffffu, h4 ? b4[k] : b4[k + 2], 4);
+    float b1 = (h2 ? b2[1] : b2[0]) + __shfl_xor_sync(0xffffffffu, h2 ? b2[0] : b2[1], 2);
+    b1 += __shfl_xor_sync(0xffffffffu, b1, 1);
+    const int k = lane >> 1;
+    if ((lane & 1) == 0 && k < 12) dst[k] = b1;
 }
-template <int Q0>
-__device__ __forceinline__ float3 warp_coarse_dot(const BatchPlan& bp, int set, const float* ainv) {
-    const int lane = threadIdx.x & 31, m3 = 3 * bp.cg.nb;
-    float3 acc = make_float3(0.f, 0.f, 0.f);
-    for (int k = lane; k < bp.n_slots; k += 32) {
-        const double* v = bp.slots + ((size_t)set * bp.n_slots + k) * kSlotW + Q0;
-        acc = coarse_slot_dot((float)__ldcg(v), (float)__ldcg(v + 1), (float)__ldcg(v + 2), m3, ainv, k, acc);
+
+// Float view of the coarse values of slot k of `set`.
+__device__ __forceinline__ float* coarse_slot(const BatchPlan& bp, int set, int k) {
+    return reinterpret_cast<float*>(bp.slots + ((size_t)set * bp.n_slots + k) * kSlotW + kCoarseOff);
+}
+
+// The CTA's coarse values (lane q < U: the sum over the CTA's nsl slices'
+// partials, in slice order) into its slot of `set` (warp 1).
+__device__ __forceinline__ void warp1_coarse_publish(const BatchPlan& bp, const float* cpart, int nsl, int own_slot,
+                                                     int set) {
+    const int lane = threadIdx.x & 31, U = 3 * bp.cg.nq;
+    if (lane < U) {
+        float acc = 0.0f;
+        for (int w = 0; w < nsl; ++w) acc += cpart[w * kCoarsePartW + lane];
+        coarse_slot(bp, set, own_slot)[lane] = acc;
     }
-    return warp_sum3(acc);
+}
+
+// Rows [r0, r0 + 4) (those below U) of this CTA's block of A_c^-1 v, v the
+// coarse values of `set`, with the block's rows of A_c^-1 in `ainv`
+// ([U][m]); lane 0 writes them to out[r0..].  A coarse block's value is the
+// sum of its CTAs' slots and the product is linear, so lane l takes the
+// slots l, l + 32, ... directly (each against its block's columns).
+template <int U>
+__device__ __forceinline__ void warp_coarse_rows(const BatchPlan& bp, int set, const float* ainv, int r0, float* out) {
+    const int lane = threadIdx.x & 31, m = bp.cg.m, G = bp.cg.g;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int k = lane; k < bp.n_slots; k += 32) {
+        const float* sl = coarse_slot(bp, set, k);
+        float v[U];
+        if (U % 4 == 0) {
+#pragma unroll
+            for (int u = 0; u < U; u += 4) {
+                const float4 q = __ldcg(reinterpret_cast<const float4*>(sl + u));
+                v[u] = q.x; v[u + 1] = q.y; v[u + 2] = q.z; v[u + 3] = q.w;
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u) v[u] = __ldcg(sl + u);
+        }
+        const int C = k / G;
+#pragma unroll
+        for (int rr = 0; rr < 4; ++rr) {
+            if (r0 + rr >= U) break;
+            const float* a = ainv + (size_t)(r0 + rr) * m + C * U;
+#pragma unroll
+            for (int u = 0; u < U; ++u) acc[rr] = fmaf(a[u], v[u], acc[rr]);
+        }
+    }
+#pragma unroll
+    for (int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], o);
+    }
+    if (lane == 0)
+        for (int rr = 0; rr < 4 && r0 + rr < U; ++rr) out[r0 + rr] = acc[rr];
+}
+
+__device__ __forceinline__ void named_barrier_w01() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
+// warp 0 and the coarse warps 1..nw: warp 0 passes it after the grid barrier
+__device__ __forceinline__ void named_barrier_coarse(int nthreads) {
+    asm volatile("bar.sync 2, %0;" ::"r"(nthreads) : "memory");
+}
+
+// This row's share of a coarse vector c ([U]): c_0 + sum_q w_q c_q per component.
+__device__ __forceinline__ float3 coarse_prolong(int nq, const float* c, float4 w) {
+    float3 o = make_float3(c[0], c[1], c[2]);
+    if (nq == 4) {
+        o.x = fmaf(w.x, c[3], fmaf(w.y, c[6], fmaf(w.z, c[9], o.x)));
+        o.y = fmaf(w.x, c[4], fmaf(w.y, c[7], fmaf(w.z, c[10], o.y)));
+        o.z = fmaf(w.x, c[5], fmaf(w.y, c[8], fmaf(w.z, c[11], o.z)));
+    }
+    return o;
 }
 
 // The same phase with the whole CTA reading the slots, for instances that
@@ -508,18 +606,18 @@ __device__ __forceinline__ void block_phase(const BatchPlan& bp, const double* s
     }
 }
 
-// Start partials of one row, kSlotW wide: r.z, r.r, b.b, b.M^-1 b, x0.b,
+// Start partials of one row, kStartW wide: r.z, r.r, b.b, b.M^-1 b, x0.b,
 // x0.r, b.z, b.r (with r = b - A x0, z = M^-1 r; the zero guess has x0 = 0,
 // r = b, z = M^-1 b).  The warp sums land in sp[q].
 __device__ __forceinline__ void start_partials(double* sp, bool write, float3 b, float3 zb, float3 x0, float3 r,
                                                float3 z) {
-    double q[kSlotW] = {dot3d(r, z), dot3d(r, r), dot3d(b, b), dot3d(b, zb),
-                        dot3d(x0, b), dot3d(x0, r), dot3d(b, z), dot3d(b, r)};
+    double q[kStartW] = {dot3d(r, z), dot3d(r, r), dot3d(b, b), dot3d(b, zb),
+                         dot3d(x0, b), dot3d(x0, r), dot3d(b, z), dot3d(b, r)};
 #pragma unroll
-    for (int k = 0; k < kSlotW; ++k) q[k] = warp_sum(q[k]);
+    for (int k = 0; k < kStartW; ++k) q[k] = warp_sum(q[k]);
     if (write) {
 #pragma unroll
-        for (int k = 0; k < kSlotW; ++k) sp[k] = q[k];
+        for (int k = 0; k < kStartW; ++k) sp[k] = q[k];
     }
 }
 
@@ -681,31 +779,36 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
         __syncthreads();                                                                             \
     } while (0)
 
-// The same protocol for single-instance two-level plans: warp 0 publishes NV
-// values and reads the totals of the first NR; warp 1 waits on the same
-// counter (the phase's target: every phase so far was one barrier) and
-// writes this CTA's block of A_c^-1 v, v the values Q0..Q0+2, to OUT[0..2].
-#define CHYSX_COARSE_PHASE(NV, NR, Q0, OUT, exit_test, STEP)                                         \
+// The same protocol for single-instance two-level plans: warp 0 publishes
+// the NR scalars (spart entries 0..NR-1), warp 1 the coarse values (floats
+// from the per-slice coarse partials), both before warp 0 arrives (named
+// barrier of warps 0 and 1: warp 0's release then covers warp 1's stores);
+// warp 0 waits on the grid barrier and then releases the coarse warps
+// 1..c_nw through a second named barrier (its acquire orders their slot
+// reads), reads the scalar totals while they form the rows of this CTA's
+// block of A_c^-1 v into OUT[0..U).
+#define CHYSX_COARSE_PHASE(NR, OUT, exit_test, STEP)                                                 \
     do {                                                                                             \
         if (warp == 0) {                                                                             \
-            const bool w0ok = warp0_phase<NV, 0, kPollMax, NR>(bp, spart, li, nloc, slot_set(ph), target, STEP); \
-            if (lane == 0) {                                                                         \
-                if (!w0ok) s_flag = 1;                                                               \
-                if ((exit_test) && w0ok) s_exit = *(volatile unsigned*)&bp.bar->ndone >= (unsigned)bp.n_inst; \
+            warp0_publish<NR, 0>(bp, spart, li, nloc, slot_set(ph));                                 \
+            named_barrier_w01();                                                                     \
+            bool w0ok = true;                                                                        \
+            if (lane == 0) w0ok = barrier_arrive_wait(bp.bar, target);                               \
+            w0ok = __shfl_sync(0xffffffffu, w0ok, 0);                                                \
+            if (lane == 0 && !w0ok) s_flag = 1;                                                      \
+            named_barrier_coarse(32 * (1 + c_nw));                                                   \
+            if (w0ok) warp0_read_totals<NR, kPollMax>(bp, li, nloc, slot_set(ph), STEP);             \
+            if (lane == 0 && (exit_test) && w0ok)                                                    \
+                s_exit = *(volatile unsigned*)&bp.bar->ndone >= (unsigned)bp.n_inst;                 \
+        } else if (warp <= c_nw) {                                                                   \
+            if (warp == 1) {                                                                         \
+                warp1_coarse_publish(bp, s_cpart, s1 - s0, li[0].own_slot, slot_set(ph));            \
+                named_barrier_w01();                                                                 \
             }                                                                                        \
-        } else if (warp == 1) {                                                                      \
-            bool w1ok = true;                                                                        \
-            if (lane == 0) w1ok = barrier_wait_only(bp.bar, (unsigned)(ph + 1) * gridDim.x);         \
-            w1ok = __shfl_sync(0xffffffffu, w1ok, 0);                                                \
-            if (w1ok) {                                                                              \
-                const float3 cw = warp_coarse_dot<Q0>(bp, slot_set(ph), c_ainv);                     \
-                if (lane == 0) {                                                                     \
-                    (OUT)[0] = cw.x;                                                                 \
-                    (OUT)[1] = cw.y;                                                                 \
-                    (OUT)[2] = cw.z;                                                                 \
-                }                                                                                    \
-            } else if (lane == 0) {                                                                  \
-                s_flag = 1;                                                                          \
+            named_barrier_coarse(32 * (1 + c_nw));                                                   \
+            if (!*(volatile int*)&s_flag) {                                                          \
+                if (c_U == 12) warp_coarse_rows<12>(bp, slot_set(ph), c_ainv, 4 * (warp - 1), OUT);  \
+                else warp_coarse_rows<3>(bp, slot_set(ph), c_ainv, 4 * (warp - 1), OUT);             \
             }                                                                                        \
         }                                                                                            \
         ++ph;                                                                                        \
@@ -731,7 +834,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
     extern __shared__ double s_mem[];
     __shared__ int s_flag;
     __shared__ int s_exit;
-    __shared__ double s_red[BLOCK * kSlotW];  // per-thread slot sums of block_phase
+    __shared__ double s_red[BLOCK * kStartW];  // per-thread slot sums of block_phase (NV <= kStartW)
     constexpr int W = BLOCK / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
@@ -784,7 +887,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
         start_partials(spart + (s - s0) * kSlotW, lane == 0, b, zb, x0, r, z);
     }
     __syncthreads();
-    CHYSX_BLOCK_PHASE(kSlotW, 1, false,
+    CHYSX_BLOCK_PHASE(kStartW, 1, false,
                       ([&](LocalInst& L, const double* tot) { step_start(bp, L, tot, cfg, warm); }));
     ok = s_flag == 0;
     if (ok && warm) {
@@ -945,7 +1048,8 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     __shared__ double s_bsum[PC ? W : 1];
     __shared__ float s_cheb[4];
     // coarse level: this block of A_c^-1 R^T (A p) and of A_c^-1 R^T r
-    __shared__ float s_cw[4], s_cu[4];
+    __shared__ float s_cw[12], s_cu[12];
+    __shared__ float s_cpart[PC == 2 ? W * kCoarsePartW : 1];  // per-slice coarse partials
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
     const int il0 = bp.cta_inst_lo[blockIdx.x], il1 = bp.cta_inst_hi[blockIdx.x];
@@ -1079,16 +1183,21 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         __syncthreads();
     }
 
-    // ---- coarse level (PC = 2 with bp.cg.on): rows 3B..3B+2 of A_c^-1 (B
-    // this CTA) in dynamic shared memory behind the LocalInst records; warp 0
-    // forms this block of A_c^-1 R^T v while it reads the blocks' slot sums
+    // ---- coarse level (PC = 2 with bp.cg.on): this CTA's coarse block
+    // Bc = blockIdx.x / G; its U rows of A_c^-1 in dynamic shared memory
+    // behind the LocalInst records; every row's field weights in a register
+    // quad.  Warps 1..3 form this block of A_c^-1 R^T v during the phases.
     constexpr bool kCoarse = PC == 2;
     const bool coarse = kCoarse && bp.cg.on;
+    const int c_nq = coarse ? bp.cg.nq : 1, c_U = 3 * c_nq;
+    const int c_nw = (c_U + 3) / 4;  // coarse warps (rows of 4)
     float* c_ainv = reinterpret_cast<float*>(li + bp.max_inst_per_cta);
+    float4 c_w = make_float4(0.f, 0.f, 0.f, 0.f);
     if (coarse) {
-        const int m3 = 3 * bp.cg.nb;
-        const float* src = bp.cg.ainv + (size_t)3 * blockIdx.x * m3;
-        for (int q = threadIdx.x; q < 3 * m3; q += blockDim.x) c_ainv[q] = src[q];
+        const int m = bp.cg.m;
+        const float* src = bp.cg.ainv + (size_t)(blockIdx.x / bp.cg.g) * c_U * m;
+        for (int q = threadIdx.x; q < c_U * m; q += blockDim.x) c_ainv[q] = src[q];
+        if (c_nq == 4 && row) c_w = bp.cg.w[i];
         __syncthreads();
     }
 
@@ -1109,30 +1218,20 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         }
         float3 cb = f3(0.f, 0.f, 0.f), cr = cb;
         if (coarse) {
-            // R^T b and R^T r0 of every block through one exchange phase
-            const float3 sb = row ? b : f3(0.f, 0.f, 0.f), sr = row ? r : f3(0.f, 0.f, 0.f);
-            const double q6[6] = {warp_sum((double)sb.x), warp_sum((double)sb.y), warp_sum((double)sb.z),
-                                  warp_sum((double)sr.x), warp_sum((double)sr.y), warp_sum((double)sr.z)};
-            if (lane == 0 && has)
-                for (int q = 0; q < 6; ++q) spart[warp * kSlotW + q] = q6[q];
-            else if (lane == 0)
-                for (int q = 0; q < 6; ++q) spart[warp * kSlotW + q] = 0.0;
-            __syncthreads();
-            CHYSX_REDUCE_PHASE(6, 1, false, no_step);
+            // A_c^-1 R^T b (s_cw) and, for a warm start, A_c^-1 R^T r0 (s_cu):
+            // one exchange phase each
+            for (int pass = 0; pass < (warm ? 2 : 1); ++pass) {
+                const float3 sv = row ? (pass ? r : b) : f3(0.f, 0.f, 0.f);
+                if (lane == 0) spart[warp * kSlotW] = 0.0;
+                warp_restrict(c_nq, sv, c_w, s_cpart + (PC == 2 ? warp * kCoarsePartW : 0));
+                __syncthreads();
+                CHYSX_COARSE_PHASE(1, pass ? s_cu : s_cw, false, no_step);
+                if (s_flag) break;
+            }
             ok = s_flag == 0;
             if (ok) {
-                // this block of A_c^-1 R^T b (s_cw) and A_c^-1 R^T r0 (s_cu)
-                if (warp == 0) {
-                    const float3 ub = warp_coarse_dot<0>(bp, slot_set(ph - 1), c_ainv);
-                    const float3 u0 = warp_coarse_dot<3>(bp, slot_set(ph - 1), c_ainv);
-                    if (lane == 0) {
-                        s_cw[0] = ub.x; s_cw[1] = ub.y; s_cw[2] = ub.z;
-                        s_cu[0] = u0.x; s_cu[1] = u0.y; s_cu[2] = u0.z;
-                    }
-                }
-                __syncthreads();
-                cb = f3(s_cw[0], s_cw[1], s_cw[2]);
-                if (warm) cr = f3(s_cu[0], s_cu[1], s_cu[2]);
+                cb = coarse_prolong(c_nq, s_cw, c_w);
+                if (warm) cr = coarse_prolong(c_nq, s_cu, c_w);
             }
         }
         zb = precond(b) + cb;
@@ -1164,7 +1263,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         start_partials(spart + warp * kSlotW, lane == 0 && has, b, zb, x, r, z);
     }
     __syncthreads();
-    CHYSX_REDUCE_PHASE(kSlotW, 1, false,
+    CHYSX_REDUCE_PHASE(kStartW, 1, false,
                        ([&](LocalInst& L, const double* tot) { step_start(bp, L, tot, cfg, warm); }));
     ok = s_flag == 0;
     if (ok && warm) {
@@ -1187,7 +1286,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         const LocalInst& L0 = li[0];
         const bool from_r0 = warm && !L0.fallback;
         __syncthreads();  // every thread has read s_cw, s_cu
-        if (threadIdx.x < 3) {
+        if ((int)threadIdx.x < c_U) {
             const float ub = s_cw[threadIdx.x], u0 = s_cu[threadIdx.x];
             s_cu[threadIdx.x] = from_r0 ? fmaf(L0.scale, u0, L0.scale_b * ub) : ub;
         }
@@ -1254,21 +1353,16 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
             sig = (double)p.x * acc.x + (double)p.y * acc.y + (double)p.z * acc.z;
         }
         sig = warp_sum(sig);
-        if (kCoarse) {
-            // the CTA's sum of Ap, for the coarse correction's update (it
-            // only feeds the preconditioner: float warp sums)
+        if (coarse) {
+            // the warp's restriction of Ap, for the coarse correction's
+            // update (it only feeds the preconditioner: float sums)
             const bool act = row && !li[li_idx].done;
-            const float3 sa = warp_sum3(act ? ap : f3(0.f, 0.f, 0.f));
-            if (lane == 0 && has) {
-                spart[warp * kSlotW + 1] = sa.x;
-                spart[warp * kSlotW + 2] = sa.y;
-                spart[warp * kSlotW + 3] = sa.z;
-            }
+            warp_restrict(c_nq, act ? ap : f3(0.f, 0.f, 0.f), c_w, s_cpart + (PC == 2 ? warp * kCoarsePartW : 0));
         }
         if (lane == 0 && has) spart[warp * kSlotW] = sig;
         __syncthreads();
         if (coarse)
-            CHYSX_COARSE_PHASE(4, 1, 1, s_cw, true, ([&](LocalInst& L, const double* tot) { step_alpha(L, tot); }));
+            CHYSX_COARSE_PHASE(1, s_cw, true, ([&](LocalInst& L, const double* tot) { step_alpha(L, tot); }));
         else
             CHYSX_REDUCE_PHASE(1, kPollMax, true, ([&](LocalInst& L, const double* tot) { step_alpha(L, tot); }));
         if (s_flag) {
@@ -1277,9 +1371,12 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         }
         if (!SYNC && s_exit) break;
         if (coarse) {
-            // A_c^-1 R^T r_new = A_c^-1 R^T r - alpha A_c^-1 R^T A p
+            // A_c^-1 R^T r_new = A_c^-1 R^T r - alpha A_c^-1 R^T A p, this row's share
             const float al = li[0].alpha;
-            c_blk = f3(fmaf(-al, s_cw[0], s_cu[0]), fmaf(-al, s_cw[1], s_cu[1]), fmaf(-al, s_cw[2], s_cu[2]));
+            float cn[12];
+#pragma unroll
+            for (int u = 0; u < 12; ++u) cn[u] = u < c_U ? fmaf(-al, s_cw[u], s_cu[u]) : 0.f;
+            c_blk = coarse_prolong(c_nq, cn, c_w);
         }
 
         double rz = 0.0, rr = 0.0;
@@ -1308,19 +1405,14 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
             spart[warp * kSlotW] = rz;
             spart[warp * kSlotW + 1] = rr;
         }
-        if (kCoarse) {
-            // the CTA's sum of the new r: the coarse correction restarts
-            // from R^T r every iteration (no drift)
-            const float3 sr = warp_sum3(act ? r : f3(0.f, 0.f, 0.f));
-            if (lane == 0 && has) {
-                spart[warp * kSlotW + 2] = sr.x;
-                spart[warp * kSlotW + 3] = sr.y;
-                spart[warp * kSlotW + 4] = sr.z;
-            }
+        if (coarse) {
+            // the warp's restriction of the new r: the coarse correction
+            // restarts from R^T r every iteration (no drift)
+            warp_restrict(c_nq, act ? r : f3(0.f, 0.f, 0.f), c_w, s_cpart + (PC == 2 ? warp * kCoarsePartW : 0));
         }
         __syncthreads();
         if (coarse)
-            CHYSX_COARSE_PHASE(5, 2, 2, s_cu, false, ([&](LocalInst& L, const double* tot) { step_beta(bp, L, tot, cfg); }));
+            CHYSX_COARSE_PHASE(2, s_cu, false, ([&](LocalInst& L, const double* tot) { step_beta(bp, L, tot, cfg); }));
         else
             CHYSX_REDUCE_PHASE(2, kPollMax, false, ([&](LocalInst& L, const double* tot) { step_beta(bp, L, tot, cfg); }));
         if (s_flag) {

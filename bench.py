@@ -442,7 +442,7 @@ def run_ours(args, rank, world, local_rank):
     # preconditioner in use)
     kern = g.sim.solver_info()[0]
     if kern == "resident":
-        kern += {0: "", 1: "_chebyshev", 2: "_twolevel"}[int(g.sim.preconditioner()[3])]
+        kern += {0: "", 1: "_chebyshev", 2: "_twolevel", 3: "_twolevel_linear"}[int(g.sim.preconditioner()[3])]
     traffic_it = read_traffic(kern, args.workload)
     steps_total = args.steps * world
     value = steps_total / (total_ms_max * 1e-3)
@@ -521,8 +521,9 @@ def run_ours(args, rank, world, local_rank):
             "note": "compiled reference ClothSimulator (springs enabled), same scene with geometric-mean "
                     "stiffness, PCG fixed at the block-Jacobi iterations/step the same steps take, stream 0"},
         # assemble, reset, persistent PCG, finalize; the two-level
-        # preconditioner adds the coarse assembly and the coarse inverse
-        "gpu_launches": (6 if g.sim.preconditioner()[3] == 2 else 4) * args.steps,
+        # preconditioner adds the coarse assembly and the coarse inverse, and
+        # with linear fields the fields kernel
+        "gpu_launches": {2: 6, 3: 7}.get(g.sim.preconditioner()[3], 4) * args.steps,
         "clocks": clk,
         "wall_s": wall,
     }

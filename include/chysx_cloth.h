@@ -389,13 +389,17 @@ int chysx_cloth_row_of_particles(const chysx_cloth* h, int n, int32_t* rows);
  * power iteration with a 10% margin.  A fixed polynomial, so the outer
  * iteration stays plain PCG with the same stopping test (||r|| / ||b||);
  * odd degrees keep p positive on the whole spectrum.  Kind 2 = kind 1 plus
- * a coarse level: z += R q(D_c^-1 A_c) D_c^-1 R^T r, R the rigid translation
- * of every CTA's block of rows, A_c = R^T A R (3 unknowns per CTA, assembled
- * on the device each step), q a Chebyshev polynomial of degree 7 on
- * [lambda_c / 100, lambda_c]; it applies to single-instance systems of at
- * most 160 CTAs and acts as kind 1 elsewhere.  Kinds 1 and 2 apply where the
- * register-resident kernel runs with synchronisation mode 0; in_use reports
- * what the last graph build uses (0 block-Jacobi, 1 local, 2 two-level). */
+ * a coarse level: z += R A_c^-1 R^T r, A_c = R^T A R assembled on the device
+ * each step, R the coarse space: on blocks of 4 consecutive CTAs (2048 rows
+ * of a spatially ordered 256 x 256 grid) the translation and the three
+ * linear fields along the principal axes of the block's positions, where
+ * that coarse system fits the device's shared memory, else the translation
+ * of every CTA's block; every CTA computes its rows of A_c^-1 by CG before
+ * the solve.  It applies to single-instance systems of at most 160 CTAs and
+ * acts as kind 1 elsewhere.  Kinds 1 and 2 apply where the register-resident
+ * kernel runs with synchronisation mode 0; in_use reports what the last graph
+ * build uses (0 block-Jacobi, 1 local, 2 two-level with translations, 3
+ * two-level with translations and linear fields). */
 int chysx_cloth_set_preconditioner(chysx_cloth* h, int kind, int degree, float ratio);
 int chysx_cloth_preconditioner(const chysx_cloth* h, int* kind, int* degree, float* ratio, int* in_use);
 /* Kernel used at the last graph build: path 0 register-resident persistent,

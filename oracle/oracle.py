@@ -77,8 +77,9 @@ def lib():
         L.orc_vbd_bending.argtypes = [ctypes.c_int, _f64p, _f64p] + [ctypes.c_double] * 5 + [_f64p, _f64p]
         L.orc_vbd_hinge_angle.argtypes = [_f64p]
         L.orc_vbd_hinge_angle.restype = ctypes.c_double
-        L.orc_set_preconditioner.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+        L.orc_set_preconditioner.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.orc_add_static_plane.argtypes = [vp, _f32p, ctypes.c_float]
+        L.orc_coarse_system.argtypes = [vp, ctypes.c_void_p]
         L.orc_add_static_box.argtypes = [vp, _f32p, _f32p, _f32p, _f32p, _f32p]
         L.orc_clear_static_shapes.argtypes = [vp]
         L.orc_set_static_contact.argtypes = [vp] + [ctypes.c_float] * 4
@@ -238,11 +239,23 @@ class OracleCloth:
         _check(self._L.orc_contact_spmv(self._h, _p(x, _f64p), _p(y, _f64p)))
         return y
 
-    def set_preconditioner(self, degree=0, ratio=30.0, block_rows=512, coarse=False):
+    def set_preconditioner(self, degree=0, ratio=30.0, block_rows=512, coarse=False, coarse_rows=0):
         """0: block-Jacobi (the reference's); odd degree: the product's
         block-local Chebyshev preconditioner on blocks of block_rows rows;
-        coarse: plus the coarse level of one translation per block."""
-        _check(self._L.orc_set_preconditioner(self._h, int(degree), float(ratio), int(block_rows), int(bool(coarse))))
+        coarse: plus the coarse level of one translation per coarse block
+        (True or "translation"), or of the translation and the linear fields
+        along the block's principal axes ("linear"); coarse blocks of
+        coarse_rows rows (0: block_rows)."""
+        c = {False: 0, True: 1, "translation": 1, "linear": 2}[coarse]
+        _check(self._L.orc_set_preconditioner(self._h, int(degree), float(ratio), int(block_rows), c,
+                                              int(coarse_rows)))
+
+    def coarse_system(self):
+        """A_c of the last solve with the coarse level (dense, float64)."""
+        m = self._L.orc_coarse_system(self._h, None)
+        out = np.zeros((m, m), np.float64)
+        self._L.orc_coarse_system(self._h, out.ctypes.data_as(ctypes.c_void_p))
+        return out
 
     def add_static_plane(self, n, d):
         n = np.ascontiguousarray(n, np.float32).reshape(3)

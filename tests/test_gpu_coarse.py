@@ -1,8 +1,10 @@
-"""The two-level preconditioner (CTA-local Chebyshev plus a coarse level of
-one rigid translation per CTA block): converged solutions as the FP64
-oracle's block-Jacobi PCG, iteration counts as the oracle's restatement of
-the same two-level operator, the warm starts, its fallback to the local
-level where the coarse level does not apply, and bitwise repeatability."""
+"""The two-level preconditioner (CTA-local Chebyshev plus a coarse level:
+the translation and linear fields of 4-CTA blocks, or the translation of
+every CTA block on small grids): converged solutions as the FP64 oracle's
+block-Jacobi PCG, iteration counts as the oracle's restatement of the same
+two-level operator, the warm starts, ragged blocks, its fallback to the
+local level where the coarse level does not apply, and bitwise
+repeatability."""
 import numpy as np
 import pytest
 
@@ -11,6 +13,14 @@ from chysx.runner import GpuCloth
 from test_gpu_precond import oracle_sim
 
 pytestmark = pytest.mark.gpu
+
+
+def oracle_coarse(c, used, block_rows):
+    """The oracle's coarse space matching the GPU's (in_use 2 or 3)."""
+    if used == 3:
+        c.set_preconditioner(7, 30.0, block_rows, coarse="linear", coarse_rows=4 * block_rows)
+    else:
+        c.set_preconditioner(7, 30.0, block_rows, coarse=True)
 
 
 def gpu(sc, kind, degree=7, order=0, **kw):
@@ -28,7 +38,7 @@ def test_coarse_solution_and_iterations(side):
     g = gpu(sc, "chebyshev_coarse", max_iter=20000, rel_tol=1e-7)
     g.step()
     kind, deg, _, used = g.sim.preconditioner()
-    assert (kind, deg, used) == ("chebyshev_coarse", 7, 2)
+    assert (kind, deg, used) == ("chebyshev_coarse", 7, 3)  # 8 and 32 CTAs: linear fields on 4-CTA blocks
     block_rows = g.sim.solver_info()[2]
     o = oracle_sim(sc, 1e-11)
     o.step(sc["dt"])
@@ -36,7 +46,7 @@ def test_coarse_solution_and_iterations(side):
     # the same two-level operator on the CPU (FP32 port, same blocks, same
     # state): counts within 15% (summation orders differ)
     c = oracle_sim(sc, 1e-7, fp64=False, degree=7, block_rows=block_rows)
-    c.set_preconditioner(7, 30.0, block_rows, coarse=True)
+    oracle_coarse(c, used, block_rows)
     c.set_state(*[a.astype(np.float32) for a in (g.positions(), g.velocities())], g.inv_mass.cpu().numpy())
     g.step()
     c.step(sc["dt"])
@@ -55,16 +65,19 @@ def test_coarse_level_cuts_iterations_on_compact_blocks():
         a.step()
         b.step()
         assert a.stats()[2] == capi.SOLVE_CONVERGED and b.stats()[2] == capi.SOLVE_CONVERGED
-    assert a.sim.preconditioner()[3] == 2
+    assert a.sim.preconditioner()[3] == 3
     assert a.sim.solver_info()[2] == 512  # 16 slices of 32 rows per CTA
     assert a.stats()[0] < 0.8 * b.stats()[0]
     np.testing.assert_allclose(a.positions(), b.positions(), atol=2e-5)
 
 
 @pytest.mark.parametrize("warm", ["zero", "previous", "previous_scaled"])
-def test_coarse_trajectories_with_ragged_blocks(warm):
-    """48 x 48 particles: 4.5 blocks of 512 rows (the last one ragged)."""
-    sc = scenes.config_small(side=48, steps=6)
+@pytest.mark.parametrize("side,used", [(48, 2), (80, 3)])
+def test_coarse_trajectories_with_ragged_blocks(warm, side, used):
+    """48 x 48 particles: 4.5 CTA blocks of 512 rows, the translation of
+    each; 80 x 80: 12.5 CTA blocks, linear fields on 4-CTA blocks, the last
+    coarse block one ragged CTA."""
+    sc = scenes.config_small(side=side, steps=6)
     a = gpu(sc, "chebyshev_coarse", max_iter=20000, rel_tol=1e-7, warm_start=warm)
     b = gpu(sc, "block_jacobi", max_iter=20000, rel_tol=1e-7, warm_start=warm)
     o = oracle_sim(sc, 1e-11)
@@ -73,7 +86,7 @@ def test_coarse_trajectories_with_ragged_blocks(warm):
         b.step()
         o.step(sc["dt"])
         assert a.stats()[2] == capi.SOLVE_CONVERGED
-    assert a.sim.preconditioner()[3] == 2
+    assert a.sim.preconditioner()[3] == used
     ref = o.state()[0]
     assert np.abs(a.positions() - ref).max() <= max(3.0 * np.abs(b.positions() - ref).max(), 2e-5)
 
