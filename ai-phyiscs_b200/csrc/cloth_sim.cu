@@ -1310,8 +1310,9 @@ private:
             build_plan(topo_.inst_slice, grid, plan_);
             plan_coarse();
             pers_smem_ = (size_t)W * kSlotW * sizeof(double) + (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
-            if (coarse_on_)  // the coarse block's rows of A_c^-1
-                pers_smem_ += (size_t)9 * coarse_nq_ * coarse_nq_ * coarse_nb_ * sizeof(float);
+            if (coarse_on_)  // the coarse block's rows of A_c^-1, the staged coarse values of a phase
+                pers_smem_ += ((size_t)9 * coarse_nq_ * coarse_nq_ * coarse_nb_ + 3 * coarse_nq_ * (size_t)plan_.grid) *
+                                  sizeof(float) + 16;
             // static + dynamic above 48 KB needs the opt-in
             ck(cudaFuncSetAttribute(persistent_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pers_smem_),
                "cudaFuncSetAttribute(resident smem)");

@@ -444,35 +444,39 @@ __device__ __forceinline__ void warp1_coarse_publish(const BatchPlan& bp, const 
     }
 }
 
+// The coarse values of every slot of `set` into stage[k * U + u] (floats),
+// by the warps 1.. of the CTA together (one float4 per thread for up to
+// 160 slots of 12 values on 15 warps).
+__device__ __forceinline__ void coarse_stage(const BatchPlan& bp, int set, int U, int tid, int nthreads, float* stage) {
+    if (U % 4 == 0) {
+        const int per = U / 4, total = bp.n_slots * per;
+        for (int x = tid; x < total; x += nthreads)
+            reinterpret_cast<float4*>(stage)[x] =
+                __ldcg(reinterpret_cast<const float4*>(coarse_slot(bp, set, x / per)) + x % per);
+    } else {
+        const int total = bp.n_slots * U;
+        for (int x = tid; x < total; x += nthreads) stage[x] = __ldcg(coarse_slot(bp, set, x / U) + x % U);
+    }
+}
+
 // Rows [r0, r0 + 4) (those below U) of this CTA's block of A_c^-1 v, v the
-// coarse values of `set`, with the block's rows of A_c^-1 in `ainv`
-// ([U][m]); lane 0 writes them to out[r0..].  A coarse block's value is the
-// sum of its CTAs' slots and the product is linear, so lane l takes the
-// slots l, l + 32, ... directly (each against its block's columns).
+// staged coarse values; lane 0 writes them to out[r0..].  A coarse block's
+// value is the sum of its CTAs' slots and the product is linear, so lane l
+// takes the slots l, l + 32, ... directly (each against its block's
+// columns of the rows of A_c^-1 in `ainv`, [U][m]).
 template <int U>
-__device__ __forceinline__ void warp_coarse_rows(const BatchPlan& bp, int set, const float* ainv, int r0, float* out) {
+__device__ __forceinline__ void warp_coarse_rows(const BatchPlan& bp, const float* stage, const float* ainv, int r0,
+                                                 float* out) {
     const int lane = threadIdx.x & 31, m = bp.cg.m, G = bp.cg.g;
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
     for (int k = lane; k < bp.n_slots; k += 32) {
-        const float* sl = coarse_slot(bp, set, k);
-        float v[U];
-        if (U % 4 == 0) {
-#pragma unroll
-            for (int u = 0; u < U; u += 4) {
-                const float4 q = __ldcg(reinterpret_cast<const float4*>(sl + u));
-                v[u] = q.x; v[u + 1] = q.y; v[u + 2] = q.z; v[u + 3] = q.w;
-            }
-        } else {
-#pragma unroll
-            for (int u = 0; u < U; ++u) v[u] = __ldcg(sl + u);
-        }
-        const int C = k / G;
+        const float* v = stage + k * U;
+        const float* a = ainv + (k / G) * U;
 #pragma unroll
         for (int rr = 0; rr < 4; ++rr) {
             if (r0 + rr >= U) break;
-            const float* a = ainv + (size_t)(r0 + rr) * m + C * U;
 #pragma unroll
-            for (int u = 0; u < U; ++u) acc[rr] = fmaf(a[u], v[u], acc[rr]);
+            for (int u = 0; u < U; ++u) acc[rr] = fmaf(a[(size_t)(r0 + rr) * m + u], v[u], acc[rr]);
         }
     }
 #pragma unroll
@@ -485,9 +489,13 @@ __device__ __forceinline__ void warp_coarse_rows(const BatchPlan& bp, int set, c
 }
 
 __device__ __forceinline__ void named_barrier_w01() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
-// warp 0 and the coarse warps 1..nw: warp 0 passes it after the grid barrier
+// the whole CTA: warp 0 passes it after the grid barrier
 __device__ __forceinline__ void named_barrier_coarse(int nthreads) {
     asm volatile("bar.sync 2, %0;" ::"r"(nthreads) : "memory");
+}
+// warps 1.. alone: the staged values are complete
+__device__ __forceinline__ void named_barrier_stage(int nthreads) {
+    asm volatile("bar.sync 3, %0;" ::"r"(nthreads) : "memory");
 }
 
 // This row's share of a coarse vector c ([U]): c_0 + sum_q w_q c_q per component.
@@ -783,10 +791,11 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
 // the NR scalars (spart entries 0..NR-1), warp 1 the coarse values (floats
 // from the per-slice coarse partials), both before warp 0 arrives (named
 // barrier of warps 0 and 1: warp 0's release then covers warp 1's stores);
-// warp 0 waits on the grid barrier and then releases the coarse warps
-// 1..c_nw through a second named barrier (its acquire orders their slot
-// reads), reads the scalar totals while they form the rows of this CTA's
-// block of A_c^-1 v into OUT[0..U).
+// warp 0 waits on the grid barrier and then releases the other warps
+// through a second named barrier (its acquire orders their slot reads); it
+// reads the scalar totals while warps 1.. stage every slot's coarse values
+// in shared memory (one float4 per thread) and warps 1..c_nw form 4 rows
+// each of this CTA's block of A_c^-1 v into OUT[0..U).
 #define CHYSX_COARSE_PHASE(NR, OUT, exit_test, STEP)                                                 \
     do {                                                                                             \
         if (warp == 0) {                                                                             \
@@ -796,19 +805,23 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
             if (lane == 0) w0ok = barrier_arrive_wait(bp.bar, target);                               \
             w0ok = __shfl_sync(0xffffffffu, w0ok, 0);                                                \
             if (lane == 0 && !w0ok) s_flag = 1;                                                      \
-            named_barrier_coarse(32 * (1 + c_nw));                                                   \
+            named_barrier_coarse(32 * W);                                                            \
             if (w0ok) warp0_read_totals<NR, kPollMax>(bp, li, nloc, slot_set(ph), STEP);             \
             if (lane == 0 && (exit_test) && w0ok)                                                    \
                 s_exit = *(volatile unsigned*)&bp.bar->ndone >= (unsigned)bp.n_inst;                 \
-        } else if (warp <= c_nw) {                                                                   \
+        } else {                                                                                     \
             if (warp == 1) {                                                                         \
                 warp1_coarse_publish(bp, s_cpart, s1 - s0, li[0].own_slot, slot_set(ph));            \
                 named_barrier_w01();                                                                 \
             }                                                                                        \
-            named_barrier_coarse(32 * (1 + c_nw));                                                   \
+            named_barrier_coarse(32 * W);                                                            \
             if (!*(volatile int*)&s_flag) {                                                          \
-                if (c_U == 12) warp_coarse_rows<12>(bp, slot_set(ph), c_ainv, 4 * (warp - 1), OUT);  \
-                else warp_coarse_rows<3>(bp, slot_set(ph), c_ainv, 4 * (warp - 1), OUT);             \
+                coarse_stage(bp, slot_set(ph), c_U, threadIdx.x - 32, 32 * (W - 1), c_stage);        \
+                named_barrier_stage(32 * (W - 1));                                                   \
+                if (warp <= c_nw) {                                                                  \
+                    if (c_U == 12) warp_coarse_rows<12>(bp, c_stage, c_ainv, 4 * (warp - 1), OUT);   \
+                    else warp_coarse_rows<3>(bp, c_stage, c_ainv, 4 * (warp - 1), OUT);              \
+                }                                                                                    \
             }                                                                                        \
         }                                                                                            \
         ++ph;                                                                                        \
@@ -1048,7 +1061,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     __shared__ double s_bsum[PC ? W : 1];
     __shared__ float s_cheb[4];
     // coarse level: this block of A_c^-1 R^T (A p) and of A_c^-1 R^T r
-    __shared__ float s_cw[12], s_cu[12];
+    __shared__ float s_cw[12], s_cu[12];  // this block of A_c^-1 R^T (Ap) / A_c^-1 R^T r
     __shared__ float s_cpart[PC == 2 ? W * kCoarsePartW : 1];  // per-slice coarse partials
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
@@ -1192,6 +1205,9 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     const int c_nq = coarse ? bp.cg.nq : 1, c_U = 3 * c_nq;
     const int c_nw = (c_U + 3) / 4;  // coarse warps (rows of 4)
     float* c_ainv = reinterpret_cast<float*>(li + bp.max_inst_per_cta);
+    // staged coarse values of a phase ([slots][U]), behind c_ainv (16-byte aligned)
+    float* c_stage = reinterpret_cast<float*>(
+        (reinterpret_cast<uintptr_t>(c_ainv + (coarse ? c_U * bp.cg.m : 0)) + 15) & ~static_cast<uintptr_t>(15));
     float4 c_w = make_float4(0.f, 0.f, 0.f, 0.f);
     if (coarse) {
         const int m = bp.cg.m;
