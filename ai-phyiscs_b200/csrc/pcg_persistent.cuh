@@ -459,33 +459,25 @@ __device__ __forceinline__ void coarse_stage(const BatchPlan& bp, int set, int U
     }
 }
 
-// Rows [r0, r0 + 4) (those below U) of this CTA's block of A_c^-1 v, v the
-// staged coarse values; lane 0 writes them to out[r0..].  A coarse block's
-// value is the sum of its CTAs' slots and the product is linear, so lane l
-// takes the slots l, l + 32, ... directly (each against its block's
-// columns of the rows of A_c^-1 in `ainv`, [U][m]).
+// Row r of this CTA's block of A_c^-1 v, v the staged coarse values; lane 0
+// writes it to out[r].  A coarse block's value is the sum of its CTAs' slots
+// and the product is linear, so lane l takes the slots l, l + 32, ...
+// directly (each against its block's columns of row r of A_c^-1, [U][m]).
 template <int U>
-__device__ __forceinline__ void warp_coarse_rows(const BatchPlan& bp, const float* stage, const float* ainv, int r0,
-                                                 float* out) {
-    const int lane = threadIdx.x & 31, m = bp.cg.m, G = bp.cg.g;
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+__device__ __forceinline__ void warp_coarse_row(const BatchPlan& bp, const float* stage, const float* ainv, int r,
+                                                float* out) {
+    const int lane = threadIdx.x & 31, G = bp.cg.g;
+    const float* arow = ainv + (size_t)r * bp.cg.m;
+    float acc = 0.f;
     for (int k = lane; k < bp.n_slots; k += 32) {
         const float* v = stage + k * U;
-        const float* a = ainv + (k / G) * U;
+        const float* a = arow + (k / G) * U;
 #pragma unroll
-        for (int rr = 0; rr < 4; ++rr) {
-            if (r0 + rr >= U) break;
-#pragma unroll
-            for (int u = 0; u < U; ++u) acc[rr] = fmaf(a[(size_t)(r0 + rr) * m + u], v[u], acc[rr]);
-        }
+        for (int u = 0; u < U; ++u) acc = fmaf(a[u], v[u], acc);
     }
 #pragma unroll
-    for (int rr = 0; rr < 4; ++rr) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], o);
-    }
-    if (lane == 0)
-        for (int rr = 0; rr < 4 && r0 + rr < U; ++rr) out[r0 + rr] = acc[rr];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) out[r] = acc;
 }
 
 __device__ __forceinline__ void named_barrier_w01() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
@@ -794,8 +786,8 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
 // warp 0 waits on the grid barrier and then releases the other warps
 // through a second named barrier (its acquire orders their slot reads); it
 // reads the scalar totals while warps 1.. stage every slot's coarse values
-// in shared memory (one float4 per thread) and warps 1..c_nw form 4 rows
-// each of this CTA's block of A_c^-1 v into OUT[0..U).
+// in shared memory (one float4 per thread) and then form one row each of
+// this CTA's block of A_c^-1 v into OUT[0..U).
 #define CHYSX_COARSE_PHASE(NR, OUT, exit_test, STEP)                                                 \
     do {                                                                                             \
         if (warp == 0) {                                                                             \
@@ -818,9 +810,9 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
             if (!*(volatile int*)&s_flag) {                                                          \
                 coarse_stage(bp, slot_set(ph), c_U, threadIdx.x - 32, 32 * (W - 1), c_stage);        \
                 named_barrier_stage(32 * (W - 1));                                                   \
-                if (warp <= c_nw) {                                                                  \
-                    if (c_U == 12) warp_coarse_rows<12>(bp, c_stage, c_ainv, 4 * (warp - 1), OUT);   \
-                    else warp_coarse_rows<3>(bp, c_stage, c_ainv, 4 * (warp - 1), OUT);              \
+                for (int r = warp - 1; r < c_U; r += W - 1) {                                        \
+                    if (c_U == 12) warp_coarse_row<12>(bp, c_stage, c_ainv, r, OUT);                 \
+                    else warp_coarse_row<3>(bp, c_stage, c_ainv, r, OUT);                            \
                 }                                                                                    \
             }                                                                                        \
         }                                                                                            \
@@ -1203,7 +1195,6 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     constexpr bool kCoarse = PC == 2;
     const bool coarse = kCoarse && bp.cg.on;
     const int c_nq = coarse ? bp.cg.nq : 1, c_U = 3 * c_nq;
-    const int c_nw = (c_U + 3) / 4;  // coarse warps (rows of 4)
     float* c_ainv = reinterpret_cast<float*>(li + bp.max_inst_per_cta);
     // staged coarse values of a phase ([slots][U]), behind c_ainv (16-byte aligned)
     float* c_stage = reinterpret_cast<float*>(
