@@ -1407,7 +1407,8 @@ private:
         for (int B = 0; B < nb; ++B)
             for (int C : lists[B]) bwb = std::max(bwb, std::abs(perm[B] - perm[C]));
         const int bw = std::min(m - 1, (bwb + 1) * U - 1);
-        const size_t direct_smem = ((size_t)m * (bw + 1) + m + (size_t)rpc * m) * sizeof(float);
+        const size_t direct_smem = ((size_t)m * (bw + 1) + 2 * (size_t)m + (size_t)rpc * m) * sizeof(float) +
+                                   (size_t)bw * (bw + 1) * sizeof(unsigned short);
         if (direct_smem > kCoarseDirectSmemMax) return false;
         std::vector<int> nbr((size_t)nb * mn, -1), cnt(nb), self(nb);
         for (int B = 0; B < nb; ++B) {
@@ -1463,7 +1464,8 @@ private:
     static constexpr size_t kCoarseDirectSmemMax = 220 * 1024;
     size_t coarse_direct_smem() const {
         const size_t m = 3 * (size_t)coarse_nq_ * coarse_nb_;
-        return (m * (coarse_bw_ + 1) + m + (size_t)coarse_rpc_ * m) * sizeof(float);
+        return (m * (coarse_bw_ + 1) + 2 * m + (size_t)coarse_rpc_ * m) * sizeof(float) +
+               (size_t)coarse_bw_ * (coarse_bw_ + 1) * sizeof(unsigned short);
     }
     CoarseArgs coarse_args() const {
         CoarseArgs c{};

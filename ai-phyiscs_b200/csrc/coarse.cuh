@@ -205,8 +205,9 @@ __global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, CoarseA
 // dropped axis) have a zero diagonal and get identity rows; a non-positive
 // pivot leaves zero rows (the coarse level then adds nothing this step).
 // The factorisation is the same in every CTA (same operations, same order),
-// so all CTAs agree bitwise.  Dynamic shared memory: (m (bw + 1) + m + rpc m)
-// floats.
+// so all CTAs agree bitwise.  Dynamic shared memory: (m (bw + 1) + 2 m +
+// rpc m) floats and bw (bw + 1) / 2 pairs of the trailing update's
+// (row, column) offsets.
 __global__ void __launch_bounds__(kCoarseThreads) coarse_direct_kernel(CoarseArgs ca) {
     extern __shared__ float cd_mem[];
     __shared__ int s_fail;
@@ -214,7 +215,17 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_direct_kernel(CoarseArg
     const int t = threadIdx.x, nt = blockDim.x;
     float* L = cd_mem;                   // [m][W1]: L[i W1 + k] = entry (i, i - k)
     float* dsc = L + (size_t)m * W1;     // [m] 1 / sqrt(A_ii)
-    float* y = dsc + m;                  // [rpc][m] right-hand sides / solutions, band order
+    float* dinv = dsc + m;               // [m] 1 / L_ii
+    float* y = dinv + m;                 // [rpc][m] right-hand sides / solutions, band order
+    // the trailing update's pairs (a, b), b <= a < bw, in row-major order:
+    // the first c (c + 1) / 2 are those of a column with c rows below it
+    unsigned short* pab = reinterpret_cast<unsigned short*>(y + (size_t)rpc * m);
+    for (int a = t; a < bw; a += nt)
+        for (int b = 0; b <= a; ++b) {
+            const int x = a * (a + 1) / 2 + b;
+            pab[2 * x] = (unsigned short)a;
+            pab[2 * x + 1] = (unsigned short)b;
+        }
     if (t == 0) s_fail = 0;
     for (int x = t; x < m * W1; x += nt) L[x] = 0.0;
     __syncthreads();
@@ -255,19 +266,17 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_direct_kernel(CoarseArg
         }
         for (int q = t; q < cnt; q += nt) L[(size_t)(j + 1 + q) * W1 + (1 + q)] *= inv;
         __syncthreads();
-        // warp w takes rows i = j+1+a for a = w, w + nwarps, ...; its lanes
-        // the columns k = j+1+b, b <= a
-        for (int a = t >> 5; a < cnt; a += nt >> 5) {
-            const int i = j + 1 + a;
-            float* Li = L + (size_t)i * W1;
-            const float lij = Li[i - j];
-            for (int b = t & 31; b <= a; b += 32) {
-                const int k = j + 1 + b;
-                Li[i - k] -= lij * L[(size_t)k * W1 + (k - j)];
-            }
+        // every (row i = j+1+a, column k = j+1+b, b <= a) pair independently
+        const int np = cnt * (cnt + 1) / 2;
+#pragma unroll 4
+        for (int x = t; x < np; x += nt) {
+            const int a = pab[2 * x], b = pab[2 * x + 1];
+            const int i = j + 1 + a, k = j + 1 + b;
+            L[(size_t)i * W1 + (a - b)] -= L[(size_t)i * W1 + (a + 1)] * L[(size_t)k * W1 + (b + 1)];
         }
         __syncthreads();
     }
+    for (int i = t; i < m; i += nt) dinv[i] = 1.0f / L[(size_t)i * W1];
     // this CTA's rows r = blockIdx.x rpc + s: right-hand side D^-1/2 e_r in band order
     const int r0 = blockIdx.x * rpc;
     for (int x = t; x < rpc * m; x += nt) y[x] = 0.0f;
@@ -285,7 +294,8 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_direct_kernel(CoarseArg
         float* ys = y + (size_t)sr * m;
         for (int j = 0; j < m; ++j) {
             const int cnt = min(m - 1, j + bw) - j;
-            const float yj = ys[j] / L[(size_t)j * W1];
+            const float yj = ys[j] * dinv[j];
+#pragma unroll 4
             for (int q = 1 + ln; q <= cnt; q += 32) ys[j + q] -= L[(size_t)(j + q) * W1 + q] * yj;
             __syncwarp();
             if (ln == 0) ys[j] = yj;
@@ -293,7 +303,8 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_direct_kernel(CoarseArg
         }
         for (int i = m - 1; i >= 0; --i) {
             const int lo = max(0, i - bw);
-            const float yi = ys[i] / L[(size_t)i * W1];
+            const float yi = ys[i] * dinv[i];
+#pragma unroll 4
             for (int k = lo + ln; k < i; k += 32) ys[k] -= L[(size_t)i * W1 + (i - k)] * yi;
             __syncwarp();
             if (ln == 0) ys[i] = yi;
