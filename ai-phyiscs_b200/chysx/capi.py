@@ -84,6 +84,7 @@ SIGNATURES = {
     "chysx_cloth_num_particles": (ctypes.c_int, [H, ip]),
     "chysx_cloth_num_off_diag_blocks": (ctypes.c_int, [H, ip]),
     "chysx_cloth_debug_dump": (ctypes.c_int, [H, f32p, i32p, i32p, f32p, f32p, f32p]),
+    "chysx_cloth_debug_coarse": (ctypes.c_int, [H, i32p, f32p, f32p, ctypes.c_int]),
     "chysx_cloth_set_network": (ctypes.c_int, [H, f32p, ctypes.c_int]),
     "chysx_cloth_set_feature_output": (ctypes.c_int, [H, u, u]),
     "chysx_cloth_guess_kept": (ctypes.c_int, [H, ip]),
@@ -426,6 +427,21 @@ class Cloth:
         check(self._L.chysx_cloth_debug_dump(self.h, _p(diag, f32p), _p(rp, i32p), _p(col, i32p),
                                              _p(vals, f32p), _p(rhs, f32p), _p(dx, f32p)))
         return diag, rp, col[:nnz], vals[:nnz], rhs, dx
+
+    def debug_coarse(self):
+        """(info dict, A_c dense, rows of A_c^-1) of the last step's coarse
+        level, or (info, None, None) when it is off."""
+        info = np.zeros(6, np.int32)
+        check(self._L.chysx_cloth_debug_coarse(self.h, _p(info, i32p), None, None, 0))
+        keys = ("on", "blocks", "ctas_per_block", "fields", "m", "band")
+        d = dict(zip(keys, (int(v) for v in info)))
+        if not d["on"]:
+            return d, None, None
+        m = d["m"]
+        ac = np.zeros((m, m), np.float32)
+        ainv = np.zeros((m, m), np.float32)
+        check(self._L.chysx_cloth_debug_coarse(self.h, _p(info, i32p), _p(ac, f32p), _p(ainv, f32p), m * m))
+        return d, ac, ainv
 
 
 class Vbd:

@@ -932,6 +932,42 @@ public:
     int num_particles() const { return n_; }
     int num_off_diag_blocks() const { return (int)topo_.nnz(); }
 
+    // The coarse level of the last step (test support): info = {on, coarse
+    // blocks, CTAs per block, fields per block, unknowns m, band half-width};
+    // with ac / ainv non-null (m x m floats each, cap >= m * m) A_c dense and
+    // the rows of A_c^-1 the CTAs computed, unknown B U + 3 q + c.
+    void debug_coarse(int32_t* info, float* ac, float* ainv, int cap) {
+        ck(cudaDeviceSynchronize(), "debug_coarse sync");
+        const int U = 3 * coarse_nq_, m = coarse_on_ ? U * coarse_nb_ : 0;
+        if (info) {
+            info[0] = coarse_on_ ? 1 : 0;
+            info[1] = coarse_nb_;
+            info[2] = coarse_g_;
+            info[3] = coarse_nq_;
+            info[4] = m;
+            info[5] = coarse_bw_;
+        }
+        if (!coarse_on_ || (!ac && !ainv)) return;
+        if (cap < m * m) throw std::invalid_argument("debug_coarse: cap below m * m");
+        if (ac) {
+            const int mn = coarse_mn_;
+            std::vector<float> blocks((size_t)coarse_nb_ * mn * U * U);
+            std::vector<int> nbr((size_t)coarse_nb_ * mn), cnt(coarse_nb_);
+            ck(cudaMemcpy(blocks.data(), d_cac_.get(), blocks.size() * sizeof(float), cudaMemcpyDeviceToHost), "copy A_c");
+            ck(cudaMemcpy(nbr.data(), d_cnbr_.get(), nbr.size() * sizeof(int), cudaMemcpyDeviceToHost), "copy lists");
+            ck(cudaMemcpy(cnt.data(), d_ccnt_.get(), cnt.size() * sizeof(int), cudaMemcpyDeviceToHost), "copy counts");
+            std::fill(ac, ac + (size_t)m * m, 0.0f);
+            for (int B = 0; B < coarse_nb_; ++B)
+                for (int k = 0; k < cnt[B]; ++k) {
+                    const int C = nbr[(size_t)B * mn + k];
+                    const float* b = blocks.data() + ((size_t)B * mn + k) * U * U;
+                    for (int r = 0; r < U; ++r)
+                        for (int c = 0; c < U; ++c) ac[(size_t)(B * U + r) * m + C * U + c] = b[r * U + c];
+                }
+        }
+        if (ainv)
+            ck(cudaMemcpy(ainv, d_cainv_.get(), (size_t)m * m * sizeof(float), cudaMemcpyDeviceToHost), "copy A_c^-1");
+    }
     void debug_dump(float* diag, int32_t* rp, int32_t* col, float* vals, float* rhs, float* dx) {
         const int n = topo_.n_ext;
         if (n == 0 || topo_.n == 0) return;
@@ -2259,6 +2295,11 @@ int chysx_cloth_debug_dump(chysx_cloth* h, float* diag, int32_t* rp, int32_t* co
                            float* dx) {
     CHYSX_H(h);
     return guard([&] { h->sim.debug_dump(diag, rp, col, vals, rhs, dx); });
+}
+
+int chysx_cloth_debug_coarse(chysx_cloth* h, int32_t* info, float* ac, float* ainv, int cap) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.debug_coarse(info, ac, ainv, cap); });
 }
 
 int chysx_cloth_set_network(chysx_cloth* h, const float* params, int n_params) {

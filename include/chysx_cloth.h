@@ -254,6 +254,13 @@ int chysx_cloth_num_off_diag_blocks(const chysx_cloth* h, int* out);
  * buffers, synchronises the device. */
 int chysx_cloth_debug_dump(chysx_cloth* h, float* diag, int32_t* row_offsets,
                            int32_t* col_indices, float* values, float* rhs, float* dx);
+/* The two-level preconditioner's coarse level of the last step (test
+ * support, no counterpart in the reference): info[6] = {in use, coarse
+ * blocks, CTAs per block, fields per block, unknowns m, band half-width};
+ * with ac / ainv non-null (host, m * m floats each, cap >= m * m) the coarse
+ * matrix A_c dense and the rows of A_c^-1 the CTAs computed, unknown
+ * index block * 3 * fields + 3 * field + component.  Synchronises. */
+int chysx_cloth_debug_coarse(chysx_cloth* h, int32_t* info, float* ac, float* ainv, int cap);
 
 /* Learned warm start (no counterpart in the reference).  A per-vertex
  * network (20 1-ring features -> 3 x 64 GELU -> dv, BF16 on tensor cores)
