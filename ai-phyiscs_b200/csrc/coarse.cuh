@@ -253,26 +253,53 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_direct_kernel(CoarseArg
         if (i - k >= 0) L[x] *= dsc[i] * dsc[i - k];
     }
     __syncthreads();
-    // band Cholesky, column j: L_jj = sqrt(a_jj); L_ij /= L_jj; trailing update
-    for (int j = 0; j < m; ++j) {
-        const int hi = min(m - 1, j + bw), cnt = hi - j;
-        const float ajj = L[(size_t)j * W1];
-        const bool piv = ajj > 1e-30f;
-        const float ljj = piv ? sqrtf(ajj) : 1.0f, inv = 1.0f / ljj;
-        __syncthreads();  // every thread has read a_jj
-        if (t == 0) {
-            L[(size_t)j * W1] = ljj;
-            if (!piv) s_fail = 1;
+    // blocked band Cholesky: panels of kPanel columns factored by warp 0
+    // (column by column, the panel's later columns updated as it goes),
+    // then one rank-kPanel update of the trailing band by the whole CTA
+    constexpr int kPanel = 4;
+    const int warp = t >> 5, lane = t & 31;
+    for (int j0 = 0; j0 < m; j0 += kPanel) {
+        const int pw = min(kPanel, m - j0);
+        if (warp == 0) {
+            for (int j = j0; j < j0 + pw; ++j) {
+                const float ajj = L[(size_t)j * W1];
+                const bool piv = ajj > 1e-30f;
+                const float ljj = piv ? sqrtf(ajj) : 1.0f, inv = 1.0f / ljj;
+                __syncwarp();
+                if (lane == 0) {
+                    L[(size_t)j * W1] = ljj;
+                    if (!piv) s_fail = 1;
+                }
+                const int hi = min(m - 1, j + bw);
+                for (int i = j + 1 + lane; i <= hi; i += 32) L[(size_t)i * W1 + (i - j)] *= inv;
+                __syncwarp();
+                for (int k = j + 1; k < j0 + pw; ++k) {
+                    const float lkj = L[(size_t)k * W1 + (k - j)];
+                    for (int i = k + lane; i <= hi; i += 32) L[(size_t)i * W1 + (i - k)] -= L[(size_t)i * W1 + (i - j)] * lkj;
+                }
+                __syncwarp();
+            }
         }
-        for (int q = t; q < cnt; q += nt) L[(size_t)(j + 1 + q) * W1 + (1 + q)] *= inv;
         __syncthreads();
-        // every (row i = j+1+a, column k = j+1+b, b <= a) pair independently
-        const int np = cnt * (cnt + 1) / 2;
-#pragma unroll 4
-        for (int x = t; x < np; x += nt) {
-            const int a = pab[2 * x], b = pab[2 * x + 1];
-            const int i = j + 1 + a, k = j + 1 + b;
-            L[(size_t)i * W1 + (a - b)] -= L[(size_t)i * W1 + (a + 1)] * L[(size_t)k * W1 + (b + 1)];
+        // rows i = base + a, columns k = base + b (b <= a): L_ik -= sum over the
+        // panel's columns p within the band of row i of L_ip L_kp
+        const int base = j0 + pw, hi = min(m - 1, j0 + pw - 1 + bw), cnt = hi - base + 1;
+        if (cnt > 0) {
+            const int np = cnt * (cnt + 1) / 2;
+#pragma unroll 2
+            for (int x = t; x < np; x += nt) {
+                const int a = pab[2 * x], b = pab[2 * x + 1];
+                const int i = base + a, k = base + b;
+                const float* Li = L + (size_t)i * W1;
+                const float* Lk = L + (size_t)k * W1;
+                float sum = 0.0f;
+#pragma unroll
+                for (int p = 0; p < kPanel; ++p) {
+                    const int col = j0 + p;
+                    if (p < pw && i - col <= bw) sum = fmaf(Li[i - col], Lk[k - col], sum);
+                }
+                L[(size_t)i * W1 + (a - b)] -= sum;
+            }
         }
         __syncthreads();
     }

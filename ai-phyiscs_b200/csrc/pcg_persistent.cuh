@@ -1052,6 +1052,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     __shared__ float4 s_d[PC ? 2 : 1][PC ? W * 32 : 1];
     __shared__ double s_bsum[PC ? W : 1];
     __shared__ float s_cheb[4];
+    __shared__ float2 s_ccoef[PC ? 64 : 1];  // per term m of the polynomial: (rn rho, rn 2/delta)
     // coarse level: this block of A_c^-1 R^T (A p) and of A_c^-1 R^T r
     __shared__ float s_cw[12], s_cu[12];  // this block of A_c^-1 R^T (Ap) / A_c^-1 R^T r
     __shared__ float s_cpart[PC == 2 ? W * kCoarsePartW : 1];  // per-slice coarse partials
@@ -1136,8 +1137,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         return tot;
     };
     auto precond = [&](float3 rin) {
-        const float th_inv = s_cheb[1], sg = s_cheb[2], two_de = s_cheb[3];
-        float rho = 1.0f / sg;
+        const float th_inv = s_cheb[1];
         float3 res = rin;
         float3 d = mul(Mi, res) * th_inv;
         float3 zc = d;
@@ -1146,12 +1146,10 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
             buf[threadIdx.x] = f4(d);
             __syncthreads();
             res = res - local_spmv(buf, d);
-            const float rn = 1.0f / (2.0f * sg - rho);
             const float3 mr = mul(Mi, res);
-            const float c0 = rn * rho, c1 = rn * two_de;
-            d = f3(fmaf(c0, d.x, c1 * mr.x), fmaf(c0, d.y, c1 * mr.y), fmaf(c0, d.z, c1 * mr.z));
+            const float2 c = s_ccoef[PC ? m : 0];  // (rn rho, rn 2/delta) of term m
+            d = f3(fmaf(c.x, d.x, c.y * mr.x), fmaf(c.x, d.y, c.y * mr.y), fmaf(c.x, d.z, c.y * mr.z));
             zc = zc + d;
-            rho = rn;
         }
         return zc;
     };
@@ -1184,6 +1182,15 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
             s_cheb[1] = (float)(1.0 / theta);
             s_cheb[2] = (float)(theta / delta);
             s_cheb[3] = (float)(2.0 / delta);
+            // the three-term recurrence's coefficients of every term, in the
+            // FP32 arithmetic the terms used to form them in
+            const float sg = s_cheb[2], two_de = s_cheb[3];
+            float rho = 1.0f / sg;
+            for (int m = 1; m < cfg.pc_degree && m < 64; ++m) {
+                const float rn = 1.0f / (2.0f * sg - rho);
+                s_ccoef[PC ? m : 0] = make_float2(rn * rho, rn * two_de);
+                rho = rn;
+            }
         }
         __syncthreads();
     }
