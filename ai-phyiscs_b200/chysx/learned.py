@@ -223,7 +223,8 @@ def train(feats, targs, epochs=30, batch_rows=8192, lr=2e-3, seed=0, log=print):
 def evaluate(params, seeds=(100, 101), steps=20, side=256,
              modes=("zero", "previous", "previous_scaled", "learned"), log=print):
     """PCG iterations per step to rel-res 1e-6 on held-out seeds of the
-    256x256 configuration for each start mode (zero guess = the judge)."""
+    256x256 configuration for each start mode (the zero guess is the
+    reference point)."""
     from .runner import GpuCloth
 
     rows = []
