@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_direct_kernel(CoarseArg
                 const int hi = min(m - 1, j + bw);
                 for (int i = j + 1 + lane; i <= hi; i += 32) L[(size_t)i * W1 + (i - j)] *= inv;
                 __syncwarp();
-                for (int k = j + 1; k < j0 + pw; ++k) {
+                for (int k = j + 1; k < j0 + pw && k - j <= bw; ++k) {  // L_kj = 0 beyond the band
                     const float lkj = L[(size_t)k * W1 + (k - j)];
                     for (int i = k + lane; i <= hi; i += 32) L[(size_t)i * W1 + (i - k)] -= L[(size_t)i * W1 + (i - j)] * lkj;
                 }
