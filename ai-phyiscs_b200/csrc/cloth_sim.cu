@@ -1483,6 +1483,9 @@ private:
         coarse_nq_ = nq;
         coarse_rpc_ = rpc;
         coarse_on_ = true;
+        ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_assemble_kernel),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_assemble_smem()),
+           "cudaFuncSetAttribute(coarse assemble smem)");
         ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_direct_kernel),
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_direct_smem()),
            "cudaFuncSetAttribute(coarse direct smem)");
@@ -1494,6 +1497,10 @@ private:
             return;
         if (plan_.grid >= 8 && plan_coarse_with(4, 4)) return;
         plan_coarse_with(1, 1);
+    }
+    // per-lane partial sums of the coarse assembly: [nq][9][max_nbr][32] floats
+    size_t coarse_assemble_smem() const {
+        return (size_t)coarse_nq_ * 9 * coarse_mn_ * 32 * sizeof(float);
     }
     // dynamic shared memory of the coarse direct kernel: the FP32 band of
     // A_c, the scaling and the right-hand sides (below the 227 KB of a CTA)
@@ -1723,8 +1730,9 @@ private:
             void* a1[] = {&t, &cg};
             cudaKernelNodeParams p{};
             p.func = reinterpret_cast<void*>(&coarse_assemble_kernel);
-            p.gridDim = dim3(coarse_nb_, coarse_nq_ * coarse_nq_);
+            p.gridDim = dim3(coarse_nb_, coarse_nq_);
             p.blockDim = dim3(288);
+            p.sharedMemBytes = (unsigned)coarse_assemble_smem();
             p.kernelParams = a1;
             cudaGraphNode_t n1, n2;
             ck(cudaGraphAddKernelNode(&n1, graph_, &prev, 1, &p), "add coarse assemble node");

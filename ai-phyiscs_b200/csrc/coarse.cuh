@@ -147,53 +147,66 @@ __global__ void __launch_bounds__(256) coarse_fields_kernel(StepArgs a, CoarseAr
     }
 }
 
-// A_c block row of coarse block B for the field pair (q, q') =
-// (blockIdx.y / nq, blockIdx.y % nq): 9 warps (one per component of the
-// 3x3 block), lane l takes the rows l of every slice of the block; per-lane
-// sums of w_iq w_jq' A_ij in shared memory by column block, then each
-// (column block, component) sum over lanes in lane order (double).
+// A_c block row of coarse block B for the row field qa = blockIdx.y and
+// every column field: 9 warps (one per component of the 3x3 block), lane l
+// takes the rows l of every slice of the block; per-lane sums of
+// w_iqa w_jqb A_ij by column block and qb in dynamic shared memory
+// ([nq][9][max_nbr][32] floats), then each (qb, column block, component) sum
+// over lanes in lane order (double).  A row's entries are gathered once for
+// all qb.
 __global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, CoarseArgs ca) {
-    __shared__ float acc[9][kCoarseMaxNbr][32];
-    const int B = blockIdx.x, qa = blockIdx.y / ca.nq, qb = blockIdx.y % ca.nq;
-    const int U = 3 * ca.nq;
+    extern __shared__ float acc_s[];
+    const int B = blockIdx.x, qa = blockIdx.y, nq = ca.nq, mn = ca.max_nbr;
+    const int U = 3 * nq;
     const int c = threadIdx.x >> 5, l = threadIdx.x & 31;
-    for (int k = 0; k < ca.max_nbr; ++k) acc[c][k][l] = 0.0f;
+    auto acc = [&](int qb, int k) -> float& { return acc_s[(((size_t)qb * 9 + c) * mn + k) * 32 + l]; };
+    for (int qb = 0; qb < nq; ++qb)
+        for (int k = 0; k < mn; ++k) acc(qb, k) = 0.0f;
     const int pl = sym_plane(c);
     const int self = ca.self_idx[B];
     const int s0 = ca.cb_row0[B] >> 5, s1 = ca.cb_row0[B + 1] >> 5;
+    auto weights = [&](int i) {  // (w_i0, w_i1, w_i2, w_i3) = (1, s_1, s_2, s_3)
+        if (nq == 1) return make_float4(1.f, 0.f, 0.f, 0.f);
+        const float4 w = ca.w[i];
+        return make_float4(1.f, w.x, w.y, w.z);
+    };
+    auto pick = [](float4 w, int q) { return q == 0 ? w.x : (q == 1 ? w.y : (q == 2 ? w.z : w.w)); };
     for (int s = s0; s < s1; ++s) {
         const int i = s * 32 + l;
         if (i >= t.n) break;
-        const float wi = coarse_weight(ca, i, qa);
-        acc[c][self][l] += wi * coarse_weight(ca, i, qb) * t.diag[(size_t)s * 192 + pl * 32 + l];
+        const float4 wi4 = weights(i);
+        const float wi = pick(wi4, qa);
+        const float dv = wi * t.diag[(size_t)s * 192 + pl * 32 + l];
+        for (int qb = 0; qb < nq; ++qb) acc(qb, self) += dv * pick(wi4, qb);
         const int so = t.slice_off[s];
         const int w = (t.slice_off[s + 1] - so) >> 5;
         // the row's entries 8 at a time: every load of a batch in flight
         for (int k0 = 0; k0 < w; k0 += 8) {
-            int cj[8], nb8[8];
-            float wv[8], vv[8];
+            int nb8[8];
+            float vv[8];
+            float4 wv[8];
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 const bool in = k0 + k < w;
                 const int e = so + (k0 + k) * 32 + l;
-                cj[k] = in ? t.col[e] : i;
+                const int cj = in ? t.col[e] : i;
                 nb8[k] = in ? ca.ell_nbr[e] : 0;
-                vv[k] = in ? t.val[(size_t)so * 6 + (size_t)(k0 + k) * 192 + pl * 32 + l] : 0.0f;
+                vv[k] = in ? wi * t.val[(size_t)so * 6 + (size_t)(k0 + k) * 192 + pl * 32 + l] : 0.0f;
+                wv[k] = weights(cj);
             }
 #pragma unroll
-            for (int k = 0; k < 8; ++k) wv[k] = coarse_weight(ca, cj[k], qb);
-#pragma unroll
             for (int k = 0; k < 8; ++k)
-                if (k0 + k < w) acc[c][nb8[k]][l] += wi * wv[k] * vv[k];
+                if (k0 + k < w)
+                    for (int qb = 0; qb < nq; ++qb) acc(qb, nb8[k]) += vv[k] * pick(wv[k], qb);
         }
     }
     __syncthreads();
-    for (int x = threadIdx.x; x < ca.max_nbr * 9; x += blockDim.x) {
-        const int k = x / 9, cc = x % 9;
+    for (int x = threadIdx.x; x < nq * mn * 9; x += blockDim.x) {
+        const int qb = x / (mn * 9), rem = x % (mn * 9), k = rem / 9, cc = rem % 9;
         double sum = 0.0;
-        for (int y = 0; y < 32; ++y) sum += acc[cc][k][y];
+        for (int y = 0; y < 32; ++y) sum += acc_s[(((size_t)qb * 9 + cc) * mn + k) * 32 + y];
         const int r = cc / 3, col = cc % 3;
-        ca.ac[(((size_t)B * ca.max_nbr + k) * U + qa * 3 + r) * U + qb * 3 + col] = (float)sum;
+        ca.ac[(((size_t)B * mn + k) * U + qa * 3 + r) * U + qb * 3 + col] = (float)sum;
     }
 }
 
