@@ -118,13 +118,18 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        # live before the timed region starts: wait (at most 2 s) for the first sample
+        t0 = time.time()
+        while not self.rows and time.time() - t0 < 2.0 and self.proc.poll() is None:
+            time.sleep(0.005)
+        self.rows.clear()
 
     def _read(self):
         for line in self.proc.stdout:
