@@ -6,9 +6,8 @@ namespace chysx_b200 {
 
 constexpr int kCoarseMaxBlocks = 160;  // CTAs of a two-level plan (one warp's slot pass)
 constexpr int kCoarseMaxNbr = 16;      // coarse blocks one block's rows touch, itself included
-constexpr int kCoarseThreads = 512;    // >= coarse unknowns: one thread per unknown
+constexpr int kCoarseThreads = 512;    // threads of the coarse direct solve; also the bound on the coarse unknowns
 constexpr int kCoarseMaxRhs = 4;       // rows of A_c^-1 one CTA computes
-constexpr int kCoarseMaxFields = 4;    // fields per coarse block: 1, or 1 + 3 linear
 
 // Coarse space: coarse block B is the rows of CTAs [B G, (B + 1) G) of the
 // plan; its fields are the translation (weight 1) and, with nq = 4, the
