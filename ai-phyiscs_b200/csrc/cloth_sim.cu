@@ -1324,7 +1324,7 @@ private:
         bp.bar = d_bar_.get();
         bp.n_slots = plan_.inst_slot.empty() ? 0 : plan_.inst_slot.back();
         bp.fslots = sync_mode_ ? d_fslots_.get() : nullptr;
-        bp.cg = coarse_args();
+        bp.cg = coarse_on_ ? d_cargs_.get() : nullptr;
         return bp;
     }
 
@@ -1483,6 +1483,8 @@ private:
         coarse_nq_ = nq;
         coarse_rpc_ = rpc;
         coarse_on_ = true;
+        const CoarseArgs cargs = coarse_args();
+        d_cargs_.upload(&cargs, 1);
         ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_assemble_kernel),
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_assemble_smem()),
            "cudaFuncSetAttribute(coarse assemble smem)");
@@ -2026,6 +2028,7 @@ private:
     DevBuf<int> d_slice_cb_, d_cb_row0_, d_cnbr_, d_ccnt_, d_cself_, d_cperm_;
     DevBuf<unsigned char> d_ell_nbr_;
     DevBuf<float4> d_cw_;
+    DevBuf<CoarseArgs> d_cargs_;  // the coarse arguments the PCG kernel reads (BatchPlan holds the pointer)
     DevBuf<float> d_cac_, d_cainv_;
     float pc_ratio_ = 0.0f;
     DevBuf<ZP> d_zp_;

@@ -63,7 +63,10 @@ struct BatchPlan {
     GridBarrier* bar;
     int n_slots = 0;                      // inst_slot[n_inst]
     unsigned long long* fslots = nullptr; // [3][n_slots][kSlotW] rotating polled slots (SYNC = 1)
-    CoarseArgs cg{};                      // coarse level of the two-level preconditioner (cg.on = 0: none)
+    // coarse level of the two-level preconditioner, in device memory (null:
+    // none); a pointer keeps this kernel parameter small (carrying the whole
+    // struct here slowed the streamed kernel by ~17 us per iteration)
+    const CoarseArgs* cg = nullptr;
 };
 
 // (z, p) of one row for the register-resident kernel's neighbour exchange
@@ -436,7 +439,7 @@ __device__ __forceinline__ float* coarse_slot(const BatchPlan& bp, int set, int 
 // partials, in slice order) into its slot of `set` (warp 1).
 __device__ __forceinline__ void warp1_coarse_publish(const BatchPlan& bp, const float* cpart, int nsl, int own_slot,
                                                      int set) {
-    const int lane = threadIdx.x & 31, U = 3 * bp.cg.nq;
+    const int lane = threadIdx.x & 31, U = 3 * bp.cg->nq;
     if (lane < U) {
         float acc = 0.0f;
         for (int w = 0; w < nsl; ++w) acc += cpart[w * kCoarsePartW + lane];
@@ -466,8 +469,8 @@ __device__ __forceinline__ void coarse_stage(const BatchPlan& bp, int set, int U
 template <int U>
 __device__ __forceinline__ void warp_coarse_row(const BatchPlan& bp, const float* stage, const float* ainv, int r,
                                                 float* out) {
-    const int lane = threadIdx.x & 31, G = bp.cg.g;
-    const float* arow = ainv + (size_t)r * bp.cg.m;
+    const int lane = threadIdx.x & 31, G = bp.cg->g;
+    const float* arow = ainv + (size_t)r * bp.cg->m;
     float acc = 0.f;
     for (int k = lane; k < bp.n_slots; k += 32) {
         const float* v = stage + k * U;
@@ -1195,23 +1198,23 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         __syncthreads();
     }
 
-    // ---- coarse level (PC = 2 with bp.cg.on): this CTA's coarse block
+    // ---- coarse level (PC = 2 with bp.cg->on): this CTA's coarse block
     // Bc = blockIdx.x / G; its U rows of A_c^-1 in dynamic shared memory
     // behind the LocalInst records; every row's field weights in a register
     // quad.  Warps 1..3 form this block of A_c^-1 R^T v during the phases.
     constexpr bool kCoarse = PC == 2;
-    const bool coarse = kCoarse && bp.cg.on;
-    const int c_nq = coarse ? bp.cg.nq : 1, c_U = 3 * c_nq;
+    const bool coarse = kCoarse && bp.cg != nullptr && bp.cg->on;
+    const int c_nq = coarse ? bp.cg->nq : 1, c_U = 3 * c_nq;
     float* c_ainv = reinterpret_cast<float*>(li + bp.max_inst_per_cta);
     // staged coarse values of a phase ([slots][U]), behind c_ainv (16-byte aligned)
     float* c_stage = reinterpret_cast<float*>(
-        (reinterpret_cast<uintptr_t>(c_ainv + (coarse ? c_U * bp.cg.m : 0)) + 15) & ~static_cast<uintptr_t>(15));
+        (reinterpret_cast<uintptr_t>(c_ainv + (coarse ? c_U * bp.cg->m : 0)) + 15) & ~static_cast<uintptr_t>(15));
     float4 c_w = make_float4(0.f, 0.f, 0.f, 0.f);
     if (coarse) {
-        const int m = bp.cg.m;
-        const float* src = bp.cg.ainv + (size_t)(blockIdx.x / bp.cg.g) * c_U * m;
+        const int m = bp.cg->m;
+        const float* src = bp.cg->ainv + (size_t)(blockIdx.x / bp.cg->g) * c_U * m;
         for (int q = threadIdx.x; q < c_U * m; q += blockDim.x) c_ainv[q] = src[q];
-        if (c_nq == 4 && row) c_w = bp.cg.w[i];
+        if (c_nq == 4 && row) c_w = bp.cg->w[i];
         __syncthreads();
     }
 
