@@ -639,9 +639,9 @@ def main():
     ap.add_argument("--pc-degree", type=int, default=7)
     ap.add_argument("--row-order", default="spatial", choices=["caller", "spatial"],
                     help="rows in the caller's particle order, or in spatially compact blocks")
-    ap.add_argument("--pc-ratio", type=float, default=30.0,
-                    help="Chebyshev interval [lambda / ratio, lambda] of the local level (30: fewest iterations "
-                         "over the 30 default steps of grid256 with the coarse level; 60 wins over the first 12)")
+    ap.add_argument("--pc-ratio", type=float, default=60.0,
+                    help="Chebyshev interval [lambda / ratio, lambda] of the local level (60: fewest iterations "
+                         "on grid256 with the coarse level)")
     ap.add_argument("--net", default=os.path.join(ROOT, "ai-phyiscs_b200", "chysx", "data", "warmstart.npz"))
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--reference-gpu", type=int, default=1, help="also time the compiled reference module")
