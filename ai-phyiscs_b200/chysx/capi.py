@@ -81,6 +81,8 @@ SIGNATURES = {
     "chysx_cloth_step": (ctypes.c_int, [H, ctypes.c_float, u]),
     "chysx_cloth_step_into": (ctypes.c_int, [H, ctypes.c_float, u, u, u, u, u]),
     "chysx_cloth_last_stats": (ctypes.c_int, [H, ip, dp, ip]),
+    "chysx_cloth_set_true_residual": (ctypes.c_int, [H, ctypes.c_int]),
+    "chysx_cloth_true_residual": (ctypes.c_int, [H, ctypes.c_int, dp, dp]),
     "chysx_cloth_num_particles": (ctypes.c_int, [H, ip]),
     "chysx_cloth_num_off_diag_blocks": (ctypes.c_int, [H, ip]),
     "chysx_cloth_debug_dump": (ctypes.c_int, [H, f32p, i32p, i32p, f32p, f32p, f32p]),
@@ -96,6 +98,7 @@ SIGNATURES = {
     "chysx_mlp_train_step": (ctypes.c_int, [u, u, u, u, u, u, ctypes.c_int, ctypes.c_float, ctypes.c_int, u,
                                             ctypes.c_uint64, dp, u]),
     "chysx_mlp_gradients_noalloc": (ctypes.c_int, [u, u, u, ctypes.c_int, u, dp, u]),
+    "chysx_mlp_noalloc_max_rows": (ctypes.c_int, []),
     "chysx_cloth_set_instances": (ctypes.c_int, [H, i32p, ctypes.c_int]),
     "chysx_cloth_num_instances": (ctypes.c_int, [H, ip]),
     "chysx_cloth_instance_stats": (ctypes.c_int, [H, ctypes.c_int, ip, dp, ip]),
@@ -412,6 +415,17 @@ class Cloth:
         rr = ctypes.c_double()
         check(self._L.chysx_cloth_last_stats(self.h, ctypes.byref(it), ctypes.byref(rr), ctypes.byref(st)))
         return it.value, rr.value, st.value
+
+    def set_true_residual(self, on=True):
+        check(self._L.chysx_cloth_set_true_residual(self.h, int(bool(on))))
+
+    def true_residual(self):
+        """(per-instance ||b - A dx|| / ||b|| of the last step, the largest)."""
+        n = self.num_instances()
+        rel = np.zeros(n, np.float64)
+        worst = ctypes.c_double()
+        check(self._L.chysx_cloth_true_residual(self.h, n, rel.ctypes.data_as(dp), ctypes.byref(worst)))
+        return rel, worst.value
 
     def debug_dump(self):
         n, nnz = ctypes.c_int(), ctypes.c_int()

@@ -877,6 +877,66 @@ __global__ void finalize_kernel(StepArgs a, Vecs v, const SolveState* st) {
 }
 
 // ---------------------------------------------------------------------------
+// True residual of the returned iterate (the reference's optional
+// compute_true_residual pass, src/solver/pcg_solver.cu:595-641): r = b -
+// (A + C) x recomputed from the stored FP32 system and the final x, with the
+// products accumulated in FP64, so that the recurrence residual the solver
+// stopped on can be checked against what the iterate actually satisfies.
+// One warp per 32-row slice; out[slice] = (sum r.r, sum b.b) of its rows,
+// summed by a fixed shuffle tree (deterministic).
+// ---------------------------------------------------------------------------
+__global__ void true_residual_kernel(DevTopo t, Vecs v, double2* __restrict__ out) {
+    const int s = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (s >= t.n_slices) return;
+    const int i = s * 32 + lane;
+    double rr = 0.0, bb = 0.0;
+    if (i < t.n) {
+        const int so = t.slice_off[s];
+        const int w = (t.slice_off[s + 1] - so) >> 5;
+        const float* d = t.diag + (size_t)s * 6 * 32 + lane;
+        const float3 xi = xyz(v.x[i]);
+        // D x in FP64: symmetric planes xx, xy, xz, yy, yz, zz
+        const double dxx = d[0], dxy = d[32], dxz = d[64], dyy = d[96], dyz = d[128], dzz = d[160];
+        double ax = dxx * xi.x + dxy * xi.y + dxz * xi.z;
+        double ay = dxy * xi.x + dyy * xi.y + dyz * xi.z;
+        double az = dxz * xi.x + dyz * xi.y + dzz * xi.z;
+        const int ow = off_width(t);
+        const float* vb = t.val + (size_t)so * ow + lane;
+        for (int k = 0; k < w; ++k) {
+            const int j = t.col[so + k * 32 + lane];
+            const float3 xj = xyz(v.x[j]);
+            const float* q = vb + (size_t)k * ow * 32;
+            if (t.nsym) {
+                ax += (double)q[0] * xj.x + (double)q[32] * xj.y + (double)q[64] * xj.z;
+                ay += (double)q[96] * xj.x + (double)q[128] * xj.y + (double)q[160] * xj.z;
+                az += (double)q[192] * xj.x + (double)q[224] * xj.y + (double)q[256] * xj.z;
+            } else {
+                const double qxx = q[0], qxy = q[32], qxz = q[64], qyy = q[96], qyz = q[128], qzz = q[160];
+                ax += qxx * xj.x + qxy * xj.y + qxz * xj.z;
+                ay += qxy * xj.x + qyy * xj.y + qyz * xj.z;
+                az += qxz * xj.x + qyz * xj.y + qzz * xj.z;
+            }
+        }
+        if (t.co.active) {
+            const float3 c = contact_spmv_row(t.co, i, [&](int j) { return xyz(v.x[j]); });
+            ax += c.x;
+            ay += c.y;
+            az += c.z;
+        }
+        const float3 b = xyz(v.b[i]);
+        const double rx = b.x - ax, ry = b.y - ay, rz = b.z - az;
+        rr = rx * rx + ry * ry + rz * rz;
+        bb = (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        rr += __shfl_down_sync(0xffffffffu, rr, o);
+        bb += __shfl_down_sync(0xffffffffu, bb, o);
+    }
+    if (lane == 0) out[s] = make_double2(rr, bb);
+}
+
+// ---------------------------------------------------------------------------
 // Setup kernels
 // ---------------------------------------------------------------------------
 

@@ -99,6 +99,30 @@ constexpr size_t kWsAlign = 256;
 size_t align_up(size_t v) { return (v + kWsAlign - 1) / kWsAlign * kWsAlign; }
 int train_blocks(int rows) { return std::max(1, std::min(1184, (rows + 16 * kTrainWarps - 1) / (16 * kTrainWarps))); }
 
+// The training kernel's dynamic shared memory is above the 48 KB default, and
+// that limit is a per-device function attribute: set it once on every device
+// that launches the kernel (the current device), under a lock.
+constexpr int kMaxDevices = 64;
+std::mutex g_dev_mu;
+bool g_train_smem_set[kMaxDevices] = {};
+
+int current_device() {
+    int dev = -1;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= kMaxDevices) throw std::out_of_range("device ordinal beyond 63");
+    return dev;
+}
+
+void ensure_train_smem() {
+    const int dev = current_device();
+    std::lock_guard<std::mutex> lock(g_dev_mu);
+    if (!g_train_smem_set[dev]) {
+        ck(cudaFuncSetAttribute(mlp_train_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem),
+           "cudaFuncSetAttribute(mlp_train_tile_kernel)");
+        g_train_smem_set[dev] = true;
+    }
+}
+
 size_t mlp_workspace_bytes(int rows) {
     const size_t r = (size_t)std::max(rows, 1);
     return align_up(sizeof(MlpPacked)) + 8 * align_up(r * 64 * sizeof(__nv_bfloat16)) +
@@ -132,12 +156,7 @@ void mlp_gradients(uintptr_t params, uintptr_t features, uintptr_t targets, int 
     bufs.out = reinterpret_cast<float*>(dv_out);
     mlp_pack_kernel<<<8, 256, 0, stream>>>(reinterpret_cast<const float*>(params), packed);
     ck(cudaGetLastError(), "mlp_pack_kernel launch");
-    static bool smem_set = false;
-    if (!smem_set) {
-        ck(cudaFuncSetAttribute(mlp_train_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem),
-           "cudaFuncSetAttribute(mlp_train_tile_kernel)");
-        smem_set = true;
-    }
+    ensure_train_smem();
     const int blocks = train_blocks(rows);
     // with no targets the kernel still runs the backward on zero residuals;
     // a zero-target buffer is not needed because target rows are only read
@@ -199,19 +218,14 @@ static_assert(kNoAllocPartials <= 1184 * kTrainWarps, "partials follow train_blo
 
 static __device__ __align__(256) unsigned char g_mlp_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mu;
-unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+unsigned char* g_noalloc_ptr[kMaxDevices] = {};
 
 // Set-up, once per device and with that device current: the device address
 // of this device's copy of the scratch array.  The lookup may load the
 // module, so the first call on a device belongs before any stream capture.
 unsigned char* noalloc_scratch() {
-    int dev = -1;
-    ck(cudaGetDevice(&dev), "cudaGetDevice");
-    if (dev < 0 || dev >= kNoAllocMaxDevices)
-        throw std::out_of_range("chysx_mlp_gradients_noalloc: device ordinal beyond 63");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    const int dev = current_device();
+    std::lock_guard<std::mutex> lock(g_dev_mu);
     if (!g_noalloc_ptr[dev]) {
         if (mlp_workspace_bytes(kNoAllocMaxRows) > kNoAllocScratchBytes)
             throw std::logic_error("chysx_mlp_gradients_noalloc: static scratch smaller than the workspace layout");
@@ -665,6 +679,38 @@ public:
         if (iters) *iters = it;
         if (relres) *relres = (bb > 0.0) ? std::sqrt(std::max(rr, 0.0) / bb) : 0.0;
         if (status) *status = st;
+    }
+
+    // True residual of the returned iterate (pcg_solver.h:78,191): when on,
+    // every step also computes ||b - (A + C) dx|| / ||b|| from the stored
+    // system and the final dx, per instance.
+    void set_true_residual(int on) {
+        if ((on != 0) != true_res_) graph_dirty_ = true;
+        true_res_ = on != 0;
+    }
+    // per-instance true relative residuals of the last step (n = instances);
+    // worst = the largest.  Needs set_true_residual(1) before that step.
+    void true_residual(int n, double* rel, double* worst) {
+        if (!true_res_ || !stepped_ || d_tres_.size() == 0)
+            throw std::runtime_error("true_residual: enable it with set_true_residual(1) before the step");
+        const int ni = (int)topo_.inst_slice.size() - 1;
+        if (rel && n != ni) throw std::invalid_argument("true_residual: wrong instance count");
+        ck(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(last_stream_)), "cudaStreamSynchronize");
+        std::vector<double2> h(d_tres_.size());
+        ck(cudaMemcpy(h.data(), d_tres_.get(), h.size() * sizeof(double2), cudaMemcpyDeviceToHost),
+           "cudaMemcpy(true residual)");
+        double w = 0.0;
+        for (int b = 0; b < ni; ++b) {
+            double rr = 0.0, bb = 0.0;
+            for (int sl = topo_.inst_slice[b]; sl < topo_.inst_slice[b + 1]; ++sl) {
+                rr += h[sl].x;
+                bb += h[sl].y;
+            }
+            const double q = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+            if (rel) rel[b] = q;
+            w = std::max(w, q);
+        }
+        if (worst) *worst = w;
     }
 
     // Learned warm start: loads a network (flat FP32 parameters, MlpOffsets).
@@ -1687,6 +1733,23 @@ private:
         return last;
     }
 
+    // Optional true-residual pass after the solve (off by default, as the
+    // reference's compute_true_residual): a branch beside the finalize node,
+    // reading b and the final x only.
+    void add_true_residual_node(cudaGraphNode_t dep, DevTopo& t, Vecs& v) {
+        if (!true_res_) return;
+        d_tres_.resize((size_t)std::max(1, topo_.n_slices));
+        double2* out = d_tres_.get();
+        void* a[] = {&t, &v, &out};
+        cudaKernelNodeParams p{};
+        p.func = reinterpret_cast<void*>(&true_residual_kernel);
+        p.gridDim = dim3(std::max(1, grid_for(std::max(1, topo_.n_slices) * 32, 256)));
+        p.blockDim = dim3(256);
+        p.kernelParams = a;
+        cudaGraphNode_t node;
+        ck(cudaGraphAddKernelNode(&node, graph_, &dep, 1, &p), "add true-residual node");
+    }
+
     void build_graph_persistent() {
         destroy_graph();
         ck(cudaFuncSetAttribute(assemble_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)asm_smem_),
@@ -1787,6 +1850,7 @@ private:
             ck(cudaGraphAddKernelNode(&fin_node_, graph_, &t2, 1, &p), "add finalize node");
             timing_node(3, fin_node_);
         }
+        add_true_residual_node(pcg_node_, t, v);
         ck(cudaGraphInstantiate(&exec_, graph_, 0), "cudaGraphInstantiate(step)");
         graph_path_ = kPathPersistent;
         graph_dirty_ = false;
@@ -1876,6 +1940,7 @@ private:
             ck(cudaGraphAddKernelNode(&fin_node_, graph_, &t2, 1, &p), "add finalize node");
             timing_node(3, fin_node_);
         }
+        add_true_residual_node(loop, t, v);
         ck(cudaGraphInstantiate(&exec_, graph_, 0), "cudaGraphInstantiate(step)");
         graph_path_ = kPathLoop;
         graph_dirty_ = false;
@@ -2034,6 +2099,8 @@ private:
     DevBuf<ZP> d_zp_;
     bool timing_ = false;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool true_res_ = false;
+    DevBuf<double2> d_tres_;  // per-slice (r.r, b.b) of the true-residual pass
     // static shapes: planes (n, d), boxes (center, half extents, axes)
     std::vector<float> planes_, boxes_;
     float sc_thickness_ = 0.0f, sc_k_ = 0.0f, sc_mu_ = 0.0f, sc_eps_ = 1.0e-4f;
@@ -2292,6 +2359,14 @@ int chysx_cloth_last_stats(chysx_cloth* h, int* iters, double* relres, int* stat
     CHYSX_H(h);
     return guard([&] { h->sim.last_stats(iters, relres, status); });
 }
+int chysx_cloth_set_true_residual(chysx_cloth* h, int on) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.set_true_residual(on); });
+}
+int chysx_cloth_true_residual(chysx_cloth* h, int n_instances, double* relres, double* worst) {
+    CHYSX_H(h);
+    return guard([&] { h->sim.true_residual(n_instances, relres, worst); });
+}
 int chysx_cloth_num_particles(const chysx_cloth* h, int* out) {
     CHYSX_H(h);
     if (out) *out = h->sim.num_particles();
@@ -2353,6 +2428,7 @@ int chysx_mlp_train_step(uintptr_t params, uintptr_t grad, uintptr_t m1, uintptr
         chysx_b200::mlp_adam(params, grad, m1, m2, lr, adam_step, stream);
     });
 }
+int chysx_mlp_noalloc_max_rows(void) { return CHYSX_MLP_NOALLOC_MAX_ROWS; }
 int chysx_mlp_gradients_noalloc(uintptr_t params, uintptr_t features, uintptr_t targets, int rows,
                                 uintptr_t grad, double* loss, uintptr_t stream) {
     return guard([&] { chysx_b200::mlp_gradients_noalloc(params, features, targets, rows, grad, loss, stream); });

@@ -344,6 +344,22 @@ PYBIND11_MODULE(_chysx_native, m) {
                  return py::make_tuple(it, rr, st);
              },
              "(iterations, relative residual ||r||/||b||, status) of the last step; synchronises.")
+        .def("set_true_residual",
+             [](PyClothSimulator& s, bool on) { check(chysx_cloth_set_true_residual(s.h(), on ? 1 : 0)); },
+             py::arg("on") = true,
+             "Also recompute ||b - A dx|| / ||b|| of the returned dx after every solve "
+             "(PCGParams::compute_true_residual).")
+        .def("last_true_residual",
+             [](PyClothSimulator& s) {
+                 int n = 0;
+                 check(chysx_cloth_num_instances(s.h(), &n));
+                 py::array_t<double> rel(n);
+                 double worst = 0.0;
+                 check(chysx_cloth_true_residual(s.h(), n, rel.mutable_data(), &worst));
+                 return py::make_tuple(rel, worst);
+             },
+             "(per-instance true relative residuals, the largest) of the last step; synchronises "
+             "(PCGSolver::host_last_true_relative_residual).")
         .def("num_particles",
              [](const PyClothSimulator& s) {
                  int n = 0;

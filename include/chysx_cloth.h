@@ -232,6 +232,19 @@ int chysx_cloth_step(chysx_cloth* h, float dt, uintptr_t stream);
  * PCGSolver::last_residual (src/solver/pcg_solver.cu:897-923). */
 int chysx_cloth_last_stats(chysx_cloth* h, int* iterations, double* rel_residual, int* status);
 
+/* The rel_residual above is the solver's recurrence residual.  With on != 0
+ * every later step also recomputes r = b - (A + C) dx from the stored system
+ * and the returned dx (FP64 accumulation) in a graph branch beside the
+ * update: PCGParams::compute_true_residual (src/solver/pcg_solver.h:78) and
+ * its pass (src/solver/pcg_solver.cu:595-641).  Off by default. */
+int chysx_cloth_set_true_residual(chysx_cloth* h, int on);
+/* ||b - (A + C) dx|| / ||b|| of the last step per instance (relres: n
+ * entries, n = chysx_cloth_num_instances, or NULL) and the largest (worst,
+ * or NULL); synchronises.  Replaces PCGSolver::host_last_true_relative_residual
+ * (src/solver/pcg_solver.h:191).  CHYSX_ERR_RUNTIME unless the last step ran
+ * with the pass on. */
+int chysx_cloth_true_residual(chysx_cloth* h, int n, double* relres, double* worst);
+
 /* Double-buffered step, the Newton bridge's stepping (SolverChysX, reference
  * README.md:113-130, which copies state_in to state_out and then steps
  * state_out in place): reads x_n, v_n from pos_in / vel_in and writes
@@ -298,8 +311,11 @@ int chysx_mlp_train_step(uintptr_t params, uintptr_t grad, uintptr_t m1, uintptr
                          uintptr_t targets, int rows, float lr, int adam_step, uintptr_t workspace,
                          uint64_t workspace_bytes, double* loss, uintptr_t stream);
 
-/* Largest `rows` accepted by chysx_mlp_gradients_noalloc. */
+/* Largest `rows` accepted by chysx_mlp_gradients_noalloc; the library's
+ * value is also returned by chysx_mlp_noalloc_max_rows(), for callers that
+ * bind the C ABI without this header. */
 #define CHYSX_MLP_NOALLOC_MAX_ROWS 4096
+int chysx_mlp_noalloc_max_rows(void);
 /* chysx_mlp_gradients without a workspace argument (no counterpart in the
  * reference, which has no training entry point at all).  Same kernels, same
  * results; the workspace is a fixed static device array inside this library

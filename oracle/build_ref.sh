@@ -1,7 +1,7 @@
 #!/usr/bin/env bash
 # TEST INFRASTRUCTURE ONLY: compile the reference ChysX cloth path from its
-# own sources (read in place under $CHYSX_REFERENCE, default /root/reference)
-# into oracle/_ref/, for parity runs on a B200.  Nothing here is shipped or
+# own sources (read in place from the directory given as the first argument,
+# or else $CHYSX_REFERENCE; no default) into oracle/_ref/, for parity runs on a B200.  Nothing here is shipped or
 # committed: oracle/_ref/ is git-ignored (it still travels with the tree to
 # the GPU box, where the reference sources are absent).
 #
@@ -20,7 +20,11 @@
 # against directly: nvcc -rdc for sm_100a, -include cstring (two sources miss
 # the header), device link, g++ for the binding.
 set -euo pipefail
-REF=${CHYSX_REFERENCE:-/root/reference}
+REF=${1:-${CHYSX_REFERENCE:-}}
+if [ -z "$REF" ]; then
+  echo "usage: build_ref.sh <reference checkout>  (or set CHYSX_REFERENCE)" >&2
+  exit 2
+fi
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT=$HERE/_ref
 NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}

@@ -159,15 +159,19 @@ def test_argument_errors_map_like_the_reference():
 
 
 def test_no_alloc_gradients_reject_sizes_before_any_device_work():
-    # CHYSX_MLP_NOALLOC_MAX_ROWS = 4096; checked before any CUDA call
+    # the limit comes from the library; sizes are checked before any CUDA call
     L = capi.lib()
-    for rows in (4097, 1 << 20, 0, -5):
+    limit = int(L.chysx_mlp_noalloc_max_rows())
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    header = open(os.path.join(root, "include", "chysx_cloth.h")).read()
+    assert limit == int(re.search(r"#define CHYSX_MLP_NOALLOC_MAX_ROWS (\d+)", header).group(1))
+    for rows in (limit + 1, 1 << 20, 0, -5):
         assert L.chysx_mlp_gradients_noalloc(16, 16, 16, rows, 16, None, 0) == capi.ERR_INVALID_ARGUMENT
-    assert "4096" in L.chysx_last_error().decode() or "positive" in L.chysx_last_error().decode()
-    assert L.chysx_mlp_gradients_noalloc(16, 16, 16, 4097, 16, None, 0) == capi.ERR_INVALID_ARGUMENT
-    assert "CHYSX_MLP_NOALLOC_MAX_ROWS" in L.chysx_last_error().decode()
+    assert L.chysx_mlp_gradients_noalloc(16, 16, 16, limit + 1, 16, None, 0) == capi.ERR_INVALID_ARGUMENT
+    msg = L.chysx_last_error().decode()
+    assert "CHYSX_MLP_NOALLOC_MAX_ROWS" in msg and str(limit) in msg
     # the static scratch is the workspace layout at the limit
-    assert L.chysx_mlp_workspace_bytes(4096) == 4243712
+    assert L.chysx_mlp_workspace_bytes(limit) == 4243712
 
 
 def test_material_round_trip():

@@ -14,7 +14,9 @@ from chysx import capi
 
 pytestmark = pytest.mark.gpu
 
-MAX_ROWS = 4096  # CHYSX_MLP_NOALLOC_MAX_ROWS
+# the library's own limit (CHYSX_MLP_NOALLOC_MAX_ROWS), so the boundary cases
+# follow the header if it changes
+MAX_ROWS = int(capi.lib().chysx_mlp_noalloc_max_rows())
 # Same kernels and the same summation order on both paths: the results are
 # expected to be identical; the bounds only leave room for FP32 re-association.
 TOL_GRAD_REL = 1e-6   # relative to max |gradient| per parameter block
@@ -89,6 +91,6 @@ def test_rows_beyond_the_limit_are_rejected_before_any_launch():
     rc = capi.lib().chysx_mlp_gradients_noalloc(p.data_ptr(), f.data_ptr(), t.data_ptr(), MAX_ROWS + 1,
                                                 grad.data_ptr(), ctypes.byref(loss), 0)
     assert rc == capi.ERR_INVALID_ARGUMENT
-    assert "4096" in capi.lib().chysx_last_error().decode()
+    assert str(MAX_ROWS) in capi.lib().chysx_last_error().decode()
     torch.cuda.synchronize()
     assert bool((grad == 7.0).all()) and loss.value == -1.0
