@@ -4,8 +4,11 @@
 //   caller's pos / vel / inv_mass / force : float3 AoS (12 B), borrowed
 //   b, r, z, x(=dx), Ap, p0, p1           : float4 per row (16-B vector loads,
 //                                           .w unused), rows padded to 32
-//   diag, minv                            : symmetric 3x3 blocks as 6 planes
-//                                           per 32-row slice (xx,xy,xz,yy,yz,zz)
+//   diag, dnl, minv                       : symmetric 3x3 blocks as 6 planes
+//                                           per 32-row slice (xx,xy,xz,yy,yz,zz):
+//                                           full diagonal, its non-elastic part
+//                                           (inertia, pins, contacts) and the
+//                                           Jacobi inverse
 //   col, val                              : sliced ELL (see topology.h); val
 //                                           holds 6 planes per entry column
 //                                           (9 with bending)
@@ -34,7 +37,8 @@ struct DevTopo {
     const int* __restrict__ slice_off;
     const int* __restrict__ col;
     float* val;
-    float* diag;
+    float* diag;  // full diagonal blocks (Jacobi inverse, debug dump)
+    float* dnl;   // non-elastic diagonal D': the operator is D'_i p_i + sum_j A_ij (p_j - p_i)
     float* minv;
     const int* __restrict__ tinc_off;
     const int* __restrict__ tinc;
@@ -54,19 +58,28 @@ struct DevTopo {
     ContactOp co;  // the contact operator's per-row lists (co.active = 0: none)
 };
 
+// Rest shape of a triangle, Dm^-1 row-major (Mat2f layout), kept in FP64:
+// the grid's triangles are all nearly the same shape, so FP32 rounding of
+// their rest data is correlated across the cloth and acts as a uniform
+// pre-strain whose smooth response (2.7e-4 m after one step of the 256 x 256
+// grid) would dominate the difference to the FP64 oracle.
+struct RestShape {
+    double m00, m01, m10, m11;
+};
+
 struct ElemData {
-    const int* __restrict__ tris;      // 3 per triangle
-    const float4* __restrict__ dminv;  // stretch: row-major 2x2 (Mat2f layout)
+    const int* __restrict__ tris;         // 3 per triangle
+    const RestShape* __restrict__ dminv;  // stretch
     const float* __restrict__ area;
     const float* __restrict__ ktri;
-    const float4* __restrict__ dminv_s;  // shear: the same with the material axes turned by pi/4
+    const RestShape* __restrict__ dminv_s;  // shear: the same with the material axes turned by pi/4
     const float* __restrict__ area_s;
     const float* __restrict__ ktri_s;
     const int* __restrict__ edges;     // 2 per edge
-    const float* __restrict__ rest;
+    const double* __restrict__ rest;   // rest lengths (FP64, like the rest shapes)
     const float* __restrict__ kedge;
     const int4* __restrict__ dih;         // bending dihedrals (v0, v1, v2, v3)
-    const float* __restrict__ rest_angle;
+    const double* __restrict__ rest_angle;
     float k_bend;
     int use_bending;
     float pin_k;
@@ -188,11 +201,6 @@ __device__ __forceinline__ float3 mul_off(const float* p, int nsym, float3 v) {
               p[192] * v.x + p[224] * v.y + p[256] * v.z);
 }
 
-}  // namespace chysx_b200
-
-#include "contact_kernels.cuh"
-
-namespace chysx_b200 {
 
 // ---------------------------------------------------------------------------
 // Single-pass deterministic grid reduction of NV doubles.  Each block writes
@@ -260,27 +268,80 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double* __restrict_
 __device__ __forceinline__ bool finite_d(double x) { return isfinite(x); }
 
 // ---------------------------------------------------------------------------
-// Element physics (FP32, same formulas as the reference kernels)
+// Element physics, evaluated in FP64 (same formulas as the reference kernels)
+//
+// The assembled system is stiff against its inertia: on the 256 x 256 grid a
+// vertex's elastic diagonal is ~2.6e4 N/m and its m/dt^2 ~5.5e-3 N/m, a
+// ratio of 2e-7, i.e. about three FP32 ulps.  FP32 element arithmetic (a few
+// ulps per block) therefore loses the inertia of the smooth modes.  Every
+// element quantity is formed in FP64 from the FP32 state and rounded once
+// when the row is written; together with the difference form of the
+// operator (assemble_kernel) and FP64 rest data (RestShape) this keeps the
+// FP32 system within rounding of the FP64 one.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ double3 d3(double x, double y, double z) { return make_double3(x, y, z); }
+__device__ __forceinline__ double3 d3(float3 v) { return make_double3(v.x, v.y, v.z); }
+__device__ __forceinline__ double3 operator+(double3 a, double3 b) { return d3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ double3 operator-(double3 a, double3 b) { return d3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ double3 operator*(double3 a, double s) { return d3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ double dot3(double3 a, double3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ double len3(double3 a) { return sqrt(dot3(a, a)); }
+__device__ __forceinline__ double3 cross3(double3 a, double3 b) {
+    return d3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double3 ld3d(const float* p, int i) { return d3(ld3(p, i)); }
+
+struct S6d {
+    double xx, xy, xz, yy, yz, zz;
+};
+__device__ __forceinline__ void axpy6(S6d& d, double s, const S6d& a) {
+    d.xx += s * a.xx; d.xy += s * a.xy; d.xz += s * a.xz;
+    d.yy += s * a.yy; d.yz += s * a.yz; d.zz += s * a.zz;
+}
+__device__ __forceinline__ void add6(S6d& d, const S6& a) {
+    d.xx += a.xx; d.xy += a.xy; d.xz += a.xz; d.yy += a.yy; d.yz += a.yz; d.zz += a.zz;
+}
+__device__ __forceinline__ S6 round6(const S6d& a) {
+    return S6{(float)a.xx, (float)a.xy, (float)a.xz, (float)a.yy, (float)a.yz, (float)a.zz};
+}
+// Adjugate inverse (no determinant guard), the symmetric specialisation of
+// math::inverse(Mat3f) (src/math/matrix.cuh:219-235), in FP64.
+__device__ __forceinline__ S6d inverse6(const S6d& m) {
+    const double a00 = m.yy * m.zz - m.yz * m.yz;
+    const double a01 = -m.xy * m.zz + m.xz * m.yz;
+    const double a02 = m.xy * m.yz - m.xz * m.yy;
+    const double a11 = m.xx * m.zz - m.xz * m.xz;
+    const double a12 = -m.xx * m.yz + m.xz * m.xy;
+    const double a22 = m.xx * m.yy - m.xy * m.xy;
+    const double det = m.xx * a00 + m.xy * a01 + m.xz * a02;
+    const double inv = 1.0 / det;
+    return S6d{a00 * inv, a01 * inv, a02 * inv, a11 * inv, a12 * inv, a22 * inv};
+}
+__device__ __forceinline__ double sel3(const double (&a)[3], int i) {
+    return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]);
+}
+__device__ __forceinline__ double3 sel4(const double3 (&a)[4], int i) {
+    return i == 0 ? a[0] : (i == 1 ? a[1] : (i == 2 ? a[2] : a[3]));
+}
 
 // Spring contribution to row `end` (0: row is edges[e].x, 1: row is .y).
 // Gradient: spring_constraint.cu:76-103; block: spring_constraint.cu:110-151.
 __device__ __forceinline__ void spring_row(const ElemData& el, const float* pos, int e, int end,
-                                           float3& g, S6& blk) {
+                                           double3& g, S6d& blk) {
     const int ia = el.edges[2 * e], ib = el.edges[2 * e + 1];
-    const float3 d = ld3(pos, ia) - ld3(pos, ib);
-    float l = len3(d);
-    if (l < 1.0e-6f) l = 1.0e-6f;
-    const float inv_l = 1.0f / l;
-    const float3 dh = d * inv_l;
-    const float k = el.kedge[e];
-    const float L = el.rest[e];
-    const float3 gv = dh * (k * (l - L));
+    const double3 d = ld3d(pos, ia) - ld3d(pos, ib);
+    double l = len3(d);
+    if (l < 1.0e-6) l = 1.0e-6;
+    const double inv_l = 1.0 / l;
+    const double3 dh = d * inv_l;
+    const double k = el.kedge[e];
+    const double L = el.rest[e];
+    const double3 gv = dh * (k * (l - L));
     g = end == 0 ? g + gv : g - gv;
-    const float a = k * L * inv_l;
-    const float diag_term = (l < L) ? 0.0f : (k - a);
-    blk = S6{diag_term + a * dh.x * dh.x, a * dh.x * dh.y, a * dh.x * dh.z,
-             diag_term + a * dh.y * dh.y, a * dh.y * dh.z, diag_term + a * dh.z * dh.z};
+    const double a = k * L * inv_l;
+    const double diag_term = (l < L) ? 0.0 : (k - a);
+    blk = S6d{diag_term + a * dh.x * dh.x, a * dh.x * dh.y, a * dh.x * dh.z,
+              diag_term + a * dh.y * dh.y, a * dh.y * dh.z, diag_term + a * dh.z * dh.z};
 }
 
 // Baraff-Witkin stretch of triangle t seen from its local vertex `la`:
@@ -291,50 +352,47 @@ __device__ __forceinline__ void spring_row(const ElemData& el, const float* pos,
 // rest shape (cloth_simulator.cu:423-449, triangle_stretch_constraint.cu:
 // 87-109), i.e. a second (Dm^-1, area, k) set over the same triangles.
 struct TriRow {
-    float3 g;       // gradient at the row's vertex
-    S6 Mu, Mv;
-    float du[3], dv[3];
+    double3 g;  // gradient at the row's vertex
+    S6d Mu, Mv;
+    double du[3], dv[3];
 };
 
-__device__ __forceinline__ void tri_row(const ElemData& el, const float4* __restrict__ dminv,
+__device__ __forceinline__ void tri_row(const ElemData& el, const RestShape* __restrict__ dminv,
                                         const float* __restrict__ area, const float* __restrict__ ktri,
                                         const float* pos, int t, int la, TriRow& o) {
     const int v0 = el.tris[3 * t], v1 = el.tris[3 * t + 1], v2 = el.tris[3 * t + 2];
-    const float3 x0 = ld3(pos, v0), x1 = ld3(pos, v1), x2 = ld3(pos, v2);
-    const float4 Dm = dminv[t];  // (0,0) (0,1) (1,0) (1,1)
-    const float3 a = x1 - x0, b = x2 - x0;
-    const float3 wu = a * Dm.x + b * Dm.z;
-    const float3 wv = a * Dm.y + b * Dm.w;
-    float lu = len3(wu), lv = len3(wv);
-    if (lu < 1.0e-6f) lu = 1.0e-6f;
-    if (lv < 1.0e-6f) lv = 1.0e-6f;
-    const float inv_lu = 1.0f / lu, inv_lv = 1.0f / lv;
-    const float cu = lu - 1.0f, cv = lv - 1.0f;
-    const float3 uh = wu * inv_lu, vh = wv * inv_lv;
+    const double3 x0 = ld3d(pos, v0), x1 = ld3d(pos, v1), x2 = ld3d(pos, v2);
+    const double2 d01 = __ldg(reinterpret_cast<const double2*>(dminv + t));
+    const double2 d23 = __ldg(reinterpret_cast<const double2*>(dminv + t) + 1);
+    const double4 Dm = make_double4(d01.x, d01.y, d23.x, d23.y);  // (0,0) (0,1) (1,0) (1,1)
+    const double3 a = x1 - x0, b = x2 - x0;
+    const double3 wu = a * Dm.x + b * Dm.z;
+    const double3 wv = a * Dm.y + b * Dm.w;
+    double lu = len3(wu), lv = len3(wv);
+    if (lu < 1.0e-6) lu = 1.0e-6;
+    if (lv < 1.0e-6) lv = 1.0e-6;
+    const double inv_lu = 1.0 / lu, inv_lv = 1.0 / lv;
+    const double cu = lu - 1.0, cv = lv - 1.0;
+    const double3 uh = wu * inv_lu, vh = wv * inv_lv;
     o.du[0] = -Dm.x - Dm.z; o.du[1] = Dm.x; o.du[2] = Dm.z;
     o.dv[0] = -Dm.y - Dm.w; o.dv[1] = Dm.y; o.dv[2] = Dm.w;
-    const float k_eff = area[t] * ktri[t];
-    const float dua = la == 0 ? o.du[0] : (la == 1 ? o.du[1] : o.du[2]);
-    const float dva = la == 0 ? o.dv[0] : (la == 1 ? o.dv[1] : o.dv[2]);
+    const double k_eff = (double)area[t] * (double)ktri[t];
+    const double dua = sel3(o.du, la), dva = sel3(o.dv, la);
     o.g = (uh * (cu * dua) + vh * (cv * dva)) * k_eff;
-    const float su = cu > 0.0f ? k_eff * cu * inv_lu : 0.0f;
-    const float sv = cv > 0.0f ? k_eff * cv * inv_lv : 0.0f;
+    const double su = cu > 0.0 ? k_eff * cu * inv_lu : 0.0;
+    const double sv = cv > 0.0 ? k_eff * cv * inv_lv : 0.0;
     // k_eff u u^T + su (I - u u^T) = (k_eff - su) u u^T + su I
-    const float cuu = k_eff - su, cvv = k_eff - sv;
-    o.Mu = S6{cuu * uh.x * uh.x + su, cuu * uh.x * uh.y, cuu * uh.x * uh.z,
-              cuu * uh.y * uh.y + su, cuu * uh.y * uh.z, cuu * uh.z * uh.z + su};
-    o.Mv = S6{cvv * vh.x * vh.x + sv, cvv * vh.x * vh.y, cvv * vh.x * vh.z,
-              cvv * vh.y * vh.y + sv, cvv * vh.y * vh.z, cvv * vh.z * vh.z + sv};
+    const double cuu = k_eff - su, cvv = k_eff - sv;
+    o.Mu = S6d{cuu * uh.x * uh.x + su, cuu * uh.x * uh.y, cuu * uh.x * uh.z,
+               cuu * uh.y * uh.y + su, cuu * uh.y * uh.z, cuu * uh.z * uh.z + su};
+    o.Mv = S6d{cvv * vh.x * vh.x + sv, cvv * vh.x * vh.y, cvv * vh.x * vh.z,
+               cvv * vh.y * vh.y + sv, cvv * vh.y * vh.z, cvv * vh.z * vh.z + sv};
 }
 
-__device__ __forceinline__ float sel3(const float (&a)[3], int i) {
-    return i == 0 ? a[0] : (i == 1 ? a[1] : a[2]);
-}
-
-// c * a added to an off-diagonal accumulator of `ow` planes (6: symmetric
-// storage; 9: row-major, the symmetric block mirrored).
-__device__ __forceinline__ void smem_acc6(float* s, int stride, int slot, float c, const S6& a, int ow = 6) {
-    float* q = s + (size_t)slot * ow * stride;
+// c * a added to an FP64 off-diagonal accumulator of `ow` planes (6:
+// symmetric storage; 9: row-major, the symmetric block mirrored).
+__device__ __forceinline__ void smem_acc6(double* s, int stride, int slot, double c, const S6d& a, int ow = 6) {
+    double* q = s + (size_t)slot * ow * stride;
     if (ow == 6) {
         q[0] += c * a.xx; q[stride] += c * a.xy; q[2 * stride] += c * a.xz;
         q[3 * stride] += c * a.yy; q[4 * stride] += c * a.yz; q[5 * stride] += c * a.zz;
@@ -344,10 +402,10 @@ __device__ __forceinline__ void smem_acc6(float* s, int stride, int slot, float 
         q[6 * stride] += c * a.xz; q[7 * stride] += c * a.yz; q[8 * stride] += c * a.zz;
     }
 }
-// c * u v^T added to a row-major 9-plane accumulator.
-__device__ __forceinline__ void smem_acc_outer(float* s, int stride, int slot, float c, float3 u, float3 v) {
-    float* q = s + (size_t)slot * 9 * stride;
-    const float ux = c * u.x, uy = c * u.y, uz = c * u.z;
+// c * u v^T added to a row-major 9-plane FP64 accumulator.
+__device__ __forceinline__ void smem_acc_outer(double* s, int stride, int slot, double c, double3 u, double3 v) {
+    double* q = s + (size_t)slot * 9 * stride;
+    const double ux = c * u.x, uy = c * u.y, uz = c * u.z;
     q[0] += ux * v.x; q[stride] += ux * v.y; q[2 * stride] += ux * v.z;
     q[3 * stride] += uy * v.x; q[4 * stride] += uy * v.y; q[5 * stride] += uy * v.z;
     q[6 * stride] += uz * v.x; q[7 * stride] += uz * v.y; q[8 * stride] += uz * v.z;
@@ -361,37 +419,33 @@ __device__ __forceinline__ void smem_acc_outer(float* s, int stride, int slot, f
 // gradient k (theta - theta0) a_i, Gauss-Newton Hessian k a_i a_j^T.
 // `valid` is false for a collapsed hinge or a wing without height.
 struct Dihedral {
-    float theta;
-    float3 a[4];
+    double theta;
+    double3 a[4];
     bool valid;
 };
 
-__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
-    return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
-}
-
-__device__ __forceinline__ Dihedral dihedral(float3 x0, float3 x1, float3 x2, float3 x3) {
-    constexpr float kFloor = 1.0e-12f;
+__device__ __forceinline__ Dihedral dihedral(double3 x0, double3 x1, double3 x2, double3 x3) {
+    constexpr double kFloor = 1.0e-12;
     Dihedral d;
     d.valid = false;
-    d.theta = 0.0f;
-    const float3 e = x1 - x0, e2 = x2 - x0, e3 = x3 - x0;
-    const float le = len3(e);
+    d.theta = 0.0;
+    const double3 e = x1 - x0, e2 = x2 - x0, e3 = x3 - x0;
+    const double le = len3(e);
     if (le < kFloor) return d;
-    const float inv_le = 1.0f / le;
-    const float3 m1 = cross3(e2, e), m2 = cross3(e, e3);
-    const float l1 = len3(m1), l2 = len3(m2);
+    const double inv_le = 1.0 / le;
+    const double3 m1 = cross3(e2, e), m2 = cross3(e, e3);
+    const double l1 = len3(m1), l2 = len3(m2);
     if (l1 < kFloor || l2 < kFloor) return d;
-    const float3 n1 = m1 * (1.0f / l1), n2 = m2 * (1.0f / l2);
-    const float st = fminf(1.0f, fmaxf(-1.0f, dot3(cross3(n1, n2), e * inv_le)));
-    d.theta = atan2f(st, dot3(n1, n2));
+    const double3 n1 = m1 * (1.0 / l1), n2 = m2 * (1.0 / l2);
+    const double st = fmin(1.0, fmax(-1.0, dot3(cross3(n1, n2), e * inv_le)));
+    d.theta = atan2(st, dot3(n1, n2));
     // foot points of the wing vertices on the hinge and their heights
-    const float inv_le2 = inv_le * inv_le;
-    const float w1 = dot3(e, e2) * inv_le2, w2 = dot3(e, e3) * inv_le2;
-    const float h1 = len3(e2 - e * w1), h2 = len3(e3 - e * w2);
+    const double inv_le2 = inv_le * inv_le;
+    const double w1 = dot3(e, e2) * inv_le2, w2 = dot3(e, e3) * inv_le2;
+    const double h1 = len3(e2 - e * w1), h2 = len3(e3 - e * w2);
     if (h1 < kFloor || h2 < kFloor) return d;
-    const float g1 = 1.0f / h1, g2 = 1.0f / h2;
-    d.a[0] = n1 * ((w1 - 1.0f) * g1) + n2 * ((w2 - 1.0f) * g2);
+    const double g1 = 1.0 / h1, g2 = 1.0 / h2;
+    d.a[0] = n1 * ((w1 - 1.0) * g1) + n2 * ((w2 - 1.0) * g2);
     d.a[1] = n1 * (-w1 * g1) + n2 * (-w2 * g2);
     d.a[2] = n1 * g1;
     d.a[3] = n2 * g2;
@@ -399,19 +453,38 @@ __device__ __forceinline__ Dihedral dihedral(float3 x0, float3 x1, float3 x2, fl
     return d;
 }
 
+}  // namespace chysx_b200
+
+#include "contact_kernels.cuh"
+
+namespace chysx_b200 {
+
 // ---------------------------------------------------------------------------
 // Fused per-row assembly: predictor (cloth_simulator.cu:83-106), mass
 // (:66-77), gradient at x_n (pins/springs/stretch), RHS (:127-142), Hessian
 // rows (pins, springs, stretch, inertia :199-210), block-Jacobi inverse
 // (pcg_solver.cu:41-42) and, for the zero guess, the PCG start
 // r = b, z = M^-1 b (pcg_solver.cu:386-404) with FP64 r.z and b.b.
-// One thread owns one row and writes every block of it exactly once.
+// One thread owns one row and writes every block of it exactly once; all
+// sums are FP64 (off-diagonal accumulators in shared memory) and each block
+// is rounded to FP32 once.
+//
+// Difference form.  Springs, stretch, shear, bending and the contact
+// operator's pairs depend on positions only through differences, so each
+// element's Hessian blocks sum to zero along a block row and a row's
+// elastic diagonal block is minus the sum of its off-diagonal blocks.  The
+// row therefore also stores its non-elastic diagonal D' (inertia m/dt^2 I,
+// pins, static contacts, the contact operator's slots) in t.dnl, and the
+// solvers apply the operator as
+//     (A p)_i = D'_i p_i + sum_j A_ij (p_j - p_i)     (+ contact pairs),
+// which in FP32 keeps the inertia that the full diagonal (stored in t.diag
+// for the Jacobi inverse and the debug dump) cannot resolve.
 // ---------------------------------------------------------------------------
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, double* part,
                 SolverCfg cfg, int zero_guess, cudaGraphConditionalHandle cond) {
-    extern __shared__ float s_off[];  // [width * ow][BLOCK]
+    extern __shared__ double s_off[];  // [width * ow][BLOCK]
     const int ow = off_width(t);
     const int tid = threadIdx.x;
     const int i = blockIdx.x * BLOCK + tid;
@@ -424,6 +497,7 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
         const int w = (t.slice_off[s + 1] - so) >> 5;
         const S6 I{1.f, 0.f, 0.f, 1.f, 0.f, 1.f};
         st6(t.diag + (size_t)s * 6 * 32 + lane, I);
+        st6(t.dnl + (size_t)s * 6 * 32 + lane, I);
         st6(t.minv + (size_t)s * 6 * 32 + lane, I);
         float* vb = t.val + (size_t)so * ow + lane;
         for (int q = 0; q < ow * w; ++q) vb[q * 32] = 0.0f;
@@ -436,35 +510,36 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
         const int s = i >> 5, lane = i & 31;
         const int so = t.slice_off[s];
         const int w = (t.slice_off[s + 1] - so) >> 5;
-        for (int q = 0; q < ow * w; ++q) s_off[q * BLOCK + tid] = 0.0f;
+        for (int q = 0; q < ow * w; ++q) s_off[q * BLOCK + tid] = 0.0;
 
-        const float3 x = ld3(a.pos, e);
-        const float3 vel = ld3(a.vel, e);
-        float m = 1.0f;
+        const float3 xf = ld3(a.pos, e);
+        const double3 x = d3(xf);
+        const float3 velf = ld3(a.vel, e);
+        const double3 vel = d3(velf);
+        double m = 1.0;
         if (a.inv_mass) {
             const float wi = a.inv_mass[e];
-            m = (wi > 1.0e-12f) ? (1.0f / wi) : 1.0e8f;
+            m = (wi > 1.0e-12f) ? (1.0 / (double)wi) : 1.0e8;
         }
-        float3 acc = f3(a.gx, a.gy, a.gz);
+        double3 acc = d3(a.gx, a.gy, a.gz);
         if (a.apply_force && a.force) {
-            const float im = (m > 0.0f) ? (1.0f / m) : 0.0f;
-            const float3 f = ld3(a.force, e);
-            acc = f3(acc.x + f.x * im, acc.y + f.y * im, acc.z + f.z * im);
+            const double im = (m > 0.0) ? (1.0 / m) : 0.0;
+            const double3 f = ld3d(a.force, e);
+            acc = acc + f * im;
         }
-        const float dt = a.dt;
-        const float3 xt = f3(x.x + dt * vel.x + dt * dt * acc.x, x.y + dt * vel.y + dt * dt * acc.y,
-                             x.z + dt * vel.z + dt * dt * acc.z);
+        const double dt = a.dt;
 
-        float3 g = f3(0.f, 0.f, 0.f);
-        S6 D{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        double3 g = d3(0.0, 0.0, 0.0);
+        S6d Del{0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // elastic diagonal (element blocks on the row)
+        S6d Dnl{0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // non-elastic diagonal D'
         float pinned = 0.f, logk = 0.f;
         int n_springs = 0;
         // pins (pin_constraint.cu:61-92)
         for (int p = t.pin_off[s]; p < t.pin_off[s + 1]; ++p) {
             if (t.pin_row[p] == i) {
-                const float3 tg = ld3(t.pin_tgt, p);
-                g = g + (x - tg) * el.pin_k;
-                D.xx += el.pin_k; D.yy += el.pin_k; D.zz += el.pin_k;
+                const double3 tg = ld3d(t.pin_tgt, p);
+                g = g + (x - tg) * (double)el.pin_k;
+                Dnl.xx += el.pin_k; Dnl.yy += el.pin_k; Dnl.zz += el.pin_k;
                 pinned = 1.f;
             }
         }
@@ -473,19 +548,21 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
             const int o = t.sinc_off[s];
             const int ws = (t.sinc_off[s + 1] - o) >> 5;
             for (int k = 0; k < ws; ++k) {
-                const int e = t.sinc[o + k * 32 + lane];
-                if (e < 0) continue;
+                const int ed = t.sinc[o + k * 32 + lane];
+                if (ed < 0) continue;
                 const unsigned meta = t.sinc_meta[o + k * 32 + lane];
-                S6 H;
-                spring_row(el, a.pos, e, (int)(meta & 1u), g, H);
+                S6d H;
+                spring_row(el, a.pos, ed, (int)(meta & 1u), g, H);
                 if (a.want_features) {
-                    logk += log10f(fmaxf(el.kedge[e], 1.0e-30f));
+                    logk += log10f(fmaxf(el.kedge[ed], 1.0e-30f));
                     ++n_springs;
                 }
-                axpy6(D, 1.0f, H);
                 const unsigned slot = (meta >> 8) & 0xFFu;
-                if (slot == 0xFFu) axpy6(D, -1.0f, H);
-                else smem_acc6(s_off + tid, BLOCK, (int)slot, -1.0f, H, ow);
+                // a self-edge adds H - H to the diagonal
+                if (slot != 0xFFu) {
+                    axpy6(Del, 1.0, H);
+                    smem_acc6(s_off + tid, BLOCK, (int)slot, -1.0, H, ow);
+                }
             }
         }
         // Baraff-Witkin stretch, then shear, per incident triangle
@@ -503,17 +580,17 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
                 if (set == 0) tri_row(el, el.dminv, el.area, el.ktri, a.pos, tri, la, tr);
                 else tri_row(el, el.dminv_s, el.area_s, el.ktri_s, a.pos, tri, la, tr);
                 g = g + tr.g;
-                const float dua = sel3(tr.du, la), dva = sel3(tr.dv, la);
-                axpy6(D, dua * dua, tr.Mu);
-                axpy6(D, dva * dva, tr.Mv);
+                const double dua = sel3(tr.du, la), dva = sel3(tr.dv, la);
+                axpy6(Del, dua * dua, tr.Mu);
+                axpy6(Del, dva * dva, tr.Mv);
 #pragma unroll
                 for (int q = 1; q <= 2; ++q) {
                     const int lb = (la + q) % 3;
                     const unsigned slot = (meta >> (8 * q)) & 0xFFu;
-                    const float cu_ = dua * sel3(tr.du, lb), cv_ = dva * sel3(tr.dv, lb);
+                    const double cu_ = dua * sel3(tr.du, lb), cv_ = dva * sel3(tr.dv, lb);
                     if (slot == 0xFFu) {
-                        axpy6(D, cu_, tr.Mu);
-                        axpy6(D, cv_, tr.Mv);
+                        axpy6(Del, cu_, tr.Mu);
+                        axpy6(Del, cv_, tr.Mv);
                     } else {
                         smem_acc6(s_off + tid, BLOCK, (int)slot, cu_, tr.Mu, ow);
                         smem_acc6(s_off + tid, BLOCK, (int)slot, cv_, tr.Mv, ow);
@@ -533,54 +610,65 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
                 const unsigned meta = t.dinc_meta[o + k * 32 + lane];
                 const int la = (int)(meta & 3u);
                 const int4 q4 = el.dih[d];
-                const Dihedral f = dihedral(ld3(a.pos, q4.x), ld3(a.pos, q4.y), ld3(a.pos, q4.z), ld3(a.pos, q4.w));
+                const Dihedral f = dihedral(ld3d(a.pos, q4.x), ld3d(a.pos, q4.y), ld3d(a.pos, q4.z),
+                                            ld3d(a.pos, q4.w));
                 if (!f.valid) continue;
-                const float3 al = f.a[la];
-                g = g + al * (el.k_bend * (f.theta - el.rest_angle[d]));
-                const float kb = el.k_bend;
-                D.xx += kb * al.x * al.x; D.xy += kb * al.x * al.y; D.xz += kb * al.x * al.z;
-                D.yy += kb * al.y * al.y; D.yz += kb * al.y * al.z; D.zz += kb * al.z * al.z;
+                const double3 al = sel4(f.a, la);
+                const double kb = el.k_bend;
+                g = g + al * (kb * (f.theta - el.rest_angle[d]));
+                Del.xx += kb * al.x * al.x; Del.xy += kb * al.x * al.y; Del.xz += kb * al.x * al.z;
+                Del.yy += kb * al.y * al.y; Del.yz += kb * al.y * al.z; Del.zz += kb * al.z * al.z;
 #pragma unroll
                 for (int q = 1; q <= 3; ++q) {
-                    const float3 am = f.a[(la + q) & 3];
+                    const double3 am = sel4(f.a, (la + q) & 3);
                     const unsigned slot = (meta >> (8 * q)) & 0xFFu;
                     if (slot == 0xFFu) {
                         // a repeated vertex (degenerate dihedral): the block
                         // lands on the diagonal, kept symmetric
-                        const float h = 0.5f * kb;
-                        D.xx += 2.f * h * al.x * am.x; D.yy += 2.f * h * al.y * am.y; D.zz += 2.f * h * al.z * am.z;
-                        D.xy += h * (al.x * am.y + al.y * am.x); D.xz += h * (al.x * am.z + al.z * am.x);
-                        D.yz += h * (al.y * am.z + al.z * am.y);
+                        const double h = 0.5 * kb;
+                        Del.xx += 2.0 * h * al.x * am.x; Del.yy += 2.0 * h * al.y * am.y;
+                        Del.zz += 2.0 * h * al.z * am.z;
+                        Del.xy += h * (al.x * am.y + al.y * am.x); Del.xz += h * (al.x * am.z + al.z * am.x);
+                        Del.yz += h * (al.y * am.z + al.z * am.y);
                     } else {
                         smem_acc_outer(s_off + tid, BLOCK, (int)slot, kb, al, am);
                     }
                 }
             }
         }
-        // contact operator: gradient and diagonal blocks of the row's slots
-        if (t.co.active) contact_assemble_row(t.co, i, g, D);
+        // contact operator: gradient and diagonal blocks of the row's slots;
         // static shapes at x_n (cloth_simulator.cu:997-1008, 1189-1193)
-        float3 sn = f3(0.f, 0.f, 0.f);
-        float sdepth = 0.0f;
-        if (el.sc.active) sdepth = static_contact_row(el.sc, x, vel, dt, g, D, sn);
-        // RHS and inertia
-        const float inv_dt2 = 1.0f / (dt * dt);
-        const float mi = m * inv_dt2;
-        float3 b = f3(mi * (xt.x - x.x) - g.x, mi * (xt.y - x.y) - g.y, mi * (xt.z - x.z) - g.z);
+        if (t.co.active) {
+            float3 gc = f3(0.f, 0.f, 0.f);
+            S6 Dc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            contact_assemble_row(t.co, i, gc, Dc);
+            g = g + d3(gc);
+            add6(Dnl, Dc);
+        }
+        double3 sn = d3(0.0, 0.0, 0.0);
+        double sdepth = 0.0;
+        if (el.sc.active) sdepth = static_contact_row(el.sc, x, vel, dt, g, Dnl, sn);
+        // RHS and inertia: m/dt^2 (x~ - x_n) = m (v / dt + acc)
+        const double mi = m / (dt * dt);
+        double3 b_d = (vel * (1.0 / dt) + acc) * m - g;
         // Coulomb cone on the assembled residual (cloth_simulator.cu:1073-1078)
-        if (sdepth > 0.0f && el.sc.mu > 0.0f) b = coulomb_project(el.sc, b, sn, sdepth);
-        D.xx += mi; D.yy += mi; D.zz += mi;
+        if (sdepth > 0.0 && el.sc.mu > 0.0f) b_d = coulomb_project(el.sc, b_d, sn, sdepth);
+        const float3 b = f3((float)b_d.x, (float)b_d.y, (float)b_d.z);
+        Dnl.xx += mi; Dnl.yy += mi; Dnl.zz += mi;
+        S6d D = Dnl;
+        axpy6(D, 1.0, Del);
 
-        // write the row: diagonal, off-diagonal blocks, M^-1
-        st6(t.diag + (size_t)s * 6 * 32 + lane, D);
+        // write the row: diagonal, non-elastic diagonal, off-diagonal blocks, M^-1
+        st6(t.diag + (size_t)s * 6 * 32 + lane, round6(D));
+        st6(t.dnl + (size_t)s * 6 * 32 + lane, round6(Dnl));
         float* vb = t.val + (size_t)so * ow + lane;
-        for (int q = 0; q < ow * w; ++q) vb[q * 32] = s_off[q * BLOCK + tid];
-        const S6 Mi = inverse6(D);
+        for (int q = 0; q < ow * w; ++q) vb[q * 32] = (float)s_off[q * BLOCK + tid];
+        const S6 Mi = round6(inverse6(D));
         st6(t.minv + (size_t)s * 6 * 32 + lane, Mi);
         v.b[i] = make_float4(b.x, b.y, b.z, n_springs ? logk / (float)n_springs : 0.f);
         if (a.want_features) {
-            const float im = 1.0f / m;
-            v.ap[i] = make_float4(-g.x * im, -g.y * im, -g.z * im, pinned);
+            const double im = 1.0 / m;
+            v.ap[i] = make_float4((float)(-g.x * im), (float)(-g.y * im), (float)(-g.z * im), pinned);
         }
         red[1] = (double)b.x * b.x + (double)b.y * b.y + (double)b.z * b.z;
         if (zero_guess) {
@@ -636,14 +724,14 @@ warm_init_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphCondi
         const int s = i >> 5, lane = i & 31;
         const int so = t.slice_off[s];
         const int w = (t.slice_off[s + 1] - so) >> 5;
-        const S6 D = ld6(t.diag + (size_t)s * 6 * 32 + lane);
+        const S6 D = ld6(t.dnl + (size_t)s * 6 * 32 + lane);
         const float3 xi = xyz(v.x[i]);
         float3 ax = mul(D, xi);
         const int ow = off_width(t);
         const float* vb = t.val + (size_t)so * ow + lane;
         for (int k = 0; k < w; ++k) {
             const int j = t.col[so + k * 32 + lane];
-            ax = ax + mul_off(vb + k * ow * 32, t.nsym, xyz(v.x[j]));
+            ax = ax + mul_off(vb + k * ow * 32, t.nsym, xyz(v.x[j]) - xi);
         }
         if (t.co.active && t.co.residual) ax = ax + contact_spmv_row(t.co, i, [&](int j) { return xyz(v.x[j]); });
         const float3 b = xyz(v.b[i]);
@@ -743,7 +831,7 @@ pcg_spmv_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphCondit
             pi = f3(fmaf(beta, po.x, zi.x), fmaf(beta, po.y, zi.y), fmaf(beta, po.z, zi.z));
         }
         pnew[i] = f4(pi);
-        const S6 D = ld6(t.diag + (size_t)s * 6 * 32 + lane);
+        const S6 D = ld6(t.dnl + (size_t)s * 6 * 32 + lane);
         float3 acc = mul(D, pi);
         const int ow = off_width(t);
         const float* vb = t.val + (size_t)so * ow + lane;
@@ -756,7 +844,7 @@ pcg_spmv_kernel(DevTopo t, Vecs v, SolveState* st, double* part, cudaGraphCondit
                 const float4 po = pold[j];
                 pj = f3(fmaf(beta, po.x, zj.x), fmaf(beta, po.y, zj.y), fmaf(beta, po.z, zj.z));
             }
-            acc = acc + mul_off(vb + k * ow * 32, t.nsym, pj);
+            acc = acc + mul_off(vb + k * ow * 32, t.nsym, pj - pi);
         }
         if (t.co.active)
             acc = acc + contact_spmv_row(t.co, i, [&](int j) {
@@ -879,7 +967,8 @@ __global__ void finalize_kernel(StepArgs a, Vecs v, const SolveState* st) {
 // ---------------------------------------------------------------------------
 // True residual of the returned iterate (the reference's optional
 // compute_true_residual pass, src/solver/pcg_solver.cu:595-641): r = b -
-// (A + C) x recomputed from the stored FP32 system and the final x, with the
+// (A + C) x recomputed from the stored FP32 system (difference form) and the
+// final x, with the
 // products accumulated in FP64, so that the recurrence residual the solver
 // stopped on can be checked against what the iterate actually satisfies.
 // One warp per 32-row slice; out[slice] = (sum r.r, sum b.b) of its rows,
@@ -894,9 +983,9 @@ __global__ void true_residual_kernel(DevTopo t, Vecs v, double2* __restrict__ ou
     if (i < t.n) {
         const int so = t.slice_off[s];
         const int w = (t.slice_off[s + 1] - so) >> 5;
-        const float* d = t.diag + (size_t)s * 6 * 32 + lane;
+        const float* d = t.dnl + (size_t)s * 6 * 32 + lane;
         const float3 xi = xyz(v.x[i]);
-        // D x in FP64: symmetric planes xx, xy, xz, yy, yz, zz
+        // D' x_i in FP64: symmetric planes xx, xy, xz, yy, yz, zz
         const double dxx = d[0], dxy = d[32], dxz = d[64], dyy = d[96], dyz = d[128], dzz = d[160];
         double ax = dxx * xi.x + dxy * xi.y + dxz * xi.z;
         double ay = dxy * xi.x + dyy * xi.y + dyz * xi.z;
@@ -905,7 +994,8 @@ __global__ void true_residual_kernel(DevTopo t, Vecs v, double2* __restrict__ ou
         const float* vb = t.val + (size_t)so * ow + lane;
         for (int k = 0; k < w; ++k) {
             const int j = t.col[so + k * 32 + lane];
-            const float3 xj = xyz(v.x[j]);
+            const float3 xjf = xyz(v.x[j]);
+            const double3 xj = make_double3((double)xjf.x - xi.x, (double)xjf.y - xi.y, (double)xjf.z - xi.z);
             const float* q = vb + (size_t)k * ow * 32;
             if (t.nsym) {
                 ax += (double)q[0] * xj.x + (double)q[32] * xj.y + (double)q[64] * xj.z;
@@ -942,48 +1032,47 @@ __global__ void true_residual_kernel(DevTopo t, Vecs v, double2* __restrict__ ou
 
 // triangle_stretch_constraint.cu:50-110
 __global__ void rest_shape_kernel(const int* __restrict__ tris, const float* __restrict__ pos,
-                                  float4* __restrict__ dminv, float* __restrict__ area, int T,
+                                  RestShape* __restrict__ dminv, float* __restrict__ area, int T,
                                   float det_eps, float cos_t, float sin_t) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
-    const float3 a = ld3(pos, tris[3 * t]), b = ld3(pos, tris[3 * t + 1]), c = ld3(pos, tris[3 * t + 2]);
-    const float3 ab = b - a, ac = c - a;
-    const float lab = len3(ab), lac = len3(ac);
-    const float3 abh = (lab > 1.0e-6f) ? ab * (1.0f / lab) : f3(1.f, 0.f, 0.f);
-    const float u_c = dot3(abh, ac);
-    const float v_c2 = lac * lac - u_c * u_c;
-    const float v_c = (v_c2 > 0.0f) ? sqrtf(v_c2) : 0.0f;
-    area[t] = 0.5f * lab * v_c;
-    const float det = lab * v_c;
-    float i00 = 1.f, i01 = 0.f, i10 = 0.f, i11 = 1.f;
-    if (det > det_eps) {
-        const float inv_det = 1.0f / (lab * v_c - u_c * 0.0f);
+    const double3 a = ld3d(pos, tris[3 * t]), b = ld3d(pos, tris[3 * t + 1]), c = ld3d(pos, tris[3 * t + 2]);
+    const double3 ab = b - a, ac = c - a;
+    const double lab = len3(ab), lac = len3(ac);
+    const double3 abh = (lab > 1.0e-6) ? ab * (1.0 / lab) : d3(1.0, 0.0, 0.0);
+    const double u_c = dot3(abh, ac);
+    const double v_c2 = lac * lac - u_c * u_c;
+    const double v_c = (v_c2 > 0.0) ? sqrt(v_c2) : 0.0;
+    area[t] = (float)(0.5 * lab * v_c);
+    const double det = lab * v_c;
+    double i00 = 1.0, i01 = 0.0, i10 = 0.0, i11 = 1.0;
+    if (det > (double)det_eps) {
+        const double inv_det = 1.0 / det;
         i00 = v_c * inv_det;
         i01 = -u_c * inv_det;
-        i10 = -0.0f * inv_det;
         i11 = lab * inv_det;
     }
-    dminv[t] = make_float4(i00 * cos_t + i01 * (-sin_t), i00 * sin_t + i01 * cos_t,
-                           i10 * cos_t + i11 * (-sin_t), i10 * sin_t + i11 * cos_t);
+    const double ct = cos_t, st = sin_t;
+    dminv[t] = RestShape{i00 * ct - i01 * st, i00 * st + i01 * ct, i10 * ct - i11 * st, i10 * st + i11 * ct};
 }
 
 // Rest angle of every bending dihedral (bending_constraint.cu:126-142);
 // degenerate dihedrals rest at 0.
 __global__ void bending_rest_kernel(const int4* __restrict__ dih, const float* __restrict__ pos,
-                                    float* __restrict__ rest, int D) {
+                                    double* __restrict__ rest, int D) {
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= D) return;
     const int4 q = dih[d];
-    const Dihedral f = dihedral(ld3(pos, q.x), ld3(pos, q.y), ld3(pos, q.z), ld3(pos, q.w));
-    rest[d] = f.valid ? f.theta : 0.0f;
+    const Dihedral f = dihedral(ld3d(pos, q.x), ld3d(pos, q.y), ld3d(pos, q.z), ld3d(pos, q.w));
+    rest[d] = f.valid ? f.theta : 0.0;
 }
 
 // spring_constraint.cu:41-52
 __global__ void rest_length_kernel(const int* __restrict__ edges, const float* __restrict__ pos,
-                                   float* __restrict__ rest, int E) {
+                                   double* __restrict__ rest, int E) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= E) return;
-    rest[e] = len3(ld3(pos, edges[2 * e]) - ld3(pos, edges[2 * e + 1]));
+    rest[e] = len3(ld3d(pos, edges[2 * e]) - ld3d(pos, edges[2 * e + 1]));
 }
 
 // Lumped area-weighted mass, cloth_simulator.cu:151-190, gathered per vertex

@@ -1106,6 +1106,7 @@ private:
         d_val_.resize(std::max<size_t>(1, (size_t)topo_.ell_entries() * off_width()));
         d_val_.zero();
         d_diag_.resize((size_t)topo_.n_pad * 6);
+        d_dnl_.resize((size_t)topo_.n_pad * 6);
         d_minv_.resize((size_t)topo_.n_pad * 6);
         d_tinc_off_.upload(topo_.tinc_off);
         d_tinc_.upload(topo_.tinc);
@@ -1137,7 +1138,11 @@ private:
         // (6 or 9) * width floats
         const int W = std::max(1, topo_.max_width);
         asm_block_ = (W * off_width() <= 96) ? 128 : (W * off_width() <= 192 ? 64 : 32);
-        asm_smem_ = (size_t)off_width() * W * asm_block_ * sizeof(float);
+        asm_smem_ = (size_t)off_width() * W * asm_block_ * sizeof(double);
+        if (asm_smem_ > kMaxAssembleSmem)
+            throw std::runtime_error("a row has " + std::to_string(W) +
+                                     " neighbours, more than the assembly's FP64 row accumulators hold (" +
+                                     std::to_string(kMaxAssembleSmem / (sizeof(double) * 32 * off_width())) + ")");
         const int max_grid = std::max(grid_for(topo_.n, asm_block_), grid_for(topo_.n, kVecBlock));
         d_part_.resize((size_t)std::max(1, max_grid) * 7);
         d_state_.resize(1);
@@ -1154,6 +1159,7 @@ private:
         t.col = d_col_.get();
         t.val = d_val_.get();
         t.diag = d_diag_.get();
+        t.dnl = d_dnl_.get();
         t.minv = d_minv_.get();
         t.tinc_off = d_tinc_off_.get();
         t.tinc = d_tinc_.get();
@@ -2031,8 +2037,9 @@ private:
     bool mesh_on_device_ = false;
     // elements
     bool springs_built_ = false, stretch_built_ = false, shear_built_ = false;
-    DevBuf<float> d_rest_, d_kedge_, d_area_, d_ktri_, d_area_s_, d_ktri_s_;
-    DevBuf<float4> d_dminv_, d_dminv_s_;
+    DevBuf<double> d_rest_;
+    DevBuf<float> d_kedge_, d_area_, d_ktri_, d_area_s_, d_ktri_s_;
+    DevBuf<RestShape> d_dminv_, d_dminv_s_;
     std::vector<int> pin_idx_;
     std::vector<float> pin_tgt_;
     float pin_k_ = 1.0e6f;
@@ -2048,7 +2055,7 @@ private:
     float k_bend_ = 0.0f;
     std::vector<int> dih_;
     DevBuf<int4> d_dih_;
-    DevBuf<float> d_rest_angle_;
+    DevBuf<double> d_rest_angle_;
     DevBuf<int> d_dinc_off_, d_dinc_;
     DevBuf<unsigned> d_dinc_meta_;
     // floats per stored off-diagonal block: bending makes them unsymmetric
@@ -2056,12 +2063,13 @@ private:
     HostTopology topo_;
     DevBuf<int> d_slice_off_, d_col_, d_tinc_off_, d_tinc_, d_sinc_off_, d_sinc_, d_pin_off_, d_pin_row_;
     DevBuf<unsigned> d_tinc_meta_, d_sinc_meta_;
-    DevBuf<float> d_val_, d_diag_, d_minv_, d_pin_tgt_;
+    DevBuf<float> d_val_, d_diag_, d_dnl_, d_minv_, d_pin_tgt_;
     DevBuf<float4> d_b_, d_r_, d_z_, d_x_, d_ap_, d_p0_, d_p1_;
     DevBuf<double> d_part_;
     DevBuf<SolveState> d_state_;
     int asm_block_ = 128;
     size_t asm_smem_ = 0;
+    static constexpr size_t kMaxAssembleSmem = 227 * 1024;  // dynamic shared memory of one CTA
     // persistent PCG plan
     static constexpr int kPathPersistent = 0, kPathLoop = 1, kPathStreamed = 2;
     int solver_path_ = kPathPersistent, graph_path_ = kPathPersistent;

@@ -150,7 +150,9 @@ __global__ void __launch_bounds__(256) coarse_fields_kernel(StepArgs a, CoarseAr
 // A_c block row of coarse block B for the row field qa = blockIdx.y and
 // every column field: 9 warps (one per component of the 3x3 block), lane l
 // takes the rows l of every slice of the block; per-lane sums of
-// w_iqa w_jqb A_ij by column block and qb in dynamic shared memory
+// w_iqa w_jqb A_ij (the operator in its difference form, so the inertia of
+// a block's translation is not lost against its elastic diagonal) by
+// column block and qb in dynamic shared memory
 // ([nq][9][max_nbr][32] floats), then each (qb, column block, component) sum
 // over lanes in lane order (double).  A row's entries are gathered once for
 // all qb.
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, CoarseA
         if (i >= t.n) break;
         const float4 wi4 = weights(i);
         const float wi = pick(wi4, qa);
-        const float dv = wi * t.diag[(size_t)s * 192 + pl * 32 + l];
+        const float dv = wi * t.dnl[(size_t)s * 192 + pl * 32 + l];
         for (int qb = 0; qb < nq; ++qb) acc(qb, self) += dv * pick(wi4, qb);
         const int so = t.slice_off[s];
         const int w = (t.slice_off[s + 1] - so) >> 5;
@@ -194,10 +196,22 @@ __global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, CoarseA
                 vv[k] = in ? wi * t.val[(size_t)so * 6 + (size_t)(k0 + k) * 192 + pl * 32 + l] : 0.0f;
                 wv[k] = weights(cj);
             }
+            // difference form: entry (i, j) adds w_i A_ij w_j^C to (B, C)
+            // and -w_i A_ij w_i to (B, B) (the row's implied elastic
+            // diagonal); inside the block both land on (B, B) as one term
+            // w_i A_ij (w_j - w_i), a difference of smooth fields
 #pragma unroll
             for (int k = 0; k < 8; ++k)
-                if (k0 + k < w)
-                    for (int qb = 0; qb < nq; ++qb) acc(qb, nb8[k]) += vv[k] * pick(wv[k], qb);
+                if (k0 + k < w) {
+                    if (nb8[k] == self) {
+                        for (int qb = 0; qb < nq; ++qb) acc(qb, self) += vv[k] * (pick(wv[k], qb) - pick(wi4, qb));
+                    } else {
+                        for (int qb = 0; qb < nq; ++qb) {
+                            acc(qb, nb8[k]) += vv[k] * pick(wv[k], qb);
+                            acc(qb, self) -= vv[k] * pick(wi4, qb);
+                        }
+                    }
+                }
         }
     }
     __syncthreads();

@@ -28,42 +28,47 @@
 namespace chysx_b200 {
 
 // IPC smoothed 1/|u| (collision/friction.cuh:29-37).
-__device__ __forceinline__ float f1_over_x(float u, float eps) {
-    return u > eps ? 1.0f / u : (-u / eps + 2.0f) / eps;
+__device__ __forceinline__ double f1_over_x(double u, double eps) {
+    return u > eps ? 1.0 / u : (-u / eps + 2.0) / eps;
 }
 
+// Static contacts are evaluated in FP64 like the elastic elements: the depth
+// is a small difference of positions of order one, and its FP32 round-off
+// times the contact stiffness is a spurious force.
+//
 // Deepest static-shape penetration of x: depth > 0 and the outward normal,
 // or depth 0 (static_contact.cu:41-146: planes first, then boxes, a strictly
 // deeper primitive wins).
-__device__ __forceinline__ float static_deepest(const StaticContacts& sc, float3 x, float3& bn) {
-    float best = 0.0f;
-    bn = f3(0.f, 0.f, 0.f);
+__device__ __forceinline__ double static_deepest(const StaticContacts& sc, double3 x, double3& bn) {
+    double best = 0.0;
+    bn = make_double3(0.0, 0.0, 0.0);
     const float* s = sc.shapes;
+    auto v3 = [](const float* p) { return make_double3(p[0], p[1], p[2]); };
     for (int q = 0; q < sc.n_planes; ++q, s += 4) {
-        const float3 nv = f3(s[0], s[1], s[2]);
-        const float depth = sc.thickness - (dot3(nv, x) + s[3]);
+        const double3 nv = v3(s);
+        const double depth = (double)sc.thickness - (dot3(nv, x) + (double)s[3]);
         if (depth > best) { best = depth; bn = nv; }
     }
     for (int q = 0; q < sc.n_boxes; ++q, s += 15) {
-        const float3 rel = x - f3(s[0], s[1], s[2]);
-        const float3 ex = f3(s[6], s[7], s[8]), ey = f3(s[9], s[10], s[11]), ez = f3(s[12], s[13], s[14]);
-        const float qx = dot3(rel, ex), qy = dot3(rel, ey), qz = dot3(rel, ez);
-        const float dx = fabsf(qx) - s[3], dy = fabsf(qy) - s[4], dz = fabsf(qz) - s[5];
-        float d;
-        float3 nv;
-        if (dx <= 0.0f && dy <= 0.0f && dz <= 0.0f) {
+        const double3 rel = x - v3(s);
+        const double3 ex = v3(s + 6), ey = v3(s + 9), ez = v3(s + 12);
+        const double qx = dot3(rel, ex), qy = dot3(rel, ey), qz = dot3(rel, ez);
+        const double dx = fabs(qx) - s[3], dy = fabs(qy) - s[4], dz = fabs(qz) - s[5];
+        double d;
+        double3 nv;
+        if (dx <= 0.0 && dy <= 0.0 && dz <= 0.0) {
             // inside: the nearest face
-            if (dx >= dy && dx >= dz) { nv = qx >= 0.0f ? ex : ex * -1.0f; d = dx; }
-            else if (dy >= dz) { nv = qy >= 0.0f ? ey : ey * -1.0f; d = dy; }
-            else { nv = qz >= 0.0f ? ez : ez * -1.0f; d = dz; }
+            if (dx >= dy && dx >= dz) { nv = qx >= 0.0 ? ex : ex * -1.0; d = dx; }
+            else if (dy >= dz) { nv = qy >= 0.0 ? ey : ey * -1.0; d = dy; }
+            else { nv = qz >= 0.0 ? ez : ez * -1.0; d = dz; }
         } else {
-            const float cx = dx > 0.0f ? dx : 0.0f, cy = dy > 0.0f ? dy : 0.0f, cz = dz > 0.0f ? dz : 0.0f;
-            d = sqrtf(cx * cx + cy * cy + cz * cz);
-            const float inv = 1.0f / fmaxf(d, 1.0e-30f);
-            const float sx = qx > 0.0f ? cx : -cx, sy = qy > 0.0f ? cy : -cy, sz = qz > 0.0f ? cz : -cz;
+            const double cx = dx > 0.0 ? dx : 0.0, cy = dy > 0.0 ? dy : 0.0, cz = dz > 0.0 ? dz : 0.0;
+            d = sqrt(cx * cx + cy * cy + cz * cz);
+            const double inv = 1.0 / fmax(d, 1.0e-300);
+            const double sx = qx > 0.0 ? cx : -cx, sy = qy > 0.0 ? cy : -cy, sz = qz > 0.0 ? cz : -cz;
             nv = ex * (sx * inv) + ey * (sy * inv) + ez * (sz * inv);
         }
-        const float depth = sc.thickness - d;
+        const double depth = (double)sc.thickness - d;
         if (depth > best) { best = depth; bn = nv; }
     }
     return best;
@@ -72,48 +77,46 @@ __device__ __forceinline__ float static_deepest(const StaticContacts& sc, float3
 // Static contact of one row at x_n with velocity vel: adds the penalty and
 // lagged-friction gradient to g and the block k n n^T + alpha (I - n n^T) to
 // D (static_contact.cu:186-285).  Returns the depth (0: no contact).
-__device__ __forceinline__ float static_contact_row(const StaticContacts& sc, float3 x, float3 vel, float dt,
-                                                    float3& g, S6& D, float3& bn) {
-    const float depth = static_deepest(sc, x, bn);
-    if (!(depth > 0.0f)) return 0.0f;
-    const float kd = -sc.k * depth;
-    g = f3(g.x + kd * bn.x, g.y + kd * bn.y, g.z + kd * bn.z);
-    float al = 0.0f;
+__device__ __forceinline__ double static_contact_row(const StaticContacts& sc, double3 x, double3 vel, double dt,
+                                                     double3& g, S6d& D, double3& bn) {
+    const double depth = static_deepest(sc, x, bn);
+    if (!(depth > 0.0)) return 0.0;
+    const double k = sc.k;
+    g = g + bn * (-k * depth);
+    double al = 0.0;
     if (sc.mu > 0.0f) {
-        const float3 dxv = vel * dt;
-        const float vn = dot3(bn, dxv);
-        const float3 ut = dxv - bn * vn;
-        const float un = sqrtf(ut.x * ut.x + ut.y * ut.y + ut.z * ut.z);
-        al = sc.mu * (sc.k * depth) * f1_over_x(un, sc.eps);
-        g = f3(g.x - al * ut.x, g.y - al * ut.y, g.z - al * ut.z);
+        const double3 dxv = vel * dt;
+        const double vn = dot3(bn, dxv);
+        const double3 ut = dxv - bn * vn;
+        const double un = len3(ut);
+        al = (double)sc.mu * (k * depth) * f1_over_x(un, (double)sc.eps);
+        g = g - ut * al;
     }
-    const float k = sc.k;
-    D.xx += k * bn.x * bn.x + al * (1.0f - bn.x * bn.x);
+    D.xx += k * bn.x * bn.x + al * (1.0 - bn.x * bn.x);
     D.xy += k * bn.x * bn.y + al * (-bn.x * bn.y);
     D.xz += k * bn.x * bn.z + al * (-bn.x * bn.z);
-    D.yy += k * bn.y * bn.y + al * (1.0f - bn.y * bn.y);
+    D.yy += k * bn.y * bn.y + al * (1.0 - bn.y * bn.y);
     D.yz += k * bn.y * bn.z + al * (-bn.y * bn.z);
-    D.zz += k * bn.z * bn.z + al * (1.0f - bn.z * bn.z);
+    D.zz += k * bn.z * bn.z + al * (1.0 - bn.z * bn.z);
     return depth;
 }
 
 // Coulomb-cone projection of the assembled residual b of a row in static
 // contact (static_contact.cu:306-381): F0 = b - k depth n; only F0's push
 // into the surface loads the cone.
-__device__ __forceinline__ float3 coulomb_project(const StaticContacts& sc, float3 b, float3 bn, float depth) {
-    const float push = sc.k * depth;
-    const float3 F0 = f3(b.x - push * bn.x, b.y - push * bn.y, b.z - push * bn.z);
-    const float f0n = F0.x * bn.x + F0.y * bn.y + F0.z * bn.z;
-    const float fn = fmaxf(0.0f, -f0n);
-    if (fn <= 0.0f) return b;
-    const float3 F0t = f3(F0.x - f0n * bn.x, F0.y - f0n * bn.y, F0.z - f0n * bn.z);
-    const float ft2 = F0t.x * F0t.x + F0t.y * F0t.y + F0t.z * F0t.z;
-    if (ft2 <= 0.0f) return b;
-    const float ft = sqrtf(ft2);
-    const float cone = sc.mu * fn;
-    if (ft <= cone) return f3(b.x - F0t.x, b.y - F0t.y, b.z - F0t.z);
-    const float shrink = cone / ft;
-    return f3(b.x - shrink * F0t.x, b.y - shrink * F0t.y, b.z - shrink * F0t.z);
+__device__ __forceinline__ double3 coulomb_project(const StaticContacts& sc, double3 b, double3 bn, double depth) {
+    const double push = (double)sc.k * depth;
+    const double3 F0 = b - bn * push;
+    const double f0n = dot3(F0, bn);
+    const double fn = fmax(0.0, -f0n);
+    if (fn <= 0.0) return b;
+    const double3 F0t = F0 - bn * f0n;
+    const double ft2 = dot3(F0t, F0t);
+    if (ft2 <= 0.0) return b;
+    const double ft = sqrt(ft2);
+    const double cone = (double)sc.mu * fn;
+    if (ft <= cone) return b - F0t;
+    return b - F0t * (cone / ft);
 }
 
 __device__ __forceinline__ float sel4(float4 v, int s) {

@@ -876,14 +876,14 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             if (warm) {
                 const int so = t.slice_off[s];
                 const int w = (t.slice_off[s + 1] - so) >> 5;
-                const S6 D = ld6(t.diag + (size_t)s * 192 + lane);
+                const S6 D = ld6(t.dnl + (size_t)s * 192 + lane);
                 x0 = xyz(v.x[i]);
                 float3 ax = mul(D, x0);
                 const int ow = off_width(t);
                 const float* vb = t.val + (size_t)so * ow + lane;
                 for (int k = 0; k < w; ++k) {
                     const int j = t.col[so + k * 32 + lane];
-                    ax = ax + mul_off(vb + k * ow * 32, t.nsym, xyz(v.x[j]));
+                    ax = ax + mul_off(vb + k * ow * 32, t.nsym, xyz(v.x[j]) - x0);
                 }
                 if (t.co.active && t.co.residual)
                     ax = ax + contact_spmv_row(t.co, i, [&](int j) { return xyz(v.x[j]); });
@@ -950,7 +950,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                     pi = f3(fmaf(beta, po.x, zi.x), fmaf(beta, po.y, zi.y), fmaf(beta, po.z, zi.z));
                 }
                 pnew[i] = f4(pi);
-                float3 acc = mul(ld6(t.diag + (size_t)s * 192 + lane), pi);
+                float3 acc = mul(ld6(t.dnl + (size_t)s * 192 + lane), pi);
                 const int ow = off_width(t);
                 const float* vb = t.val + (size_t)so * ow + lane;
                 const int* cb = t.col + so + lane;
@@ -962,7 +962,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                         const float4 po = ldcg4(pold + j);
                         pj = f3(fmaf(beta, po.x, zj.x), fmaf(beta, po.y, zj.y), fmaf(beta, po.z, zj.z));
                     }
-                    acc = acc + mul_off(vb + k * ow * 32, t.nsym, pj);
+                    acc = acc + mul_off(vb + k * ow * 32, t.nsym, pj - pi);
                 }
                 if (t.co.active)
                     acc = acc + contact_spmv_row(t.co, i, [&](int j) {
@@ -1083,6 +1083,8 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     const int li_idx = has ? bp.slice_inst[s] - il0 : 0;
 
     // ---- load the row --------------------------------------------------
+    // D: the row's non-elastic diagonal D'; the operator is applied in the
+    // difference form D'_i p_i + sum_k B_k (p_j - p_i)
     S6 D{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, Mi{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     S6 B[MAXW];
     // column indices: registers, or shared memory in the slot-polling build
@@ -1098,7 +1100,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         col_at(k) = row ? i : 0;
     }
     if (row) {
-        D = ld6(t.diag + (size_t)s * 192 + lane);
+        D = ld6(t.dnl + (size_t)s * 192 + lane);
         Mi = ld6(t.minv + (size_t)s * 192 + lane);
         b = xyz(v.b[i]);
         const int so = t.slice_off[s];
@@ -1118,15 +1120,26 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     // A_cc the CTA's diagonal block of rows (couplings to other CTAs
     // dropped), block-Jacobi inner preconditioner; a fixed polynomial, so P is
     // linear and symmetric and the outer PCG stays plain PCG.  Called by every
-    // thread of the CTA (it synchronises); inactive rows pass r = 0.
+    // thread of the CTA (it synchronises); inactive rows pass r = 0.  A_cc in
+    // the difference form: columns outside the CTA count as zero, their
+    // blocks still enter the row's implied diagonal.
     auto local_spmv = [&](const float4* buf, float3 in) {
         float3 acc = mul(D, in);
 #pragma unroll
         for (int k = 0; k < MAXW; ++k) {
             if (k >= w) continue;
             const int lr = col_at(k) - row0;
-            if ((unsigned)lr < (unsigned)nrows) acc = acc + mul(B[k], xyz(buf[lr]));
+            const float3 nb = (unsigned)lr < (unsigned)nrows ? xyz(buf[lr]) : f3(0.f, 0.f, 0.f);
+            acc = acc + mul(B[k], nb - in);
         }
+        return acc;
+    };
+    // the full diagonal block times a vector: D' v - sum_k B_k v
+    auto full_diag = [&](float3 in) {
+        float3 acc = mul(D, in);
+#pragma unroll
+        for (int k = 0; k < MAXW; ++k)
+            if (k < w) acc = acc - mul(B[k], in);
         return acc;
     };
     auto block_sum = [&](double q) {
@@ -1175,7 +1188,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
         buf[threadIdx.x] = f4(pv);
         __syncthreads();
         const double num = block_sum(dot3d(pv, local_spmv(buf, pv)));
-        const double den = block_sum(dot3d(pv, mul(D, pv)));
+        const double den = block_sum(dot3d(pv, full_diag(pv)));
         if (threadIdx.x == 0) {
             double hi = den > 0.0 ? kPcMargin * num / den : 1.0;
             if (!(hi > 0.0) || !isfinite(hi)) hi = 1.0;
@@ -1229,7 +1242,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
                 float3 ax = mul(D, x);
 #pragma unroll
                 for (int k = 0; k < MAXW; ++k)
-                    if (k < w) ax = ax + mul(B[k], xyz(v.x[col_at(k)]));
+                    if (k < w) ax = ax + mul(B[k], xyz(v.x[col_at(k)]) - x);
                 r = b - ax;
             }
         }
@@ -1270,7 +1283,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
                 float3 ax = mul(D, x);
 #pragma unroll
                 for (int k = 0; k < MAXW; ++k)
-                    if (k < w) ax = ax + mul(B[k], xyz(v.x[col_at(k)]));
+                    if (k < w) ax = ax + mul(B[k], xyz(v.x[col_at(k)]) - x);
                 r = b - ax;
                 z = mul(Mi, r);
             }
@@ -1363,7 +1376,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
                     const float3 q = first ? xyz(zj[k])
                                            : f3(fmaf(beta, pj[k].x, zj[k].x), fmaf(beta, pj[k].y, zj[k].y),
                                                 fmaf(beta, pj[k].z, zj[k].z));
-                    acc = acc + mul(B[k0 + k], q);
+                    acc = acc + mul(B[k0 + k], q - p);
                 }
             }
             ap = acc;

@@ -38,6 +38,10 @@ def test_batch_matches_individual_solves(path):
 def test_batch_instances_converge_independently():
     inst, sc, offs = packed(5, seed=12, lo=6, hi=40)
     g = GpuCloth(sc, max_iter=20000, rel_tol=1e-6, warm_start="zero", instances=offs)
+    # the first step from the stress-free rest state of these regular grids
+    # converges in one iteration for every instance (the FP64 oracle too), so
+    # the counts are compared on the second step
+    g.step()
     g.step()
     it, rr, st = g.sim.instance_stats()
     assert len(it) == 5 and (st == capi.SOLVE_CONVERGED).all()
