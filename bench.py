@@ -4,6 +4,15 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload grid256]
                     [--impl ours|reference] [--warm zero|previous|learned]
 
+Besides the base contract's keys the line carries `arms` (each device-timed
+on its own simulator: plain zero-guess block-Jacobi PCG in the caller's row
+order -- the product's baseline and judge -- against the benchmarked
+configuration on grid256 and grid1024, the learned warm start on grid256
+and the batched 512-instance solve), `oracle_error` (one-step position
+error against the FP64 oracle from the device's state, and the true
+relative residual of each returned step) and `cpu_baseline` (the FP32 CPU
+port on one core in the same configuration, full steps timed whole).
+
 Prints one JSON line.  A "step" is one cloth time step of the workload
 (seeded synthetic scene; the default `grid256` is the 256x256 plain-method
 configuration: per-edge spring k log-U[1e2,1e4], Baraff-Witkin k=1e4, two
@@ -29,7 +38,20 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "ai-phyiscs_b200"))
 
-from chysx import scenes  # noqa: E402
+
+def _load_scenes():
+    # the scene generators by file path: importing the chysx package would
+    # load the product's native library, which the reference arm must not map
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location(
+        "chysx_bench_scenes", os.path.join(ROOT, "ai-phyiscs_b200", "chysx", "scenes.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+scenes = _load_scenes()
 
 METRIC = "cloth steps/s & PCG iters/step at rel-res 1e-6: learned+batched vs plain PCG, 1 B200"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
@@ -157,7 +179,64 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU legs (test infrastructure: the oracle port)
 # ---------------------------------------------------------------------------
-def oracle_setup(sc, fp64, threads):
+def spatial_order(pos, block=512, slice_rows=32):
+    """Particles in spatially compact blocks: recursive coordinate bisection
+    along the longest extent, split sizes multiples of `block` rows (then of
+    `slice_rows`), ties by index -- the partition the device's row order
+    (set_row_order(1)) uses, so the CPU port's 512-row local blocks and
+    2048-row coarse blocks are the same particle sets."""
+    order = np.arange(pos.shape[0])
+
+    def bisect(lo, hi):
+        m = hi - lo
+        if m <= slice_rows:
+            return
+        idx = order[lo:hi]
+        ext = pos[idx].max(axis=0) - pos[idx].min(axis=0)
+        ax = int(np.argmax(ext))
+        unit = block if m > 2 * block else slice_rows
+        left = (m // 2 + unit - 1) // unit * unit
+        if left >= m:
+            left = (m - 1) // slice_rows * slice_rows
+        if left <= 0:
+            return
+        key = np.lexsort((idx, pos[idx, ax].astype(np.float32)))
+        order[lo:hi] = idx[key]
+        bisect(lo, lo + left)
+        bisect(lo + left, hi)
+
+    bisect(0, pos.shape[0])
+    return order
+
+
+def permuted(sc, order):
+    """The scene with its particles renumbered in `order` (order[new] = old)."""
+    inv = np.empty_like(order)
+    inv[order] = np.arange(order.shape[0])
+    out = dict(sc)
+    out["edges"] = scenes.unique_edges(inv[sc["tris"]].astype(np.int32))
+    out["pos"] = sc["pos"][order]
+    out["vel"] = sc["vel"][order]
+    out["tris"] = inv[sc["tris"]].astype(np.int32)
+    out["pin_idx"] = inv[sc["pin_idx"]].astype(np.int32)
+    if np.ndim(sc["k_spring"]):
+        e_old = np.asarray(sc["edges"], np.int64)
+        key = np.minimum(e_old[:, 0], e_old[:, 1]) * sc["pos"].shape[0] + np.maximum(e_old[:, 0], e_old[:, 1])
+        e_new = scenes.unique_edges(out["tris"])
+        a, b = order[e_new[:, 0]], order[e_new[:, 1]]
+        key_new = np.minimum(a, b) * sc["pos"].shape[0] + np.maximum(a, b)
+        srt = np.argsort(key)
+        out["k_spring"] = np.asarray(sc["k_spring"], np.float32)[srt[np.searchsorted(key[srt], key_new)]]
+        out["edges"] = e_new
+    return out
+
+
+def oracle_setup(sc, fp64, threads, pc=None):
+    """The oracle (fp64) or the FP32 CPU port of a scene; pc = (degree,
+    ratio) adds the two-level preconditioner of the device's benchmarked
+    configuration (local blocks of 512 rows, coarse blocks of 2048 rows with
+    translation and linear fields) -- the scene must then be in the
+    spatially compact order."""
     import oracle.oracle as O
 
     O.set_threads(threads)
@@ -172,40 +251,41 @@ def oracle_setup(sc, fp64, threads):
     s.build_springs(sc["k_spring"])
     s.build_stretch(sc["k_stretch"])
     s.set_pins(sc["pin_idx"], sc["pin_targets"], sc.get("k_pin", 1e6))
+    if pc is not None:
+        s.set_preconditioner(int(pc[0]), float(pc[1]), 512, "linear", 2048)
+    s._inv_mass = im
     return s
 
 
-def cpu_step_costs(sc, threads, iters_per_step, budget_s):
-    """Times assembly (a 0-iteration step) and a bounded number of PCG
-    iterations on the CPU port; returns (t_assembly, t_iteration, M)."""
-    s = oracle_setup(sc, fp64=False, threads=threads)
-    s.set_solver(0, 0.0, "zero")
-    t0 = time.perf_counter()
-    s.step(sc["dt"])
-    t_asm = time.perf_counter() - t0
-    s = oracle_setup(sc, fp64=False, threads=threads)
-    probe = 10
-    s.set_solver(probe, 0.0, "zero")
-    t0 = time.perf_counter()
-    s.step(sc["dt"])
-    t_probe = time.perf_counter() - t0
-    t_it = max((t_probe - t_asm) / probe, 1e-9)
-    m = int(max(probe, min(iters_per_step, (budget_s - t_asm) / t_it)))
-    s = oracle_setup(sc, fp64=False, threads=threads)
-    s.set_solver(m, 0.0, "zero")
-    t0 = time.perf_counter()
-    s.step(sc["dt"])
-    t = time.perf_counter() - t0
-    return t_asm, max((t - t_asm) / m, 1e-9), m
+def cpu_full_steps(sc, threads, pc, rel_tol, untimed, timed, budget_s):
+    """Full steps of the CPU port (assembly + solve to rel_tol + update, each
+    its own iteration count): `untimed` steps first, then up to `timed`
+    steps timed one by one, stopping once budget_s is spent.  Returns
+    (seconds per timed step, iterations of each timed step)."""
+    s = oracle_setup(sc, fp64=False, threads=threads, pc=pc)
+    s.set_solver(sc["max_iter"], rel_tol, "zero")
+    for _ in range(untimed):
+        s.step(sc["dt"])
+    secs, iters = [], []
+    t_all = time.perf_counter()
+    for _ in range(timed):
+        t0 = time.perf_counter()
+        s.step(sc["dt"])
+        secs.append(time.perf_counter() - t0)
+        iters.append(int(s.stats()[0]))
+        if time.perf_counter() - t_all > budget_s:
+            break
+    return secs, iters
 
 
 def time_reference_gpu(sc, iters, steps=3, warmup=2):
     """Times the compiled reference ClothSimulator (oracle/_ref, built from the
     reference sources) on the same scene with its PCG fixed at `iters`
-    iterations per step -- the same solver work as our converged steps.  The
-    reference supports one scalar spring / stretch stiffness, so per-element
-    stiffness arrays are replaced by their geometric mean (timing only).
-    Returns steps/s or None when the module is absent."""
+    iterations per step -- the same solver work as our converged
+    block-Jacobi steps.  The reference supports one scalar spring / stretch
+    stiffness, so per-element stiffness arrays are replaced by their
+    geometric mean (timing only).  Returns steps/s or None when the module
+    is absent."""
     import glob
 
     import torch
@@ -242,27 +322,31 @@ def time_reference_gpu(sc, iters, steps=3, warmup=2):
     return steps / (e0.elapsed_time(e1) * 1e-3)
 
 
-def oracle_error(args, sc, offs, make_sim, steps):
-    """Position error of the device path against the FP64 oracle (same
-    scene, same start, same rel-res stop; all host threads) after each of the
-    first `steps` steps, plus the oracle run to rel-res 1e-10.  Returns
-    {"steps", "max_abs_m_vs_fp64_same_tol", "max_abs_m_vs_fp64_tight", ...}."""
+def oracle_error(sc, make_sim, steps):
+    """Parity leg: the device steps the workload in the benchmarked
+    configuration with its true-residual pass on; before each step the FP64
+    oracle (all host threads) is given the device's FP32 state and takes the
+    same step, solved to rel-res 1e-10.  Reports per step max |x_gpu -
+    x_fp64| and the device's true relative residual of the returned dx.
+    (The caller's state is FP32, and this cloth amplifies a one-ulp state
+    change ~1e4-fold within a step or two, so independent trajectories part
+    whatever the arithmetic; the step from a common state is the measure.)"""
     g = make_sim()
-    s_same = oracle_setup(sc, fp64=True, threads=cpu_threads())
-    s_tight = oracle_setup(sc, fp64=True, threads=cpu_threads())
-    s_same.set_solver(sc["max_iter"], 1e-6, "zero")
-    s_tight.set_solver(sc["max_iter"] * 4, 1e-10, "zero")
-    errs_same, errs_tight = [], []
+    g.sim.set_true_residual(True)
+    errs, trues = [], []
     t0 = time.perf_counter()
     for _ in range(steps):
+        p0 = g.positions().astype(np.float32)
+        v0 = g.velocities().astype(np.float32)
         g.step()
-        s_same.step(sc["dt"])
-        s_tight.step(sc["dt"])
-        p = g.positions()
-        errs_same.append(float(np.abs(p - s_same.state()[0]).max()))
-        errs_tight.append(float(np.abs(p - s_tight.state()[0]).max()))
-    return {"steps": steps, "max_abs_m_vs_fp64_same_tol": errs_same, "max_abs_m_vs_fp64_tight": errs_tight,
-            "oracle_threads": cpu_threads(), "seconds": time.perf_counter() - t0}
+        trues.append(float(g.sim.true_residual()[1]))
+        o = oracle_setup(sc, fp64=True, threads=cpu_threads())
+        o.set_state(p0, v0, o._inv_mass)
+        o.set_solver(sc["max_iter"] * 20, 1e-10, "zero")
+        o.step(sc["dt"])
+        errs.append(float(np.abs(g.positions() - o.state()[0]).max()))
+    return {"steps": steps, "one_step_max_abs_m_vs_fp64": errs, "true_rel_residual": trues,
+            "oracle_rel_tol": 1e-10, "oracle_threads": cpu_threads(), "seconds": time.perf_counter() - t0}
 
 
 def cpu_threads():
@@ -273,50 +357,112 @@ def cpu_threads():
 
 
 def run_reference_arm(args, rank):
+    """The reference has no CPU implementation of this path: its restatement
+    (the FP32 CPU port of the oracle, FP64 dots) on all host threads, in the
+    configuration of our arm (same workload, rel-res 1e-6, zero guess, the
+    same two-level preconditioner on the same spatially compact blocks).
+    Every timed step is a full step with its own iteration count."""
     if rank != 0:
         return None
     sc, _ = workload(args.workload)
     threads = cpu_threads()
-    import oracle.oracle as O
-
-    # iterations per step needed at rel-res 1e-6 by the CPU port itself:
-    # the first warm-up step is a complete solve
-    s = oracle_setup(sc, fp64=False, threads=threads)
-    s.set_solver(sc["max_iter"], 1e-6, "zero")
-    t0 = time.perf_counter()
-    s.step(sc["dt"])
-    full_step_s = time.perf_counter() - t0
-    iters = s.stats()[0]
-    per_step = []
-    budget = max(0.2, min(2.0, 150.0 / max(1, args.steps + args.warmup)))
-    samples = []
-    for k in range(args.warmup + args.steps):
-        t_asm, t_it, m = cpu_step_costs(sc, threads, iters, budget)
-        if k >= args.warmup:
-            per_step.append(t_asm + iters * t_it)
-            samples.append(m)
-    sec = float(np.mean(per_step))
+    pc = None if args.pc == "block_jacobi" else (args.pc_degree, args.pc_ratio)
+    if pc is not None or args.row_order == "spatial":
+        sc = permuted(sc, spatial_order(sc["pos"]))
+    budget = 150.0
+    secs, iters = cpu_full_steps(sc, threads, pc, 1e-6, untimed=min(args.warmup, 1), timed=args.steps,
+                                 budget_s=budget)
+    sec = float(np.mean(secs))
     value = 1.0 / sec
-    n_rows = sc["pos"].shape[0]
-    line = {
+    pc_name = "block-Jacobi" if pc is None else f"two-level (Chebyshev {pc[0]} on [lambda/{pc[1]:g}, lambda] + coarse)"
+    return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "steps": len(secs), "warmup": min(args.warmup, 1), "ms_per_step": sec * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 dots)", "data": "synthetic",
-        "pcg_iters_per_step": iters,
-        "config": {"workload": args.workload, "particles": n_rows, "rel_tol": 1e-6, "warm_start": "zero"},
+        "pcg_iters_per_step": float(np.mean(iters)), "pcg_iters_each_step": iters,
+        "config": {"workload": args.workload, "particles": int(sc["pos"].shape[0]), "rel_tol": 1e-6,
+                   "warm_start": "zero", "preconditioner": pc_name, "row_order": "spatial"},
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port",
-                         "sample": (f"each step: assembly + {int(np.mean(samples))} PCG iterations of the "
-                                    f"{args.workload} workload on the FP32 CPU port ({threads} threads), "
-                                    f"scaled to the {iters} iterations/step a full solve took "
-                                    f"(first full step: {full_step_s:.1f} s)")},
+                         "sample": (f"{len(secs)} full steps of {args.workload} (after {min(args.warmup, 1)} untimed) "
+                                    f"on the FP32 CPU port with {pc_name}, {threads} threads, each step timed "
+                                    f"whole with its own iteration count; steps stop after {budget:.0f} s")},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    return line
 
 
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def timed_arm(sim, steps, warmup, flush, inst=False):
+    """Device-timed steps of one simulator (CUDA events around each step,
+    L2 flushed between steps outside the events)."""
+    import torch
+
+    for _ in range(warmup):
+        sim.step()
+    torch.cuda.synchronize()
+    ms, iters, solve_ms = [], [], []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sim.step()
+        e1.record()
+        it, rr, st = sim.stats()
+        if st != 0:
+            raise RuntimeError(f"arm solve status {st}")
+        ms.append(e0.elapsed_time(e1))
+        iters.append(it)
+        solve_ms.append(sim.sim.last_timing()[1])
+    out = {"steps_per_s": steps / (np.sum(ms) * 1e-3), "pcg_iters_per_step": float(np.mean(iters)),
+           "us_per_pcg_iteration": float(np.sum(solve_ms) * 1e3 / max(1, np.sum(iters))), "steps": steps,
+           "kernel": sim.sim.solver_info()[0], "preconditioner_in_use": int(sim.sim.preconditioner()[3])}
+    if inst:
+        out["instances"] = int(sim.sim.num_instances())
+        out["note"] = "pcg_iters_per_step: the slowest instance of each step"
+    return out
+
+
+def comparison_arms(args, flush, make_best):
+    from chysx.runner import GpuCloth
+
+    def sim(sc, offs=None, pc=None, spatial=False, warm="zero", net=None):
+        g = GpuCloth(sc, max_iter=sc["max_iter"], rel_tol=1e-6, warm_start="zero", instances=offs)
+        if net is not None:
+            g.sim.set_network(net)
+        g.sim.set_solver(sc["max_iter"], 1e-6, warm)
+        if pc:
+            g.sim.set_preconditioner(pc, args.pc_degree, args.pc_ratio)
+        if spatial:
+            g.sim.set_row_order(1)
+        g.sim.enable_timing(True)
+        return g
+
+    arms = {}
+    k = min(args.steps, 10)
+    g256, _ = workload("grid256")
+    arms["grid256_plain"] = timed_arm(sim(g256), k, args.warmup, flush)
+    try:
+        from chysx import learned
+
+        net, _ = learned.load(args.net)
+        arms["grid256_learned"] = timed_arm(sim(g256, pc=args.pc, spatial=True, warm="learned", net=net), k,
+                                            args.warmup, flush)
+    except Exception as exc:  # reported, never fatal to the line
+        arms["grid256_learned"] = f"failed: {exc}"
+    g1024, _ = workload("grid1024")
+    arms["grid1024_plain"] = timed_arm(sim(g1024), 2, args.warmup, flush)
+    arms["grid1024_best"] = timed_arm(sim(g1024, pc=args.pc, spatial=True), 2, args.warmup, flush)
+    bsc, boffs = workload("batch512")
+    arms["batch512_best"] = timed_arm(sim(bsc, offs=boffs, pc=args.pc, spatial=True), 3, args.warmup, flush, inst=True)
+    for name in ("grid256", "grid1024"):
+        pl, be = arms.get(f"{name}_plain"), arms.get(f"{name}_best")
+        if isinstance(pl, dict) and isinstance(be, dict):
+            arms[f"{name}_speedup_best_vs_plain"] = be["steps_per_s"] / pl["steps_per_s"]
+            arms[f"{name}_iteration_ratio_plain_vs_best"] = pl["pcg_iters_per_step"] / be["pcg_iters_per_step"]
+    return arms
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -453,36 +599,37 @@ def run_ours(args, rank, world, local_rank):
     value = steps_total / (total_ms_max * 1e-3)
     mean_iters = float(iters.mean())
 
-    # CPU baseline: single-threaded FP32 port, bounded sample.  A batch is
-    # charged the row-weighted mean of its per-instance iteration counts (the
-    # GPU stops each instance at its own convergence).
-    cpu_iters = mean_iters
-    if offs is not None:
-        it_b = g.sim.instance_stats()[0].astype(np.float64)
-        cpu_iters = float(np.sum(np.diff(offs) * it_b) / np.sum(np.diff(offs)))
-    # with the CTA-local preconditioner the CPU port and the reference module,
-    # both block-Jacobi, are charged the block-Jacobi iterations the same
-    # steps need (counted on an untimed block-Jacobi run of the same steps)
-    bj_iters = None
-    pc_used = bool(g.sim.preconditioner()[3])
-    if pc_used and args.legs == "all":
-        bj = GpuCloth(sc, max_iter=sc["max_iter"], rel_tol=rel_tol, warm_start="zero", instances=offs)
-        bj.sim.set_solver(sc["max_iter"], rel_tol, args.warm)
-        counts = []
-        for _ in range(args.warmup + args.steps):
-            bj.step()
-            counts.append(bj.stats()[0])
-        bj_iters = float(np.mean(counts[args.warmup:]))
-        cpu_iters = bj_iters
-    cpu_value = None
-    if args.legs == "all":
-        t_asm, t_it, m = cpu_step_costs(sc, 1, int(cpu_iters), budget_s=args.cpu_budget)
-        cpu_value = 1.0 / (t_asm + cpu_iters * t_it)
+    # the comparison the metric names, each arm device-timed on its own
+    # simulator (N = 1 only): plain zero-guess block-Jacobi PCG in the
+    # caller's row order (the product's baseline and judge) against the
+    # benchmarked configuration, on grid256 and grid1024, the learned warm
+    # start on grid256, and the batched solve
+    arms = None
+    if args.legs == "all" and world == 1 and offs is None and not args.pcg_fixed and args.arms:
+        arms = comparison_arms(args, flush, make_best=make_sim)
+        arms["grid256_best"] = {"steps_per_s": value, "pcg_iters_per_step": mean_iters,
+                                "us_per_pcg_iteration": float(np.sum(solve_ms) * 1e3 / np.sum(iters)),
+                                "steps": args.steps}
+    plain_iters = arms["grid256_plain"]["pcg_iters_per_step"] if arms else None
+
+    # CPU baseline: the FP32 CPU port on one core in the same configuration
+    # (same preconditioner on the same spatially compact blocks), full steps
+    # timed whole; the first step (from rest, the most iterations) untimed
+    cpu = None
+    if args.legs == "all" and offs is None and not args.pcg_fixed:
+        pc = None if args.pc == "block_jacobi" else (args.pc_degree, args.pc_ratio)
+        sc_cpu = permuted(sc, spatial_order(sc["pos"])) if (pc or args.row_order == "spatial") else sc
+        secs, its = cpu_full_steps(sc_cpu, 1, pc, rel_tol, untimed=1, timed=3, budget_s=args.cpu_budget)
+        cpu = {"value": 1.0 / float(np.mean(secs)), "unit": "steps/s", "cores": 1, "kind": "port",
+               "sample": (f"steps 2..{1 + len(secs)} of {args.workload} on the single-threaded FP32 CPU port, "
+                          f"same preconditioner and row blocks as the device ({'block-Jacobi' if pc is None else 'two-level'}), "
+                          f"each step timed whole with its own iterations {its}")}
 
     ref_gpu = None
     if args.reference_gpu and offs is None and args.legs == "all":
         try:
-            ref_gpu = time_reference_gpu(sc, int(round(bj_iters if bj_iters else mean_iters)))
+            ref_iters = plain_iters if plain_iters else mean_iters
+            ref_gpu = time_reference_gpu(sc, int(round(ref_iters)))
         except Exception as exc:  # reported, never fatal to our own line
             ref_gpu = f"failed: {exc}"
 
@@ -499,7 +646,6 @@ def run_ours(args, rank, world, local_rank):
                    "preconditioner": dict(zip(("kind", "degree", "ratio", "in_use"), g.sim.preconditioner())),
                    "row_order": args.row_order},
         "pcg_iters_per_step": mean_iters,
-        "block_jacobi_iters_per_step": bj_iters,
         "pcg_iters_per_step_minmax": [int(iters.min()), int(iters.max())],
         "solve_status": sorted(set(int(s) for s in statuses)),
         "us_per_pcg_iteration": float(np.sum(solve_ms) * 1e3 / np.sum(iters)),
@@ -514,17 +660,15 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic_bytes_per_iteration": b_it,
                      "reference_format_bytes_per_iteration": b_ref,
                      "achieved_reference_format": achieved_ref},
-        "cpu_baseline": None if cpu_value is None else {"value": cpu_value, "unit": "steps/s", "cores": 1, "kind": "port",
-                         "sample": (f"1 step of {args.workload}: assembly + {m} PCG iterations on the "
-                                    f"single-threaded FP32 CPU port, scaled to {cpu_iters:.0f} "
-                                    f"iterations/step")},
+        "cpu_baseline": cpu,
         "e2e": None if not e2e_steps else {"value": e2e_steps * world / (e2e_ms_max * 1e-3), "unit": "steps/s",
                 "h2d_bytes_per_step": 2 * 12 * n, "d2h_bytes_per_step": 2 * 12 * n},
         "reference_gpu": None if ref_gpu is None else {
             "value": ref_gpu, "unit": "steps/s",
-            "pcg_iterations_fixed": int(round(bj_iters if bj_iters else mean_iters)),
+            "pcg_iterations_fixed": int(round(plain_iters if plain_iters else mean_iters)),
             "note": "compiled reference ClothSimulator (springs enabled), same scene with geometric-mean "
-                    "stiffness, PCG fixed at the block-Jacobi iterations/step the same steps take, stream 0"},
+                    "stiffness, PCG fixed at the block-Jacobi iterations/step of the plain arm, stream 0"},
+        "arms": arms,
         # assemble, reset, persistent PCG, finalize; the two-level
         # preconditioner adds the coarse assembly and the coarse inverse, and
         # with linear fields the fields kernel
@@ -532,8 +676,8 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk,
         "wall_s": wall,
     }
-    if args.oracle_steps > 0 and offs is None:
-        line["oracle_error"] = oracle_error(args, sc, offs, make_sim, args.oracle_steps)
+    if args.oracle_steps > 0 and offs is None and args.legs == "all" and not args.pcg_fixed:
+        line["oracle_error"] = oracle_error(sc, make_sim, args.oracle_steps)
     if args.path == 1:
         # assemble + WHILE{2 per iteration} + finalize
         line["gpu_launches"] = int(2 * args.steps + 2 * np.sum(iters))
@@ -643,12 +787,16 @@ def main():
                     help="Chebyshev interval [lambda / ratio, lambda] of the local level (60: fewest iterations "
                          "on grid256 with the coarse level)")
     ap.add_argument("--net", default=os.path.join(ROOT, "ai-phyiscs_b200", "chysx", "data", "warmstart.npz"))
-    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--reference-gpu", type=int, default=1, help="also time the compiled reference module")
     ap.add_argument("--pcg-fixed", type=int, default=0,
                     help="K > 0: fixed K PCG iterations per step (rel_tol 0), the small profiling case")
-    ap.add_argument("--oracle-steps", type=int, default=0,
-                    help="N > 0: also report the position error vs the FP64 oracle over the first N steps")
+    ap.add_argument("--oracle-steps", type=int, default=3,
+                    help="N > 0: also report, for N steps, the one-step position error vs the FP64 oracle and the "
+                         "true residual")
+    ap.add_argument("--arms", type=int, default=1,
+                    help="1: also time the comparison arms (plain block-Jacobi vs the benchmarked configuration on "
+                         "grid256 and grid1024, the learned start, the batched solve)")
     ap.add_argument("--solver", default="pcg", choices=["pcg", "vbd"],
                     help="pcg: the implicit step (headline); vbd: the cloth VBD solver and the reference's")
     ap.add_argument("--vbd-iterations", type=int, default=10)
