@@ -844,7 +844,7 @@ public:
         if (kind) *kind = pc_kind_;
         if (degree) *degree = pc_degree_;
         if (ratio) *ratio = pc_ratio_;
-        if (in_use) *in_use = pc_active() ? (coarse_on_ ? (coarse_nq_ > 1 ? 3 : 2) : 1) : 0;
+        if (in_use) *in_use = coarse_on_ ? (coarse_nq_ > 1 ? 3 : 2) : (pc_active() ? 1 : 0);
     }
     // the CTA-local preconditioner runs in the register-resident kernel of
     // the default synchronisation mode (with the coarse level where the plan
@@ -1421,11 +1421,11 @@ private:
     // the coarse block of every slice and its first row, every block's sorted
     // list of the blocks its rows touch, and the list position of every ELL
     // entry's column block.
-    bool plan_coarse_with(int G, int nq) {
+    bool plan_coarse_with(int G, int nq, bool dense = false) {
         const int grid = plan_.grid, ns = topo_.n_slices;
         const int nb = (grid + G - 1) / G, U = 3 * nq, m = U * nb;
         const int rpc = (m + grid - 1) / grid;
-        if (m > kCoarseThreads || rpc > kCoarseMaxRhs) return false;
+        if (dense ? m > kCoarseDenseMax : (m > kCoarseThreads || rpc > kCoarseMaxRhs)) return false;
         std::vector<int> slice_cb(std::max(1, ns), 0), row0(nb + 1, 0);
         for (int c = 0; c < grid; ++c)
             for (int sl = plan_.cta_slice[c]; sl < plan_.cta_slice[c + 1]; ++sl) slice_cb[sl] = c / G;
@@ -1442,62 +1442,67 @@ private:
         }
         int mn = 1;
         for (const auto& l : lists) mn = std::max(mn, (int)l.size());
-        // band order of the blocks: reverse Cuthill-McKee (breadth-first from
+        // band order of the blocks (direct mode): reverse Cuthill-McKee (breadth-first from
         // a block of least degree, neighbours by increasing degree, ties by
         // index), then the band half-width in unknowns
-        std::vector<int> order, perm(nb, -1);
-        std::vector<char> seen(nb, 0);
-        auto degree = [&](int B) { return (int)lists[B].size(); };
-        while ((int)order.size() < nb) {
-            int start = -1;
-            for (int B = 0; B < nb; ++B)
-                if (!seen[B] && (start < 0 || degree(B) < degree(start))) start = B;
-            // pseudo-peripheral start (George-Liu): from the last level of a
-            // breadth-first search, a block of least degree, while the
-            // eccentricity grows
-            for (int rep = 0, ecc = -1; rep < 8; ++rep) {
-                std::vector<int> lev(nb, -1), q{start};
-                lev[start] = 0;
-                for (size_t h = 0; h < q.size(); ++h)
-                    for (int C : lists[q[h]])
-                        if (lev[C] < 0 && !seen[C]) {
-                            lev[C] = lev[q[h]] + 1;
-                            q.push_back(C);
-                        }
-                const int e = lev[q.back()];
-                if (e <= ecc) break;
-                ecc = e;
-                int best = -1;
-                for (int C : q)
-                    if (lev[C] == e && (best < 0 || degree(C) < degree(best))) best = C;
-                start = best;
-            }
-            seen[start] = 1;
-            size_t head = order.size();
-            order.push_back(start);
-            while (head < order.size()) {
-                const int B = order[head++];
-                std::vector<int> nx;
-                for (int C : lists[B])
-                    if (!seen[C]) nx.push_back(C);
-                std::sort(nx.begin(), nx.end(), [&](int a, int b) {
-                    return degree(a) != degree(b) ? degree(a) < degree(b) : a < b;
-                });
-                for (int C : nx) {
-                    seen[C] = 1;
-                    order.push_back(C);
+        std::vector<int> perm(nb, 0);
+        int bw = 0;
+        if (!dense) {
+            std::vector<int> order;
+            std::fill(perm.begin(), perm.end(), -1);
+            std::vector<char> seen(nb, 0);
+            auto degree = [&](int B) { return (int)lists[B].size(); };
+            while ((int)order.size() < nb) {
+                int start = -1;
+                for (int B = 0; B < nb; ++B)
+                    if (!seen[B] && (start < 0 || degree(B) < degree(start))) start = B;
+                // pseudo-peripheral start (George-Liu): from the last level of a
+                // breadth-first search, a block of least degree, while the
+                // eccentricity grows
+                for (int rep = 0, ecc = -1; rep < 8; ++rep) {
+                    std::vector<int> lev(nb, -1), q{start};
+                    lev[start] = 0;
+                    for (size_t h = 0; h < q.size(); ++h)
+                        for (int C : lists[q[h]])
+                            if (lev[C] < 0 && !seen[C]) {
+                                lev[C] = lev[q[h]] + 1;
+                                q.push_back(C);
+                            }
+                    const int e = lev[q.back()];
+                    if (e <= ecc) break;
+                    ecc = e;
+                    int best = -1;
+                    for (int C : q)
+                        if (lev[C] == e && (best < 0 || degree(C) < degree(best))) best = C;
+                    start = best;
+                }
+                seen[start] = 1;
+                size_t head = order.size();
+                order.push_back(start);
+                while (head < order.size()) {
+                    const int B = order[head++];
+                    std::vector<int> nx;
+                    for (int C : lists[B])
+                        if (!seen[C]) nx.push_back(C);
+                    std::sort(nx.begin(), nx.end(), [&](int a, int b) {
+                        return degree(a) != degree(b) ? degree(a) < degree(b) : a < b;
+                    });
+                    for (int C : nx) {
+                        seen[C] = 1;
+                        order.push_back(C);
+                    }
                 }
             }
+            std::reverse(order.begin(), order.end());
+            for (int p = 0; p < nb; ++p) perm[order[p]] = p;
+            int bwb = 0;
+            for (int B = 0; B < nb; ++B)
+                for (int C : lists[B]) bwb = std::max(bwb, std::abs(perm[B] - perm[C]));
+            bw = std::min(m - 1, (bwb + 1) * U - 1);
+            const size_t direct_smem = ((size_t)m * (bw + 1) + 2 * (size_t)m + (size_t)rpc * m) * sizeof(float) +
+                                       (size_t)bw * (bw + 1) * sizeof(unsigned short);
+            if (direct_smem > kCoarseDirectSmemMax) return false;
         }
-        std::reverse(order.begin(), order.end());
-        for (int p = 0; p < nb; ++p) perm[order[p]] = p;
-        int bwb = 0;
-        for (int B = 0; B < nb; ++B)
-            for (int C : lists[B]) bwb = std::max(bwb, std::abs(perm[B] - perm[C]));
-        const int bw = std::min(m - 1, (bwb + 1) * U - 1);
-        const size_t direct_smem = ((size_t)m * (bw + 1) + 2 * (size_t)m + (size_t)rpc * m) * sizeof(float) +
-                                   (size_t)bw * (bw + 1) * sizeof(unsigned short);
-        if (direct_smem > kCoarseDirectSmemMax) return false;
         std::vector<int> nbr((size_t)nb * mn, -1), cnt(nb), self(nb);
         for (int B = 0; B < nb; ++B) {
             cnt[B] = (int)lists[B].size();
@@ -1529,6 +1534,14 @@ private:
         d_cac_.zero();
         d_cainv_.resize((size_t)m * m);
         d_cainv_.zero();
+        coarse_dense_ = dense;
+        if (dense) {
+            d_cwork_.resize((size_t)m * m + m);
+            d_cfail_.resize(1);
+            d_cfail_.zero();
+            d_cbar_.resize(1);
+            d_cbar_.zero();
+        }
         coarse_nb_ = nb;
         coarse_mn_ = mn;
         coarse_g_ = G;
@@ -1540,15 +1553,30 @@ private:
         ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_assemble_kernel),
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_assemble_smem()),
            "cudaFuncSetAttribute(coarse assemble smem)");
-        ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_direct_kernel),
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_direct_smem()),
-           "cudaFuncSetAttribute(coarse direct smem)");
+        if (!dense)
+            ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_direct_kernel),
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_direct_smem()),
+               "cudaFuncSetAttribute(coarse direct smem)");
         return true;
     }
     void plan_coarse() {
         coarse_on_ = false;
-        if (pc_kind_ != 2 || !resident_ || sync_mode_ != 0 || plan_.n_inst != 1 || plan_.grid > kCoarseMaxBlocks)
+        if (pc_kind_ != 2 || sync_mode_ != 0 || plan_.n_inst != 1) return;
+        if (!resident_) {
+            // streamed kernel: coarse blocks of G CTAs, about
+            // kCoarseStreamRows rows each, translation and linear fields,
+            // A_c inverted densely (at most kCoarseDenseMax unknowns)
+            const int rows_per_cta = std::max(1, 32 * topo_.n_slices / std::max(1, plan_.grid));
+            int G = std::max(1, (kCoarseStreamRows + rows_per_cta / 2) / rows_per_cta);
+            while (G <= plan_.grid) {
+                const int nb = (plan_.grid + G - 1) / G;
+                if (nb >= 2 && plan_coarse_with(G, 4, true)) return;
+                if (nb < 2) return;
+                ++G;
+            }
             return;
+        }
+        if (plan_.grid > kCoarseMaxBlocks) return;
         if (plan_.grid >= 8 && plan_coarse_with(4, 4)) return;
         plan_coarse_with(1, 1);
     }
@@ -1584,6 +1612,9 @@ private:
         c.w = coarse_nq_ > 1 ? d_cw_.get() : nullptr;
         c.ac = d_cac_.get();
         c.ainv = d_cainv_.get();
+        c.dense = coarse_dense_ ? 1 : 0;
+        c.work = coarse_dense_ ? d_cwork_.get() : nullptr;
+        c.fail = coarse_dense_ ? d_cfail_.get() : nullptr;
         return c;
     }
 
@@ -1616,6 +1647,20 @@ private:
             if (plan_.grid <= cap) break;
             grid = cap;
         }
+        plan_coarse();
+        if (coarse_on_) {
+            // the coarse restriction sums of every block (m floats) behind the records
+            pers_smem_ += (size_t)3 * coarse_nq_ * coarse_nb_ * sizeof(float) + 16;
+            ck(cudaFuncSetAttribute(persistent_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pers_smem_),
+               "cudaFuncSetAttribute(persistent smem)");
+            int per_sm = 0;
+            ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_fn(), pcg_block_, pers_smem_),
+               "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+            if (per_sm * sms < plan_.grid) {
+                coarse_on_ = false;  // the extra shared memory costs co-residency: plain block-Jacobi
+                pers_smem_ -= (size_t)3 * coarse_nq_ * coarse_nb_ * sizeof(float) + 16;
+            }
+        }
         upload_plan();
     }
 
@@ -1624,8 +1669,9 @@ private:
     // the resident kernel owns at most one slice per warp.
     void check_plan() const {
         const size_t li_bytes = (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
-        const size_t need = resident_ ? (size_t)resident_warps_ * kSlotW * sizeof(double) + li_bytes
-                                      : (size_t)plan_.max_slices_per_cta * kSlotW * sizeof(double) + li_bytes;
+        size_t need = resident_ ? (size_t)resident_warps_ * kSlotW * sizeof(double) + li_bytes
+                                : (size_t)plan_.max_slices_per_cta * kSlotW * sizeof(double) + li_bytes;
+        if (!resident_ && coarse_on_) need += (size_t)3 * coarse_nq_ * coarse_nb_ * sizeof(float);
         if (pers_smem_ < need || (resident_ && plan_.max_slices_per_cta > resident_warps_) ||
             (!resident_ && pcg_block_ / 32 < 1))
             throw std::logic_error("persistent PCG plan is inconsistent with the selected kernel");
@@ -1807,14 +1853,44 @@ private:
             p.kernelParams = a1;
             cudaGraphNode_t n1, n2;
             ck(cudaGraphAddKernelNode(&n1, graph_, &prev, 1, &p), "add coarse assemble node");
-            void* a2[] = {&cg};
-            cudaKernelNodeParams p2{};
-            p2.func = reinterpret_cast<void*>(&coarse_direct_kernel);
-            p2.gridDim = dim3(plan_.grid);
-            p2.blockDim = dim3(kCoarseThreads);
-            p2.sharedMemBytes = (unsigned)coarse_direct_smem();
-            p2.kernelParams = a2;
-            ck(cudaGraphAddKernelNode(&n2, graph_, &n1, 1, &p2), "add coarse direct node");
+            if (!coarse_dense_) {
+                void* a2[] = {&cg};
+                cudaKernelNodeParams p2{};
+                p2.func = reinterpret_cast<void*>(&coarse_direct_kernel);
+                p2.gridDim = dim3(plan_.grid);
+                p2.blockDim = dim3(kCoarseThreads);
+                p2.sharedMemBytes = (unsigned)coarse_direct_smem();
+                p2.kernelParams = a2;
+                ck(cudaGraphAddKernelNode(&n2, graph_, &n1, 1, &p2), "add coarse direct node");
+            } else {
+                // zero the inversion's barrier and failure flag, then invert
+                cudaGraphNode_t z1, z2;
+                cudaMemsetParams mp{};
+                mp.dst = d_cbar_.get();
+                mp.value = 0;
+                mp.elementSize = 4;
+                mp.width = sizeof(GridBarrier) / 4;
+                mp.height = 1;
+                ck(cudaGraphAddMemsetNode(&z1, graph_, &n1, 1, &mp), "add coarse barrier reset node");
+                mp.dst = d_cfail_.get();
+                mp.width = 1;
+                ck(cudaGraphAddMemsetNode(&z2, graph_, &z1, 1, &mp), "add coarse fail reset node");
+                int dev = 0, sms = 0;
+                ck(cudaGetDevice(&dev), "cudaGetDevice");
+                ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+                GridBarrier* gb = d_cbar_.get();
+                void* a2[] = {&cg, &gb};
+                cudaKernelNodeParams p2{};
+                p2.func = reinterpret_cast<void*>(&coarse_invert_kernel);
+                p2.gridDim = dim3(sms);
+                p2.blockDim = dim3(kCoarseInvertThreads);
+                p2.kernelParams = a2;
+                ck(cudaGraphAddKernelNode(&n2, graph_, &z2, 1, &p2), "add coarse invert node");
+                cudaLaunchAttributeValue coop{};
+                coop.cooperative = 1;
+                ck(cudaGraphKernelNodeSetAttribute(n2, cudaLaunchAttributeCooperative, &coop),
+                   "cooperative attribute (coarse invert)");
+            }
             t1 = n2;
         }
         t1 = timing_node(1, t1);
@@ -2103,6 +2179,10 @@ private:
     DevBuf<float4> d_cw_;
     DevBuf<CoarseArgs> d_cargs_;  // the coarse arguments the PCG kernel reads (BatchPlan holds the pointer)
     DevBuf<float> d_cac_, d_cainv_;
+    bool coarse_dense_ = false;  // streamed kernel's coarse level: dense A_c^-1 formed each step
+    DevBuf<double> d_cwork_;
+    DevBuf<int> d_cfail_;
+    DevBuf<GridBarrier> d_cbar_;
     float pc_ratio_ = 0.0f;
     DevBuf<ZP> d_zp_;
     bool timing_ = false;

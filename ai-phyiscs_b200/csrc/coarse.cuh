@@ -376,4 +376,100 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_direct_kernel(CoarseArg
     }
 }
 
+
+// Dense inverse of A_c for the streamed kernel's coarse level (m <=
+// kCoarseDenseMax): FP64 Gauss-Jordan elimination in place on the
+// symmetrically scaled and shifted matrix S A_c S + kCoarseShift I
+// (S = diag(A_c)^-1/2), no pivoting
+// (A_c is symmetric positive definite on the fields in use; an unknown whose
+// field has zero weight on its whole block has an empty row and column and
+// is given an identity row).  Rows are owned by the grid's warps; each pivot
+// step updates every row against the scaled pivot row, and the owner of the
+// next pivot row scales it right after its own update, so one grid barrier
+// separates consecutive pivots.  Cooperative launch (all CTAs co-resident),
+// the barrier's counter zeroed before the launch, every wait bounded; a
+// failed wait or a non-positive scaled pivot sets ca.fail and the PCG kernel
+// then runs without the coarse level.  Cross-CTA data goes through L2
+// (__ldcg / __stcg).  Output: ca.ainv = S W S in FP32.
+__global__ void __launch_bounds__(kCoarseInvertThreads) coarse_invert_kernel(CoarseArgs ca, GridBarrier* gb) {
+    __shared__ int s_ok;
+    const int m = ca.m, U = 3 * ca.nq, mn = ca.max_nbr, nb = ca.nb;
+    double* W = ca.work;
+    double* sc = W + (size_t)m * m;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int gt = blockIdx.x * blockDim.x + tid, gn = gridDim.x * blockDim.x;
+    const int gwarp = gt >> 5, nwarps = gn >> 5;
+    unsigned target = 0;
+    if (tid == 0) s_ok = 1;
+    __syncthreads();
+    auto gsync = [&]() -> bool {
+        __syncthreads();
+        if (tid == 0 && s_ok) s_ok = barrier_arrive_wait(gb, target) ? 1 : 0;
+        __syncthreads();
+        return s_ok != 0;
+    };
+    // dense A_c from its block rows
+    for (size_t q = gt; q < (size_t)m * m; q += gn) __stcg(W + q, 0.0);
+    if (!gsync()) goto fail;
+    for (int e = gt; e < nb * mn * U * U; e += gn) {
+        const int B = e / (mn * U * U), rem = e % (mn * U * U), k = rem / (U * U), rc = rem % (U * U);
+        if (k >= ca.nbr_cnt[B]) continue;
+        const int C = ca.nbr[B * mn + k];
+        __stcg(W + (size_t)(B * U + rc / U) * m + C * U + rc % U, (double)ca.ac[e]);
+    }
+    if (!gsync()) goto fail;
+    for (int i = gt; i < m; i += gn) {
+        const double d = __ldcg(W + (size_t)i * m + i);
+        __stcg(sc + i, d > 0.0 ? 1.0 / sqrt(d) : 0.0);
+    }
+    if (!gsync()) goto fail;
+    for (size_t q = gt; q < (size_t)m * m; q += gn) {
+        const int i = (int)(q / m), j = (int)(q % m);
+        const double si = __ldcg(sc + i), sj = __ldcg(sc + j);
+        __stcg(W + q, si == 0.0 ? (i == j ? 1.0 : 0.0) : __ldcg(W + q) * si * sj + (i == j ? kCoarseShift : 0.0));
+    }
+    if (!gsync()) goto fail;
+    {
+        // pivot row k scaled: W[k][k] = 1 / p, W[k][j] = W[k][j] / p
+        auto scale_row = [&](int k) {
+            const double p = __ldcg(W + (size_t)k * m + k);
+            const bool good = p > 1.0e-12;
+            if (!good && lane == 0) atomicExch(ca.fail, 1);
+            const double ip = good ? 1.0 / p : 0.0;
+            for (int j = lane; j < m; j += 32) {
+                const double v = j == k ? 1.0 : __ldcg(W + (size_t)k * m + j);
+                __stcg(W + (size_t)k * m + j, v * ip);
+            }
+            __syncwarp();
+        };
+        if (gwarp == 0) scale_row(0);
+        if (!gsync()) goto fail;
+        for (int k = 0; k < m; ++k) {
+            for (int i = gwarp; i < m; i += nwarps) {
+                if (i == k) continue;
+                const double f = __ldcg(W + (size_t)i * m + k);
+                for (int j = lane; j < m; j += 32) {
+                    const double rk = __ldcg(W + (size_t)k * m + j);
+                    const double v = j == k ? 0.0 : __ldcg(W + (size_t)i * m + j);
+                    __stcg(W + (size_t)i * m + j, v - f * rk);
+                }
+                __syncwarp();
+                if (i == k + 1) scale_row(i);
+            }
+            if (!gsync()) goto fail;
+        }
+    }
+    {
+        const bool bad = *(volatile int*)ca.fail != 0;
+        for (size_t q = gt; q < (size_t)m * m; q += gn) {
+            const int i = (int)(q / m), j = (int)(q % m);
+            const double v = __ldcg(W + q) * __ldcg(sc + i) * __ldcg(sc + j);
+            ca.ainv[q] = (bad || !isfinite(v)) ? 0.0f : (float)v;
+        }
+    }
+    return;
+fail:
+    if (tid == 0) atomicExch(ca.fail, 1);
+}
+
 }  // namespace chysx_b200

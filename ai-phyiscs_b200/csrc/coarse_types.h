@@ -8,6 +8,20 @@ constexpr int kCoarseMaxBlocks = 160;  // CTAs of a two-level plan (one warp's s
 constexpr int kCoarseMaxNbr = 16;      // coarse blocks one block's rows touch, itself included
 constexpr int kCoarseThreads = 512;    // threads of the coarse direct solve; also the bound on the coarse unknowns
 constexpr int kCoarseMaxRhs = 4;       // rows of A_c^-1 one CTA computes
+// The streamed kernel's coarse level (systems too large for the register-
+// resident kernel): coarse blocks of about kCoarseStreamRows rows, at most
+// kCoarseDenseMax unknowns, A_c inverted densely once per step
+constexpr int kCoarseStreamRows = 8192;
+constexpr int kCoarseDenseMax = 2048;
+constexpr int kCoarseInvertThreads = 256;
+// Relative diagonal shift of the dense-mode coarse matrix: A_c + shift
+// diag(A_c) is inverted instead of A_c.  The coarse matrix of a flat,
+// unstretched cloth (the first step from rest) has out-of-plane modes held
+// only by inertia, with a scaled condition number ~1e7 on the 1024 x 1024
+// grid; an FP32 inverse and FP32 restrictions of such a matrix are not a
+// usable preconditioner (the solve stalls).  The shift bounds the scaled
+// condition number near 3e5 and still leaves an SPD coarse correction.
+constexpr double kCoarseShift = 1.0e-5;
 
 // Coarse space: coarse block B is the rows of CTAs [B G, (B + 1) G) of the
 // plan; its fields are the translation (weight 1) and, with nq = 4, the
@@ -34,6 +48,13 @@ struct CoarseArgs {
     float4* w = nullptr;                      // [rows] linear-field weights s_1, s_2, s_3 (nq = 4)
     float* ac = nullptr;                      // [nb][max_nbr][U][U] A_c, row-major U x U blocks
     float* ainv = nullptr;                    // [m][m] rows of A_c^-1 (rows r..r+rpc by CTA r / rpc)
+    // dense mode (streamed kernel): A_c^-1 in full, formed by
+    // coarse_invert_kernel in the FP64 workspace (m * m + m doubles); fail != 0
+    // after a step whose inversion met a non-positive pivot or a failed wait
+    // (the coarse level then adds nothing in that step's solve)
+    int dense = 0;
+    double* work = nullptr;
+    int* fail = nullptr;
 };
 
 }  // namespace chysx_b200

@@ -834,7 +834,63 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
     } while (0)
 
 // ---------------------------------------------------------------------------
+// Coarse level of the streamed kernel (dense mode).  Each CTA belongs to
+// coarse block blockIdx.x / G and needs its U entries of y = A_c^-1 v, v the
+// restriction of a vector: every CTA publishes its rows' restriction in its
+// reduction slot (floats at kCoarseOff) before the phase's barrier; after it
+// every CTA sums the slots of each coarse block into vbuf[m] (shared memory)
+// and forms its block's U rows of A_c^-1 vbuf, one row per warp.
+// ---------------------------------------------------------------------------
+// Restriction partials of one slice into its spart entry (floats at
+// kCoarseOff): sum over the warp's rows of w_iq v_i (w_i0 = 1).
+__device__ __forceinline__ float* slice_cpart(double* spart, int sl) {
+    return reinterpret_cast<float*>(spart + (size_t)sl * kSlotW + kCoarseOff);
+}
+// The CTA's restriction (sum of its slices' partials, in slice order) into
+// its slot of `set`; threads 0..U-1 of the calling warp.
+__device__ __forceinline__ void coarse_publish_cta(const BatchPlan& bp, double* spart, int nsl, int own_slot, int set,
+                                                   int lane) {
+    const int U = 3 * bp.cg->nq;
+    if (lane < U) {
+        float acc = 0.0f;
+        for (int sl = 0; sl < nsl; ++sl) acc += slice_cpart(spart, sl)[lane];
+        coarse_slot(bp, set, own_slot)[lane] = acc;
+    }
+}
+template <int BLOCK>
+__device__ __forceinline__ void coarse_apply_dense(const BatchPlan& bp, int set, float* vbuf, float* out) {
+    const CoarseArgs& cg = *bp.cg;
+    const int U = 3 * cg.nq, m = cg.m, G = cg.g, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int j = tid; j < m; j += BLOCK) {
+        const int B = j / U, u = j % U;
+        const int c1 = min((B + 1) * G, bp.n_slots);
+        float acc = 0.0f;
+        for (int c = B * G; c < c1; ++c) acc += __ldcg(coarse_slot(bp, set, c) + u);
+        vbuf[j] = acc;
+    }
+    __syncthreads();
+    const float* rows = cg.ainv + (size_t)((int)blockIdx.x / G) * U * m;
+    for (int r = warp; r < U; r += BLOCK / 32) {
+        const float* a = rows + (size_t)r * m;
+        float acc = 0.0f;
+        for (int j = lane; j < m; j += 32) acc = fmaf(__ldg(a + j), vbuf[j], acc);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) out[r] = acc;
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
 // Streamed persistent kernel: rows are re-read from HBM every iteration.
+// Preconditioner: block-Jacobi, or (single instance, counter barrier, dense
+// coarse level planned) block-Jacobi plus the coarse correction
+//     z = D^-1 r + R A_c^-1 R^T r,
+// a fixed symmetric positive-definite operator, so the outer iteration stays
+// plain PCG.  The coarse part of z rides on the existing phases: phase 1
+// publishes R^T (A p) beside sigma, phase 2 forms A_c^-1 R^T r_new as
+// A_c^-1 R^T r - alpha A_c^-1 R^T A p and publishes R^T r_new beside the
+// dots, from which the next iteration's A_c^-1 R^T r restarts (no drift).
 // ---------------------------------------------------------------------------
 template <int BLOCK, int SYNC = 0>
 __global__ void __launch_bounds__(BLOCK)
@@ -843,6 +899,8 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
     __shared__ int s_flag;
     __shared__ int s_exit;
     __shared__ double s_red[BLOCK * kStartW];  // per-thread slot sums of block_phase (NV <= kStartW)
+    // coarse level: A_c^-1 R^T of b, of r0, of A p, of r; the new r's
+    __shared__ float s_cb[12], s_c0[12], s_cw[12], s_cu[12], s_cn[12];
     constexpr int W = BLOCK / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s0 = bp.cta_slice[blockIdx.x], s1 = bp.cta_slice[blockIdx.x + 1];
@@ -850,6 +908,11 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
     const int nloc = il1 - il0 + 1;
     double* spart = s_mem;
     LocalInst* li = reinterpret_cast<LocalInst*>(s_mem + (size_t)bp.max_slices_per_cta * kSlotW);
+    // dense coarse level (uniform over the grid): off when the step's
+    // inversion failed
+    const bool coarse = !SYNC && bp.cg != nullptr && bp.cg->on && bp.cg->dense && *(volatile int*)bp.cg->fail == 0;
+    const int c_nq = coarse ? bp.cg->nq : 1, c_U = 3 * c_nq;
+    float* c_vbuf = reinterpret_cast<float*>(li + bp.max_inst_per_cta);
     unsigned target = 0;  // barrier target; the counter starts at 0 every solve
     int ph = 0;           // reduction phase (SYNC = 1 slot set ph % 3)
     if (threadIdx.x == 0) {
@@ -860,17 +923,40 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
     __syncthreads();
     bool ok = true;
     auto no_step = [](LocalInst&, const double*) {};
+    auto cw = [&](int i) { return c_nq == 4 ? __ldg(bp.cg->w + i) : make_float4(0.f, 0.f, 0.f, 0.f); };
+    // one exchange phase carrying only the CTA's restriction of a vector;
+    // leaves A_c^-1 R^T v (this block's U entries) in out
+    auto coarse_exchange = [&](float* out) {
+        if (warp == 1) coarse_publish_cta(bp, spart, s1 - s0, li[0].own_slot, slot_set(ph), lane);
+        __syncthreads();
+        const int set = slot_set(ph);
+        CHYSX_BLOCK_PHASE(1, 5, false, no_step);
+        if (!s_flag) coarse_apply_dense<BLOCK>(bp, set, c_vbuf, out);
+    };
 
     // ---- phase 0: initial residual and per-instance start ----------------
     // zero guess: r = b, z = M^-1 b were written by the assembly kernel.
     // warm guess: r = b - A x0, z = M^-1 r (pcg_solver.cu:29-51).
-    for (int s = s0 + warp; s < s1; s += W) {
+    if (coarse) {
+        // A_c^-1 R^T b and, for a warm start, A_c^-1 R^T r0
+        for (int s = s0 + warp; s < s1; s += W) {
+            const int i = s * 32 + lane;
+            const float3 b = i < t.n ? xyz(v.b[i]) : f3(0.f, 0.f, 0.f);
+            if (lane == 0) spart[(s - s0) * kSlotW] = 0.0;
+            warp_restrict(c_nq, b, i < t.n ? cw(i) : make_float4(0.f, 0.f, 0.f, 0.f), slice_cpart(spart, s - s0));
+        }
+        __syncthreads();
+        coarse_exchange(s_cb);
+        ok = s_flag == 0;
+    }
+    for (int s = s0 + warp; s < s1 && ok; s += W) {
         const int i = s * 32 + lane;
         float3 b = f3(0.f, 0.f, 0.f), zb = b, x0 = b, r = b, z = b;
         if (i < t.n) {
             b = xyz(v.b[i]);
             const S6 Mi = ld6(t.minv + (size_t)s * 192 + lane);
             zb = mul(Mi, b);
+            if (coarse) zb = zb + coarse_prolong(c_nq, s_cb, cw(i));
             r = b;
             z = zb;
             if (warm) {
@@ -890,14 +976,45 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                 r = b - ax;
                 z = mul(Mi, r);
                 v.r[i] = f4(r);
+            } else if (coarse) {
+                v.z[i] = f4(zb);
             }
         }
-        start_partials(spart + (s - s0) * kSlotW, lane == 0, b, zb, x0, r, z);
+        if (!coarse || !warm) start_partials(spart + (s - s0) * kSlotW, lane == 0, b, zb, x0, r, z);
+    }
+    if (coarse && warm && ok) {
+        // A_c^-1 R^T r0, then the start partials with z = M^-1 r0 + its prolongation
+        __syncthreads();
+        for (int s = s0 + warp; s < s1; s += W) {
+            const int i = s * 32 + lane;
+            const float3 r = i < t.n ? xyz(v.r[i]) : f3(0.f, 0.f, 0.f);
+            if (lane == 0) spart[(s - s0) * kSlotW] = 0.0;
+            warp_restrict(c_nq, r, i < t.n ? cw(i) : make_float4(0.f, 0.f, 0.f, 0.f), slice_cpart(spart, s - s0));
+        }
+        __syncthreads();
+        coarse_exchange(s_c0);
+        ok = s_flag == 0;
+        for (int s = s0 + warp; s < s1 && ok; s += W) {
+            const int i = s * 32 + lane;
+            float3 b = f3(0.f, 0.f, 0.f), zb = b, x0 = b, r = b, z = b;
+            if (i < t.n) {
+                const S6 Mi = ld6(t.minv + (size_t)s * 192 + lane);
+                const float4 w4 = cw(i);
+                b = xyz(v.b[i]);
+                zb = mul(Mi, b) + coarse_prolong(c_nq, s_cb, w4);
+                x0 = xyz(v.x[i]);
+                r = xyz(v.r[i]);
+                z = mul(Mi, r) + coarse_prolong(c_nq, s_c0, w4);
+            }
+            start_partials(spart + (s - s0) * kSlotW, lane == 0, b, zb, x0, r, z);
+        }
     }
     __syncthreads();
-    CHYSX_BLOCK_PHASE(kStartW, 1, false,
-                      ([&](LocalInst& L, const double* tot) { step_start(bp, L, tot, cfg, warm); }));
-    ok = s_flag == 0;
+    if (ok) {
+        CHYSX_BLOCK_PHASE(kStartW, 1, false,
+                          ([&](LocalInst& L, const double* tot) { step_start(bp, L, tot, cfg, warm); }));
+        ok = s_flag == 0;
+    }
     if (ok && warm) {
         // the scaled guess, or the zero guess where the instance fell back
         for (int s = s0 + warp; s < s1; s += W) {
@@ -905,7 +1022,16 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             if (i >= t.n) continue;
             const S6 Mi = ld6(t.minv + (size_t)s * 192 + lane);
             float3 x = xyz(v.x[i]), r = xyz(v.r[i]), z;
-            start_row(li[bp.slice_inst[s] - il0], xyz(v.b[i]), Mi, x, r, z);
+            const LocalInst& L = li[bp.slice_inst[s] - il0];
+            if (coarse) {
+                const float4 w4 = cw(i);
+                const float3 b = xyz(v.b[i]);
+                const float3 zb = mul(Mi, b) + coarse_prolong(c_nq, s_cb, w4);
+                z = mul(Mi, r) + coarse_prolong(c_nq, s_c0, w4);
+                start_row_linear(L, b, zb, x, r, z);
+            } else {
+                start_row(L, xyz(v.b[i]), Mi, x, r, z);
+            }
             v.x[i] = f4(x);
             v.r[i] = f4(r);
             v.z[i] = f4(z);
@@ -915,6 +1041,15 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
         __syncthreads();
         CHYSX_BLOCK_PHASE(1, 5, false, no_step);
         ok = s_flag == 0;
+    }
+    if (coarse && ok) {
+        // A_c^-1 R^T r of the start: of r0, of the scaled mix of r0 and b, or of b
+        const LocalInst& L0 = li[0];
+        const bool from_r0 = warm && !L0.fallback;
+        if ((int)threadIdx.x < c_U)
+            s_cu[threadIdx.x] = from_r0 ? fmaf(L0.scale, s_c0[threadIdx.x], L0.scale_b * s_cb[threadIdx.x])
+                                        : s_cb[threadIdx.x];
+        __syncthreads();
     }
 
     // ---- iterations ---------------------------------------------------------
@@ -931,11 +1066,12 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             if (s_exit) break;
         }
         // phase 1: p = z + beta p (own row and recomputed for neighbours),
-        // Ap = A p, sigma = p.Ap
+        // Ap = A p, sigma = p.Ap (and the restriction of Ap)
         for (int s = s0 + warp; s < s1; s += W) {
             const LocalInst& L = li[bp.slice_inst[s] - il0];
             const int i = s * 32 + lane;
             double sig = 0.0;
+            float3 acc = f3(0.f, 0.f, 0.f);
             if (!L.done && i < t.n) {
                 const bool first = L.iter == 0;
                 const float beta = L.beta;
@@ -950,7 +1086,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                     pi = f3(fmaf(beta, po.x, zi.x), fmaf(beta, po.y, zi.y), fmaf(beta, po.z, zi.z));
                 }
                 pnew[i] = f4(pi);
-                float3 acc = mul(ld6(t.dnl + (size_t)s * 192 + lane), pi);
+                acc = mul(ld6(t.dnl + (size_t)s * 192 + lane), pi);
                 const int ow = off_width(t);
                 const float* vb = t.val + (size_t)so * ow + lane;
                 const int* cb = t.col + so + lane;
@@ -976,8 +1112,16 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             }
             sig = warp_sum(sig);
             if (lane == 0) spart[(s - s0) * kSlotW] = sig;
+            if (coarse)
+                warp_restrict(c_nq, acc, i < t.n ? cw(i) : make_float4(0.f, 0.f, 0.f, 0.f),
+                              slice_cpart(spart, s - s0));
         }
         __syncthreads();
+        if (coarse) {
+            if (warp == 1) coarse_publish_cta(bp, spart, s1 - s0, li[0].own_slot, slot_set(ph), lane);
+            __syncthreads();
+        }
+        const int set1 = slot_set(ph);
         // ndone only changes in the start and beta steps, i.e. never between
         // this barrier and the next, so every CTA takes the same exit decision
         CHYSX_BLOCK_PHASE(1, 5, true, ([&](LocalInst& L, const double* tot) { step_alpha(L, tot); }));
@@ -986,19 +1130,27 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             break;
         }
         if (!SYNC && s_exit) break;
+        if (coarse) {
+            coarse_apply_dense<BLOCK>(bp, set1, c_vbuf, s_cw);
+            // A_c^-1 R^T r_new = A_c^-1 R^T r - alpha A_c^-1 R^T A p
+            if ((int)threadIdx.x < c_U) s_cn[threadIdx.x] = fmaf(-li[0].alpha, s_cw[threadIdx.x], s_cu[threadIdx.x]);
+            __syncthreads();
+        }
 
-        // phase 2: x += alpha p; r -= alpha Ap; z = M^-1 r
+        // phase 2: x += alpha p; r -= alpha Ap; z = M^-1 r (+ its coarse part)
         for (int s = s0 + warp; s < s1; s += W) {
             const LocalInst& L = li[bp.slice_inst[s] - il0];
             const int i = s * 32 + lane;
             double rz = 0.0, rr = 0.0;
+            float3 rn = f3(0.f, 0.f, 0.f);
             if (!L.done && i < t.n) {
                 const float alpha = L.alpha;
                 const float4 pi = ((L.iter & 1) ? v.p0 : v.p1)[i];
                 const float4 api = v.ap[i], xi = v.x[i], ri = v.r[i];
                 const float3 xn = f3(fmaf(alpha, pi.x, xi.x), fmaf(alpha, pi.y, xi.y), fmaf(alpha, pi.z, xi.z));
-                const float3 rn = f3(fmaf(-alpha, api.x, ri.x), fmaf(-alpha, api.y, ri.y), fmaf(-alpha, api.z, ri.z));
-                const float3 zn = mul(ld6(t.minv + (size_t)s * 192 + lane), rn);
+                rn = f3(fmaf(-alpha, api.x, ri.x), fmaf(-alpha, api.y, ri.y), fmaf(-alpha, api.z, ri.z));
+                float3 zn = mul(ld6(t.minv + (size_t)s * 192 + lane), rn);
+                if (coarse) zn = zn + coarse_prolong(c_nq, s_cn, cw(i));
                 v.x[i] = f4(xn);
                 v.r[i] = f4(rn);
                 v.z[i] = f4(zn);
@@ -1011,8 +1163,16 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                 spart[(s - s0) * kSlotW] = rz;
                 spart[(s - s0) * kSlotW + 1] = rr;
             }
+            if (coarse)
+                warp_restrict(c_nq, rn, i < t.n ? cw(i) : make_float4(0.f, 0.f, 0.f, 0.f),
+                              slice_cpart(spart, s - s0));
         }
         __syncthreads();
+        if (coarse) {
+            if (warp == 1) coarse_publish_cta(bp, spart, s1 - s0, li[0].own_slot, slot_set(ph), lane);
+            __syncthreads();
+        }
+        const int set2 = slot_set(ph);
         // phase 3: beta, iteration count, convergence
         CHYSX_BLOCK_PHASE(2, 5, false,
                           ([&](LocalInst& L, const double* tot) { step_beta(bp, L, tot, cfg); }));
@@ -1020,6 +1180,8 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             ok = false;
             break;
         }
+        // the coarse part restarts from R^T r_new (no recurrence drift)
+        if (coarse) coarse_apply_dense<BLOCK>(bp, set2, c_vbuf, s_cu);
     }
     if (!ok) instances_fail(bp, li, nloc);
 }

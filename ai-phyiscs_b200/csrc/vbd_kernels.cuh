@@ -11,9 +11,9 @@
 //     Green strain's deviatoric (mu) and volumetric (lambda) parts;
 //   * bending: the discrete-shell hinge energy of Grinspun et al. (2003),
 //     k/2 (theta - theta0)^2 with k = stiffness x rest length, theta the
-//     signed dihedral angle atan2((n1 x n2).e, n1.n2) of the two unit face
-//     normals, Gauss-Newton Hessian k dtheta dtheta^T, damping on dtheta/dt.
-// Every function below is written from those formulas.
+//     signed dihedral angle of the two face normals, Gauss-Newton Hessian
+//     k dtheta dtheta^T with the closed-form angle gradient of Bridson et
+//     al. (2003), damping on dtheta/dt.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -60,27 +60,6 @@ __device__ __forceinline__ V3 mul(const M3& a, V3 v) {
     return v3(a.m[0] * v.x + a.m[1] * v.y + a.m[2] * v.z, a.m[3] * v.x + a.m[4] * v.y + a.m[5] * v.z,
               a.m[6] * v.x + a.m[7] * v.y + a.m[8] * v.z);
 }
-__device__ __forceinline__ V3 mul_t(const M3& a, V3 v) {  // a^T v
-    return v3(a.m[0] * v.x + a.m[3] * v.y + a.m[6] * v.z, a.m[1] * v.x + a.m[4] * v.y + a.m[7] * v.z,
-              a.m[2] * v.x + a.m[5] * v.y + a.m[8] * v.z);
-}
-// [a]_x: the matrix of u -> a x u
-__device__ __forceinline__ M3 skew(V3 a) {
-    M3 r;
-    r.m[0] = 0.f; r.m[1] = -a.z; r.m[2] = a.y;
-    r.m[3] = a.z; r.m[4] = 0.f; r.m[5] = -a.x;
-    r.m[6] = -a.y; r.m[7] = a.x; r.m[8] = 0.f;
-    return r;
-}
-__device__ __forceinline__ M3 mul(const M3& a, const M3& b) {
-    M3 r;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-            r.m[3 * i + j] = a.m[3 * i] * b.m[j] + a.m[3 * i + 1] * b.m[3 + j] + a.m[3 * i + 2] * b.m[6 + j];
-    return r;
-}
 __device__ __forceinline__ float det3(const M3& a) {
     return a.m[0] * (a.m[4] * a.m[8] - a.m[5] * a.m[7]) - a.m[1] * (a.m[3] * a.m[8] - a.m[5] * a.m[6]) +
            a.m[2] * (a.m[3] * a.m[7] - a.m[4] * a.m[6]);
@@ -108,140 +87,137 @@ __device__ __forceinline__ void st(float* p, int i, V3 v) {
     p[3 * i + 2] = v.z;
 }
 
+// Adds s * (first-order damping of a strain measure c): with c's gradient
+// gc at the vertex and its rate cdot, the force -kd cdot gc and the
+// Hessian kd / dt gc gc^T, both times the element area (the reference's
+// Rayleigh-style damping of the membrane's two strain measures and of the
+// hinge angle).
+__device__ __forceinline__ void add_damping(float kd, V3 gc, float cdot, float inv_dt, float area, V3& force,
+                                            M3& hm) {
+    force = force - gc * (kd * cdot * area);
+    add_outer(hm, gc, gc, kd * inv_dt * area);
+}
+
 // Membrane force and Hessian block of vertex `which` (0, 1, 2) of one
 // triangle, added to f and h.  Dm^-1 row-major {d00, d01, d10, d11}.
+//
+// Energy density: 2D Stable Neo-Hookean (Smith, de Goes & Kim 2018) of the
+// 3x2 deformation gradient F = [f0 f1] = [x1 - x0, x2 - x0] Dm^-1,
+//     psi = mu/2 (|f0|^2 + |f1|^2 - 2) + lam/2 (J - alpha)^2,
+// with lam = lambda + mu, alpha = 1 + mu / lam and J = |f0 x f1| the area
+// ratio.  Seen from one vertex, whose displacement dx moves the columns by
+// df_k = q_k dx, the area normal nrm = f0 x f1 moves by dx x w with
+// w = q0 f1 - q1 f0, which does not depend on dx.  Hence
+//     dJ/dx = w x nhat,   d2J/dx2 = (|w|^2 I - w w^T - dJ dJ^T) / J,
+// the latter positive semi-definite, and the vertex Hessian
+//     mu |q|^2 I + lam dJ dJ^T + max(0, lam (J - alpha)) d2J/dx2
+// keeps only the non-negative part of the volumetric coefficient (the
+// reference's projection), so it is PSD by construction.
+// Damping acts on the Green strain G = (F^T F - I) / 2 through its norm |G|
+// (weight mu * damping) and its trace (weight lambda * damping), with rates
+// from the step's displacement (x - p) / dt.
 __device__ void membrane(int which, V3 x0, V3 x1, V3 x2, V3 p0, V3 p1, V3 p2, const float* dmi, float area,
                          float mu, float lambda, float damping, float dt, V3& f, M3& h) {
     const float d00 = dmi[0], d01 = dmi[1], d10 = dmi[2], d11 = dmi[3];
     const V3 e1 = x1 - x0, e2 = x2 - x0;
-    // columns of F
-    const V3 c0 = e1 * d00 + e2 * d10;
-    const V3 c1 = e1 * d01 + e2 * d11;
-    const float a00 = dot(c0, c0), a11 = dot(c1, c1), a01 = dot(c0, c1);
-    // J = area ratio = sqrt(det F^T F)
-    const float jj = fmaxf(a00 * a11 - a01 * a01, 1.0e-20f);
-    const float J = sqrtf(jj);
-    const float inv_j = 1.0f / J;
+    const V3 f0 = e1 * d00 + e2 * d10, f1 = e1 * d01 + e2 * d11;
+    // column weights of this vertex: f_k = sum_v x_v q_k(v)
+    float q0, q1;
+    if (which == 0) {
+        q0 = -(d00 + d10);
+        q1 = -(d01 + d11);
+    } else if (which == 1) {
+        q0 = d00;
+        q1 = d01;
+    } else {
+        q0 = d10;
+        q1 = d11;
+    }
+    const V3 nrm = cross(f0, f1);
+    const float J = fmaxf(norm(nrm), 1.0e-10f);
+    const V3 nhat = nrm * (1.0f / J);
+    const V3 w = f1 * q0 - f0 * q1;
+    const V3 dJ = cross(w, nhat);
     const float lam = lambda + mu;
-    const float lam_guard = copysignf(fmaxf(fabsf(lam), 1.0e-6f), lam);
-    const float alpha = 1.0f + mu / lam_guard;
-    // dJ/dF columns
-    const V3 g0 = (c0 * a11 - c1 * a01) * inv_j;
-    const V3 g1 = (c1 * a00 - c0 * a01) * inv_j;
-    const float s = lam * (J - alpha);
-    const V3 P0 = c0 * mu + g0 * s;
-    const V3 P1 = c1 * mu + g1 * s;
-    // d(F columns)/dx_which = scalar weights of the vertex
-    const float w1 = which == 1 ? 1.0f : 0.0f, w2 = which == 2 ? 1.0f : 0.0f, w0 = which == 0 ? 1.0f : 0.0f;
-    const float q0 = d00 * (w1 - w0) + d10 * (w2 - w0);
-    const float q1 = d01 * (w1 - w0) + d11 * (w2 - w0);
-    V3 force = (P0 * q0 + P1 * q1) * (-area);
-    const float r = fmaxf(0.0f, s) * inv_j;
-    const V3 dj = g0 * q0 + g1 * q1;
-    const V3 w = c1 * q0 - c0 * q1;
+    const float alpha = lam != 0.0f ? 1.0f + mu / lam : 1.0f;
+    const float vol = lam * (J - alpha);  // d psi / dJ
+    // gradient of psi at the vertex: mu (q0 f0 + q1 f1) + vol dJ
+    V3 force = ((f0 * q0 + f1 * q1) * mu + dJ * vol) * (-area);
+    const float r = fmaxf(vol, 0.0f) / J;
+    const float ww = dot(w, w);
     M3 hm = zero3();
-    add_scaled_identity(hm, mu * (q0 * q0 + q1 * q1) + r * (q0 * q0 * a11 + q1 * q1 * a00 - 2.0f * q0 * q1 * a01));
-    add_outer(hm, dj, dj, lam - r);
-    add_outer(hm, w, w, -r);
+    add_scaled_identity(hm, (mu * (q0 * q0 + q1 * q1) + r * ww) * area);
+    add_outer(hm, dJ, dJ, (lam - r) * area);
+    add_outer(hm, w, w, -r * area);
     if (damping > 0.0f) {
-        // Green strain G = (F^T F - I) / 2
-        const float G00 = 0.5f * (a00 - 1.0f), G11 = 0.5f * (a11 - 1.0f), G01 = 0.5f * a01;
-        const float gn2 = G00 * G00 + G11 * G11 + 2.0f * G01 * G01;
-        if (gn2 >= 1.0e-20f) {
+        const float c00 = dot(f0, f0), c11 = dot(f1, f1), c01 = dot(f0, f1);
+        const float g00 = 0.5f * (c00 - 1.0f), g11 = 0.5f * (c11 - 1.0f), g01 = 0.5f * c01;
+        const float gnorm2 = g00 * g00 + g11 * g11 + 2.0f * g01 * g01;
+        if (gnorm2 >= 1.0e-20f) {
             const float inv_dt = 1.0f / dt;
-            const V3 v1 = (e1 - (p1 - p0)) * inv_dt, v2 = (e2 - (p2 - p0)) * inv_dt;
-            const V3 dc0 = v1 * d00 + v2 * d10, dc1 = v1 * d01 + v2 * d11;
-            const float gn = sqrtf(gn2);
-            const float n00 = G00 / gn, n01 = G01 / gn, n11 = G11 / gn;
-            const float r00 = dot(c0, dc0), r11 = dot(c1, dc1), r01 = 0.5f * (dot(c0, dc1) + dot(c1, dc0));
-            // deviatoric part: C_mu = |G|
-            const float cmu_t = n00 * r00 + n11 * r11 + 2.0f * n01 * r01;
-            const V3 cmu_x = (c0 * n00 + c1 * n01) * q0 + (c0 * n01 + c1 * n11) * q1;
-            const float kmu = mu * damping;
-            force = force - cmu_x * (kmu * cmu_t * area);
-            add_outer(hm, cmu_x, cmu_x, kmu * inv_dt);
-            // volumetric part: C_lambda = tr G
-            const float clam_t = r00 + r11;
-            const V3 clam_x = c0 * q0 + c1 * q1;
-            const float klam = lambda * damping;
-            force = force - clam_x * (klam * clam_t * area);
-            add_outer(hm, clam_x, clam_x, klam * inv_dt);
+            // column rates from the element's displacement over the step
+            const V3 u1 = (e1 - (p1 - p0)) * inv_dt, u2 = (e2 - (p2 - p0)) * inv_dt;
+            const V3 f0d = u1 * d00 + u2 * d10, f1d = u1 * d01 + u2 * d11;
+            // Gdot = (F^T Fdot + Fdot^T F) / 2
+            const float gd00 = dot(f0, f0d), gd11 = dot(f1, f1d), gd01 = 0.5f * (dot(f0, f1d) + dot(f1, f0d));
+            // |G|: gradient sum_kl (G_kl / |G|) f_k q_l, rate (G : Gdot) / |G|
+            const float ig = 1.0f / sqrtf(gnorm2);
+            const V3 gdev = (f0 * g00 + f1 * g01) * (q0 * ig) + (f0 * g01 + f1 * g11) * (q1 * ig);
+            const float rdev = (g00 * gd00 + g11 * gd11 + 2.0f * g01 * gd01) * ig;
+            add_damping(mu * damping, gdev, rdev, inv_dt, area, force, hm);
+            // tr G: gradient q0 f0 + q1 f1, rate tr Gdot
+            add_damping(lambda * damping, f0 * q0 + f1 * q1, gd00 + gd11, inv_dt, area, force, hm);
         }
     }
     f = f + force;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) h.m[k] += hm.m[k] * area;
+    for (int k = 0; k < 9; ++k) h.m[k] += hm.m[k];
 }
 
 // Hinge bending force and Hessian block of vertex `which` (0..3) of one
-// edge (x0, x1 the opposite vertices, x2 -> x3 the hinge).
+// edge: x0, x1 the wing vertices opposite the hinge x2 -> x3.
+//
+// Energy k/2 (theta - theta0)^2, k = stiffness * rest length (discrete
+// shells, Grinspun et al. 2003), theta the signed angle between the face
+// normals n1 = (x2 - x0) x (x3 - x0) and n2 = (x3 - x1) x (x2 - x1) about
+// the hinge direction.  Its gradient in closed form (Bridson, Marino &
+// Fedkiw 2003; Tamstorf & Grinspun 2013): with a = n1 / |n1|^2,
+// b = n2 / |n2|^2, e = x3 - x2 and t = e / |e|,
+//     dtheta/dx0 = -|e| a,                dtheta/dx1 = -|e| b,
+//     dtheta/dx2 = -((x0 - x3).t) a - ((x1 - x3).t) b,
+//     dtheta/dx3 =  ((x0 - x2).t) a + ((x1 - x2).t) b
+// (they sum to zero).  Gauss-Newton Hessian k g g^T; damping on the angle's
+// rate sum_i g_i . (x_i - p_i) / dt with weight damping * k.  A hinge with
+// a collapsed face or edge contributes nothing.
 __device__ void bending(int which, const V3 (&x)[4], const V3 (&p)[4], float rest_angle, float rest_length,
                         float stiffness, float damping, float dt, V3& f, M3& h) {
-    const float eps = 1.0e-6f;
-    const V3 x02 = x[2] - x[0], x03 = x[3] - x[0], x13 = x[3] - x[1], x12 = x[2] - x[1];
+    constexpr float kMin = 1.0e-6f;
     const V3 e = x[3] - x[2];
-    const V3 n1 = cross(x02, x03), n2 = cross(x13, x12);
-    const float l1 = norm(n1), l2 = norm(n2), le = norm(e);
-    if (l1 < eps || l2 < eps || le < eps) return;
-    const V3 u1 = n1 * (1.0f / l1), u2 = n2 * (1.0f / l2), ue = e * (1.0f / le);
-    const float sn = dot(cross(u1, u2), ue), cs = dot(u1, u2);
-    const float theta = atan2f(sn, cs);
+    const V3 n1 = cross(x[2] - x[0], x[3] - x[0]);
+    const V3 n2 = cross(x[3] - x[1], x[2] - x[1]);
+    const float l1sq = dot(n1, n1), l2sq = dot(n2, n2), le = norm(e);
+    if (sqrtf(l1sq) < kMin || sqrtf(l2sq) < kMin || le < kMin) return;
+    const V3 t = e * (1.0f / le);
+    const V3 a = n1 * (1.0f / l1sq), b = n2 * (1.0f / l2sq);
+    // signed angle: sin from the normals' cross product along the hinge
+    const float l12 = sqrtf(l1sq * l2sq);
+    const float theta = atan2f(dot(cross(n1, n2), t) / l12, dot(n1, n2) / l12);
+    V3 g[4];
+    g[0] = a * (-le);
+    g[1] = b * (-le);
+    g[2] = a * (-dot(x[0] - x[3], t)) - b * dot(x[1] - x[3], t);
+    g[3] = a * dot(x[0] - x[2], t) + b * dot(x[1] - x[2], t);
+    const V3 gv = which == 0 ? g[0] : (which == 1 ? g[1] : (which == 2 ? g[2] : g[3]));
     const float k = stiffness * rest_length;
-    const float dedt = k * (theta - rest_angle);
-    // d(unit normal)/dx = (I - u u^T) / |n| dn/dx
-    auto unit_d = [](float len, V3 u, const M3& raw) {
-        M3 pr = zero3();
-        add_scaled_identity(pr, 1.0f);
-        add_outer(pr, u, u, -1.0f);
-        M3 r = mul(pr, raw);
-#pragma unroll
-        for (int q = 0; q < 9; ++q) r.m[q] *= 1.0f / len;
-        return r;
-    };
-    const M3 su1 = skew(u1), su2 = skew(u2);
-    // dtheta/dx_i = cos d(sin) - sin d(cos)
-    auto dtheta = [&](const M3& du1, const M3& du2) {
-        const M3 a = mul(su1, du2), b = mul(su2, du1);
-        M3 ds;
-#pragma unroll
-        for (int q = 0; q < 9; ++q) ds.m[q] = a.m[q] - b.m[q];
-        const V3 dsin = mul_t(ds, ue);
-        const V3 dcos = mul_t(du1, u2) + mul_t(du2, u1);
-        return dsin * cs - dcos * sn;
-    };
-    const M3 z = zero3();
-    const M3 se = skew(e);
-    M3 se_n;
-#pragma unroll
-    for (int q = 0; q < 9; ++q) se_n.m[q] = -se.m[q];
-    // dn1/dx: x0 -> [e]_x, x2 -> -[x03]_x, x3 -> [x02]_x; dn2/dx: x1 -> -[e]_x,
-    // x2 -> [x13]_x, x3 -> -[x12]_x
-    V3 dth[4];
-    {
-        dth[0] = dtheta(unit_d(l1, u1, se), z);
-        dth[1] = dtheta(z, unit_d(l2, u2, se_n));
-        M3 a = skew(x03), b = skew(x12);
-#pragma unroll
-        for (int q = 0; q < 9; ++q) {
-            a.m[q] = -a.m[q];
-            b.m[q] = -b.m[q];
-        }
-        dth[2] = dtheta(unit_d(l1, u1, a), unit_d(l2, u2, skew(x13)));
-        dth[3] = dtheta(unit_d(l1, u1, skew(x02)), unit_d(l2, u2, b));
-    }
-    const V3 dv = which == 0 ? dth[0] : (which == 1 ? dth[1] : (which == 2 ? dth[2] : dth[3]));
-    V3 force = dv * (-dedt);
+    V3 force = gv * (-k * (theta - rest_angle));
     M3 hb = zero3();
-    add_outer(hb, dv, dv, k);
+    add_outer(hb, gv, gv, k);
     if (damping > 0.0f) {
         const float inv_dt = 1.0f / dt;
         float rate = 0.0f;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) rate += dot(dth[i], x[i] - p[i]);
-        rate *= inv_dt;
-        const float dk = damping * k;
-        force = force - dv * (dk * rate);
-        add_outer(hb, dv, dv, dk * inv_dt);
+        for (int i = 0; i < 4; ++i) rate += dot(g[i], x[i] - p[i]);
+        add_damping(damping * k, gv, rate * inv_dt, inv_dt, 1.0f, force, hb);
     }
     f = f + force;
 #pragma unroll
