@@ -1536,7 +1536,8 @@ private:
         d_cainv_.zero();
         coarse_dense_ = dense;
         if (dense) {
-            d_cwork_.resize((size_t)m * m + m);
+            const size_t mp = (size_t)(m + 31) / 32 * 32;  // kInvTile padding
+            d_cwork_.resize(mp * mp + mp + 2 * 32 * 32);
             d_cfail_.resize(1);
             d_cfail_.zero();
             d_cbar_.resize(1);

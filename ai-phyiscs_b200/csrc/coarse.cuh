@@ -378,27 +378,47 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_direct_kernel(CoarseArg
 
 
 // Dense inverse of A_c for the streamed kernel's coarse level (m <=
-// kCoarseDenseMax): FP64 Gauss-Jordan elimination in place on the
+// kCoarseDenseMax): FP64 blocked Gauss-Jordan elimination in place on the
 // symmetrically scaled and shifted matrix S A_c S + kCoarseShift I
-// (S = diag(A_c)^-1/2), no pivoting
-// (A_c is symmetric positive definite on the fields in use; an unknown whose
-// field has zero weight on its whole block has an empty row and column and
-// is given an identity row).  Rows are owned by the grid's warps; each pivot
-// step updates every row against the scaled pivot row, and the owner of the
-// next pivot row scales it right after its own update, so one grid barrier
-// separates consecutive pivots.  Cooperative launch (all CTAs co-resident),
-// the barrier's counter zeroed before the launch, every wait bounded; a
-// failed wait or a non-positive scaled pivot sets ca.fail and the PCG kernel
-// then runs without the coarse level.  Cross-CTA data goes through L2
-// (__ldcg / __stcg).  Output: ca.ainv = S W S in FP32.
+// (S = diag(A_c)^-1/2), padded to a multiple of 32 with identity rows, no
+// pivoting (the shifted matrix is symmetric positive definite; an unknown
+// whose field has zero weight on its whole block has an empty row and column
+// and is given an identity row).  Per 32-column panel K, with T the inverse
+// of the diagonal tile:
+//     P1  W_KK <- T = W_KK^-1                      (one CTA, in shared memory)
+//     P2  W_KJ <- T W_KJ             (J != K)
+//     P3  W_IJ <- W_IJ - W_IK W_KJ   (I, J != K)
+//     P4  W_IK <- -W_IK T            (I != K; done beside the next panel's P1)
+// with a grid barrier between the phases (three per panel).  Cooperative
+// launch (all CTAs co-resident), the barrier's counter zeroed before the
+// launch, every wait bounded; a failed wait or a non-positive pivot sets
+// ca.fail and the PCG kernel then runs without the coarse level.  Cross-CTA
+// data goes through L2 (__ldcg / __stcg).  Output: ca.ainv = S W S (FP32).
+constexpr int kInvTile = 32;
+
+// c = a * b for 32 x 32 tiles in shared memory (row stride 33), every
+// thread of the CTA four outputs; sign -1 stores -a * b.
+__device__ __forceinline__ void tile_mul(const double (*a)[kInvTile + 1], const double (*b)[kInvTile + 1],
+                                         double (*c)[kInvTile + 1], double sign) {
+    for (int o = threadIdx.x; o < kInvTile * kInvTile; o += blockDim.x) {
+        const int r = o / kInvTile, q = o % kInvTile;
+        double acc = 0.0;
+#pragma unroll 8
+        for (int k = 0; k < kInvTile; ++k) acc = fma(a[r][k], b[k][q], acc);
+        c[r][q] = sign * acc;
+    }
+}
+
 __global__ void __launch_bounds__(kCoarseInvertThreads) coarse_invert_kernel(CoarseArgs ca, GridBarrier* gb) {
     __shared__ int s_ok;
+    __shared__ double sa[kInvTile][kInvTile + 1], sb[kInvTile][kInvTile + 1], sc_[kInvTile][kInvTile + 1];
     const int m = ca.m, U = 3 * ca.nq, mn = ca.max_nbr, nb = ca.nb;
-    double* W = ca.work;
-    double* sc = W + (size_t)m * m;
-    const int tid = threadIdx.x, lane = tid & 31;
+    const int nt = (m + kInvTile - 1) / kInvTile, mp = nt * kInvTile;
+    double* W = ca.work;                   // [mp][mp]
+    double* sc = W + (size_t)mp * mp;      // [mp] scaling
+    double* Tg = sc + mp;                  // [2][32][32] diagonal-tile inverses by panel parity
+    const int tid = threadIdx.x;
     const int gt = blockIdx.x * blockDim.x + tid, gn = gridDim.x * blockDim.x;
-    const int gwarp = gt >> 5, nwarps = gn >> 5;
     unsigned target = 0;
     if (tid == 0) s_ok = 1;
     __syncthreads();
@@ -408,62 +428,127 @@ __global__ void __launch_bounds__(kCoarseInvertThreads) coarse_invert_kernel(Coa
         __syncthreads();
         return s_ok != 0;
     };
+    auto ld_tile = [&](double (*t)[kInvTile + 1], const double* src) {  // tile at src, row stride mp
+        for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x)
+            t[o / kInvTile][o % kInvTile] = __ldcg(src + (size_t)(o / kInvTile) * mp + o % kInvTile);
+    };
+    auto st_tile = [&](double* dst, const double (*t)[kInvTile + 1]) {
+        for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x)
+            __stcg(dst + (size_t)(o / kInvTile) * mp + o % kInvTile, t[o / kInvTile][o % kInvTile]);
+    };
+    auto tile_at = [&](int I, int J) { return W + (size_t)I * kInvTile * mp + (size_t)J * kInvTile; };
     // dense A_c from its block rows
-    for (size_t q = gt; q < (size_t)m * m; q += gn) __stcg(W + q, 0.0);
+    for (size_t q = gt; q < (size_t)mp * mp; q += gn) __stcg(W + q, 0.0);
     if (!gsync()) goto fail;
     for (int e = gt; e < nb * mn * U * U; e += gn) {
         const int B = e / (mn * U * U), rem = e % (mn * U * U), k = rem / (U * U), rc = rem % (U * U);
         if (k >= ca.nbr_cnt[B]) continue;
         const int C = ca.nbr[B * mn + k];
-        __stcg(W + (size_t)(B * U + rc / U) * m + C * U + rc % U, (double)ca.ac[e]);
+        __stcg(W + (size_t)(B * U + rc / U) * mp + C * U + rc % U, (double)ca.ac[e]);
     }
     if (!gsync()) goto fail;
-    for (int i = gt; i < m; i += gn) {
-        const double d = __ldcg(W + (size_t)i * m + i);
+    for (int i = gt; i < mp; i += gn) {
+        const double d = i < m ? __ldcg(W + (size_t)i * mp + i) : 0.0;
         __stcg(sc + i, d > 0.0 ? 1.0 / sqrt(d) : 0.0);
     }
     if (!gsync()) goto fail;
-    for (size_t q = gt; q < (size_t)m * m; q += gn) {
-        const int i = (int)(q / m), j = (int)(q % m);
+    for (size_t q = gt; q < (size_t)mp * mp; q += gn) {
+        const int i = (int)(q / mp), j = (int)(q % mp);
         const double si = __ldcg(sc + i), sj = __ldcg(sc + j);
-        __stcg(W + q, si == 0.0 ? (i == j ? 1.0 : 0.0) : __ldcg(W + q) * si * sj + (i == j ? kCoarseShift : 0.0));
+        __stcg(W + q, si == 0.0 || sj == 0.0 ? (i == j ? 1.0 : 0.0)
+                                             : __ldcg(W + q) * si * sj + (i == j ? kCoarseShift : 0.0));
     }
     if (!gsync()) goto fail;
-    {
-        // pivot row k scaled: W[k][k] = 1 / p, W[k][j] = W[k][j] / p
-        auto scale_row = [&](int k) {
-            const double p = __ldcg(W + (size_t)k * m + k);
-            const bool good = p > 1.0e-12;
-            if (!good && lane == 0) atomicExch(ca.fail, 1);
-            const double ip = good ? 1.0 / p : 0.0;
-            for (int j = lane; j < m; j += 32) {
-                const double v = j == k ? 1.0 : __ldcg(W + (size_t)k * m + j);
-                __stcg(W + (size_t)k * m + j, v * ip);
+    for (int K = 0; K <= nt; ++K) {
+        // P4 of the previous panel: W_I,K-1 <- -W_I,K-1 T_{K-1}
+        if (K > 0) {
+            const double* Tp = Tg + (size_t)((K - 1) & 1) * kInvTile * kInvTile;
+            for (int I = blockIdx.x; I < nt; I += gridDim.x) {
+                if (I == K - 1) continue;
+                for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x)
+                    sb[o / kInvTile][o % kInvTile] = __ldcg(Tp + o);
+                ld_tile(sa, tile_at(I, K - 1));
+                __syncthreads();
+                tile_mul(sa, sb, sc_, -1.0);
+                __syncthreads();
+                st_tile(tile_at(I, K - 1), sc_);
+                __syncthreads();
             }
-            __syncwarp();
-        };
-        if (gwarp == 0) scale_row(0);
-        if (!gsync()) goto fail;
-        for (int k = 0; k < m; ++k) {
-            for (int i = gwarp; i < m; i += nwarps) {
-                if (i == k) continue;
-                const double f = __ldcg(W + (size_t)i * m + k);
-                for (int j = lane; j < m; j += 32) {
-                    const double rk = __ldcg(W + (size_t)k * m + j);
-                    const double v = j == k ? 0.0 : __ldcg(W + (size_t)i * m + j);
-                    __stcg(W + (size_t)i * m + j, v - f * rk);
-                }
-                __syncwarp();
-                if (i == k + 1) scale_row(i);
-            }
-            if (!gsync()) goto fail;
         }
+        if (K == nt) {
+            if (!gsync()) goto fail;
+            break;
+        }
+        // P1: T = W_KK^-1 by Gauss-Jordan in shared memory (the last CTA,
+        // the others being busy with P4 above)
+        if (blockIdx.x == gridDim.x - 1) {
+            ld_tile(sa, tile_at(K, K));
+            __syncthreads();
+            for (int k = 0; k < kInvTile; ++k) {
+                const double p = sa[k][k];
+                const bool good = p > 1.0e-12;
+                if (!good && tid == 0) atomicExch(ca.fail, 1);
+                const double ip = good ? 1.0 / p : 0.0;
+                __syncthreads();
+                if (tid < kInvTile) sa[k][tid] = (tid == k ? 1.0 : sa[k][tid]) * ip;
+                __syncthreads();
+                for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x) {
+                    const int r = o / kInvTile, q = o % kInvTile;
+                    if (r == k) continue;
+                    sb[r][q] = sa[r][k];  // the factor of row r
+                }
+                __syncthreads();
+                for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x) {
+                    const int r = o / kInvTile, q = o % kInvTile;
+                    if (r == k) continue;
+                    sa[r][q] = (q == k ? 0.0 : sa[r][q]) - sb[r][q] * sa[k][q];
+                }
+                __syncthreads();
+            }
+            double* Tk = Tg + (size_t)(K & 1) * kInvTile * kInvTile;
+            for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x) __stcg(Tk + o, sa[o / kInvTile][o % kInvTile]);
+            st_tile(tile_at(K, K), sa);
+        }
+        if (!gsync()) goto fail;
+        // P2: W_KJ <- T W_KJ
+        {
+            const double* Tk = Tg + (size_t)(K & 1) * kInvTile * kInvTile;
+            for (int J = blockIdx.x; J < nt; J += gridDim.x) {
+                if (J == K) continue;
+                for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x)
+                    sa[o / kInvTile][o % kInvTile] = __ldcg(Tk + o);
+                ld_tile(sb, tile_at(K, J));
+                __syncthreads();
+                tile_mul(sa, sb, sc_, 1.0);
+                __syncthreads();
+                st_tile(tile_at(K, J), sc_);
+                __syncthreads();
+            }
+        }
+        if (!gsync()) goto fail;
+        // P3: W_IJ <- W_IJ - W_IK W_KJ
+        for (int x = blockIdx.x; x < nt * nt; x += gridDim.x) {
+            const int I = x / nt, J = x % nt;
+            if (I == K || J == K) continue;
+            ld_tile(sa, tile_at(I, K));
+            ld_tile(sb, tile_at(K, J));
+            __syncthreads();
+            tile_mul(sa, sb, sc_, 1.0);
+            __syncthreads();
+            double* dst = tile_at(I, J);
+            for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x) {
+                double* q = dst + (size_t)(o / kInvTile) * mp + o % kInvTile;
+                __stcg(q, __ldcg(q) - sc_[o / kInvTile][o % kInvTile]);
+            }
+            __syncthreads();
+        }
+        if (!gsync()) goto fail;
     }
     {
         const bool bad = *(volatile int*)ca.fail != 0;
         for (size_t q = gt; q < (size_t)m * m; q += gn) {
             const int i = (int)(q / m), j = (int)(q % m);
-            const double v = __ldcg(W + q) * __ldcg(sc + i) * __ldcg(sc + j);
+            const double v = __ldcg(W + (size_t)i * mp + j) * __ldcg(sc + i) * __ldcg(sc + j);
             ca.ainv[q] = (bad || !isfinite(v)) ? 0.0f : (float)v;
         }
     }
