@@ -1346,6 +1346,11 @@ private:
                        ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, kResidentMaxWidth, SYNC>)
                        : reinterpret_cast<const void*>(&pcg_resident_kernel<8, kResidentMaxWidth, SYNC>);
         }
+        if (coarse_on_ && coarse_dense_ && SYNC == 0) {
+            if (pcg_block_ == 128) return reinterpret_cast<const void*>(&pcg_persistent_kernel<128, 0, 1>);
+            if (pcg_block_ == 512) return reinterpret_cast<const void*>(&pcg_persistent_kernel<512, 0, 1>);
+            return reinterpret_cast<const void*>(&pcg_persistent_kernel<256, 0, 1>);
+        }
         if (pcg_block_ == 128) return reinterpret_cast<const void*>(&pcg_persistent_kernel<128, SYNC>);
         if (pcg_block_ == 512) return reinterpret_cast<const void*>(&pcg_persistent_kernel<512, SYNC>);
         return reinterpret_cast<const void*>(&pcg_persistent_kernel<256, SYNC>);

@@ -883,8 +883,8 @@ __device__ __forceinline__ void coarse_apply_dense(const BatchPlan& bp, int set,
 
 // ---------------------------------------------------------------------------
 // Streamed persistent kernel: rows are re-read from HBM every iteration.
-// Preconditioner: block-Jacobi, or (single instance, counter barrier, dense
-// coarse level planned) block-Jacobi plus the coarse correction
+// Preconditioner: block-Jacobi, or (CO = 1: single instance, counter
+// barrier, dense coarse level planned) block-Jacobi plus the coarse correction
 //     z = D^-1 r + R A_c^-1 R^T r,
 // a fixed symmetric positive-definite operator, so the outer iteration stays
 // plain PCG.  The coarse part of z rides on the existing phases: phase 1
@@ -892,7 +892,7 @@ __device__ __forceinline__ void coarse_apply_dense(const BatchPlan& bp, int set,
 // A_c^-1 R^T r - alpha A_c^-1 R^T A p and publishes R^T r_new beside the
 // dots, from which the next iteration's A_c^-1 R^T r restarts (no drift).
 // ---------------------------------------------------------------------------
-template <int BLOCK, int SYNC = 0>
+template <int BLOCK, int SYNC = 0, int CO = 0>
 __global__ void __launch_bounds__(BLOCK)
 pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP*, ZP*) {
     extern __shared__ double s_mem[];
@@ -908,9 +908,12 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
     const int nloc = il1 - il0 + 1;
     double* spart = s_mem;
     LocalInst* li = reinterpret_cast<LocalInst*>(s_mem + (size_t)bp.max_slices_per_cta * kSlotW);
-    // dense coarse level (uniform over the grid): off when the step's
-    // inversion failed
-    const bool coarse = !SYNC && bp.cg != nullptr && bp.cg->on && bp.cg->dense && *(volatile int*)bp.cg->fail == 0;
+    // dense coarse level (CO = 1 builds; uniform over the grid): off when
+    // the step's inversion failed.  The CO = 0 builds keep the block-Jacobi
+    // code alone, so both synchronisation modes compile to the same
+    // arithmetic (bit-identical iterates)
+    const bool coarse = CO && !SYNC && bp.cg != nullptr && bp.cg->on && bp.cg->dense &&
+                        *(volatile int*)bp.cg->fail == 0;
     const int c_nq = coarse ? bp.cg->nq : 1, c_U = 3 * c_nq;
     float* c_vbuf = reinterpret_cast<float*>(li + bp.max_inst_per_cta);
     unsigned target = 0;  // barrier target; the counter starts at 0 every solve

@@ -6,7 +6,8 @@ configuration (zero guess, rel-res 1e-6):
 * grid256: 256 x 256 plain-method configuration, two-level preconditioner
   (CTA-local Chebyshev of degree 7 on [lambda/60, lambda] plus the coarse
   level of translation and linear fields), spatially compact row order.
-* grid1024: 1024 x 1024 configuration, one step (streamed kernel).
+* grid1024: 1024 x 1024 configuration, its second step (streamed kernel,
+  block-Jacobi plus the coarse level, spatially compact row order).
 * batch: 16 instances of the batched configuration (sides U{16..128},
   seed 1) packed into one system and solved together.
 
@@ -147,21 +148,36 @@ def test_grid256_bench_configuration_steps_match_fp64_oracle():
 # system blocks of the 1024^2 step, FP32 (one rounding of an FP64 sum)
 # against the FP64 assembly, relative to the largest block
 TOL_BLOCK_REL = 2.0e-7
-# right-hand side: FP64 sums rounded once, |b| <= ~1e-6 N on this grid
+# right-hand side: FP64 sums rounded once (relative to the largest entry,
+# the pinned rows' ~15 N; measured 2.3e-7), plus 1e-11 N for the ~1e-6 N
+# loads of the free vertices
+TOL_RHS_REL = 1.0e-6
 TOL_RHS_ABS = 1.0e-11
-TOL_GRID1024_RESIDUAL = 10.0
+# the returned dx of a steady step (the second) in the FP64 system; the
+# first step from rest, whose load is gravity alone (~1e-6 N per vertex),
+# leaves the FP32 iterate at a true residual of order one
+TOL_GRID1024_RESIDUAL = 1.0e-3
 
 
 def test_grid1024_step_matches_fp64_oracle_system():
+    """The second step of grid1024 in the benchmarked configuration (streamed
+    kernel, block-Jacobi plus the coarse level, spatial order): the step's
+    system against the FP64 oracle's assembly from the same FP32 state, and
+    the returned dx in that FP64 system."""
     sc = scenes.config_huge(max_iter=100000)
     g = GpuCloth(sc, max_iter=100000, rel_tol=1e-6, warm_start="zero")
     g.sim.set_row_order(1)
+    g.sim.set_preconditioner("chebyshev_coarse", 7, 60.0)
     g.sim.set_true_residual(True)
+    g.step()
+    p0, v0 = g.positions().astype(np.float32), g.velocities().astype(np.float32)
     g.step()
     it, rr, st = g.stats()
     assert st == capi.SOLVE_CONVERGED and rr <= 1e-6
+    assert g.sim.solver_info()[0] == "streamed" and g.sim.preconditioner()[3] == 3
     diag, rp, col, vals, rhs, dx = g.dump()
-    o, _ = oracle_sim(sc, tol=0.0, max_iter=0)
+    o, im = oracle_sim(sc, tol=0.0, max_iter=0)
+    o.set_state(p0, v0, im)
     o.set_solver(0, 0.0, "zero")
     o.step(sc["dt"])  # assembles the step's system from the same state
     system = o.dump_system()
@@ -171,15 +187,11 @@ def test_grid1024_step_matches_fp64_oracle_system():
     scale = float(np.abs(od).max())
     assert float(np.abs(diag - od).max()) <= TOL_BLOCK_REL * scale
     assert float(np.abs(vals - ovals).max()) <= TOL_BLOCK_REL * scale
-    assert float(np.abs(rhs - orhs).max()) <= TOL_RHS_ABS
+    assert float(np.abs(rhs - orhs).max()) <= TOL_RHS_REL * float(np.abs(orhs).max()) + TOL_RHS_ABS
     res = fp64_residual(system, dx)
     floor = rounding_floor(system, dx)
-    print(f"grid1024: {it} iterations, residual in the FP64 system {res:.2e} (FP32 rounding floor {floor:.2e}, "
-          f"device true residual {g.sim.true_residual()[1]:.2e})")
-    # measured 6.5 (floor 2.9e-2): over the 43k block-Jacobi iterations of
-    # this first step the FP32 recurrence residual drifts far from the true
-    # one; this bounds that drift where it stands, it is not a convergence
-    # claim
+    print(f"grid1024 step 2: {it} iterations, residual in the FP64 system {res:.2e} (FP32 rounding floor "
+          f"{floor:.2e}, device true residual {g.sim.true_residual()[1]:.2e})")
     assert res < TOL_GRID1024_RESIDUAL
 
 
