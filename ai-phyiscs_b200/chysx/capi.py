@@ -447,7 +447,7 @@ class Cloth:
         level, or (info, None, None) when it is off."""
         info = np.zeros(6, np.int32)
         check(self._L.chysx_cloth_debug_coarse(self.h, _p(info, i32p), None, None, 0))
-        keys = ("on", "blocks", "ctas_per_block", "fields", "m", "band")
+        keys = ("on", "blocks", "ctas_per_block", "fields", "m", "unused")
         d = dict(zip(keys, (int(v) for v in info)))
         if not d["on"]:
             return d, None, None

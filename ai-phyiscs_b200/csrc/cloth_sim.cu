@@ -991,7 +991,7 @@ public:
             info[2] = coarse_g_;
             info[3] = coarse_nq_;
             info[4] = m;
-            info[5] = coarse_bw_;
+            info[5] = 0;  // no band: A_c is inverted densely
         }
         if (!coarse_on_ || (!ac && !ainv)) return;
         if (cap < m * m) throw std::invalid_argument("debug_coarse: cap below m * m");
@@ -1346,7 +1346,7 @@ private:
                        ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, kResidentMaxWidth, SYNC>)
                        : reinterpret_cast<const void*>(&pcg_resident_kernel<8, kResidentMaxWidth, SYNC>);
         }
-        if (coarse_on_ && coarse_dense_ && SYNC == 0) {
+        if (coarse_on_ && SYNC == 0) {
             if (pcg_block_ == 128) return reinterpret_cast<const void*>(&pcg_persistent_kernel<128, 0, 1>);
             if (pcg_block_ == 512) return reinterpret_cast<const void*>(&pcg_persistent_kernel<512, 0, 1>);
             return reinterpret_cast<const void*>(&pcg_persistent_kernel<256, 0, 1>);
@@ -1426,11 +1426,10 @@ private:
     // the coarse block of every slice and its first row, every block's sorted
     // list of the blocks its rows touch, and the list position of every ELL
     // entry's column block.
-    bool plan_coarse_with(int G, int nq, bool dense = false) {
+    bool plan_coarse_with(int G, int nq, double shift) {
         const int grid = plan_.grid, ns = topo_.n_slices;
         const int nb = (grid + G - 1) / G, U = 3 * nq, m = U * nb;
-        const int rpc = (m + grid - 1) / grid;
-        if (dense ? m > kCoarseDenseMax : (m > kCoarseThreads || rpc > kCoarseMaxRhs)) return false;
+        if (m > kCoarseDenseMax) return false;
         std::vector<int> slice_cb(std::max(1, ns), 0), row0(nb + 1, 0);
         for (int c = 0; c < grid; ++c)
             for (int sl = plan_.cta_slice[c]; sl < plan_.cta_slice[c + 1]; ++sl) slice_cb[sl] = c / G;
@@ -1447,67 +1446,6 @@ private:
         }
         int mn = 1;
         for (const auto& l : lists) mn = std::max(mn, (int)l.size());
-        // band order of the blocks (direct mode): reverse Cuthill-McKee (breadth-first from
-        // a block of least degree, neighbours by increasing degree, ties by
-        // index), then the band half-width in unknowns
-        std::vector<int> perm(nb, 0);
-        int bw = 0;
-        if (!dense) {
-            std::vector<int> order;
-            std::fill(perm.begin(), perm.end(), -1);
-            std::vector<char> seen(nb, 0);
-            auto degree = [&](int B) { return (int)lists[B].size(); };
-            while ((int)order.size() < nb) {
-                int start = -1;
-                for (int B = 0; B < nb; ++B)
-                    if (!seen[B] && (start < 0 || degree(B) < degree(start))) start = B;
-                // pseudo-peripheral start (George-Liu): from the last level of a
-                // breadth-first search, a block of least degree, while the
-                // eccentricity grows
-                for (int rep = 0, ecc = -1; rep < 8; ++rep) {
-                    std::vector<int> lev(nb, -1), q{start};
-                    lev[start] = 0;
-                    for (size_t h = 0; h < q.size(); ++h)
-                        for (int C : lists[q[h]])
-                            if (lev[C] < 0 && !seen[C]) {
-                                lev[C] = lev[q[h]] + 1;
-                                q.push_back(C);
-                            }
-                    const int e = lev[q.back()];
-                    if (e <= ecc) break;
-                    ecc = e;
-                    int best = -1;
-                    for (int C : q)
-                        if (lev[C] == e && (best < 0 || degree(C) < degree(best))) best = C;
-                    start = best;
-                }
-                seen[start] = 1;
-                size_t head = order.size();
-                order.push_back(start);
-                while (head < order.size()) {
-                    const int B = order[head++];
-                    std::vector<int> nx;
-                    for (int C : lists[B])
-                        if (!seen[C]) nx.push_back(C);
-                    std::sort(nx.begin(), nx.end(), [&](int a, int b) {
-                        return degree(a) != degree(b) ? degree(a) < degree(b) : a < b;
-                    });
-                    for (int C : nx) {
-                        seen[C] = 1;
-                        order.push_back(C);
-                    }
-                }
-            }
-            std::reverse(order.begin(), order.end());
-            for (int p = 0; p < nb; ++p) perm[order[p]] = p;
-            int bwb = 0;
-            for (int B = 0; B < nb; ++B)
-                for (int C : lists[B]) bwb = std::max(bwb, std::abs(perm[B] - perm[C]));
-            bw = std::min(m - 1, (bwb + 1) * U - 1);
-            const size_t direct_smem = ((size_t)m * (bw + 1) + 2 * (size_t)m + (size_t)rpc * m) * sizeof(float) +
-                                       (size_t)bw * (bw + 1) * sizeof(unsigned short);
-            if (direct_smem > kCoarseDirectSmemMax) return false;
-        }
         std::vector<int> nbr((size_t)nb * mn, -1), cnt(nb), self(nb);
         for (int B = 0; B < nb; ++B) {
             cnt[B] = (int)lists[B].size();
@@ -1529,8 +1467,6 @@ private:
         d_ccnt_.upload(cnt);
         d_cself_.upload(self);
         d_ell_nbr_.upload(ell);
-        d_cperm_.upload(perm);
-        coarse_bw_ = bw;
         if (nq > 1) {
             d_cw_.resize((size_t)std::max(1, row0[nb]));
             d_cw_.zero();
@@ -1539,8 +1475,7 @@ private:
         d_cac_.zero();
         d_cainv_.resize((size_t)m * m);
         d_cainv_.zero();
-        coarse_dense_ = dense;
-        if (dense) {
+        {
             const size_t mp = (size_t)(m + 31) / 32 * 32;  // kInvTile padding
             d_cwork_.resize(mp * mp + mp + 2 * 32 * 32);
             d_cfail_.resize(1);
@@ -1548,21 +1483,17 @@ private:
             d_cbar_.resize(1);
             d_cbar_.zero();
         }
+        coarse_shift_ = shift;
         coarse_nb_ = nb;
         coarse_mn_ = mn;
         coarse_g_ = G;
         coarse_nq_ = nq;
-        coarse_rpc_ = rpc;
         coarse_on_ = true;
         const CoarseArgs cargs = coarse_args();
         d_cargs_.upload(&cargs, 1);
         ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_assemble_kernel),
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_assemble_smem()),
            "cudaFuncSetAttribute(coarse assemble smem)");
-        if (!dense)
-            ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_direct_kernel),
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_direct_smem()),
-               "cudaFuncSetAttribute(coarse direct smem)");
         return true;
     }
     void plan_coarse() {
@@ -1576,27 +1507,19 @@ private:
             int G = std::max(1, (kCoarseStreamRows + rows_per_cta / 2) / rows_per_cta);
             while (G <= plan_.grid) {
                 const int nb = (plan_.grid + G - 1) / G;
-                if (nb >= 2 && plan_coarse_with(G, 4, true)) return;
+                if (nb >= 2 && plan_coarse_with(G, 4, kCoarseShift)) return;
                 if (nb < 2) return;
                 ++G;
             }
             return;
         }
         if (plan_.grid > kCoarseMaxBlocks) return;
-        if (plan_.grid >= 8 && plan_coarse_with(4, 4)) return;
-        plan_coarse_with(1, 1);
+        if (plan_.grid >= 8 && plan_coarse_with(4, 4, 0.0)) return;
+        plan_coarse_with(1, 1, 0.0);
     }
     // per-lane partial sums of the coarse assembly: [nq][9][max_nbr][32] floats
     size_t coarse_assemble_smem() const {
         return (size_t)coarse_nq_ * 9 * coarse_mn_ * 32 * sizeof(float);
-    }
-    // dynamic shared memory of the coarse direct kernel: the FP32 band of
-    // A_c, the scaling and the right-hand sides (below the 227 KB of a CTA)
-    static constexpr size_t kCoarseDirectSmemMax = 220 * 1024;
-    size_t coarse_direct_smem() const {
-        const size_t m = 3 * (size_t)coarse_nq_ * coarse_nb_;
-        return (m * (coarse_bw_ + 1) + 2 * m + (size_t)coarse_rpc_ * m) * sizeof(float) +
-               (size_t)coarse_bw_ * (coarse_bw_ + 1) * sizeof(unsigned short);
     }
     CoarseArgs coarse_args() const {
         CoarseArgs c{};
@@ -1605,7 +1528,6 @@ private:
         c.g = coarse_g_;
         c.nq = coarse_nq_;
         c.m = 3 * coarse_nq_ * coarse_nb_;
-        c.rpc = coarse_rpc_;
         c.max_nbr = coarse_mn_;
         c.slice_cb = d_slice_cb_.get();
         c.cb_row0 = d_cb_row0_.get();
@@ -1613,14 +1535,13 @@ private:
         c.nbr_cnt = d_ccnt_.get();
         c.self_idx = d_cself_.get();
         c.ell_nbr = d_ell_nbr_.get();
-        c.perm = d_cperm_.get();
-        c.bw = coarse_bw_;
         c.w = coarse_nq_ > 1 ? d_cw_.get() : nullptr;
         c.ac = d_cac_.get();
         c.ainv = d_cainv_.get();
-        c.dense = coarse_dense_ ? 1 : 0;
-        c.work = coarse_dense_ ? d_cwork_.get() : nullptr;
-        c.fail = coarse_dense_ ? d_cfail_.get() : nullptr;
+        c.dense = resident_ ? 0 : 1;
+        c.shift = coarse_shift_;
+        c.work = d_cwork_.get();
+        c.fail = d_cfail_.get();
         return c;
     }
 
@@ -1859,16 +1780,7 @@ private:
             p.kernelParams = a1;
             cudaGraphNode_t n1, n2;
             ck(cudaGraphAddKernelNode(&n1, graph_, &prev, 1, &p), "add coarse assemble node");
-            if (!coarse_dense_) {
-                void* a2[] = {&cg};
-                cudaKernelNodeParams p2{};
-                p2.func = reinterpret_cast<void*>(&coarse_direct_kernel);
-                p2.gridDim = dim3(plan_.grid);
-                p2.blockDim = dim3(kCoarseThreads);
-                p2.sharedMemBytes = (unsigned)coarse_direct_smem();
-                p2.kernelParams = a2;
-                ck(cudaGraphAddKernelNode(&n2, graph_, &n1, 1, &p2), "add coarse direct node");
-            } else {
+            {
                 // zero the inversion's barrier and failure flag, then invert
                 cudaGraphNode_t z1, z2;
                 cudaMemsetParams mp{};
@@ -2179,13 +2091,13 @@ private:
     int sync_mode_ = 0;    // 0 grid counter barrier, 1 polled per-instance slots
     int pc_kind_ = 0, pc_degree_ = 0;  // preconditioner: 0 block-Jacobi, 1 CTA-local Chebyshev, 2 + coarse level
     bool coarse_on_ = false;
-    int coarse_nb_ = 0, coarse_mn_ = 0, coarse_g_ = 1, coarse_nq_ = 1, coarse_rpc_ = 1, coarse_bw_ = 0;
-    DevBuf<int> d_slice_cb_, d_cb_row0_, d_cnbr_, d_ccnt_, d_cself_, d_cperm_;
+    int coarse_nb_ = 0, coarse_mn_ = 0, coarse_g_ = 1, coarse_nq_ = 1;
+    double coarse_shift_ = 0.0;
+    DevBuf<int> d_slice_cb_, d_cb_row0_, d_cnbr_, d_ccnt_, d_cself_;
     DevBuf<unsigned char> d_ell_nbr_;
     DevBuf<float4> d_cw_;
     DevBuf<CoarseArgs> d_cargs_;  // the coarse arguments the PCG kernel reads (BatchPlan holds the pointer)
     DevBuf<float> d_cac_, d_cainv_;
-    bool coarse_dense_ = false;  // streamed kernel's coarse level: dense A_c^-1 formed each step
     DevBuf<double> d_cwork_;
     DevBuf<int> d_cfail_;
     DevBuf<GridBarrier> d_cbar_;

@@ -12,8 +12,8 @@
 // positive-definite operator, so the outer iteration stays plain PCG.  Per
 // step: coarse_fields_kernel (the weights), coarse_assemble_kernel (one CTA
 // per block and field pair, deterministic per-lane partial sums added in
-// lane order) and coarse_direct_kernel (every CTA factors A_c and solves
-// for its rows of A_c^-1); per iteration the resident kernel forms its
+// lane order) and coarse_invert_kernel (A_c^-1 densely, FP64 blocked
+// Gauss-Jordan across the grid); per iteration the resident kernel forms its
 // block of A_c^-1 R^T r from the blocks' restricted residuals, which ride on
 // the existing reduction slots.
 #pragma once
@@ -224,162 +224,9 @@ __global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, CoarseA
     }
 }
 
-// Rows blockIdx.x * rpc + j (j < rpc) of A_c^-1 by a direct solve: every
-// CTA factors A_c (band storage in shared memory, FP32, blocks in the band
-// order perm, symmetric diagonal scaling D^-1/2 A_c D^-1/2) by a
-// column-oriented band Cholesky and solves L L^T y = D^-1/2 e_r for its rows;
-// A_c^-1 e_r = D^-1/2 y.  Unknowns of a field of weight 0 everywhere (a
-// dropped axis) have a zero diagonal and get identity rows; a non-positive
-// pivot leaves zero rows (the coarse level then adds nothing this step).
-// The factorisation is the same in every CTA (same operations, same order),
-// so all CTAs agree bitwise.  Dynamic shared memory: (m (bw + 1) + 2 m +
-// rpc m) floats and bw (bw + 1) / 2 pairs of the trailing update's
-// (row, column) offsets.
-__global__ void __launch_bounds__(kCoarseThreads) coarse_direct_kernel(CoarseArgs ca) {
-    extern __shared__ float cd_mem[];
-    __shared__ int s_fail;
-    const int nb = ca.nb, mn = ca.max_nbr, U = 3 * ca.nq, m = ca.m, bw = ca.bw, W1 = bw + 1, rpc = ca.rpc;
-    const int t = threadIdx.x, nt = blockDim.x;
-    float* L = cd_mem;                   // [m][W1]: L[i W1 + k] = entry (i, i - k)
-    float* dsc = L + (size_t)m * W1;     // [m] 1 / sqrt(A_ii)
-    float* dinv = dsc + m;               // [m] 1 / L_ii
-    float* y = dinv + m;                 // [rpc][m] right-hand sides / solutions, band order
-    // the trailing update's pairs (a, b), b <= a < bw, in row-major order:
-    // the first c (c + 1) / 2 are those of a column with c rows below it
-    unsigned short* pab = reinterpret_cast<unsigned short*>(y + (size_t)rpc * m);
-    for (int a = t; a < bw; a += nt)
-        for (int b = 0; b <= a; ++b) {
-            const int x = a * (a + 1) / 2 + b;
-            pab[2 * x] = (unsigned short)a;
-            pab[2 * x + 1] = (unsigned short)b;
-        }
-    if (t == 0) s_fail = 0;
-    for (int x = t; x < m * W1; x += nt) L[x] = 0.0;
-    __syncthreads();
-    const int bsz = mn * U * U;
-    for (int x = t; x < nb * bsz; x += nt) {
-        const int B = x / bsz, rem = x % bsz, k = rem / (U * U), e = rem % (U * U);
-        if (k >= ca.nbr_cnt[B]) continue;
-        const int C = ca.nbr[B * mn + k];
-        const int pi = ca.perm[B] * U + e / U, pj = ca.perm[C] * U + e % U;
-        if (pj > pi) continue;  // the lower triangle (A_c symmetric)
-        L[(size_t)pi * W1 + (pi - pj)] = ca.ac[x];
-    }
-    __syncthreads();
-    for (int i = t; i < m; i += nt) {
-        float d = L[(size_t)i * W1];
-        if (!(d > 0.0f)) {  // a dropped field: identity row (its other entries are zero)
-            d = 1.0f;
-            L[(size_t)i * W1] = 1.0f;
-        }
-        dsc[i] = rsqrtf(d);
-    }
-    __syncthreads();
-    for (int x = t; x < m * W1; x += nt) {
-        const int i = x / W1, k = x % W1;
-        if (i - k >= 0) L[x] *= dsc[i] * dsc[i - k];
-    }
-    __syncthreads();
-    // blocked band Cholesky: panels of kPanel columns factored by warp 0
-    // (column by column, the panel's later columns updated as it goes),
-    // then one rank-kPanel update of the trailing band by the whole CTA
-    constexpr int kPanel = 4;
-    const int warp = t >> 5, lane = t & 31;
-    for (int j0 = 0; j0 < m; j0 += kPanel) {
-        const int pw = min(kPanel, m - j0);
-        if (warp == 0) {
-            for (int j = j0; j < j0 + pw; ++j) {
-                const float ajj = L[(size_t)j * W1];
-                const bool piv = ajj > 1e-30f;
-                const float ljj = piv ? sqrtf(ajj) : 1.0f, inv = 1.0f / ljj;
-                __syncwarp();
-                if (lane == 0) {
-                    L[(size_t)j * W1] = ljj;
-                    if (!piv) s_fail = 1;
-                }
-                const int hi = min(m - 1, j + bw);
-                for (int i = j + 1 + lane; i <= hi; i += 32) L[(size_t)i * W1 + (i - j)] *= inv;
-                __syncwarp();
-                for (int k = j + 1; k < j0 + pw && k - j <= bw; ++k) {  // L_kj = 0 beyond the band
-                    const float lkj = L[(size_t)k * W1 + (k - j)];
-                    for (int i = k + lane; i <= hi; i += 32) L[(size_t)i * W1 + (i - k)] -= L[(size_t)i * W1 + (i - j)] * lkj;
-                }
-                __syncwarp();
-            }
-        }
-        __syncthreads();
-        // rows i = base + a, columns k = base + b (b <= a): L_ik -= sum over the
-        // panel's columns p within the band of row i of L_ip L_kp
-        const int base = j0 + pw, hi = min(m - 1, j0 + pw - 1 + bw), cnt = hi - base + 1;
-        if (cnt > 0) {
-            const int np = cnt * (cnt + 1) / 2;
-#pragma unroll 2
-            for (int x = t; x < np; x += nt) {
-                const int a = pab[2 * x], b = pab[2 * x + 1];
-                const int i = base + a, k = base + b;
-                const float* Li = L + (size_t)i * W1;
-                const float* Lk = L + (size_t)k * W1;
-                float sum = 0.0f;
-#pragma unroll
-                for (int p = 0; p < kPanel; ++p) {
-                    const int col = j0 + p;
-                    if (p < pw && i - col <= bw) sum = fmaf(Li[i - col], Lk[k - col], sum);
-                }
-                L[(size_t)i * W1 + (a - b)] -= sum;
-            }
-        }
-        __syncthreads();
-    }
-    for (int i = t; i < m; i += nt) dinv[i] = 1.0f / L[(size_t)i * W1];
-    // this CTA's rows r = blockIdx.x rpc + s: right-hand side D^-1/2 e_r in band order
-    const int r0 = blockIdx.x * rpc;
-    for (int x = t; x < rpc * m; x += nt) y[x] = 0.0f;
-    __syncthreads();
-    if (t < rpc && r0 + t < m) {
-        const int r = r0 + t, pr = ca.perm[r / U] * U + r % U;
-        y[(size_t)t * m + pr] = dsc[pr];
-    }
-    __syncthreads();
-    // the triangular solves: warp sr takes right-hand side sr (the band's
-    // entries of a column across its lanes); forward L z = b column by
-    // column, then backward L^T y = z
-    const int sr = t >> 5, ln = t & 31;
-    if (sr < rpc) {
-        float* ys = y + (size_t)sr * m;
-        for (int j = 0; j < m; ++j) {
-            const int cnt = min(m - 1, j + bw) - j;
-            const float yj = ys[j] * dinv[j];
-#pragma unroll 4
-            for (int q = 1 + ln; q <= cnt; q += 32) ys[j + q] -= L[(size_t)(j + q) * W1 + q] * yj;
-            __syncwarp();
-            if (ln == 0) ys[j] = yj;
-            __syncwarp();
-        }
-        for (int i = m - 1; i >= 0; --i) {
-            const int lo = max(0, i - bw);
-            const float yi = ys[i] * dinv[i];
-#pragma unroll 4
-            for (int k = lo + ln; k < i; k += 32) ys[k] -= L[(size_t)i * W1 + (i - k)] * yi;
-            __syncwarp();
-            if (ln == 0) ys[i] = yi;
-            __syncwarp();
-        }
-    }
-    __syncthreads();
-    // rows of A_c^-1 in the original unknown order: A_c^-1[r][q] = dsc_q y[p(q)]
-    for (int x = t; x < rpc * m; x += nt) {
-        const int s = x / m, q = x % m;
-        if (r0 + s >= m) continue;
-        const int pq = ca.perm[q / U] * U + q % U;
-        const float v = dsc[pq] * y[(size_t)s * m + pq];
-        ca.ainv[(size_t)(r0 + s) * m + q] = (s_fail || !isfinite(v)) ? 0.0f : v;
-    }
-}
-
-
-// Dense inverse of A_c for the streamed kernel's coarse level (m <=
+// Dense inverse of A_c for both two-level preconditioners (m <=
 // kCoarseDenseMax): FP64 blocked Gauss-Jordan elimination in place on the
-// symmetrically scaled and shifted matrix S A_c S + kCoarseShift I
+// symmetrically scaled and shifted matrix S A_c S + ca.shift I
 // (S = diag(A_c)^-1/2), padded to a multiple of 32 with identity rows, no
 // pivoting (the shifted matrix is symmetric positive definite; an unknown
 // whose field has zero weight on its whole block has an empty row and column
@@ -456,7 +303,7 @@ __global__ void __launch_bounds__(kCoarseInvertThreads) coarse_invert_kernel(Coa
         const int i = (int)(q / mp), j = (int)(q % mp);
         const double si = __ldcg(sc + i), sj = __ldcg(sc + j);
         __stcg(W + q, si == 0.0 || sj == 0.0 ? (i == j ? 1.0 : 0.0)
-                                             : __ldcg(W + q) * si * sj + (i == j ? kCoarseShift : 0.0));
+                                             : __ldcg(W + q) * si * sj + (i == j ? ca.shift : 0.0));
     }
     if (!gsync()) goto fail;
     for (int K = 0; K <= nt; ++K) {

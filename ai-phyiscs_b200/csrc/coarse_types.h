@@ -6,16 +6,15 @@ namespace chysx_b200 {
 
 constexpr int kCoarseMaxBlocks = 160;  // CTAs of a two-level plan (one warp's slot pass)
 constexpr int kCoarseMaxNbr = 16;      // coarse blocks one block's rows touch, itself included
-constexpr int kCoarseThreads = 512;    // threads of the coarse direct solve; also the bound on the coarse unknowns
-constexpr int kCoarseMaxRhs = 4;       // rows of A_c^-1 one CTA computes
 // The streamed kernel's coarse level (systems too large for the register-
 // resident kernel): coarse blocks of about kCoarseStreamRows rows, at most
 // kCoarseDenseMax unknowns, A_c inverted densely once per step
 constexpr int kCoarseStreamRows = 8192;
 constexpr int kCoarseDenseMax = 2048;
 constexpr int kCoarseInvertThreads = 256;
-// Relative diagonal shift of the dense-mode coarse matrix: A_c + shift
-// diag(A_c) is inverted instead of A_c.  The coarse matrix of a flat,
+// Relative diagonal shift of the streamed kernel's coarse matrix: A_c +
+// shift diag(A_c) is inverted instead of A_c (the resident kernel's coarse
+// matrix, on smaller blocks, is inverted unshifted).  The coarse matrix of a flat,
 // unstretched cloth (the first step from rest) has out-of-plane modes held
 // only by inertia, with a scaled condition number ~1e7 on the 1024 x 1024
 // grid; an FP32 inverse and FP32 restrictions of such a matrix are not a
@@ -35,7 +34,6 @@ struct CoarseArgs {
     int g = 1;                                // CTAs per coarse block
     int nq = 1;                               // fields per coarse block (1 or 4)
     int m = 0;                                // coarse unknowns, 3 nq nb
-    int rpc = 0;                              // rows of A_c^-1 per CTA (ceil(m / CTAs))
     int max_nbr = 0;                          // block entries per block row of A_c
     const int* slice_cb = nullptr;            // [n_slices] coarse block of every slice
     const int* cb_row0 = nullptr;             // [nb + 1] first internal row of every coarse block
@@ -43,16 +41,16 @@ struct CoarseArgs {
     const int* nbr_cnt = nullptr;             // [nb]
     const int* self_idx = nullptr;            // [nb] position of the block itself in its list
     const unsigned char* ell_nbr = nullptr;   // [ELL entries] list position of the entry's column block
-    const int* perm = nullptr;                // [nb] band position of every block (reverse Cuthill-McKee)
-    int bw = 0;                               // band half-width of A_c in unknowns, block order perm
     float4* w = nullptr;                      // [rows] linear-field weights s_1, s_2, s_3 (nq = 4)
     float* ac = nullptr;                      // [nb][max_nbr][U][U] A_c, row-major U x U blocks
-    float* ainv = nullptr;                    // [m][m] rows of A_c^-1 (rows r..r+rpc by CTA r / rpc)
-    // dense mode (streamed kernel): A_c^-1 in full, formed by
-    // coarse_invert_kernel in the FP64 workspace (m * m + m doubles); fail != 0
+    float* ainv = nullptr;                    // [m][m] A_c^-1 (row-major)
+    // A_c^-1 is formed by coarse_invert_kernel in the FP64 workspace
+    // (padded m * m + m + 2048 doubles) from A_c + shift diag(A_c); fail != 0
     // after a step whose inversion met a non-positive pivot or a failed wait
-    // (the coarse level then adds nothing in that step's solve)
+    // (the coarse level then adds nothing in that step's solve); dense = 1:
+    // the streamed kernel's level (its CTAs read their rows from L2)
     int dense = 0;
+    double shift = 0.0;
     double* work = nullptr;
     int* fail = nullptr;
 };

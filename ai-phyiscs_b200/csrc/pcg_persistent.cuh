@@ -1381,7 +1381,7 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     // behind the LocalInst records; every row's field weights in a register
     // quad.  Warps 1..3 form this block of A_c^-1 R^T v during the phases.
     constexpr bool kCoarse = PC == 2;
-    const bool coarse = kCoarse && bp.cg != nullptr && bp.cg->on;
+    const bool coarse = kCoarse && bp.cg != nullptr && bp.cg->on && *(volatile int*)bp.cg->fail == 0;
     const int c_nq = coarse ? bp.cg->nq : 1, c_U = 3 * c_nq;
     float* c_ainv = reinterpret_cast<float*>(li + bp.max_inst_per_cta);
     // staged coarse values of a phase ([slots][U]), behind c_ainv (16-byte aligned)

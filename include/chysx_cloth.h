@@ -269,9 +269,11 @@ int chysx_cloth_debug_dump(chysx_cloth* h, float* diag, int32_t* row_offsets,
                            int32_t* col_indices, float* values, float* rhs, float* dx);
 /* The two-level preconditioner's coarse level of the last step (test
  * support, no counterpart in the reference): info[6] = {in use, coarse
- * blocks, CTAs per block, fields per block, unknowns m, band half-width};
+ * blocks, CTAs per block, fields per block, unknowns m, 0};
  * with ac / ainv non-null (host, m * m floats each, cap >= m * m) the coarse
- * matrix A_c dense and the rows of A_c^-1 the CTAs computed, unknown
+ * matrix A_c dense and the inverse the solver used (of A_c + shift
+ * diag(A_c), shift 0 on the register-resident kernel, 1e-5 on the streamed
+ * one), unknown
  * index block * 3 * fields + 3 * field + component.  Synchronises. */
 int chysx_cloth_debug_coarse(chysx_cloth* h, int32_t* info, float* ac, float* ainv, int cap);
 
