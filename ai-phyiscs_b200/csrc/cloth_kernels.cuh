@@ -480,7 +480,10 @@ namespace chysx_b200 {
 // which in FP32 keeps the inertia that the full diagonal (stored in t.diag
 // for the Jacobi inverse and the debug dump) cannot resolve.
 // ---------------------------------------------------------------------------
-template <int BLOCK>
+// COND = 1: the graph-loop build, which sets the WHILE node's condition for
+// an already-converged zero-guess start; the persistent path launches the
+// COND = 0 build, free of the device graph API.
+template <int BLOCK, int COND>
 __global__ void __launch_bounds__(BLOCK)
 assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, double* part,
                 SolverCfg cfg, int zero_guess, cudaGraphConditionalHandle cond) {
@@ -698,7 +701,7 @@ assemble_kernel(StepArgs a, ElemData el, DevTopo t, Vecs v, SolveState* st, doub
             const bool conv = cfg.use_tol && bb <= st->tol2;
             st->status = bad ? kSolveNonfinite : kSolveConverged;
             st->done = (bad || conv || cfg.max_iter <= 0) ? 1 : 0;
-            if (cond) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
+            if (COND && cond) cudaGraphSetConditional(cond, st->done ? 0u : 1u);
         } else {
             st->status = finite_d(bb) ? kSolveConverged : kSolveNonfinite;
             st->done = 0;

@@ -1243,10 +1243,17 @@ private:
         return c;
     }
 
+    // the graph-loop path needs the build that sets the WHILE condition
     const void* assemble_fn() const {
-        if (asm_block_ == 128) return reinterpret_cast<const void*>(&assemble_kernel<128>);
-        if (asm_block_ == 64) return reinterpret_cast<const void*>(&assemble_kernel<64>);
-        return reinterpret_cast<const void*>(&assemble_kernel<32>);
+        const bool loop = solver_path_ == kPathLoop;
+        if (asm_block_ == 128)
+            return loop ? reinterpret_cast<const void*>(&assemble_kernel<128, 1>)
+                        : reinterpret_cast<const void*>(&assemble_kernel<128, 0>);
+        if (asm_block_ == 64)
+            return loop ? reinterpret_cast<const void*>(&assemble_kernel<64, 1>)
+                        : reinterpret_cast<const void*>(&assemble_kernel<64, 0>);
+        return loop ? reinterpret_cast<const void*>(&assemble_kernel<32, 1>)
+                    : reinterpret_cast<const void*>(&assemble_kernel<32, 0>);
     }
 
     void asm_params(cudaKernelNodeParams& p, void** args) {
