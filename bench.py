@@ -589,11 +589,14 @@ def run_ours(args, rank, world, local_rank):
     achieved = float(np.sum(moved) / (np.sum(solve_ms) * 1e-3) / 1e9)
     achieved_ref = float(np.sum(moved_ref) / (np.sum(solve_ms) * 1e-3) / 1e9)
     peak, peak_kind = read_peaks()
-    # the ncu summary of the kernel variant that ran (resident kernels: by
-    # preconditioner in use)
+    # the ncu summary of the kernel variant that ran (by preconditioner in
+    # use)
     kern = g.sim.solver_info()[0]
+    in_use = int(g.sim.preconditioner()[3])
     if kern == "resident":
-        kern += {0: "", 1: "_chebyshev", 2: "_twolevel", 3: "_twolevel_linear"}[int(g.sim.preconditioner()[3])]
+        kern += {0: "", 1: "_chebyshev", 2: "_twolevel", 3: "_twolevel_linear"}[in_use]
+    elif kern == "streamed" and in_use >= 2:
+        kern += "_twolevel"
     traffic_it = read_traffic(kern, args.workload)
     steps_total = args.steps * world
     value = steps_total / (total_ms_max * 1e-3)
