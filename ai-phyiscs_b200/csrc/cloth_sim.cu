@@ -1410,9 +1410,9 @@ private:
             build_plan(topo_.inst_slice, grid, plan_);
             plan_coarse();
             pers_smem_ = (size_t)W * kSlotW * sizeof(double) + (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
-            if (coarse_on_)  // the coarse block's rows of A_c^-1, the staged coarse values of a phase
-                pers_smem_ += ((size_t)9 * coarse_nq_ * coarse_nq_ * coarse_nb_ + 3 * coarse_nq_ * (size_t)plan_.grid) *
-                                  sizeof(float) + 16;
+            if (coarse_on_)  // the coarse block's rows of A_c^-1, a phase's block values and its staged slots
+                pers_smem_ += ((size_t)9 * coarse_nq_ * coarse_nq_ * coarse_nb_ + (size_t)3 * coarse_nq_ * coarse_nb_) *
+                                  sizeof(float) + 16 + (size_t)plan_.inst_slot.back() * kSlotW * sizeof(double) + 16;
             // static + dynamic above 48 KB needs the opt-in
             ck(cudaFuncSetAttribute(persistent_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pers_smem_),
                "cudaFuncSetAttribute(resident smem)");
@@ -1428,8 +1428,10 @@ private:
     // Coarse level of the two-level preconditioner (kind 2) of a
     // single-instance resident plan: coarse blocks of G consecutive CTAs with
     // nq fields each; (G, nq) = (4, 4) (translation and linear fields on
-    // 4-CTA blocks) where its coarse system fits the inverse kernel's shared
-    // memory, else (1, 1) (the translation of every CTA block).  Host side:
+    // 4-CTA blocks) where the plan has at least 8 CTAs and the coarse system
+    // at most kCoarseDenseMax unknowns, else (1, 1) (the translation of
+    // every CTA block).  The streamed kernel's blocks are larger (about
+    // kCoarseStreamRows rows).  Host side:
     // the coarse block of every slice and its first row, every block's sorted
     // list of the blocks its rows touch, and the list position of every ELL
     // entry's column block.
@@ -1605,7 +1607,7 @@ private:
         const size_t li_bytes = (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
         size_t need = resident_ ? (size_t)resident_warps_ * kSlotW * sizeof(double) + li_bytes
                                 : (size_t)plan_.max_slices_per_cta * kSlotW * sizeof(double) + li_bytes;
-        if (!resident_ && coarse_on_) need += (size_t)3 * coarse_nq_ * coarse_nb_ * sizeof(float);
+        if (!resident_ && coarse_on_) need += (size_t)3 * coarse_nq_ * coarse_nb_ * sizeof(float) + 16;
         if (pers_smem_ < need || (resident_ && plan_.max_slices_per_cta > resident_warps_) ||
             (!resident_ && pcg_block_ / 32 < 1))
             throw std::logic_error("persistent PCG plan is inconsistent with the selected kernel");

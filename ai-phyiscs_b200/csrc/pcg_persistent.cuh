@@ -388,6 +388,27 @@ __device__ __forceinline__ bool warp0_phase(const BatchPlan& bp, const double* s
 }
 
 // ---- coarse level of a single-instance two-level plan (counter barrier) --
+// Its parameters, read once per solve (into registers, or shared memory
+// where registers are short): every grid barrier ends in an acquire, which
+// invalidates L1, so a field read through bp.cg after a barrier would put an
+// L2 round trip on the phase's critical path.
+struct CoarseRegs {
+    const float* ainv;  // [blocks][U][m] rows of A_c^-1
+    const float4* w;    // per-row field weights (nq = 4)
+    int nq, U, G, m;    // fields, values per block, CTAs per block, unknowns
+};
+__device__ __forceinline__ CoarseRegs coarse_regs(const BatchPlan& bp, bool on) {
+    CoarseRegs c{nullptr, nullptr, 1, 3, 1, 0};
+    if (on) {
+        c.ainv = bp.cg->ainv;
+        c.w = bp.cg->w;
+        c.nq = bp.cg->nq;
+        c.U = 3 * bp.cg->nq;
+        c.G = bp.cg->g;
+        c.m = bp.cg->m;
+    }
+    return c;
+}
 // Coarse values of a phase sit in slot entries kCoarseOff.. of every CTA;
 // coarse block C's value is the sum over its CTAs C G .. C G + G - 1.
 
@@ -437,9 +458,9 @@ __device__ __forceinline__ float* coarse_slot(const BatchPlan& bp, int set, int 
 
 // The CTA's coarse values (lane q < U: the sum over the CTA's nsl slices'
 // partials, in slice order) into its slot of `set` (warp 1).
-__device__ __forceinline__ void warp1_coarse_publish(const BatchPlan& bp, const float* cpart, int nsl, int own_slot,
-                                                     int set) {
-    const int lane = threadIdx.x & 31, U = 3 * bp.cg->nq;
+__device__ __forceinline__ void warp1_coarse_publish(const BatchPlan& bp, int U, const float* cpart, int nsl,
+                                                     int own_slot, int set) {
+    const int lane = threadIdx.x & 31;
     if (lane < U) {
         float acc = 0.0f;
         for (int w = 0; w < nsl; ++w) acc += cpart[w * kCoarsePartW + lane];
@@ -447,47 +468,68 @@ __device__ __forceinline__ void warp1_coarse_publish(const BatchPlan& bp, const 
     }
 }
 
-// The coarse values of every slot of `set` into stage[k * U + u] (floats),
-// by the warps 1.. of the CTA together (one float4 per thread for up to
-// 160 slots of 12 values on 15 warps).
-__device__ __forceinline__ void coarse_stage(const BatchPlan& bp, int set, int U, int tid, int nthreads, float* stage) {
-    if (U % 4 == 0) {
-        const int per = U / 4, total = bp.n_slots * per;
-        for (int x = tid; x < total; x += nthreads)
-            reinterpret_cast<float4*>(stage)[x] =
-                __ldcg(reinterpret_cast<const float4*>(coarse_slot(bp, set, x / per)) + x % per);
-    } else {
-        const int total = bp.n_slots * U;
-        for (int x = tid; x < total; x += nthreads) stage[x] = __ldcg(coarse_slot(bp, set, x / U) + x % U);
+// The whole slot set `set` (n_slots x kSlotW doubles: the scalars, then the
+// coarse floats at kCoarseOff) into shared memory, one 16-byte load per
+// thread and pass; called by every thread of the CTA.
+__device__ __forceinline__ void coarse_stage_slots(const BatchPlan& bp, int set, double* dst) {
+    constexpr int kPer = kSlotW / 2;  // 16-byte pieces per slot
+    const float4* src = reinterpret_cast<const float4*>(bp.slots + (size_t)set * bp.n_slots * kSlotW);
+    float4* d = reinterpret_cast<float4*>(dst);
+    for (int x = threadIdx.x; x < bp.n_slots * kPer; x += blockDim.x) d[x] = __ldcg(src + x);
+}
+
+// Scalar totals of the single instance from the staged slots (warp 0):
+// lane l adds the slots l, l + 32, ... in ascending order, then the xor
+// tree, so the totals equal those of warp0_read_totals; lane 0 applies
+// `step`.
+template <int NR, class Step>
+__device__ __forceinline__ void warp0_staged_totals(LocalInst* li, const double* slots, Step&& step) {
+    const int lane = threadIdx.x & 31;
+    LocalInst& L = li[0];
+    if (L.done) return;
+    double tot[NR];
+#pragma unroll
+    for (int q = 0; q < NR; ++q) tot[q] = 0.0;
+    for (int k = L.slot_lo + lane; k < L.slot_hi; k += 32) {
+#pragma unroll
+        for (int q = 0; q < NR; ++q) tot[q] += slots[(size_t)k * kSlotW + q];
+    }
+#pragma unroll
+    for (int q = 0; q < NR; ++q) tot[q] = warp_sum(tot[q]);
+    if (lane == 0) step(L, tot);
+    __syncwarp();
+}
+
+// Every coarse block's values v[B * U + u] (floats) from the staged slots:
+// the sum of its G CTAs' coarse floats, added in slot order (threads tid
+// of nthreads).
+__device__ __forceinline__ void coarse_block_values(const double* slots, int n_slots, int U, int G, int m, int tid,
+                                                    int nthreads, float* v) {
+    const float* f = reinterpret_cast<const float*>(slots) + 2 * kCoarseOff;
+    for (int j = tid; j < m; j += nthreads) {
+        const int B = j / U, u = j - B * U;
+        const int c1 = min((B + 1) * G, n_slots);
+        float acc = 0.0f;
+        for (int c = B * G; c < c1; ++c) acc += f[(size_t)c * 2 * kSlotW + u];
+        v[j] = acc;
     }
 }
 
-// Row r of this CTA's block of A_c^-1 v, v the staged coarse values; lane 0
-// writes it to out[r].  A coarse block's value is the sum of its CTAs' slots
-// and the product is linear, so lane l takes the slots l, l + 32, ...
-// directly (each against its block's columns of row r of A_c^-1, [U][m]).
-template <int U>
-__device__ __forceinline__ void warp_coarse_row(const BatchPlan& bp, const float* stage, const float* ainv, int r,
-                                                float* out) {
-    const int lane = threadIdx.x & 31, G = bp.cg->g;
-    const float* arow = ainv + (size_t)r * bp.cg->m;
+// Row r of this CTA's block of A_c^-1 v (v the m staged block values, row r
+// of A_c^-1 at ainv + r m); lane 0 writes it to out[r].  Lanes take
+// consecutive entries (conflict-free shared-memory reads).
+__device__ __forceinline__ void warp_coarse_row(int m, const float* v, const float* ainv, int r, float* out) {
+    const int lane = threadIdx.x & 31;
+    const float* arow = ainv + (size_t)r * m;
     float acc = 0.f;
-    for (int k = lane; k < bp.n_slots; k += 32) {
-        const float* v = stage + k * U;
-        const float* a = arow + (k / G) * U;
-#pragma unroll
-        for (int u = 0; u < U; ++u) acc = fmaf(a[u], v[u], acc);
-    }
+#pragma unroll 4
+    for (int j = lane; j < m; j += 32) acc = fmaf(arow[j], v[j], acc);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) out[r] = acc;
 }
 
 __device__ __forceinline__ void named_barrier_w01() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
-// the whole CTA: warp 0 passes it after the grid barrier
-__device__ __forceinline__ void named_barrier_coarse(int nthreads) {
-    asm volatile("bar.sync 2, %0;" ::"r"(nthreads) : "memory");
-}
 // warps 1.. alone: the staged values are complete
 __device__ __forceinline__ void named_barrier_stage(int nthreads) {
     asm volatile("bar.sync 3, %0;" ::"r"(nthreads) : "memory");
@@ -786,11 +828,13 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
 // the NR scalars (spart entries 0..NR-1), warp 1 the coarse values (floats
 // from the per-slice coarse partials), both before warp 0 arrives (named
 // barrier of warps 0 and 1: warp 0's release then covers warp 1's stores);
-// warp 0 waits on the grid barrier and then releases the other warps
-// through a second named barrier (its acquire orders their slot reads); it
-// reads the scalar totals while warps 1.. stage every slot's coarse values
-// in shared memory (one float4 per thread) and then form one row each of
-// this CTA's block of A_c^-1 v into OUT[0..U).
+// warp 0 waits on the grid barrier, and after a CTA barrier (its acquire
+// orders their reads) every thread copies one 16-byte piece of the phase's
+// slot set into shared memory: one L2 round trip, and the fewest requests
+// on the lines every CTA reads at that moment.  Then warp 0 adds the
+// scalar totals while warps 1.. add every coarse block's values (the sums
+// of its CTAs' slots) and form one row each of this CTA's block of
+// A_c^-1 v into OUT[0..U).
 #define CHYSX_COARSE_PHASE(NR, OUT, exit_test, STEP)                                                 \
     do {                                                                                             \
         if (warp == 0) {                                                                             \
@@ -798,25 +842,24 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
             named_barrier_w01();                                                                     \
             bool w0ok = true;                                                                        \
             if (lane == 0) w0ok = barrier_arrive_wait(bp.bar, target);                               \
-            w0ok = __shfl_sync(0xffffffffu, w0ok, 0);                                                \
             if (lane == 0 && !w0ok) s_flag = 1;                                                      \
-            named_barrier_coarse(32 * W);                                                            \
-            if (w0ok) warp0_read_totals<NR, kPollMax>(bp, li, nloc, slot_set(ph), STEP);             \
-            if (lane == 0 && (exit_test) && w0ok)                                                    \
-                s_exit = *(volatile unsigned*)&bp.bar->ndone >= (unsigned)bp.n_inst;                 \
-        } else {                                                                                     \
-            if (warp == 1) {                                                                         \
-                warp1_coarse_publish(bp, s_cpart, s1 - s0, li[0].own_slot, slot_set(ph));            \
-                named_barrier_w01();                                                                 \
-            }                                                                                        \
-            named_barrier_coarse(32 * W);                                                            \
-            if (!*(volatile int*)&s_flag) {                                                          \
-                coarse_stage(bp, slot_set(ph), c_U, threadIdx.x - 32, 32 * (W - 1), c_stage);        \
+        } else if (warp == 1) {                                                                      \
+            warp1_coarse_publish(bp, c_U, s_cpart, s1 - s0, li[0].own_slot, slot_set(ph));           \
+            named_barrier_w01();                                                                     \
+        }                                                                                            \
+        __syncthreads();                                                                             \
+        if (!s_flag) coarse_stage_slots(bp, slot_set(ph), c_slots);                                  \
+        __syncthreads();                                                                             \
+        if (!s_flag) {                                                                               \
+            if (warp == 0) {                                                                         \
+                warp0_staged_totals<NR>(li, c_slots, STEP);                                          \
+                /* one instance, whose done flag every CTA sets alike */                             \
+                if (lane == 0 && (exit_test)) s_exit = li[0].done;                                   \
+            } else {                                                                                 \
+                coarse_block_values(c_slots, bp.n_slots, c_U, c_g, c_m, threadIdx.x - 32, 32 * (W - 1), \
+                                    c_stage);                                                        \
                 named_barrier_stage(32 * (W - 1));                                                   \
-                for (int r = warp - 1; r < c_U; r += W - 1) {                                        \
-                    if (c_U == 12) warp_coarse_row<12>(bp, c_stage, c_ainv, r, OUT);                 \
-                    else warp_coarse_row<3>(bp, c_stage, c_ainv, r, OUT);                            \
-                }                                                                                    \
+                for (int r = warp - 1; r < c_U; r += W - 1) warp_coarse_row(c_m, c_stage, c_ainv, r, OUT); \
             }                                                                                        \
         }                                                                                            \
         ++ph;                                                                                        \
@@ -848,9 +891,8 @@ __device__ __forceinline__ float* slice_cpart(double* spart, int sl) {
 }
 // The CTA's restriction (sum of its slices' partials, in slice order) into
 // its slot of `set`; threads 0..U-1 of the calling warp.
-__device__ __forceinline__ void coarse_publish_cta(const BatchPlan& bp, double* spart, int nsl, int own_slot, int set,
-                                                   int lane) {
-    const int U = 3 * bp.cg->nq;
+__device__ __forceinline__ void coarse_publish_cta(const BatchPlan& bp, int U, double* spart, int nsl, int own_slot,
+                                                   int set, int lane) {
     if (lane < U) {
         float acc = 0.0f;
         for (int sl = 0; sl < nsl; ++sl) acc += slice_cpart(spart, sl)[lane];
@@ -858,25 +900,78 @@ __device__ __forceinline__ void coarse_publish_cta(const BatchPlan& bp, double* 
     }
 }
 template <int BLOCK>
-__device__ __forceinline__ void coarse_apply_dense(const BatchPlan& bp, int set, float* vbuf, float* out) {
-    const CoarseArgs& cg = *bp.cg;
-    const int U = 3 * cg.nq, m = cg.m, G = cg.g, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int j = tid; j < m; j += BLOCK) {
-        const int B = j / U, u = j % U;
-        const int c1 = min((B + 1) * G, bp.n_slots);
-        float acc = 0.0f;
-        for (int c = B * G; c < c1; ++c) acc += __ldcg(coarse_slot(bp, set, c) + u);
-        vbuf[j] = acc;
+__device__ __forceinline__ void coarse_apply_dense(const BatchPlan& bp, const CoarseRegs& cr, int set, float* vbuf,
+                                                   float* out) {
+    constexpr int kChunk = 4;  // slot loads in flight per value
+    const int U = cr.U, m = cr.m, G = cr.G, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (U % 4 == 0) {
+        // one 16-byte piece (4 values) of one block per thread: its G slots
+        // added in slot order, all loads of a chunk in flight at once
+        const int per = U / 4;
+        for (int x = tid; x < m / 4; x += BLOCK) {
+            const int B = x / per, q = x - B * per;
+            const int c1 = min((B + 1) * G, bp.n_slots);
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (int c0 = B * G; c0 < c1; c0 += kChunk) {
+                float4 val[kChunk];
+#pragma unroll
+                for (int k = 0; k < kChunk; ++k)
+                    val[k] = c0 + k < c1 ? __ldcg(reinterpret_cast<const float4*>(coarse_slot(bp, set, c0 + k)) + q)
+                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int k = 0; k < kChunk; ++k) {
+                    acc.x += val[k].x;
+                    acc.y += val[k].y;
+                    acc.z += val[k].z;
+                    acc.w += val[k].w;
+                }
+            }
+            reinterpret_cast<float4*>(vbuf)[x] = acc;
+        }
+    } else {
+        for (int j = tid; j < m; j += BLOCK) {
+            const int B = j / U, u = j % U;
+            const int c1 = min((B + 1) * G, bp.n_slots);
+            float acc = 0.0f;
+            for (int c0 = B * G; c0 < c1; c0 += kChunk) {
+                float val[kChunk];
+#pragma unroll
+                for (int k = 0; k < kChunk; ++k) val[k] = c0 + k < c1 ? __ldcg(coarse_slot(bp, set, c0 + k) + u) : 0.0f;
+#pragma unroll
+                for (int k = 0; k < kChunk; ++k) acc += val[k];
+            }
+            vbuf[j] = acc;
+        }
     }
     __syncthreads();
-    const float* rows = cg.ainv + (size_t)((int)blockIdx.x / G) * U * m;
-    for (int r = warp; r < U; r += BLOCK / 32) {
-        const float* a = rows + (size_t)r * m;
-        float acc = 0.0f;
-        for (int j = lane; j < m; j += 32) acc = fmaf(__ldg(a + j), vbuf[j], acc);
+    const float* rows = cr.ainv + (size_t)((int)blockIdx.x / G) * U * m;
+    if (m % 4 == 0) {
+        // one half-warp per row, 16-byte loads of the row, 8 in flight per
+        // lane (rows are 16-byte aligned: m % 4 == 0)
+        const int hw = tid >> 4, hl = lane & 15, m4 = m / 4;
+        const float4* v4 = reinterpret_cast<const float4*>(vbuf);
+        for (int r = hw; r < U; r += BLOCK / 16) {
+            const float4* a = reinterpret_cast<const float4*>(rows + (size_t)r * m);
+            float acc = 0.0f;
+#pragma unroll 4
+            for (int j = hl; j < m4; j += 16) {
+                const float4 av = __ldg(a + j), vv = v4[j];
+                acc = fmaf(av.x, vv.x, fmaf(av.y, vv.y, fmaf(av.z, vv.z, fmaf(av.w, vv.w, acc))));
+            }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) out[r] = acc;
+            for (int o = 8; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (hl == 0) out[r] = acc;
+        }
+    } else {
+        for (int r = warp; r < U; r += BLOCK / 32) {
+            const float* a = rows + (size_t)r * m;
+            float acc = 0.0f;
+#pragma unroll 8
+            for (int j = lane; j < m; j += 32) acc = fmaf(__ldg(a + j), vbuf[j], acc);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) out[r] = acc;
+        }
     }
     __syncthreads();
 }
@@ -893,7 +988,7 @@ __device__ __forceinline__ void coarse_apply_dense(const BatchPlan& bp, int set,
 // dots, from which the next iteration's A_c^-1 R^T r restarts (no drift).
 // ---------------------------------------------------------------------------
 template <int BLOCK, int SYNC = 0, int CO = 0>
-__global__ void __launch_bounds__(BLOCK)
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)  // 1024 threads per SM: at most 64 registers
 pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP*, ZP*) {
     extern __shared__ double s_mem[];
     __shared__ int s_flag;
@@ -914,8 +1009,13 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
     // arithmetic (bit-identical iterates)
     const bool coarse = CO && !SYNC && bp.cg != nullptr && bp.cg->on && bp.cg->dense &&
                         *(volatile int*)bp.cg->fail == 0;
-    const int c_nq = coarse ? bp.cg->nq : 1, c_U = 3 * c_nq;
-    float* c_vbuf = reinterpret_cast<float*>(li + bp.max_inst_per_cta);
+    __shared__ CoarseRegs creg;
+    if (threadIdx.x == 0) creg = coarse_regs(bp, coarse);  // ordered by the __syncthreads after init_local
+    const int& c_U = creg.U;
+    const int& c_nq = creg.nq;
+    // the coarse block values behind the records, 16-byte aligned (float4 stores)
+    float* c_vbuf = reinterpret_cast<float*>(
+        (reinterpret_cast<uintptr_t>(li + bp.max_inst_per_cta) + 15) & ~static_cast<uintptr_t>(15));
     unsigned target = 0;  // barrier target; the counter starts at 0 every solve
     int ph = 0;           // reduction phase (SYNC = 1 slot set ph % 3)
     if (threadIdx.x == 0) {
@@ -926,15 +1026,15 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
     __syncthreads();
     bool ok = true;
     auto no_step = [](LocalInst&, const double*) {};
-    auto cw = [&](int i) { return c_nq == 4 ? __ldg(bp.cg->w + i) : make_float4(0.f, 0.f, 0.f, 0.f); };
+    auto cw = [&](int i) { return c_nq == 4 ? __ldg(creg.w + i) : make_float4(0.f, 0.f, 0.f, 0.f); };
     // one exchange phase carrying only the CTA's restriction of a vector;
     // leaves A_c^-1 R^T v (this block's U entries) in out
     auto coarse_exchange = [&](float* out) {
-        if (warp == 1) coarse_publish_cta(bp, spart, s1 - s0, li[0].own_slot, slot_set(ph), lane);
+        if (warp == 1) coarse_publish_cta(bp, c_U, spart, s1 - s0, li[0].own_slot, slot_set(ph), lane);
         __syncthreads();
         const int set = slot_set(ph);
         CHYSX_BLOCK_PHASE(1, 5, false, no_step);
-        if (!s_flag) coarse_apply_dense<BLOCK>(bp, set, c_vbuf, out);
+        if (!s_flag) coarse_apply_dense<BLOCK>(bp, creg, set, c_vbuf, out);
     };
 
     // ---- phase 0: initial residual and per-instance start ----------------
@@ -1121,7 +1221,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
         }
         __syncthreads();
         if (coarse) {
-            if (warp == 1) coarse_publish_cta(bp, spart, s1 - s0, li[0].own_slot, slot_set(ph), lane);
+            if (warp == 1) coarse_publish_cta(bp, c_U, spart, s1 - s0, li[0].own_slot, slot_set(ph), lane);
             __syncthreads();
         }
         const int set1 = slot_set(ph);
@@ -1134,7 +1234,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
         }
         if (!SYNC && s_exit) break;
         if (coarse) {
-            coarse_apply_dense<BLOCK>(bp, set1, c_vbuf, s_cw);
+            coarse_apply_dense<BLOCK>(bp, creg, set1, c_vbuf, s_cw);
             // A_c^-1 R^T r_new = A_c^-1 R^T r - alpha A_c^-1 R^T A p
             if ((int)threadIdx.x < c_U) s_cn[threadIdx.x] = fmaf(-li[0].alpha, s_cw[threadIdx.x], s_cu[threadIdx.x]);
             __syncthreads();
@@ -1172,7 +1272,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
         }
         __syncthreads();
         if (coarse) {
-            if (warp == 1) coarse_publish_cta(bp, spart, s1 - s0, li[0].own_slot, slot_set(ph), lane);
+            if (warp == 1) coarse_publish_cta(bp, c_U, spart, s1 - s0, li[0].own_slot, slot_set(ph), lane);
             __syncthreads();
         }
         const int set2 = slot_set(ph);
@@ -1184,7 +1284,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             break;
         }
         // the coarse part restarts from R^T r_new (no recurrence drift)
-        if (coarse) coarse_apply_dense<BLOCK>(bp, set2, c_vbuf, s_cu);
+        if (coarse) coarse_apply_dense<BLOCK>(bp, creg, set2, c_vbuf, s_cu);
     }
     if (!ok) instances_fail(bp, li, nloc);
 }
@@ -1382,17 +1482,21 @@ pcg_resident_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, ZP
     // quad.  Warps 1..3 form this block of A_c^-1 R^T v during the phases.
     constexpr bool kCoarse = PC == 2;
     const bool coarse = kCoarse && bp.cg != nullptr && bp.cg->on && *(volatile int*)bp.cg->fail == 0;
-    const int c_nq = coarse ? bp.cg->nq : 1, c_U = 3 * c_nq;
+    const CoarseRegs creg = coarse_regs(bp, coarse);
+    const int c_U = creg.U, c_nq = creg.nq, c_g = creg.G, c_m = creg.m;
     float* c_ainv = reinterpret_cast<float*>(li + bp.max_inst_per_cta);
-    // staged coarse values of a phase ([slots][U]), behind c_ainv (16-byte aligned)
+    // a phase's coarse block values ([m]) behind c_ainv, then its staged
+    // slot set ([n_slots][kSlotW] doubles), each 16-byte aligned
     float* c_stage = reinterpret_cast<float*>(
-        (reinterpret_cast<uintptr_t>(c_ainv + (coarse ? c_U * bp.cg->m : 0)) + 15) & ~static_cast<uintptr_t>(15));
+        (reinterpret_cast<uintptr_t>(c_ainv + (coarse ? c_U * c_m : 0)) + 15) & ~static_cast<uintptr_t>(15));
+    double* c_slots = reinterpret_cast<double*>(
+        (reinterpret_cast<uintptr_t>(c_stage + (coarse ? c_m : 0)) + 15) & ~static_cast<uintptr_t>(15));
     float4 c_w = make_float4(0.f, 0.f, 0.f, 0.f);
     if (coarse) {
-        const int m = bp.cg->m;
-        const float* src = bp.cg->ainv + (size_t)(blockIdx.x / bp.cg->g) * c_U * m;
+        const int m = c_m;
+        const float* src = creg.ainv + (size_t)(blockIdx.x / c_g) * c_U * m;
         for (int q = threadIdx.x; q < c_U * m; q += blockDim.x) c_ainv[q] = src[q];
-        if (c_nq == 4 && row) c_w = bp.cg->w[i];
+        if (c_nq == 4 && row) c_w = creg.w[i];
         __syncthreads();
     }
 
