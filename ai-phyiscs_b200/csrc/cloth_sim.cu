@@ -1482,6 +1482,11 @@ private:
         }
         d_cac_.resize((size_t)nb * mn * U * U);
         d_cac_.zero();
+        // split every block's slices over CTAs of ~kCoarseSplitSlices slices
+        int spb = 1;
+        for (int B = 0; B < nb; ++B) spb = std::max(spb, (row0[B + 1] - row0[B] + 31) / 32);
+        const int splits = std::min(kCoarseMaxSplits, std::max(1, (spb + kCoarseSplitSlices - 1) / kCoarseSplitSlices));
+        d_cacp_.resize((size_t)splits * nb * mn * U * U);
         d_cainv_.resize((size_t)m * m);
         d_cainv_.zero();
         {
@@ -1495,6 +1500,7 @@ private:
         coarse_shift_ = shift;
         coarse_nb_ = nb;
         coarse_mn_ = mn;
+        coarse_splits_ = splits;
         coarse_g_ = G;
         coarse_nq_ = nq;
         coarse_on_ = true;
@@ -1546,6 +1552,8 @@ private:
         c.ell_nbr = d_ell_nbr_.get();
         c.w = coarse_nq_ > 1 ? d_cw_.get() : nullptr;
         c.ac = d_cac_.get();
+        c.acp = d_cacp_.get();
+        c.splits = coarse_splits_;
         c.ainv = d_cainv_.get();
         c.dense = resident_ ? 0 : 1;
         c.shift = coarse_shift_;
@@ -1783,7 +1791,7 @@ private:
             void* a1[] = {&t, &cg};
             cudaKernelNodeParams p{};
             p.func = reinterpret_cast<void*>(&coarse_assemble_kernel);
-            p.gridDim = dim3(coarse_nb_, coarse_nq_);
+            p.gridDim = dim3(coarse_nb_, coarse_nq_, coarse_splits_);
             p.blockDim = dim3(288);
             p.sharedMemBytes = (unsigned)coarse_assemble_smem();
             p.kernelParams = a1;
@@ -2100,13 +2108,14 @@ private:
     int sync_mode_ = 0;    // 0 grid counter barrier, 1 polled per-instance slots
     int pc_kind_ = 0, pc_degree_ = 0;  // preconditioner: 0 block-Jacobi, 1 CTA-local Chebyshev, 2 + coarse level
     bool coarse_on_ = false;
-    int coarse_nb_ = 0, coarse_mn_ = 0, coarse_g_ = 1, coarse_nq_ = 1;
+    int coarse_nb_ = 0, coarse_mn_ = 0, coarse_g_ = 1, coarse_nq_ = 1, coarse_splits_ = 1;
     double coarse_shift_ = 0.0;
     DevBuf<int> d_slice_cb_, d_cb_row0_, d_cnbr_, d_ccnt_, d_cself_;
     DevBuf<unsigned char> d_ell_nbr_;
     DevBuf<float4> d_cw_;
     DevBuf<CoarseArgs> d_cargs_;  // the coarse arguments the PCG kernel reads (BatchPlan holds the pointer)
     DevBuf<float> d_cac_, d_cainv_;
+    DevBuf<double> d_cacp_;  // the coarse assembly's per-split partial sums
     DevBuf<double> d_cwork_;
     DevBuf<int> d_cfail_;
     DevBuf<GridBarrier> d_cbar_;

@@ -10,9 +10,10 @@
 //     M^-1 = P_local + R A_c^-1 R^T,
 // P_local the CTA-local Chebyshev polynomial, is a fixed symmetric
 // positive-definite operator, so the outer iteration stays plain PCG.  Per
-// step: coarse_fields_kernel (the weights), coarse_assemble_kernel (one CTA
-// per block and field pair, deterministic per-lane partial sums added in
-// lane order) and coarse_invert_kernel (A_c^-1 densely, FP64 blocked
+// step: coarse_fields_kernel (the weights), coarse_assemble_kernel (CTAs per
+// block, field pair and slice split, deterministic per-lane partial sums
+// added in lane order, the splits added in order by the inversion) and
+// coarse_invert_kernel (A_c^-1 densely, FP64 blocked
 // Gauss-Jordan across the grid); per iteration the resident kernel forms its
 // block of A_c^-1 R^T r from the blocks' restricted residuals, which ride on
 // the existing reduction slots.
@@ -148,14 +149,15 @@ __global__ void __launch_bounds__(256) coarse_fields_kernel(StepArgs a, CoarseAr
 }
 
 // A_c block row of coarse block B for the row field qa = blockIdx.y and
-// every column field: 9 warps (one per component of the 3x3 block), lane l
-// takes the rows l of every slice of the block; per-lane sums of
+// every column field, over split blockIdx.z of the block's slices (every
+// ca.splits-th slice): 9 warps (one per component of the 3x3 block), lane l
+// takes the rows l of the split's slices; per-lane sums of
 // w_iqa w_jqb A_ij (the operator in its difference form, so the inertia of
 // a block's translation is not lost against its elastic diagonal) by
 // column block and qb in dynamic shared memory
 // ([nq][9][max_nbr][32] floats), then each (qb, column block, component) sum
-// over lanes in lane order (double).  A row's entries are gathered once for
-// all qb.
+// over lanes in lane order (double) into the split's partial block row.  A
+// row's entries are gathered once for all qb.
 __global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, CoarseArgs ca) {
     extern __shared__ float acc_s[];
     const int B = blockIdx.x, qa = blockIdx.y, nq = ca.nq, mn = ca.max_nbr;
@@ -173,7 +175,7 @@ __global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, CoarseA
         return make_float4(1.f, w.x, w.y, w.z);
     };
     auto pick = [](float4 w, int q) { return q == 0 ? w.x : (q == 1 ? w.y : (q == 2 ? w.z : w.w)); };
-    for (int s = s0; s < s1; ++s) {
+    for (int s = s0 + (int)blockIdx.z; s < s1; s += ca.splits) {
         const int i = s * 32 + l;
         if (i >= t.n) break;
         const float4 wi4 = weights(i);
@@ -220,7 +222,8 @@ __global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, CoarseA
         double sum = 0.0;
         for (int y = 0; y < 32; ++y) sum += acc_s[(((size_t)qb * 9 + cc) * mn + k) * 32 + y];
         const int r = cc / 3, col = cc % 3;
-        ca.ac[(((size_t)B * mn + k) * U + qa * 3 + r) * U + qb * 3 + col] = (float)sum;
+        ca.acp[(size_t)blockIdx.z * ca.nb * mn * U * U + (((size_t)B * mn + k) * U + qa * 3 + r) * U + qb * 3 + col] =
+            sum;
     }
 }
 
@@ -289,9 +292,15 @@ __global__ void __launch_bounds__(kCoarseInvertThreads) coarse_invert_kernel(Coa
     if (!gsync()) goto fail;
     for (int e = gt; e < nb * mn * U * U; e += gn) {
         const int B = e / (mn * U * U), rem = e % (mn * U * U), k = rem / (U * U), rc = rem % (U * U);
+        // the assembly's splits added in order, rounded once to FP32 (the
+        // stored A_c that the inverse is of)
+        double v = 0.0;
+        for (int z = 0; z < ca.splits; ++z) v += __ldcg(ca.acp + (size_t)z * nb * mn * U * U + e);
+        const float vf = (float)v;
+        ca.ac[e] = vf;
         if (k >= ca.nbr_cnt[B]) continue;
         const int C = ca.nbr[B * mn + k];
-        __stcg(W + (size_t)(B * U + rc / U) * mp + C * U + rc % U, (double)ca.ac[e]);
+        __stcg(W + (size_t)(B * U + rc / U) * mp + C * U + rc % U, (double)vf);
     }
     if (!gsync()) goto fail;
     for (int i = gt; i < mp; i += gn) {

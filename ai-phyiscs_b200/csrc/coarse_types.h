@@ -12,6 +12,12 @@ constexpr int kCoarseMaxNbr = 16;      // coarse blocks one block's rows touch, 
 constexpr int kCoarseStreamRows = 8192;
 constexpr int kCoarseDenseMax = 2048;
 constexpr int kCoarseInvertThreads = 256;
+// The coarse assembly splits a block's slices over CTAs of about
+// kCoarseSplitSlices slices each (at most kCoarseMaxSplits per block): each
+// slice costs dependent L2 round trips, so one CTA per block would walk a
+// 2048-row block's 64 slices one after another
+constexpr int kCoarseSplitSlices = 8;
+constexpr int kCoarseMaxSplits = 32;
 // Relative diagonal shift of the streamed kernel's coarse matrix: A_c +
 // shift diag(A_c) is inverted instead of A_c (the resident kernel's coarse
 // matrix, on smaller blocks, is inverted unshifted).  The coarse matrix of a flat,
@@ -43,6 +49,12 @@ struct CoarseArgs {
     const unsigned char* ell_nbr = nullptr;   // [ELL entries] list position of the entry's column block
     float4* w = nullptr;                      // [rows] linear-field weights s_1, s_2, s_3 (nq = 4)
     float* ac = nullptr;                      // [nb][max_nbr][U][U] A_c, row-major U x U blocks
+    // the assembly's partial sums: a block's slices are split over `splits`
+    // CTAs (slice s to split (s - first) % splits), each writing its sums
+    // in double to acp[split][nb][max_nbr][U][U]; the inversion adds the
+    // splits in order and rounds once into ac
+    double* acp = nullptr;
+    int splits = 1;
     float* ainv = nullptr;                    // [m][m] A_c^-1 (row-major)
     // A_c^-1 is formed by coarse_invert_kernel in the FP64 workspace
     // (padded m * m + m + 2048 doubles) from A_c + shift diag(A_c); fail != 0
