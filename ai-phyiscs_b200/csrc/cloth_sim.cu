@@ -1816,8 +1816,13 @@ private:
                 GridBarrier* gb = d_cbar_.get();
                 void* a2[] = {&cg, &gb};
                 cudaKernelNodeParams p2{};
+                // two CTAs per SM where they fit (the tile phases are latency-bound)
+                int inv_per_sm = 0;
+                ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&inv_per_sm, coarse_invert_kernel,
+                                                                 kCoarseInvertThreads, 0),
+                   "cudaOccupancyMaxActiveBlocksPerMultiprocessor(coarse invert)");
                 p2.func = reinterpret_cast<void*>(&coarse_invert_kernel);
-                p2.gridDim = dim3(sms);
+                p2.gridDim = dim3(sms * std::max(1, std::min(2, inv_per_sm)));
                 p2.blockDim = dim3(kCoarseInvertThreads);
                 p2.kernelParams = a2;
                 ck(cudaGraphAddKernelNode(&n2, graph_, &z2, 1, &p2), "add coarse invert node");

@@ -245,6 +245,7 @@ __global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, CoarseA
 // ca.fail and the PCG kernel then runs without the coarse level.  Cross-CTA
 // data goes through L2 (__ldcg / __stcg).  Output: ca.ainv = S W S (FP32).
 constexpr int kInvTile = 32;
+static_assert(kInvTile * kInvTile % kCoarseInvertThreads == 0, "P3 gives every thread whole tile entries");
 
 // c = a * b for 32 x 32 tiles in shared memory (row stride 33), every
 // thread of the CTA four outputs; sign -1 stores -a * b.
@@ -336,34 +337,35 @@ __global__ void __launch_bounds__(kCoarseInvertThreads) coarse_invert_kernel(Coa
             break;
         }
         // P1: T = W_KK^-1 by Gauss-Jordan in shared memory (the last CTA,
-        // the others being busy with P4 above)
+        // the others being busy with P4 above): every pivot step reads the
+        // tile of the previous step and writes the other of two buffers, so
+        // one CTA barrier per pivot; every thread forms 1 / pivot itself
         if (blockIdx.x == gridDim.x - 1) {
             ld_tile(sa, tile_at(K, K));
             __syncthreads();
+            double(*cur)[kInvTile + 1] = sa;
+            double(*nxt)[kInvTile + 1] = sc_;
+            bool bad = false;
             for (int k = 0; k < kInvTile; ++k) {
-                const double p = sa[k][k];
+                const double p = cur[k][k];
                 const bool good = p > 1.0e-12;
-                if (!good && tid == 0) atomicExch(ca.fail, 1);
+                bad = bad || !good;
                 const double ip = good ? 1.0 / p : 0.0;
-                __syncthreads();
-                if (tid < kInvTile) sa[k][tid] = (tid == k ? 1.0 : sa[k][tid]) * ip;
-                __syncthreads();
                 for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x) {
                     const int r = o / kInvTile, q = o % kInvTile;
-                    if (r == k) continue;
-                    sb[r][q] = sa[r][k];  // the factor of row r
+                    // row k: (q == k ? 1 : a_kq) / p; the others subtract a_rk times it
+                    const double rk = (q == k ? 1.0 : cur[k][q]) * ip;
+                    nxt[r][q] = r == k ? rk : fma(-cur[r][k], rk, q == k ? 0.0 : cur[r][q]);
                 }
                 __syncthreads();
-                for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x) {
-                    const int r = o / kInvTile, q = o % kInvTile;
-                    if (r == k) continue;
-                    sa[r][q] = (q == k ? 0.0 : sa[r][q]) - sb[r][q] * sa[k][q];
-                }
-                __syncthreads();
+                double(*t)[kInvTile + 1] = cur;
+                cur = nxt;
+                nxt = t;
             }
+            if (bad && tid == 0) atomicExch(ca.fail, 1);
             double* Tk = Tg + (size_t)(K & 1) * kInvTile * kInvTile;
-            for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x) __stcg(Tk + o, sa[o / kInvTile][o % kInvTile]);
-            st_tile(tile_at(K, K), sa);
+            for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x) __stcg(Tk + o, cur[o / kInvTile][o % kInvTile]);
+            st_tile(tile_at(K, K), cur);
         }
         if (!gsync()) goto fail;
         // P2: W_KJ <- T W_KJ
@@ -386,15 +388,23 @@ __global__ void __launch_bounds__(kCoarseInvertThreads) coarse_invert_kernel(Coa
         for (int x = blockIdx.x; x < nt * nt; x += gridDim.x) {
             const int I = x / nt, J = x % nt;
             if (I == K || J == K) continue;
+            // the tile to update is read with the two factors (one round trip)
+            double* dst = tile_at(I, J);
+            double cur[kInvTile * kInvTile / kCoarseInvertThreads];
+#pragma unroll
+            for (int j = 0; j < kInvTile * kInvTile / kCoarseInvertThreads; ++j) {
+                const int o = tid + j * kCoarseInvertThreads;
+                cur[j] = __ldcg(dst + (size_t)(o / kInvTile) * mp + o % kInvTile);
+            }
             ld_tile(sa, tile_at(I, K));
             ld_tile(sb, tile_at(K, J));
             __syncthreads();
             tile_mul(sa, sb, sc_, 1.0);
             __syncthreads();
-            double* dst = tile_at(I, J);
-            for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x) {
-                double* q = dst + (size_t)(o / kInvTile) * mp + o % kInvTile;
-                __stcg(q, __ldcg(q) - sc_[o / kInvTile][o % kInvTile]);
+#pragma unroll
+            for (int j = 0; j < kInvTile * kInvTile / kCoarseInvertThreads; ++j) {
+                const int o = tid + j * kCoarseInvertThreads;
+                __stcg(dst + (size_t)(o / kInvTile) * mp + o % kInvTile, cur[j] - sc_[o / kInvTile][o % kInvTile]);
             }
             __syncthreads();
         }
