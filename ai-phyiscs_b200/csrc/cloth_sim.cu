@@ -1427,10 +1427,10 @@ private:
 
     // Coarse level of the two-level preconditioner (kind 2) of a
     // single-instance resident plan: coarse blocks of G consecutive CTAs with
-    // nq fields each; (G, nq) = (4, 4) (translation and linear fields on
-    // 4-CTA blocks) where the plan has at least 8 CTAs and the coarse system
-    // at most kCoarseDenseMax unknowns, else (1, 1) (the translation of
-    // every CTA block).  The streamed kernel's blocks are larger (about
+    // nq fields each; (G, nq) = (kCoarseResidentCtas, 4) (translation and
+    // linear fields on 2-CTA blocks) where the plan has at least 8 CTAs and
+    // the coarse system at most kCoarseDenseMax unknowns, else (1, 1) (the
+    // translation of every CTA block).  The streamed kernel's blocks are larger (about
     // kCoarseStreamRows rows).  Host side:
     // the coarse block of every slice and its first row, every block's sorted
     // list of the blocks its rows touch, and the list position of every ELL
@@ -1529,7 +1529,7 @@ private:
             return;
         }
         if (plan_.grid > kCoarseMaxBlocks) return;
-        if (plan_.grid >= 8 && plan_coarse_with(4, 4, 0.0)) return;
+        if (plan_.grid >= 8 && plan_coarse_with(kCoarseResidentCtas, 4, 0.0)) return;
         plan_coarse_with(1, 1, 0.0);
     }
     // per-lane partial sums of the coarse assembly: [nq][9][max_nbr][32] floats

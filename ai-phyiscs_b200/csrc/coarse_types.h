@@ -12,6 +12,13 @@ constexpr int kCoarseMaxNbr = 16;      // coarse blocks one block's rows touch, 
 constexpr int kCoarseStreamRows = 8192;
 constexpr int kCoarseDenseMax = 2048;
 constexpr int kCoarseInvertThreads = 256;
+// CTAs per coarse block of the register-resident kernel's level (1,024 rows
+// at 512 rows per CTA).  Measured on the 256 x 256 configuration: 2-CTA
+// blocks (768 unknowns) take 253 iterations per step against 325 with 4-CTA
+// blocks (384 unknowns) and 376 with 8-CTA blocks, for a dearer inverse
+// (0.95 against 0.50 ms of set-up per step) and a dearer coarse row per CTA
+// (14.5 against 13.6 us per iteration): 216 against 202 steps/s
+constexpr int kCoarseResidentCtas = 2;
 // The coarse assembly splits a block's slices over CTAs of about
 // kCoarseSplitSlices slices each (at most kCoarseMaxSplits per block): each
 // slice costs dependent L2 round trips, so one CTA per block would walk a

@@ -415,16 +415,20 @@ int chysx_cloth_row_of_particles(const chysx_cloth* h, int n, int32_t* rows);
  * iteration stays plain PCG with the same stopping test (||r|| / ||b||);
  * odd degrees keep p positive on the whole spectrum.  Kind 2 = kind 1 plus
  * a coarse level: z += R A_c^-1 R^T r, A_c = R^T A R assembled on the device
- * each step, R the coarse space: on blocks of 4 consecutive CTAs (2048 rows
+ * each step, R the coarse space: on blocks of 2 consecutive CTAs (1024 rows
  * of a spatially ordered 256 x 256 grid) the translation and the three
- * linear fields along the principal axes of the block's positions, where
- * that coarse system fits the device's shared memory, else the translation
- * of every CTA's block; every CTA computes its rows of A_c^-1 by CG before
- * the solve.  It applies to single-instance systems of at most 160 CTAs and
- * acts as kind 1 elsewhere.  Kinds 1 and 2 apply where the register-resident
- * kernel runs with synchronisation mode 0; in_use reports what the last graph
- * build uses (0 block-Jacobi, 1 local, 2 two-level with translations, 3
- * two-level with translations and linear fields). */
+ * linear fields along the principal axes of the block's positions, where the
+ * plan has at least 8 CTAs, else the translation of every CTA's block;
+ * A_c^-1 is formed densely each step by an FP64 Gauss-Jordan kernel (at
+ * most 2048 unknowns).  It applies to single-instance systems of at most
+ * 160 CTAs and acts as kind 1 elsewhere.  Kinds 1 and 2 apply where the
+ * register-resident kernel runs with synchronisation mode 0.  On systems too
+ * large for that kernel (the streamed kernel), kinds 1 and 2 give
+ * block-Jacobi plus the coarse level on blocks of about 8192 rows, A_c
+ * shifted by 1e-5 diag(A_c) (single instance, synchronisation mode 0).
+ * in_use reports what the last graph build uses (0 block-Jacobi, 1 local,
+ * 2 two-level with translations, 3 two-level with translations and linear
+ * fields). */
 int chysx_cloth_set_preconditioner(chysx_cloth* h, int kind, int degree, float ratio);
 int chysx_cloth_preconditioner(const chysx_cloth* h, int* kind, int* degree, float* ratio, int* in_use);
 /* Kernel used at the last graph build: path 0 register-resident persistent,

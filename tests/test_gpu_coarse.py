@@ -1,5 +1,5 @@
 """The two-level preconditioner (CTA-local Chebyshev plus a coarse level:
-the translation and linear fields of 4-CTA blocks, or the translation of
+the translation and linear fields of 2-CTA blocks, or the translation of
 every CTA block on small grids): converged solutions as the FP64 oracle's
 block-Jacobi PCG, iteration counts as the oracle's restatement of the same
 two-level operator, the warm starts, ragged blocks, its fallback to the
@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 def oracle_coarse(c, used, block_rows):
     """The oracle's coarse space matching the GPU's (in_use 2 or 3)."""
     if used == 3:
-        c.set_preconditioner(7, 30.0, block_rows, coarse="linear", coarse_rows=4 * block_rows)
+        c.set_preconditioner(7, 30.0, block_rows, coarse="linear", coarse_rows=2 * block_rows)
     else:
         c.set_preconditioner(7, 30.0, block_rows, coarse=True)
 
@@ -38,7 +38,7 @@ def test_coarse_solution_and_iterations(side):
     g = gpu(sc, "chebyshev_coarse", max_iter=20000, rel_tol=1e-7)
     g.step()
     kind, deg, _, used = g.sim.preconditioner()
-    assert (kind, deg, used) == ("chebyshev_coarse", 7, 3)  # 8 and 32 CTAs: linear fields on 4-CTA blocks
+    assert (kind, deg, used) == ("chebyshev_coarse", 7, 3)  # 8 and 32 CTAs: linear fields on 2-CTA blocks
     block_rows = g.sim.solver_info()[2]
     o = oracle_sim(sc, 1e-11)
     o.step(sc["dt"])
@@ -75,7 +75,7 @@ def test_coarse_level_cuts_iterations_on_compact_blocks():
 @pytest.mark.parametrize("side,used", [(48, 2), (80, 3)])
 def test_coarse_trajectories_with_ragged_blocks(warm, side, used):
     """48 x 48 particles: 4.5 CTA blocks of 512 rows, the translation of
-    each; 80 x 80: 12.5 CTA blocks, linear fields on 4-CTA blocks, the last
+    each; 80 x 80: 12.5 CTA blocks, linear fields on 2-CTA blocks, the last
     coarse block one ragged CTA."""
     sc = scenes.config_small(side=side, steps=6)
     a = gpu(sc, "chebyshev_coarse", max_iter=20000, rel_tol=1e-7, warm_start=warm)
@@ -114,14 +114,14 @@ def test_coarse_system_matches_the_oracle():
     Gauss-Jordan inverse against the exact inverse of the device matrix.  Principal axes are defined up to
     sign, so entries are compared in magnitude, spectra directly.  The rows
     of the inverse are checked against the device matrix's exact inverse."""
-    sc = scenes.config_small(side=64, steps=2)  # 8 CTAs: 2 coarse blocks of 4 CTAs
+    sc = scenes.config_small(side=64, steps=2)  # 8 CTAs: 4 coarse blocks of 2 CTAs
     g = gpu(sc, "chebyshev_coarse", max_iter=20000, rel_tol=1e-7)
     g.step()
     info, ac, ainv = g.sim.debug_coarse()
-    assert (info["on"], info["fields"], info["ctas_per_block"], info["blocks"]) == (1, 4, 4, 2)
+    assert (info["on"], info["fields"], info["ctas_per_block"], info["blocks"]) == (1, 4, 2, 4)
     block_rows = g.sim.solver_info()[2]
     o = oracle_sim(sc, 1e-11)
-    o.set_preconditioner(7, 30.0, block_rows, coarse="linear", coarse_rows=4 * block_rows)
+    o.set_preconditioner(7, 30.0, block_rows, coarse="linear", coarse_rows=2 * block_rows)
     o.step(sc["dt"])
     A = o.coarse_system()
     keep = np.diag(ac) != 0  # a dropped axis: zero weights, identity rows in the solve
