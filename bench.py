@@ -179,12 +179,17 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU legs (test infrastructure: the oracle port)
 # ---------------------------------------------------------------------------
+# the two-level preconditioner's blocks on the device's register-resident
+# plan: local blocks of one CTA (512 rows), coarse blocks of two CTAs
+LOCAL_ROWS = 512
+COARSE_ROWS = 1024
+
 def spatial_order(pos, block=512, slice_rows=32):
     """Particles in spatially compact blocks: recursive coordinate bisection
     along the longest extent, split sizes multiples of `block` rows (then of
     `slice_rows`), ties by index -- the partition the device's row order
     (set_row_order(1)) uses, so the CPU port's 512-row local blocks and
-    2048-row coarse blocks are the same particle sets."""
+    1024-row coarse blocks are the same particle sets."""
     order = np.arange(pos.shape[0])
 
     def bisect(lo, hi):
@@ -234,9 +239,9 @@ def permuted(sc, order):
 def oracle_setup(sc, fp64, threads, pc=None):
     """The oracle (fp64) or the FP32 CPU port of a scene; pc = (degree,
     ratio) adds the two-level preconditioner of the device's benchmarked
-    configuration (local blocks of 512 rows, coarse blocks of 2048 rows with
-    translation and linear fields) -- the scene must then be in the
-    spatially compact order."""
+    configuration (local blocks of LOCAL_ROWS rows, coarse blocks of
+    COARSE_ROWS rows with translation and linear fields) -- the scene must
+    then be in the spatially compact order."""
     import oracle.oracle as O
 
     O.set_threads(threads)
@@ -252,7 +257,7 @@ def oracle_setup(sc, fp64, threads, pc=None):
     s.build_stretch(sc["k_stretch"])
     s.set_pins(sc["pin_idx"], sc["pin_targets"], sc.get("k_pin", 1e6))
     if pc is not None:
-        s.set_preconditioner(int(pc[0]), float(pc[1]), 512, "linear", 2048)
+        s.set_preconditioner(int(pc[0]), float(pc[1]), LOCAL_ROWS, "linear", COARSE_ROWS)
     s._inv_mass = im
     return s
 
@@ -615,6 +620,12 @@ def run_ours(args, rank, world, local_rank):
                                 "steps": args.steps}
     plain_iters = arms["grid256_plain"]["pcg_iters_per_step"] if arms else None
 
+    # the device's coarse blocks in rows (the CPU legs restate them)
+    cinfo = g.sim.debug_coarse()[0] if int(g.sim.preconditioner()[3]) >= 2 else None
+    coarse_rows = int(cinfo["ctas_per_block"]) * int(g.sim.solver_info()[2]) if cinfo else 0
+    if cinfo and g.sim.solver_info()[0] == "resident" and coarse_rows != COARSE_ROWS:
+        print(f"warning: device coarse blocks of {coarse_rows} rows, CPU legs use {COARSE_ROWS}", file=sys.stderr)
+
     # CPU baseline: the FP32 CPU port on one core in the same configuration
     # (same preconditioner on the same spatially compact blocks), full steps
     # timed whole; the first step (from rest, the most iterations) untimed
@@ -646,7 +657,8 @@ def run_ours(args, rank, world, local_rank):
                    "instances": 1 if offs is None else len(offs) - 1,
                    "pcg_kernel": g.sim.solver_info()[0], "pcg_grid": g.sim.solver_info()[1],
                    "pcg_block": g.sim.solver_info()[2], "l2": "flushed between steps (256 MiB write)",
-                   "preconditioner": dict(zip(("kind", "degree", "ratio", "in_use"), g.sim.preconditioner())),
+                   "preconditioner": dict(zip(("kind", "degree", "ratio", "in_use"), g.sim.preconditioner()),
+                                          coarse_block_rows=coarse_rows),
                    "row_order": args.row_order},
         "pcg_iters_per_step": mean_iters,
         "pcg_iters_per_step_minmax": [int(iters.min()), int(iters.max())],
