@@ -945,7 +945,39 @@ __device__ __forceinline__ void coarse_apply_dense(const BatchPlan& bp, const Co
     }
     __syncthreads();
     const float* rows = cr.ainv + (size_t)((int)blockIdx.x / G) * U * m;
-    if (m % 4 == 0) {
+    if (U == 12 && m % 4 == 0) {
+        // every thread takes the 16-byte pieces j = tid, tid + BLOCK, ... of
+        // all 12 rows at once (12 loads in flight per piece), then the
+        // CTA's per-row sums (warp trees, then the warps in order)
+        __shared__ float s_rsum[BLOCK / 32][12];
+        const int m4 = m / 4;
+        const float4* v4 = reinterpret_cast<const float4*>(vbuf);
+        const float4* a4 = reinterpret_cast<const float4*>(rows);
+        float acc[12];
+#pragma unroll
+        for (int r = 0; r < 12; ++r) acc[r] = 0.0f;
+        for (int j = tid; j < m4; j += BLOCK) {
+            const float4 vv = v4[j];
+#pragma unroll
+            for (int r = 0; r < 12; ++r) {
+                const float4 av = __ldg(a4 + (size_t)r * m4 + j);
+                acc[r] = fmaf(av.x, vv.x, fmaf(av.y, vv.y, fmaf(av.z, vv.z, fmaf(av.w, vv.w, acc[r]))));
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 12; ++r) {
+            float x = acc[r];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if (lane == 0) s_rsum[warp][r] = x;
+        }
+        __syncthreads();
+        if (tid < 12) {
+            float x = 0.0f;
+            for (int w = 0; w < BLOCK / 32; ++w) x += s_rsum[w][tid];
+            out[tid] = x;
+        }
+    } else if (m % 4 == 0) {
         // one half-warp per row, 16-byte loads of the row, 8 in flight per
         // lane (rows are 16-byte aligned: m % 4 == 0)
         const int hw = tid >> 4, hl = lane & 15, m4 = m / 4;
