@@ -247,17 +247,26 @@ __global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, CoarseA
 constexpr int kInvTile = 32;
 static_assert(kInvTile * kInvTile % kCoarseInvertThreads == 0, "P3 gives every thread whole tile entries");
 
-// c = a * b for 32 x 32 tiles in shared memory (row stride 33), every
-// thread of the CTA four outputs; sign -1 stores -a * b.
+// c = a * b for 32 x 32 tiles in shared memory (row stride 33); thread t
+// of the kCoarseInvertThreads computes the outputs (t / 32 + j * R, t % 32),
+// j < kTileOut, R = kCoarseInvertThreads / 32: one b entry serves its
+// kTileOut independent sums; sign -1 stores -a * b.
+constexpr int kTileOut = kInvTile * kInvTile / kCoarseInvertThreads;
 __device__ __forceinline__ void tile_mul(const double (*a)[kInvTile + 1], const double (*b)[kInvTile + 1],
                                          double (*c)[kInvTile + 1], double sign) {
-    for (int o = threadIdx.x; o < kInvTile * kInvTile; o += blockDim.x) {
-        const int r = o / kInvTile, q = o % kInvTile;
-        double acc = 0.0;
+    constexpr int R = kCoarseInvertThreads / kInvTile;
+    const int r0 = threadIdx.x / kInvTile, q = threadIdx.x % kInvTile;
+    double acc[kTileOut];
+#pragma unroll
+    for (int j = 0; j < kTileOut; ++j) acc[j] = 0.0;
 #pragma unroll 8
-        for (int k = 0; k < kInvTile; ++k) acc = fma(a[r][k], b[k][q], acc);
-        c[r][q] = sign * acc;
+    for (int k = 0; k < kInvTile; ++k) {
+        const double bk = b[k][q];
+#pragma unroll
+        for (int j = 0; j < kTileOut; ++j) acc[j] = fma(a[r0 + j * R][k], bk, acc[j]);
     }
+#pragma unroll
+    for (int j = 0; j < kTileOut; ++j) c[r0 + j * R][q] = sign * acc[j];
 }
 
 __global__ void __launch_bounds__(kCoarseInvertThreads) coarse_invert_kernel(CoarseArgs ca, GridBarrier* gb) {
@@ -351,10 +360,14 @@ __global__ void __launch_bounds__(kCoarseInvertThreads) coarse_invert_kernel(Coa
                 const bool good = p > 1.0e-12;
                 bad = bad || !good;
                 const double ip = good ? 1.0 / p : 0.0;
-                for (int o = tid; o < kInvTile * kInvTile; o += blockDim.x) {
-                    const int r = o / kInvTile, q = o % kInvTile;
-                    // row k: (q == k ? 1 : a_kq) / p; the others subtract a_rk times it
-                    const double rk = (q == k ? 1.0 : cur[k][q]) * ip;
+                // the thread's outputs (tid / 32 + j * R, tid % 32), as in tile_mul;
+                // row k: (q == k ? 1 : a_kq) / p; the others subtract a_rk times it
+                constexpr int R = kCoarseInvertThreads / kInvTile;
+                const int r0 = tid / kInvTile, q = tid % kInvTile;
+                const double rk = (q == k ? 1.0 : cur[k][q]) * ip;
+#pragma unroll
+                for (int j = 0; j < kTileOut; ++j) {
+                    const int r = r0 + j * R;
                     nxt[r][q] = r == k ? rk : fma(-cur[r][k], rk, q == k ? 0.0 : cur[r][q]);
                 }
                 __syncthreads();
