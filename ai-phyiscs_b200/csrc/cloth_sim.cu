@@ -1283,9 +1283,9 @@ private:
     void guess_params(cudaKernelNodeParams& p, void** args) const {
         p = cudaKernelNodeParams{};
         p.func = reinterpret_cast<void*>(&learned_guess_kernel);
-        const int slices = std::max(1, topo_.n_slices);
-        p.gridDim = dim3(std::max(1, std::min(2048, (slices + kGuessWarps - 1) / kGuessWarps)));
-        p.blockDim = dim3(kGuessWarps * 32);
+        const int tiles = std::max(1, (topo_.n + kGuessThreads - 1) / kGuessThreads);
+        p.gridDim = dim3(std::max(1, std::min(2048, tiles)));
+        p.blockDim = dim3(kGuessThreads);
         p.kernelParams = args;
     }
     // Appends the feature / learned-guess node after `dep` when needed.

@@ -230,28 +230,196 @@ __device__ __forceinline__ void row_features(const StepArgs& a, const DevTopo& t
 }
 
 // ---------------------------------------------------------------------------
-// Step kernel: features (optionally exported in caller order) and, when a
-// network is loaded, the initial guess x = dt (v + dv).  One warp per
-// 32-row slice; two 16-row tensor-core tiles per slice.
+// Fifth-generation tensor cores (tcgen05, sm_100a) for the network's
+// inference: one elected thread issues the MMAs, operands sit in shared
+// memory in the canonical K-major layout without swizzle (8-row x 16-byte
+// core matrices), the FP32 accumulator lives in tensor memory (TMEM) and
+// comes back to registers with tcgen05.ld.
 // ---------------------------------------------------------------------------
-constexpr int kGuessWarps = 4;
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// Byte offset of element (r, k) of a K-major bf16 operand with `sbo` bytes
+// between 8-row groups and 128 bytes between K-adjacent core matrices.
+__device__ __forceinline__ uint32_t umma_off(int r, int k, uint32_t sbo) {
+    return (uint32_t)(r >> 3) * sbo + (uint32_t)(k >> 3) * 128u + (uint32_t)(r & 7) * 16u + (uint32_t)(k & 7) * 2u;
+}
+// Shared-memory matrix descriptor of that layout (start address, leading
+// byte offset 128 = the two K-halves of one K = 16 step, stride byte offset
+// `sbo`, descriptor version 1, no swizzle).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) |
+           (1ull << 46);
+}
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, int accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// Bounded wait for phase `parity` of an mbarrier (1 s of globaltimer).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    unsigned long long t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    while (true) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+        unsigned long long t1;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+        if (t1 - t0 > 1000000000ull) return false;
+    }
+}
+// 16 consecutive FP32 columns of this warp's 32 TMEM lanes (one per thread).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&r)[16]) {
+    uint32_t u[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n\ttcgen05.wait::ld.sync.aligned;"
+        : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7]), "=r"(u[8]),
+          "=r"(u[9]), "=r"(u[10]), "=r"(u[11]), "=r"(u[12]), "=r"(u[13]), "=r"(u[14]), "=r"(u[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int q = 0; q < 16; ++q) r[q] = __uint_as_float(u[q]);
+}
 
-__global__ void __launch_bounds__(kGuessWarps * 32)
+// ---------------------------------------------------------------------------
+// Step kernel: features (optionally exported in caller order) and, when a
+// network is loaded, the initial guess x = dt (v + dv).  One CTA of 128
+// threads per 128-row tile, one row per thread: the thread gathers its
+// row's features and writes them, standardised, as row `tid` of the A
+// operand; thread 0 issues the layer's tcgen05 MMAs (M = 128, N = 64,
+// K = 32 or 64; the last layer N = 16) into the TMEM accumulator, commits
+// them to an mbarrier, and each warp reads its 32 rows back, adds the bias,
+// applies GELU and writes the next layer's A rows.  Every wait is bounded;
+// a failed wait leaves the guess of that tile as it was (the solve is
+// correct from any start) and the CTA stops predicting.
+// ---------------------------------------------------------------------------
+constexpr int kGuessThreads = 128;  // = the tile's rows = the MMA's M
+constexpr int kGuessTmemCols = 64;
+
+__global__ void __launch_bounds__(kGuessThreads)
 learned_guess_kernel(StepArgs a, DevTopo t, Vecs v, const MlpPacked* __restrict__ net, float* feat_out,
                      float* pred_out, int predict) {
-    __shared__ MlpFwd W;
-    __shared__ __align__(16) __nv_bfloat16 s_feat[kGuessWarps][32 * kT1];
-    __shared__ float s_out[kGuessWarps][32 * kMlpOutPad];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr uint32_t kSbo32 = 4 * 128, kSbo64 = 8 * 128;  // 8-row group strides for K = 32, 64
+    __shared__ __align__(1024) uint8_t s_a[kGuessThreads * kMlpHid * 2];
+    __shared__ __align__(1024) uint8_t s_w1[kMlpHid * kMlpInPad * 2];
+    __shared__ __align__(1024) uint8_t s_w2[kMlpHid * kMlpHid * 2];
+    __shared__ __align__(1024) uint8_t s_w3[kMlpHid * kMlpHid * 2];
+    __shared__ __align__(1024) uint8_t s_w4[16 * kMlpHid * 2];
+    __shared__ float s_b[3][kMlpHid], s_b4[4], s_mu[kMlpInPad], s_isd[kMlpInPad], s_muo[4], s_sdo[4];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5;
     if (predict) {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(&net->f);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(&W);
-        for (int q = threadIdx.x; q < (int)(sizeof(MlpFwd) / 4); q += blockDim.x) dst[q] = src[q];
+        // the weights as B operands ([N][K], K-major), biases and scalings
+        const MlpFwd& F = net->f;
+        for (int q = tid; q < kMlpHid * kMlpInPad; q += kGuessThreads) {
+            const int nn = q / kMlpInPad, k = q % kMlpInPad;
+            *reinterpret_cast<__nv_bfloat16*>(s_w1 + umma_off(nn, k, kSbo32)) = F.wt1[nn * kT1 + k];
+        }
+        for (int q = tid; q < kMlpHid * kMlpHid; q += kGuessThreads) {
+            const int nn = q / kMlpHid, k = q % kMlpHid;
+            *reinterpret_cast<__nv_bfloat16*>(s_w2 + umma_off(nn, k, kSbo64)) = F.wt2[nn * kTH + k];
+            *reinterpret_cast<__nv_bfloat16*>(s_w3 + umma_off(nn, k, kSbo64)) = F.wt3[nn * kTH + k];
+        }
+        for (int q = tid; q < 16 * kMlpHid; q += kGuessThreads) {
+            const int nn = q / kMlpHid, k = q % kMlpHid;
+            *reinterpret_cast<__nv_bfloat16*>(s_w4 + umma_off(nn, k, kSbo64)) =
+                nn < kMlpOutPad ? F.wt4[nn * kTH + k] : __float2bfloat16_rn(0.f);
+        }
+        for (int q = tid; q < kMlpHid; q += kGuessThreads) {
+            s_b[0][q] = F.b1[q];
+            s_b[1][q] = F.b2[q];
+            s_b[2][q] = F.b3[q];
+        }
+        if (tid < kMlpInPad) {
+            s_mu[tid] = F.mu_in[tid];
+            s_isd[tid] = F.inv_sd_in[tid];
+        }
+        if (tid < 4) {
+            s_b4[tid] = F.b4[tid];
+            s_muo[tid] = F.mu_out[tid];
+            s_sdo[tid] = F.sd_out[tid];
+        }
+        if (warp == 0) {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
+                         "r"(kGuessTmemCols)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        }
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&s_bar)), "r"(1) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        fence_async_smem();
     }
+    tc_fence_before();
     __syncthreads();
-    const int n_slices = (t.n + 31) >> 5;
-    for (int s = blockIdx.x * kGuessWarps + warp; s < n_slices; s += gridDim.x * kGuessWarps) {
-        const int i = s * 32 + lane;
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const uint32_t tmem_warp = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's 32 lanes
+    uint32_t phase = 0;
+    bool live = predict != 0;  // uniform over the CTA
+    const uint32_t a0 = smem_addr(s_a), w1 = smem_addr(s_w1), w2 = smem_addr(s_w2), w3 = smem_addr(s_w3),
+                   w4 = smem_addr(s_w4);
+    // one layer: MMAs over K in steps of 16, commit, bounded wait; every
+    // thread then reads its row of the accumulator; false after a failed wait
+    auto layer = [&](uint32_t wb, int kdim, int n) -> bool {
+        const uint32_t sbo = kdim == kMlpInPad ? kSbo32 : kSbo64;
+        fence_async_smem();  // the A rows written by every thread, for the tensor core
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (tid == 0) {
+            for (int s = 0; s < kdim / 16; ++s)
+                umma_bf16(tmem, umma_desc(a0 + 256u * s, sbo), umma_desc(wb + 256u * s, sbo), umma_idesc_bf16(n), s > 0);
+            umma_commit(&s_bar);
+        }
+        const bool ok = mbar_wait(&s_bar, phase);
+        phase ^= 1u;
+        tc_fence_after();
+        return __syncthreads_and(ok) != 0;
+    };
+    // bias, GELU and BF16 of this thread's 64 accumulator columns into its A row (K = 64 layout)
+    auto hidden = [&](const float* bias) {
+#pragma unroll
+        for (int c = 0; c < kMlpHid; c += 16) {
+            float h[16];
+            tmem_ld16(tmem_warp + c, h);
+#pragma unroll
+            for (int q = 0; q < 16; q += 8) {
+                uint4 pk;
+                pk.x = pack_bf16(gelu(h[q] + bias[c + q]), gelu(h[q + 1] + bias[c + q + 1]));
+                pk.y = pack_bf16(gelu(h[q + 2] + bias[c + q + 2]), gelu(h[q + 3] + bias[c + q + 3]));
+                pk.z = pack_bf16(gelu(h[q + 4] + bias[c + q + 4]), gelu(h[q + 5] + bias[c + q + 5]));
+                pk.w = pack_bf16(gelu(h[q + 6] + bias[c + q + 6]), gelu(h[q + 7] + bias[c + q + 7]));
+                *reinterpret_cast<uint4*>(s_a + umma_off(tid, c + q, kSbo64)) = pk;
+            }
+        }
+    };
+    const int n_tiles = (t.n + kGuessThreads - 1) / kGuessThreads;
+    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const int i = tile * kGuessThreads + tid;
         const int e = (i < t.n) ? (a.row_to_ext ? a.row_to_ext[i] : i) : -1;
         float f[kMlpIn];
 #pragma unroll
@@ -263,40 +431,52 @@ learned_guess_kernel(StepArgs a, DevTopo t, Vecs v, const MlpPacked* __restrict_
                 for (int q = 0; q < kMlpIn; ++q) feat_out[(size_t)e * kMlpIn + q] = f[q];
             }
         }
-        if (!predict) continue;
-        __nv_bfloat16* fr = s_feat[warp] + lane * kT1;
+        if (!live) continue;
+        // standardised BF16 features: row tid of A (K = 32 layout)
 #pragma unroll
-        for (int q = 0; q < kMlpInPad; ++q) {
-            const float z = q < kMlpIn ? (f[q] - W.mu_in[q]) * W.inv_sd_in[q] : 0.f;
-            fr[q] = __float2bfloat16_rn(e >= 0 ? z : 0.f);
-        }
-        __syncwarp();
+        for (int q = 0; q < kMlpInPad; q += 8) {
+            float z[8];
 #pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            float out[1][4];
-            mlp_tile_forward(W, s_feat[warp] + half * 16 * kT1, lane, out);
-            const int g = lane >> 2, tt = lane & 3;
-            float* so = s_out[warp] + half * 16 * kMlpOutPad;
-            so[g * kMlpOutPad + 2 * tt] = out[0][0];
-            so[g * kMlpOutPad + 2 * tt + 1] = out[0][1];
-            so[(g + 8) * kMlpOutPad + 2 * tt] = out[0][2];
-            so[(g + 8) * kMlpOutPad + 2 * tt + 1] = out[0][3];
+            for (int u = 0; u < 8; ++u)
+                z[u] = (e >= 0 && q + u < kMlpIn) ? (f[q + u] - s_mu[q + u]) * s_isd[q + u] : 0.f;
+            uint4 pk;
+            pk.x = pack_bf16(z[0], z[1]);
+            pk.y = pack_bf16(z[2], z[3]);
+            pk.z = pack_bf16(z[4], z[5]);
+            pk.w = pack_bf16(z[6], z[7]);
+            *reinterpret_cast<uint4*>(s_a + umma_off(tid, q, kSbo32)) = pk;
         }
-        __syncwarp();
+        if (!layer(w1, kMlpInPad, kMlpHid)) { live = false; continue; }
+        hidden(s_b[0]);
+        if (!layer(w2, kMlpHid, kMlpHid)) { live = false; continue; }
+        hidden(s_b[1]);
+        if (!layer(w3, kMlpHid, kMlpHid)) { live = false; continue; }
+        hidden(s_b[2]);
+        if (!layer(w4, kMlpHid, 16)) { live = false; continue; }
+        float o[16];
+        tmem_ld16(tmem_warp, o);
         if (e >= 0) {
-            const float* o = s_out[warp] + lane * kMlpOutPad;
             const float dt = a.dt;
-            const float3 vi = f3(f[0], f[1], f[2]);
-            const float3 dv = f3(o[0] * W.sd_out[0] + W.mu_out[0], o[1] * W.sd_out[1] + W.mu_out[1],
-                                 o[2] * W.sd_out[2] + W.mu_out[2]);
-            v.x[i] = make_float4(dt * (vi.x + dv.x), dt * (vi.y + dv.y), dt * (vi.z + dv.z), 0.f);
+            const float3 dv = f3((o[0] + s_b4[0]) * s_sdo[0] + s_muo[0], (o[1] + s_b4[1]) * s_sdo[1] + s_muo[1],
+                                 (o[2] + s_b4[2]) * s_sdo[2] + s_muo[2]);
+            v.x[i] = make_float4(dt * (f[0] + dv.x), dt * (f[1] + dv.y), dt * (f[2] + dv.z), 0.f);
             if (pred_out) {
                 pred_out[(size_t)e * 3] = dv.x;
                 pred_out[(size_t)e * 3 + 1] = dv.y;
                 pred_out[(size_t)e * 3 + 2] = dv.z;
             }
         }
-        __syncwarp();
+    }
+    // every MMA has completed (or its wait gave up: one more bounded wait
+    // for it) before the columns are released
+    if (predict) {
+        if (!live) (void)mbar_wait(&s_bar, phase ^ 1u);  // the phase whose wait gave up
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (warp == 0)
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kGuessTmemCols)
+                         : "memory");
     }
 }
 
