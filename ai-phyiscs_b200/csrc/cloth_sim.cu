@@ -123,10 +123,15 @@ void ensure_train_smem() {
     }
 }
 
+// the weight-gradient kernel's per-chunk partials: a 64 x 64 block and 64 biases per kDwRows rows
+size_t dw_partial_bytes(int rows) {
+    return (size_t)((std::max(rows, 1) + kDwRows - 1) / kDwRows) * (64 * 64 + 64) * sizeof(float);
+}
+
 size_t mlp_workspace_bytes(int rows) {
     const size_t r = (size_t)std::max(rows, 1);
     return align_up(sizeof(MlpPacked)) + 8 * align_up(r * 64 * sizeof(__nv_bfloat16)) +
-           align_up((size_t)train_blocks(rows) * kTrainWarps * sizeof(double));
+           align_up((size_t)train_blocks(rows) * kTrainWarps * sizeof(double)) + align_up(dw_partial_bytes(rows));
 }
 
 // Forward + backward (when targets != 0) of rows feature vectors; grads in
@@ -153,6 +158,10 @@ void mlp_gradients(uintptr_t params, uintptr_t features, uintptr_t targets, int 
         off += mat;
     }
     bufs.sse = reinterpret_cast<double*>(ws + off);
+    off += align_up((size_t)train_blocks(rows) * kTrainWarps * sizeof(double));
+    const int chunks = (rows + kDwRows - 1) / kDwRows;
+    float* part_w = reinterpret_cast<float*>(ws + off);
+    float* part_b = part_w + (size_t)chunks * 64 * 64;
     bufs.out = reinterpret_cast<float*>(dv_out);
     mlp_pack_kernel<<<8, 256, 0, stream>>>(reinterpret_cast<const float*>(params), packed);
     ck(cudaGetLastError(), "mlp_pack_kernel launch");
@@ -173,10 +182,17 @@ void mlp_gradients(uintptr_t params, uintptr_t features, uintptr_t targets, int 
             {kMlpIn, kMlpHid, O::w1, O::b1}, {kMlpHid, kMlpHid, O::w2, O::b2},
             {kMlpHid, kMlpHid, O::w3, O::b3}, {kMlpHid, kMlpOut, O::w4, O::b4}};
         for (int l = 0; l < 4; ++l) {
-            const int tiles = ((layers[l].in + 15) / 16) * ((layers[l].out + 7) / 8);
-            mlp_dw_kernel<<<(tiles + 3) / 4, 128, 0, stream>>>(bufs.act[l], bufs.dz[l], rows, layers[l].in,
-                                                               layers[l].out, g + layers[l].w, g + layers[l].b);
+            // kDwPadSmem bytes of unused dynamic shared memory hold an SM to
+            // at most 6 of these CTAs (6 x 64 TMEM columns of 512), so no CTA
+            // waits in tcgen05.alloc
+            mlp_dw_kernel<<<chunks, kDwThreads, kDwPadSmem, stream>>>(bufs.act[l], bufs.dz[l], rows, layers[l].in,
+                                                                      layers[l].out, part_w, part_b);
             ck(cudaGetLastError(), "mlp_dw_kernel launch");
+            const int outs = layers[l].in * layers[l].out + layers[l].out;
+            mlp_dw_reduce_kernel<<<(outs + 255) / 256, 256, 0, stream>>>(part_w, part_b, chunks, layers[l].in,
+                                                                        layers[l].out, g + layers[l].w,
+                                                                        g + layers[l].b);
+            ck(cudaGetLastError(), "mlp_dw_reduce_kernel launch");
         }
         if (loss) {
             std::vector<double> part((size_t)blocks * kTrainWarps);
@@ -213,7 +229,8 @@ constexpr int kNoAllocPartials = (kNoAllocMaxRows + 16 * kTrainWarps - 1) / (16 
 // the layout of mlp_workspace_bytes(kNoAllocMaxRows)
 constexpr size_t kNoAllocScratchBytes =
     align_up_c(sizeof(MlpPacked)) + 8 * align_up_c((size_t)kNoAllocMaxRows * 64 * sizeof(__nv_bfloat16)) +
-    align_up_c((size_t)kNoAllocPartials * sizeof(double));
+    align_up_c((size_t)kNoAllocPartials * sizeof(double)) +
+    align_up_c((size_t)((kNoAllocMaxRows + kDwRows - 1) / kDwRows) * (64 * 64 + 64) * sizeof(float));
 static_assert(kNoAllocPartials <= 1184 * kTrainWarps, "partials follow train_blocks()");
 
 static __device__ __align__(256) unsigned char g_mlp_noalloc_scratch[kNoAllocScratchBytes];

@@ -674,52 +674,117 @@ mlp_train_tile_kernel(const MlpPacked* __restrict__ net, const float* __restrict
     if (lane == 0) bufs.sse[(size_t)blockIdx.x * kTrainWarps + warp] = sse;
 }
 
-// Weight gradients of layer l: G[in][out] = sum_rows A[row][in] dZ[row][out]
-// (tensor cores, K = rows), bias gradients sum_rows dZ[row][out].  One warp
-// per 16 x 8 output tile; deterministic (each warp owns its tile).
-__global__ void mlp_dw_kernel(const __nv_bfloat16* __restrict__ act, const __nv_bfloat16* __restrict__ dz,
-                              int rows, int in_dim, int out_dim, float* __restrict__ gw, float* __restrict__ gb) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    const int g = lane >> 2, t = lane & 3;
-    const int m_tiles = (in_dim + 15) / 16, n_tiles = (out_dim + 7) / 8;
-    if (warp >= m_tiles * n_tiles) return;
-    const int mt = warp / n_tiles, nt = warp % n_tiles;
-    float acc[4] = {0.f, 0.f, 0.f, 0.f};
-    float bacc = 0.f;
-    auto A = [&](int m, int k) -> __nv_bfloat16 {  // A(m=in, k=row)
-        return (k < rows && m < in_dim) ? act[(size_t)k * 64 + m] : __float2bfloat16_rn(0.f);
+// Weight gradients on the fifth-generation tensor cores, split over the
+// rows (the GEMM's K): CTA c forms the partial dW = act^T dz of rows
+// [c kDwRows, (c + 1) kDwRows) as one M = 128 (in features, padded with
+// zero rows) x N = 64 (out features, zero-padded) MMA chain from shared
+// memory -- both operands MN-major (features contiguous, as act and dz are
+// stored [row][64]) in the no-swizzle layout -- into TMEM, and its partial
+// bias gradient; mlp_dw_reduce_kernel adds the partials in chunk order.
+constexpr int kDwRows = 64;
+constexpr int kDwThreads = 128;
+constexpr int kDwPadSmem = 12 * 1024;
+__host__ __device__ constexpr uint32_t umma_idesc_bf16_mn(int n) {
+    return umma_idesc_bf16(n) | (1u << 15) | (1u << 16);  // A and B MN-major
+}
+__global__ void __launch_bounds__(kDwThreads)
+mlp_dw_kernel(const __nv_bfloat16* __restrict__ act, const __nv_bfloat16* __restrict__ dz, int rows, int in_dim,
+              int out_dim, float* __restrict__ part_w, float* __restrict__ part_b) {
+    constexpr uint32_t kSbo = (kDwRows / 8) * 128;  // bytes between 8-feature groups
+    __shared__ __align__(1024) uint8_t s_a[128 * kDwRows * 2];
+    __shared__ __align__(1024) uint8_t s_b[64 * kDwRows * 2];
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5, c = blockIdx.x;
+    const int r0 = c * kDwRows, nr = min(kDwRows, rows - r0);
+    // element (f, k) of a feature-major operand: feature group f / 8 at
+    // kSbo, row group k / 8 at 128 bytes, row k % 8 at 16, feature f % 8 at 2
+    auto keep8 = [](uint4 v, int f0, int dim) {  // features f0 .. f0 + 7, those >= dim zeroed
+        uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t lo = f0 + 2 * q < dim ? 0x0000FFFFu : 0u, hi = f0 + 2 * q + 1 < dim ? 0xFFFF0000u : 0u;
+            w[q] &= lo | hi;
+        }
+        return make_uint4(w[0], w[1], w[2], w[3]);
     };
-    auto B = [&](int k, int n) -> __nv_bfloat16 {  // B(k=row, n=out)
-        return (k < rows && n < out_dim) ? dz[(size_t)k * 64 + n] : __float2bfloat16_rn(0.f);
-    };
-    auto pk = [](__nv_bfloat16 lo, __nv_bfloat16 hi) {
-        __nv_bfloat162 v;
-        v.x = lo;
-        v.y = hi;
-        return *reinterpret_cast<uint32_t*>(&v);
-    };
-    const int m0 = mt * 16, n0 = nt * 8;
-    for (int k0 = 0; k0 < rows; k0 += 16) {
-        uint32_t a[4];
-        a[0] = pk(A(m0 + g, k0 + 2 * t), A(m0 + g, k0 + 2 * t + 1));
-        a[1] = pk(A(m0 + g + 8, k0 + 2 * t), A(m0 + g + 8, k0 + 2 * t + 1));
-        a[2] = pk(A(m0 + g, k0 + 2 * t + 8), A(m0 + g, k0 + 2 * t + 9));
-        a[3] = pk(A(m0 + g + 8, k0 + 2 * t + 8), A(m0 + g + 8, k0 + 2 * t + 9));
-        const uint32_t b0 = pk(B(k0 + 2 * t, n0 + g), B(k0 + 2 * t + 1, n0 + g));
-        const uint32_t b1 = pk(B(k0 + 2 * t + 8, n0 + g), B(k0 + 2 * t + 9, n0 + g));
-        float d[4] = {acc[0], acc[1], acc[2], acc[3]};
-        mma16816(d, a, b0, b1);
-        acc[0] = d[0]; acc[1] = d[1]; acc[2] = d[2]; acc[3] = d[3];
-        if (mt == 0 && lane < 8) {
-            for (int q = 0; q < 16; ++q) bacc += __bfloat162float(B(k0 + q, n0 + lane));
+    for (int x = tid; x < kDwRows * 8; x += kDwThreads) {
+        const int k = x >> 3, g = x & 7;
+        uint4 va = make_uint4(0u, 0u, 0u, 0u), vb = va;
+        if (k < nr) {
+            va = keep8(*reinterpret_cast<const uint4*>(act + (size_t)(r0 + k) * 64 + g * 8), g * 8, in_dim);
+            vb = keep8(*reinterpret_cast<const uint4*>(dz + (size_t)(r0 + k) * 64 + g * 8), g * 8, out_dim);
+        }
+        const uint32_t off = (uint32_t)g * kSbo + (uint32_t)(k >> 3) * 128u + (uint32_t)(k & 7) * 16u;
+        *reinterpret_cast<uint4*>(s_a + off) = va;
+        *reinterpret_cast<uint4*>(s_b + off) = vb;
+    }
+    for (int x = tid; x < 8 * (int)kSbo / 16; x += kDwThreads)  // feature groups 8..15 of A: zero
+        reinterpret_cast<uint4*>(s_a + 8 * kSbo)[x] = make_uint4(0u, 0u, 0u, 0u);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
+                     "r"(64)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&s_bar)), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    if (tid == 0) {
+        const uint32_t a0 = smem_addr(s_a), b0 = smem_addr(s_b);
+        for (int s = 0; s < kDwRows / 16; ++s)
+            umma_bf16(tmem, umma_desc(a0 + 256u * s, kSbo), umma_desc(b0 + 256u * s, kSbo), umma_idesc_bf16_mn(64),
+                      s > 0);
+        umma_commit(&s_bar);
+    }
+    const bool ok = __syncthreads_and(mbar_wait(&s_bar, 0)) != 0;
+    tc_fence_after();
+    float* pw = part_w + (size_t)c * 64 * 64;
+    if (warp < 2) {  // TMEM lanes 0..63: the in features
+        const int m = tid;
+#pragma unroll
+        for (int c16 = 0; c16 < 64; c16 += 16) {
+            float h[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c16, h);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) pw[m * 64 + c16 + q] = ok ? h[q] : __int_as_float(0x7fc00000);
         }
     }
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-        const int m = m0 + g + 8 * (e >> 1), n = n0 + 2 * t + (e & 1);
-        if (m < in_dim && n < out_dim) gw[(size_t)m * out_dim + n] = acc[e];
+    if (tid < 64) {  // partial bias gradient of output tid
+        float bacc = 0.f;
+        if (tid < out_dim)
+            for (int k = 0; k < nr; ++k) bacc += __bfloat162float(dz[(size_t)(r0 + k) * 64 + tid]);
+        part_b[(size_t)c * 64 + tid] = bacc;
     }
-    if (mt == 0 && lane < 8 && n0 + lane < out_dim) gb[n0 + lane] = bacc;
+    if (!ok) (void)mbar_wait(&s_bar, 0);  // the MMAs must be done before the columns go
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
+}
+
+// gw[in][out] and gb[out]: the chunks' partials added in chunk order.
+__global__ void mlp_dw_reduce_kernel(const float* __restrict__ part_w, const float* __restrict__ part_b, int chunks,
+                                     int in_dim, int out_dim, float* __restrict__ gw, float* __restrict__ gb) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < in_dim * out_dim) {
+        const int m = q / out_dim, n = q % out_dim;
+        float acc = 0.f;
+        for (int c = 0; c < chunks; ++c) acc += part_w[(size_t)c * 64 * 64 + m * 64 + n];
+        gw[q] = acc;
+    } else if (q < in_dim * out_dim + out_dim) {
+        const int n = q - in_dim * out_dim;
+        float acc = 0.f;
+        for (int c = 0; c < chunks; ++c) acc += part_b[(size_t)c * 64 + n];
+        gb[n] = acc;
+    }
 }
 
 // Adam on the FP32 master weights (only the trainable slice, from w1).
