@@ -321,7 +321,7 @@ int chysx_mlp_noalloc_max_rows(void);
 /* chysx_mlp_gradients without a workspace argument (no counterpart in the
  * reference, which has no training entry point at all).  Same kernels, same
  * results; the workspace is a fixed static device array inside this library
- * (4,243,712 bytes per device, enough for CHYSX_MLP_NOALLOC_MAX_ROWS rows),
+ * (5,308,672 bytes per device, enough for CHYSX_MLP_NOALLOC_MAX_ROWS rows),
  * so the call allocates no device memory and, on success, no host memory.
  * It is for callers that cannot allocate: a host program that drives the
  * training through this C ABI (ctypes, cgo, JNI) without a device allocator
