@@ -8,9 +8,13 @@ constexpr int kCoarseMaxBlocks = 160;  // CTAs of a two-level plan (one warp's s
 constexpr int kCoarseMaxNbr = 16;      // coarse blocks one block's rows touch, itself included
 // The streamed kernel's coarse level (systems too large for the register-
 // resident kernel): coarse blocks of about kCoarseStreamRows rows, at most
-// kCoarseDenseMax unknowns, A_c inverted densely once per step
-constexpr int kCoarseStreamRows = 8192;
-constexpr int kCoarseDenseMax = 2048;
+// kCoarseDenseMax unknowns, A_c inverted densely once per step.  Measured
+// on the 1024 x 1024 configuration (10 steps): blocks of 3, 2 and 5 CTAs
+// (~5,300, ~3,500 and ~8,900 rows) took 1,383, 1,269 and 1,662 iterations
+// per step at 124, 131 and 119 us per iteration with 7.6, 19.4 and 3.7 ms of
+// coarse set-up: 5.59, 5.37 and 4.95 steps/s
+constexpr int kCoarseStreamRows = 5120;
+constexpr int kCoarseDenseMax = 2560;
 constexpr int kCoarseInvertThreads = 256;
 // CTAs per coarse block of the register-resident kernel's level (1,024 rows
 // at 512 rows per CTA).  Measured on the 256 x 256 configuration: 2-CTA

@@ -424,7 +424,7 @@ int chysx_cloth_row_of_particles(const chysx_cloth* h, int n, int32_t* rows);
  * 160 CTAs and acts as kind 1 elsewhere.  Kinds 1 and 2 apply where the
  * register-resident kernel runs with synchronisation mode 0.  On systems too
  * large for that kernel (the streamed kernel), kinds 1 and 2 give
- * block-Jacobi plus the coarse level on blocks of about 8192 rows, A_c
+ * block-Jacobi plus the coarse level on blocks of about 5120 rows, A_c
  * shifted by 1e-5 diag(A_c) (single instance, synchronisation mode 0).
  * in_use reports what the last graph build uses (0 block-Jacobi, 1 local,
  * 2 two-level with translations, 3 two-level with translations and linear

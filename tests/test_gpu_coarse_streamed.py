@@ -1,5 +1,5 @@
 """GPU: the streamed kernel's two-level preconditioner (block-Jacobi plus the
-coarse level of translation and linear fields on blocks of ~8192 rows, A_c
+coarse level of translation and linear fields on blocks of ~5120 rows, A_c
 inverted densely every step) against the FP64 oracle's restatement of the
 same operator on the same blocks."""
 import numpy as np
@@ -73,8 +73,8 @@ def oracle_sim(sc, tol, coarse_rows=0, state=None):
 
 
 def test_streamed_coarse_steps_match_fp64_oracle_and_its_iterations():
-    # 192^2: 144 CTAs of 256 rows, coarse blocks of 32 CTAs = 8192 rows
-    # (five blocks, the last one half size), 60 unknowns
+    # 192^2: 144 CTAs of 256 rows, coarse blocks of 20 CTAs = 5120 rows
+    # (eight blocks, the last one of 4 CTAs), 96 unknowns
     sc = scenes.config_large(side=192)
     g = gpu(sc)
     n = sc["pos"].shape[0]
@@ -92,7 +92,7 @@ def test_streamed_coarse_steps_match_fp64_oracle_and_its_iterations():
     # the same operator in the oracle, on the device's row blocks
     order = np.argsort(g.sim.row_of_particles(n))
     ps = permuted(sc, order)
-    o = oracle_sim(ps, 1e-6, coarse_rows=8192)
+    o = oracle_sim(ps, 1e-6, coarse_rows=5120)
     for _ in range(3):
         o.step(sc["dt"])
         oits.append(o.stats()[0])
@@ -100,7 +100,7 @@ def test_streamed_coarse_steps_match_fp64_oracle_and_its_iterations():
     # device's own A_c with its relative diagonal shift of 1e-5 (rows rounded
     # to FP32 once)
     info, ac, ainv = g.sim.debug_coarse()
-    assert (info["on"], info["fields"], info["blocks"]) == (1, 4, 5)
+    assert (info["on"], info["fields"], info["blocks"]) == (1, 4, 8)
     keep = np.diag(ac) != 0
     A = ac[np.ix_(keep, keep)].astype(np.float64)
     inv = np.linalg.inv(A + 1e-5 * np.diag(np.diag(A)))
