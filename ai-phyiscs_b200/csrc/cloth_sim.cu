@@ -1028,8 +1028,19 @@ public:
                         for (int c = 0; c < U; ++c) ac[(size_t)(B * U + r) * m + C * U + c] = b[r * U + c];
                 }
         }
-        if (ainv)
+        if (ainv && coarse_batched_) {
+            // the batched level's block-diagonal inverse: one U x U block per instance
+            std::vector<float> blocks((size_t)coarse_nb_ * U * U);
+            ck(cudaMemcpy(blocks.data(), d_cainv_.get(), blocks.size() * sizeof(float), cudaMemcpyDeviceToHost),
+               "copy A_c^-1 blocks");
+            std::fill(ainv, ainv + (size_t)m * m, 0.0f);
+            for (int B = 0; B < coarse_nb_; ++B)
+                for (int r = 0; r < U; ++r)
+                    for (int c = 0; c < U; ++c)
+                        ainv[(size_t)(B * U + r) * m + B * U + c] = blocks[((size_t)B * U + r) * U + c];
+        } else if (ainv) {
             ck(cudaMemcpy(ainv, d_cainv_.get(), (size_t)m * m * sizeof(float), cudaMemcpyDeviceToHost), "copy A_c^-1");
+        }
     }
     void debug_dump(float* diag, int32_t* rp, int32_t* col, float* vals, float* rhs, float* dx) {
         const int n = topo_.n_ext;
@@ -1370,6 +1381,11 @@ private:
                        ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, kResidentMaxWidth, SYNC>)
                        : reinterpret_cast<const void*>(&pcg_resident_kernel<8, kResidentMaxWidth, SYNC>);
         }
+        if (coarse_on_ && SYNC == 0 && coarse_batched_) {
+            if (pcg_block_ == 128) return reinterpret_cast<const void*>(&pcg_persistent_kernel<128, 0, 2>);
+            if (pcg_block_ == 512) return reinterpret_cast<const void*>(&pcg_persistent_kernel<512, 0, 2>);
+            return reinterpret_cast<const void*>(&pcg_persistent_kernel<256, 0, 2>);
+        }
         if (coarse_on_ && SYNC == 0) {
             if (pcg_block_ == 128) return reinterpret_cast<const void*>(&pcg_persistent_kernel<128, 0, 1>);
             if (pcg_block_ == 512) return reinterpret_cast<const void*>(&pcg_persistent_kernel<512, 0, 1>);
@@ -1530,7 +1546,14 @@ private:
     }
     void plan_coarse() {
         coarse_on_ = false;
-        if (pc_kind_ != 2 || sync_mode_ != 0 || plan_.n_inst != 1) return;
+        coarse_batched_ = false;
+        if (pc_kind_ != 2 || sync_mode_ != 0) return;
+        if (plan_.n_inst != 1) {
+            // several instances on the streamed kernel, zero-guess solves:
+            // one coarse block per instance
+            if (!resident_ && warm_mode_ == CHYSX_WARM_ZERO) plan_coarse_batched();
+            return;
+        }
         if (!resident_) {
             // streamed kernel: coarse blocks of G CTAs, about
             // kCoarseStreamRows rows each, translation and linear fields,
@@ -1548,6 +1571,59 @@ private:
         if (plan_.grid > kCoarseMaxBlocks) return;
         if (plan_.grid >= 8 && plan_coarse_with(kCoarseResidentCtas, 4, 0.0)) return;
         plan_coarse_with(1, 1, 0.0);
+    }
+    // The batched coarse level of the streamed kernel: one coarse block per
+    // instance (its rows, translation and linear fields: 12 unknowns), so
+    // A_c is block-diagonal and each instance's 12 x 12 block is inverted
+    // on its own (coarse_invert_batched_kernel).
+    void plan_coarse_batched() {
+        const int nb = plan_.n_inst, ns = topo_.n_slices, nq = 4, U = 3 * nq, mn = 1;
+        std::vector<int> slice_cb(std::max(1, ns), 0), row0(nb + 1, 0);
+        for (int sl = 0; sl < ns; ++sl) slice_cb[sl] = plan_.slice_inst[sl];
+        for (int B = 0; B <= nb; ++B) row0[B] = plan_.inst_slice[B] * 32;
+        std::vector<int> nbr(nb), cnt(nb, 1), self(nb, 0);
+        for (int B = 0; B < nb; ++B) nbr[B] = B;
+        std::vector<unsigned char> ell(std::max<size_t>(1, topo_.col.size()), 0);
+        d_slice_cb_.upload(slice_cb);
+        d_cb_row0_.upload(row0);
+        d_cnbr_.upload(nbr);
+        d_ccnt_.upload(cnt);
+        d_cself_.upload(self);
+        d_ell_nbr_.upload(ell);
+        d_cw_.resize((size_t)std::max(1, row0[nb]));
+        d_cw_.zero();
+        d_cac_.resize((size_t)nb * mn * U * U);
+        d_cac_.zero();
+        int spb = 1;
+        for (int B = 0; B < nb; ++B) spb = std::max(spb, (row0[B + 1] - row0[B] + 31) / 32);
+        const int splits = std::min(kCoarseMaxSplits, std::max(1, (spb + kCoarseSplitSlices - 1) / kCoarseSplitSlices));
+        d_cacp_.resize((size_t)splits * nb * mn * U * U);
+        d_cainv_.resize((size_t)nb * U * U);
+        d_cainv_.zero();
+        d_cfail_.resize(1);
+        d_cfail_.zero();
+        d_cbar_.resize(1);
+        d_cbar_.zero();
+        coarse_shift_ = kCoarseShift;
+        coarse_nb_ = nb;
+        coarse_mn_ = mn;
+        coarse_splits_ = splits;
+        coarse_g_ = 1;
+        coarse_nq_ = nq;
+        coarse_on_ = true;
+        coarse_batched_ = true;
+        const CoarseArgs cargs = coarse_args();
+        d_cargs_.upload(&cargs, 1);
+        ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_assemble_kernel),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_assemble_smem()),
+           "cudaFuncSetAttribute(coarse assemble smem)");
+    }
+    // the streamed kernel's shared memory for its coarse level: the block
+    // values (dense level) or the per-instance values (batched level)
+    size_t coarse_stream_smem() const {
+        if (!coarse_on_) return 0;
+        if (coarse_batched_) return (size_t)plan_.max_inst_per_cta * kInstCoarseW * sizeof(float) + 16;
+        return (size_t)3 * coarse_nq_ * coarse_nb_ * sizeof(float) + 16;
     }
     // per-lane partial sums of the coarse assembly: [nq][9][max_nbr][32] floats
     size_t coarse_assemble_smem() const {
@@ -1572,7 +1648,8 @@ private:
         c.acp = d_cacp_.get();
         c.splits = coarse_splits_;
         c.ainv = d_cainv_.get();
-        c.dense = resident_ ? 0 : 1;
+        c.dense = resident_ || coarse_batched_ ? 0 : 1;
+        c.batched = coarse_batched_ ? 1 : 0;
         c.shift = coarse_shift_;
         c.work = d_cwork_.get();
         c.fail = d_cfail_.get();
@@ -1610,8 +1687,9 @@ private:
         }
         plan_coarse();
         if (coarse_on_) {
-            // the coarse restriction sums of every block (m floats) behind the records
-            pers_smem_ += (size_t)3 * coarse_nq_ * coarse_nb_ * sizeof(float) + 16;
+            // the coarse block values (or the batched level's per-instance values) behind the records
+            const size_t extra = coarse_stream_smem();
+            pers_smem_ += extra;
             ck(cudaFuncSetAttribute(persistent_fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pers_smem_),
                "cudaFuncSetAttribute(persistent smem)");
             int per_sm = 0;
@@ -1619,7 +1697,8 @@ private:
                "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
             if (per_sm * sms < plan_.grid) {
                 coarse_on_ = false;  // the extra shared memory costs co-residency: plain block-Jacobi
-                pers_smem_ -= (size_t)3 * coarse_nq_ * coarse_nb_ * sizeof(float) + 16;
+                coarse_batched_ = false;
+                pers_smem_ -= extra;
             }
         }
         upload_plan();
@@ -1632,7 +1711,7 @@ private:
         const size_t li_bytes = (size_t)plan_.max_inst_per_cta * sizeof(LocalInst);
         size_t need = resident_ ? (size_t)resident_warps_ * kSlotW * sizeof(double) + li_bytes
                                 : (size_t)plan_.max_slices_per_cta * kSlotW * sizeof(double) + li_bytes;
-        if (!resident_ && coarse_on_) need += (size_t)3 * coarse_nq_ * coarse_nb_ * sizeof(float) + 16;
+        if (!resident_) need += coarse_stream_smem();
         if (pers_smem_ < need || (resident_ && plan_.max_slices_per_cta > resident_warps_) ||
             (!resident_ && pcg_block_ / 32 < 1))
             throw std::logic_error("persistent PCG plan is inconsistent with the selected kernel");
@@ -1827,26 +1906,37 @@ private:
                 mp.dst = d_cfail_.get();
                 mp.width = 1;
                 ck(cudaGraphAddMemsetNode(&z2, graph_, &z1, 1, &mp), "add coarse fail reset node");
-                int dev = 0, sms = 0;
-                ck(cudaGetDevice(&dev), "cudaGetDevice");
-                ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
-                GridBarrier* gb = d_cbar_.get();
-                void* a2[] = {&cg, &gb};
-                cudaKernelNodeParams p2{};
-                // two CTAs per SM where they fit (the tile phases are latency-bound)
-                int inv_per_sm = 0;
-                ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&inv_per_sm, coarse_invert_kernel,
-                                                                 kCoarseInvertThreads, 0),
-                   "cudaOccupancyMaxActiveBlocksPerMultiprocessor(coarse invert)");
-                p2.func = reinterpret_cast<void*>(&coarse_invert_kernel);
-                p2.gridDim = dim3(sms * std::max(1, std::min(2, inv_per_sm)));
-                p2.blockDim = dim3(kCoarseInvertThreads);
-                p2.kernelParams = a2;
-                ck(cudaGraphAddKernelNode(&n2, graph_, &z2, 1, &p2), "add coarse invert node");
-                cudaLaunchAttributeValue coop{};
-                coop.cooperative = 1;
-                ck(cudaGraphKernelNodeSetAttribute(n2, cudaLaunchAttributeCooperative, &coop),
-                   "cooperative attribute (coarse invert)");
+                if (coarse_batched_) {
+                    // one CTA per instance: its 12 x 12 block of A_c
+                    void* ab[] = {&cg};
+                    cudaKernelNodeParams pb{};
+                    pb.func = reinterpret_cast<void*>(&coarse_invert_batched_kernel);
+                    pb.gridDim = dim3(coarse_nb_);
+                    pb.blockDim = dim3(kBatchInvThreads);
+                    pb.kernelParams = ab;
+                    ck(cudaGraphAddKernelNode(&n2, graph_, &z2, 1, &pb), "add batched coarse invert node");
+                } else {
+                    int dev = 0, sms = 0;
+                    ck(cudaGetDevice(&dev), "cudaGetDevice");
+                    ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+                    GridBarrier* gb = d_cbar_.get();
+                    void* a2[] = {&cg, &gb};
+                    cudaKernelNodeParams p2{};
+                    // two CTAs per SM where they fit (the tile phases are latency-bound)
+                    int inv_per_sm = 0;
+                    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&inv_per_sm, coarse_invert_kernel,
+                                                                     kCoarseInvertThreads, 0),
+                       "cudaOccupancyMaxActiveBlocksPerMultiprocessor(coarse invert)");
+                    p2.func = reinterpret_cast<void*>(&coarse_invert_kernel);
+                    p2.gridDim = dim3(sms * std::max(1, std::min(2, inv_per_sm)));
+                    p2.blockDim = dim3(kCoarseInvertThreads);
+                    p2.kernelParams = a2;
+                    ck(cudaGraphAddKernelNode(&n2, graph_, &z2, 1, &p2), "add coarse invert node");
+                    cudaLaunchAttributeValue coop{};
+                    coop.cooperative = 1;
+                    ck(cudaGraphKernelNodeSetAttribute(n2, cudaLaunchAttributeCooperative, &coop),
+                       "cooperative attribute (coarse invert)");
+                }
             }
             t1 = n2;
         }
@@ -2131,6 +2221,7 @@ private:
     int pc_kind_ = 0, pc_degree_ = 0;  // preconditioner: 0 block-Jacobi, 1 CTA-local Chebyshev, 2 + coarse level
     bool coarse_on_ = false;
     int coarse_nb_ = 0, coarse_mn_ = 0, coarse_g_ = 1, coarse_nq_ = 1, coarse_splits_ = 1;
+    bool coarse_batched_ = false;  // the streamed kernel's per-instance level (plan_coarse_batched)
     double coarse_shift_ = 0.0;
     DevBuf<int> d_slice_cb_, d_cb_row0_, d_cnbr_, d_ccnt_, d_cself_;
     DevBuf<unsigned char> d_ell_nbr_;

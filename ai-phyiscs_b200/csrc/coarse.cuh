@@ -227,6 +227,64 @@ __global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, CoarseA
     }
 }
 
+// Inverse of the block-diagonal A_c of the batched coarse level (one coarse
+// block per instance): one CTA per instance adds the assembly's splits of
+// its U x U block in order and rounds them once to FP32 (the stored A_c),
+// scales by S = diag^-1/2, shifts by ca.shift I and inverts by Gauss-Jordan
+// without pivoting in FP64 shared memory (one entry per thread, two
+// buffers, one CTA barrier per pivot); an unknown whose field has zero
+// weight on the whole instance gets an identity row.  Output S W S (FP32)
+// into ca.ainv[b][U][U]; a non-positive pivot sets ca.fail (the level is
+// then off in the step's solve).
+constexpr int kBatchInvThreads = 160;  // >= 12 x 12 entries
+__global__ void __launch_bounds__(kBatchInvThreads) coarse_invert_batched_kernel(CoarseArgs ca) {
+    constexpr int kU = 12;
+    __shared__ double a[2][kU][kU + 1];
+    __shared__ double s_sc[kU];
+    const int B = blockIdx.x, U = 3 * ca.nq, tid = threadIdx.x;
+    const int r = tid / U, c = tid % U;
+    const bool mine = tid < U * U;
+    const size_t base = (size_t)B * U * U, total = (size_t)ca.nb * U * U;
+    if (mine) {
+        double v = 0.0;
+        for (int z = 0; z < ca.splits; ++z) v += __ldcg(ca.acp + (size_t)z * total + base + tid);
+        const float vf = (float)v;
+        ca.ac[base + tid] = vf;
+        a[0][r][c] = (double)vf;
+    }
+    __syncthreads();
+    if (tid < U) {
+        const double d = a[0][tid][tid];
+        s_sc[tid] = d > 0.0 ? 1.0 / sqrt(d) : 0.0;
+    }
+    __syncthreads();
+    if (mine) {
+        const double si = s_sc[r], sj = s_sc[c];
+        a[0][r][c] = si == 0.0 || sj == 0.0 ? (r == c ? 1.0 : 0.0) : a[0][r][c] * si * sj + (r == c ? ca.shift : 0.0);
+    }
+    __syncthreads();
+    int cur = 0;
+    bool bad = false;
+    for (int k = 0; k < U; ++k) {
+        const double p = a[cur][k][k];
+        const bool good = p > 1.0e-12;
+        bad = bad || !good;
+        const double ip = good ? 1.0 / p : 0.0;
+        if (mine) {
+            // row k: (c == k ? 1 : a_kc) / p; the others subtract a_rk times it
+            const double rk = (c == k ? 1.0 : a[cur][k][c]) * ip;
+            a[cur ^ 1][r][c] = r == k ? rk : fma(-a[cur][r][k], rk, c == k ? 0.0 : a[cur][r][c]);
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+    if (bad && tid == 0) atomicExch(ca.fail, 1);
+    if (mine) {
+        const double vv = a[cur][r][c] * s_sc[r] * s_sc[c];
+        ca.ainv[base + tid] = (bad || !isfinite(vv)) ? 0.0f : (float)vv;
+    }
+}
+
 // Dense inverse of A_c for both two-level preconditioners (m <=
 // kCoarseDenseMax): FP64 blocked Gauss-Jordan elimination in place on the
 // symmetrically scaled and shifted matrix S A_c S + ca.shift I

@@ -73,6 +73,10 @@ struct CoarseArgs {
     // (the coarse level then adds nothing in that step's solve); dense = 1:
     // the streamed kernel's level (its CTAs read their rows from L2)
     int dense = 0;
+    // batched = 1: the streamed kernel's level for several instances, one
+    // coarse block per instance (A_c block-diagonal; ainv holds each
+    // instance's U x U inverse, [nb][U][U])
+    int batched = 0;
     double shift = 0.0;
     double* work = nullptr;
     int* fail = nullptr;

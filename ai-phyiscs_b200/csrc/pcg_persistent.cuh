@@ -889,15 +889,41 @@ __device__ __forceinline__ void instances_fail(const BatchPlan& bp, const LocalI
 __device__ __forceinline__ float* slice_cpart(double* spart, int sl) {
     return reinterpret_cast<float*>(spart + (size_t)sl * kSlotW + kCoarseOff);
 }
-// The CTA's restriction (sum of its slices' partials, in slice order) into
-// its slot of `set`; threads 0..U-1 of the calling warp.
-__device__ __forceinline__ void coarse_publish_cta(const BatchPlan& bp, int U, double* spart, int nsl, int own_slot,
-                                                   int set, int lane) {
-    if (lane < U) {
+// The restriction of each of the CTA's segments (an instance's slices in
+// this CTA, or all of them for the single-instance level) into the
+// segment's slot of `set`, by the whole CTA: P threads per value each add
+// every P-th slice's partial, then one thread adds the P sums in order (a
+// fixed order: bitwise repeatable).  seg(q, lo, hi, slot) gives segment q's
+// slices [lo, hi) relative to the CTA's first slice and its slot; tmp holds
+// BLOCK floats.  Called by every thread; ends with a __syncthreads.
+template <int BLOCK, typename Seg>
+__device__ __forceinline__ void coarse_publish(const BatchPlan& bp, int U, double* spart, int nseg, Seg&& seg,
+                                               int set, float* tmp) {
+    const int nv = nseg * 12;
+    const int P = nv == 0 || 2 * nv > BLOCK ? 1 : min(8, BLOCK / nv);
+    for (int x = threadIdx.x; x < nv * P; x += BLOCK) {
+        const int h = x % P, qu = x / P, q = qu / 12, u = qu - 12 * q;
+        int lo, hi, slot;
+        seg(q, lo, hi, slot);
         float acc = 0.0f;
-        for (int sl = 0; sl < nsl; ++sl) acc += slice_cpart(spart, sl)[lane];
-        coarse_slot(bp, set, own_slot)[lane] = acc;
+        if (u < U)
+            for (int sl = lo + h; sl < hi; sl += P) acc += slice_cpart(spart, sl)[u];
+        if (P > 1) tmp[x] = acc;
+        else if (u < U) coarse_slot(bp, set, slot)[u] = acc;
     }
+    if (P > 1) {
+        __syncthreads();
+        for (int x = threadIdx.x; x < nv; x += BLOCK) {
+            const int q = x / 12, u = x - 12 * q;
+            if (u >= U) continue;
+            int lo, hi, slot;
+            seg(q, lo, hi, slot);
+            float acc = 0.0f;
+            for (int h = 0; h < P; ++h) acc += tmp[x * P + h];
+            coarse_slot(bp, set, slot)[u] = acc;
+        }
+    }
+    __syncthreads();
 }
 template <int BLOCK>
 __device__ __forceinline__ void coarse_apply_dense(const BatchPlan& bp, const CoarseRegs& cr, int set, float* vbuf,
@@ -1008,6 +1034,59 @@ __device__ __forceinline__ void coarse_apply_dense(const BatchPlan& bp, const Co
     __syncthreads();
 }
 
+// ---- batched coarse level of the streamed kernel: one coarse block per
+// instance, so A_c is block-diagonal and an instance's coarse values ride
+// on its own reduction slots.  Per local instance the CTA keeps
+// kInstCoarseW floats: A_b^-1 R_b^T r (kCU) and of the new r (kCN).
+constexpr int kInstCoarseW = 24, kCU = 0, kCN = 12;
+// Each unfinished local instance's 12 values of y = A_b^-1 R_b^T v (the
+// batched level always carries the translation and three linear fields),
+// one warp per instance: lane u < 12 adds the instance's slots' value u in
+// slot order (four loads in flight), reads its row of the instance's block
+// of A_c^-1 (three 16-byte loads, issued before the slot sums are needed)
+// and forms its row of the product from the sums broadcast by shuffles.
+// Writes y into out[q * kInstCoarseW + off + u], or, with alpha (the
+// phase after A p), A_b^-1 R_b^T r_new = out[kCU] - alpha_b y into kCN.
+__device__ __forceinline__ void coarse_apply_inst(const BatchPlan& bp, const CoarseRegs& cr, const LocalInst* li,
+                                                  int nloc, int set, float* out, int off, int nwarps,
+                                                  bool with_alpha) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool mine = lane < 12;
+    for (int q = warp; q < nloc; q += nwarps) {
+        const LocalInst& L = li[q];
+        if (L.done) continue;
+        float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0, a2 = a0;
+        if (mine) {
+            const float4* A = reinterpret_cast<const float4*>(cr.ainv + (size_t)L.b * 144 + lane * 12);
+            a0 = __ldg(A);
+            a1 = __ldg(A + 1);
+            a2 = __ldg(A + 2);
+        }
+        float tot = 0.0f;
+        if (mine) {
+            int k = L.slot_lo;
+            for (; k + 4 <= L.slot_hi; k += 4) {
+                const float v0 = __ldcg(coarse_slot(bp, set, k) + lane), v1 = __ldcg(coarse_slot(bp, set, k + 1) + lane),
+                            v2 = __ldcg(coarse_slot(bp, set, k + 2) + lane), v3 = __ldcg(coarse_slot(bp, set, k + 3) + lane);
+                tot += v0;
+                tot += v1;
+                tot += v2;
+                tot += v3;
+            }
+            for (; k < L.slot_hi; ++k) tot += __ldcg(coarse_slot(bp, set, k) + lane);
+        }
+        const float a[12] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w};
+        float y = 0.0f;
+#pragma unroll
+        for (int u = 0; u < 12; ++u) y = fmaf(a[u], __shfl_sync(0xffffffffu, tot, u), y);
+        float* o = out + q * kInstCoarseW;
+        if (mine) {
+            if (with_alpha) o[kCN + lane] = fmaf(-L.alpha, y, o[kCU + lane]);
+            else o[off + lane] = y;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Streamed persistent kernel: rows are re-read from HBM every iteration.
 // Preconditioner: block-Jacobi, or (CO = 1: single instance, counter
@@ -1039,15 +1118,20 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
     // the step's inversion failed.  The CO = 0 builds keep the block-Jacobi
     // code alone, so both synchronisation modes compile to the same
     // arithmetic (bit-identical iterates)
-    const bool coarse = CO && !SYNC && bp.cg != nullptr && bp.cg->on && bp.cg->dense &&
+    const bool coarse = CO == 1 && !SYNC && bp.cg != nullptr && bp.cg->on && bp.cg->dense &&
                         *(volatile int*)bp.cg->fail == 0;
+    // batched coarse level (CO = 2 builds; zero-guess solves of several
+    // instances): one coarse block per instance
+    const bool coarse_b = CO == 2 && !SYNC && !warm && bp.cg != nullptr && bp.cg->on && bp.cg->batched &&
+                          *(volatile int*)bp.cg->fail == 0;
     __shared__ CoarseRegs creg;
-    if (threadIdx.x == 0) creg = coarse_regs(bp, coarse);  // ordered by the __syncthreads after init_local
+    if (threadIdx.x == 0) creg = coarse_regs(bp, coarse || coarse_b);  // ordered by the __syncthreads after init_local
     const int& c_U = creg.U;
     const int& c_nq = creg.nq;
     // the coarse block values behind the records, 16-byte aligned (float4 stores)
     float* c_vbuf = reinterpret_cast<float*>(
         (reinterpret_cast<uintptr_t>(li + bp.max_inst_per_cta) + 15) & ~static_cast<uintptr_t>(15));
+    float* c_inst = c_vbuf;  // the batched level's per-instance values ([nloc][kInstCoarseW]) in the same place
     unsigned target = 0;  // barrier target; the counter starts at 0 every solve
     int ph = 0;           // reduction phase (SYNC = 1 slot set ph % 3)
     if (threadIdx.x == 0) {
@@ -1059,11 +1143,23 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
     bool ok = true;
     auto no_step = [](LocalInst&, const double*) {};
     auto cw = [&](int i) { return c_nq == 4 ? __ldg(creg.w + i) : make_float4(0.f, 0.f, 0.f, 0.f); };
+    // coarse publication: the segments of the single-instance and batched
+    // levels, and scratch for the partial sums (s_red is idle between phases)
+    auto seg_cta = [&](int, int& lo, int& hi, int& slot) {
+        lo = 0;
+        hi = s1 - s0;
+        slot = li[0].own_slot;
+    };
+    auto seg_inst = [&](int q, int& lo, int& hi, int& slot) {
+        lo = li[q].seg_lo;
+        hi = li[q].seg_hi;
+        slot = li[q].own_slot;
+    };
+    float* c_tmp = reinterpret_cast<float*>(s_red);
     // one exchange phase carrying only the CTA's restriction of a vector;
     // leaves A_c^-1 R^T v (this block's U entries) in out
     auto coarse_exchange = [&](float* out) {
-        if (warp == 1) coarse_publish_cta(bp, c_U, spart, s1 - s0, li[0].own_slot, slot_set(ph), lane);
-        __syncthreads();
+        coarse_publish<BLOCK>(bp, c_U, spart, 1, seg_cta, slot_set(ph), c_tmp);
         const int set = slot_set(ph);
         CHYSX_BLOCK_PHASE(1, 5, false, no_step);
         if (!s_flag) coarse_apply_dense<BLOCK>(bp, creg, set, c_vbuf, out);
@@ -1084,6 +1180,22 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
         coarse_exchange(s_cb);
         ok = s_flag == 0;
     }
+    if (coarse_b) {
+        // every instance's A_b^-1 R_b^T b (the zero guess's r) into kCU
+        for (int s = s0 + warp; s < s1; s += W) {
+            const int i = s * 32 + lane;
+            const float3 b = i < t.n ? xyz(v.b[i]) : f3(0.f, 0.f, 0.f);
+            if (lane == 0) spart[(s - s0) * kSlotW] = 0.0;
+            warp_restrict(c_nq, b, i < t.n ? cw(i) : make_float4(0.f, 0.f, 0.f, 0.f), slice_cpart(spart, s - s0));
+        }
+        __syncthreads();
+        coarse_publish<BLOCK>(bp, c_U, spart, nloc, seg_inst, slot_set(ph), c_tmp);
+        const int set = slot_set(ph);
+        CHYSX_BLOCK_PHASE(1, 5, false, no_step);
+        if (!s_flag) coarse_apply_inst(bp, creg, li, nloc, set, c_inst, kCU, W, false);
+        __syncthreads();
+        ok = s_flag == 0;
+    }
     for (int s = s0 + warp; s < s1 && ok; s += W) {
         const int i = s * 32 + lane;
         float3 b = f3(0.f, 0.f, 0.f), zb = b, x0 = b, r = b, z = b;
@@ -1092,6 +1204,8 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             const S6 Mi = ld6(t.minv + (size_t)s * 192 + lane);
             zb = mul(Mi, b);
             if (coarse) zb = zb + coarse_prolong(c_nq, s_cb, cw(i));
+            if (coarse_b)
+                zb = zb + coarse_prolong(c_nq, c_inst + (bp.slice_inst[s] - il0) * kInstCoarseW + kCU, cw(i));
             r = b;
             z = zb;
             if (warm) {
@@ -1111,7 +1225,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                 r = b - ax;
                 z = mul(Mi, r);
                 v.r[i] = f4(r);
-            } else if (coarse) {
+            } else if (coarse || coarse_b) {
                 v.z[i] = f4(zb);
             }
         }
@@ -1207,6 +1321,8 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             const int i = s * 32 + lane;
             double sig = 0.0;
             float3 acc = f3(0.f, 0.f, 0.f);
+            // the coarse weights first: their load overlaps the row's
+            const float4 w4 = (coarse || coarse_b) && i < t.n ? cw(i) : make_float4(0.f, 0.f, 0.f, 0.f);
             if (!L.done && i < t.n) {
                 const bool first = L.iter == 0;
                 const float beta = L.beta;
@@ -1247,15 +1363,11 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             }
             sig = warp_sum(sig);
             if (lane == 0) spart[(s - s0) * kSlotW] = sig;
-            if (coarse)
-                warp_restrict(c_nq, acc, i < t.n ? cw(i) : make_float4(0.f, 0.f, 0.f, 0.f),
-                              slice_cpart(spart, s - s0));
+            if (coarse || coarse_b) warp_restrict(c_nq, acc, w4, slice_cpart(spart, s - s0));
         }
         __syncthreads();
-        if (coarse) {
-            if (warp == 1) coarse_publish_cta(bp, c_U, spart, s1 - s0, li[0].own_slot, slot_set(ph), lane);
-            __syncthreads();
-        }
+        if (coarse) coarse_publish<BLOCK>(bp, c_U, spart, 1, seg_cta, slot_set(ph), c_tmp);
+        if (coarse_b) coarse_publish<BLOCK>(bp, c_U, spart, nloc, seg_inst, slot_set(ph), c_tmp);
         const int set1 = slot_set(ph);
         // ndone only changes in the start and beta steps, i.e. never between
         // this barrier and the next, so every CTA takes the same exit decision
@@ -1271,13 +1383,20 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             if ((int)threadIdx.x < c_U) s_cn[threadIdx.x] = fmaf(-li[0].alpha, s_cw[threadIdx.x], s_cu[threadIdx.x]);
             __syncthreads();
         }
+        if (coarse_b) {
+            // per instance: A_b^-1 R_b^T r_new = A_b^-1 R_b^T r - alpha_b A_b^-1 R_b^T A p
+            coarse_apply_inst(bp, creg, li, nloc, set1, c_inst, 0, W, true);
+            __syncthreads();
+        }
 
         // phase 2: x += alpha p; r -= alpha Ap; z = M^-1 r (+ its coarse part)
         for (int s = s0 + warp; s < s1; s += W) {
-            const LocalInst& L = li[bp.slice_inst[s] - il0];
+            const int q = bp.slice_inst[s] - il0;
+            const LocalInst& L = li[q];
             const int i = s * 32 + lane;
             double rz = 0.0, rr = 0.0;
             float3 rn = f3(0.f, 0.f, 0.f);
+            const float4 w4 = (coarse || coarse_b) && i < t.n ? cw(i) : make_float4(0.f, 0.f, 0.f, 0.f);
             if (!L.done && i < t.n) {
                 const float alpha = L.alpha;
                 const float4 pi = ((L.iter & 1) ? v.p0 : v.p1)[i];
@@ -1285,7 +1404,8 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                 const float3 xn = f3(fmaf(alpha, pi.x, xi.x), fmaf(alpha, pi.y, xi.y), fmaf(alpha, pi.z, xi.z));
                 rn = f3(fmaf(-alpha, api.x, ri.x), fmaf(-alpha, api.y, ri.y), fmaf(-alpha, api.z, ri.z));
                 float3 zn = mul(ld6(t.minv + (size_t)s * 192 + lane), rn);
-                if (coarse) zn = zn + coarse_prolong(c_nq, s_cn, cw(i));
+                if (coarse) zn = zn + coarse_prolong(c_nq, s_cn, w4);
+                if (coarse_b) zn = zn + coarse_prolong(c_nq, c_inst + q * kInstCoarseW + kCN, w4);
                 v.x[i] = f4(xn);
                 v.r[i] = f4(rn);
                 v.z[i] = f4(zn);
@@ -1298,15 +1418,11 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                 spart[(s - s0) * kSlotW] = rz;
                 spart[(s - s0) * kSlotW + 1] = rr;
             }
-            if (coarse)
-                warp_restrict(c_nq, rn, i < t.n ? cw(i) : make_float4(0.f, 0.f, 0.f, 0.f),
-                              slice_cpart(spart, s - s0));
+            if (coarse || coarse_b) warp_restrict(c_nq, rn, w4, slice_cpart(spart, s - s0));
         }
         __syncthreads();
-        if (coarse) {
-            if (warp == 1) coarse_publish_cta(bp, c_U, spart, s1 - s0, li[0].own_slot, slot_set(ph), lane);
-            __syncthreads();
-        }
+        if (coarse) coarse_publish<BLOCK>(bp, c_U, spart, 1, seg_cta, slot_set(ph), c_tmp);
+        if (coarse_b) coarse_publish<BLOCK>(bp, c_U, spart, nloc, seg_inst, slot_set(ph), c_tmp);
         const int set2 = slot_set(ph);
         // phase 3: beta, iteration count, convergence
         CHYSX_BLOCK_PHASE(2, 5, false,
@@ -1317,6 +1433,10 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
         }
         // the coarse part restarts from R^T r_new (no recurrence drift)
         if (coarse) coarse_apply_dense<BLOCK>(bp, creg, set2, c_vbuf, s_cu);
+        if (coarse_b) {
+            coarse_apply_inst(bp, creg, li, nloc, set2, c_inst, kCU, W, false);
+            __syncthreads();
+        }
     }
     if (!ok) instances_fail(bp, li, nloc);
 }
