@@ -87,6 +87,7 @@ SIGNATURES = {
     "chysx_cloth_num_off_diag_blocks": (ctypes.c_int, [H, ip]),
     "chysx_cloth_debug_dump": (ctypes.c_int, [H, f32p, i32p, i32p, f32p, f32p, f32p]),
     "chysx_cloth_debug_coarse": (ctypes.c_int, [H, i32p, f32p, f32p, ctypes.c_int]),
+    "chysx_cloth_debug_coarse_rows": (ctypes.c_int, [H, i32p, ctypes.c_int, i32p]),
     "chysx_cloth_set_network": (ctypes.c_int, [H, f32p, ctypes.c_int]),
     "chysx_cloth_set_feature_output": (ctypes.c_int, [H, u, u]),
     "chysx_cloth_guess_kept": (ctypes.c_int, [H, ip]),
@@ -456,6 +457,16 @@ class Cloth:
         ainv = np.zeros((m, m), np.float32)
         check(self._L.chysx_cloth_debug_coarse(self.h, _p(info, i32p), _p(ac, f32p), _p(ainv, f32p), m * m))
         return d, ac, ainv
+
+    def debug_coarse_rows(self):
+        """First internal row of every coarse block of the last graph build
+        (blocks + 1 entries; empty without a coarse level)."""
+        n = np.zeros(1, np.int32)
+        check(self._L.chysx_cloth_debug_coarse_rows(self.h, None, 0, _p(n, i32p)))
+        rows = np.zeros(max(1, int(n[0])), np.int32)
+        if n[0]:
+            check(self._L.chysx_cloth_debug_coarse_rows(self.h, _p(rows, i32p), int(n[0]), _p(n, i32p)))
+        return rows[:int(n[0])]
 
 
 class Vbd:

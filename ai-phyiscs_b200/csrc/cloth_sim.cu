@@ -1029,18 +1029,34 @@ public:
                 }
         }
         if (ainv && coarse_batched_) {
-            // the batched level's block-diagonal inverse: one U x U block per instance
-            std::vector<float> blocks((size_t)coarse_nb_ * U * U);
-            ck(cudaMemcpy(blocks.data(), d_cainv_.get(), blocks.size() * sizeof(float), cudaMemcpyDeviceToHost),
+            // the batched level's inverse, block-diagonal by instance
+            const int ni = plan_.n_inst;
+            std::vector<int> ib(ni + 1), ao(ni + 1);
+            ck(cudaMemcpy(ib.data(), d_inst_blk_.get(), ib.size() * sizeof(int), cudaMemcpyDeviceToHost), "copy blocks");
+            ck(cudaMemcpy(ao.data(), d_inst_aoff_.get(), ao.size() * sizeof(int), cudaMemcpyDeviceToHost), "copy offsets");
+            std::vector<float> inv((size_t)std::max(1, ao[ni]));
+            ck(cudaMemcpy(inv.data(), d_cainv_.get(), (size_t)ao[ni] * sizeof(float), cudaMemcpyDeviceToHost),
                "copy A_c^-1 blocks");
             std::fill(ainv, ainv + (size_t)m * m, 0.0f);
-            for (int B = 0; B < coarse_nb_; ++B)
-                for (int r = 0; r < U; ++r)
-                    for (int c = 0; c < U; ++c)
-                        ainv[(size_t)(B * U + r) * m + B * U + c] = blocks[((size_t)B * U + r) * U + c];
+            for (int b = 0; b < ni; ++b) {
+                const int o = U * ib[b], mb = U * (ib[b + 1] - ib[b]);
+                for (int r = 0; r < mb; ++r)
+                    for (int c = 0; c < mb; ++c) ainv[(size_t)(o + r) * m + o + c] = inv[(size_t)ao[b] + (size_t)r * mb + c];
+            }
         } else if (ainv) {
             ck(cudaMemcpy(ainv, d_cainv_.get(), (size_t)m * m * sizeof(float), cudaMemcpyDeviceToHost), "copy A_c^-1");
         }
+    }
+    // The coarse blocks' first internal rows (nb + 1 entries, the last the
+    // row count rounded to slices); returns nb + 1 (0 without a coarse level).
+    int debug_coarse_rows(int32_t* row0, int cap) {
+        if (!coarse_on_) return 0;
+        const int n = coarse_nb_ + 1;
+        if (row0) {
+            if (cap < n) throw std::invalid_argument("debug_coarse_rows: cap below the block count + 1");
+            ck(cudaMemcpy(row0, d_cb_row0_.get(), (size_t)n * sizeof(int), cudaMemcpyDeviceToHost), "copy block rows");
+        }
+        return n;
     }
     void debug_dump(float* diag, int32_t* rp, int32_t* col, float* vals, float* rhs, float* dx) {
         const int n = topo_.n_ext;
@@ -1468,14 +1484,11 @@ private:
     // the coarse block of every slice and its first row, every block's sorted
     // list of the blocks its rows touch, and the list position of every ELL
     // entry's column block.
-    bool plan_coarse_with(int G, int nq, double shift) {
-        const int grid = plan_.grid, ns = topo_.n_slices;
-        const int nb = (grid + G - 1) / G, U = 3 * nq, m = U * nb;
-        if (m > kCoarseDenseMax) return false;
-        std::vector<int> slice_cb(std::max(1, ns), 0), row0(nb + 1, 0);
-        for (int c = 0; c < grid; ++c)
-            for (int sl = plan_.cta_slice[c]; sl < plan_.cta_slice[c + 1]; ++sl) slice_cb[sl] = c / G;
-        for (int B = 0; B <= nb; ++B) row0[B] = plan_.cta_slice[std::min(grid, B * G)] * 32;
+    // The coarse blocks' neighbour lists (every block a coarse row of A_c
+    // touches, itself included, sorted), the list position of every ELL
+    // entry's column block, and the block layout, uploaded; false (nothing
+    // uploaded) when a block touches more than kCoarseMaxNbr blocks.
+    bool coarse_neighbours(const std::vector<int>& slice_cb, const std::vector<int>& row0, int nb, int& mn) {
         std::vector<std::vector<int>> lists(nb);
         for (int B = 0; B < nb; ++B) {
             std::vector<int>& l = lists[B];
@@ -1486,7 +1499,7 @@ private:
             l.erase(std::unique(l.begin(), l.end()), l.end());
             if ((int)l.size() > kCoarseMaxNbr) return false;
         }
-        int mn = 1;
+        mn = 1;
         for (const auto& l : lists) mn = std::max(mn, (int)l.size());
         std::vector<int> nbr((size_t)nb * mn, -1), cnt(nb), self(nb);
         for (int B = 0; B < nb; ++B) {
@@ -1509,6 +1522,18 @@ private:
         d_ccnt_.upload(cnt);
         d_cself_.upload(self);
         d_ell_nbr_.upload(ell);
+        return true;
+    }
+    bool plan_coarse_with(int G, int nq, double shift) {
+        const int grid = plan_.grid, ns = topo_.n_slices;
+        const int nb = (grid + G - 1) / G, U = 3 * nq, m = U * nb;
+        if (m > kCoarseDenseMax) return false;
+        std::vector<int> slice_cb(std::max(1, ns), 0), row0(nb + 1, 0);
+        for (int c = 0; c < grid; ++c)
+            for (int sl = plan_.cta_slice[c]; sl < plan_.cta_slice[c + 1]; ++sl) slice_cb[sl] = c / G;
+        for (int B = 0; B <= nb; ++B) row0[B] = plan_.cta_slice[std::min(grid, B * G)] * 32;
+        int mn = 0;
+        if (!coarse_neighbours(slice_cb, row0, nb, mn)) return false;
         if (nq > 1) {
             d_cw_.resize((size_t)std::max(1, row0[nb]));
             d_cw_.zero();
@@ -1551,7 +1576,8 @@ private:
         if (plan_.n_inst != 1) {
             // several instances on the streamed kernel, zero-guess solves:
             // one coarse block per instance
-            if (!resident_ && warm_mode_ == CHYSX_WARM_ZERO) plan_coarse_batched();
+            if (!resident_ && warm_mode_ == CHYSX_WARM_ZERO && !plan_coarse_batched(kBatchMaxBlocks))
+                plan_coarse_batched(1);
             return;
         }
         if (!resident_) {
@@ -1572,24 +1598,50 @@ private:
         if (plan_.grid >= 8 && plan_coarse_with(kCoarseResidentCtas, 4, 0.0)) return;
         plan_coarse_with(1, 1, 0.0);
     }
-    // The batched coarse level of the streamed kernel: one coarse block per
-    // instance (its rows, translation and linear fields: 12 unknowns), so
-    // A_c is block-diagonal and each instance's 12 x 12 block is inverted
-    // on its own (coarse_invert_batched_kernel).
-    void plan_coarse_batched() {
-        const int nb = plan_.n_inst, ns = topo_.n_slices, nq = 4, U = 3 * nq, mn = 1;
-        std::vector<int> slice_cb(std::max(1, ns), 0), row0(nb + 1, 0);
-        for (int sl = 0; sl < ns; ++sl) slice_cb[sl] = plan_.slice_inst[sl];
-        for (int B = 0; B <= nb; ++B) row0[B] = plan_.inst_slice[B] * 32;
-        std::vector<int> nbr(nb), cnt(nb, 1), self(nb, 0);
-        for (int B = 0; B < nb; ++B) nbr[B] = B;
-        std::vector<unsigned char> ell(std::max<size_t>(1, topo_.col.size()), 0);
-        d_slice_cb_.upload(slice_cb);
-        d_cb_row0_.upload(row0);
-        d_cnbr_.upload(nbr);
-        d_ccnt_.upload(cnt);
-        d_cself_.upload(self);
-        d_ell_nbr_.upload(ell);
+    // The batched coarse level of the streamed kernel: coarse blocks inside
+    // instances, each a run of G_b consecutive segment slots of instance b
+    // (a segment: the instance's rows in one CTA), G_b the least that keeps
+    // at most kBatchMaxBlocks blocks per instance; translation and linear
+    // fields (12 unknowns) per block.  Blocks couple inside their instance
+    // only, so A_c is block-diagonal by instance and each instance's dense
+    // inverse (at most 96 unknowns) is formed on its own
+    // (coarse_invert_batched_kernel).  With max_blocks = 1: one block per
+    // instance.
+    bool plan_coarse_batched(int max_blocks) {
+        const int ni = plan_.n_inst, ns = topo_.n_slices, nq = 4, U = 3 * nq;
+        const int n_slots = plan_.inst_slot.back();
+        std::vector<int> blk_slot{0}, inst_blk(ni + 1, 0), inst_aoff(ni + 1, 0), slot_cb(std::max(1, n_slots), 0);
+        int mmax = U;
+        for (int b = 0; b < ni; ++b) {
+            const int lo = plan_.inst_slot[b], hi = plan_.inst_slot[b + 1];
+            const int G = std::max(1, (hi - lo + max_blocks - 1) / max_blocks);
+            for (int k = lo; k < hi; k += G) {
+                const int B = (int)blk_slot.size() - 1, k1 = std::min(hi, k + G);
+                for (int kk = k; kk < k1; ++kk) slot_cb[kk] = B;
+                blk_slot.push_back(k1);
+            }
+            inst_blk[b + 1] = (int)blk_slot.size() - 1;
+            const int m = U * (inst_blk[b + 1] - inst_blk[b]);
+            mmax = std::max(mmax, m);
+            inst_aoff[b + 1] = inst_aoff[b] + m * m;
+        }
+        const int nb = (int)blk_slot.size() - 1;
+        // a block's rows: from the first slice of its first segment (slot k of
+        // instance b is CTA inst_cta_lo[b] + k - inst_slot[b]) to the next block's
+        std::vector<int> row0(nb + 1, ns * 32), slice_cb(std::max(1, ns), 0);
+        for (int b = 0; b < ni; ++b)
+            for (int B = inst_blk[b]; B < inst_blk[b + 1]; ++B) {
+                const int c = plan_.inst_cta_lo[b] + blk_slot[B] - plan_.inst_slot[b];
+                row0[B] = std::max(plan_.cta_slice[c], plan_.inst_slice[b]) * 32;
+            }
+        for (int B = 0; B < nb; ++B)
+            for (int sl = row0[B] / 32; sl < row0[B + 1] / 32; ++sl) slice_cb[sl] = B;
+        int mn = 0;
+        if (!coarse_neighbours(slice_cb, row0, nb, mn)) return false;
+        d_blk_slot_.upload(blk_slot);
+        d_inst_blk_.upload(inst_blk);
+        d_inst_aoff_.upload(inst_aoff);
+        d_slot_cb_.upload(slot_cb);
         d_cw_.resize((size_t)std::max(1, row0[nb]));
         d_cw_.zero();
         d_cac_.resize((size_t)nb * mn * U * U);
@@ -1598,7 +1650,7 @@ private:
         for (int B = 0; B < nb; ++B) spb = std::max(spb, (row0[B + 1] - row0[B] + 31) / 32);
         const int splits = std::min(kCoarseMaxSplits, std::max(1, (spb + kCoarseSplitSlices - 1) / kCoarseSplitSlices));
         d_cacp_.resize((size_t)splits * nb * mn * U * U);
-        d_cainv_.resize((size_t)nb * U * U);
+        d_cainv_.resize((size_t)std::max(1, inst_aoff[ni]));
         d_cainv_.zero();
         d_cfail_.resize(1);
         d_cfail_.zero();
@@ -1612,11 +1664,16 @@ private:
         coarse_nq_ = nq;
         coarse_on_ = true;
         coarse_batched_ = true;
+        batched_mmax_ = mmax;
         const CoarseArgs cargs = coarse_args();
         d_cargs_.upload(&cargs, 1);
         ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_assemble_kernel),
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coarse_assemble_smem()),
            "cudaFuncSetAttribute(coarse assemble smem)");
+        ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(&coarse_invert_batched_kernel),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batched_invert_smem(mmax)),
+           "cudaFuncSetAttribute(batched coarse inverse smem)");
+        return true;
     }
     // the streamed kernel's shared memory for its coarse level: the block
     // values (dense level) or the per-instance values (batched level)
@@ -1650,6 +1707,10 @@ private:
         c.ainv = d_cainv_.get();
         c.dense = resident_ || coarse_batched_ ? 0 : 1;
         c.batched = coarse_batched_ ? 1 : 0;
+        c.blk_slot = coarse_batched_ ? d_blk_slot_.get() : nullptr;
+        c.inst_blk = coarse_batched_ ? d_inst_blk_.get() : nullptr;
+        c.inst_aoff = coarse_batched_ ? d_inst_aoff_.get() : nullptr;
+        c.slot_cb = coarse_batched_ ? d_slot_cb_.get() : nullptr;
         c.shift = coarse_shift_;
         c.work = d_cwork_.get();
         c.fail = d_cfail_.get();
@@ -1907,12 +1968,13 @@ private:
                 mp.width = 1;
                 ck(cudaGraphAddMemsetNode(&z2, graph_, &z1, 1, &mp), "add coarse fail reset node");
                 if (coarse_batched_) {
-                    // one CTA per instance: its 12 x 12 block of A_c
+                    // one CTA per instance: the dense inverse of its coarse blocks
                     void* ab[] = {&cg};
                     cudaKernelNodeParams pb{};
                     pb.func = reinterpret_cast<void*>(&coarse_invert_batched_kernel);
-                    pb.gridDim = dim3(coarse_nb_);
+                    pb.gridDim = dim3(plan_.n_inst);
                     pb.blockDim = dim3(kBatchInvThreads);
+                    pb.sharedMemBytes = (unsigned)batched_invert_smem(batched_mmax_);
                     pb.kernelParams = ab;
                     ck(cudaGraphAddKernelNode(&n2, graph_, &z2, 1, &pb), "add batched coarse invert node");
                 } else {
@@ -2222,6 +2284,8 @@ private:
     bool coarse_on_ = false;
     int coarse_nb_ = 0, coarse_mn_ = 0, coarse_g_ = 1, coarse_nq_ = 1, coarse_splits_ = 1;
     bool coarse_batched_ = false;  // the streamed kernel's per-instance level (plan_coarse_batched)
+    int batched_mmax_ = 0;         // its largest per-instance inverse
+    DevBuf<int> d_blk_slot_, d_inst_blk_, d_inst_aoff_, d_slot_cb_;
     double coarse_shift_ = 0.0;
     DevBuf<int> d_slice_cb_, d_cb_row0_, d_cnbr_, d_ccnt_, d_cself_;
     DevBuf<unsigned char> d_ell_nbr_;
@@ -2523,6 +2587,13 @@ int chysx_cloth_debug_dump(chysx_cloth* h, float* diag, int32_t* rp, int32_t* co
 int chysx_cloth_debug_coarse(chysx_cloth* h, int32_t* info, float* ac, float* ainv, int cap) {
     CHYSX_H(h);
     return guard([&] { h->sim.debug_coarse(info, ac, ainv, cap); });
+}
+int chysx_cloth_debug_coarse_rows(chysx_cloth* h, int32_t* row0, int cap, int32_t* count) {
+    CHYSX_H(h);
+    return guard([&] {
+        if (!count) throw std::invalid_argument("debug_coarse_rows: null count");
+        *count = h->sim.debug_coarse_rows(row0, cap);
+    });
 }
 
 int chysx_cloth_set_network(chysx_cloth* h, const float* params, int n_params) {

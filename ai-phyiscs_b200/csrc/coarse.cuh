@@ -227,61 +227,83 @@ __global__ void __launch_bounds__(288) coarse_assemble_kernel(DevTopo t, CoarseA
     }
 }
 
-// Inverse of the block-diagonal A_c of the batched coarse level (one coarse
-// block per instance): one CTA per instance adds the assembly's splits of
-// its U x U block in order and rounds them once to FP32 (the stored A_c),
+// Inverse of the block-diagonal A_c of the batched coarse level: one CTA
+// per instance b builds the dense m_b x m_b matrix of its coarse blocks
+// (m_b = U x blocks <= U kBatchMaxBlocks) from their block rows, adding the
+// assembly's splits in order and rounding once to FP32 (the stored A_c),
 // scales by S = diag^-1/2, shifts by ca.shift I and inverts by Gauss-Jordan
-// without pivoting in FP64 shared memory (one entry per thread, two
-// buffers, one CTA barrier per pivot); an unknown whose field has zero
-// weight on the whole instance gets an identity row.  Output S W S (FP32)
-// into ca.ainv[b][U][U]; a non-positive pivot sets ca.fail (the level is
-// then off in the step's solve).
-constexpr int kBatchInvThreads = 160;  // >= 12 x 12 entries
+// without pivoting in FP64 shared memory (per pivot the pivot row and column
+// are copied aside, then every entry updated: two CTA barriers per pivot);
+// an unknown whose field has zero weight on its whole block gets an identity
+// row.  Output S W S (FP32) into ca.ainv + ca.inst_aoff[b]; a non-positive
+// pivot sets ca.fail (the level is then off in the step's solve).  Dynamic
+// shared memory: batched_invert_smem(max m_b) bytes.
+constexpr int kBatchInvThreads = 256;
+__host__ __device__ constexpr size_t batched_invert_smem(int m) {
+    return ((size_t)m * (m + 1) + 3 * (size_t)m) * sizeof(double);
+}
 __global__ void __launch_bounds__(kBatchInvThreads) coarse_invert_batched_kernel(CoarseArgs ca) {
-    constexpr int kU = 12;
-    __shared__ double a[2][kU][kU + 1];
-    __shared__ double s_sc[kU];
-    const int B = blockIdx.x, U = 3 * ca.nq, tid = threadIdx.x;
-    const int r = tid / U, c = tid % U;
-    const bool mine = tid < U * U;
-    const size_t base = (size_t)B * U * U, total = (size_t)ca.nb * U * U;
-    if (mine) {
+    extern __shared__ double inv_s[];
+    const int b = blockIdx.x, U = 3 * ca.nq, mn = ca.max_nbr, tid = threadIdx.x;
+    const int B0 = ca.inst_blk[b], nbk = ca.inst_blk[b + 1] - B0, m = U * nbk, ld = m + 1;
+    double* a = inv_s;
+    double* prow = a + (size_t)m * ld;
+    double* pcol = prow + m;
+    double* s_sc = pcol + m;
+    const size_t total = (size_t)ca.nb * mn * U * U;
+    for (int x = tid; x < m * ld; x += kBatchInvThreads) a[x] = 0.0;
+    __syncthreads();
+    for (int e = tid; e < nbk * mn * U * U; e += kBatchInvThreads) {
+        const int Bl = e / (mn * U * U), rem = e % (mn * U * U), k = rem / (U * U), rc = rem % (U * U);
+        const int B = B0 + Bl;
+        if (k >= ca.nbr_cnt[B]) continue;
+        const int C = ca.nbr[(size_t)B * mn + k] - B0;  // blocks couple inside their instance only
+        const size_t src = ((size_t)B * mn + k) * U * U + rc;
         double v = 0.0;
-        for (int z = 0; z < ca.splits; ++z) v += __ldcg(ca.acp + (size_t)z * total + base + tid);
+        for (int z = 0; z < ca.splits; ++z) v += __ldcg(ca.acp + (size_t)z * total + src);
         const float vf = (float)v;
-        ca.ac[base + tid] = vf;
-        a[0][r][c] = (double)vf;
+        ca.ac[src] = vf;
+        a[(size_t)(Bl * U + rc / U) * ld + C * U + rc % U] = (double)vf;
     }
     __syncthreads();
-    if (tid < U) {
-        const double d = a[0][tid][tid];
-        s_sc[tid] = d > 0.0 ? 1.0 / sqrt(d) : 0.0;
+    for (int i = tid; i < m; i += kBatchInvThreads) {
+        const double d = a[(size_t)i * ld + i];
+        s_sc[i] = d > 0.0 ? 1.0 / sqrt(d) : 0.0;
     }
     __syncthreads();
-    if (mine) {
-        const double si = s_sc[r], sj = s_sc[c];
-        a[0][r][c] = si == 0.0 || sj == 0.0 ? (r == c ? 1.0 : 0.0) : a[0][r][c] * si * sj + (r == c ? ca.shift : 0.0);
+    for (int x = tid; x < m * m; x += kBatchInvThreads) {
+        const int i = x / m, j = x % m;
+        const double si = s_sc[i], sj = s_sc[j];
+        double& v = a[(size_t)i * ld + j];
+        v = si == 0.0 || sj == 0.0 ? (i == j ? 1.0 : 0.0) : v * si * sj + (i == j ? ca.shift : 0.0);
     }
     __syncthreads();
-    int cur = 0;
     bool bad = false;
-    for (int k = 0; k < U; ++k) {
-        const double p = a[cur][k][k];
+    for (int k = 0; k < m; ++k) {
+        const double p = a[(size_t)k * ld + k];
         const bool good = p > 1.0e-12;
         bad = bad || !good;
         const double ip = good ? 1.0 / p : 0.0;
-        if (mine) {
-            // row k: (c == k ? 1 : a_kc) / p; the others subtract a_rk times it
-            const double rk = (c == k ? 1.0 : a[cur][k][c]) * ip;
-            a[cur ^ 1][r][c] = r == k ? rk : fma(-a[cur][r][k], rk, c == k ? 0.0 : a[cur][r][c]);
+        for (int x = tid; x < m; x += kBatchInvThreads) {
+            prow[x] = a[(size_t)k * ld + x];
+            pcol[x] = a[(size_t)x * ld + k];
         }
         __syncthreads();
-        cur ^= 1;
+        // row k: (j == k ? 1 : a_kj) / p; the others subtract a_ik times it
+        for (int x = tid; x < m * m; x += kBatchInvThreads) {
+            const int i = x / m, j = x % m;
+            const double rk = (j == k ? 1.0 : prow[j]) * ip;
+            double& v = a[(size_t)i * ld + j];
+            v = i == k ? rk : fma(-pcol[i], rk, j == k ? 0.0 : v);
+        }
+        __syncthreads();
     }
     if (bad && tid == 0) atomicExch(ca.fail, 1);
-    if (mine) {
-        const double vv = a[cur][r][c] * s_sc[r] * s_sc[c];
-        ca.ainv[base + tid] = (bad || !isfinite(vv)) ? 0.0f : (float)vv;
+    float* out = ca.ainv + ca.inst_aoff[b];
+    for (int x = tid; x < m * m; x += kBatchInvThreads) {
+        const int i = x / m, j = x % m;
+        const double vv = a[(size_t)i * ld + j] * s_sc[i] * s_sc[j];
+        out[x] = (bad || !isfinite(vv)) ? 0.0f : (float)vv;
     }
 }
 

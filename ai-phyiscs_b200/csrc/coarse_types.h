@@ -38,6 +38,10 @@ constexpr int kCoarseMaxSplits = 32;
 // usable preconditioner (the solve stalls).  The shift bounds the scaled
 // condition number near 3e5 and still leaves an SPD coarse correction.
 constexpr double kCoarseShift = 1.0e-5;
+// The streamed kernel's coarse level for batches: at most this many coarse
+// blocks per instance (each an instance's rows in one CTA, or a run of such
+// segments), so an instance's dense inverse has at most 96 unknowns.
+constexpr int kBatchMaxBlocks = 8;
 
 // Coarse space: coarse block B is the rows of CTAs [B G, (B + 1) G) of the
 // plan; its fields are the translation (weight 1) and, with nq = 4, the
@@ -73,10 +77,16 @@ struct CoarseArgs {
     // (the coarse level then adds nothing in that step's solve); dense = 1:
     // the streamed kernel's level (its CTAs read their rows from L2)
     int dense = 0;
-    // batched = 1: the streamed kernel's level for several instances, one
-    // coarse block per instance (A_c block-diagonal; ainv holds each
-    // instance's U x U inverse, [nb][U][U])
+    // batched = 1: the streamed kernel's level for several instances.  Its
+    // coarse blocks are runs of an instance's segment slots (the rows one
+    // CTA holds of it), at most kBatchMaxBlocks per instance, so A_c is
+    // block-diagonal by instance; ainv holds each instance's dense inverse
+    // (m_b x m_b, m_b = U x its blocks) at inst_aoff[b]
     int batched = 0;
+    const int* blk_slot = nullptr;            // [nb + 1] first segment slot of every coarse block
+    const int* inst_blk = nullptr;            // [n_inst + 1] first coarse block of every instance
+    const int* inst_aoff = nullptr;           // [n_inst + 1] offset of every instance's inverse in ainv
+    const int* slot_cb = nullptr;             // [n_slots] coarse block of every segment slot
     double shift = 0.0;
     double* work = nullptr;
     int* fail = nullptr;

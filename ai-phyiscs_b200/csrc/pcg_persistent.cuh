@@ -393,12 +393,14 @@ __device__ __forceinline__ bool warp0_phase(const BatchPlan& bp, const double* s
 // invalidates L1, so a field read through bp.cg after a barrier would put an
 // L2 round trip on the phase's critical path.
 struct CoarseRegs {
-    const float* ainv;  // [blocks][U][m] rows of A_c^-1
+    const float* ainv;  // [blocks][U][m] rows of A_c^-1 (batched level: per-instance inverses)
     const float4* w;    // per-row field weights (nq = 4)
     int nq, U, G, m;    // fields, values per block, CTAs per block, unknowns
+    // the batched level's block layout (CoarseArgs)
+    const int *blk_slot, *inst_blk, *inst_aoff, *slot_cb;
 };
 __device__ __forceinline__ CoarseRegs coarse_regs(const BatchPlan& bp, bool on) {
-    CoarseRegs c{nullptr, nullptr, 1, 3, 1, 0};
+    CoarseRegs c{nullptr, nullptr, 1, 3, 1, 0, nullptr, nullptr, nullptr, nullptr};
     if (on) {
         c.ainv = bp.cg->ainv;
         c.w = bp.cg->w;
@@ -406,6 +408,10 @@ __device__ __forceinline__ CoarseRegs coarse_regs(const BatchPlan& bp, bool on) 
         c.U = 3 * bp.cg->nq;
         c.G = bp.cg->g;
         c.m = bp.cg->m;
+        c.blk_slot = bp.cg->blk_slot;
+        c.inst_blk = bp.cg->inst_blk;
+        c.inst_aoff = bp.cg->inst_aoff;
+        c.slot_cb = bp.cg->slot_cb;
     }
     return c;
 }
@@ -1034,55 +1040,82 @@ __device__ __forceinline__ void coarse_apply_dense(const BatchPlan& bp, const Co
     __syncthreads();
 }
 
-// ---- batched coarse level of the streamed kernel: one coarse block per
-// instance, so A_c is block-diagonal and an instance's coarse values ride
-// on its own reduction slots.  Per local instance the CTA keeps
-// kInstCoarseW floats: A_b^-1 R_b^T r (kCU) and of the new r (kCN).
+// ---- batched coarse level of the streamed kernel: coarse blocks inside
+// instances (an instance's rows in one CTA, or a run of such segments), so
+// A_c is block-diagonal by instance and a block's coarse values ride on its
+// segments' own reduction slots.  Per local instance the CTA keeps
+// kInstCoarseW floats for its own block: A_b^-1 R_b^T r (kCU) and of the
+// new r (kCN).
 constexpr int kInstCoarseW = 24, kCU = 0, kCN = 12;
-// Each unfinished local instance's 12 values of y = A_b^-1 R_b^T v (the
-// batched level always carries the translation and three linear fields),
-// one warp per instance: lane u < 12 adds the instance's slots' value u in
-// slot order (four loads in flight), reads its row of the instance's block
-// of A_c^-1 (three 16-byte loads, issued before the slot sums are needed)
-// and forms its row of the product from the sums broadcast by shuffles.
-// Writes y into out[q * kInstCoarseW + off + u], or, with alpha (the
-// phase after A p), A_b^-1 R_b^T r_new = out[kCU] - alpha_b y into kCN.
+static_assert(kBatchMaxBlocks * 12 <= 96, "coarse_apply_inst: three coarse values per lane");
+// Sums over a warp's lanes of 16 values per lane by recursive halving (16
+// shuffles): value k's total lands in lanes 2k and 2k + 1.
+__device__ __forceinline__ float warp_sum16(const float (&a)[16]) {
+    const int lane = threadIdx.x & 31;
+    float b8[8], b4[4], b2[2];
+    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4, h2 = lane & 2;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        b8[k] = (h16 ? a[k + 8] : a[k]) + __shfl_xor_sync(0xffffffffu, h16 ? a[k] : a[k + 8], 16);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        b4[k] = (h8 ? b8[k + 4] : b8[k]) + __shfl_xor_sync(0xffffffffu, h8 ? b8[k] : b8[k + 4], 8);
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+        b2[k] = (h4 ? b4[k + 2] : b4[k]) + __shfl_xor_sync(0xffffffffu, h4 ? b4[k] : b4[k + 2], 4);
+    float b1 = (h2 ? b2[1] : b2[0]) + __shfl_xor_sync(0xffffffffu, h2 ? b2[0] : b2[1], 2);
+    b1 += __shfl_xor_sync(0xffffffffu, b1, 1);
+    return b1;
+}
+
+// Each unfinished local instance's 12 values of y = (A_b^-1 R_b^T v) on the
+// CTA's own coarse block (the batched level always carries the translation
+// and three linear fields), one warp per instance: lane l takes the
+// instance's coarse values j = l, l + 32, l + 64 (< m_b = 12 x its blocks),
+// each the sum of its block's segment slots in slot order, multiplies them
+// with the own block's 12 rows of the instance's A_b^-1 (coalesced rows
+// from L2) and the warp adds the 12 products by recursive halving.  Writes
+// y into out[q * kInstCoarseW + off + u], or, with alpha (the phase after
+// A p), A_b^-1 R_b^T r_new = out[kCU] - alpha_b y into kCN.
 __device__ __forceinline__ void coarse_apply_inst(const BatchPlan& bp, const CoarseRegs& cr, const LocalInst* li,
                                                   int nloc, int set, float* out, int off, int nwarps,
                                                   bool with_alpha) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const bool mine = lane < 12;
     for (int q = warp; q < nloc; q += nwarps) {
         const LocalInst& L = li[q];
         if (L.done) continue;
-        float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0, a2 = a0;
-        if (mine) {
-            const float4* A = reinterpret_cast<const float4*>(cr.ainv + (size_t)L.b * 144 + lane * 12);
-            a0 = __ldg(A);
-            a1 = __ldg(A + 1);
-            a2 = __ldg(A + 2);
-        }
-        float tot = 0.0f;
-        if (mine) {
-            int k = L.slot_lo;
-            for (; k + 4 <= L.slot_hi; k += 4) {
-                const float v0 = __ldcg(coarse_slot(bp, set, k) + lane), v1 = __ldcg(coarse_slot(bp, set, k + 1) + lane),
-                            v2 = __ldcg(coarse_slot(bp, set, k + 2) + lane), v3 = __ldcg(coarse_slot(bp, set, k + 3) + lane);
-                tot += v0;
-                tot += v1;
-                tot += v2;
-                tot += v3;
-            }
-            for (; k < L.slot_hi; ++k) tot += __ldcg(coarse_slot(bp, set, k) + lane);
-        }
-        const float a[12] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w};
-        float y = 0.0f;
+        const int B0 = cr.inst_blk[L.b], m = 12 * (cr.inst_blk[L.b + 1] - B0);
+        const int ob = cr.slot_cb[L.own_slot] - B0;
+        const float* A = cr.ainv + cr.inst_aoff[L.b] + (size_t)(12 * ob) * m;
+        float c[3];
 #pragma unroll
-        for (int u = 0; u < 12; ++u) y = fmaf(a[u], __shfl_sync(0xffffffffu, tot, u), y);
+        for (int t = 0; t < 3; ++t) {
+            const int j = lane + 32 * t;
+            float sum = 0.0f;
+            if (j < m) {
+                const int jb = j / 12, u = j - 12 * jb;
+                const int k1 = cr.blk_slot[B0 + jb + 1];
+                for (int k = cr.blk_slot[B0 + jb]; k < k1; ++k) sum += __ldcg(coarse_slot(bp, set, k) + u);
+            }
+            c[t] = sum;
+        }
+        float prod[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) prod[r] = 0.0f;
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            const int j = lane + 32 * t;
+            if (j < m) {
+#pragma unroll
+                for (int r = 0; r < 12; ++r) prod[r] = fmaf(__ldg(A + (size_t)r * m + j), c[t], prod[r]);
+            }
+        }
+        const float y = warp_sum16(prod);
+        const int u = lane >> 1;
         float* o = out + q * kInstCoarseW;
-        if (mine) {
-            if (with_alpha) o[kCN + lane] = fmaf(-L.alpha, y, o[kCU + lane]);
-            else o[off + lane] = y;
+        if ((lane & 1) == 0 && u < 12) {
+            if (with_alpha) o[kCN + u] = fmaf(-L.alpha, y, o[kCU + u]);
+            else o[off + u] = y;
         }
     }
 }

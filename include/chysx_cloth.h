@@ -277,6 +277,11 @@ int chysx_cloth_debug_dump(chysx_cloth* h, float* diag, int32_t* row_offsets,
  * block-diagonal), unknown
  * index block * 3 * fields + 3 * field + component.  Synchronises. */
 int chysx_cloth_debug_coarse(chysx_cloth* h, int32_t* info, float* ac, float* ainv, int cap);
+/* The coarse blocks' first internal rows of the last graph build (test
+ * support, no counterpart in the reference): *count = blocks + 1 (0 without
+ * a coarse level); with row0 non-null (cap >= *count entries) the rows, the
+ * last one the internal row count rounded up to whole 32-row slices. */
+int chysx_cloth_debug_coarse_rows(chysx_cloth* h, int32_t* row0, int cap, int32_t* count);
 
 /* Learned warm start (no counterpart in the reference).  A per-vertex
  * network (20 1-ring features -> 3 x 64 GELU -> dv, BF16 on tensor cores)

@@ -78,6 +78,7 @@ def lib():
         L.orc_vbd_hinge_angle.argtypes = [_f64p]
         L.orc_vbd_hinge_angle.restype = ctypes.c_double
         L.orc_set_preconditioner.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.orc_set_coarse_bounds.argtypes = [vp, ctypes.c_void_p, ctypes.c_int]
         L.orc_add_static_plane.argtypes = [vp, _f32p, ctypes.c_float]
         L.orc_coarse_system.argtypes = [vp, ctypes.c_void_p]
         L.orc_add_static_box.argtypes = [vp, _f32p, _f32p, _f32p, _f32p, _f32p]
@@ -249,6 +250,16 @@ class OracleCloth:
         c = {False: 0, True: 1, "translation": 1, "linear": 2}[coarse]
         _check(self._L.orc_set_preconditioner(self._h, int(degree), float(ratio), int(block_rows), c,
                                               int(coarse_rows)))
+
+    def set_coarse_bounds(self, bounds=None):
+        """Explicit coarse blocks: their first rows (increasing from 0, the
+        last entry n or more) instead of blocks of coarse_rows rows; None
+        goes back to those."""
+        if bounds is None:
+            _check(self._L.orc_set_coarse_bounds(self._h, None, 0))
+            return
+        b = np.ascontiguousarray(bounds, np.int32)
+        _check(self._L.orc_set_coarse_bounds(self._h, b.ctypes.data_as(ctypes.c_void_p), int(b.size)))
 
     def coarse_system(self):
         """A_c of the last solve with the coarse level (dense, float64)."""

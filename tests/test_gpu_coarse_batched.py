@@ -1,10 +1,12 @@
-"""GPU: the streamed kernel's coarse level for batches (one coarse block per
-instance: its translation and linear fields, A_c block-diagonal, each 12 x 12
-block inverted on its own) on zero-guess solves of several instances: the
-converged states against the block-Jacobi batch and the FP64 oracle, the
-iteration counts against the oracle's restatement of the same operator per
-instance, the per-instance inverse blocks against the exact inverses of the
-device's own blocks, and bitwise repeatability."""
+"""GPU: the streamed kernel's coarse level for batches (coarse blocks inside
+instances, one per CTA segment of an instance or a run of them, at most 8 per
+instance: translation and linear fields, A_c block-diagonal by instance, each
+instance's dense inverse formed on its own) on zero-guess solves of several
+instances: the converged states against the block-Jacobi batch and the FP64
+oracle, the iteration counts against the oracle's restatement of the same
+operator on the device's blocks per instance, the per-instance inverses
+against the exact inverses of the device's own matrices, and bitwise
+repeatability."""
 import numpy as np
 import pytest
 
@@ -38,10 +40,29 @@ def batch(sc, offs, pc=True, warm="zero", tol=1e-7):
     return g
 
 
+def inst_rows(offs):
+    """First internal row of every instance (each starts on a fresh 32-row
+    slice), and the padded total."""
+    n = np.diff(np.asarray(offs, np.int64))
+    return np.concatenate([[0], np.cumsum((n + 31) // 32 * 32)])
+
+
+def inst_bounds(g, offs):
+    """Per instance, the device's coarse block starts relative to the
+    instance's first row (ending with its row count)."""
+    rows = g.sim.debug_coarse_rows()
+    r0 = inst_rows(offs)
+    out = []
+    for b in range(len(offs) - 1):
+        starts = [int(r) - int(r0[b]) for r in rows[:-1] if r0[b] <= r < r0[b + 1]]
+        out.append(starts + [int(offs[b + 1] - offs[b])])
+    return out
+
+
 def oracle_inst(sc, tol, state, coarse):
-    """One instance's step from `state` in the FP64 oracle; `coarse`: the
-    restatement of the batched level (block-Jacobi plus one coarse block of
-    translation and linear fields over all of the instance's rows)."""
+    """One instance's step from `state` in the FP64 oracle; `coarse`: None,
+    or the restatement of the batched level on the given block starts
+    (block-Jacobi plus translation and linear fields per block)."""
     n = sc["pos"].shape[0]
     s = O.OracleCloth(True)
     s.set_material(sc["density"], sc.get("damping", 0.0), sc["gravity"])
@@ -55,8 +76,9 @@ def oracle_inst(sc, tol, state, coarse):
     s.set_pins(sc["pin_idx"], sc["pin_targets"], sc.get("k_pin", 1e6))
     s.set_state(state[0], state[1], im)
     s.set_solver(400000, tol, "zero")
-    if coarse:
-        s.set_preconditioner(0, 60.0, 512, "linear", ((n + 31) // 32) * 32)
+    if coarse is not None:
+        s.set_preconditioner(0, 60.0, 512, "linear", 0)
+        s.set_coarse_bounds(coarse)
     return s
 
 
@@ -73,19 +95,22 @@ def test_batched_coarse_matches_oracle_and_its_iterations():
         it, rr, st = g.sim.instance_stats()
         assert (st == capi.SOLVE_CONVERGED).all() and (rr <= 1e-7).all()
         pos = g.positions()
+        bounds = inst_bounds(g, offs)
         for b, s in enumerate(inst):
             a, e = int(offs[b]), int(offs[b + 1])
             state = (p0[a:e], v0[a:e])
-            o = oracle_inst(s, 1e-11, state, coarse=False)
+            o = oracle_inst(s, 1e-11, state, coarse=None)
             o.step(s["dt"])
             errs.append(float(np.abs(pos[a:e] - o.state()[0]).max()))
             if step > 0:  # from rest the first step converges in a handful of iterations
-                c = oracle_inst(s, 1e-7, state, coarse=True)
+                c = oracle_inst(s, 1e-7, state, coarse=bounds[b])
                 c.step(s["dt"])
                 ci = c.stats()[0]
                 if abs(int(it[b]) - ci) > 0.25 * ci + 3:
                     bad.append((step, b, int(it[b]), ci))
-    print(f"batched two-level: max|dx| vs FP64 {max(errs):.3g}, iteration mismatches {bad}")
+    print(f"batched two-level: blocks per instance {[len(x) - 1 for x in bounds]}, max|dx| vs FP64 "
+          f"{max(errs):.3g}, iteration mismatches {bad}")
+    assert max(len(x) - 1 for x in bounds) > 1  # blocks inside instances
     assert max(errs) < 1e-5
     assert not bad
 
@@ -117,7 +142,7 @@ def test_batched_coarse_cuts_iterations():
 
 def _oracle_step(s, p0, v0, offs, b):
     a, e = int(offs[b]), int(offs[b + 1])
-    o = oracle_inst(s, 1e-11, (p0[a:e], v0[a:e]), coarse=False)
+    o = oracle_inst(s, 1e-11, (p0[a:e], v0[a:e]), coarse=None)
     o.step(s["dt"])
     return o.state()[0]
 
@@ -128,11 +153,17 @@ def test_batched_coarse_inverse_blocks():
     for _ in range(2):
         g.step()
     info, ac, ainv = g.sim.debug_coarse()
-    assert (info["on"], info["fields"], info["blocks"]) == (1, 4, 5)
+    rows = g.sim.debug_coarse_rows()
+    assert (info["on"], info["fields"], info["blocks"]) == (1, 4, len(rows) - 1)
+    r0 = inst_rows(offs)
+    nblk = [int(((rows[:-1] >= r0[b]) & (rows[:-1] < r0[b + 1])).sum()) for b in range(5)]
+    assert sum(nblk) == info["blocks"] and 1 <= max(nblk) <= 8
+    first = np.concatenate([[0], np.cumsum(nblk)])
     for b in range(5):
-        sl = slice(12 * b, 12 * b + 12)
+        sl = slice(12 * first[b], 12 * first[b + 1])
         A = ac[sl, sl].astype(np.float64)
-        assert np.all(ac[sl, :12 * b] == 0) and np.all(ac[sl, 12 * b + 12:] == 0)
+        assert np.all(ac[sl, :sl.start] == 0) and np.all(ac[sl, sl.stop:] == 0)
+        assert np.all(ainv[sl, :sl.start] == 0) and np.all(ainv[sl, sl.stop:] == 0)
         keep = np.diag(A) != 0
         Ak = A[np.ix_(keep, keep)]
         inv = np.linalg.inv(Ak + 1e-5 * np.diag(np.diag(Ak)))

@@ -66,3 +66,28 @@ def test_block_jacobi_with_the_coarse_level():
     assert b.stats()[0] < 0.75 * a.stats()[0]  # 638 against 1140 here (strips of the caller order)
     with pytest.raises(ValueError):
         b.set_preconditioner(4, 30.0, 256)  # even degree
+
+
+def test_explicit_coarse_bounds_restate_fixed_blocks_and_accept_ragged_ones():
+    """Explicit coarse block starts (the device's batched blocks, one per CTA
+    segment of an instance): bounds equal to fixed 512-row blocks give the
+    same coarse system and iterations; ragged bounds converge to the same
+    solution; bad bounds are rejected."""
+    sc = scenes.config_large(side=40, steps=2)
+    n = sc["pos"].shape[0]
+    a, b, c = oracle_sim(sc, 1e-10), oracle_sim(sc, 1e-10), oracle_sim(sc, 1e-10)
+    a.set_preconditioner(0, 60.0, 512, coarse="linear", coarse_rows=512)
+    b.set_preconditioner(0, 60.0, 512, coarse="linear", coarse_rows=0)
+    b.set_coarse_bounds(list(range(0, n, 512)) + [n])
+    c.set_preconditioner(0, 60.0, 512, coarse="linear", coarse_rows=0)
+    c.set_coarse_bounds([0, 96, 800, 832, n + 20])  # ragged; the last start past n ends the list
+    for s in (a, b, c):
+        s.step(sc["dt"])
+        assert s.stats()[2] == 0
+    np.testing.assert_array_equal(a.coarse_system(), b.coarse_system())
+    assert a.stats()[0] == b.stats()[0]
+    assert c.coarse_system().shape[0] <= 36  # three blocks
+    assert np.abs(c.state()[0] - a.state()[0]).max() < 1e-8
+    for bad in ([1, 5, n], [0, 10, 10, n], [0]):
+        with pytest.raises(ValueError):
+            c.set_coarse_bounds(bad)
