@@ -372,7 +372,9 @@ int chysx_cloth_instance_stats(chysx_cloth* h, int n, int* iterations, double* r
  * in registers when the system fits (default), 1 = CUDA-graph WHILE loop of
  * two kernels per iteration, 2 = the streamed persistent kernel forced.
  * block (0, 128, 256, 512) and grid (0 = automatic) size the streamed
- * persistent kernel. */
+ * persistent kernel; block 0 lets the planner choose (128 for batches that
+ * get the coarse level, whose blocks are the instances' CTA segments, else
+ * 256). */
 int chysx_cloth_set_tuning(chysx_cloth* h, int solver_path, int block, int grid);
 /* Synchronisation of the persistent PCG kernels (no counterpart in the
  * reference): 0 = one grid-wide counter barrier per reduction (default),
