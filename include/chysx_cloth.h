@@ -273,8 +273,8 @@ int chysx_cloth_debug_dump(chysx_cloth* h, float* diag, int32_t* row_offsets,
  * with ac / ainv non-null (host, m * m floats each, cap >= m * m) the coarse
  * matrix A_c dense and the inverse the solver used (of A_c + shift
  * diag(A_c), shift 0 on the register-resident kernel, 1e-5 on the streamed
- * one; for the batched level, blocks = instances and the inverse is
- * block-diagonal), unknown
+ * one; for the batched level the inverse is block-diagonal by instance),
+ * unknown
  * index block * 3 * fields + 3 * field + component.  Synchronises. */
 int chysx_cloth_debug_coarse(chysx_cloth* h, int32_t* info, float* ac, float* ainv, int cap);
 /* The coarse blocks' first internal rows of the last graph build (test
@@ -435,9 +435,10 @@ int chysx_cloth_row_of_particles(const chysx_cloth* h, int n, int32_t* rows);
  * block-Jacobi plus the coarse level on blocks of about 5120 rows, A_c
  * shifted by 1e-5 diag(A_c) (single instance, synchronisation mode 0); on
  * batches of instances there (zero-guess solves, synchronisation mode 0),
- * block-Jacobi plus one coarse block per instance (its translation and
- * linear fields; A_c block-diagonal, each instance's 12 x 12 block inverted
- * on its own, same shift).
+ * block-Jacobi plus coarse blocks inside the instances (an instance's rows in
+ * one CTA, or runs of such segments, at most 8 per instance; translation and
+ * linear fields; A_c block-diagonal by instance, each instance's dense
+ * inverse formed on its own, same shift).
  * in_use reports what the last graph build uses (0 block-Jacobi, 1 local,
  * 2 two-level with translations, 3 two-level with translations and linear
  * fields). */
