@@ -1355,7 +1355,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             double sig = 0.0;
             float3 acc = f3(0.f, 0.f, 0.f);
             // the coarse weights first: their load overlaps the row's
-            const float4 w4 = (coarse || coarse_b) && !L.done && i < t.n ? cw(i) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 w4 = (coarse || (coarse_b && !L.done)) && i < t.n ? cw(i) : make_float4(0.f, 0.f, 0.f, 0.f);
             if (!L.done && i < t.n) {
                 const bool first = L.iter == 0;
                 const float beta = L.beta;
@@ -1396,8 +1396,8 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             }
             sig = warp_sum(sig);
             if (lane == 0) spart[(s - s0) * kSlotW] = sig;
-            // (a finished instance's restriction is never read: left out)
-            if ((coarse || coarse_b) && !L.done) warp_restrict(c_nq, acc, w4, slice_cpart(spart, s - s0));
+            // (a finished instance's restriction is never read: left out of batches)
+            if (coarse || (coarse_b && !L.done)) warp_restrict(c_nq, acc, w4, slice_cpart(spart, s - s0));
         }
         __syncthreads();
         if (coarse) coarse_publish<BLOCK>(bp, c_U, spart, 1, seg_cta, slot_set(ph), c_tmp);
@@ -1430,7 +1430,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
             const int i = s * 32 + lane;
             double rz = 0.0, rr = 0.0;
             float3 rn = f3(0.f, 0.f, 0.f);
-            const float4 w4 = (coarse || coarse_b) && !L.done && i < t.n ? cw(i) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 w4 = (coarse || (coarse_b && !L.done)) && i < t.n ? cw(i) : make_float4(0.f, 0.f, 0.f, 0.f);
             if (!L.done && i < t.n) {
                 const float alpha = L.alpha;
                 const float4 pi = ((L.iter & 1) ? v.p0 : v.p1)[i];
@@ -1452,7 +1452,7 @@ pcg_persistent_kernel(DevTopo t, Vecs v, BatchPlan bp, SolverCfg cfg, int warm, 
                 spart[(s - s0) * kSlotW] = rz;
                 spart[(s - s0) * kSlotW + 1] = rr;
             }
-            if ((coarse || coarse_b) && !L.done) warp_restrict(c_nq, rn, w4, slice_cpart(spart, s - s0));
+            if (coarse || (coarse_b && !L.done)) warp_restrict(c_nq, rn, w4, slice_cpart(spart, s - s0));
         }
         __syncthreads();
         if (coarse) coarse_publish<BLOCK>(bp, c_U, spart, 1, seg_cta, slot_set(ph), c_tmp);
