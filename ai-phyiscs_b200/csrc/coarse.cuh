@@ -290,11 +290,13 @@ __global__ void __launch_bounds__(kBatchInvThreads) coarse_invert_batched_kernel
         }
         __syncthreads();
         // row k: (j == k ? 1 : a_kj) / p; the others subtract a_ik times it
-        for (int x = tid; x < m * m; x += kBatchInvThreads) {
-            const int i = x / m, j = x % m;
+        // (warp w takes rows w, w + 8, ..., lane l columns l, l + 32, ...)
+        for (int j = tid & 31; j < m; j += 32) {
             const double rk = (j == k ? 1.0 : prow[j]) * ip;
-            double& v = a[(size_t)i * ld + j];
-            v = i == k ? rk : fma(-pcol[i], rk, j == k ? 0.0 : v);
+            for (int i = tid >> 5; i < m; i += kBatchInvThreads / 32) {
+                double& v = a[(size_t)i * ld + j];
+                v = i == k ? rk : fma(-pcol[i], rk, j == k ? 0.0 : v);
+            }
         }
         __syncthreads();
     }
