@@ -1400,6 +1400,12 @@ private:
                        ? reinterpret_cast<const void*>(&pcg_resident_kernel<16, kResidentMaxWidth, SYNC>)
                        : reinterpret_cast<const void*>(&pcg_resident_kernel<8, kResidentMaxWidth, SYNC>);
         }
+        if (pcg_block_ == 64) {
+            // the planner's choice for batches with the coarse level only (synchronisation mode 0)
+            if (SYNC != 0) throw std::logic_error("64-thread streamed kernel without synchronisation mode 0");
+            if (coarse_on_ && coarse_batched_) return reinterpret_cast<const void*>(&pcg_persistent_kernel<64, 0, 2>);
+            return reinterpret_cast<const void*>(&pcg_persistent_kernel<64, 0, 0>);
+        }
         if (coarse_on_ && SYNC == 0 && coarse_batched_) {
             if (pcg_block_ == 128) return reinterpret_cast<const void*>(&pcg_persistent_kernel<128, 0, 2>);
             if (pcg_block_ == 512) return reinterpret_cast<const void*>(&pcg_persistent_kernel<512, 0, 2>);
@@ -1607,7 +1613,7 @@ private:
     // at most kBatchMaxBlocks blocks per instance; translation and linear
     // fields (12 unknowns) per block.  Blocks couple inside their instance
     // only, so A_c is block-diagonal by instance and each instance's dense
-    // inverse (at most 96 unknowns) is formed on its own
+    // inverse (at most 144 unknowns) is formed on its own
     // (coarse_invert_batched_kernel).  With max_blocks = 1: one block per
     // instance.
     bool plan_coarse_batched(int max_blocks) {
@@ -1737,7 +1743,7 @@ private:
             // the same time per iteration); otherwise 256
             const bool batched_coarse = pc_kind_ == 2 && sync_mode_ == 0 && warm_mode_ == CHYSX_WARM_ZERO &&
                                         topo_.inst_slice.size() > 2;
-            pcg_block_ = batched_coarse ? 128 : 256;
+            pcg_block_ = batched_coarse ? 64 : 256;
         }
         const int W = pcg_block_ / 32;
         const int n_slices = std::max(1, topo_.n_slices);

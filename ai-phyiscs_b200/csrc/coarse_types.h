@@ -40,8 +40,8 @@ constexpr int kCoarseMaxSplits = 32;
 constexpr double kCoarseShift = 1.0e-5;
 // The streamed kernel's coarse level for batches: at most this many coarse
 // blocks per instance (each an instance's rows in one CTA, or a run of such
-// segments), so an instance's dense inverse has at most 96 unknowns.
-constexpr int kBatchMaxBlocks = 8;
+// segments), so an instance's dense inverse has at most 144 unknowns.
+constexpr int kBatchMaxBlocks = 12;
 
 // Coarse space: coarse block B is the rows of CTAs [B G, (B + 1) G) of the
 // plan; its fields are the translation (weight 1) and, with nq = 4, the

@@ -1047,7 +1047,7 @@ __device__ __forceinline__ void coarse_apply_dense(const BatchPlan& bp, const Co
 // kInstCoarseW floats for its own block: A_b^-1 R_b^T r (kCU) and of the
 // new r (kCN).
 constexpr int kInstCoarseW = 24, kCU = 0, kCN = 12;
-static_assert(kBatchMaxBlocks * 12 <= 96, "coarse_apply_inst: three coarse values per lane");
+static_assert(kBatchMaxBlocks * 12 <= 160, "coarse_apply_inst: five coarse values per lane");
 // Sums over a warp's lanes of 16 values per lane by recursive halving (16
 // shuffles): value k's total lands in lanes 2k and 2k + 1.
 __device__ __forceinline__ float warp_sum16(const float (&a)[16]) {
@@ -1071,7 +1071,7 @@ __device__ __forceinline__ float warp_sum16(const float (&a)[16]) {
 // Each unfinished local instance's 12 values of y = (A_b^-1 R_b^T v) on the
 // CTA's own coarse block (the batched level always carries the translation
 // and three linear fields), one warp per instance: lane l takes the
-// instance's coarse values j = l, l + 32, l + 64 (< m_b = 12 x its blocks),
+// instance's coarse values j = l, l + 32, ... (< m_b = 12 x its blocks),
 // each the sum of its block's segment slots in slot order, multiplies them
 // with the own block's 12 rows of the instance's A_b^-1 (coalesced rows
 // from L2) and the warp adds the 12 products by recursive halving.  Writes
@@ -1087,9 +1087,9 @@ __device__ __forceinline__ void coarse_apply_inst(const BatchPlan& bp, const Coa
         const int B0 = cr.inst_blk[L.b], m = 12 * (cr.inst_blk[L.b + 1] - B0);
         const int ob = cr.slot_cb[L.own_slot] - B0;
         const float* A = cr.ainv + cr.inst_aoff[L.b] + (size_t)(12 * ob) * m;
-        float c[3];
+        float c[5];
 #pragma unroll
-        for (int t = 0; t < 3; ++t) {
+        for (int t = 0; t < 5; ++t) {
             const int j = lane + 32 * t;
             float sum = 0.0f;
             if (j < m) {
@@ -1103,7 +1103,7 @@ __device__ __forceinline__ void coarse_apply_inst(const BatchPlan& bp, const Coa
 #pragma unroll
         for (int r = 0; r < 16; ++r) prod[r] = 0.0f;
 #pragma unroll
-        for (int t = 0; t < 3; ++t) {
+        for (int t = 0; t < 5; ++t) {
             const int j = lane + 32 * t;
             if (j < m) {
 #pragma unroll

@@ -624,7 +624,7 @@ def run_ours(args, rank, world, local_rank):
     cinfo = g.sim.debug_coarse()[0] if int(g.sim.preconditioner()[3]) >= 2 else None
     coarse_rows = int(cinfo["ctas_per_block"]) * int(g.sim.solver_info()[2]) if cinfo else 0
     if cinfo and offs is not None:
-        coarse_rows = "blocks inside instances: one per CTA segment, at most 8 per instance"
+        coarse_rows = "blocks inside instances: one per CTA segment, at most 12 per instance"
     if cinfo and g.sim.solver_info()[0] == "resident" and coarse_rows != COARSE_ROWS:
         print(f"warning: device coarse blocks of {coarse_rows} rows, CPU legs use {COARSE_ROWS}", file=sys.stderr)
 

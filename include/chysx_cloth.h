@@ -372,9 +372,9 @@ int chysx_cloth_instance_stats(chysx_cloth* h, int n, int* iterations, double* r
  * in registers when the system fits (default), 1 = CUDA-graph WHILE loop of
  * two kernels per iteration, 2 = the streamed persistent kernel forced.
  * block (0, 128, 256, 512) and grid (0 = automatic) size the streamed
- * persistent kernel; block 0 lets the planner choose (128 for batches that
- * get the coarse level, whose blocks are the instances' CTA segments, else
- * 256). */
+ * persistent kernel; block 0 lets the planner choose (64-thread CTAs, a
+ * build of its own, for batches that get the coarse level, whose blocks are
+ * the instances' CTA segments; else 256). */
 int chysx_cloth_set_tuning(chysx_cloth* h, int solver_path, int block, int grid);
 /* Synchronisation of the persistent PCG kernels (no counterpart in the
  * reference): 0 = one grid-wide counter barrier per reduction (default),
@@ -436,7 +436,7 @@ int chysx_cloth_row_of_particles(const chysx_cloth* h, int n, int32_t* rows);
  * shifted by 1e-5 diag(A_c) (single instance, synchronisation mode 0); on
  * batches of instances there (zero-guess solves, synchronisation mode 0),
  * block-Jacobi plus coarse blocks inside the instances (an instance's rows in
- * one CTA, or runs of such segments, at most 8 per instance; translation and
+ * one CTA, or runs of such segments, at most 12 per instance; translation and
  * linear fields; A_c block-diagonal by instance, each instance's dense
  * inverse formed on its own, same shift).
  * in_use reports what the last graph build uses (0 block-Jacobi, 1 local,

@@ -157,7 +157,7 @@ def test_batched_coarse_inverse_blocks():
     assert (info["on"], info["fields"], info["blocks"]) == (1, 4, len(rows) - 1)
     r0 = inst_rows(offs)
     nblk = [int(((rows[:-1] >= r0[b]) & (rows[:-1] < r0[b + 1])).sum()) for b in range(5)]
-    assert sum(nblk) == info["blocks"] and 1 <= max(nblk) <= 8
+    assert sum(nblk) == info["blocks"] and 1 <= max(nblk) <= 12
     first = np.concatenate([[0], np.cumsum(nblk)])
     for b in range(5):
         sl = slice(12 * first[b], 12 * first[b + 1])
